@@ -1,0 +1,19 @@
+"""aldic_b200 -- the AL-DIC hot path (integer search, IC-GN, ADMM Subproblems 1
+and 2) as sm_100a CUDA kernels behind a C ABI (include/aldic_b200.h), with
+this host package mirroring the reference MATLAB functions by name.
+
+The package directory is ``2d_aldic_b200``; import it with
+``importlib.import_module("2d_aldic_b200")``.
+"""
+from .api import (ALDIC, FP32, FP64, Context, IntegerSearch, Init, LocalICGN, MeshSetUp, Subpb1,
+                  Subpb2, ba_interp2, default_context, funGlobal_NodalStrainAvg, funICGN,
+                  funICGN_Subpb1, funImgGradient, funIntegerSearch, funNormalizeImg,
+                  funSmoothDisp, funSmoothStrain, gridfit_springs, inpaint_nans, local_icgn)
+from ._lib import AldicError, exported_symbols
+from . import synth
+
+__all__ = ["ALDIC", "FP32", "FP64", "Context", "IntegerSearch", "Init", "LocalICGN", "MeshSetUp",
+           "Subpb1", "Subpb2", "ba_interp2", "default_context", "funGlobal_NodalStrainAvg",
+           "funICGN", "funICGN_Subpb1", "funImgGradient", "funIntegerSearch", "funNormalizeImg",
+           "funSmoothDisp", "funSmoothStrain", "gridfit_springs", "inpaint_nans", "local_icgn",
+           "AldicError", "exported_symbols", "synth"]

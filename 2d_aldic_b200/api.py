@@ -1,0 +1,612 @@
+"""Reference-named host API over the C ABI (libaldic_b200.so).
+
+Every function keeps the name, argument meaning and return values of the
+reference MATLAB function it replaces (jyang526843/2D_ALDIC, cited per
+function), so code written against the reference's frame loop can call these
+one for one.  Layout conventions follow the reference after ReadImage's
+transpose: an image Img(x, y) of W x H is a numpy array of shape (H, W)
+(x fastest); U is interleaved [u1 v1 u2 v2 ...]; F is [F11 F21 F12 F22] per
+node; coordinatesFEM is n x 2; HtempPar / HPar is n x 21.
+
+Arrays may be numpy (host) arrays or CUDA torch tensors; outputs follow the
+inputs (CUDA inputs give CUDA outputs, computed without host round trips).
+All arithmetic runs in the sm_100a kernels -- there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import threading
+import time
+from typing import Any
+
+import numpy as np
+
+from . import _lib
+from ._lib import AldicError, FrameParams, FrameStats, call
+
+try:  # torch is optional for host callers
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+U8, U16, F32, F64 = 0, 1, 2, 3
+FP32, FP64 = 0, 1
+_DT = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.float32): F32,
+       np.dtype(np.float64): F64}
+
+
+# ------------------------------------------------------------------ arrays
+def _is_cuda(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if _is_cuda(a):
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)
+
+
+def _prep(a, dtype=np.float64):
+    """numpy -> contiguous array of dtype; CUDA tensor -> contiguous tensor."""
+    if a is None:
+        return None
+    if _is_cuda(a):
+        tdt = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32,
+               np.uint8: torch.uint8, np.uint16: torch.uint16}[np.dtype(dtype).type]
+        return a.to(tdt).contiguous()
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+def _empty(like, shape, dtype=np.float64):
+    if like is not None and _is_cuda(like):
+        tdt = {np.float64: torch.float64, np.float32: torch.float32,
+               np.int32: torch.int32}[np.dtype(dtype).type]
+        return torch.empty(shape, dtype=tdt, device=like.device)
+    return np.empty(shape, dtype=dtype)
+
+
+def _first_cuda(*arrs):
+    for a in arrs:
+        if _is_cuda(a):
+            return a
+    return None
+
+
+# ------------------------------------------------------------------ context
+class Context:
+    """A device context: images, gradients and work buffers resident on one
+    GPU across calls (the MEX-session state of the reference's loop)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        call("aldic_ctx_create", int(device), C.byref(h))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().aldic_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        """Use an existing CUDA stream (torch.cuda.Stream or raw handle)."""
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        call("aldic_ctx_set_stream", self.h, C.c_void_p(handle))
+
+    # -- images
+    def set_ref(self, img, roi=None, mask=None):
+        H, W = img.shape
+        dt = _dtype_code(img)
+        r = (C.c_int * 4)(*roi) if roi is not None else None
+        m = _prep(mask) if mask is not None else None
+        call("aldic_set_ref", self.h, _ptr(_contig(img)), dt, W, H, r, _ptr(m))
+
+    def set_def(self, img):
+        call("aldic_set_def", self.h, _ptr(_contig(img)), _dtype_code(img))
+
+    def set_fields(self, f=None, g=None, dfdx=None, dfdy=None, shape=None):
+        ref = next(a for a in (f, g, dfdx, dfdy) if a is not None)
+        H, W = ref.shape if shape is None else shape
+        args = [_prep(a) for a in (f, g, dfdx, dfdy)]
+        call("aldic_set_fields", self.h, *[_ptr(a) for a in args], W, H)
+
+    def get_images(self, W, H, like=None):
+        out = [_empty(like, (H, W)) for _ in range(4)]
+        st = np.empty(4)
+        call("aldic_get_images", self.h, *[_ptr(o) for o in out], _ptr(st))
+        return (*out, st)
+
+
+def _contig(a):
+    if _is_cuda(a):
+        return a.contiguous()
+    return np.ascontiguousarray(a)
+
+
+def _dtype_code(img) -> int:
+    if _is_cuda(img):
+        m = {torch.uint8: U8, torch.uint16: U16, torch.float32: F32, torch.float64: F64}
+        return m[img.dtype]
+    return _DT[np.asarray(img).dtype]
+
+
+_ctx_lock = threading.Lock()
+_ctxs: dict[int, Context] = {}
+
+
+def default_context(device: int | None = None) -> Context:
+    if device is None:
+        device = torch.cuda.current_device() if torch is not None and torch.cuda.is_available() else 0
+    with _ctx_lock:
+        if device not in _ctxs:
+            _ctxs[device] = Context(device)
+        return _ctxs[device]
+
+
+def _ctx_for(*arrs) -> Context:
+    t = _first_cuda(*arrs)
+    return default_context(t.device.index if t is not None else None)
+
+
+# ------------------------------------------------------------------ a3
+def ba_interp2(F, X, Y, method: str = "cubic"):
+    """Z = ba_interp2(F, X, Y, [method]) -- ba_interp2.cpp:318-335.
+
+    F is MATLAB's M x N (x P) column-major image: pass the numpy array of
+    shape (N, M) or (P, N, M) (its transpose in C order).  X indexes columns
+    (N) and Y rows (M), 1-based; the method string is ignored (cubic only, as
+    in the reference).  All of F, X, Y must be float64 or all float32."""
+    dt = (F.dtype if not _is_cuda(F) else {torch.float64: np.float64, torch.float32: np.float32}[F.dtype])
+    dt = np.dtype(dt)
+    if dt not in (np.dtype(np.float64), np.dtype(np.float32)):
+        raise TypeError("ba_interp2 takes only double or single arguments for IMG,X,Y, and all "
+                        "must have the same class")
+    for a in (X, Y):
+        adt = a.dtype if not _is_cuda(a) else {torch.float64: np.float64, torch.float32: np.float32}.get(a.dtype)
+        if np.dtype(adt) != dt:
+            raise TypeError("ba_interp2 takes only double or single arguments for IMG,X,Y, and "
+                            "all must have the same class")
+    if tuple(X.shape) != tuple(Y.shape):
+        raise ValueError("X, Y should have the same size")
+    Fc, Xc, Yc = _contig(F), _contig(X), _contig(Y)
+    if Fc.ndim == 2:
+        Pn, N, M = 1, Fc.shape[0], Fc.shape[1]
+    else:
+        Pn, N, M = Fc.shape
+    n = int(np.prod(X.shape)) if not _is_cuda(X) else X.numel()
+    out = _empty(_first_cuda(F, X, Y), (Pn,) + tuple(X.shape), dt.type)
+    fn = "aldic_ba_interp2_f64" if dt == np.dtype(np.float64) else "aldic_ba_interp2_f32"
+    stream = None
+    if _first_cuda(F, X, Y) is not None:
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    call(fn, _ptr(Fc), M, N, Pn, _ptr(Xc), _ptr(Yc), n, _ptr(out), stream)
+    return out[0] if Pn == 1 else out
+
+
+# ------------------------------------------------------------------ a1/a2
+def funNormalizeImg(Img, gridxyROIRange):
+    """[ImgNormalized, gridxyROIRange] = funNormalizeImg(Img, gridxyROIRange)
+    -- funNormalizeImg.m:1.  Img is a list of (H, W) images."""
+    gx = list(gridxyROIRange["gridx"])
+    gy = list(gridxyROIRange["gridy"])
+    H, W = Img[0].shape
+    gx = [max(gx[0], 1), min(gx[1], W)]
+    gy = [max(gy[0], 1), min(gy[1], H)]
+    ctx = _ctx_for(*Img)
+    out = []
+    for im in Img:
+        o = _empty(_first_cuda(im), (H, W))
+        call("aldic_normalize", ctx.h, _ptr(_contig(im)), _dtype_code(im), W, H,
+             (C.c_int * 4)(gx[0], gx[1], gy[0], gy[1]), _ptr(o), None)
+        out.append(o)
+    return out, {"gridx": gx, "gridy": gy}
+
+
+def funImgGradient(ImgRef, ImgDef=None, ImgRefMask=None):
+    """Df = funImgGradient(ImgRef, ImgDef, [ImgRefMask]) -- funImgGradient.m:1.
+    Returns a dict with DfDx, DfDy ((H-6) x (W-6), i.e. MATLAB's
+    (W-6) x (H-6)), DfCropWidth = 3, DfAxis and imgSize = (W, H)."""
+    H, W = ImgRef.shape
+    f = _prep(ImgRef)
+    m = _prep(ImgRefMask) if ImgRefMask is not None else None
+    gx = _empty(_first_cuda(f), (H, W))
+    gy = _empty(_first_cuda(f), (H, W))
+    call("aldic_gradient", _ctx_for(f).h, _ptr(f), W, H, _ptr(m), _ptr(gx), _ptr(gy))
+    return {"DfDx": gx[3:H - 3, 3:W - 3], "DfDy": gy[3:H - 3, 3:W - 3], "DfCropWidth": 3,
+            "DfAxis": [4, W - 3, 4, H - 3], "imgSize": (W, H),
+            "ImgRefMask": ImgRefMask if ImgRefMask is not None else None}
+
+
+def _df_full(Df, shape, like):
+    H, W = shape
+    if _is_cuda(like):
+        fx = torch.zeros((H, W), dtype=torch.float64, device=like.device)
+        fy = torch.zeros_like(fx)
+    else:
+        fx = np.zeros((H, W))
+        fy = np.zeros((H, W))
+    fx[3:H - 3, 3:W - 3] = Df["DfDx"]
+    fy[3:H - 3, 3:W - 3] = Df["DfDy"]
+    return fx, fy
+
+
+def _load_fields(ctx, ImgRef, ImgDef, Df):
+    H, W = ImgRef.shape
+    fx, fy = _df_full(Df, (H, W), ImgRef)
+    ctx.set_fields(ImgRef, ImgDef, fx, fy)
+
+
+# ------------------------------------------------------------------ a4/a5
+def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winstepsize,
+                     tempNoOfInitPt=0, *varargin, qfactors: bool = True, ctx: Context | None = None):
+    """[x,y,u,v,cc] = funIntegerSearch(f,g,tempSizeOfSearchRegion,gridx,gridy,
+    winsize,winstepsize,0,winstepsize) -- funIntegerSearch.m:3 (whole field).
+
+    f, g: images (H, W); integer images (uint8/uint16) give exact correlation
+    maps.  Returns x, y, u, v as ny x nx arrays and cc = {'max': ...,
+    'qfactors': n x 2}."""
+    if tempNoOfInitPt != 0:
+        raise NotImplementedError("only the whole-field search (tempNoOfInitPt = 0) is on the "
+                                  "GPU path; the seed-point mode is interactive in the reference")
+    s = tempSizeOfSearchRegion
+    s = [int(s), int(s)] if np.ndim(s) == 0 else [int(s[0]), int(s[1])]
+    ctx = ctx or _ctx_for(f, g)
+    H, W = f.shape
+    if _dtype_code(f) in (U8, U16):
+        ctx.set_ref(f)
+        ctx.set_def(g)
+    else:
+        ctx.set_fields(_prep(f), _prep(g), _zeros_like_img(f), _zeros_like_img(f))
+    gxa = (C.c_int * 2)(int(gridx[0]), int(gridx[-1]))
+    gya = (C.c_int * 2)(int(gridy[0]), int(gridy[-1]))
+    sa = (C.c_int * 2)(*s)
+    nx, ny = C.c_int(), C.c_int()
+    call("aldic_search_dims", W, H, gxa, gya, int(winsize), int(winstepsize), sa, C.byref(nx),
+         C.byref(ny))
+    nx, ny = nx.value, ny.value
+    like = _first_cuda(f, g)
+    outs = [_empty(like, (nx, ny)) for _ in range(5)]  # column-major ny x nx
+    q = _empty(like, (2, nx * ny)) if qfactors else None
+    call("aldic_int_search", ctx.h, gxa, gya, int(winsize), int(winstepsize), sa,
+         *[_ptr(o) for o in outs], _ptr(q))
+    x, y, u, v, cmax = (o.T for o in outs)
+    cc = {"max": cmax, "qfactors": q.T if q is not None else None, "A": []}
+    return x, y, u, v, cc
+
+
+def _zeros_like_img(f):
+    if _is_cuda(f):
+        return torch.zeros(f.shape, dtype=torch.float64, device=f.device)
+    return np.zeros(f.shape)
+
+
+def IntegerSearch(ImgRef, ImgDef, file_name, DICpara):
+    """[DICpara,x0,y0,u,v,cc] = IntegerSearch(ImgRef,ImgDef,file_name,DICpara)
+    -- IntegerSearch.m:1, non-interactive: the search zone comes from
+    DICpara['SizeOfFFTSearchRegion'] instead of input() and only the whole-
+    field method (InitFFTSearchMethod = 1) is available."""
+    s = DICpara.get("SizeOfFFTSearchRegion")
+    if s is None:
+        raise ValueError("DICpara['SizeOfFFTSearchRegion'] is required (the reference asks "
+                         "for it interactively)")
+    roi = DICpara["gridxyROIRange"]
+    x0, y0, u, v, cc = funIntegerSearch(ImgRef, ImgDef, s, roi["gridx"], roi["gridy"],
+                                        DICpara["winsize"], DICpara["winstepsize"], 0,
+                                        DICpara["winstepsize"])
+    mask = DICpara.get("ImgRefMask")
+    if mask is not None:  # IntegerSearch.m:68-73
+        xi = np.asarray(x0, int).ravel() - 1
+        yi = np.asarray(y0, int).ravel() - 1
+        hole = np.asarray(mask)[yi, xi].reshape(np.shape(x0)).astype(float)
+        hole[hole == 0] = np.nan
+        u = u * hole
+        v = v * hole
+    return DICpara, x0, y0, u, v, cc
+
+
+# ------------------------------------------------------------------ a6
+def MeshSetUp(x, y, DICpara):
+    """DICmesh = MeshSetUp(x, y, DICpara) -- MeshSetUp.m:23-39, 80-89."""
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    N, M = x.shape  # N vertical (y), M horizontal (x)
+    xt, yt = x.T, y.T
+    coords = np.stack([xt.ravel(order="F"), yt.ravel(order="F")], axis=1)
+    j, i = np.meshgrid(np.arange(1, N), np.arange(1, M), indexing="ij")
+    i, j = i.ravel(), j.ravel()
+    elems = np.stack([(j - 1) * M + i, (j - 1) * M + i + 1, j * M + i + 1, j * M + i], axis=1)
+    H = DICpara.get("ImgSize", (0, 0))[1]
+    return {"coordinatesFEM": coords, "elementsFEM": elems.astype(np.int64), "dirichlet": [],
+            "neumann": [], "x0": xt, "y0": yt, "M": M, "N": N,
+            "y0World": H + 1 - yt,
+            "coordinatesFEMWorld": np.stack([coords[:, 0], H + 1 - coords[:, 1]], axis=1)}
+
+
+def Init(u, v, Phi, x, y, index=0):
+    """U0 = Init(u, v, Phi, x, y, 0) -- Init.m:13,168-179: NaNs filled by the
+    4-neighbour spring inpainting (inpaint_nans method 4, on the GPU), then
+    interleaved x-fastest."""
+    if index != 0:
+        raise NotImplementedError("Init index 1 (outlier spring test) is not on the GPU path")
+    u = np.array(u, np.float64)
+    v = np.array(v, np.float64)
+    ny, nx = u.shape
+    z = np.stack([u.ravel(), v.ravel()])  # row-major (ny, nx) == x fastest
+    call("aldic_inpaint_springs", default_context().h, nx, ny, 2, _ptr(z))
+    U0 = np.empty(2 * nx * ny)
+    U0[0::2] = z[0]
+    U0[1::2] = z[1]
+    return U0
+
+
+# ------------------------------------------------------------------ a7/a8
+def _winsize_arr(winsize, n, like):
+    if np.ndim(winsize) == 0:
+        return None, int(winsize)
+    return _prep(np.asarray(winsize, np.int32) if not _is_cuda(winsize) else winsize, np.int32), 0
+
+
+def local_icgn(ctx: Context, coords, U0, winsize, tol, precision=FP32):
+    """Batch funICGN over every node on the images resident in ctx.  Returns
+    U (2n), F (4n), ConvItPerEle (n), HtempPar (n x 21)."""
+    cf = _coords_cm(coords)
+    n = cf.shape[-1] if not _is_cuda(cf) else cf.shape[-1]
+    like = _first_cuda(coords, U0)
+    U0p = _prep(U0)
+    wa, w = _winsize_arr(winsize, n, like)
+    U = _empty(like, (2 * n,))
+    F = _empty(like, (4 * n,))
+    it = _empty(like, (n,), np.int32)
+    Hp = _empty(like, (21, n))
+    call("aldic_icgn", ctx.h, _ptr(cf), n, _ptr(U0p), _ptr(wa), w, float(tol), int(precision),
+         _ptr(U), _ptr(F), _ptr(it), _ptr(Hp))
+    return U, F, it, Hp.T
+
+
+def _coords_cm(coords):
+    """n x 2 coordinatesFEM -> column-major [x1..xn y1..yn] buffer of shape (2, n)."""
+    if _is_cuda(coords):
+        return coords.to(torch.float64).t().contiguous()
+    return np.ascontiguousarray(np.asarray(coords, np.float64).reshape(-1, 2).T)
+
+
+def funICGN(U0, x0, y0, Df, ImgRef, ImgDef, winsize, tol, ICGNmethod="GaussNewton"):
+    """[U,F,stepwithinwhile,HGlobal] = funICGN(U0,x0,y0,Df,ImgRef,ImgDef,
+    winsize,tol,ICGNmethod) -- funICGN.m:1 for one subset (FP64)."""
+    _check_method(ICGNmethod)
+    ctx = _ctx_for(ImgRef)
+    _load_fields(ctx, ImgRef, ImgDef, Df)
+    U, F, it, Hp = local_icgn(ctx, np.array([[x0, y0]], float), np.asarray(U0, float)[:2],
+                              winsize, tol, FP64)
+    return U, F, int(it[0]), np.asarray(Hp)[0]
+
+
+def _check_method(m):
+    if m not in ("GaussNewton", "Gauss-Newton", None):
+        # the reference's LevenbergMarquardt branch calls ImgDef.eval on a
+        # numeric array and always errors (funICGN.m:199)
+        raise NotImplementedError("only ICGNmethod='GaussNewton' exists on the reference's "
+                                  "working path")
+
+
+def LocalICGN(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmethod="GaussNewton",
+              tol=1e-2, precision=FP64):
+    """[U,F,HtempPar,LocalTime,ConvItPerEle,LocalICGNBadPtNum] = LocalICGN(U0,
+    coordinatesFEM,Df,ImgRef,ImgDef,DICpara,ICGNmethod,tol) -- LocalICGN.m:1,
+    including the bad-subset flags and refill of :117-161 (refill by spring
+    inpainting on the node grid)."""
+    _check_method(ICGNmethod)
+    ctx = _ctx_for(ImgRef)
+    t0 = time.perf_counter()
+    _load_fields(ctx, ImgRef, ImgDef, Df)
+    U, F, it, Hp = local_icgn(ctx, coordinatesFEM, U0, DICpara["winsize"], tol, precision)
+    M, N = _grid_dims(coordinatesFEM)
+    bad = C.c_int()
+    call("aldic_localicgn_post", ctx.h, M, N, _ptr(_prep(it, np.int32)), _ptr(U), _ptr(F),
+         C.byref(bad))
+    return U, F, Hp, time.perf_counter() - t0, it, bad.value
+
+
+def _grid_dims(coords):
+    c = coords.cpu().numpy() if _is_cuda(coords) else np.asarray(coords)
+    M = len(np.unique(c[:, 0]))
+    N = len(np.unique(c[:, 1]))
+    if M * N != c.shape[0]:
+        raise ValueError("coordinatesFEM is not a uniform M x N grid")
+    return M, N
+
+
+# ------------------------------------------------------------------ a9
+def funICGN_Subpb1(x0, y0, Df, ImgRef, ImgDef, winsize, H, beta, mu, udual, vdual, UOld, FOld,
+                   tol, ICGNmethod="GaussNewton"):
+    """[U,H,stepwithinwhile] = funICGN_Subpb1(...) -- funICGN_Subpb1.m:1 for
+    one subset (FP64).  H is the 6x6 Hessian of the subset."""
+    _check_method(ICGNmethod)
+    ctx = _ctx_for(ImgRef)
+    _load_fields(ctx, ImgRef, ImgDef, Df)
+    Hm = np.asarray(H, float)
+    H21 = np.array([Hm[r, c] for c in range(6) for r in range(c, 6)]).reshape(21, 1)
+    U = np.empty(2)
+    it = np.empty(1, np.int32)
+    coords = np.array([[x0], [y0]], float)
+    wa, w = _winsize_arr(winsize, 1, None)
+    call("aldic_subpb1", ctx.h, _ptr(coords), 1, _ptr(np.asarray(UOld, float)[:2].copy()),
+         _ptr(np.asarray(FOld, float)[:4].copy()), _ptr(np.asarray(vdual, float)[:2].copy()),
+         _ptr(H21), _ptr(wa), w, float(mu), float(tol), FP64, _ptr(U), _ptr(it))
+    return U, Hm, int(it[0])
+
+
+def Subpb1(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef, mu, beta, HPar,
+           ALSolveStep, DICpara, ICGNmethod="GaussNewton", tol=1e-2, precision=FP64):
+    """[U,HPar,ALSub1Time,ConvItPerEle,LocalICGNBadPtNum] = Subpb1(...) --
+    Subpb1.m:1 (ALSolveStep > 1) with the gridfit 'springs' post-processing
+    of :186-199.  HPar: n x 21 array (or the reference's 21-cell of n)."""
+    _check_method(ICGNmethod)
+    if ALSolveStep <= 1:
+        raise ValueError("Subpb1 is called with ALSolveStep > 1 in the reference's loop "
+                         "(HPar is only read then)")
+    ctx = _ctx_for(ImgRef)
+    t0 = time.perf_counter()
+    _load_fields(ctx, ImgRef, ImgDef, Df)
+    Hp = np.column_stack(HPar) if isinstance(HPar, (list, tuple)) else HPar
+    H21 = _prep(Hp.T if not _is_cuda(Hp) else Hp.t())
+    cf = _coords_cm(coordinatesFEM)
+    n = cf.shape[-1]
+    like = _first_cuda(coordinatesFEM, UOld)
+    U = _empty(like, (2 * n,))
+    it = _empty(like, (n,), np.int32)
+    wa, w = _winsize_arr(DICpara["winsize"], n, like)
+    call("aldic_subpb1", ctx.h, _ptr(cf), n, _ptr(_prep(UOld)), _ptr(_prep(FOld)),
+         _ptr(_prep(vdual)), _ptr(H21), _ptr(wa), w, float(mu), float(tol), int(precision),
+         _ptr(U), _ptr(it))
+    M, N = _grid_dims(coordinatesFEM)
+    bad = C.c_int()
+    call("aldic_subpb1_post", ctx.h, M, N, _ptr(it), _ptr(U), C.byref(bad))
+    return U, HPar, time.perf_counter() - t0, it, bad.value
+
+
+# ------------------------------------------------------------------ a10/a11
+def Subpb2(DICmesh, beta, mu, U, F, udual, vdual, alpha=0, GaussPtOrder=2):
+    """Uhat = Subpb2(DICmesh,beta,mu,U,F,udual,vdual,alpha,GaussPtOrder) --
+    Subpb2.m:1 on the uniform mesh (dirichlet and neumann empty)."""
+    if alpha != 0:
+        raise NotImplementedError("alpha != 0 is never used by the reference's loop")
+    if len(DICmesh.get("dirichlet", [])) or len(DICmesh.get("neumann", [])):
+        raise NotImplementedError("Dirichlet/Neumann nodes belong to the quadtree path")
+    coords = DICmesh["coordinatesFEM"]
+    c = coords.cpu().numpy() if _is_cuda(coords) else np.asarray(coords)
+    step = abs(c[0, 0] - c[1, 0])  # Subpb2.m:29
+    M, N = int(DICmesh["M"]), int(DICmesh["N"])
+    like = _first_cuda(U, F)
+    out = _empty(like, (2 * M * N,))
+    ctx = _ctx_for(U)
+    call("aldic_subpb2", ctx.h, M, N, float(step), float(beta), float(mu), _ptr(_prep(U)),
+         _ptr(_prep(F)), _ptr(_prep(udual)), _ptr(_prep(vdual)), _ptr(out))
+    return out
+
+
+def funGlobal_NodalStrainAvg(coordinatesFEM, elementsFEM, U, GaussPtOrder=2):
+    """StrainNodalPt = funGlobal_NodalStrainAvg(coordinatesFEM,elementsFEM,U,
+    GaussPtOrder) -- funGlobal_NodalStrainAvg.m:1 on the uniform mesh."""
+    M, N = _grid_dims(coordinatesFEM)
+    c = coordinatesFEM.cpu().numpy() if _is_cuda(coordinatesFEM) else np.asarray(coordinatesFEM)
+    step = abs(c[1, 0] - c[0, 0])
+    out = _empty(_first_cuda(U), (4 * M * N,))
+    call("aldic_nodal_strain", _ctx_for(U).h, M, N, float(step), _ptr(_prep(U)), _ptr(out))
+    return out
+
+
+# ------------------------------------------------------------------ a14
+def gridfit_springs(M, N, fields):
+    """gridfit(x, y, z, xnodes, ynodes, 'regularizer', 'springs') for data on
+    the nodes of an M x N grid (NaN = no data); fields: (nf, M*N)."""
+    z = _prep(fields).reshape(-1, M * N) if not _is_cuda(fields) else _prep(fields).reshape(-1, M * N)
+    out = _empty(_first_cuda(fields), tuple(z.shape))
+    call("aldic_gridfit_springs", _ctx_for(fields).h, M, N, z.shape[0], _ptr(z), _ptr(out))
+    return out
+
+
+def inpaint_nans(A, method=4):
+    """B = inpaint_nans(A, 4) -- spring method of inpaint_nans.m."""
+    if method != 4:
+        raise NotImplementedError("only the spring method (4) is used on the reference's path")
+    A = np.array(A, np.float64)
+    ny, nx = A.shape
+    call("aldic_inpaint_springs", default_context().h, nx, ny, 1, _ptr(A))
+    return A
+
+
+def funSmoothDisp(ULocal, DICmesh, DICpara=None):
+    """ULocal = funSmoothDisp(ULocal,DICmesh,DICpara) -- funSmoothDisp.m with
+    the default filter (3x3, sigma 0.5), two passes."""
+    M, N = int(DICmesh["M"]), int(DICmesh["N"])
+    v = _prep(ULocal).copy() if not _is_cuda(ULocal) else _prep(ULocal).clone()
+    call("aldic_smooth", _ctx_for(ULocal).h, M, N, 2, _ptr(v))
+    return v
+
+
+def funSmoothStrain(F, DICmesh, DICpara=None):
+    """F = funSmoothStrain(F,DICmesh,DICpara) -- funSmoothStrain.m, default
+    filter, two passes."""
+    M, N = int(DICmesh["M"]), int(DICmesh["N"])
+    v = _prep(F).copy() if not _is_cuda(F) else _prep(F).clone()
+    call("aldic_smooth", _ctx_for(F).h, M, N, 4, _ptr(v))
+    return v
+
+
+# ------------------------------------------------------------------ a12
+class ALDIC:
+    """One-frame AL-DIC driver (main_ALDIC.m Sections 3-6) on a context.
+
+        al = ALDIC(winsize=32, step=8, search=16)
+        al.set_images(f, g)           # raw uint8/uint16/float images (H, W)
+        res = al.frame()              # dict: x0, y0, U, F, iters, stats
+    """
+
+    def __init__(self, winsize, step, search, tol=1e-2, mu=1e-3, beta=0.0, n_admm=3,
+                 precision=FP32, smooth=False, gridx=(0, 0), gridy=(0, 0), use_graph=True,
+                 device=None, ctx: Context | None = None):
+        self.ctx = ctx or default_context(device)
+        p = FrameParams()
+        p.winsize, p.step = int(winsize), int(step)
+        s = (search, search) if np.ndim(search) == 0 else search
+        p.search[0], p.search[1] = int(s[0]), int(s[1])
+        p.gridx[0], p.gridx[1] = gridx
+        p.gridy[0], p.gridy[1] = gridy
+        p.tol, p.mu, p.beta, p.n_admm = float(tol), float(mu), float(beta), int(n_admm)
+        p.tol2 = 0.0
+        p.precision, p.smooth, p.use_graph = int(precision), int(bool(smooth)), int(bool(use_graph))
+        self.p = p
+
+    def set_images(self, f=None, g=None, roi=None, mask=None):
+        if f is not None:
+            self.ctx.set_ref(f, roi=roi, mask=mask)
+        if g is not None:
+            self.ctx.set_def(g)
+
+    def dims(self):
+        M, N = C.c_int(), C.c_int()
+        call("aldic_frame_dims", self.ctx.h, C.byref(self.p), C.byref(M), C.byref(N))
+        return M.value, N.value
+
+    def frame(self, out: dict | None = None, stats: bool = True, device_out: bool = False):
+        """Run one frame.  With out (dict of preallocated arrays x0, y0, U, F,
+        iters -- numpy or CUDA tensors) the results are written there."""
+        M, N = self.dims()
+        n = M * N
+        if out is None:
+            if device_out:
+                dev = torch.device("cuda", self.ctx.device)
+                out = {"x0": torch.empty(n, dtype=torch.float64, device=dev),
+                       "y0": torch.empty(n, dtype=torch.float64, device=dev),
+                       "U": torch.empty(2 * n, dtype=torch.float64, device=dev),
+                       "F": torch.empty(4 * n, dtype=torch.float64, device=dev),
+                       "iters": torch.empty(n, dtype=torch.int32, device=dev)}
+            else:
+                out = {"x0": np.empty(n), "y0": np.empty(n), "U": np.empty(2 * n),
+                       "F": np.empty(4 * n), "iters": np.empty(n, np.int32)}
+        st = FrameStats()
+        call("aldic_frame", self.ctx.h, C.byref(self.p), _ptr(out["x0"]), _ptr(out["y0"]),
+             _ptr(out["U"]), _ptr(out["F"]), _ptr(out["iters"]), C.byref(st) if stats else None)
+        res = dict(out)
+        res["M"], res["N"] = M, N
+        if stats:
+            res["stats"] = {"beta": st.beta, "bad_icgn": st.bad_icgn,
+                            "converged_icgn": st.converged_icgn,
+                            "mean_iters_icgn": st.mean_iters_icgn,
+                            "update_y": list(st.update_y)[:st.admm_steps],
+                            "update_y2": list(st.update_y2)[:st.admm_steps],
+                            "kernel_launches": st.kernel_launches,
+                            "t_stage_ms": dict(zip(("normalize", "search", "icgn", "icgn_post",
+                                                    "section5", "admm", "frame"),
+                                                   list(st.t_stage_ms)[:7]))}
+        return res

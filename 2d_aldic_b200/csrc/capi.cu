@@ -1,0 +1,1219 @@
+// capi.cu -- the C ABI of libaldic_b200.so (include/aldic_b200.h): context,
+// host/device argument staging, the per-function entry points and the
+// captured frame pipeline of main_ALDIC.m Sections 3-6.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/aldic_b200.h"
+#include "aldic_internal.cuh"
+#include "kernels.cuh"
+
+namespace aldic {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+const char *last_error() { return g_err.c_str(); }
+
+// ------------------------------------------------------------------ buffers
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMalloc of " + std::to_string(want) + " bytes failed");
+      return E_NOMEM;
+    }
+    cap = want;
+    return OK;
+  }
+  template <typename T> T *as() const { return (T *)p; }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// bump arena for staging host arguments (chunks persist, reset per call)
+struct Arena {
+  std::vector<DevBuf> chunks;
+  size_t chunk = 0, off = 0;
+  void reset() { chunk = 0; off = 0; }
+  void *get(size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    while (true) {
+      if (chunk >= chunks.size()) {
+        chunks.emplace_back();
+        size_t want = bytes > (size_t(64) << 20) ? bytes : (size_t(64) << 20);
+        if (chunks.back().ensure(want) != OK) return nullptr;
+      }
+      DevBuf &c = chunks[chunk];
+      if (off + bytes <= c.cap) {
+        void *p = (char *)c.p + off;
+        off += bytes;
+        return p;
+      }
+      chunk++;
+      off = 0;
+    }
+  }
+  void release() {
+    for (auto &c : chunks) c.release();
+    chunks.clear();
+    reset();
+  }
+};
+
+static bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace aldic
+
+using namespace aldic;
+
+struct aldic_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::mutex mu;
+  Arena arena;
+  // images
+  int W = 0, H = 0, dtype = -1, roi[4] = {0, 0, 0, 0};
+  bool have_ref = false, have_def = false;
+  bool prepared = false;  // fields given by aldic_set_fields (no normalisation)
+  DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
+  DevBuf stats;   // double[4]: mean_f std_f mean_g std_g
+  DevBuf isums;   // u64[2]
+  DevBuf part;    // double[1024]
+  // grid solver work (sized for 6 fields of the largest node grid seen)
+  DevBuf gw_vec, gw_part, gw_mask, gw_misc;
+  long long gw_n = 0;
+  GridWork gw{};
+  DevBuf queue;
+  // frame state
+  DevBuf fr;  // one slab for all frame arrays
+  long long fr_n = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_kernels = -1;
+  cudaEvent_t ev[8] = {};   // frame stage marks
+  std::string graph_key;
+  bool graph_failed = false;
+};
+
+namespace {
+
+// host or device argument: device pointers pass through, host arrays are
+// staged in the context arena
+template <typename T>
+struct Arg {
+  T *host = nullptr;
+  T *dev = nullptr;
+  size_t count = 0;
+  bool staged = false;
+};
+
+template <typename T>
+int arg_in(aldic_ctx *c, const T *p, size_t count, Arg<T> &a) {
+  a.count = count;
+  if (!p || count == 0) {
+    a.dev = nullptr;
+    return OK;
+  }
+  if (is_device_ptr(p)) {
+    a.dev = const_cast<T *>(p);
+    return OK;
+  }
+  a.dev = (T *)c->arena.get(sizeof(T) * count);
+  ALDIC_CHECK(a.dev, E_NOMEM, "staging buffer allocation failed");
+  a.host = const_cast<T *>(p);
+  a.staged = true;
+  ALDIC_CUDA(cudaMemcpyAsync(a.dev, p, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
+  return OK;
+}
+
+template <typename T>
+int arg_out(aldic_ctx *c, T *p, size_t count, Arg<T> &a, bool copy_in = false) {
+  a.count = count;
+  if (!p || count == 0) {
+    a.dev = nullptr;
+    return OK;
+  }
+  if (is_device_ptr(p)) {
+    a.dev = p;
+    return OK;
+  }
+  a.dev = (T *)c->arena.get(sizeof(T) * count);
+  ALDIC_CHECK(a.dev, E_NOMEM, "staging buffer allocation failed");
+  a.host = p;
+  a.staged = true;
+  if (copy_in)
+    ALDIC_CUDA(cudaMemcpyAsync(a.dev, p, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
+  return OK;
+}
+
+template <typename T>
+int arg_back(aldic_ctx *c, Arg<T> &a) {
+  if (a.staged && a.host)
+    ALDIC_CUDA(cudaMemcpyAsync(a.host, a.dev, sizeof(T) * a.count, cudaMemcpyDeviceToHost,
+                               c->stream));
+  return OK;
+}
+
+// synchronise when any argument was staged (the copies back must land
+// before the call returns)
+int finish(aldic_ctx *c, bool staged) {
+  if (staged) ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+struct Guard {
+  aldic_ctx *c;
+  int prev = 0;
+  std::unique_lock<std::mutex> lk;
+  explicit Guard(aldic_ctx *ctx) : c(ctx), lk(ctx->mu) {
+    cudaGetDevice(&prev);
+    cudaSetDevice(ctx->device);
+    ctx->arena.reset();
+  }
+  ~Guard() { cudaSetDevice(prev); }
+};
+
+size_t dtype_size(int dt) { return dt == 0 ? 1 : dt == 1 ? 2 : dt == 2 ? 4 : 8; }
+
+int ensure_grid_work(aldic_ctx *c, long long n) {
+  if (n <= c->gw_n && c->gw.x) return OK;
+  const long long R = 6;
+  int rc;
+  // x r z p(2 buffers) q b diag -> 8 * R * n doubles
+  if ((rc = c->gw_vec.ensure(sizeof(double) * 8 * R * n))) return rc;
+  c->gw.max_blocks = 148 * 8;
+  if ((rc = c->gw_part.ensure(sizeof(double) * 4 * R * c->gw.max_blocks))) return rc;
+  if ((rc = c->gw_mask.ensure(R * n))) return rc;
+  if ((rc = c->gw_misc.ensure(64))) return rc;
+  double *v = c->gw_vec.as<double>();
+  c->gw.x = v;
+  c->gw.r = v + R * n;
+  c->gw.z = v + 2 * R * n;
+  c->gw.p = v + 3 * R * n;  // two buffers
+  c->gw.q = v + 5 * R * n;
+  c->gw.b = v + 6 * R * n;
+  c->gw.diag = v + 7 * R * n;
+  c->gw.part = c->gw_part.as<double>();
+  c->gw.mask = c->gw_mask.as<unsigned char>();
+  unsigned int *misc = c->gw_misc.as<unsigned int>();
+  c->gw.bar = misc;
+  c->gw.err = (int *)(misc + 2);
+  c->gw.iters_out = (int *)(misc + 3);
+  c->gw_n = n;
+  ALDIC_CUDA(cudaMemsetAsync(c->gw_misc.p, 0, 64, c->stream));
+  return OK;
+}
+
+int check_grid_err(aldic_ctx *c) {
+  int err = 0;
+  ALDIC_CUDA(cudaMemcpyAsync(&err, c->gw.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  if (err == 1) {
+    cudaMemsetAsync(c->gw.err, 0, sizeof(int), c->stream);
+    set_error("grid solver: barrier wait timed out");
+    return E_TIMEOUT;
+  }
+  if (err == 2) {
+    cudaMemsetAsync(c->gw.err, 0, sizeof(int), c->stream);
+    set_error("grid solver: PCG did not reach its tolerance");
+    return E_TIMEOUT;
+  }
+  return OK;
+}
+
+IcgnImages images_of(aldic_ctx *c) {
+  IcgnImages im;
+  im.f32 = c->f32.as<float>(); im.g32 = c->g32.as<float>();
+  im.gx32 = c->gx32.as<float>(); im.gy32 = c->gy32.as<float>();
+  im.f64 = c->f64.as<double>(); im.g64 = c->g64.as<double>();
+  im.gx64 = c->gx64.as<double>(); im.gy64 = c->gy64.as<double>();
+  im.W = c->W; im.H = c->H;
+  return im;
+}
+
+constexpr double kGridfitLam2Interior = 1.0 / ((4.0 + 2.0 * 1.4142135623730951) * (4.0 + 2.0 * 1.4142135623730951));
+
+// norm(Areg,1) of gridfit.m:592 for the springs regulariser on an M x N grid
+double springs_lam2(int M, int N) {
+  double best = 0;
+  const double d = 1.0 / std::sqrt(2.0);
+  const int is[3] = {0, M > 2 ? 1 : 0, M - 1}, js[3] = {0, N > 2 ? 1 : 0, N - 1};
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const int i = is[a], j = js[b];
+      double s = (i > 0) + (i < M - 1) + (j > 0) + (j < N - 1);
+      s += d * ((i > 0 && j > 0) + (i < M - 1 && j > 0) + (i > 0 && j < N - 1) +
+                (i < M - 1 && j < N - 1));
+      if (s > best) best = s;
+    }
+  (void)kGridfitLam2Interior;
+  return 1.0 / (best * best);
+}
+
+// PCG tolerances of the node-grid solves
+constexpr double kRtolFE = 1e-11, kRtolFit = 1e-11, kRtolInpaint = 1e-11;
+constexpr int kMaxitFE = 4000, kMaxitFit = 8000, kMaxitInpaint = 50000;
+
+}  // namespace
+
+// ======================================================================
+extern "C" {
+
+int aldic_version(void) { return 100; }
+const char *aldic_last_error(void) { return aldic::last_error(); }
+
+static int interp_any(bool f64, const void *F, int64_t M, int64_t N, int64_t P, const void *X,
+                      const void *Y, int64_t n, void *Z, void *stream) {
+  ALDIC_CHECK(F && X && Y && Z && M > 0 && N > 0 && P > 0 && n >= 0, E_ARG,
+              "ba_interp2: bad arguments");
+  if (n == 0) return OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t es = f64 ? 8 : 4;
+  const bool dev = is_device_ptr(F) && is_device_ptr(X) && is_device_ptr(Y) && is_device_ptr(Z);
+  const void *dF = F, *dX = X, *dY = Y;
+  void *dZ = Z;
+  std::vector<void *> tmp;
+  if (!dev) {
+    void *a, *b, *c, *d;
+    ALDIC_CUDA(cudaMalloc(&a, es * M * N * P));
+    ALDIC_CUDA(cudaMalloc(&b, es * n));
+    ALDIC_CUDA(cudaMalloc(&c, es * n));
+    ALDIC_CUDA(cudaMalloc(&d, es * n * P));
+    tmp = {a, b, c, d};
+    ALDIC_CUDA(cudaMemcpyAsync(a, F, es * M * N * P, cudaMemcpyDefault, st));
+    ALDIC_CUDA(cudaMemcpyAsync(b, X, es * n, cudaMemcpyDefault, st));
+    ALDIC_CUDA(cudaMemcpyAsync(c, Y, es * n, cudaMemcpyDefault, st));
+    dF = a; dX = b; dY = c; dZ = d;
+  }
+  int rc = f64 ? interp_f64((const double *)dF, M, N, P, (const double *)dX, (const double *)dY, n,
+                            (double *)dZ, st)
+               : interp_f32((const float *)dF, M, N, P, (const float *)dX, (const float *)dY, n,
+                            (float *)dZ, st);
+  if (!dev) {
+    if (rc == OK) {
+      ALDIC_CUDA(cudaMemcpyAsync(Z, dZ, es * n * P, cudaMemcpyDefault, st));
+      ALDIC_CUDA(cudaStreamSynchronize(st));
+    }
+    for (void *p : tmp) cudaFree(p);
+  }
+  return rc;
+}
+
+int aldic_ba_interp2_f64(const double *F, int64_t M, int64_t N, int64_t P, const double *X,
+                         const double *Y, int64_t n, double *Z, void *stream) {
+  return interp_any(true, F, M, N, P, X, Y, n, Z, stream);
+}
+int aldic_ba_interp2_f32(const float *F, int64_t M, int64_t N, int64_t P, const float *X,
+                         const float *Y, int64_t n, float *Z, void *stream) {
+  return interp_any(false, F, M, N, P, X, Y, n, Z, stream);
+}
+
+int aldic_ctx_create(int device, aldic_ctx **out) {
+  ALDIC_CHECK(out, E_ARG, "ctx_create: out is NULL");
+  int ndev = 0;
+  ALDIC_CUDA(cudaGetDeviceCount(&ndev));
+  ALDIC_CHECK(device >= 0 && device < ndev, E_ARG, "ctx_create: no such device");
+  aldic_ctx *c = new aldic_ctx();
+  c->device = device;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaSetDevice(prev);
+    delete c;
+    set_error("ctx_create: stream creation failed");
+    return E_CUDA;
+  }
+  c->own_stream = true;
+  int rc = c->stats.ensure(sizeof(double) * 8);
+  if (!rc) rc = c->isums.ensure(sizeof(unsigned long long) * 2);
+  if (!rc) rc = c->part.ensure(sizeof(double) * 1024);
+  if (!rc) rc = c->queue.ensure(sizeof(unsigned int) * 4);
+  for (int k = 0; k < 8 && !rc; ++k)
+    if (cudaEventCreate(&c->ev[k]) != cudaSuccess) rc = E_CUDA;
+  cudaSetDevice(prev);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return OK;
+}
+
+int aldic_ctx_destroy(aldic_ctx *c) {
+  if (!c) return OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (int k = 0; k < 8; ++k)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  DevBuf *bufs[] = {&c->f_raw, &c->g_raw, &c->f64, &c->g64, &c->f32, &c->g32, &c->gx64,
+                    &c->gy64, &c->gx32, &c->gy32, &c->mask, &c->stats, &c->isums, &c->part,
+                    &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr};
+  for (DevBuf *b : bufs) b->release();
+  c->arena.release();
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  cudaSetDevice(prev);
+  delete c;
+  return OK;
+}
+
+int aldic_ctx_set_stream(aldic_ctx *c, void *stream) {
+  ALDIC_CHECK(c, E_ARG, "null context");
+  Guard g(c);
+  cudaStreamSynchronize(c->stream);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return OK;
+}
+
+int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const int roi[4],
+                  const double *mask) {
+  ALDIC_CHECK(c && img, E_ARG, "set_ref: null argument");
+  ALDIC_CHECK(dtype >= 0 && dtype <= 3, E_ARG, "set_ref: dtype must be ALDIC_U8/U16/F32/F64");
+  ALDIC_CHECK(W >= 8 && H >= 8, E_ARG, "set_ref: image smaller than 8 x 8");
+  Guard g(c);
+  const long long n = (long long)W * H;
+  const size_t es = dtype_size(dtype);
+  int rc;
+  DevBuf *b8[] = {&c->f64, &c->g64, &c->gx64, &c->gy64};
+  DevBuf *b4[] = {&c->f32, &c->g32, &c->gx32, &c->gy32};
+  for (DevBuf *b : b8)
+    if ((rc = b->ensure(sizeof(double) * n))) return rc;
+  for (DevBuf *b : b4)
+    if ((rc = b->ensure(sizeof(float) * n))) return rc;
+  if ((rc = c->f_raw.ensure(es * n))) return rc;
+  if ((rc = c->g_raw.ensure(es * n))) return rc;
+  if (c->dtype != dtype || c->W != W || c->H != H) c->have_def = false;
+  c->W = W;
+  c->H = H;
+  c->dtype = dtype;
+  int r[4] = {1, W, 1, H};
+  if (roi) {
+    r[0] = roi[0] < 1 ? 1 : roi[0];
+    r[1] = roi[1] > W ? W : roi[1];
+    r[2] = roi[2] < 1 ? 1 : roi[2];
+    r[3] = roi[3] > H ? H : roi[3];
+  }
+  ALDIC_CHECK(r[1] >= r[0] + 1 && r[3] >= r[2] + 1, E_ARG, "set_ref: empty ROI");
+  memcpy(c->roi, r, sizeof r);
+  c->prepared = false;
+  ALDIC_CUDA(cudaMemcpyAsync(c->f_raw.p, img, es * n, cudaMemcpyDefault, c->stream));
+  const double *dmask = nullptr;
+  if (mask) {
+    if ((rc = c->mask.ensure(sizeof(double) * n))) return rc;
+    ALDIC_CUDA(cudaMemcpyAsync(c->mask.p, mask, sizeof(double) * n, cudaMemcpyDefault, c->stream));
+    dmask = c->mask.as<double>();
+  }
+  double *st = c->stats.as<double>();
+  if ((rc = roi_stats(c->f_raw.p, dtype, W, r, st, c->isums.as<unsigned long long>(),
+                      c->part.as<double>(), c->stream)))
+    return rc;
+  if ((rc = normalize(c->f_raw.p, dtype, n, st, c->f64.as<double>(), c->f32.as<float>(), c->stream)))
+    return rc;
+  if ((rc = gradient(c->f64.as<double>(), dmask, W, H, c->gx64.as<double>(), c->gy64.as<double>(),
+                     c->gx32.as<float>(), c->gy32.as<float>(), c->stream)))
+    return rc;
+  c->have_ref = true;
+  return finish(c, true);
+}
+
+static int prep_def(aldic_ctx *c) {
+  double *st = c->stats.as<double>();
+  int rc = roi_stats(c->g_raw.p, c->dtype, c->W, c->roi, st + 2, c->isums.as<unsigned long long>(),
+                     c->part.as<double>(), c->stream);
+  if (rc) return rc;
+  return normalize(c->g_raw.p, c->dtype, (long long)c->W * c->H, st + 2, c->g64.as<double>(),
+                   c->g32.as<float>(), c->stream);
+}
+
+int aldic_set_def(aldic_ctx *c, const void *img, int dtype) {
+  ALDIC_CHECK(c && img, E_ARG, "set_def: null argument");
+  ALDIC_CHECK(c->have_ref, E_STATE, "set_def: set the reference image first");
+  ALDIC_CHECK(dtype == c->dtype, E_ARG, "set_def: dtype differs from the reference image");
+  Guard g(c);
+  const long long n = (long long)c->W * c->H;
+  ALDIC_CUDA(cudaMemcpyAsync(c->g_raw.p, img, dtype_size(dtype) * n, cudaMemcpyDefault, c->stream));
+  int rc = prep_def(c);
+  if (rc) return rc;
+  c->have_def = true;
+  return finish(c, !is_device_ptr(img));
+}
+
+int aldic_normalize(aldic_ctx *c, const void *img, int dtype, int W, int H, const int roi[4],
+                    double *out, double stats[2]) {
+  ALDIC_CHECK(c && img && out && dtype >= 0 && dtype <= 3 && W > 1 && H > 1, E_ARG,
+              "normalize: bad arguments");
+  Guard g(c);
+  const long long n = (long long)W * H;
+  int r[4] = {1, W, 1, H};
+  if (roi) {
+    r[0] = roi[0] < 1 ? 1 : roi[0];
+    r[1] = roi[1] > W ? W : roi[1];
+    r[2] = roi[2] < 1 ? 1 : roi[2];
+    r[3] = roi[3] > H ? H : roi[3];
+  }
+  ALDIC_CHECK(r[1] >= r[0] + 1 && r[3] >= r[2] + 1, E_ARG, "normalize: empty ROI");
+  int rc;
+  Arg<unsigned char> ai;
+  Arg<double> ao;
+  if ((rc = arg_in(c, (const unsigned char *)img, dtype_size(dtype) * n, ai)) ||
+      (rc = arg_out(c, out, n, ao)))
+    return rc;
+  float *tmp32 = (float *)c->arena.get(sizeof(float) * n);
+  double *st = (double *)c->arena.get(sizeof(double) * 4);
+  ALDIC_CHECK(tmp32 && st, E_NOMEM, "staging buffer allocation failed");
+  if ((rc = roi_stats(ai.dev, dtype, W, r, st, c->isums.as<unsigned long long>(), c->part.as<double>(),
+                      c->stream)))
+    return rc;
+  if ((rc = normalize(ai.dev, dtype, n, st, ao.dev, tmp32, c->stream))) return rc;
+  arg_back(c, ao);
+  if (stats) ALDIC_CUDA(cudaMemcpyAsync(stats, st, 2 * sizeof(double), cudaMemcpyDefault, c->stream));
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  return OK;
+}
+
+int aldic_gradient(aldic_ctx *c, const double *f, int W, int H, const double *mask, double *dfdx,
+                   double *dfdy) {
+  ALDIC_CHECK(c && f && dfdx && dfdy && W >= 8 && H >= 8, E_ARG, "gradient: bad arguments");
+  Guard g(c);
+  const long long n = (long long)W * H;
+  int rc;
+  Arg<double> af, am, ax, ay;
+  if ((rc = arg_in(c, f, n, af)) || (rc = arg_in(c, mask, mask ? n : 0, am)) ||
+      (rc = arg_out(c, dfdx, n, ax)) || (rc = arg_out(c, dfdy, n, ay)))
+    return rc;
+  float *t1 = (float *)c->arena.get(sizeof(float) * n), *t2 = (float *)c->arena.get(sizeof(float) * n);
+  ALDIC_CHECK(t1 && t2, E_NOMEM, "staging buffer allocation failed");
+  if ((rc = gradient(af.dev, am.dev, W, H, ax.dev, ay.dev, t1, t2, c->stream))) return rc;
+  arg_back(c, ax); arg_back(c, ay);
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  return OK;
+}
+
+__global__ void k_to_f32(const double *a, float *b, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    b[k] = __double2float_rn(a[k]);
+}
+
+int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const double *dfdx,
+                     const double *dfdy, int W, int H) {
+  ALDIC_CHECK(c, E_ARG, "set_fields: null context");
+  ALDIC_CHECK(W >= 8 && H >= 8, E_ARG, "set_fields: image smaller than 8 x 8");
+  const bool first = !(c->have_ref && c->dtype == 3 && c->W == W && c->H == H);
+  ALDIC_CHECK(!first || (f && dfdx && dfdy), E_ARG, "set_fields: f, dfdx and dfdy are required first");
+  Guard g(c);
+  const long long n = (long long)W * H;
+  const size_t bytes = sizeof(double) * n;
+  int rc;
+  DevBuf *b8[] = {&c->f64, &c->g64, &c->gx64, &c->gy64, &c->f_raw, &c->g_raw};
+  DevBuf *b4[] = {&c->f32, &c->g32, &c->gx32, &c->gy32};
+  for (DevBuf *b : b8)
+    if ((rc = b->ensure(bytes))) return rc;
+  for (DevBuf *b : b4)
+    if ((rc = b->ensure(sizeof(float) * n))) return rc;
+  if (first) c->have_def = false;
+  c->W = W; c->H = H; c->dtype = 3;
+  c->prepared = true;
+  c->roi[0] = 1; c->roi[1] = W; c->roi[2] = 1; c->roi[3] = H;
+  const double *src[4] = {f, gimg, dfdx, dfdy};
+  DevBuf *d64[4] = {&c->f64, &c->g64, &c->gx64, &c->gy64};
+  DevBuf *d32[4] = {&c->f32, &c->g32, &c->gx32, &c->gy32};
+  for (int k = 0; k < 4; ++k) {
+    if (!src[k]) continue;
+    ALDIC_CUDA(cudaMemcpyAsync(d64[k]->p, src[k], bytes, cudaMemcpyDefault, c->stream));
+    k_to_f32<<<1184, 256, 0, c->stream>>>(d64[k]->as<double>(), d32[k]->as<float>(), n);
+  }
+  if (f) ALDIC_CUDA(cudaMemcpyAsync(c->f_raw.p, c->f64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (gimg) ALDIC_CUDA(cudaMemcpyAsync(c->g_raw.p, c->g64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  // the normalised fields have mean 0 in the units the search pads with
+  const double st[4] = {0.0, 1.0, 0.0, 1.0};
+  ALDIC_CUDA(cudaMemcpyAsync(c->stats.p, st, sizeof st, cudaMemcpyHostToDevice, c->stream));
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  c->have_ref = true;
+  if (gimg) c->have_def = true;
+  return OK;
+}
+
+int aldic_get_images(aldic_ctx *c, double *f, double *gimg, double *dfdx, double *dfdy,
+                     double stats[4]) {
+  ALDIC_CHECK(c && c->have_ref, E_STATE, "get_images: no reference image");
+  Guard g(c);
+  const size_t bytes = sizeof(double) * (size_t)c->W * c->H;
+  if (f) ALDIC_CUDA(cudaMemcpyAsync(f, c->f64.p, bytes, cudaMemcpyDefault, c->stream));
+  if (gimg) {
+    ALDIC_CHECK(c->have_def, E_STATE, "get_images: no deformed image");
+    ALDIC_CUDA(cudaMemcpyAsync(gimg, c->g64.p, bytes, cudaMemcpyDefault, c->stream));
+  }
+  if (dfdx) ALDIC_CUDA(cudaMemcpyAsync(dfdx, c->gx64.p, bytes, cudaMemcpyDefault, c->stream));
+  if (dfdy) ALDIC_CUDA(cudaMemcpyAsync(dfdy, c->gy64.p, bytes, cudaMemcpyDefault, c->stream));
+  if (stats) ALDIC_CUDA(cudaMemcpyAsync(stats, c->stats.p, 4 * sizeof(double), cudaMemcpyDefault, c->stream));
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  return OK;
+}
+
+int aldic_search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsize, int step,
+                      const int search[2], int *nx, int *ny) {
+  ALDIC_CHECK(gridx && gridy && search && nx && ny, E_ARG, "search_dims: null argument");
+  int rc = search_dims(W, H, gridx, gridy, winsize, step, search, nx, ny, nullptr, nullptr);
+  if (rc) set_error("search_dims: winsize, step and search must be positive");
+  return rc;
+}
+
+int aldic_int_search(aldic_ctx *c, const int gridx[2], const int gridy[2], int winsize, int step,
+                     const int search[2], double *x, double *y, double *u, double *v,
+                     double *ccmax, double *qfactors) {
+  ALDIC_CHECK(c && c->have_ref && c->have_def, E_STATE, "int_search: set both images first");
+  ALDIC_CHECK(gridx && gridy && search && x && y && u && v && ccmax, E_ARG,
+              "int_search: null argument");
+  Guard g(c);
+  int nx, ny;
+  int rc = search_dims(c->W, c->H, gridx, gridy, winsize, step, search, &nx, &ny, nullptr, nullptr);
+  ALDIC_CHECK(rc == OK, E_ARG, "int_search: winsize, step and search must be positive");
+  const size_t n = (size_t)nx * ny;
+  if (n == 0) return OK;
+  Arg<double> ax, ay, au, av, ac;
+  if ((rc = arg_out(c, x, n, ax)) || (rc = arg_out(c, y, n, ay)) || (rc = arg_out(c, u, n, au)) ||
+      (rc = arg_out(c, v, n, av)) || (rc = arg_out(c, ccmax, n, ac)))
+    return rc;
+  double *pce = nullptr, *ppe = nullptr;
+  if (qfactors) {
+    pce = (double *)c->arena.get(sizeof(double) * 2 * n);
+    ALDIC_CHECK(pce, E_NOMEM, "staging buffer allocation failed");
+    ppe = pce + n;
+  }
+  rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H, c->stats.as<double>() + 2, gridx,
+                  gridy, winsize, step, search, ax.dev, ay.dev, au.dev, av.dev, ac.dev, pce, ppe,
+                  c->stream);
+  if (rc) return rc;
+  arg_back(c, ax); arg_back(c, ay); arg_back(c, au); arg_back(c, av); arg_back(c, ac);
+  if (qfactors) {
+    // funIntegerSearch.m:174-177 normalisation on the host
+    std::vector<double> q(2 * n);
+    ALDIC_CUDA(cudaMemcpyAsync(q.data(), pce, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, c->stream));
+    ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 2; ++k) {
+      double mn = INFINITY, mx = -INFINITY;
+      for (size_t i = 0; i < n; ++i) mn = q[k * n + i] < mn ? q[k * n + i] : mn;
+      for (size_t i = 0; i < n; ++i) {
+        const double t = q[k * n + i] - mn;
+        mx = t > mx ? t : mx;
+      }
+      for (size_t i = 0; i < n; ++i) q[k * n + i] = (q[k * n + i] - mn) / mx;
+    }
+    ALDIC_CUDA(cudaMemcpyAsync(qfactors, q.data(), sizeof(double) * 2 * n, cudaMemcpyDefault, c->stream));
+    ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return finish(c, ax.staged || qfactors);
+}
+
+int aldic_icgn(aldic_ctx *c, const double *coords, int64_t n, const double *U0,
+               const int32_t *winsize_arr, int winsize, double tol, int precision, double *U,
+               double *F, int32_t *iters, double *H21) {
+  ALDIC_CHECK(c && c->have_ref && c->have_def, E_STATE, "icgn: set both images first");
+  ALDIC_CHECK(coords && U0 && U && F && iters && H21 && n >= 0, E_ARG, "icgn: null argument");
+  ALDIC_CHECK(winsize_arr || winsize > 0, E_ARG, "icgn: winsize must be positive");
+  if (n == 0) return OK;
+  Guard g(c);
+  Arg<double> ac, au0, au, af, ah;
+  Arg<int32_t> aw, ai;
+  int rc;
+  if ((rc = arg_in(c, coords, 2 * n, ac)) || (rc = arg_in(c, U0, 2 * n, au0)) ||
+      (rc = arg_in(c, winsize_arr, winsize_arr ? n : 0, aw)) || (rc = arg_out(c, U, 2 * n, au)) ||
+      (rc = arg_out(c, F, 4 * n, af)) || (rc = arg_out(c, iters, n, ai)) ||
+      (rc = arg_out(c, H21, 21 * n, ah)))
+    return rc;
+  rc = icgn(images_of(c), ac.dev, n, au0.dev, (const int *)aw.dev, winsize, tol, precision, au.dev,
+            af.dev, (int *)ai.dev, ah.dev, c->queue.as<unsigned int>(), c->stream);
+  if (rc) return rc;
+  arg_back(c, au); arg_back(c, af); arg_back(c, ai); arg_back(c, ah);
+  return finish(c, au.staged || af.staged || ai.staged || ah.staged);
+}
+
+int aldic_subpb1(aldic_ctx *c, const double *coords, int64_t n, const double *UOld,
+                 const double *FOld, const double *vdual, const double *H21,
+                 const int32_t *winsize_arr, int winsize, double mu, double tol, int precision,
+                 double *U, int32_t *iters) {
+  ALDIC_CHECK(c && c->have_ref && c->have_def, E_STATE, "subpb1: set both images first");
+  ALDIC_CHECK(coords && UOld && FOld && vdual && H21 && U && iters && n >= 0, E_ARG,
+              "subpb1: null argument");
+  ALDIC_CHECK(winsize_arr || winsize > 0, E_ARG, "subpb1: winsize must be positive");
+  if (n == 0) return OK;
+  Guard g(c);
+  Arg<double> ac, auo, afo, avd, ah, au;
+  Arg<int32_t> aw, ai;
+  int rc;
+  if ((rc = arg_in(c, coords, 2 * n, ac)) || (rc = arg_in(c, UOld, 2 * n, auo)) ||
+      (rc = arg_in(c, FOld, 4 * n, afo)) || (rc = arg_in(c, vdual, 2 * n, avd)) ||
+      (rc = arg_in(c, H21, 21 * n, ah)) || (rc = arg_in(c, winsize_arr, winsize_arr ? n : 0, aw)) ||
+      (rc = arg_out(c, U, 2 * n, au)) || (rc = arg_out(c, iters, n, ai)))
+    return rc;
+  rc = subpb1(images_of(c), ac.dev, n, auo.dev, afo.dev, avd.dev, ah.dev, (const int *)aw.dev,
+              winsize, mu, tol, precision, au.dev, (int *)ai.dev, c->queue.as<unsigned int>(),
+              c->stream);
+  if (rc) return rc;
+  arg_back(c, au); arg_back(c, ai);
+  return finish(c, au.staged || ai.staged);
+}
+
+// ---------------------------------------------------------------- grid ops
+static int do_inpaint(aldic_ctx *c, int M, int N, int nf, double *vals, int stride,
+                      const unsigned char *bad, int f0, bool solve) {
+  int rc = inpaint_load(c->gw, M, N, nf, vals, stride, bad, c->stream, f0);
+  if (rc || !solve) return rc;
+  return OK;
+}
+
+int aldic_localicgn_post(aldic_ctx *c, int M, int N, const int32_t *iters, double *U, double *F,
+                         int *bad_num) {
+  ALDIC_CHECK(c && iters && U && F && M > 0 && N > 0, E_ARG, "localicgn_post: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<int32_t> ai;
+  Arg<double> au, af;
+  if ((rc = arg_in(c, iters, n, ai)) || (rc = arg_out(c, U, 2 * n, au, true)) ||
+      (rc = arg_out(c, F, 4 * n, af, true)))
+    return rc;
+  unsigned char *bad = (unsigned char *)c->arena.get(n);
+  int *dnum = (int *)c->arena.get(64);
+  ALDIC_CHECK(bad && dnum, E_NOMEM, "staging buffer allocation failed");
+  if ((rc = icgn_flags(M, N, (const int *)ai.dev, bad, dnum, (double *)(dnum + 2), dnum + 4, c->stream)))
+    return rc;
+  if ((rc = do_inpaint(c, M, N, 2, au.dev, 2, bad, 0, false))) return rc;
+  if ((rc = do_inpaint(c, M, N, 4, af.dev, 4, bad, 2, false))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 6, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, c->stream)))
+    return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 2, au.dev, 2, c->stream, 0))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 4, af.dev, 4, c->stream, 2))) return rc;
+  arg_back(c, au); arg_back(c, af);
+  int hb = 0;
+  ALDIC_CUDA(cudaMemcpyAsync(&hb, dnum, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = check_grid_err(c))) return rc;
+  if (bad_num) *bad_num = hb;
+  return OK;
+}
+
+int aldic_subpb1_post(aldic_ctx *c, int M, int N, const int32_t *iters, double *U, int *bad_num) {
+  ALDIC_CHECK(c && iters && U && M > 0 && N > 0, E_ARG, "subpb1_post: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<int32_t> ai;
+  Arg<double> au;
+  if ((rc = arg_in(c, iters, n, ai)) || (rc = arg_out(c, U, 2 * n, au, true))) return rc;
+  unsigned char *bad = (unsigned char *)c->arena.get(n);
+  int *dnum = (int *)c->arena.get(64);
+  ALDIC_CHECK(bad && dnum, E_NOMEM, "staging buffer allocation failed");
+  if ((rc = subpb1_flags((int)n, (const int *)ai.dev, bad, dnum, c->stream))) return rc;
+  if ((rc = gridfit_load(c->gw, M, N, 2, au.dev, 2, (const int *)ai.dev, c->stream))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, 2, 0, 0, 1, springs_lam2(M, N), kRtolFit, kMaxitFit,
+                     c->stream)))
+    return rc;
+  if ((rc = grid_store(c->gw, M, N, 2, au.dev, 2, c->stream))) return rc;
+  arg_back(c, au);
+  int hb = 0;
+  ALDIC_CUDA(cudaMemcpyAsync(&hb, dnum, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = check_grid_err(c))) return rc;
+  if (bad_num) *bad_num = hb;
+  return OK;
+}
+
+int aldic_subpb2(aldic_ctx *c, int M, int N, double step, double beta, double mu,
+                 const double *U, const double *F, const double *udual, const double *vdual,
+                 double *Uhat) {
+  ALDIC_CHECK(c && U && F && udual && vdual && Uhat && M > 1 && N > 1 && step > 0, E_ARG,
+              "subpb2: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> au, af, aud, avd, ao;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_in(c, F, 4 * n, af)) ||
+      (rc = arg_in(c, udual, 4 * n, aud)) || (rc = arg_in(c, vdual, 2 * n, avd)) ||
+      (rc = arg_out(c, Uhat, 2 * n, ao)))
+    return rc;
+  if ((rc = fe_rhs(c->gw, M, N, step, beta, mu, au.dev, af.dev, aud.dev, avd.dev, c->stream)))
+    return rc;
+  if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, beta, mu, step, 0, kRtolFE, kMaxitFE, c->stream)))
+    return rc;
+  if ((rc = fe_store(c->gw, M, N, ao.dev, c->stream))) return rc;
+  arg_back(c, ao);
+  return check_grid_err(c);
+}
+
+int aldic_nodal_strain(aldic_ctx *c, int M, int N, double step, const double *U, double *F) {
+  ALDIC_CHECK(c && U && F && M > 1 && N > 1 && step > 0, E_ARG, "nodal_strain: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  Arg<double> au, af;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_out(c, F, 4 * n, af))) return rc;
+  if ((rc = nodal_strain(M, N, step, au.dev, af.dev, c->stream))) return rc;
+  arg_back(c, af);
+  return finish(c, af.staged);
+}
+
+int aldic_gridfit_springs(aldic_ctx *c, int M, int N, int nf, const double *in, double *out) {
+  ALDIC_CHECK(c && in && out && M > 1 && N > 1 && nf >= 1 && nf <= 6, E_ARG,
+              "gridfit_springs: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> ai, ao;
+  if ((rc = arg_in(c, in, nf * n, ai)) || (rc = arg_out(c, out, nf * n, ao))) return rc;
+  // field-major input: one field of n values after another (stride 1)
+  for (int f = 0; f < nf; ++f)
+    if ((rc = gridfit_load(c->gw, M, N, 1, ai.dev + f * n, 1, nullptr, c->stream, f))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, nf, 0, 0, 1, springs_lam2(M, N), kRtolFit, kMaxitFit,
+                     c->stream)))
+    return rc;
+  for (int f = 0; f < nf; ++f)
+    if ((rc = grid_store(c->gw, M, N, 1, ao.dev + f * n, 1, c->stream, f))) return rc;
+  arg_back(c, ao);
+  return check_grid_err(c);
+}
+
+int aldic_inpaint_springs(aldic_ctx *c, int M, int N, int nf, double *z) {
+  ALDIC_CHECK(c && z && M > 0 && N > 0 && nf >= 1 && nf <= 6, E_ARG, "inpaint_springs: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> az;
+  if ((rc = arg_out(c, z, nf * n, az, true))) return rc;
+  for (int f = 0; f < nf; ++f)
+    if ((rc = inpaint_load(c->gw, M, N, 1, az.dev + f * n, 1, nullptr, c->stream, f))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, nf, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, c->stream)))
+    return rc;
+  for (int f = 0; f < nf; ++f)
+    if ((rc = inpaint_store(c->gw, M, N, 1, az.dev + f * n, 1, c->stream, f))) return rc;
+  arg_back(c, az);
+  return check_grid_err(c);
+}
+
+static int smooth_dev(aldic_ctx *c, int M, int N, int nf, double *vals) {
+  // funSmoothDisp.m:64-101 / funSmoothStrain.m:63-109: twice (gridfit, nanconv)
+  int rc;
+  const double lam2 = springs_lam2(M, N);
+  for (int pass = 0; pass < 2; ++pass) {
+    if ((rc = gridfit_load(c->gw, M, N, nf, vals, nf, nullptr, c->stream))) return rc;
+    if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, nf, 0, 0, 1, lam2, kRtolFit, kMaxitFit, c->stream)))
+      return rc;
+    if ((rc = nanconv3(c->gw, M, N, nf, c->stream))) return rc;
+    if ((rc = grid_store(c->gw, M, N, nf, vals, nf, c->stream))) return rc;
+  }
+  return OK;
+}
+
+int aldic_smooth(aldic_ctx *c, int M, int N, int nf, double *vals) {
+  ALDIC_CHECK(c && vals && M > 1 && N > 1 && nf >= 1 && nf <= 6, E_ARG, "smooth: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> av;
+  if ((rc = arg_out(c, vals, nf * n, av, true))) return rc;
+  if ((rc = smooth_dev(c, M, N, nf, av.dev))) return rc;
+  arg_back(c, av);
+  return check_grid_err(c);
+}
+
+}  // extern "C"
+
+// ======================================================================
+// frame pipeline
+namespace {
+
+struct FrameBufs {
+  double *sx, *sy, *su, *sv, *scc;   // search outputs (ny x nx)
+  double *coords, *x0, *y0, *U0;
+  double *U1, *F1, *H21, *U2, *F2, *udual, *vdual, *U2old, *U1old;
+  double *err;                      // [6] Err1, [6] Err2, misc
+  double *beta;                     // [1]
+  double *upd;                      // [2*16] update norms
+  double *part;                     // [1024]
+  int *it1, *itb;
+  unsigned char *bad;
+  int *ints;                        // [8] bad num, nconv, ...
+  double *meanit;
+};
+
+__global__ void k_mesh_init(int M, int N, const double *sx, const double *sy, const double *su,
+                            const double *sv, double *coords, double *x0, double *y0,
+                            double *U0) {
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    const long long src = (long long)j + (long long)i * N;  // ny x nx column-major
+    coords[k] = sx[src];
+    coords[n + k] = sy[src];
+    x0[k] = sx[src];
+    y0[k] = sy[src];
+    U0[2 * k] = su[src];
+    U0[2 * k + 1] = sv[src];
+  }
+}
+
+__global__ void k_zero(double *a, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    a[k] = 0.0;
+}
+
+__global__ void k_set1(double *a, double v) { *a = v; }
+
+__global__ void k_scale_store(const double *src, double *dst, double s) { *dst = *src * s; }
+
+// main_ALDIC.m:285-301: beta from the sweep (device-side so the frame stays
+// capturable); err[0..5] = Err1, err[6..11] = Err2, betas on the fly
+__global__ void k_beta_select(const double *err, double base, double *beta_out) {
+  const double bl[6] = {1e-3, 3.1622776601683795e-3, 1e-2, 3.1622776601683794e-2, 1e-1,
+                        3.1622776601683794e-1};
+  double bs[6], e1[6], e2[6];
+  for (int k = 0; k < 6; ++k) {
+    bs[k] = bl[k] * base;
+    e1[k] = err[k];
+    e2[k] = err[6 + k];
+  }
+  double m1 = 0, m2 = 0;
+  for (int k = 0; k < 6; ++k) { m1 += e1[k]; m2 += e2[k]; }
+  m1 /= 6; m2 /= 6;
+  double v1 = 0, v2 = 0;
+  for (int k = 0; k < 6; ++k) { v1 += (e1[k] - m1) * (e1[k] - m1); v2 += (e2[k] - m2) * (e2[k] - m2); }
+  v1 = sqrt(v1 / 5); v2 = sqrt(v2 / 5);
+  double es[6];
+  int ib = 0;
+  for (int k = 0; k < 6; ++k) {
+    es[k] = (e1[k] - m1) / v1 + (e2[k] - m2) / v2;
+    if (es[k] < es[ib]) ib = k;
+  }
+  double beta;
+  if (ib >= 1 && ib <= 4) {
+    const double x0 = log10(bs[ib - 1]), x1 = log10(bs[ib]), x2 = log10(bs[ib + 1]);
+    const double y0 = es[ib - 1], y1 = es[ib], y2 = es[ib + 1];
+    const double d01 = (y1 - y0) / (x1 - x0), d12 = (y2 - y1) / (x2 - x1);
+    const double p1 = (d12 - d01) / (x2 - x0);
+    const double p2 = d01 - p1 * (x0 + x1);
+    beta = pow(10.0, -p2 / 2.0 / p1);
+  } else {
+    beta = bs[ib];
+  }
+  *beta_out = beta;
+}
+
+template <typename T>
+T *carve(char *&p, long long count) {
+  T *r = (T *)p;
+  p += ((sizeof(T) * count + 255) / 256) * 256;
+  return r;
+}
+
+int frame_geometry(aldic_ctx *c, const aldic_frame_params *p, int gx[2], int gy[2], int *M, int *N) {
+  gx[0] = p->gridx[0]; gx[1] = p->gridx[1];
+  gy[0] = p->gridy[0]; gy[1] = p->gridy[1];
+  if (gx[0] == 0 && gx[1] == 0) { gx[0] = 1; gx[1] = c->W; }
+  if (gy[0] == 0 && gy[1] == 0) { gy[0] = 1; gy[1] = c->H; }
+  int rc = search_dims(c->W, c->H, gx, gy, p->winsize, p->step, p->search, M, N, nullptr, nullptr);
+  if (rc) {
+    set_error("frame: winsize, step and search must be positive");
+    return rc;
+  }
+  if (*M < 2 || *N < 2) {
+    set_error("frame: fewer than 2 x 2 grid points after trimming");
+    return E_ARG;
+  }
+  return OK;
+}
+
+// All device work of one frame, stream-ordered, no host synchronisation.
+// stage mark: an event record node when the stream is being captured
+int mark(aldic_ctx *c, int k) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ALDIC_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+  ALDIC_CUDA(cudaEventRecordWithFlags(c->ev[k], c->stream,
+                                      cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                          : cudaEventRecordDefault));
+  return OK;
+}
+
+int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, int M, int N,
+                 const int gx[2], const int gy[2]) {
+  cudaStream_t st = c->stream;
+  int rcm;
+  if ((rcm = mark(c, 0))) return rcm;
+  const long long n = (long long)M * N;
+  const double h = (double)p->step, mu = p->mu;
+  const double lam2 = springs_lam2(M, N);
+  const int nb = (int)((n + 255) / 256 > 1184 ? 1184 : (n + 255) / 256);
+  int rc;
+  // Section 2: normalise the deformed image (the reference's was done once)
+  if (!c->prepared && (rc = prep_def(c))) return rc;
+  if ((rc = mark(c, 1))) return rc;
+  // Section 3: integer search, MeshSetUp, Init (inpaint_nans of u, v)
+  if ((rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H, c->stats.as<double>() + 2, gx,
+                       gy, p->winsize, p->step, p->search, B.sx, B.sy, B.su, B.sv, B.scc, nullptr,
+                       nullptr, st)))
+    return rc;
+  k_mesh_init<<<nb, 256, 0, st>>>(M, N, B.sx, B.sy, B.su, B.sv, B.coords, B.x0, B.y0, B.U0);
+  if ((rc = inpaint_load(c->gw, M, N, 2, B.U0, 2, nullptr, st, 0))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 2, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 2, B.U0, 2, st, 0))) return rc;
+  // Section 4: LocalICGN + post-processing
+  if ((rc = mark(c, 2))) return rc;
+  const IcgnImages im = images_of(c);
+  if ((rc = icgn(im, B.coords, n, B.U0, nullptr, p->winsize, p->tol, p->precision, B.U1, B.F1,
+                 B.it1, B.H21, c->queue.as<unsigned int>(), st)))
+    return rc;
+  if ((rc = mark(c, 3))) return rc;
+  if ((rc = icgn_flags(M, N, B.it1, B.bad, B.ints, B.meanit, B.ints + 1, st))) return rc;
+  if ((rc = inpaint_load(c->gw, M, N, 2, B.U1, 2, B.bad, st, 0))) return rc;
+  if ((rc = inpaint_load(c->gw, M, N, 4, B.F1, 4, B.bad, st, 2))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 6, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 2, B.U1, 2, st, 0))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 4, B.F1, 4, st, 2))) return rc;
+  // Section 5
+  if ((rc = mark(c, 4))) return rc;
+  if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F1))) return rc;
+  k_zero<<<nb, 256, 0, st>>>(B.udual, 4 * n);
+  k_zero<<<nb, 256, 0, st>>>(B.vdual, 2 * n);
+  if (p->beta > 0) {
+    k_set1<<<1, 1, 0, st>>>(B.beta, p->beta);
+  } else {
+    const double base = h * h * mu;
+    const double bl[6] = {1e-3, std::sqrt(1e-5), 1e-2, std::sqrt(1e-3), 1e-1, std::sqrt(1e-1)};
+    for (int k = 0; k < 6; ++k) {
+      const double bk = bl[k] * base;
+      if ((rc = fe_rhs(c->gw, M, N, h, bk, mu, B.U1, B.F1, B.udual, B.vdual, st))) return rc;
+      if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, bk, mu, h, 0, kRtolFE, kMaxitFE, st))) return rc;
+      if ((rc = fe_store(c->gw, M, N, B.U2, st))) return rc;
+      if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
+      if ((rc = vdiffnorm(B.U1, B.U2, 2 * n, B.part, B.err + k, st))) return rc;
+      if ((rc = vdiffnorm(B.F1, B.F2, 4 * n, B.part, B.err + 6 + k, st))) return rc;
+    }
+    k_beta_select<<<1, 1, 0, st>>>(B.err, base, B.beta);
+  }
+  if ((rc = fe_rhs(c->gw, M, N, h, 0, mu, B.U1, B.F1, B.udual, B.vdual, st, B.beta))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, 0, mu, h, 0, kRtolFE, kMaxitFE, st, B.beta))) return rc;
+  if ((rc = fe_store(c->gw, M, N, B.U2, st))) return rc;
+  if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
+  if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F2))) return rc;
+  if ((rc = vsub(B.F2, B.F1, B.udual, 4 * n, st))) return rc;
+  if ((rc = vsub(B.U2, B.U1, B.vdual, 2 * n, st))) return rc;
+  ALDIC_CUDA(cudaMemcpyAsync(B.U1old, B.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+  // Section 6: ADMM iterations
+  if ((rc = mark(c, 5))) return rc;
+  const double inv = 1.0 / std::sqrt((double)(2 * n));
+  for (int a = 0; a < p->n_admm; ++a) {
+    ALDIC_CUDA(cudaMemcpyAsync(B.U2old, B.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    if ((rc = subpb1(im, B.coords, n, B.U2, B.F2, B.vdual, B.H21, nullptr, p->winsize, mu, p->tol,
+                     p->precision, B.U1, B.itb, c->queue.as<unsigned int>(), st)))
+      return rc;
+    if ((rc = gridfit_load(c->gw, M, N, 2, B.U1, 2, B.itb, st))) return rc;
+    if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, 2, 0, 0, 1, lam2, kRtolFit, kMaxitFit, st))) return rc;
+    if ((rc = grid_store(c->gw, M, N, 2, B.U1, 2, st))) return rc;
+    ALDIC_CUDA(cudaMemcpyAsync(B.F1, B.F2, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, st));
+    if (a < 16) {
+      if ((rc = vdiffnorm(B.U1old, B.U1, 2 * n, B.part, B.upd + 16 + a, st))) return rc;
+      k_scale_store<<<1, 1, 0, st>>>(B.upd + 16 + a, B.upd + 16 + a, inv);
+    }
+    ALDIC_CUDA(cudaMemcpyAsync(B.U1old, B.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    if (p->smooth && (rc = smooth_dev(c, M, N, 2, B.U1))) return rc;
+    if ((rc = fe_rhs(c->gw, M, N, h, 0, mu, B.U1, B.F1, B.udual, B.vdual, st, B.beta))) return rc;
+    if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, 0, mu, h, 0, kRtolFE, kMaxitFE, st, B.beta))) return rc;
+    if ((rc = fe_store(c->gw, M, N, B.U2, st))) return rc;
+    if (p->smooth && (rc = smooth_dev(c, M, N, 2, B.U2))) return rc;
+    if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
+    if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F2))) return rc;
+    if (a < 16) {
+      if ((rc = vdiffnorm(B.U2old, B.U2, 2 * n, B.part, B.upd + a, st))) return rc;
+      k_scale_store<<<1, 1, 0, st>>>(B.upd + a, B.upd + a, inv);
+    }
+    if ((rc = vsub(B.F2, B.F1, B.udual, 4 * n, st))) return rc;
+    if ((rc = vsub(B.U2, B.U1, B.vdual, 2 * n, st))) return rc;
+  }
+  if ((rc = mark(c, 6))) return rc;
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aldic_frame_dims(aldic_ctx *c, const aldic_frame_params *p, int *M, int *N) {
+  ALDIC_CHECK(c && p && M && N && c->have_ref, E_ARG, "frame_dims: bad arguments");
+  int gx[2], gy[2];
+  return frame_geometry(c, p, gx, gy, M, N);
+}
+
+int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y0, double *U,
+                double *F, int32_t *iters, aldic_frame_stats *stats) {
+  ALDIC_CHECK(c && p, E_ARG, "frame: null argument");
+  ALDIC_CHECK(c->have_ref && c->have_def, E_STATE, "frame: set both images first");
+  ALDIC_CHECK(p->n_admm >= 0 && p->n_admm <= 64, E_ARG, "frame: n_admm must be in [0, 64]");
+  ALDIC_CHECK(p->tol > 0 && p->mu > 0, E_ARG, "frame: tol and mu must be positive");
+  ALDIC_CHECK(p->tol2 <= 0, E_ARG, "frame: the tol2 early stop is not supported on this path; pass tol2 <= 0 and read update_y");
+  Guard g(c);
+  int gx[2], gy[2], M, N;
+  int rc = frame_geometry(c, p, gx, gy, &M, &N);
+  if (rc) return rc;
+  const long long n = (long long)M * N;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  // frame slab
+  const long long ny_nx = n;
+  const size_t need = 256 * 40 + sizeof(double) * (5 * ny_nx + 2 * n + 2 * n + 2 * n + 2 * n + 4 * n +
+                                                   21 * n + 2 * n + 4 * n + 4 * n + 2 * n + 2 * n +
+                                                   2 * n + 64 + 1024) +
+                      sizeof(int) * (2 * n + 16) + n + 256;
+  bool realloc = c->fr.cap < need;
+  if ((rc = c->fr.ensure(need))) return rc;
+  char *q = (char *)c->fr.p;
+  FrameBufs B;
+  B.sx = carve<double>(q, n); B.sy = carve<double>(q, n); B.su = carve<double>(q, n);
+  B.sv = carve<double>(q, n); B.scc = carve<double>(q, n);
+  B.coords = carve<double>(q, 2 * n); B.x0 = carve<double>(q, n); B.y0 = carve<double>(q, n);
+  B.U0 = carve<double>(q, 2 * n); B.U1 = carve<double>(q, 2 * n); B.F1 = carve<double>(q, 4 * n);
+  B.H21 = carve<double>(q, 21 * n); B.U2 = carve<double>(q, 2 * n); B.F2 = carve<double>(q, 4 * n);
+  B.udual = carve<double>(q, 4 * n); B.vdual = carve<double>(q, 2 * n);
+  B.U2old = carve<double>(q, 2 * n); B.U1old = carve<double>(q, 2 * n);
+  B.err = carve<double>(q, 16); B.beta = carve<double>(q, 4); B.upd = carve<double>(q, 32);
+  B.part = carve<double>(q, 1024); B.meanit = carve<double>(q, 4);
+  B.it1 = carve<int>(q, n); B.itb = carve<int>(q, n); B.ints = carve<int>(q, 16);
+  B.bad = carve<unsigned char>(q, n);
+  // graph key: geometry and every parameter that changes the recorded work
+  char key[512];
+  snprintf(key, sizeof key, "%d %d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %.17g %d %d %d|%p %p %p",
+           c->W, c->H, c->dtype, (int)realloc, p->winsize, p->step, p->search[0], p->search[1],
+           gx[0], gx[1], gy[0], gy[1], p->tol, p->mu, p->beta, p->n_admm, p->precision, p->smooth,
+           c->fr.p, c->gw_vec.p, c->g_raw.p);
+  const bool want_graph = p->use_graph && !c->graph_failed;
+  if (want_graph && c->graph && c->graph_key != key) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  if (want_graph && !c->graph) {
+    cudaGraph_t gr = nullptr;
+    bool okc = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (okc) {
+      int rc2 = frame_device(c, p, B, M, N, gx, gy);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+      okc = rc2 == OK && e == cudaSuccess && gr;
+      if (okc) okc = cudaGraphInstantiate(&c->graph, gr, 0) == cudaSuccess;
+      if (okc) {
+        size_t nn = 0;
+        cudaGraphGetNodes(gr, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(gr, nodes.data(), &nn);
+        int kn = 0;
+        for (auto nd : nodes) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kn++;
+        }
+        c->graph_kernels = kn;
+      }
+      if (gr) cudaGraphDestroy(gr);
+    }
+    cudaGetLastError();
+    if (!okc) {
+      c->graph = nullptr;
+      c->graph_failed = true;  // fall back to direct launches from now on
+    } else {
+      c->graph_key = key;
+    }
+  }
+  if (c->graph && want_graph) {
+    ALDIC_CUDA(cudaGraphLaunch(c->graph, c->stream));
+  } else {
+    if ((rc = frame_device(c, p, B, M, N, gx, gy))) return rc;
+  }
+  // outputs
+  Arg<double> ax, ay, au, af;
+  Arg<int32_t> ai;
+  if ((rc = arg_out(c, x0, n, ax)) || (rc = arg_out(c, y0, n, ay)) || (rc = arg_out(c, U, 2 * n, au)) ||
+      (rc = arg_out(c, F, 4 * n, af)) || (rc = arg_out(c, iters, n, ai)))
+    return rc;
+  if (ax.dev) ALDIC_CUDA(cudaMemcpyAsync(ax.dev, B.x0, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  if (ay.dev) ALDIC_CUDA(cudaMemcpyAsync(ay.dev, B.y0, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  if (au.dev) ALDIC_CUDA(cudaMemcpyAsync(au.dev, B.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, c->stream));
+  if (af.dev) ALDIC_CUDA(cudaMemcpyAsync(af.dev, B.F2, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, c->stream));
+  if (ai.dev) ALDIC_CUDA(cudaMemcpyAsync(ai.dev, B.it1, sizeof(int) * n, cudaMemcpyDeviceToDevice, c->stream));
+  arg_back(c, ax); arg_back(c, ay); arg_back(c, au); arg_back(c, af); arg_back(c, ai);
+  if (stats) {
+    struct {
+      double upd[32];
+      double beta;
+      double meanit;
+      int ints[16];
+    } hs;
+    ALDIC_CUDA(cudaMemcpyAsync(hs.upd, B.upd, sizeof(hs.upd), cudaMemcpyDeviceToHost, c->stream));
+    ALDIC_CUDA(cudaMemcpyAsync(&hs.beta, B.beta, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ALDIC_CUDA(cudaMemcpyAsync(&hs.meanit, B.meanit, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ALDIC_CUDA(cudaMemcpyAsync(hs.ints, B.ints, sizeof(hs.ints), cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = check_grid_err(c))) return rc;
+    memset(stats, 0, sizeof(*stats));
+    stats->M = M;
+    stats->N = N;
+    stats->admm_steps = p->n_admm;
+    stats->bad_icgn = hs.ints[0];
+    stats->converged_icgn = hs.ints[1];
+    stats->beta = hs.beta;
+    stats->mean_iters_icgn = hs.meanit;
+    stats->kernel_launches = (c->graph && want_graph) ? c->graph_kernels : -1;
+    for (int k = 0; k < 6; ++k) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]) == cudaSuccess) stats->t_stage_ms[k] = ms;
+    }
+    float tot = 0.f;
+    if (cudaEventElapsedTime(&tot, c->ev[0], c->ev[6]) == cudaSuccess) stats->t_stage_ms[6] = tot;
+    cudaGetLastError();
+    for (int a = 0; a < 16; ++a) {
+      stats->update_y[a] = hs.upd[a];
+      stats->update_y2[a] = hs.upd[16 + a];
+    }
+    return OK;
+  }
+  const bool staged = ax.staged || ay.staged || au.staged || af.staged || ai.staged;
+  if (staged) return check_grid_err(c);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+}  // extern "C"

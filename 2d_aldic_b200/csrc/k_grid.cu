@@ -1,0 +1,707 @@
+// k_grid.cu -- solvers and field kernels on the M x N node grid of the
+// uniform Q4 mesh (MeshSetUp.m): Subproblem 2 (Subpb2.m), nodal strain
+// (funGlobal_NodalStrainAvg.m), gridfit 'springs' (gridfit.m), spring
+// inpainting (inpaint_nans.m method 4), the bad-subset flags of LocalICGN.m /
+// Subpb1.m and the 3x3 Gaussian nanconv of funSmoothDisp.m.
+//
+// All systems are SPD and solved by Jacobi-preconditioned CG in FP64 inside
+// ONE cooperative persistent launch: blocks meet at a bounded grid barrier
+// (two per iteration -- the search direction p = z + beta*p_prev is formed on
+// the fly from ping-pong buffers, so no barrier separates its update from the
+// next mat-vec).  Dot products are per-block partials summed in block order
+// by every block, so all blocks take identical convergence decisions and the
+// result is bit-reproducible.  Several right-hand sides (u and v, or the four
+// components of F) share the operator and are solved in the same launch.
+#include <cooperative_groups.h>
+
+#include "aldic_internal.cuh"
+#include "kernels.cuh"
+
+namespace aldic {
+
+namespace {
+
+constexpr int PCG_THREADS = 256;
+constexpr int MAXRHS = 6;
+
+struct PcgArgs {
+  double *x, *r, *z, *p0, *p1, *q, *b, *diag, *part;
+  const unsigned char *mask;
+  int M, N, nrhs, maxit, blocks;
+  double beta, mu, h, lam2, rtol;
+  const double *beta_ptr;  // if set, beta is read from device memory
+  GridSync gs;
+  int *iters_out;
+};
+
+// Scalar Q4 element matrices on a square element of size h, local nodes
+// (-,-), (+,-), (+,+), (-,+): Laplacian stiffness and consistent mass (the
+// 3x3 Gauss rule of Subpb2.m:100-101 integrates both exactly).
+__constant__ double c_K[4][4] = {{4.0 / 6, -1.0 / 6, -2.0 / 6, -1.0 / 6},
+                                 {-1.0 / 6, 4.0 / 6, -1.0 / 6, -2.0 / 6},
+                                 {-2.0 / 6, -1.0 / 6, 4.0 / 6, -1.0 / 6},
+                                 {-1.0 / 6, -2.0 / 6, -1.0 / 6, 4.0 / 6}};
+__constant__ double c_Mm[4][4] = {{4.0 / 36, 2.0 / 36, 1.0 / 36, 2.0 / 36},
+                                  {2.0 / 36, 4.0 / 36, 2.0 / 36, 1.0 / 36},
+                                  {1.0 / 36, 2.0 / 36, 4.0 / 36, 2.0 / 36},
+                                  {2.0 / 36, 1.0 / 36, 2.0 / 36, 4.0 / 36}};
+
+// local node index -> (di, dj) offset from the element's first node
+__device__ __forceinline__ int lx(int a) { return (a == 1 || a == 2) ? 1 : 0; }
+__device__ __forceinline__ int ly(int a) { return (a >= 2) ? 1 : 0; }
+
+template <int OP>
+__device__ __forceinline__ double op_diag(const PcgArgs &A, int i, int j, long long k, int f) {
+  const int M = A.M, N = A.N;
+  if (OP == OP_FE) {
+    int ne = 0;
+    for (int ej = j - 1; ej <= j; ++ej)
+      for (int ei = i - 1; ei <= i; ++ei) ne += (ei >= 0 && ei < M - 1 && ej >= 0 && ej < N - 1);
+    return ne * (A.beta * (4.0 / 6.0) + A.mu * A.h * A.h * (4.0 / 36.0));
+  } else if (OP == OP_GRIDFIT) {
+    const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
+    const int na = (i > 0) + (i < M - 1) + (j > 0) + (j < N - 1);
+    const int nd = (i > 0 && j > 0) + (i < M - 1 && j > 0) + (i > 0 && j < N - 1) +
+                   (i < M - 1 && j < N - 1);
+    return w + A.lam2 * (na + 0.5 * nd);
+  } else {
+    if (!A.mask[(long long)f * M * N + k]) return 1.0;
+    return (double)((i > 0) + (i < M - 1) + (j > 0) + (j < N - 1));
+  }
+}
+
+// y = op(v)_k where v(node) is supplied by the functor
+template <int OP, typename Fv>
+__device__ __forceinline__ double op_apply(const PcgArgs &A, int i, int j, long long k, int f,
+                                           Fv v) {
+  const int M = A.M, N = A.N;
+  if (OP == OP_FE) {
+    double y = 0.0;
+    const double kb = A.beta, km = A.mu * A.h * A.h;
+    for (int ej = j - 1; ej <= j; ++ej)
+      for (int ei = i - 1; ei <= i; ++ei) {
+        if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
+        const int la = (i - ei) + (j - ej) * 3 - 2 * (i - ei) * (j - ej);  // (0,0)->0 (1,0)->1 (1,1)->2 (0,1)->3
+#pragma unroll
+        for (int lb = 0; lb < 4; ++lb) {
+          const int ni = ei + lx(lb), nj = ej + ly(lb);
+          y += (kb * c_K[la][lb] + km * c_Mm[la][lb]) * v((long long)nj * M + ni);
+        }
+      }
+    return y;
+  } else if (OP == OP_GRIDFIT) {
+    const double xk = v(k);
+    double s = 0.0, sd = 0.0;
+    if (i > 0) s += xk - v(k - 1);
+    if (i < M - 1) s += xk - v(k + 1);
+    if (j > 0) s += xk - v(k - M);
+    if (j < N - 1) s += xk - v(k + M);
+    if (i > 0 && j > 0) sd += xk - v(k - M - 1);
+    if (i < M - 1 && j > 0) sd += xk - v(k - M + 1);
+    if (i > 0 && j < N - 1) sd += xk - v(k + M - 1);
+    if (i < M - 1 && j < N - 1) sd += xk - v(k + M + 1);
+    const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
+    return w * xk + A.lam2 * (s + 0.5 * sd);
+  } else {
+    const unsigned char *unk = A.mask + (long long)f * M * N;
+    const double xk = v(k);
+    if (!unk[k]) return xk;
+    double s = 0.0;
+    if (i > 0) s += xk - (unk[k - 1] ? v(k - 1) : 0.0);
+    if (i < M - 1) s += xk - (unk[k + 1] ? v(k + 1) : 0.0);
+    if (j > 0) s += xk - (unk[k - M] ? v(k - M) : 0.0);
+    if (j < N - 1) s += xk - (unk[k + M] ? v(k + M) : 0.0);
+    return s;
+  }
+}
+
+// block reduction of up to 2*MAXRHS doubles into part[slot][f][blockIdx]
+__device__ void block_partials(double *vals, int cnt, double *part, int blocks, int slot_base) {
+  __shared__ double sh[PCG_THREADS / 32][2 * MAXRHS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = 0; c < cnt; ++c) {
+    const double v = warp_sum(vals[c]);
+    if (lane == 0) sh[wid][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < cnt) {
+    double t = 0.0;
+    for (int w = 0; w < PCG_THREADS / 32; ++w) t += sh[w][threadIdx.x];
+    part[(long long)(slot_base + threadIdx.x) * blocks + blockIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double sum_partials(const double *part, int slot, int blocks) {
+  double t = 0.0;
+  for (int b = 0; b < blocks; ++b) t += part[(long long)slot * blocks + b];
+  return t;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
+  if (A.beta_ptr) A.beta = *A.beta_ptr;
+  const long long n = (long long)A.M * A.N;
+  const int nr = A.nrhs;
+  const long long tid0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  __shared__ double s_g[4 * MAXRHS];
+  // slots: [0,nr) rz  [nr,2nr) rr  [2nr,3nr) bb  [3nr,4nr) pq
+  double acc[2 * MAXRHS];
+  // ---- r = b - A x, z = D^-1 r; partial rz, rr, bb
+  for (int c = 0; c < 2 * MAXRHS; ++c) acc[c] = 0.0;
+  double accb[MAXRHS];
+  for (int c = 0; c < MAXRHS; ++c) accb[c] = 0.0;
+  for (long long k = tid0; k < n; k += stride) {
+    const int i = (int)(k % A.M), j = (int)(k / A.M);
+    for (int f = 0; f < nr; ++f) {
+      const double *xf = A.x + f * n;
+      const double ax = op_apply<OP>(A, i, j, k, f, [&](long long q) { return xf[q]; });
+      const double bv = A.b[f * n + k];
+      const double rv = bv - ax;
+      const double d = op_diag<OP>(A, i, j, k, f);
+      const double zv = rv / d;
+      A.r[f * n + k] = rv;
+      A.z[f * n + k] = zv;
+      A.diag[f * n + k] = d;
+      A.p1[f * n + k] = 0.0;
+      acc[f] += rv * zv;
+      acc[MAXRHS + f] += rv * rv;
+      accb[f] += bv * bv;
+    }
+  }
+  {
+    double v[3 * MAXRHS];
+    for (int f = 0; f < nr; ++f) {
+      v[f] = acc[f];
+      v[nr + f] = acc[MAXRHS + f];
+    }
+    block_partials(v, 2 * nr, A.part, A.blocks, 0);
+    for (int f = 0; f < nr; ++f) v[f] = accb[f];
+    block_partials(v, nr, A.part, A.blocks, 2 * nr);
+  }
+  if (!grid_sync(A.gs, A.blocks)) return;
+  double rz[MAXRHS], bb[MAXRHS], betaf[MAXRHS];
+  bool done[MAXRHS];
+  for (int f = 0; f < nr; ++f) {
+    rz[f] = sum_partials(A.part, f, A.blocks);
+    const double rr = sum_partials(A.part, nr + f, A.blocks);
+    bb[f] = sum_partials(A.part, 2 * nr + f, A.blocks);
+    done[f] = !(rr > A.rtol * A.rtol * bb[f]);
+    betaf[f] = 0.0;
+  }
+  (void)s_g;
+  int it = 0;
+  for (; it < A.maxit; ++it) {
+    bool all = true;
+    for (int f = 0; f < nr; ++f) all &= done[f];
+    if (all) break;
+    double *pc = (it & 1) ? A.p1 : A.p0;
+    const double *pp = (it & 1) ? A.p0 : A.p1;
+    // ---- p = z + beta p_prev (own nodes), q = A p (neighbours on the fly)
+    for (int c = 0; c < nr; ++c) acc[c] = 0.0;
+    for (long long k = tid0; k < n; k += stride) {
+      const int i = (int)(k % A.M), j = (int)(k / A.M);
+      for (int f = 0; f < nr; ++f) {
+        if (done[f]) continue;
+        const double *zf = A.z + f * n;
+        const double *pf = pp + f * n;
+        const double bt = betaf[f];
+        const double pk = zf[k] + bt * pf[k];
+        pc[f * n + k] = pk;
+        const double qk =
+            op_apply<OP>(A, i, j, k, f, [&](long long q) { return zf[q] + bt * pf[q]; });
+        A.q[f * n + k] = qk;
+        acc[f] += pk * qk;
+      }
+    }
+    block_partials(acc, nr, A.part, A.blocks, 3 * nr);
+    if (!grid_sync(A.gs, A.blocks)) return;
+    double alpha[MAXRHS];
+    for (int f = 0; f < nr; ++f) alpha[f] = done[f] ? 0.0 : rz[f] / sum_partials(A.part, 3 * nr + f, A.blocks);
+    // ---- x += alpha p, r -= alpha q, z = D^-1 r
+    for (int c = 0; c < 2 * MAXRHS; ++c) acc[c] = 0.0;
+    for (long long k = tid0; k < n; k += stride) {
+      for (int f = 0; f < nr; ++f) {
+        if (done[f]) continue;
+        const long long o = f * n + k;
+        A.x[o] += alpha[f] * pc[o];
+        const double rv = A.r[o] - alpha[f] * A.q[o];
+        const double zv = rv / A.diag[o];
+        A.r[o] = rv;
+        A.z[o] = zv;
+        acc[f] += rv * zv;
+        acc[MAXRHS + f] += rv * rv;
+      }
+    }
+    {
+      double v[2 * MAXRHS];
+      for (int f = 0; f < nr; ++f) {
+        v[f] = acc[f];
+        v[nr + f] = acc[MAXRHS + f];
+      }
+      block_partials(v, 2 * nr, A.part, A.blocks, 0);
+    }
+    if (!grid_sync(A.gs, A.blocks)) return;
+    for (int f = 0; f < nr; ++f) {
+      if (done[f]) continue;
+      const double rzn = sum_partials(A.part, f, A.blocks);
+      const double rr = sum_partials(A.part, nr + f, A.blocks);
+      betaf[f] = rzn / rz[f];
+      rz[f] = rzn;
+      done[f] = !(rr > A.rtol * A.rtol * bb[f]);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *A.iters_out = it;
+    bool all = true;
+    for (int f = 0; f < nr; ++f) all &= done[f];
+    if (!all) atomicExch(A.gs.err, 2);  // not converged within maxit
+  }
+}
+
+// ------------------------------------------------------------------ Subpb2 RHS
+// Subpb2.m:88-149 per node, gathered from its (up to 4) elements.
+__global__ void k_fe_rhs(int M, int N, double h, double beta, const double *beta_ptr, double mu,
+                         const double *__restrict__ U, const double *__restrict__ F,
+                         const double *__restrict__ ud, const double *__restrict__ vd,
+                         double *__restrict__ b) {
+  if (beta_ptr) beta = *beta_ptr;
+  const long long n = (long long)M * N;
+  const double gp[3] = {-0.7745966692414834, 0.0, 0.7745966692414834};  // sqrt(3/5)
+  const double gw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    // F - W with the column order [4a-3, 4a-1, 4a-2, 4a] of Subpb2.m:88-91
+    const double fw0 = F[4 * k + 0] - ud[4 * k + 0];
+    const double fw1 = F[4 * k + 2] - ud[4 * k + 2];
+    const double fw2 = F[4 * k + 1] - ud[4 * k + 1];
+    const double fw3 = F[4 * k + 3] - ud[4 * k + 3];
+    double bu = 0.0, bv = 0.0;
+    for (int ej = j - 1; ej <= j; ++ej)
+      for (int ei = i - 1; ei <= i; ++ei) {
+        if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
+        const int la = (i - ei) + (j - ej) * 3 - 2 * (i - ei) * (j - ej);
+        double uvu[4], uvv[4];
+        for (int lb = 0; lb < 4; ++lb) {
+          const long long q = (long long)(ej + ly(lb)) * M + (ei + lx(lb));
+          uvu[lb] = U[2 * q] - vd[2 * q];
+          uvv[lb] = U[2 * q + 1] - vd[2 * q + 1];
+        }
+        for (int ti = 0; ti < 3; ++ti)
+          for (int tj = 0; tj < 3; ++tj) {
+            const double ksi = gp[ti], eta = gp[tj];
+            const double Nn[4] = {(1 - ksi) * (1 - eta) * 0.25, (1 + ksi) * (1 - eta) * 0.25,
+                                  (1 + ksi) * (1 + eta) * 0.25, (1 - ksi) * (1 + eta) * 0.25};
+            const double dks[4] = {-(1 - eta) / 4, (1 - eta) / 4, (1 + eta) / 4, -(1 + eta) / 4};
+            const double det_[4] = {-(1 - ksi) / 4, -(1 + ksi) / 4, (1 + ksi) / 4, (1 - ksi) / 4};
+            const double s = (0.25 * h * h) * (gw[ti] * gw[tj]);
+            const double gx = (2.0 / h) * dks[la], gy = (2.0 / h) * det_[la];
+            double nu = 0.0, nv = 0.0;
+            for (int lb = 0; lb < 4; ++lb) {
+              nu += Nn[lb] * uvu[lb];
+              nv += Nn[lb] * uvv[lb];
+            }
+            bu += s * (beta * (gx * fw0 + gy * fw1) + mu * Nn[la] * nu);
+            bv += s * (beta * (gx * fw2 + gy * fw3) + mu * Nn[la] * nv);
+          }
+      }
+    b[k] = bu;
+    b[n + k] = bv;
+  }
+}
+
+__global__ void k_fe_init(long long n, double *__restrict__ x, unsigned char *mask) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < 2 * n;
+       k += (long long)gridDim.x * blockDim.x) {
+    x[k] = 0.0;
+    mask[k] = 1;
+  }
+}
+
+__global__ void k_fe_store(long long n, const double *__restrict__ x, double *__restrict__ U) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    U[2 * k] = x[k];
+    U[2 * k + 1] = x[n + k];
+  }
+}
+
+// ------------------------------------------------------------------ nodal strain
+// funGlobal_NodalStrainAvg.m:51-144: per element, DN*U at the 2x2 Gauss points
+// in the order (-,-), (+,-), (+,+), (-,+); extrapolated to the corners with
+// the matrix of :105-108; averaged over the elements sharing a node.  Output
+// slots per node are [du/dx, du/dy, dv/dx, dv/dy] as written at :123-137.
+__global__ void k_nodal_strain(int M, int N, double h, const double *__restrict__ U,
+                               double *__restrict__ F) {
+  const long long n = (long long)M * N;
+  const double r3 = 0.5773502691896257;  // 1/sqrt(3)
+  const double s3 = 1.7320508075688772;
+  const double gks[4] = {-r3, r3, r3, -r3}, get_[4] = {-r3, -r3, r3, r3};
+  const double E[4][4] = {{1 + 0.5 * s3, -0.5, 1 - 0.5 * s3, -0.5},
+                          {-0.5, 1 + 0.5 * s3, -0.5, 1 - 0.5 * s3},
+                          {1 - 0.5 * s3, -0.5, 1 + 0.5 * s3, -0.5},
+                          {-0.5, 1 - 0.5 * s3, -0.5, 1 + 0.5 * s3}};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    double acc[4] = {0, 0, 0, 0};
+    int cnt = 0;
+    for (int ej = j - 1; ej <= j; ++ej)
+      for (int ei = i - 1; ei <= i; ++ei) {
+        if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
+        const int la = (i - ei) + (j - ej) * 3 - 2 * (i - ei) * (j - ej);
+        double ue[8];
+        for (int lb = 0; lb < 4; ++lb) {
+          const long long q = (long long)(ej + ly(lb)) * M + (ei + lx(lb));
+          ue[2 * lb] = U[2 * q];
+          ue[2 * lb + 1] = U[2 * q + 1];
+        }
+        double G[4][4];
+        for (int g = 0; g < 4; ++g) {
+          const double ksi = gks[g], eta = get_[g];
+          const double dks[4] = {-(1 - eta) / 4, (1 - eta) / 4, (1 + eta) / 4, -(1 + eta) / 4};
+          const double det_[4] = {-(1 - ksi) / 4, -(1 + ksi) / 4, (1 + ksi) / 4, (1 - ksi) / 4};
+          double v[4] = {0, 0, 0, 0};
+          for (int a = 0; a < 4; ++a) {
+            const double gx = (2.0 / h) * dks[a], gy = (2.0 / h) * det_[a];
+            v[0] += gx * ue[2 * a];
+            v[1] += gy * ue[2 * a];
+            v[2] += gx * ue[2 * a + 1];
+            v[3] += gy * ue[2 * a + 1];
+          }
+          for (int c = 0; c < 4; ++c) G[g][c] = v[c];
+        }
+        for (int c = 0; c < 4; ++c) {
+          double s = 0.0;
+          for (int g = 0; g < 4; ++g) s += E[la][g] * G[g][c];
+          acc[c] += s;
+        }
+        cnt++;
+      }
+    for (int c = 0; c < 4; ++c) F[4 * k + c] = acc[c] / cnt;
+  }
+}
+
+// ------------------------------------------------------------------ loaders
+__global__ void k_gridfit_load(int M, int N, int nf, const double *__restrict__ vals, int stride,
+                               const int *__restrict__ iters, double *__restrict__ b,
+                               double *__restrict__ x, unsigned char *__restrict__ mask) {
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const bool bad = iters && (iters[k] < 0 || iters[k] > 99);
+    for (int f = 0; f < nf; ++f) {
+      const double v = vals[k * stride + f];
+      const bool ok = !bad && !isnan(v);
+      mask[f * n + k] = ok;
+      b[f * n + k] = ok ? v : 0.0;
+      x[f * n + k] = ok ? v : 0.0;
+    }
+  }
+}
+
+
+__global__ void k_grid_store(int M, int N, int nf, const double *__restrict__ x,
+                             double *__restrict__ vals, int stride) {
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    for (int f = 0; f < nf; ++f) vals[k * stride + f] = x[f * n + k];
+}
+
+__global__ void k_inpaint_load(int M, int N, int nf, const double *__restrict__ vals, int stride,
+                               const unsigned char *__restrict__ badmask,
+                               double *__restrict__ b, double *__restrict__ x,
+                               unsigned char *__restrict__ mask) {
+  // fields [0, nf) of vals land in slots f0.. of the work vectors (the
+  // caller offsets b, x, mask by f0 * n)
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    for (int f = 0; f < nf; ++f) {
+      auto known = [&](long long q) {
+        return !(badmask && badmask[q]) && !isnan(vals[q * stride + f]);
+      };
+      const bool kn = known(k);
+      mask[f * n + k] = !kn;
+      double bv;
+      if (kn) {
+        bv = vals[k * stride + f];
+      } else {
+        bv = 0.0;
+        if (i > 0 && known(k - 1)) bv += vals[(k - 1) * stride + f];
+        if (i < M - 1 && known(k + 1)) bv += vals[(k + 1) * stride + f];
+        if (j > 0 && known(k - M)) bv += vals[(k - M) * stride + f];
+        if (j < N - 1 && known(k + M)) bv += vals[(k + M) * stride + f];
+      }
+      b[f * n + k] = bv;
+      x[f * n + k] = kn ? bv : 0.0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ flags
+__global__ void k_icgn_flags(long long n, const int *__restrict__ it,
+                             unsigned char *__restrict__ bad, int *badnum, double *meanit,
+                             int *nconv) {
+  __shared__ long long sh[32][3];
+  __shared__ double shd[32];
+  __shared__ double s_mean, s_thr;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  long long cb = 0, c102 = 0, sg = 0, ng = 0;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    const int v = it[k];
+    const bool b1 = v < 0 || v > 99;
+    cb += b1;
+    c102 += (v == 102);
+    if (!b1) {
+      sg += v;
+      ng++;
+    }
+  }
+  cb = warp_sum_ll(cb); c102 = warp_sum_ll(c102); sg = warp_sum_ll(sg); ng = warp_sum_ll(ng);
+  if (lane == 0) { sh[wid][0] = cb; sh[wid][1] = c102; sh[wid][2] = sg; shd[wid] = (double)ng; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long a = 0, b = 0, c = 0, d = 0;
+    for (int w = 0; w < nw; ++w) { a += sh[w][0]; b += sh[w][1]; c += sh[w][2]; d += (long long)shd[w]; }
+    *badnum = (int)(a - b);
+    *nconv = (int)d;
+    s_mean = d ? (double)c / (double)d : __longlong_as_double(0x7ff8000000000000ll);
+    *meanit = s_mean;
+    sh[0][0] = d;
+  }
+  __syncthreads();
+  const long long ngood = sh[0][0];
+  const double m = s_mean;
+  double ss = 0.0;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    const int v = it[k];
+    if (!(v < 0 || v > 99)) ss += (v - m) * (v - m);
+  }
+  ss = warp_sum(ss);
+  __syncthreads();
+  if (lane == 0) shd[wid] = ss;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += shd[w];
+    const double sd = ngood > 1 ? sqrt(t / (double)(ngood - 1))
+                                : (ngood == 1 ? 0.0 : __longlong_as_double(0x7ff8000000000000ll));
+    s_thr = m + 0.15 * sd;
+  }
+  __syncthreads();
+  const double thr = s_thr;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    const int v = it[k];
+    bad[k] = (v < 0 || v > 99 || (double)v > thr) ? 1 : 0;
+  }
+}
+
+__global__ void k_subpb1_flags(long long n, const int *__restrict__ it,
+                               unsigned char *__restrict__ bad, int *badnum) {
+  __shared__ long long sh[32];
+  long long c = 0;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    const bool b = it[k] < 0 || it[k] > 99;
+    bad[k] = b;
+    c += b;
+  }
+  c = warp_sum_ll(c);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    *badnum = (int)t;
+  }
+}
+
+// nanconv(z, fspecial('gaussian',3,0.5), 'edge', 'nanout') with no NaN input
+__global__ void k_nanconv3(int M, int N, int nf, const double *__restrict__ in,
+                           double *__restrict__ out) {
+  const long long n = (long long)M * N;
+  const double e1 = 0.1353352832366127;   // exp(-2)
+  const double e2 = 0.01831563888873418;  // exp(-4)
+  const double ks = 1.0 + 4.0 * e1 + 4.0 * e2;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * nf;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long kk = k % n, f = k / n;
+    const int i = (int)(kk % M), j = (int)(kk / M);
+    double s = 0.0, w = 0.0;
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) {
+        const int ii = i + di, jj = j + dj;
+        if (ii < 0 || ii >= M || jj < 0 || jj >= N) continue;
+        const int d2 = di * di + dj * dj;
+        const double kv = (d2 == 0 ? 1.0 : (d2 == 1 ? e1 : e2)) / ks;
+        s += kv * in[f * n + (long long)jj * M + ii];
+        w += kv;
+      }
+    out[k] = s / w;
+  }
+}
+
+__global__ void k_vsub(const double *a, const double *b, double *o, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    o[k] = a[k] - b[k];
+}
+
+__global__ void k_diffnorm_part(const double *a, const double *b, long long n, double *part) {
+  double s = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const double d = a[k] - b[k];
+    s += d * d;
+  }
+  s = warp_sum(s);
+  __shared__ double sh[32];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_diffnorm_final(const double *part, int np, double *res) {
+  double t = 0.0;
+  for (int k = 0; k < np; ++k) t += part[k];
+  *res = sqrt(t);
+}
+
+inline int blocks_for(long long n, int threads = 256) {
+  long long b = (n + threads - 1) / threads;
+  if (b > 148 * 8) b = 148 * 8;
+  return b < 1 ? 1 : (int)b;
+}
+
+}  // namespace
+
+int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
+             double lam2, double rtol, int maxit, cudaStream_t st, const double *beta_ptr) {
+  ALDIC_CHECK(nrhs >= 1 && nrhs <= MAXRHS, E_ARG, "grid_pcg: 1..6 right-hand sides");
+  const long long n = (long long)M * N;
+  int dev = 0, sms = 148, per = 1;
+  ALDIC_CUDA(cudaGetDevice(&dev));
+  ALDIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  void *fn = op == OP_FE ? (void *)k_pcg<OP_FE>
+                         : (op == OP_GRIDFIT ? (void *)k_pcg<OP_GRIDFIT> : (void *)k_pcg<OP_INPAINT>);
+  ALDIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, PCG_THREADS, 0));
+  long long blocks = (long long)sms * (per < 1 ? 1 : per);
+  const long long need = (n + PCG_THREADS - 1) / PCG_THREADS;
+  if (blocks > need) blocks = need;
+  if (blocks > w.max_blocks) blocks = w.max_blocks;
+  if (blocks < 1) blocks = 1;
+  PcgArgs A;
+  A.x = w.x; A.r = w.r; A.z = w.z; A.p0 = w.p; A.p1 = w.p + MAXRHS * n; A.q = w.q; A.b = w.b;
+  A.diag = w.diag; A.part = w.part; A.mask = w.mask;
+  A.M = M; A.N = N; A.nrhs = nrhs; A.maxit = maxit; A.blocks = (int)blocks;
+  A.beta = beta; A.mu = mu; A.h = h; A.lam2 = lam2; A.rtol = rtol;
+  A.gs.count = w.bar; A.gs.gen = w.bar + 1; A.gs.err = w.err;
+  A.iters_out = w.iters_out;
+  A.beta_ptr = beta_ptr;
+  ALDIC_CUDA(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned int), st));
+  void *args[] = {&A};
+  ALDIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(PCG_THREADS), args, 0, st));
+  return OK;
+}
+
+int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
+           const double *F, const double *udual, const double *vdual, cudaStream_t st,
+           const double *beta_ptr) {
+  const long long n = (long long)M * N;
+  k_fe_rhs<<<blocks_for(n), 256, 0, st>>>(M, N, h, beta, beta_ptr, mu, U, F, udual, vdual, w.b);
+  k_fe_init<<<blocks_for(2 * n), 256, 0, st>>>(n, w.x, w.mask);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st) {
+  const long long n = (long long)M * N;
+  k_fe_store<<<blocks_for(n), 256, 0, st>>>(n, w.x, Uhat);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st) {
+  const long long n = (long long)M * N;
+  k_nodal_strain<<<blocks_for(n), 256, 0, st>>>(M, N, h, U, F);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int gridfit_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
+                 const int *bad_iters, cudaStream_t st, int f0) {
+  const long long n = (long long)M * N;
+  k_gridfit_load<<<blocks_for(n), 256, 0, st>>>(M, N, nf, vals, stride, bad_iters, w.b + f0 * n,
+                                                w.x + f0 * n, w.mask + f0 * n);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int grid_store(const GridWork &w, int M, int N, int nf, double *vals, int stride,
+               cudaStream_t st, int f0) {
+  const long long n = (long long)M * N;
+  k_grid_store<<<blocks_for(n), 256, 0, st>>>(M, N, nf, w.x + f0 * n, vals, stride);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int inpaint_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
+                 const unsigned char *badmask, cudaStream_t st, int f0) {
+  const long long n = (long long)M * N;
+  k_inpaint_load<<<blocks_for(n), 256, 0, st>>>(M, N, nf, vals, stride, badmask, w.b + f0 * n,
+                                                w.x + f0 * n, w.mask + f0 * n);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int inpaint_store(const GridWork &w, int M, int N, int nf, double *vals, int stride,
+                  cudaStream_t st, int f0) {
+  return grid_store(w, M, N, nf, vals, stride, st, f0);
+}
+
+int icgn_flags(int M, int N, const int *iters, unsigned char *badmask, int *d_badnum,
+               double *d_meaniters, int *d_nconv, cudaStream_t st) {
+  k_icgn_flags<<<1, 1024, 0, st>>>((long long)M * N, iters, badmask, d_badnum, d_meaniters,
+                                   d_nconv);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int subpb1_flags(int n, const int *iters, unsigned char *badmask, int *d_badnum,
+                 cudaStream_t st) {
+  k_subpb1_flags<<<1, 1024, 0, st>>>(n, iters, badmask, d_badnum);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int nanconv3(GridWork &w, int M, int N, int nf, cudaStream_t st) {
+  const long long n = (long long)M * N;
+  k_nanconv3<<<blocks_for(n * nf), 256, 0, st>>>(M, N, nf, w.x, w.r);
+  ALDIC_CUDA(cudaMemcpyAsync(w.x, w.r, sizeof(double) * n * nf, cudaMemcpyDeviceToDevice, st));
+  return OK;
+}
+
+int vsub(const double *a, const double *b, double *out, long long n, cudaStream_t st) {
+  k_vsub<<<blocks_for(n), 256, 0, st>>>(a, b, out, n);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int vdiffnorm(const double *a, const double *b, long long n, double *part, double *res,
+              cudaStream_t st) {
+  const int nb = 148;
+  k_diffnorm_part<<<nb, 256, 0, st>>>(a, b, n, part);
+  k_diffnorm_final<<<1, 1, 0, st>>>(part, nb, res);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace aldic

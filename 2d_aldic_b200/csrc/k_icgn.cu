@@ -1,0 +1,500 @@
+// k_icgn.cu -- local IC-GN (funICGN.m) and the ADMM local step
+// (funICGN_Subpb1.m) for every subset of a frame in one persistent launch.
+//
+// Mapping: one warp per subset; warps pull subset indices from a global
+// atomic counter, so subsets that converge early free their warp at once
+// (per-subset early exit with load balance).  Each lane owns pixels
+// lane, lane+32, ... of the (w+1)^2 subset.  Per iteration a lane samples the
+// deformed image at its warped pixels (Keys bicubic, a = -1/2, as
+// ba_interp2.cpp) and accumulates 8 residual sums in the working precision;
+// the warp reduces them in FP64 with a butterfly (every lane ends with the
+// identical value, so control flow stays warp-uniform), and every lane then
+// forms b, the convergence test and dP = -H\b with the FP64 Cholesky factor
+// of H, and applies the inverse-compositional update in FP64.
+//
+// ZNSSD residual (funICGN.m:238): r = (f - fbar)/bf - (g - gbar)/bg.  With
+// sd_k the steepest-descent images,
+//   b2_k = S_fk/bf - (T_k - gm S_k)/bg,
+// where S_fk = sum sd_k (f - fbar), S_k = sum sd_k are fixed per subset and
+// T_k = sum sd_k (g - c), gm = mean(g) - c are accumulated per iteration with
+// the shift c = fbar (which keeps the one-pass variance well conditioned).
+#include "aldic_internal.cuh"
+#include "kernels.cuh"
+
+namespace aldic {
+
+namespace {
+
+constexpr int WARPS = 8;  // warps per CTA
+
+struct Args {
+  IcgnImages im;
+  const double *coords;
+  long long n;
+  const double *U0;     // IC-GN: U0; Subpb1: UOld
+  const double *FOld;   // Subpb1
+  const double *vdual;  // Subpb1
+  const double *H21in;  // Subpb1
+  const int *wins;
+  int w;
+  double tol, mu;
+  double *U, *F, *H21out;
+  int *iters;
+  unsigned int *queue;
+};
+
+__device__ __forceinline__ double nan64() { return __longlong_as_double(0x7ff8000000000000ll); }
+
+// Subset bounds of funICGN.m:34-50: integral, Df index x-3 in [1, W-6].
+__device__ __forceinline__ bool subset_ok(const IcgnImages &im, double x0, double y0, int w,
+                                          int *xl, int *yl) {
+  const double a = x0 - 0.5 * w, b = y0 - 0.5 * w;
+  if (a != floor(a) || b != floor(b)) return false;
+  *xl = (int)a;
+  *yl = (int)b;
+  return *xl >= 4 && *yl >= 4 && *xl + w <= im.W - 3 && *yl + w <= im.H - 3;
+}
+
+template <typename Real> struct Img;
+template <> struct Img<float> {
+  static __device__ __forceinline__ const float *f(const IcgnImages &m) { return m.f32; }
+  static __device__ __forceinline__ const float *g(const IcgnImages &m) { return m.g32; }
+  static __device__ __forceinline__ const float *gx(const IcgnImages &m) { return m.gx32; }
+  static __device__ __forceinline__ const float *gy(const IcgnImages &m) { return m.gy32; }
+};
+template <> struct Img<double> {
+  static __device__ __forceinline__ const double *f(const IcgnImages &m) { return m.f64; }
+  static __device__ __forceinline__ const double *g(const IcgnImages &m) { return m.g64; }
+  static __device__ __forceinline__ const double *gx(const IcgnImages &m) { return m.gx64; }
+  static __device__ __forceinline__ const double *gy(const IcgnImages &m) { return m.gy64; }
+};
+
+// Cholesky of the 6x6 SPD matrix (lower, packed row-wise in L[21]).
+__device__ bool chol6(const double H[36], double L[21]) {
+  int idx = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = H[i * 6 + j];
+      for (int k = 0; k < j; ++k) s -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+      if (i == j) {
+        if (!(s > 0.0)) return false;
+        L[idx++] = sqrt(s);
+      } else {
+        L[idx++] = s / L[j * (j + 1) / 2 + j];
+      }
+    }
+  return true;
+}
+
+__device__ void chol6_solve(const double *L, const double b[6], double x[6]) {
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double t = b[i];
+    for (int k = 0; k < i; ++k) t -= L[i * (i + 1) / 2 + k] * y[k];
+    y[i] = t / L[i * (i + 1) / 2 + i];
+  }
+  for (int i = 5; i >= 0; --i) {
+    double t = y[i];
+    for (int k = i + 1; k < 6; ++k) t -= L[k * (k + 1) / 2 + i] * x[k];
+    x[i] = t / L[i * (i + 1) / 2 + i];
+  }
+}
+
+// inverse-compositional update of funICGN.m:268-286
+__device__ __forceinline__ bool ic_compose(double P[6], const double d[6]) {
+  const double det = (1 + d[0]) * (1 + d[3]) - d[1] * d[2];
+  if (!(det != 0.0)) return false;
+  const double t1 = (-d[0] - d[0] * d[3] + d[1] * d[2]) / det;
+  const double t2 = -d[1] / det;
+  const double t3 = -d[2] / det;
+  const double t4 = (-d[3] - d[0] * d[3] + d[1] * d[2]) / det;
+  const double t5 = (-d[4] - d[3] * d[4] + d[2] * d[5]) / det;
+  const double t6 = (-d[5] - d[0] * d[5] + d[1] * d[4]) / det;
+  const double a11 = 1 + P[0], a12 = P[2], a13 = P[4];
+  const double a21 = P[1], a22 = 1 + P[3], a23 = P[5];
+  P[0] = a11 * (1 + t1) + a12 * t2 - 1;
+  P[1] = a21 * (1 + t1) + a22 * t2;
+  P[2] = a11 * t3 + a12 * (1 + t4);
+  P[3] = a21 * t3 + a22 * (1 + t4) - 1;
+  P[4] = a11 * t5 + a12 * t6 + a13;
+  P[5] = a21 * t5 + a22 * t6 + a23;
+  return true;
+}
+
+// Keys bicubic sample of img (W wide) around the 0-based floor corner
+// (cx, cy) with fractional parts (tu, tv).
+template <typename Real>
+__device__ __forceinline__ Real sample(const Real *__restrict__ img, int W, int cx, int cy,
+                                       Real tu, Real tv) {
+  Real wu[4], wv[4];
+  keys_w(tu, wu);
+  keys_w(tv, wv);
+  const Real *p = img + (long long)(cy - 1) * W + (cx - 1);
+  Real acc = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const Real *q = p + (long long)r * W;
+    Real s = wu[0] * __ldg(q) + wu[1] * __ldg(q + 1) + wu[2] * __ldg(q + 2) + wu[3] * __ldg(q + 3);
+    acc += wv[r] * s;
+  }
+  return acc;
+}
+
+template <typename Real, bool SUB>
+__device__ void process(const Args &a, long long s, int lane, double *Lsh) {
+  const IcgnImages &im = a.im;
+  const double x0 = a.coords[s], y0 = a.coords[a.n + s];
+  int w = a.wins ? a.wins[s] : a.w;
+  double P[6];
+  if (SUB) {
+    for (int q = 0; q < 4; ++q) P[q] = a.FOld[4 * s + q];
+    P[4] = a.U0[2 * s];
+    P[5] = a.U0[2 * s + 1];
+  } else {
+    P[0] = P[1] = P[2] = P[3] = 0.0;
+    P[4] = a.U0[2 * s];
+    P[5] = a.U0[2 * s + 1];
+  }
+  int xl, yl;
+  bool ok = subset_ok(im, x0, y0, w, &xl, &yl);
+  int status = 0;
+  if (ok) {
+    // masked-pixel test of funICGN.m:54-65
+    const Real *gx = Img<Real>::gx(im);
+    int cnt = 0;
+    const int nw = w + 1, npx = nw * nw;
+    for (int p = lane; p < npx; p += 32) {
+      const int iy = p / nw, ix = p - iy * nw;
+      cnt += gx[(long long)(yl - 1 + iy) * im.W + (xl - 1 + ix)] == (Real)0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    const double nn = (double)npx;
+    if (!((double)cnt < 0.5 * nn)) {
+      status = 102;
+    } else if ((double)cnt > 0.1 * nn) {
+      w = (int)round(sqrt(2.0) * w);
+      ok = subset_ok(im, x0, y0, w, &xl, &yl);
+    }
+  }
+  if (!ok) {
+    // LocalICGN.m:75-80 / Subpb1.m:89-92: catch -> -1 and NaN
+    if (lane == 0) {
+      a.iters[s] = -1;
+      a.U[2 * s] = nan64();
+      a.U[2 * s + 1] = nan64();
+      if (!SUB) {
+        for (int q = 0; q < 4; ++q) a.F[4 * s + q] = nan64();
+        for (int q = 0; q < 21; ++q) a.H21out[(long long)q * a.n + s] = 0.0;
+      }
+    }
+    return;
+  }
+  if (status == 102) {
+    if (lane == 0) {
+      a.iters[s] = 102;
+      a.U[2 * s] = P[4];
+      a.U[2 * s + 1] = P[5];
+      if (!SUB) {
+        for (int q = 0; q < 4; ++q) a.F[4 * s + q] = P[q];
+        for (int q = 0; q < 21; ++q) a.H21out[(long long)q * a.n + s] = 0.0;
+      }
+    }
+    return;
+  }
+
+  const Real *fI = Img<Real>::f(im);
+  const Real *gI = Img<Real>::g(im);
+  const Real *gxI = Img<Real>::gx(im);
+  const Real *gyI = Img<Real>::gy(im);
+  const int nw = w + 1, npx = nw * nw;
+  // pixel (ix, iy) of the subset sits at X = ox + ix, Y = oy + iy relative to
+  // the node (exact in FP32; half-integers when w is odd)
+  const double oxd = (double)xl - x0, oyd = (double)yl - y0;
+  const Real ox = (Real)oxd, oy = (Real)oyd;
+  const int W = im.W;
+  const long long base = (long long)(yl - 1) * W + (xl - 1);  // subset top-left, 0-based
+
+  // ---- pass 1: sum f, and H (funICGN.m:67-79)
+  double sf;
+  double Hs[18];
+  {
+    Real af = 0;
+    Real hh[18];
+#pragma unroll
+    for (int q = 0; q < 18; ++q) hh[q] = 0;
+    for (int p = lane; p < npx; p += 32) {
+      const int iy = p / nw, ix = p - iy * nw;
+      const long long k = base + (long long)iy * W + ix;
+      af += fI[k];
+      if (!SUB) {
+        const Real fx = gxI[k], fy = gyI[k];
+        const Real X = ox + (Real)ix, Y = oy + (Real)iy;
+        const Real fxx = fx * fx, fyy = fy * fy, fxy = fx * fy;
+        const Real XX = X * X, YY = Y * Y, XY = X * Y;
+        hh[0] += XX * fxx;  hh[1] += XX * fxy;  hh[2] += XY * fxx;  hh[3] += XY * fxy;
+        hh[4] += X * fxx;   hh[5] += X * fxy;   hh[6] += XX * fyy;  hh[7] += XY * fyy;
+        hh[8] += X * fyy;   hh[9] += YY * fxx;  hh[10] += YY * fxy; hh[11] += Y * fxx;
+        hh[12] += Y * fxy;  hh[13] += YY * fyy; hh[14] += Y * fyy;  hh[15] += fxx;
+        hh[16] += fxy;      hh[17] += fyy;
+      }
+    }
+    sf = warp_sum((double)af);
+    if (!SUB) {
+#pragma unroll
+      for (int q = 0; q < 18; ++q) Hs[q] = warp_sum((double)hh[q]);
+    }
+  }
+  const double meanf = sf / (double)npx;
+  // ---- pass 2: bf, S_fk = sum sd_k (f - fbar), S_k = sum sd_k
+  double ssf, Sf[6], Sk[6];
+  {
+    const Real mf = (Real)meanf;
+    Real a2 = 0, sfk[6], sk[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sfk[q] = sk[q] = 0;
+    for (int p = lane; p < npx; p += 32) {
+      const int iy = p / nw, ix = p - iy * nw;
+      const long long k = base + (long long)iy * W + ix;
+      const Real d = fI[k] - mf;
+      a2 += d * d;
+      const Real fx = gxI[k], fy = gyI[k];
+      if (SUB) {
+        sfk[4] += fx * d; sfk[5] += fy * d;
+        sk[4] += fx; sk[5] += fy;
+      } else {
+        const Real X = ox + (Real)ix, Y = oy + (Real)iy;
+        const Real sd[6] = {fx * X, fy * X, fx * Y, fy * Y, fx, fy};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          sfk[q] += sd[q] * d;
+          sk[q] += sd[q];
+        }
+      }
+    }
+    // residual of the shift mf vs meanf, exact in FP64
+    const double dm = (double)mf - meanf;
+    ssf = warp_sum((double)a2);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      Sk[q] = (SUB && q < 4) ? 0.0 : warp_sum((double)sk[q]);
+      Sf[q] = (SUB && q < 4) ? 0.0 : warp_sum((double)sfk[q]) + dm * Sk[q];
+    }
+    // sum (f - meanf)^2 = sum (f - mf)^2 + 2 dm sum(f - mf) + n dm^2
+    ssf = ssf + 2.0 * dm * (sf - (double)npx * (double)mf) + (double)npx * dm * dm;
+  }
+  const double bf = sqrt(ssf);
+
+  // ---- Hessian factor (IC-GN) or the damped 2x2 system (Subpb1)
+  double Hm[36];
+  bool spd = true;
+  double s2 = 0, Ha = 0, Hb = 0, Hd = 0;
+  if (!SUB) {
+    const double *q = Hs;
+    const double H[36] = {q[0], q[1], q[2], q[3], q[4], q[5],  q[1], q[6], q[3], q[7], q[5], q[8],
+                          q[2], q[3], q[9], q[10], q[11], q[12], q[3], q[7], q[10], q[13], q[12], q[14],
+                          q[4], q[5], q[11], q[12], q[15], q[16], q[5], q[8], q[12], q[14], q[16], q[17]};
+#pragma unroll
+    for (int k = 0; k < 36; ++k) Hm[k] = H[k];
+    if (lane == 0) spd = chol6(Hm, Lsh);
+    spd = __shfl_sync(0xffffffffu, (int)spd, 0);
+    __syncwarp();
+  } else {
+    // funICGN_Subpb1.m:73,281-283
+    s2 = 2.0 / (bf * bf);
+    const double h55 = a.H21in[18 * a.n + s], h65 = a.H21in[19 * a.n + s],
+                 h66 = a.H21in[20 * a.n + s];
+    const double H2a = h55 * s2 + a.mu, H2b = h65 * s2, H2d = h66 * s2 + a.mu;
+    const double dmax = H2a > H2d ? H2a : H2d;
+    Ha = H2a + 1e-3 * dmax;
+    Hb = H2b;
+    Hd = H2d + 1e-3 * dmax;
+  }
+
+  // ---- iterations (funICGN.m:107-294 / funICGN_Subpb1.m:94-337)
+  const double tol = a.tol;
+  double normNew = 1, normAbs = 1, normInit = 1;
+  int step = 0;
+  const Real cg = (Real)meanf;
+  // u22 = x0 + ru: split x0 into its floor xb and fraction (0 or 1/2)
+  const double xbd = floor(x0), ybd = floor(y0);
+  const int xb = (int)xbd, yb = (int)ybd;
+  const Real fx0 = (Real)(x0 - xbd), fy0 = (Real)(y0 - ybd);
+  while (step <= 100 && normNew > tol && normAbs > tol) {
+    step++;
+    // out-of-image test (funICGN.m:118): an affine map takes its extremes at
+    // the subset corners
+    bool out = false;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double X = (c & 1) ? oxd + w : oxd, Y = (c & 2) ? oyd + w : oyd;
+      const double u22 = (1 + P[0]) * X + P[2] * Y + (x0 + P[4]);
+      const double v22 = P[1] * X + (1 + P[3]) * Y + (y0 + P[5]);
+      out |= (u22 < 3 || u22 > W - 2 || v22 < 3 || v22 > im.H - 2);
+    }
+    if (out) {
+      normNew = 1e6;
+      break;
+    }
+    bool pfin = true;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) pfin &= isfinite(P[q]);
+    double sums[8];
+    if (pfin) {
+      const Real a11 = (Real)(1 + P[0]), a12 = (Real)P[2], a21 = (Real)P[1],
+                 a22 = (Real)(1 + P[3]), p4 = (Real)P[4], p5 = (Real)P[5];
+      Real s1 = 0, s2r = 0, t[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) t[q] = 0;
+      int iy = lane / nw, ix = lane - (lane / nw) * nw;
+      for (int p = lane; p < npx; p += 32) {
+        const Real X = ox + (Real)ix, Y = oy + (Real)iy;
+        const Real ru = a11 * X + a12 * Y + p4 + fx0;
+        const Real rv = a21 * X + a22 * Y + p5 + fy0;
+        const Real fu = floor(ru), fv = floor(rv);
+        const int cx = xb + (int)fu - 1, cy = yb + (int)fv - 1;  // 0-based floor corner
+        const Real gval = sample<Real>(gI, W, cx, cy, ru - fu, rv - fv);
+        const long long k = base + (long long)iy * W + ix;
+        const Real d = gval - cg;
+        s1 += d;
+        s2r += d * d;
+        const Real fx = gxI[k], fy = gyI[k];
+        const Real ax = fx * d, ay = fy * d;
+        t[4] += ax;
+        t[5] += ay;
+        if (!SUB) {
+          t[0] += ax * X;
+          t[1] += ay * X;
+          t[2] += ax * Y;
+          t[3] += ay * Y;
+        }
+        ix += 32;
+        while (ix >= nw) {
+          ix -= nw;
+          iy++;
+        }
+      }
+      sums[0] = warp_sum((double)s1);
+      sums[1] = warp_sum((double)s2r);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) sums[2 + q] = (SUB && q < 4) ? 0.0 : warp_sum((double)t[q]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sums[q] = nan64();
+    }
+    const double n = (double)npx;
+    const double gm = sums[0] / n;                 // mean(g) - c
+    const double ssg = sums[1] - sums[0] * gm;     // sum (g - gbar)^2
+    const double bg = sqrt(ssg);
+    double b[6], nb = 0;
+    if (!SUB) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const double b2 = Sf[q] / bf - (sums[2 + q] - gm * Sk[q]) / bg;
+        b[q] = bf * b2;
+        nb += b[q] * b[q];
+      }
+    } else {
+      const double b5 = bf * (Sf[4] / bf - (sums[6] - gm * Sk[4]) / bg);
+      const double b6 = bf * (Sf[5] / bf - (sums[7] - gm * Sk[5]) / bg);
+      b[4] = b5 * s2 + a.mu * (P[4] - a.U0[2 * s] - a.vdual[2 * s]);
+      b[5] = b6 * s2 + a.mu * (P[5] - a.U0[2 * s + 1] - a.vdual[2 * s + 1]);
+      nb = b[4] * b[4] + b[5] * b[5];
+    }
+    normNew = sqrt(nb);
+    normAbs = normNew;
+    if (step == 1) normInit = normNew;
+    if (normInit > tol) normNew = normNew / normInit;
+    else normNew = 0;
+    if (normNew < tol || normAbs < tol) break;
+    double dP[6] = {0, 0, 0, 0, 0, 0};
+    if (!SUB) {
+      if (spd) {
+        chol6_solve(Lsh, b, dP);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) dP[q] = -dP[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) dP[q] = nan64();
+      }
+    } else {
+      // 2x2 SPD solve by Cholesky
+      const double l11 = sqrt(Ha), l21 = Hb / l11, l22 = sqrt(Hd - l21 * l21);
+      const double y1 = b[4] / l11, y2 = (b[5] - l21 * y1) / l22;
+      const double x2 = y2 / l22, x1 = (y1 - l21 * x2) / l11;
+      dP[4] = -x1;
+      dP[5] = -x2;
+    }
+    if (!ic_compose(P, dP)) break;
+  }
+  if (!(normNew < tol || normAbs < tol)) step = 101;
+  if (isnan(normNew)) step = 101;
+  if (lane == 0) {
+    a.iters[s] = step;
+    a.U[2 * s] = P[4];
+    a.U[2 * s + 1] = P[5];
+    if (!SUB) {
+      for (int q = 0; q < 4; ++q) a.F[4 * s + q] = P[q];
+      int idx = 0;
+      for (int c = 0; c < 6; ++c)
+        for (int r = c; r < 6; ++r) a.H21out[(long long)(idx++) * a.n + s] = Hm[r * 6 + c];
+    }
+  }
+}
+
+template <typename Real, bool SUB>
+__global__ void __launch_bounds__(WARPS * 32) k_icgn(Args a) {
+  __shared__ double Lsh[WARPS][24];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  while (true) {
+    unsigned int s = 0;
+    if (lane == 0) s = atomicAdd(a.queue, 1u);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if ((long long)s >= a.n) break;
+    process<Real, SUB>(a, (long long)s, lane, Lsh[wid]);
+    __syncwarp();
+  }
+}
+
+template <typename Real, bool SUB>
+int launch(const Args &a, cudaStream_t st) {
+  int dev = 0, sms = 148, per = 1;
+  ALDIC_CUDA(cudaGetDevice(&dev));
+  ALDIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  ALDIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icgn<Real, SUB>, WARPS * 32, 0));
+  if (per < 1) per = 1;
+  long long blocks = (long long)sms * per;
+  const long long need = (a.n + WARPS - 1) / WARPS;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  ALDIC_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned int), st));
+  k_icgn<Real, SUB><<<(int)blocks, WARPS * 32, 0, st>>>(a);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace
+
+int icgn(const IcgnImages &im, const double *coords, long long n, const double *U0,
+         const int *wins, int w, double tol, int precision, double *U, double *F, int *iters,
+         double *H21, unsigned int *queue, cudaStream_t st) {
+  if (n <= 0) return OK;
+  Args a{};
+  a.im = im; a.coords = coords; a.n = n; a.U0 = U0; a.wins = wins; a.w = w; a.tol = tol;
+  a.U = U; a.F = F; a.H21out = H21; a.iters = iters; a.queue = queue;
+  return precision ? launch<double, false>(a, st) : launch<float, false>(a, st);
+}
+
+int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,
+           const double *FOld, const double *vdual, const double *H21, const int *wins, int w,
+           double mu, double tol, int precision, double *U, int *iters, unsigned int *queue,
+           cudaStream_t st) {
+  if (n <= 0) return OK;
+  Args a{};
+  a.im = im; a.coords = coords; a.n = n; a.U0 = UOld; a.FOld = FOld; a.vdual = vdual;
+  a.H21in = H21; a.wins = wins; a.w = w; a.mu = mu; a.tol = tol; a.U = U; a.iters = iters;
+  a.queue = queue;
+  return precision ? launch<double, true>(a, st) : launch<float, true>(a, st);
+}
+
+}  // namespace aldic

@@ -1,0 +1,91 @@
+// kernels.cuh -- launchers of the sm_100a kernels (called by capi.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace aldic {
+
+// ---- k_image.cu
+int roi_stats(const void *img, int dtype, int W, const int roi[4], double *d_stats,
+              unsigned long long *d_isums, double *d_part, cudaStream_t st);
+int normalize(const void *img, int dtype, long long n, const double *d_stats, double *o64,
+              float *o32, cudaStream_t st);
+int gradient(const double *f, const double *mask, int W, int H, double *gx64, double *gy64,
+             float *gx32, float *gy32, cudaStream_t st);
+int interp_f64(const double *F, long long M, long long N, long long P, const double *X,
+               const double *Y, long long n, double *Z, cudaStream_t st);
+int interp_f32(const float *F, long long M, long long N, long long P, const float *X,
+               const float *Y, long long n, float *Z, cudaStream_t st);
+
+// ---- k_search.cu
+int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsize, int step,
+                const int search[2], int *nx, int *ny, int *gx1, int *gy1);
+int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,
+               const int gridx[2], const int gridy[2], int winsize, int step,
+               const int search[2], double *x, double *y, double *u, double *v, double *cc,
+               double *pce, double *ppe, cudaStream_t st);
+
+// ---- k_icgn.cu
+struct IcgnImages {
+  const float *f32, *g32, *gx32, *gy32;
+  const double *f64, *g64, *gx64, *gy64;
+  int W, H;
+};
+int icgn(const IcgnImages &im, const double *coords, long long n, const double *U0,
+         const int *wins, int w, double tol, int precision, double *U, double *F, int *iters,
+         double *H21, unsigned int *queue, cudaStream_t st);
+int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,
+           const double *FOld, const double *vdual, const double *H21, const int *wins, int w,
+           double mu, double tol, int precision, double *U, int *iters, unsigned int *queue,
+           cudaStream_t st);
+
+// ---- k_grid.cu: node-grid solvers and field kernels on the M x N mesh
+struct GridWork {
+  // PCG vectors for up to 6 right-hand sides of M*N (x fastest) each
+  double *x, *r, *z, *p, *q, *b, *diag;
+  double *part;          // per-block partial sums: [3][nrhs][blocks]
+  unsigned char *mask;   // per node flags (data present / unknown)
+  unsigned int *bar;     // grid barrier {count, gen}
+  int *err;              // barrier / solver error flag
+  int *iters_out;        // PCG iterations used
+  int max_blocks;
+};
+enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2 };
+
+// solve op(x) = b for nrhs fields; b and x live in w.b / w.x (field-major)
+int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
+             double lam2, double rtol, int maxit, cudaStream_t st,
+             const double *beta_ptr = nullptr);
+// Subpb2 right-hand side (Subpb2.m:76-159) into w.b (2 fields: u, v)
+int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
+           const double *F, const double *udual, const double *vdual, cudaStream_t st,
+           const double *beta_ptr = nullptr);
+// interleave w.x (2 fields) into Uhat
+int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st);
+// nodal strain (funGlobal_NodalStrainAvg.m)
+int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st);
+// gridfit springs: load nf interleaved (stride, offset) fields, NaN = no data
+int gridfit_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
+                 const int *bad_iters, cudaStream_t st, int f0 = 0);
+int grid_store(const GridWork &w, int M, int N, int nf, double *vals, int stride,
+               cudaStream_t st, int f0 = 0);
+// inpaint springs: load nf fields, nodes flagged (NaN or bad) are unknown
+int inpaint_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
+                 const unsigned char *badmask, cudaStream_t st, int f0 = 0);
+int inpaint_store(const GridWork &w, int M, int N, int nf, double *vals, int stride,
+                  cudaStream_t st, int f0 = 0);
+// LocalICGN.m:117-131 flags; writes badmask and the bad count to d_badnum
+int icgn_flags(int M, int N, const int *iters, unsigned char *badmask, int *d_badnum,
+               double *d_meaniters, int *d_nconv, cudaStream_t st);
+// Subpb1.m:167-169 flags
+int subpb1_flags(int n, const int *iters, unsigned char *badmask, int *d_badnum,
+                 cudaStream_t st);
+// 3x3 Gaussian nanconv with edge normalisation on nf fields (in w.x)
+int nanconv3(GridWork &w, int M, int N, int nf, cudaStream_t st);
+// out = a - b (n elements)
+int vsub(const double *a, const double *b, double *out, long long n, cudaStream_t st);
+// ||a - b||_2 into *res (deterministic)
+int vdiffnorm(const double *a, const double *b, long long n, double *part, double *res,
+              cudaStream_t st);
+
+}  // namespace aldic

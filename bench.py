@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the AL-DIC frame pipeline (integer search -> IC-GN -> ADMM
+Subproblems 1/2) on the large uniform workload: 2048 x 2048 8-bit speckle
+(130k dots, seed 1), sinusoidal displacement u = 2 sin(2 pi y/256),
+v = 1.5 cos(2 pi x/256), noise sigma 2, subset 32, step 8 (~63k subsets),
+search +-16 px, IC-GN tol 1e-2, 3 ADMM iterations, FP32 sampling with FP64
+reductions and solves.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One step = one frame of the pipeline over one deformed image with the
+reference image resident.  Prints one JSON line (rank 0).  Under torchrun
+every rank runs independent frames (frames are independent in accumulative
+mode: weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged subsets/s & frames/s at <=0.01px vs FP64; learned vs FFT init, 1 B200"
+UNIT = "subsets/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="uniform2048")
+    ap.add_argument("--cpu-crop", type=int, default=768,
+                    help="side of the image crop the CPU baseline runs on")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except Exception:
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference arm
+def oracle_sample(wl, crop: int):
+    f, g = wl.images()
+    c = min(crop, wl.W, wl.H)
+    return f[:c, :c].copy(), g[:c, :c].copy(), c
+
+
+def run_oracle_frames(oracle, wl, f, g, k):
+    times, conv = [], 0
+    for _ in range(k):
+        t0 = time.perf_counter()
+        r = oracle.frame(f, g, wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=wl.n_admm)
+        times.append(time.perf_counter() - t0)
+        it = r["iters_icgn"]
+        conv = int(((it >= 1) & (it <= 100)).sum())
+    return times, conv
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    synth = importlib.import_module("2d_aldic_b200.synth")
+    import oracle
+    oracle.set_threads(host_cores())
+    wl = synth.workload(args.workload)
+    f, g, c = oracle_sample(wl, args.cpu_crop)
+    run_oracle_frames(oracle, wl, f, g, max(0, min(args.warmup, 1)))
+    times, conv = run_oracle_frames(oracle, wl, f, g, args.steps)
+    tot = sum(times)
+    value = conv * args.steps / tot
+    sample = (f"{c}x{c} top-left crop of the {args.workload} workload ({conv} converged subsets "
+              f"per frame), full frame pipeline of the FP64 CPU restatement per step")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "frames_per_s": args.steps / tot,
+        "config": {"workload": f"{args.workload} (CPU sample {c}x{c})", "threads": oracle.get_threads()},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is MATLAB and cannot run here; its CPU path is timed through the "
+                "project's FP64 C restatement (OpenMP over subsets, the parfor analogue)",
+    }), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def icgn_bytes(iters: np.ndarray, winsize: int) -> float:
+    """Algorithmic bytes of one IC-GN launch: per subset 12 N (f, df/dx,
+    df/dy as FP32, read once) + 4 N k (the deformed-image footprint per
+    evaluation) + 224 (U, F, H21, status out), N = (w+1)^2, k = evaluations."""
+    N = (winsize + 1) ** 2
+    k = np.where((iters >= 1) & (iters <= 101), iters, 0).astype(np.float64)
+    active = (iters >= 1) & (iters <= 101)
+    return float((12 * N * active + 4 * N * k + 224 * active).sum())
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=dev)
+    aldic = importlib.import_module("2d_aldic_b200")
+    synth = importlib.import_module("2d_aldic_b200.synth")
+    wl = synth.workload(args.workload)
+    f, g = wl.images()
+    H, W = f.shape
+
+    stream = torch.cuda.Stream(device=dev)
+    ctx = aldic.Context(local)
+    ctx.set_stream(stream)
+    al = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=wl.n_admm,
+                     precision=aldic.FP32, ctx=ctx)
+    fd = torch.from_numpy(f).to(dev)
+    gd = torch.from_numpy(g).to(dev)
+    al.set_images(fd, gd)
+    M, N = al.dims()
+    n = M * N
+    out = {"x0": torch.empty(n, dtype=torch.float64, device=dev),
+           "y0": torch.empty(n, dtype=torch.float64, device=dev),
+           "U": torch.empty(2 * n, dtype=torch.float64, device=dev),
+           "F": torch.empty(4 * n, dtype=torch.float64, device=dev),
+           "iters": torch.empty(n, dtype=torch.int32, device=dev)}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def l2_flush(k):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)
+
+    for k in range(args.warmup):
+        al.frame(out, stats=True)
+    torch.cuda.synchronize()
+
+    # ---------------- timed region: K frames, inputs resident in HBM
+    clocks = Clocks(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    icgn_ms, frame_ms, conv, stages = [], [], [], []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        l2_flush(k)
+        ev[k][0].record(stream)
+        r = al.frame(out, stats=True)
+        ev[k][1].record(stream)
+        st = r["stats"]
+        icgn_ms.append(st["t_stage_ms"]["icgn"])
+        frame_ms.append(st["t_stage_ms"]["frame"])
+        conv.append(st["converged_icgn"])
+        stages.append(st["t_stage_ms"])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    csum = torch.tensor([float(sum(conv))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(csum, op=dist.ReduceOp.SUM)
+    total_ms = float(tmax.item())
+    value = float(csum.item()) / (total_ms / 1e3)
+    frames_per_s = world * args.steps / (total_ms / 1e3)
+    iters = out["iters"].cpu().numpy()
+    kernels = r["stats"]["kernel_launches"]
+
+    # ---------------- accuracy vs an FP64 run of the same pipeline (untimed)
+    al64 = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=wl.n_admm,
+                       precision=aldic.FP64, ctx=ctx)
+    r64 = al64.frame(stats=True)
+    U32 = out["U"].cpu().numpy()
+    rms_fp64 = float(np.sqrt(np.mean((U32 - r64["U"]) ** 2)))
+    ut, vt = synth.truth(wl, out["x0"].cpu().numpy(), out["y0"].cpu().numpy())
+    rms_truth = float(np.sqrt(np.mean(np.r_[U32[0::2] - ut, U32[1::2] - vt] ** 2)))
+
+    # ---------------- roofline of the dominant kernel (IC-GN), live events
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    b_icgn = icgn_bytes(iters, wl.winsize)
+    t_icgn = statistics.mean(icgn_ms) / 1e3
+    achieved = b_icgn / t_icgn / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "icgn_traffic.json")))
+        traffic = prof.get("bytes_per_launch")
+    except Exception:
+        pass
+
+    # ---------------- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        g_pin = torch.from_numpy(g).pin_memory()
+        outs_h = {"x0": torch.empty(n, dtype=torch.float64).pin_memory(),
+                  "y0": torch.empty(n, dtype=torch.float64).pin_memory(),
+                  "U": torch.empty(2 * n, dtype=torch.float64).pin_memory(),
+                  "F": torch.empty(4 * n, dtype=torch.float64).pin_memory(),
+                  "iters": torch.empty(n, dtype=torch.int32).pin_memory()}
+        outs_np = {k: v.numpy() for k, v in outs_h.items()}
+        g_np = g_pin.numpy()
+        for _ in range(2):
+            al.set_images(g=g_np)
+            al.frame(outs_np, stats=False)
+        torch.cuda.synchronize()
+        e2e_ms, conv_e = [], int(((outs_np["iters"] >= 1) & (outs_np["iters"] <= 100)).sum())
+        for k in range(args.steps):
+            l2_flush(k)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            al.set_images(g=g_np)          # H2D of the frame's input from pinned memory
+            al.frame(outs_np, stats=False)  # frame + D2H of U, F, x0, y0, iters
+            b.record(stream)
+            b.synchronize()
+            e2e_ms.append(a.elapsed_time(b))
+        tot_e = torch.tensor([float(sum(e2e_ms))], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tot_e, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * conv_e * args.steps / (tot_e.item() / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(g_np.nbytes),
+               "d2h_bytes_per_step": int(sum(v.nbytes for v in outs_np.values())),
+               "frames_per_s": world * args.steps / (tot_e.item() / 1e3)}
+
+    # ---------------- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        oracle.set_threads(host_cores())
+        fs, gs, c = oracle_sample(wl, args.cpu_crop)
+        times, cconv = run_oracle_frames(oracle, wl, fs, gs, 1)
+        cpu = {"value": cconv / times[0], "unit": UNIT, "cores": oracle.get_threads(),
+               "kind": "port",
+               "sample": f"one frame of the FP64 CPU restatement on a {c}x{c} crop of the "
+                         f"workload ({cconv} converged subsets, {times[0]:.1f} s)"}
+
+    if rank == 0:
+        mst = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 sampling/residuals, f64 sums+solves", "data": "synthetic",
+            "frames_per_s": frames_per_s,
+            "accuracy": {"rms_px_vs_fp64_pipeline": rms_fp64, "rms_px_vs_truth": rms_truth,
+                         "fp64_frame_ms": r64["stats"]["t_stage_ms"]["frame"]},
+            "config": {"workload": "uniform2048: 2048x2048 u8 speckle, 130k dots (seed 1), "
+                                   "u=2sin(2pi y/256), v=1.5cos(2pi x/256), noise 2; subset 32, "
+                                   "step 8, search 16, tol 1e-2, 3 ADMM iterations",
+                       "subsets": n, "l2": "flushed between steps (256 MB write)",
+                       "parallelism": f"replicas x{world}",
+                       "stage_ms": mst},
+            "roofline": {"kernel": "k_icgn (IC-GN, FP32)", "bound": "hbm", "achieved": achieved,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": traffic, "peak_source": peak_src,
+                         "bytes_per_launch": b_icgn, "launch_ms": t_icgn * 1e3},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": kernels * args.steps if kernels and kernels > 0 else None,
+            "clocks": clk,
+            "wall_s": t_wall,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,219 @@
+/*
+ * aldic_b200.h -- C ABI of libaldic_b200.so, the B200 (sm_100a) AL-DIC hot path.
+ *
+ * The entry points replace, one for one, the calls of the reference's frame
+ * loop (jyang526843/2D_ALDIC, main_ALDIC.m Sections 2-6) that a MEX gateway
+ * would bind.  Each declaration names the reference interface it replaces.
+ *
+ * Conventions (identical to the reference after ReadImage's transpose):
+ *   - an image is W x H, Img(x, y), x = image column, 1-based coordinates,
+ *     stored x-fastest (MATLAB's column-major W x H array);
+ *   - node order x-fastest; U interleaved [u1 v1 u2 v2 ...]; F per node
+ *     [F11 F21 F12 F22]; coords n x 2 column-major ([x1..xn y1..yn]);
+ *   - H21 is n x 21 column-major (entry k of node j at k*n + j): the packing
+ *     of funICGN.m:320, i.e. HtempPar of LocalICGN.m:46 / HPar of Subpb1.m;
+ *   - status codes in iters: 1..100 converged after that many evaluations,
+ *     101 not converged / left the image / NaN, 102 more than half the subset
+ *     masked, -1 subset outside the valid area (MATLAB's catch branch).
+ *
+ * Memory: every array argument may point to host memory or to device memory
+ * of the context's GPU; the library detects which.  Host arrays are staged
+ * through the context's device buffers and the call returns after the copy
+ * back; device arrays are used in place and the call is stream-ordered on
+ * the context stream (no host synchronisation).  The caller owns all arrays.
+ *
+ * Errors: every function returns ALDIC_OK (0) or a negative code; the text of
+ * the last error of the calling thread is returned by aldic_last_error().
+ * No function aborts the process or longjmps across CUDA frames.
+ */
+#ifndef ALDIC_B200_H
+#define ALDIC_B200_H
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ALDIC_API __attribute__((visibility("default")))
+#else
+#define ALDIC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALDIC_OK 0
+#define ALDIC_E_ARG (-1)
+#define ALDIC_E_STATE (-2)
+#define ALDIC_E_CUDA (-3)
+#define ALDIC_E_TIMEOUT (-4)
+#define ALDIC_E_NOMEM (-5)
+
+#define ALDIC_U8 0
+#define ALDIC_U16 1
+#define ALDIC_F32 2
+#define ALDIC_F64 3
+
+#define ALDIC_FP32 0 /* FP32 sampling/residuals, FP64 sums and 6x6 solve */
+#define ALDIC_FP64 1 /* FP64 throughout */
+
+typedef struct aldic_ctx aldic_ctx;
+
+ALDIC_API int aldic_version(void);
+ALDIC_API const char *aldic_last_error(void);
+
+/* Z = ba_interp2(F, X, Y[, method]) -- ba_interp2.cpp:318-335.
+ * F: M x N x P column-major; X indexes columns (N), Y rows (M), 1-based;
+ * Z: n x P.  Bit-identical to the reference in both precisions.
+ * stream: cudaStream_t (NULL = default stream). */
+ALDIC_API int aldic_ba_interp2_f64(const double *F, int64_t M, int64_t N, int64_t P,
+                         const double *X, const double *Y, int64_t n, double *Z,
+                         void *stream);
+ALDIC_API int aldic_ba_interp2_f32(const float *F, int64_t M, int64_t N, int64_t P,
+                         const float *X, const float *Y, int64_t n, float *Z,
+                         void *stream);
+
+/* Context: device-resident images, gradients and work buffers that persist
+ * across calls (the MEX side keeps one per MATLAB session: mexLock/mexAtExit). */
+ALDIC_API int aldic_ctx_create(int device, aldic_ctx **out);
+ALDIC_API int aldic_ctx_destroy(aldic_ctx *ctx);
+ALDIC_API int aldic_ctx_set_stream(aldic_ctx *ctx, void *stream);
+
+/* Reference image: funNormalizeImg.m:1 (ROI mean/std normalisation) and
+ * funImgGradient.m:1 (7-tap gradients times the mask, DfCropWidth = 3).
+ * roi = {gx1, gx2, gy1, gy2} (gridxyROIRange) or NULL for the whole image;
+ * mask: W*H doubles (ImgRefMask) or NULL. */
+ALDIC_API int aldic_set_ref(aldic_ctx *ctx, const void *img, int dtype, int W, int H,
+                  const int roi[4], const double *mask);
+/* Deformed image: funNormalizeImg.m:1 with the reference image's ROI. */
+ALDIC_API int aldic_set_def(aldic_ctx *ctx, const void *img, int dtype);
+/* funNormalizeImg.m:1 for one image: out = (img - mean_ROI) / std_ROI (W x H
+ * doubles); stats receives {mean, std}.  Stateless apart from scratch. */
+ALDIC_API int aldic_normalize(aldic_ctx *ctx, const void *img, int dtype, int W, int H,
+                              const int roi[4], double *out, double stats[2]);
+/* funImgGradient.m:1 for a normalised image f (W x H doubles): dfdx, dfdy are
+ * W x H with a zero 3-pixel border (Df.DfDx is the interior), times mask
+ * (W x H doubles, or NULL). */
+ALDIC_API int aldic_gradient(aldic_ctx *ctx, const double *f, int W, int H, const double *mask,
+                             double *dfdx, double *dfdy);
+
+/* Prepared fields as the reference's functions receive them: normalised
+ * ImgRef/ImgDef (W x H doubles) and Df.DfDx/Df.DfDy expanded to W x H with a
+ * zero 3-pixel border.  Any pointer may be NULL to keep the current field
+ * (f, dfdx and dfdy are required on the first call).  The integer search then
+ * runs on the normalised doubles (padding value 0). */
+ALDIC_API int aldic_set_fields(aldic_ctx *ctx, const double *f, const double *g,
+                               const double *dfdx, const double *dfdy, int W, int H);
+/* Export the prepared fields (any pointer may be NULL).  dfdx/dfdy are W x H
+ * with a zero 3-pixel border: Df.DfDx of the reference is the interior
+ * (x, y in [4, W-3] x [4, H-3]).  stats = {mean_f, std_f, mean_g, std_g}. */
+ALDIC_API int aldic_get_images(aldic_ctx *ctx, double *f, double *g, double *dfdx,
+                     double *dfdy, double stats[4]);
+
+/* Integer search -- funIntegerSearch.m:3 (whole field, tempNoOfInitPt = 0):
+ * grid trimming of :14-25, then per grid point the normalised cross-
+ * correlation of the (w+1)^2 template against the (w+1+2s)^2 region and the
+ * sub-pixel peak of findpeak.m.  Outputs are ny x nx column-major (MATLAB's
+ * x, y, u, v, cc.max); qfactors (n x 2, cc.qfactors) may be NULL to skip.
+ * On integer images the correlation maps are exact and the peaks match the
+ * project's CPU restatement bit for bit. */
+ALDIC_API int aldic_search_dims(int W, int H, const int gridx[2], const int gridy[2],
+                      int winsize, int step, const int search[2], int *nx, int *ny);
+ALDIC_API int aldic_int_search(aldic_ctx *ctx, const int gridx[2], const int gridy[2],
+                     int winsize, int step, const int search[2], double *x,
+                     double *y, double *u, double *v, double *ccmax,
+                     double *qfactors);
+
+/* Local IC-GN -- funICGN.m:1 for every node (the loop of LocalICGN.m:64-81,
+ * one launch): 6-DOF affine inverse-compositional Gauss-Newton with the
+ * ZNSSD residual.  winsize_arr (n subsets, may be NULL) overrides winsize
+ * per subset. */
+ALDIC_API int aldic_icgn(aldic_ctx *ctx, const double *coords, int64_t n, const double *U0,
+               const int32_t *winsize_arr, int winsize, double tol, int precision,
+               double *U, double *F, int32_t *iters, double *H21);
+
+/* LocalICGN.m:114-161: bad subsets (status < 0 or > 99, plus iterations
+ * above mean + 0.15 std of the good ones) set to NaN and refilled on the
+ * M x N node grid (4-neighbour spring inpainting).  U, F modified in place.
+ * bad_num receives LocalICGNBadPtNum. */
+ALDIC_API int aldic_localicgn_post(aldic_ctx *ctx, int M, int N, const int32_t *iters,
+                         double *U, double *F, int *bad_num);
+
+/* ADMM local step -- funICGN_Subpb1.m:1 for every node (Subpb1.m:64-103):
+ * translation-only IC-GN with F fixed at FOld and the augmented-Lagrangian
+ * penalty mu (P - UOld - vdual), reusing H(5:6,5:6) from H21. */
+ALDIC_API int aldic_subpb1(aldic_ctx *ctx, const double *coords, int64_t n,
+                 const double *UOld, const double *FOld, const double *vdual,
+                 const double *H21, const int32_t *winsize_arr, int winsize,
+                 double mu, double tol, int precision, double *U, int32_t *iters);
+/* Subpb1.m:162-199: bad -> NaN, then gridfit 'springs' of u and v. */
+ALDIC_API int aldic_subpb1_post(aldic_ctx *ctx, int M, int N, const int32_t *iters, double *U,
+                      int *bad_num);
+
+/* ADMM global step -- Subpb2.m:1 on the uniform Q4 mesh of MeshSetUp.m
+ * (M x N nodes, spacing step, no Dirichlet/Neumann nodes): assembles
+ * beta*DN'DN + mu*N'N with 3x3 Gauss points matrix-free and solves by PCG. */
+ALDIC_API int aldic_subpb2(aldic_ctx *ctx, int M, int N, double step, double beta, double mu,
+                 const double *U, const double *F, const double *udual,
+                 const double *vdual, double *Uhat);
+
+/* funGlobal_NodalStrainAvg.m:1 on the uniform mesh (2x2 Gauss points,
+ * extrapolation to the nodes, average over elements).  Output slots per node
+ * are [du/dx du/dy dv/dx dv/dy], the order funGlobal_NodalStrainAvg.m:97,
+ * 123-137 writes them (the middle two are swapped against funICGN's F). */
+ALDIC_API int aldic_nodal_strain(aldic_ctx *ctx, int M, int N, double step, const double *U,
+                       double *F);
+
+/* gridfit.m (regularizer 'springs', smoothness 1, data on the nodes, NaN =
+ * no data) for nf fields of M*N values; out may alias in. */
+ALDIC_API int aldic_gridfit_springs(aldic_ctx *ctx, int M, int N, int nf, const double *in,
+                          double *out);
+/* inpaint_nans.m method 4 for nf fields of M*N values, in place. */
+ALDIC_API int aldic_inpaint_springs(aldic_ctx *ctx, int M, int N, int nf, double *z);
+/* funSmoothDisp.m / funSmoothStrain.m core: gridfit + 3x3 Gaussian nanconv,
+ * twice, on nf interleaved fields (stride nf). */
+ALDIC_API int aldic_smooth(aldic_ctx *ctx, int M, int N, int nf, double *vals);
+
+/* One frame of main_ALDIC.m Sections 3-6 (accumulative mode) on the images
+ * set on the context: integer search, MeshSetUp/Init, LocalICGN and its
+ * post-processing, beta selection, Subproblem 2, then n_admm ADMM iterations
+ * (Subpb1 + post, Subpb2, nodal strain, dual update).  The device part is
+ * recorded once as a CUDA graph and replayed on later calls with the same
+ * geometry. */
+typedef struct {
+  int winsize, step;
+  int search[2];
+  int gridx[2], gridy[2];   /* ROI; {0,0} = whole image */
+  double tol;               /* IC-GN / Subpb1 tolerance (reference: 1e-2) */
+  double mu;                /* 1e-3 */
+  double beta;              /* <= 0: tune over betaList (main_ALDIC.m:237) */
+  int n_admm;               /* ADMM iterations after step 1 (reference: 4) */
+  double tol2;              /* ADMM stop threshold (reference 1e-4); <= 0 off */
+  int precision;            /* ALDIC_FP32 or ALDIC_FP64 */
+  int smooth;               /* 1: funSmoothDisp/funSmoothStrain as main_ALDIC */
+  int use_graph;            /* 1: capture/replay the device work as a CUDA graph */
+} aldic_frame_params;
+
+typedef struct {
+  int M, N;                 /* node grid */
+  int admm_steps;           /* ADMM iterations run */
+  int bad_icgn;             /* LocalICGNBadPtNum of step 1 */
+  int converged_icgn;       /* subsets with status 1..100 in step 1 */
+  double beta;              /* beta used */
+  double update_y[16];      /* ||dU Subpb2|| / sqrt(2n) per ADMM iteration */
+  double update_y2[16];     /* ||dU Subpb1|| / sqrt(2n) per ADMM iteration */
+  double mean_iters_icgn;   /* mean status over converged subsets */
+  int kernel_launches;      /* kernels launched by the frame (graph kernel nodes) */
+  /* device time of the frame's stages (CUDA events recorded on the context
+   * stream inside the frame, ms): 0 deformed-image normalisation, 1 integer
+   * search + Init, 2 IC-GN kernel, 3 LocalICGN post-processing, 4 Section 5
+   * (beta, Subpb2, nodal strain), 5 ADMM iterations, 6 whole frame */
+  double t_stage_ms[8];
+} aldic_frame_stats;
+
+ALDIC_API int aldic_frame_dims(aldic_ctx *ctx, const aldic_frame_params *p, int *M, int *N);
+ALDIC_API int aldic_frame(aldic_ctx *ctx, const aldic_frame_params *p, double *x0, double *y0,
+                double *U, double *F, int32_t *iters, aldic_frame_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

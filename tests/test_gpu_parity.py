@@ -1,0 +1,275 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and with the
+reference's own ba_interp2, on seeded synthetic speckle.
+
+Tolerances (stated per test): bit-exact where the arithmetic is integer or
+reproduced operation by operation (ba_interp2, normalisation of integer
+images, gradients, integer-search peaks); FP64 kernels within 1e-8 px of the
+FP64 oracle; the FP32 IC-GN within 1e-3 px (U) and 1e-5 (F) of the FP64
+oracle, as the specification of this path requires.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def torch_mod():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ctx(aldic, torch_mod):
+    return aldic.Context(0)
+
+
+@pytest.fixture(scope="module")
+def plain(synth, oracle):
+    wl = synth.workload("plain512")
+    f, g = wl.images()
+    fn, mf, sf = oracle.normalize(f)
+    gn, mg, sg = oracle.normalize(g)
+    dx, dy = oracle.gradient(fn)
+    return dict(wl=wl, f=f, g=g, fn=fn, gn=gn, dx=dx, dy=dy, mg=mg)
+
+
+# ------------------------------------------------------------------ a3
+def test_ba_interp2_matches_reference_golden(aldic, torch_mod):
+    g = np.load(os.path.join(HERE, "golden", "ba_interp2_ref.npz"))
+    for t in ("f64", "f32"):
+        z = aldic.ba_interp2(g[f"F_{t}"], g[f"X_{t}"], g[f"Y_{t}"])
+        np.testing.assert_array_equal(z, g[f"Z_{t}"])  # bit-exact, host arrays
+        dev = [torch_mod.from_numpy(g[k]).cuda() for k in (f"F_{t}", f"X_{t}", f"Y_{t}")]
+        zd = aldic.ba_interp2(*dev)
+        np.testing.assert_array_equal(zd.cpu().numpy(), g[f"Z_{t}"])  # device arrays
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_ba_interp2_random_bit_exact(aldic, oracle, dt):
+    rng = np.random.default_rng(4)
+    F = rng.uniform(0, 255, (300, 257)).astype(dt)
+    X = rng.uniform(-4, 305, 200_000).astype(dt)
+    Y = rng.uniform(-4, 262, 200_000).astype(dt)
+    X[:3] = [np.nan, np.inf, 5.0]
+    Y[:3] = [1.0, 2.0, np.nan]
+    z = aldic.ba_interp2(F, X, Y)
+    np.testing.assert_array_equal(z, oracle.ba_interp2(F, X, Y))
+
+
+# ------------------------------------------------------------------ a1/a2
+def test_normalize_and_gradient_bit_exact(aldic, ctx, plain):
+    H, W = plain["f"].shape
+    ctx.set_ref(plain["f"])
+    ctx.set_def(plain["g"])
+    f, g, dx, dy, st = ctx.get_images(W, H)
+    np.testing.assert_array_equal(f, plain["fn"])
+    np.testing.assert_array_equal(g, plain["gn"])
+    np.testing.assert_array_equal(dx, plain["dx"])
+    np.testing.assert_array_equal(dy, plain["dy"])
+    Df = aldic.funImgGradient(plain["fn"])
+    np.testing.assert_array_equal(Df["DfDx"], plain["dx"][3:-3, 3:-3])
+
+
+# ------------------------------------------------------------------ a4/a5
+@pytest.mark.parametrize("scale", [1, 257])
+def test_int_search_bit_exact(aldic, oracle, plain, scale):
+    f, g = plain["f"], plain["g"]
+    if scale > 1:
+        f = (f.astype(np.uint32) * scale).astype(np.uint16)
+        g = (g.astype(np.uint32) * scale).astype(np.uint16)
+    wl = plain["wl"]
+    H, W = f.shape
+    x, y, u, v, cc = aldic.funIntegerSearch(f, g, wl.search, [1, W], [1, H], wl.winsize, wl.step,
+                                            0, qfactors=False)
+    mg = g.astype(np.float64).mean()
+    xo, yo, uo, vo, co, _ = oracle.int_search(f, g, mg, [1, W], [1, H], wl.winsize, wl.step,
+                                              [wl.search, wl.search])
+    for a, b in ((x, xo), (y, yo), (u, uo), (v, vo), (cc["max"], co)):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_int_search_qfactors_and_edges(aldic, oracle, synth):
+    W = H = 160
+    f = synth.speckle(W, H, 800, 21)
+    g = synth.warp(f, synth.uniform_affine(0.0, 0.0, 4.6, -3.2), 2.0, 21)  # shift near s = 5
+    f[:40, :40] = 50  # flat templates -> NaN, q-factors Inf
+    x, y, u, v, cc = aldic.funIntegerSearch(f, g, 5, [1, W], [1, H], 16, 12, 0, qfactors=True)
+    mg = g.astype(np.float64).mean()
+    xo, yo, uo, vo, co, qo = oracle.int_search(f, g, mg, [1, W], [1, H], 16, 12, [5, 5], True)
+    np.testing.assert_array_equal(u, uo)
+    np.testing.assert_array_equal(v, vo)
+    np.testing.assert_array_equal(cc["max"], co)
+    assert np.isnan(u).any()
+    np.testing.assert_allclose(cc["qfactors"], qo, rtol=1e-9, equal_nan=True)
+
+
+# ------------------------------------------------------------------ a7/a9
+def _mesh(oracle, plain):
+    wl = plain["wl"]
+    H, W = plain["f"].shape
+    x, y, u, v, cc, _ = oracle.int_search(plain["f"], plain["g"], plain["mg"], [1, W], [1, H],
+                                          wl.winsize, wl.step, [wl.search, wl.search])
+    ny, nx = x.shape
+    coords = np.stack([x.ravel(), y.ravel()], 1)  # row-major (ny, nx) == x fastest
+    U0 = np.empty(2 * nx * ny)
+    U0[0::2] = u.ravel()
+    U0[1::2] = v.ravel()
+    return coords, U0, nx, ny
+
+
+def _oracle_icgn(oracle, plain, coords, U0, w, tol):
+    return oracle.icgn_batch(plain["fn"], plain["gn"], plain["dx"], plain["dy"], coords, U0, w, tol)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_icgn_matches_oracle(aldic, ctx, oracle, plain, prec):
+    wl = plain["wl"]
+    coords, U0, nx, ny = _mesh(oracle, plain)
+    ctx.set_ref(plain["f"])
+    ctx.set_def(plain["g"])
+    p = aldic.FP64 if prec == "fp64" else aldic.FP32
+    U, F, it, Hp = aldic.local_icgn(ctx, coords, U0, wl.winsize, wl.tol, p)
+    Uo, Fo, ito, Ho = _oracle_icgn(oracle, plain, coords, U0, wl.winsize, wl.tol)
+    same = it == ito
+    ok = (ito >= 1) & (ito <= 100)
+    assert same.mean() > (0.999 if prec == "fp64" else 0.97), same.mean()
+    m = same & ok
+    du = np.abs(U - Uo).reshape(-1, 2)[m].max()
+    dF = np.abs(F - Fo).reshape(-1, 4)[m].max()
+    if prec == "fp64":
+        assert du < 1e-8 and dF < 1e-9, (du, dF)
+        np.testing.assert_allclose(Hp, Ho.T, rtol=1e-10, atol=1e-8)
+    else:
+        assert du < 1e-3 and dF < 1e-5, (du, dF)     # specification tolerances
+        np.testing.assert_allclose(Hp, Ho.T, rtol=1e-4, atol=1e-4)
+
+
+def test_icgn_status_codes_gpu(aldic, ctx, oracle, plain):
+    ctx.set_ref(plain["f"])
+    ctx.set_def(plain["g"])
+    coords = np.array([[5.0, 50.0], [40.5, 50.0], [256.0, 256.0], [60.0, 60.0]])
+    U0 = np.array([0, 0, 0, 0, 0.5, 0.5, -300.0, 0.0])
+    U, F, it, Hp = aldic.local_icgn(ctx, coords, U0, 20, 1e-3, aldic.FP64)
+    Uo, Fo, ito, Ho = _oracle_icgn(oracle, plain, coords, U0, 20, 1e-3)
+    np.testing.assert_array_equal(it, ito)
+    assert it[0] == -1 and it[1] == -1 and it[3] == 101
+    assert np.isnan(U[0]) and np.isnan(F[0])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_subpb1_matches_oracle(aldic, ctx, oracle, plain, prec):
+    wl = plain["wl"]
+    coords, U0, nx, ny = _mesh(oracle, plain)
+    Uo, Fo, ito, Ho = _oracle_icgn(oracle, plain, coords, U0, wl.winsize, wl.tol)
+    Uo, Fo, _ = oracle.localicgn_post(nx, ny, ito, Uo, Fo)
+    rng = np.random.default_rng(9)
+    vd = 0.01 * rng.standard_normal(Uo.size)
+    ctx.set_ref(plain["f"])
+    ctx.set_def(plain["g"])
+    p = aldic.FP64 if prec == "fp64" else aldic.FP32
+    import ctypes as C
+    n = nx * ny
+    U = np.empty(2 * n)
+    it = np.empty(n, np.int32)
+    cf = np.ascontiguousarray(coords.T)
+    H21 = np.ascontiguousarray(Ho)
+    aldic._lib.call("aldic_subpb1", ctx.h, C.c_void_p(cf.ctypes.data), n,
+                    C.c_void_p(Uo.ctypes.data), C.c_void_p(Fo.ctypes.data),
+                    C.c_void_p(vd.ctypes.data), C.c_void_p(H21.ctypes.data), None, wl.winsize,
+                    1e-3, wl.tol, p, C.c_void_p(U.ctypes.data), C.c_void_p(it.ctypes.data))
+    Ur, itr = oracle.subpb1_batch(plain["fn"], plain["gn"], plain["dx"], plain["dy"], coords, Uo,
+                                  Fo, vd, Ho, wl.winsize, 1e-3, wl.tol)
+    same = it == itr
+    assert same.mean() > (0.999 if prec == "fp64" else 0.97)
+    du = np.abs(U - Ur).reshape(-1, 2)[same].max()
+    assert du < (1e-8 if prec == "fp64" else 1e-3), du
+
+
+# ------------------------------------------------------------------ post + grid solvers
+def test_grid_kernels_match_oracle(aldic, ctx, oracle):
+    import ctypes as C
+    rng = np.random.default_rng(12)
+    M, N, h = 37, 29, 8.0
+    n = M * N
+    call = aldic._lib.call
+    ptr = lambda a: C.c_void_p(a.ctypes.data)
+    # LocalICGN post
+    it = rng.integers(2, 7, n).astype(np.int32)
+    it[rng.choice(n, 20, replace=False)] = 101
+    it[5] = 102
+    it[7] = -1
+    U = rng.standard_normal(2 * n)
+    F = 0.01 * rng.standard_normal(4 * n)
+    Uo, Fo, nbo = oracle.localicgn_post(M, N, it, U, F)
+    Ug, Fg = U.copy(), F.copy()
+    nb = C.c_int()
+    call("aldic_localicgn_post", ctx.h, M, N, ptr(it), ptr(Ug), ptr(Fg), C.byref(nb))
+    assert nb.value == nbo
+    np.testing.assert_allclose(Ug, Uo, atol=1e-8)
+    np.testing.assert_allclose(Fg, Fo, atol=1e-8)
+    # Subpb1 post (gridfit springs)
+    Uo2, nbo2 = oracle.subpb1_post(M, N, it, U)
+    Ug2 = U.copy()
+    call("aldic_subpb1_post", ctx.h, M, N, ptr(it), ptr(Ug2), C.byref(nb))
+    assert nb.value == nbo2
+    np.testing.assert_allclose(Ug2, Uo2, atol=1e-8)
+    # Subpb2
+    ud = 0.001 * rng.standard_normal(4 * n)
+    vd = 0.01 * rng.standard_normal(2 * n)
+    for beta in (6.4e-5, 2e-2):
+        xo, _ = oracle.subpb2(M, N, h, beta, 1e-3, U, F, ud, vd)
+        xg = np.empty(2 * n)
+        call("aldic_subpb2", ctx.h, M, N, h, beta, 1e-3, ptr(U), ptr(F), ptr(ud), ptr(vd), ptr(xg))
+        np.testing.assert_allclose(xg, xo, rtol=1e-8, atol=1e-9)
+    # nodal strain
+    Fo3 = oracle.nodal_strain(M, N, h, U)
+    Fg3 = np.empty(4 * n)
+    call("aldic_nodal_strain", ctx.h, M, N, h, ptr(U), ptr(Fg3))
+    np.testing.assert_allclose(Fg3, Fo3, rtol=1e-12, atol=1e-14)
+    # smoothing
+    So = oracle.smooth_fields(M, N, F, 4)
+    Sg = F.copy()
+    call("aldic_smooth", ctx.h, M, N, 4, ptr(Sg))
+    np.testing.assert_allclose(Sg, So, atol=1e-8)
+
+
+# ------------------------------------------------------------------ a12 frame
+def test_frame_fp64_matches_oracle(aldic, oracle, plain):
+    wl = plain["wl"]
+    ro = oracle.frame(plain["f"], plain["g"], wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=3)
+    al = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=3, precision=aldic.FP64)
+    al.set_images(plain["f"], plain["g"])
+    r = al.frame()
+    np.testing.assert_array_equal(r["x0"], ro["x0"])
+    np.testing.assert_array_equal(r["y0"], ro["y0"])
+    assert (r["iters"] == ro["iters_icgn"]).mean() > 0.999
+    assert r["stats"]["beta"] == pytest.approx(ro["beta"], rel=1e-6)
+    assert np.abs(r["U"] - ro["U"]).max() < 1e-4     # ADMM U within 1e-4 px
+    assert np.abs(r["F"] - ro["F"]).max() < 1e-4
+    np.testing.assert_allclose(r["stats"]["update_y"], ro["update_y"], rtol=1e-3, atol=1e-7)
+
+
+def test_frame_fp32_accuracy_and_replay(aldic, oracle, plain, synth):
+    wl = plain["wl"]
+    ro = oracle.frame(plain["f"], plain["g"], wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=3)
+    al = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=3, precision=aldic.FP32)
+    al.set_images(plain["f"], plain["g"])
+    r1 = al.frame()
+    r2 = al.frame()  # graph replay
+    for k in ("U", "F", "iters"):
+        np.testing.assert_array_equal(r1[k], r2[k])
+    d = r1["U"] - ro["U"]
+    assert np.sqrt(np.mean(d ** 2)) < 0.01      # <= 0.01 px RMS vs the FP64 oracle
+    ut, vt = synth.truth(wl, r1["x0"], r1["y0"])
+    e = np.r_[r1["U"][0::2] - ut, r1["U"][1::2] - vt]
+    assert np.sqrt(np.mean(e ** 2)) < 0.01
+    al2 = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=3, precision=aldic.FP32,
+                      use_graph=False)
+    al2.set_images(plain["f"], plain["g"])
+    r3 = al2.frame()
+    np.testing.assert_array_equal(r1["U"], r3["U"])
