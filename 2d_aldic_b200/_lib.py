@@ -56,7 +56,7 @@ class FrameStats(C.Structure):
     _fields_ = [("M", I32), ("N", I32), ("admm_steps", I32), ("bad_icgn", I32),
                 ("converged_icgn", I32), ("beta", D), ("update_y", D * 16),
                 ("update_y2", D * 16), ("mean_iters_icgn", D), ("kernel_launches", I32),
-                ("t_stage_ms", D * 8)]
+                ("t_stage_ms", D * 8), ("max_pcg_iters", I32)]
 
 
 class AldicError(RuntimeError):

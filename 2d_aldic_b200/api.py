@@ -606,6 +606,7 @@ class ALDIC:
                             "update_y": list(st.update_y)[:st.admm_steps],
                             "update_y2": list(st.update_y2)[:st.admm_steps],
                             "kernel_launches": st.kernel_launches,
+                            "max_pcg_iters": st.max_pcg_iters,
                             "t_stage_ms": dict(zip(("normalize", "search", "icgn", "icgn_post",
                                                     "section5", "admm", "frame"),
                                                    list(st.t_stage_ms)[:7]))}

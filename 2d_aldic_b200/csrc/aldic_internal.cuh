@@ -79,11 +79,11 @@ __device__ __forceinline__ bool grid_sync(const GridSync &g, unsigned int nblock
           s_fail = 1;
           break;
         }
-        if (*((volatile int *)g.err)) {
+        if ((spins & 255) == 0 && *((volatile int *)g.err)) {
           s_fail = 1;
           break;
         }
-        __nanosleep(64);
+        if (spins > 256) __nanosleep(32);
       }
     }
     __threadfence();

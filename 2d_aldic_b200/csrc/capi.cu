@@ -202,7 +202,7 @@ size_t dtype_size(int dt) { return dt == 0 ? 1 : dt == 1 ? 2 : dt == 2 ? 4 : 8; 
 
 int ensure_grid_work(aldic_ctx *c, long long n) {
   if (n <= c->gw_n && c->gw.x) return OK;
-  const long long R = 6;
+  const long long R = 12;
   int rc;
   // x r z p(2 buffers) q b diag -> 8 * R * n doubles
   if ((rc = c->gw_vec.ensure(sizeof(double) * 8 * R * n))) return rc;
@@ -790,7 +790,7 @@ int aldic_nodal_strain(aldic_ctx *c, int M, int N, double step, const double *U,
 }
 
 int aldic_gridfit_springs(aldic_ctx *c, int M, int N, int nf, const double *in, double *out) {
-  ALDIC_CHECK(c && in && out && M > 1 && N > 1 && nf >= 1 && nf <= 6, E_ARG,
+  ALDIC_CHECK(c && in && out && M > 1 && N > 1 && nf >= 1 && nf <= 12, E_ARG,
               "gridfit_springs: bad arguments");
   Guard g(c);
   const long long n = (long long)M * N;
@@ -811,7 +811,7 @@ int aldic_gridfit_springs(aldic_ctx *c, int M, int N, int nf, const double *in, 
 }
 
 int aldic_inpaint_springs(aldic_ctx *c, int M, int N, int nf, double *z) {
-  ALDIC_CHECK(c && z && M > 0 && N > 0 && nf >= 1 && nf <= 6, E_ARG, "inpaint_springs: bad arguments");
+  ALDIC_CHECK(c && z && M > 0 && N > 0 && nf >= 1 && nf <= 12, E_ARG, "inpaint_springs: bad arguments");
   Guard g(c);
   const long long n = (long long)M * N;
   int rc;
@@ -979,6 +979,7 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   cudaStream_t st = c->stream;
   int rcm;
   if ((rcm = mark(c, 0))) return rcm;
+  ALDIC_CUDA(cudaMemsetAsync(c->gw.iters_out, 0, sizeof(int), st));
   const long long n = (long long)M * N;
   const double h = (double)p->step, mu = p->mu;
   const double lam2 = springs_lam2(M, N);
@@ -1019,11 +1020,18 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   } else {
     const double base = h * h * mu;
     const double bl[6] = {1e-3, std::sqrt(1e-5), 1e-2, std::sqrt(1e-3), 1e-1, std::sqrt(1e-1)};
+    double be[12];
     for (int k = 0; k < 6; ++k) {
-      const double bk = bl[k] * base;
-      if ((rc = fe_rhs(c->gw, M, N, h, bk, mu, B.U1, B.F1, B.udual, B.vdual, st))) return rc;
-      if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, bk, mu, h, 0, kRtolFE, kMaxitFE, st))) return rc;
-      if ((rc = fe_store(c->gw, M, N, B.U2, st))) return rc;
+      be[2 * k] = be[2 * k + 1] = bl[k] * base;
+      if ((rc = fe_rhs(c->gw, M, N, h, bl[k] * base, mu, B.U1, B.F1, B.udual, B.vdual, st,
+                       nullptr, 2 * k)))
+        return rc;
+    }
+    // the six systems of the sweep in one launch (12 right-hand sides)
+    if ((rc = grid_pcg(c->gw, OP_FE, M, N, 12, 0, mu, h, 0, kRtolFE, kMaxitFE, st, nullptr, be)))
+      return rc;
+    for (int k = 0; k < 6; ++k) {
+      if ((rc = fe_store(c->gw, M, N, B.U2, st, 2 * k))) return rc;
       if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
       if ((rc = vdiffnorm(B.U1, B.U2, 2 * n, B.part, B.err + k, st))) return rc;
       if ((rc = vdiffnorm(B.F1, B.F2, 4 * n, B.part, B.err + 6 + k, st))) return rc;
@@ -1182,7 +1190,9 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
       double beta;
       double meanit;
       int ints[16];
+      int pcg_its;
     } hs;
+    ALDIC_CUDA(cudaMemcpyAsync(&hs.pcg_its, c->gw.iters_out, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     ALDIC_CUDA(cudaMemcpyAsync(hs.upd, B.upd, sizeof(hs.upd), cudaMemcpyDeviceToHost, c->stream));
     ALDIC_CUDA(cudaMemcpyAsync(&hs.beta, B.beta, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     ALDIC_CUDA(cudaMemcpyAsync(&hs.meanit, B.meanit, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1197,6 +1207,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     stats->beta = hs.beta;
     stats->mean_iters_icgn = hs.meanit;
     stats->kernel_launches = (c->graph && want_graph) ? c->graph_kernels : -1;
+    stats->max_pcg_iters = hs.pcg_its;
     for (int k = 0; k < 6; ++k) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]) == cudaSuccess) stats->t_stage_ms[k] = ms;

@@ -21,43 +21,46 @@ namespace aldic {
 
 namespace {
 
-constexpr int PCG_THREADS = 256;
-constexpr int MAXRHS = 6;
+constexpr int PCG_THREADS = 512;
+constexpr int MAXRHS = 12;
 
 struct PcgArgs {
   double *x, *r, *z, *p0, *p1, *q, *b, *diag, *part;
   const unsigned char *mask;
   int M, N, nrhs, maxit, blocks;
-  double beta, mu, h, lam2, rtol;
-  const double *beta_ptr;  // if set, beta is read from device memory
+  double mu, h, lam2, rtol;
+  double beta[MAXRHS];     // FE: beta per right-hand side
+  const double *beta_ptr;  // if set, every right-hand side uses *beta_ptr
   GridSync gs;
   int *iters_out;
 };
 
-// Scalar Q4 element matrices on a square element of size h, local nodes
-// (-,-), (+,-), (+,+), (-,+): Laplacian stiffness and consistent mass (the
-// 3x3 Gauss rule of Subpb2.m:100-101 integrates both exactly).
-__constant__ double c_K[4][4] = {{4.0 / 6, -1.0 / 6, -2.0 / 6, -1.0 / 6},
-                                 {-1.0 / 6, 4.0 / 6, -1.0 / 6, -2.0 / 6},
-                                 {-2.0 / 6, -1.0 / 6, 4.0 / 6, -1.0 / 6},
-                                 {-1.0 / 6, -2.0 / 6, -1.0 / 6, 4.0 / 6}};
-__constant__ double c_Mm[4][4] = {{4.0 / 36, 2.0 / 36, 1.0 / 36, 2.0 / 36},
-                                  {2.0 / 36, 4.0 / 36, 2.0 / 36, 1.0 / 36},
-                                  {1.0 / 36, 2.0 / 36, 4.0 / 36, 2.0 / 36},
-                                  {2.0 / 36, 1.0 / 36, 2.0 / 36, 4.0 / 36}};
+// Scalar Q4 element matrices on a square element of size h with local nodes
+// (-,-), (+,-), (+,+), (-,+) -- the 3x3 Gauss rule of Subpb2.m:100-101
+// integrates them exactly: stiffness (1/6)[4 -1 -2 -1; ...] (Laplacian of
+// u and v separately, beta*DN'DN) and mass (h^2/36)[4 2 1 2; ...]
+// (mu*N'N).  Their node-pair sums give the 9-point stencil below.
 
 // local node index -> (di, dj) offset from the element's first node
 __device__ __forceinline__ int lx(int a) { return (a == 1 || a == 2) ? 1 : 0; }
 __device__ __forceinline__ int ly(int a) { return (a >= 2) ? 1 : 0; }
 
+// FE stencil weights on a square-element grid: the element matrices above
+// summed over the elements two nodes share.  kap[0] centre, [1] axial, [2]
+// diagonal; the coefficient of neighbour (di, dj) of node (i, j) is
+// cnt(i, di) * cnt(j, dj) * kap[|di| + |dj|], cnt counting the element
+// columns (rows) adjacent to both nodes.
+__device__ __forceinline__ int ecnt(int i, int di, int M) {
+  return di == 0 ? (i >= 1) + (i <= M - 2) : (di > 0 ? (i <= M - 2) : (i >= 1));
+}
+
 template <int OP>
-__device__ __forceinline__ double op_diag(const PcgArgs &A, int i, int j, long long k, int f) {
+__device__ __forceinline__ double op_diag(const PcgArgs &A, double beta, int i, int j,
+                                          long long k, int f) {
   const int M = A.M, N = A.N;
   if (OP == OP_FE) {
-    int ne = 0;
-    for (int ej = j - 1; ej <= j; ++ej)
-      for (int ei = i - 1; ei <= i; ++ei) ne += (ei >= 0 && ei < M - 1 && ej >= 0 && ej < N - 1);
-    return ne * (A.beta * (4.0 / 6.0) + A.mu * A.h * A.h * (4.0 / 36.0));
+    const double kc = beta * (4.0 / 6.0) + A.mu * A.h * A.h * (4.0 / 36.0);
+    return ecnt(i, 0, M) * ecnt(j, 0, N) * kc;
   } else if (OP == OP_GRIDFIT) {
     const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
     const int na = (i > 0) + (i < M - 1) + (j > 0) + (j < N - 1);
@@ -70,192 +73,237 @@ __device__ __forceinline__ double op_diag(const PcgArgs &A, int i, int j, long l
   }
 }
 
-// y = op(v)_k where v(node) is supplied by the functor
-template <int OP, typename Fv>
-__device__ __forceinline__ double op_apply(const PcgArgs &A, int i, int j, long long k, int f,
-                                           Fv v) {
+// y = op(v)_k, v = one field (M*N values)
+template <int OP>
+__device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i, int j,
+                                           long long k, int f, const double *__restrict__ v) {
   const int M = A.M, N = A.N;
   if (OP == OP_FE) {
+    const double km = A.mu * A.h * A.h;
+    const double kap[3] = {beta * (4.0 / 6.0) + km * (4.0 / 36.0),
+                           beta * (-1.0 / 6.0) + km * (2.0 / 36.0),
+                           beta * (-2.0 / 6.0) + km * (1.0 / 36.0)};
     double y = 0.0;
-    const double kb = A.beta, km = A.mu * A.h * A.h;
-    for (int ej = j - 1; ej <= j; ++ej)
-      for (int ei = i - 1; ei <= i; ++ei) {
-        if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
-        const int la = (i - ei) + (j - ej) * 3 - 2 * (i - ei) * (j - ej);  // (0,0)->0 (1,0)->1 (1,1)->2 (0,1)->3
 #pragma unroll
-        for (int lb = 0; lb < 4; ++lb) {
-          const int ni = ei + lx(lb), nj = ej + ly(lb);
-          y += (kb * c_K[la][lb] + km * c_Mm[la][lb]) * v((long long)nj * M + ni);
-        }
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int cj = ecnt(j, dj, N);
+      if (!cj) continue;
+#pragma unroll
+      for (int di = -1; di <= 1; ++di) {
+        const int ci = ecnt(i, di, M);
+        if (!ci) continue;
+        const int t = (di != 0) + (dj != 0);
+        y += (double)(ci * cj) * kap[t] * v[k + di + (long long)dj * M];
       }
+    }
     return y;
   } else if (OP == OP_GRIDFIT) {
-    const double xk = v(k);
+    const double xk = v[k];
     double s = 0.0, sd = 0.0;
-    if (i > 0) s += xk - v(k - 1);
-    if (i < M - 1) s += xk - v(k + 1);
-    if (j > 0) s += xk - v(k - M);
-    if (j < N - 1) s += xk - v(k + M);
-    if (i > 0 && j > 0) sd += xk - v(k - M - 1);
-    if (i < M - 1 && j > 0) sd += xk - v(k - M + 1);
-    if (i > 0 && j < N - 1) sd += xk - v(k + M - 1);
-    if (i < M - 1 && j < N - 1) sd += xk - v(k + M + 1);
+    if (i > 0) s += xk - v[k - 1];
+    if (i < M - 1) s += xk - v[k + 1];
+    if (j > 0) s += xk - v[k - M];
+    if (j < N - 1) s += xk - v[k + M];
+    if (i > 0 && j > 0) sd += xk - v[k - M - 1];
+    if (i < M - 1 && j > 0) sd += xk - v[k - M + 1];
+    if (i > 0 && j < N - 1) sd += xk - v[k + M - 1];
+    if (i < M - 1 && j < N - 1) sd += xk - v[k + M + 1];
     const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
     return w * xk + A.lam2 * (s + 0.5 * sd);
   } else {
     const unsigned char *unk = A.mask + (long long)f * M * N;
-    const double xk = v(k);
+    const double xk = v[k];
     if (!unk[k]) return xk;
     double s = 0.0;
-    if (i > 0) s += xk - (unk[k - 1] ? v(k - 1) : 0.0);
-    if (i < M - 1) s += xk - (unk[k + 1] ? v(k + 1) : 0.0);
-    if (j > 0) s += xk - (unk[k - M] ? v(k - M) : 0.0);
-    if (j < N - 1) s += xk - (unk[k + M] ? v(k + M) : 0.0);
+    if (i > 0) s += xk - (unk[k - 1] ? v[k - 1] : 0.0);
+    if (i < M - 1) s += xk - (unk[k + 1] ? v[k + 1] : 0.0);
+    if (j > 0) s += xk - (unk[k - M] ? v[k - M] : 0.0);
+    if (j < N - 1) s += xk - (unk[k + M] ? v[k + M] : 0.0);
     return s;
   }
 }
 
-// block reduction of up to 2*MAXRHS doubles into part[slot][f][blockIdx]
-__device__ void block_partials(double *vals, int cnt, double *part, int blocks, int slot_base) {
-  __shared__ double sh[PCG_THREADS / 32][2 * MAXRHS];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int c = 0; c < cnt; ++c) {
-    const double v = warp_sum(vals[c]);
-    if (lane == 0) sh[wid][c] = v;
-  }
+// Per-warp partials staged in shared memory: sh[warp][slot]; a warp adds
+// its butterfly-reduced values for `cnt` slots starting at s0.
+struct PcgShared {
+  double warp_part[PCG_THREADS / 32][4 * MAXRHS];
+  double gsum[4 * MAXRHS];
+  double alpha[MAXRHS], beta[MAXRHS], gam[MAXRHS], bb[MAXRHS];
+  int done[MAXRHS];
+};
+
+__device__ __forceinline__ void warp_stage(PcgShared &S, int slot, double v) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) S.warp_part[threadIdx.x >> 5][slot] = v;
+}
+
+// block partial of slots [0, cnt) -> part[slot][blockIdx]
+__device__ __forceinline__ void block_partials(PcgShared &S, int cnt, double *part, int blocks) {
   __syncthreads();
   if (threadIdx.x < cnt) {
     double t = 0.0;
-    for (int w = 0; w < PCG_THREADS / 32; ++w) t += sh[w][threadIdx.x];
-    part[(long long)(slot_base + threadIdx.x) * blocks + blockIdx.x] = t;
+    for (int w = 0; w < PCG_THREADS / 32; ++w) t += S.warp_part[w][threadIdx.x];
+    part[(long long)threadIdx.x * blocks + blockIdx.x] = t;
+  }
+}
+
+// Global sums of slots [0, cnt) after a grid barrier: warp w of every block
+// reduces slots w, w+16, ... over the block partials (independent loads, then
+// a fixed-order butterfly), so every block obtains bit-identical totals.
+__device__ void global_sums(PcgShared &S, const double *part, int cnt, int blocks) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = wid; c < cnt; c += PCG_THREADS / 32) {
+    const double *pp = part + (long long)c * blocks;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int b = lane + 32 * q;
+      v[q] = b < blocks ? pp[b] : 0.0;
+    }
+    double t = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+    for (int b = lane + 256; b < blocks; b += 32) t += pp[b];
+    t = warp_sum(t);
+    if (lane == 0) S.gsum[c] = t;
   }
   __syncthreads();
 }
 
-__device__ __forceinline__ double sum_partials(const double *part, int slot, int blocks) {
-  double t = 0.0;
-  for (int b = 0; b < blocks; ++b) t += part[(long long)slot * blocks + b];
-  return t;
-}
-
-template <int OP>
+// Preconditioned CG in the Chronopoulos-Gear arrangement: one mat-vec per
+// iteration on the preconditioned residual u (w = A u), the recurrences
+// p = u + beta p, s = w + beta s (s = A p), and the three dot products
+// (r,u), (w,u), (r,r) reduced together -- two grid barriers per iteration.
+// Fields are processed one after another inside each phase (few live
+// registers); per-field scalars live in shared memory.
+// Buffers: x, r, u (= z slot), w (= q slot), p (p0), s (p1), 1/diag.
+template <int OP, int NR>
 __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
-  if (A.beta_ptr) A.beta = *A.beta_ptr;
+  __shared__ PcgShared S;
+  if (A.beta_ptr) {
+    const double bv = *A.beta_ptr;
+#pragma unroll
+    for (int f = 0; f < NR; ++f) A.beta[f] = bv;
+  }
   const long long n = (long long)A.M * A.N;
-  const int nr = A.nrhs;
+  const int M = A.M;
   const long long tid0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  __shared__ double s_g[4 * MAXRHS];
-  // slots: [0,nr) rz  [nr,2nr) rr  [2nr,3nr) bb  [3nr,4nr) pq
-  double acc[2 * MAXRHS];
-  // ---- r = b - A x, z = D^-1 r; partial rz, rr, bb
-  for (int c = 0; c < 2 * MAXRHS; ++c) acc[c] = 0.0;
-  double accb[MAXRHS];
-  for (int c = 0; c < MAXRHS; ++c) accb[c] = 0.0;
-  for (long long k = tid0; k < n; k += stride) {
-    const int i = (int)(k % A.M), j = (int)(k / A.M);
-    for (int f = 0; f < nr; ++f) {
-      const double *xf = A.x + f * n;
-      const double ax = op_apply<OP>(A, i, j, k, f, [&](long long q) { return xf[q]; });
-      const double bv = A.b[f * n + k];
-      const double rv = bv - ax;
-      const double d = op_diag<OP>(A, i, j, k, f);
-      const double zv = rv / d;
-      A.r[f * n + k] = rv;
-      A.z[f * n + k] = zv;
-      A.diag[f * n + k] = d;
-      A.p1[f * n + k] = 0.0;
-      acc[f] += rv * zv;
-      acc[MAXRHS + f] += rv * rv;
-      accb[f] += bv * bv;
+  double *const X = A.x, *const R = A.r, *const Uv = A.z, *const Wv = A.q, *const Pv = A.p0,
+               *const Sv = A.p1, *const Di = A.diag;
+  // ---- r = b - A x, u = D^-1 r, p = s = 0
+#pragma unroll 1
+  for (int f = 0; f < NR; ++f) {
+    const double bt = A.beta[f];
+    for (long long k = tid0; k < n; k += stride) {
+      const int i = (int)(k % M), j = (int)(k / M);
+      const long long o = f * n + k;
+      const double rv = A.b[o] - op_apply<OP>(A, bt, i, j, k, f, X + f * n);
+      const double dinv = 1.0 / op_diag<OP>(A, bt, i, j, k, f);
+      R[o] = rv;
+      Uv[o] = rv * dinv;
+      Di[o] = dinv;
+      Pv[o] = 0.0;
+      Sv[o] = 0.0;
     }
-  }
-  {
-    double v[3 * MAXRHS];
-    for (int f = 0; f < nr; ++f) {
-      v[f] = acc[f];
-      v[nr + f] = acc[MAXRHS + f];
-    }
-    block_partials(v, 2 * nr, A.part, A.blocks, 0);
-    for (int f = 0; f < nr; ++f) v[f] = accb[f];
-    block_partials(v, nr, A.part, A.blocks, 2 * nr);
   }
   if (!grid_sync(A.gs, A.blocks)) return;
-  double rz[MAXRHS], bb[MAXRHS], betaf[MAXRHS];
-  bool done[MAXRHS];
-  for (int f = 0; f < nr; ++f) {
-    rz[f] = sum_partials(A.part, f, A.blocks);
-    const double rr = sum_partials(A.part, nr + f, A.blocks);
-    bb[f] = sum_partials(A.part, 2 * nr + f, A.blocks);
-    done[f] = !(rr > A.rtol * A.rtol * bb[f]);
-    betaf[f] = 0.0;
+  // ---- w = A u; partials (r,u) (w,u) (r,r) (b,b)
+#pragma unroll 1
+  for (int f = 0; f < NR; ++f) {
+    const double bt = A.beta[f];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    for (long long k = tid0; k < n; k += stride) {
+      const int i = (int)(k % M), j = (int)(k / M);
+      const long long o = f * n + k;
+      const double wv = op_apply<OP>(A, bt, i, j, k, f, Uv + f * n);
+      Wv[o] = wv;
+      const double rv = R[o], uv = Uv[o], bv = A.b[o];
+      a0 += rv * uv;
+      a1 += wv * uv;
+      a2 += rv * rv;
+      a3 += bv * bv;
+    }
+    warp_stage(S, f, a0);
+    warp_stage(S, NR + f, a1);
+    warp_stage(S, 2 * NR + f, a2);
+    warp_stage(S, 3 * NR + f, a3);
   }
-  (void)s_g;
+  block_partials(S, 4 * NR, A.part, A.blocks);
+  if (!grid_sync(A.gs, A.blocks)) return;
+  global_sums(S, A.part, 4 * NR, A.blocks);
+  if (threadIdx.x < NR) {
+    const int f = threadIdx.x;
+    S.gam[f] = S.gsum[f];
+    S.alpha[f] = S.gsum[f] / S.gsum[NR + f];
+    S.beta[f] = 0.0;
+    S.bb[f] = S.gsum[3 * NR + f];
+    S.done[f] = !(S.gsum[2 * NR + f] > A.rtol * A.rtol * S.bb[f]);
+  }
+  __syncthreads();
   int it = 0;
   for (; it < A.maxit; ++it) {
     bool all = true;
-    for (int f = 0; f < nr; ++f) all &= done[f];
+#pragma unroll
+    for (int f = 0; f < NR; ++f) all &= (S.done[f] != 0);
     if (all) break;
-    double *pc = (it & 1) ? A.p1 : A.p0;
-    const double *pp = (it & 1) ? A.p0 : A.p1;
-    // ---- p = z + beta p_prev (own nodes), q = A p (neighbours on the fly)
-    for (int c = 0; c < nr; ++c) acc[c] = 0.0;
-    for (long long k = tid0; k < n; k += stride) {
-      const int i = (int)(k % A.M), j = (int)(k / A.M);
-      for (int f = 0; f < nr; ++f) {
-        if (done[f]) continue;
-        const double *zf = A.z + f * n;
-        const double *pf = pp + f * n;
-        const double bt = betaf[f];
-        const double pk = zf[k] + bt * pf[k];
-        pc[f * n + k] = pk;
-        const double qk =
-            op_apply<OP>(A, i, j, k, f, [&](long long q) { return zf[q] + bt * pf[q]; });
-        A.q[f * n + k] = qk;
-        acc[f] += pk * qk;
-      }
-    }
-    block_partials(acc, nr, A.part, A.blocks, 3 * nr);
-    if (!grid_sync(A.gs, A.blocks)) return;
-    double alpha[MAXRHS];
-    for (int f = 0; f < nr; ++f) alpha[f] = done[f] ? 0.0 : rz[f] / sum_partials(A.part, 3 * nr + f, A.blocks);
-    // ---- x += alpha p, r -= alpha q, z = D^-1 r
-    for (int c = 0; c < 2 * MAXRHS; ++c) acc[c] = 0.0;
-    for (long long k = tid0; k < n; k += stride) {
-      for (int f = 0; f < nr; ++f) {
-        if (done[f]) continue;
+    // ---- p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = D^-1 r
+#pragma unroll 1
+    for (int f = 0; f < NR; ++f) {
+      if (S.done[f]) continue;
+      const double al = S.alpha[f], be = S.beta[f];
+      for (long long k = tid0; k < n; k += stride) {
         const long long o = f * n + k;
-        A.x[o] += alpha[f] * pc[o];
-        const double rv = A.r[o] - alpha[f] * A.q[o];
-        const double zv = rv / A.diag[o];
-        A.r[o] = rv;
-        A.z[o] = zv;
-        acc[f] += rv * zv;
-        acc[MAXRHS + f] += rv * rv;
+        const double pv = Uv[o] + be * Pv[o];
+        const double sv = Wv[o] + be * Sv[o];
+        Pv[o] = pv;
+        Sv[o] = sv;
+        X[o] += al * pv;
+        const double rv = R[o] - al * sv;
+        R[o] = rv;
+        Uv[o] = rv * Di[o];
       }
-    }
-    {
-      double v[2 * MAXRHS];
-      for (int f = 0; f < nr; ++f) {
-        v[f] = acc[f];
-        v[nr + f] = acc[MAXRHS + f];
-      }
-      block_partials(v, 2 * nr, A.part, A.blocks, 0);
     }
     if (!grid_sync(A.gs, A.blocks)) return;
-    for (int f = 0; f < nr; ++f) {
-      if (done[f]) continue;
-      const double rzn = sum_partials(A.part, f, A.blocks);
-      const double rr = sum_partials(A.part, nr + f, A.blocks);
-      betaf[f] = rzn / rz[f];
-      rz[f] = rzn;
-      done[f] = !(rr > A.rtol * A.rtol * bb[f]);
+    // ---- w = A u and the three dot products
+#pragma unroll 1
+    for (int f = 0; f < NR; ++f) {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      if (!S.done[f]) {
+        const double bt = A.beta[f];
+        for (long long k = tid0; k < n; k += stride) {
+          const int i = (int)(k % M), j = (int)(k / M);
+          const long long o = f * n + k;
+          const double wv = op_apply<OP>(A, bt, i, j, k, f, Uv + f * n);
+          Wv[o] = wv;
+          const double rv = R[o], uv = Uv[o];
+          a0 += rv * uv;
+          a1 += wv * uv;
+          a2 += rv * rv;
+        }
+      }
+      warp_stage(S, f, a0);
+      warp_stage(S, NR + f, a1);
+      warp_stage(S, 2 * NR + f, a2);
     }
+    block_partials(S, 3 * NR, A.part, A.blocks);
+    if (!grid_sync(A.gs, A.blocks)) return;
+    global_sums(S, A.part, 3 * NR, A.blocks);
+    if (threadIdx.x < NR) {
+      const int f = threadIdx.x;
+      if (!S.done[f]) {
+        const double gn = S.gsum[f], dl = S.gsum[NR + f];
+        const double be = gn / S.gam[f];
+        S.beta[f] = be;
+        S.alpha[f] = gn / (dl - be * gn / S.alpha[f]);
+        S.gam[f] = gn;
+        S.done[f] = !(S.gsum[2 * NR + f] > A.rtol * A.rtol * S.bb[f]);
+      }
+    }
+    __syncthreads();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *A.iters_out = it;
+    *A.iters_out = it > *A.iters_out ? it : *A.iters_out;
     bool all = true;
-    for (int f = 0; f < nr; ++f) all &= done[f];
+    for (int f = 0; f < NR; ++f) all &= (S.done[f] != 0);
     if (!all) atomicExch(A.gs.err, 2);  // not converged within maxit
   }
 }
@@ -313,7 +361,7 @@ __global__ void k_fe_rhs(int M, int N, double h, double beta, const double *beta
 }
 
 __global__ void k_fe_init(long long n, double *__restrict__ x, unsigned char *mask) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < 2 * n;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
     x[k] = 0.0;
     mask[k] = 1;
@@ -584,16 +632,31 @@ inline int blocks_for(long long n, int threads = 256) {
 }  // namespace
 
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
-             double lam2, double rtol, int maxit, cudaStream_t st, const double *beta_ptr) {
-  ALDIC_CHECK(nrhs >= 1 && nrhs <= MAXRHS, E_ARG, "grid_pcg: 1..6 right-hand sides");
+             double lam2, double rtol, int maxit, cudaStream_t st, const double *beta_ptr,
+             const double *beta_each) {
+  ALDIC_CHECK(nrhs >= 1 && nrhs <= MAXRHS, E_ARG, "grid_pcg: 1..12 right-hand sides");
   const long long n = (long long)M * N;
   int dev = 0, sms = 148, per = 1;
   ALDIC_CUDA(cudaGetDevice(&dev));
   ALDIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  void *fn = op == OP_FE ? (void *)k_pcg<OP_FE>
-                         : (op == OP_GRIDFIT ? (void *)k_pcg<OP_GRIDFIT> : (void *)k_pcg<OP_INPAINT>);
+  void *fn = nullptr;
+#define ALDIC_PCG_FN(OPV)                                                         \
+  switch (nrhs) {                                                                 \
+    case 1: fn = (void *)k_pcg<OPV, 1>; break;                                    \
+    case 2: fn = (void *)k_pcg<OPV, 2>; break;                                    \
+    case 3: case 4: fn = (void *)k_pcg<OPV, 4>; break;                            \
+    case 5: case 6: fn = (void *)k_pcg<OPV, 6>; break;                            \
+    default: fn = (void *)k_pcg<OPV, 12>; break;                                  \
+  }
+  if (op == OP_FE) { ALDIC_PCG_FN(OP_FE) }
+  else if (op == OP_GRIDFIT) { ALDIC_PCG_FN(OP_GRIDFIT) }
+  else { ALDIC_PCG_FN(OP_INPAINT) }
+#undef ALDIC_PCG_FN
+  const int nr_pad = nrhs <= 2 ? nrhs : (nrhs <= 4 ? 4 : (nrhs <= 6 ? 6 : 12));
   ALDIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, PCG_THREADS, 0));
-  long long blocks = (long long)sms * (per < 1 ? 1 : per);
+  // one block per SM at most: fewer partials and cheaper barriers, while the
+  // grid-stride loops still cover every node
+  long long blocks = (long long)sms * (per < 1 ? 1 : (per > 1 ? 1 : per));
   const long long need = (n + PCG_THREADS - 1) / PCG_THREADS;
   if (blocks > need) blocks = need;
   if (blocks > w.max_blocks) blocks = w.max_blocks;
@@ -601,8 +664,14 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
   PcgArgs A;
   A.x = w.x; A.r = w.r; A.z = w.z; A.p0 = w.p; A.p1 = w.p + MAXRHS * n; A.q = w.q; A.b = w.b;
   A.diag = w.diag; A.part = w.part; A.mask = w.mask;
-  A.M = M; A.N = N; A.nrhs = nrhs; A.maxit = maxit; A.blocks = (int)blocks;
-  A.beta = beta; A.mu = mu; A.h = h; A.lam2 = lam2; A.rtol = rtol;
+  if (nr_pad > nrhs) {  // padded right-hand sides: b = x = 0 converge at once
+    ALDIC_CUDA(cudaMemsetAsync(w.b + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
+    ALDIC_CUDA(cudaMemsetAsync(w.x + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
+    ALDIC_CUDA(cudaMemsetAsync(w.mask + nrhs * n, 0, (size_t)(nr_pad - nrhs) * n, st));
+  }
+  A.M = M; A.N = N; A.nrhs = nr_pad; A.maxit = maxit; A.blocks = (int)blocks;
+  for (int f = 0; f < MAXRHS; ++f) A.beta[f] = (beta_each && f < nrhs) ? beta_each[f] : beta;
+  A.mu = mu; A.h = h; A.lam2 = lam2; A.rtol = rtol;
   A.gs.count = w.bar; A.gs.gen = w.bar + 1; A.gs.err = w.err;
   A.iters_out = w.iters_out;
   A.beta_ptr = beta_ptr;
@@ -614,17 +683,18 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
 
 int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
            const double *F, const double *udual, const double *vdual, cudaStream_t st,
-           const double *beta_ptr) {
+           const double *beta_ptr, int f0) {
   const long long n = (long long)M * N;
-  k_fe_rhs<<<blocks_for(n), 256, 0, st>>>(M, N, h, beta, beta_ptr, mu, U, F, udual, vdual, w.b);
-  k_fe_init<<<blocks_for(2 * n), 256, 0, st>>>(n, w.x, w.mask);
+  k_fe_rhs<<<blocks_for(n), 256, 0, st>>>(M, N, h, beta, beta_ptr, mu, U, F, udual, vdual,
+                                          w.b + f0 * n);
+  k_fe_init<<<blocks_for(2 * n), 256, 0, st>>>(2 * n, w.x + f0 * n, w.mask + f0 * n);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
 
-int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st) {
+int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int f0) {
   const long long n = (long long)M * N;
-  k_fe_store<<<blocks_for(n), 256, 0, st>>>(n, w.x, Uhat);
+  k_fe_store<<<blocks_for(n), 256, 0, st>>>(n, w.x + f0 * n, Uhat);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

@@ -129,107 +129,109 @@ __device__ __forceinline__ Real sample(const Real *__restrict__ img, int W, int 
   Real wu[4], wv[4];
   keys_w(tu, wu);
   keys_w(tv, wv);
-  const Real *p = img + (long long)(cy - 1) * W + (cx - 1);
+  const Real *p = img + ((cy - 1) * W + (cx - 1));
   Real acc = 0;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    const Real *q = p + (long long)r * W;
+    const Real *q = p + r * W;
     Real s = wu[0] * __ldg(q) + wu[1] * __ldg(q + 1) + wu[2] * __ldg(q + 2) + wu[3] * __ldg(q + 3);
     acc += wv[r] * s;
   }
   return acc;
 }
 
+// MATLAB's catch branch (LocalICGN.m:75-80, Subpb1.m:89-92): -1 and NaN
+template <bool SUB>
+__device__ __forceinline__ void fail_minus1(const Args &a, long long s, int lane) {
+  if (lane == 0) {
+    a.iters[s] = -1;
+    a.U[2 * s] = nan64();
+    a.U[2 * s + 1] = nan64();
+    if (!SUB) {
+      for (int q = 0; q < 4; ++q) a.F[4 * s + q] = nan64();
+      for (int q = 0; q < 21; ++q) a.H21out[(long long)q * a.n + s] = 0.0;
+    }
+  }
+}
+
+// more than half of the subset masked (funICGN.m:309-313): 102, P unchanged
+template <bool SUB>
+__device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
+  if (lane == 0) {
+    a.iters[s] = 102;
+    a.U[2 * s] = a.U0[2 * s];
+    a.U[2 * s + 1] = a.U0[2 * s + 1];
+    if (!SUB) {
+      for (int q = 0; q < 4; ++q) a.F[4 * s + q] = 0.0;
+      for (int q = 0; q < 21; ++q) a.H21out[(long long)q * a.n + s] = 0.0;
+    }
+  }
+}
+
+// ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
+// S_f[6] at 57 and S[6] at 63 (kept out of registers to raise occupancy)
+constexpr int WS = 72;
+
 template <typename Real, bool SUB>
-__device__ void process(const Args &a, long long s, int lane, double *Lsh) {
+__device__ void process(const Args &a, long long s, int lane, double *ws) {
+  double *Lsh = ws + 36, *Sfs = ws + 57, *Sks = ws + 63;
   const IcgnImages &im = a.im;
   const double x0 = a.coords[s], y0 = a.coords[a.n + s];
   int w = a.wins ? a.wins[s] : a.w;
-  double P[6];
-  if (SUB) {
-    for (int q = 0; q < 4; ++q) P[q] = a.FOld[4 * s + q];
-    P[4] = a.U0[2 * s];
-    P[5] = a.U0[2 * s + 1];
-  } else {
-    P[0] = P[1] = P[2] = P[3] = 0.0;
-    P[4] = a.U0[2 * s];
-    P[5] = a.U0[2 * s + 1];
-  }
   int xl, yl;
   bool ok = subset_ok(im, x0, y0, w, &xl, &yl);
-  int status = 0;
-  if (ok) {
-    // masked-pixel test of funICGN.m:54-65
-    const Real *gx = Img<Real>::gx(im);
-    int cnt = 0;
-    const int nw = w + 1, npx = nw * nw;
-    for (int p = lane; p < npx; p += 32) {
-      const int iy = p / nw, ix = p - iy * nw;
-      cnt += gx[(long long)(yl - 1 + iy) * im.W + (xl - 1 + ix)] == (Real)0;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    const double nn = (double)npx;
-    if (!((double)cnt < 0.5 * nn)) {
-      status = 102;
-    } else if ((double)cnt > 0.1 * nn) {
-      w = (int)round(sqrt(2.0) * w);
-      ok = subset_ok(im, x0, y0, w, &xl, &yl);
-    }
-  }
   if (!ok) {
-    // LocalICGN.m:75-80 / Subpb1.m:89-92: catch -> -1 and NaN
-    if (lane == 0) {
-      a.iters[s] = -1;
-      a.U[2 * s] = nan64();
-      a.U[2 * s + 1] = nan64();
-      if (!SUB) {
-        for (int q = 0; q < 4; ++q) a.F[4 * s + q] = nan64();
-        for (int q = 0; q < 21; ++q) a.H21out[(long long)q * a.n + s] = 0.0;
-      }
-    }
+    fail_minus1<SUB>(a, s, lane);
     return;
   }
-  if (status == 102) {
-    if (lane == 0) {
-      a.iters[s] = 102;
-      a.U[2 * s] = P[4];
-      a.U[2 * s + 1] = P[5];
-      if (!SUB) {
-        for (int q = 0; q < 4; ++q) a.F[4 * s + q] = P[q];
-        for (int q = 0; q < 21; ++q) a.H21out[(long long)q * a.n + s] = 0.0;
-      }
-    }
-    return;
-  }
-
   const Real *fI = Img<Real>::f(im);
   const Real *gI = Img<Real>::g(im);
   const Real *gxI = Img<Real>::gx(im);
   const Real *gyI = Img<Real>::gy(im);
-  const int nw = w + 1, npx = nw * nw;
-  // pixel (ix, iy) of the subset sits at X = ox + ix, Y = oy + iy relative to
-  // the node (exact in FP32; half-integers when w is odd)
-  const double oxd = (double)xl - x0, oyd = (double)yl - y0;
-  const Real ox = (Real)oxd, oy = (Real)oyd;
   const int W = im.W;
-  const long long base = (long long)(yl - 1) * W + (xl - 1);  // subset top-left, 0-based
-
-  // ---- pass 1: sum f, and H (funICGN.m:67-79)
-  double sf;
-  double Hs[18];
-  {
-    Real af = 0;
-    Real hh[18];
+  // One fused pass over the subset: the masked-pixel count of funICGN.m:54,
+  // the Hessian sums of :67-79, and -- with a shift c (the subset's centre
+  // pixel, keeping the one-pass variance well conditioned) -- sum(f - c),
+  // sum(f - c)^2, S_k = sum sd_k and sum sd_k (f - c).  A 10-50 % masked
+  // subset grows (funICGN.m:57-65) and the pass runs again on the new window.
+  int nw, npx, base;
+  Real ox, oy;
+  double oxd, oyd, c0, A1, A2;
+  for (int attempt = 0;; ++attempt) {
+    nw = w + 1;
+    npx = nw * nw;
+    oxd = (double)xl - x0;
+    oyd = (double)yl - y0;
+    ox = (Real)oxd;
+    oy = (Real)oyd;
+    base = (yl - 1) * W + (xl - 1);  // subset top-left, 0-based
+    const Real c = fI[base + (nw / 2) * W + nw / 2];
+    c0 = (double)c;
+    int cnt = 0;
+    Real a1 = 0, a2 = 0, sk[6], sfk[6], hh[18];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sk[q] = sfk[q] = 0;
 #pragma unroll
     for (int q = 0; q < 18; ++q) hh[q] = 0;
+    int iy = lane / nw, ix = lane - iy * nw;
     for (int p = lane; p < npx; p += 32) {
-      const int iy = p / nw, ix = p - iy * nw;
-      const long long k = base + (long long)iy * W + ix;
-      af += fI[k];
-      if (!SUB) {
-        const Real fx = gxI[k], fy = gyI[k];
+      const int k = base + iy * W + ix;
+      const Real fx = gxI[k], fy = gyI[k];
+      const Real d = fI[k] - c;
+      cnt += fx == (Real)0;
+      a1 += d;
+      a2 += d * d;
+      if (SUB) {
+        sk[4] += fx; sk[5] += fy;
+        sfk[4] += fx * d; sfk[5] += fy * d;
+      } else {
         const Real X = ox + (Real)ix, Y = oy + (Real)iy;
+        const Real sd[6] = {fx * X, fy * X, fx * Y, fy * Y, fx, fy};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          sk[q] += sd[q];
+          sfk[q] += sd[q] * d;
+        }
         const Real fxx = fx * fx, fyy = fy * fy, fxy = fx * fy;
         const Real XX = X * X, YY = Y * Y, XY = X * Y;
         hh[0] += XX * fxx;  hh[1] += XX * fxy;  hh[2] += XY * fxx;  hh[3] += XY * fxy;
@@ -238,68 +240,87 @@ __device__ void process(const Args &a, long long s, int lane, double *Lsh) {
         hh[12] += Y * fxy;  hh[13] += YY * fyy; hh[14] += Y * fyy;  hh[15] += fxx;
         hh[16] += fxy;      hh[17] += fyy;
       }
-    }
-    sf = warp_sum((double)af);
-    if (!SUB) {
-#pragma unroll
-      for (int q = 0; q < 18; ++q) Hs[q] = warp_sum((double)hh[q]);
-    }
-  }
-  const double meanf = sf / (double)npx;
-  // ---- pass 2: bf, S_fk = sum sd_k (f - fbar), S_k = sum sd_k
-  double ssf, Sf[6], Sk[6];
-  {
-    const Real mf = (Real)meanf;
-    Real a2 = 0, sfk[6], sk[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) sfk[q] = sk[q] = 0;
-    for (int p = lane; p < npx; p += 32) {
-      const int iy = p / nw, ix = p - iy * nw;
-      const long long k = base + (long long)iy * W + ix;
-      const Real d = fI[k] - mf;
-      a2 += d * d;
-      const Real fx = gxI[k], fy = gyI[k];
-      if (SUB) {
-        sfk[4] += fx * d; sfk[5] += fy * d;
-        sk[4] += fx; sk[5] += fy;
-      } else {
-        const Real X = ox + (Real)ix, Y = oy + (Real)iy;
-        const Real sd[6] = {fx * X, fy * X, fx * Y, fy * Y, fx, fy};
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          sfk[q] += sd[q] * d;
-          sk[q] += sd[q];
-        }
+      ix += 32;
+      while (ix >= nw) {
+        ix -= nw;
+        iy++;
       }
     }
-    // residual of the shift mf vs meanf, exact in FP64
-    const double dm = (double)mf - meanf;
-    ssf = warp_sum((double)a2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    const double nn = (double)npx;
+    if (attempt == 0) {
+      if (!((double)cnt < 0.5 * nn)) {
+        done_102<SUB>(a, s, lane);
+        return;
+      }
+      if ((double)cnt > 0.1 * nn) {
+        w = (int)round(sqrt(2.0) * w);
+        if (!subset_ok(im, x0, y0, w, &xl, &yl)) {
+          fail_minus1<SUB>(a, s, lane);
+          return;
+        }
+        continue;
+      }
+    }
+    A1 = warp_sum((double)a1);
+    A2 = warp_sum((double)a2);
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
-      Sk[q] = (SUB && q < 4) ? 0.0 : warp_sum((double)sk[q]);
-      Sf[q] = (SUB && q < 4) ? 0.0 : warp_sum((double)sfk[q]) + dm * Sk[q];
+      const double vk = (SUB && q < 4) ? 0.0 : warp_sum((double)sk[q]);
+      const double vf = (SUB && q < 4) ? 0.0 : warp_sum((double)sfk[q]);
+      if (lane == 0) {
+        Sks[q] = vk;
+        Sfs[q] = vf;  // sum sd_k (f - c); corrected to f - mean f below
+      }
     }
-    // sum (f - meanf)^2 = sum (f - mf)^2 + 2 dm sum(f - mf) + n dm^2
-    ssf = ssf + 2.0 * dm * (sf - (double)npx * (double)mf) + (double)npx * dm * dm;
+    if (!SUB) {
+      // the 18 distinct Hessian sums are staged in ws[0..17] (lane 0) until
+      // H is expanded in place below
+#pragma unroll
+      for (int q = 0; q < 18; ++q) {
+        const double v = warp_sum((double)hh[q]);
+        if (lane == 0) ws[q] = v;
+      }
+    }
+    break;
   }
+  const double dmc = A1 / (double)npx;  // mean(f) - c
+  const double meanf = c0 + dmc;
+  const double ssf = A2 - A1 * dmc;      // sum (f - mean f)^2
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) Sfs[q] -= dmc * Sks[q];  // sum sd_k (f - mean f)
+  }
+  double P[6];
+  if (SUB) {
+    for (int q = 0; q < 4; ++q) P[q] = a.FOld[4 * s + q];
+  } else {
+    P[0] = P[1] = P[2] = P[3] = 0.0;
+  }
+  P[4] = a.U0[2 * s];
+  P[5] = a.U0[2 * s + 1];
   const double bf = sqrt(ssf);
 
   // ---- Hessian factor (IC-GN) or the damped 2x2 system (Subpb1)
-  double Hm[36];
+  double *Hm = ws;
   bool spd = true;
   double s2 = 0, Ha = 0, Hb = 0, Hd = 0;
   if (!SUB) {
-    const double *q = Hs;
-    const double H[36] = {q[0], q[1], q[2], q[3], q[4], q[5],  q[1], q[6], q[3], q[7], q[5], q[8],
-                          q[2], q[3], q[9], q[10], q[11], q[12], q[3], q[7], q[10], q[13], q[12], q[14],
-                          q[4], q[5], q[11], q[12], q[15], q[16], q[5], q[8], q[12], q[14], q[16], q[17]};
-#pragma unroll
-    for (int k = 0; k < 36; ++k) Hm[k] = H[k];
-    if (lane == 0) spd = chol6(Hm, Lsh);
+    if (lane == 0) {
+      // H of funICGN.m:67-79 from its 18 distinct sums (index map)
+      const unsigned char map[36] = {0, 1, 2, 3, 4, 5,   1, 6, 3, 7, 5, 8,
+                                     2, 3, 9, 10, 11, 12, 3, 7, 10, 13, 12, 14,
+                                     4, 5, 11, 12, 15, 16, 5, 8, 12, 14, 16, 17};
+      double q[18];
+      for (int k = 0; k < 18; ++k) q[k] = ws[k];
+      for (int k = 0; k < 36; ++k) Hm[k] = q[map[k]];
+      spd = chol6(Hm, Lsh);
+    }
     spd = __shfl_sync(0xffffffffu, (int)spd, 0);
     __syncwarp();
   } else {
+    __syncwarp();
     // funICGN_Subpb1.m:73,281-283
     s2 = 2.0 / (bf * bf);
     const double h55 = a.H21in[18 * a.n + s], h65 = a.H21in[19 * a.n + s],
@@ -354,7 +375,7 @@ __device__ void process(const Args &a, long long s, int lane, double *Lsh) {
         const Real fu = floor(ru), fv = floor(rv);
         const int cx = xb + (int)fu - 1, cy = yb + (int)fv - 1;  // 0-based floor corner
         const Real gval = sample<Real>(gI, W, cx, cy, ru - fu, rv - fv);
-        const long long k = base + (long long)iy * W + ix;
+        const int k = base + iy * W + ix;
         const Real d = gval - cg;
         s1 += d;
         s2r += d * d;
@@ -390,13 +411,13 @@ __device__ void process(const Args &a, long long s, int lane, double *Lsh) {
     if (!SUB) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const double b2 = Sf[q] / bf - (sums[2 + q] - gm * Sk[q]) / bg;
+        const double b2 = Sfs[q] / bf - (sums[2 + q] - gm * Sks[q]) / bg;
         b[q] = bf * b2;
         nb += b[q] * b[q];
       }
     } else {
-      const double b5 = bf * (Sf[4] / bf - (sums[6] - gm * Sk[4]) / bg);
-      const double b6 = bf * (Sf[5] / bf - (sums[7] - gm * Sk[5]) / bg);
+      const double b5 = bf * (Sfs[4] / bf - (sums[6] - gm * Sks[4]) / bg);
+      const double b6 = bf * (Sfs[5] / bf - (sums[7] - gm * Sks[5]) / bg);
       b[4] = b5 * s2 + a.mu * (P[4] - a.U0[2 * s] - a.vdual[2 * s]);
       b[5] = b6 * s2 + a.mu * (P[5] - a.U0[2 * s + 1] - a.vdual[2 * s + 1]);
       nb = b[4] * b[4] + b[5] * b[5];
@@ -443,8 +464,8 @@ __device__ void process(const Args &a, long long s, int lane, double *Lsh) {
 }
 
 template <typename Real, bool SUB>
-__global__ void __launch_bounds__(WARPS * 32) k_icgn(Args a) {
-  __shared__ double Lsh[WARPS][24];
+__global__ void __launch_bounds__(WARPS * 32, sizeof(Real) == 4 ? 3 : 2) k_icgn(Args a) {
+  __shared__ double Lsh[WARPS][WS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   while (true) {
     unsigned int s = 0;

@@ -158,6 +158,80 @@ __device__ void findpeak_fit(const double *map, int nr, int nc, int im, double *
   *max_f = m;
 }
 
+// Argmax of the cropped map (first maximum in column-major order, as
+// MATLAB's max), the sub-pixel fit of findpeak.m and the outputs of
+// funIntegerSearch.m:148-159.  Called by all threads of the block.
+__device__ void peak_epilogue(const double *map, const SearchGeom &G, int ii, int jj,
+                              long long out_idx, double *redv, int *redi, double *ox,
+                              double *oy, double *ou, double *ov, double *occ) {
+  const int tid = threadIdx.x, nth = blockDim.x;
+  double best = -1e300;
+  int bi = 0x7fffffff;
+  const int nm = G.cr * G.cc;
+  for (int i = tid; i < nm; i += nth) {
+    const double v = map[i];
+    if (v > best || (v == best && i < bi)) {
+      best = v;
+      bi = i;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
+    }
+  }
+  if ((tid & 31) == 0) {
+    redv[tid >> 5] = best;
+    redi[tid >> 5] = bi;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int k = 1; k < (nth + 31) / 32; ++k)
+      if (redv[k] > best || (redv[k] == best && redi[k] < bi)) {
+        best = redv[k];
+        bi = redi[k];
+      }
+    double rpk, cpk, mf;
+    findpeak_fit(map, G.cr, G.cc, bi, &rpk, &cpk, &mf);
+    ox[out_idx] = (ii + ii + G.w) / 2.0;
+    oy[out_idx] = (jj + jj + G.w) / 2.0;
+    ou[out_idx] = __dsub_rn(rpk, (double)(G.sx + 2));
+    ov[out_idx] = __dsub_rn(cpk, (double)(G.sy + 2));
+    occ[out_idx] = mf;
+  }
+}
+
+// Template pixels of a placement that fall into the padding: column t is
+// outside when t + a - 1 lies outside [0, dw), row t when t + b - 1 lies
+// outside [0, dh).  Returns their template sum and count.
+template <typename S, typename TV>
+__device__ __forceinline__ void pad_terms(const SearchGeom &G, int a, int b, const S *colsum,
+                                          const S *rowsum, TV tpix, S *st_out, long long *n_out) {
+  S so = 0;
+  long long nco = 0, nro = 0;
+  for (int t = 0; t < G.tw; ++t) {
+    const int xo = t + a - 1, yo = t + b - 1;
+    if (xo < 0 || xo >= G.dw) { so += colsum[t]; nco++; }
+    if (yo < 0 || yo >= G.dh) { so += rowsum[t]; nro++; }
+  }
+  if (nco && nro) {
+    for (int ty = 0; ty < G.tw; ++ty) {
+      const int yo = ty + b - 1;
+      if (!(yo < 0 || yo >= G.dh)) continue;
+      for (int tx = 0; tx < G.tw; ++tx) {
+        const int xo = tx + a - 1;
+        if (xo < 0 || xo >= G.dw) so -= (S)tpix(ty, tx);
+      }
+    }
+  }
+  *st_out = so;
+  *n_out = nco * G.tw + nro * G.tw - nco * nro;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(512) k_search(const T *__restrict__ f, const T *__restrict__ g,
                                                 SearchGeom G, double *__restrict__ ox,
@@ -298,26 +372,10 @@ __global__ void __launch_bounds__(512) k_search(const T *__restrict__ f, const T
         sd += RS[(b + ty) * G.cr + a];
         sd2 += RS2[(b + ty) * G.cr + a];
       }
-      // template pixels falling into the padding: column tx is outside when
-      // tx + a - 1 < 0 or >= dw, row ty when ty + b - 1 < 0 or >= dh
-      S st_out = 0;
-      long long n_out = 0, nco = 0, nro = 0;
-      for (int t = 0; t < G.tw; ++t) {
-        const int xo = t + a - 1, yo = t + b - 1;
-        if (xo < 0 || xo >= G.dw) { st_out += colsum[t]; nco++; }
-        if (yo < 0 || yo >= G.dh) { st_out += rowsum[t]; nro++; }
-      }
-      if (nco && nro) {
-        for (int ty = 0; ty < G.tw; ++ty) {
-          const int yo = ty + b - 1;
-          if (!(yo < 0 || yo >= G.dh)) continue;
-          for (int tx = 0; tx < G.tw; ++tx) {
-            const int xo = tx + a - 1;
-            if (xo < 0 || xo >= G.dw) st_out -= (S)Tp[ty * G.twp + tx];
-          }
-        }
-      }
-      n_out = nco * G.tw + nro * G.tw - nco * nro;
+      S st_out;
+      long long n_out;
+      pad_terms<S>(G, a, b, colsum, rowsum, [&](int ty, int tx) { return Tp[ty * G.twp + tx]; },
+                   &st_out, &n_out);
       double r;
       if (Tr::integer)
         r = ncc_combine(mn, (long long)st, (long long)st2, (long long)acc[k], (long long)sd,
@@ -329,45 +387,215 @@ __global__ void __launch_bounds__(512) k_search(const T *__restrict__ f, const T
     }
   }
   __syncthreads();
-  // ---- argmax, first index in column-major order
-  double best = -1e300;
-  int bi = 0x7fffffff;
-  const int nm = G.cr * G.cc;
-  for (int i = tid; i < nm; i += nth) {
-    const double v = map[i];
-    if (v > best || (v == best && i < bi)) {
-      best = v;
-      bi = i;
-    }
+  peak_epilogue(map, G, ii, jj, out_idx, redv, redi, ox, oy, ou, ov, occ);
+}
+
+// ---- 8-bit images: byte-packed correlation with __dp4a (exact int32).
+// The padded region is staged once as aligned 32-bit words (4 pixels each);
+// the 4-pixel window starting at any column is one funnel shift of two
+// neighbouring words, and the template row is packed 4 pixels per word.  A
+// thread owns 8 consecutive shifts of one window row: per template word it
+// loads one template word and one region word, forms 8 windows and issues 8
+// dp4a -- 32 exact multiply-adds.
+struct U8Layout {
+  int tw4, dqw;  // template words per row, region words per row (odd pitch)
+  size_t tb, dw, tq, rs, cs, map, red, total;
+  __host__ __device__ U8Layout(const SearchGeom &g) {
+    tw4 = (g.tw + 3) / 4;
+    // words read: up to (nsx-1)*2 + tw4 + 1; the bytes must also hold the
+    // padded region (dw + 2) and the row-sum window (cr + tw)
+    int need = 2 * g.nsx + tw4 + 2;
+    const int nb = (g.cr + g.tw + 3) / 4 + 1;
+    if (need < nb) need = nb;
+    dqw = need | 1;  // odd pitch: the rows a warp touches fall on different banks
+    size_t o = 0;
+    tb = o; o = align16(o + (size_t)g.tw * g.tw);
+    dw = o; o = align16(o + sizeof(unsigned) * g.dph * dqw);
+    tq = o; o = align16(o + sizeof(unsigned) * g.tw * tw4);
+    // window row sums RS, RS2 (dph x cr each); dead once the box sums are
+    // formed, after which the NCC map (cr x cc doubles) reuses the space
+    rs = o;
+    const size_t rsz = sizeof(int) * 2 * g.dph * g.cr, msz = sizeof(double) * g.cr * g.cc;
+    o = align16(o + (rsz > msz ? rsz : msz));
+    map = rs;
+    cs = o; o = align16(o + sizeof(int) * 2 * g.cc * g.cr);  // box sums of D and D^2
+    red = o; o = align16(o + (sizeof(double) + sizeof(int)) * 32 + 64);
+    total = o;
   }
+};
+
+__global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f,
+                                                   const uint8_t *__restrict__ g, SearchGeom G,
+                                                   double *__restrict__ ox,
+                                                   double *__restrict__ oy,
+                                                   double *__restrict__ ou,
+                                                   double *__restrict__ ov,
+                                                   double *__restrict__ occ) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const U8Layout L(G);
+  uint8_t *Tb = smem + L.tb;                 // template bytes, tw x tw
+  unsigned *Dw = (unsigned *)(smem + L.dw);  // padded region, dph rows of dqw words
+  const uint8_t *Db = (const uint8_t *)Dw;   // the same, as bytes (row pitch 4*dqw)
+  unsigned *Tq = (unsigned *)(smem + L.tq);
+  int *RS = (int *)(smem + L.rs);
+  int *RS2 = RS + G.dph * G.cr;
+  int *CS = (int *)(smem + L.cs);
+  int *CS2 = CS + G.cc * G.cr;
+  double *map = (double *)(smem + L.map);
+  double *redv = (double *)(smem + L.red);
+  int *redi = (int *)(redv + 32);
+  __shared__ long long s_st, s_st2;
+  __shared__ int colsum_s[72], rowsum_s[72];
+  const double mu = *G.mu;
+  const int pt = blockIdx.x;
+  const int ix = pt % G.nx, iy = pt / G.nx;
+  const int ii = G.gx1 + ix * G.step, jj = G.gy1 + iy * G.step;  // 1-based
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5, nwarp = nth >> 5;
+  const uint8_t *trow0 = f + (long long)(jj - 1) * G.W + (ii - 1);
+  const uint8_t *drow0 = g + (long long)(jj - 1 - G.sy) * G.W + (ii - 1 - G.sx);
+  const int dbp = 4 * L.dqw;  // byte pitch
+  // ---- stage template bytes and the padded region (warp per row, lanes over
+  // columns; 1-pixel zero border at the top/left, zeros beyond the region)
+  for (int ty = wid; ty < G.tw; ty += nwarp)
+    for (int tx = lane; tx < G.tw; tx += 32) Tb[ty * G.tw + tx] = trow0[(long long)ty * G.W + tx];
+  for (int y = wid; y < G.dph; y += nwarp) {
+    const bool rin = y >= 1 && y <= G.dh;
+    const uint8_t *src = drow0 + (long long)(y - 1) * G.W;
+    for (int w4 = lane; w4 < L.dqw; w4 += 32) {
+      unsigned v = 0;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    if (ob > best || (ob == best && oi < bi)) {
-      best = ob;
-      bi = oi;
+      for (int k = 0; k < 4; ++k) {
+        const int x = 4 * w4 + k;
+        if (rin && x >= 1 && x <= G.dw) v |= (unsigned)src[x - 1] << (8 * k);
+      }
+      Dw[y * L.dqw + w4] = v;
     }
-  }
-  if ((tid & 31) == 0) {
-    redv[tid >> 5] = best;
-    redi[tid >> 5] = bi;
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int k = 1; k < (nth + 31) / 32; ++k)
-      if (redv[k] > best || (redv[k] == best && redi[k] < bi)) {
-        best = redv[k];
-        bi = redi[k];
+  // ---- packed template words, window row sums, template sums
+  for (int ty = wid; ty < G.tw; ty += nwarp)
+    for (int w4 = lane; w4 < L.tw4; w4 += 32) {
+      unsigned v = 0;
+      for (int k = 0; k < 4; ++k) {
+        const int tx = 4 * w4 + k;
+        if (tx < G.tw) v |= (unsigned)Tb[ty * G.tw + tx] << (8 * k);
       }
-    double rpk, cpk, mf;
-    findpeak_fit(map, G.cr, G.cc, bi, &rpk, &cpk, &mf);
-    ox[out_idx] = (ii + ii + G.w) / 2.0;
-    oy[out_idx] = (jj + jj + G.w) / 2.0;
-    ou[out_idx] = __dsub_rn(rpk, (double)(G.sx + 2));
-    ov[out_idx] = __dsub_rn(cpk, (double)(G.sy + 2));
-    occ[out_idx] = mf;
+      Tq[ty * L.tw4 + w4] = v;
+    }
+  for (int y = tid; y < G.dph; y += nth) {
+    const uint8_t *row = Db + y * dbp;
+    int s1 = 0, s2 = 0;
+    for (int k = 0; k < G.tw; ++k) {
+      const int v = row[k];
+      s1 += v;
+      s2 += v * v;
+    }
+    for (int a = 0; a < G.cr; ++a) {
+      RS[y * G.cr + a] = s1;
+      RS2[y * G.cr + a] = s2;
+      const int vo = row[a], vi = row[a + G.tw];
+      s1 += vi - vo;
+      s2 += vi * vi - vo * vo;
+    }
   }
+  for (int i = tid; i < G.tw; i += nth) {
+    int cs = 0, rsum = 0;
+    for (int k = 0; k < G.tw; ++k) {
+      cs += Tb[k * G.tw + i];
+      rsum += Tb[i * G.tw + k];
+    }
+    colsum_s[i] = cs;
+    rowsum_s[i] = rsum;
+  }
+  if (tid < 32) {
+    long long a = 0, a2 = 0;
+    for (int i = tid; i < G.tw * G.tw; i += 32) {
+      const long long v = Tb[i];
+      a += v;
+      a2 += v * v;
+    }
+    a = warp_sum_ll(a);
+    a2 = warp_sum_ll(a2);
+    if (tid == 0) {
+      s_st = a;
+      s_st2 = a2;
+    }
+  }
+  __syncthreads();
+  // ---- box sums of D and D^2 over every window: slide the row sums down
+  for (int a = tid; a < 2 * G.cr; a += nth) {
+    const int col = a < G.cr ? a : a - G.cr;
+    const int *R = a < G.cr ? RS : RS2;
+    int *Cc = a < G.cr ? CS : CS2;
+    int s1 = 0;
+    for (int k = 0; k < G.tw; ++k) s1 += R[k * G.cr + col];
+    for (int b = 0; b < G.cc; ++b) {
+      Cc[b * G.cr + col] = s1;
+      s1 += R[(b + G.tw) * G.cr + col] - R[b * G.cr + col];
+    }
+  }
+  __syncthreads();  // RS is dead from here on; the map takes its place
+  const long long st = s_st, st2 = s_st2;
+  const long long mn = (long long)G.tw * G.tw;
+  const long long out_idx = (long long)iy + (long long)ix * G.ny;
+  if (mn * st2 - st * st == 0) {
+    if (tid == 0) {
+      const double nan = __longlong_as_double(0x7ff8000000000000ll);
+      ox[out_idx] = (ii + ii + G.w) / 2.0;
+      oy[out_idx] = (jj + jj + G.w) / 2.0;
+      ou[out_idx] = nan;
+      ov[out_idx] = nan;
+      occ[out_idx] = nan;
+    }
+    return;
+  }
+  // ---- correlation strips: 8 shifts of one window row per thread
+  const int nstrips = G.cc * G.nsx;
+  for (int sidx = tid; sidx < nstrips; sidx += nth) {
+    const int b = sidx / G.nsx;
+    const int a0 = (sidx % G.nsx) * KX;  // multiple of 8
+    unsigned acc[KX];
+#pragma unroll
+    for (int k = 0; k < KX; ++k) acc[k] = 0u;
+    const int wbase = a0 >> 2;
+    for (int ty = 0; ty < G.tw; ++ty) {
+      const unsigned *trow = Tq + ty * L.tw4;
+      const unsigned *dr = Dw + (b + ty) * L.dqw + wbase;
+      unsigned w0 = dr[0], w1 = dr[1];
+#pragma unroll 3
+      for (int jw = 0; jw < L.tw4; ++jw) {
+        const unsigned t = trow[jw];
+        const unsigned w2 = dr[jw + 2];
+        acc[0] = __dp4a(t, w0, acc[0]);
+        acc[1] = __dp4a(t, __funnelshift_r(w0, w1, 8), acc[1]);
+        acc[2] = __dp4a(t, __funnelshift_r(w0, w1, 16), acc[2]);
+        acc[3] = __dp4a(t, __funnelshift_r(w0, w1, 24), acc[3]);
+        acc[4] = __dp4a(t, w1, acc[4]);
+        acc[5] = __dp4a(t, __funnelshift_r(w1, w2, 8), acc[5]);
+        acc[6] = __dp4a(t, __funnelshift_r(w1, w2, 16), acc[6]);
+        acc[7] = __dp4a(t, __funnelshift_r(w1, w2, 24), acc[7]);
+        w0 = w1;
+        w1 = w2;
+      }
+    }
+    const bool ring_b = (b == 0 || b == G.cc - 1);
+#pragma unroll
+    for (int k = 0; k < KX; ++k) {
+      const int a = a0 + k;
+      if (a >= G.cr) break;
+      const long long sd = CS[b * G.cr + a], sd2 = CS2[b * G.cr + a];
+      int st_out = 0;
+      long long n_out = 0;
+      // only the outermost ring of the cropped map overhangs the region
+      if (ring_b || a == 0 || a == G.cr - 1)
+        pad_terms<int>(G, a, b, colsum_s, rowsum_s,
+                       [&](int ty, int tx) { return (int)Tb[ty * G.tw + tx]; }, &st_out, &n_out);
+      map[b * G.cr + a] = ncc_combine(mn, st, st2, (long long)acc[k], sd, sd2, st_out, n_out, mu);
+    }
+  }
+  __syncthreads();
+  peak_epilogue(map, G, ii, jj, out_idx, redv, redi, ox, oy, ou, ov, occ);
 }
 
 // ---- q-factors over the full (2w+2s+1)^2 map (optional, direct sums)
@@ -493,17 +721,28 @@ int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, 
   using Tr = SearchTraits<T>;
   using V = typename Tr::V;
   using S = typename SumT<Tr::integer>::type;
-  SmemLayout<V, S> L(G);
-  ALDIC_CHECK(L.total <= 227 * 1024, E_ARG, "integer search: window/search size too large for shared memory");
-  ALDIC_CUDA(cudaFuncSetAttribute(k_search<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)L.total));
   const int nstrips = G.cc * G.nsx;
   int threads = ((nstrips + 31) / 32) * 32;
   if (threads < 64) threads = 64;
   if (threads > 512) threads = 512;
   const int npts = G.nx * G.ny;
   if (npts == 0) return OK;
-  k_search<T><<<npts, threads, L.total, st>>>((const T *)f, (const T *)g, G, x, y, u, v, cc);
+  if (sizeof(T) == 1) {
+    U8Layout L(G);
+    ALDIC_CHECK(L.total <= 227 * 1024 && G.tw <= 72, E_ARG,
+                "integer search: window/search size too large for shared memory");
+    ALDIC_CUDA(cudaFuncSetAttribute(k_search_u8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)L.total));
+    k_search_u8<<<npts, threads, L.total, st>>>((const uint8_t *)f, (const uint8_t *)g, G, x, y,
+                                                 u, v, cc);
+  } else {
+    SmemLayout<V, S> L(G);
+    ALDIC_CHECK(L.total <= 227 * 1024, E_ARG,
+                "integer search: window/search size too large for shared memory");
+    ALDIC_CUDA(cudaFuncSetAttribute(k_search<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)L.total));
+    k_search<T><<<npts, threads, L.total, st>>>((const T *)f, (const T *)g, G, x, y, u, v, cc);
+  }
   ALDIC_CUDA(cudaGetLastError());
   if (pce) {
     const int fr = 2 * G.w + 2 * G.sx + 1, fc = 2 * G.w + 2 * G.sy + 1;

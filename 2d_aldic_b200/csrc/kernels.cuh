@@ -41,7 +41,7 @@ int subpb1(const IcgnImages &im, const double *coords, long long n, const double
 
 // ---- k_grid.cu: node-grid solvers and field kernels on the M x N mesh
 struct GridWork {
-  // PCG vectors for up to 6 right-hand sides of M*N (x fastest) each
+  // PCG vectors for up to 12 right-hand sides of M*N (x fastest) each
   double *x, *r, *z, *p, *q, *b, *diag;
   double *part;          // per-block partial sums: [3][nrhs][blocks]
   unsigned char *mask;   // per node flags (data present / unknown)
@@ -55,13 +55,13 @@ enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2 };
 // solve op(x) = b for nrhs fields; b and x live in w.b / w.x (field-major)
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
              double lam2, double rtol, int maxit, cudaStream_t st,
-             const double *beta_ptr = nullptr);
+             const double *beta_ptr = nullptr, const double *beta_each = nullptr);
 // Subpb2 right-hand side (Subpb2.m:76-159) into w.b (2 fields: u, v)
 int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
            const double *F, const double *udual, const double *vdual, cudaStream_t st,
-           const double *beta_ptr = nullptr);
-// interleave w.x (2 fields) into Uhat
-int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st);
+           const double *beta_ptr = nullptr, int f0 = 0);
+// interleave w.x (2 fields from slot f0) into Uhat
+int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int f0 = 0);
 // nodal strain (funGlobal_NodalStrainAvg.m)
 int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st);
 // gridfit springs: load nf interleaved (stride, offset) fields, NaN = no data

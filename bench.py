@@ -337,7 +337,10 @@ def main():
                                    "step 8, search 16, tol 1e-2, 3 ADMM iterations",
                        "subsets": n, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"replicas x{world}",
-                       "stage_ms": mst},
+                       "stage_ms": mst,
+                       "max_pcg_iters": r["stats"].get("max_pcg_iters"),
+                       "mean_iters_icgn": r["stats"].get("mean_iters_icgn"),
+                       "beta": r["stats"].get("beta")},
             "roofline": {"kernel": "k_icgn (IC-GN, FP32)", "bound": "hbm", "achieved": achieved,
                          "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "traffic": traffic, "peak_source": peak_src,

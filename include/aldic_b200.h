@@ -207,6 +207,7 @@ typedef struct {
    * search + Init, 2 IC-GN kernel, 3 LocalICGN post-processing, 4 Section 5
    * (beta, Subpb2, nodal strain), 5 ADMM iterations, 6 whole frame */
   double t_stage_ms[8];
+  int max_pcg_iters;        /* most PCG iterations taken by one node-grid solve */
 } aldic_frame_stats;
 
 ALDIC_API int aldic_frame_dims(aldic_ctx *ctx, const aldic_frame_params *p, int *M, int *N);
