@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="uniform2048")
-    ap.add_argument("--cpu-crop", type=int, default=768,
+    ap.add_argument("--cpu-crop", type=int, default=1536,
                     help="side of the image crop the CPU baseline runs on")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

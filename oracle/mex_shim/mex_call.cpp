@@ -39,3 +39,34 @@ extern "C" int shim_call_mex(int nlhs, int nrhs, const int *cls, const int *ndim
   for (int i = 0; i < 4; ++i) mxDestroyArray(plhs[i]);
   return rc;
 }
+
+// Several outputs: outs[i] receives plhs[i] (out_bytes[i] capacity).
+extern "C" int shim_call_mex_n(int nlhs, int nrhs, const int *cls, const int *ndims,
+                               const long long *dims, void **datas, void **outs,
+                               const size_t *out_bytes) {
+  mxArray *prhs[16];
+  mxArray *plhs[8] = {nullptr};
+  int rc = 0;
+  const long long *dp = dims;
+  for (int i = 0; i < nrhs; ++i) {
+    mwSize d[8];
+    for (int k = 0; k < ndims[i]; ++k) d[k] = (mwSize)dp[k];
+    dp += ndims[i];
+    prhs[i] = shim_wrap((mxClassID)cls[i], (mwSize)ndims[i], d, datas[i]);
+  }
+  try {
+    mexFunction(nlhs, plhs, nrhs, (const mxArray **)prhs);
+    for (int o = 0; o < nlhs && o < 8; ++o) {
+      if (!plhs[o]) continue;
+      size_t n = mxGetNumberOfElements(plhs[o]);
+      size_t es = mxIsDouble(plhs[o]) ? 8 : 4;
+      if (n * es > out_bytes[o]) rc = -2;
+      else std::memcpy(outs[o], mxGetData(plhs[o]), n * es);
+    }
+  } catch (const std::exception &) {
+    rc = -1;
+  }
+  for (int i = 0; i < nrhs; ++i) mxDestroyArray(prhs[i]);
+  for (int i = 0; i < 8; ++i) mxDestroyArray(plhs[i]);
+  return rc;
+}

@@ -1,0 +1,142 @@
+"""The MEX gateways of 2d_aldic_b200/mex, built against the project's MEX
+shim and driven exactly as MATLAB calls a MEX function.  The drop-in
+ba_interp2 gateway must reproduce the reference's ba_interp2 (errors without
+a GPU, results bit for bit with one)."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILD = os.path.join(ROOT, "tests", "_build")
+SHIM = os.path.join(ROOT, "oracle", "mex_shim")
+CLS = {np.dtype(np.float64): 6, np.dtype(np.float32): 7, np.dtype(np.int32): 12}
+
+
+def build_gateway(src_name, out_name):
+    os.makedirs(BUILD, exist_ok=True)
+    out = os.path.join(BUILD, out_name)
+    src = os.path.join(ROOT, "2d_aldic_b200", "mex", src_name)
+    libdir = os.path.join(ROOT, "2d_aldic_b200")
+    if not os.path.exists(out) or os.path.getmtime(out) < max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(libdir, "libaldic_b200.so"))):
+        subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", f"-I{SHIM}",
+                        f"-I{os.path.join(ROOT, 'include')}", "-o", out, src,
+                        os.path.join(SHIM, "mex_shim.cpp"), os.path.join(SHIM, "mex_call.cpp"),
+                        f"-L{libdir}", "-laldic_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    lib = C.CDLL(out)
+    lib.shim_last_error.restype = C.c_char_p
+    return lib
+
+
+def mex_call(lib, nlhs, args, out_bytes):
+    """Call mexFunction with numpy arrays (column-major MATLAB shapes given as
+    the arrays' .T) or str (char arrays); returns (rc, outputs)."""
+    cls, ndims, dims, datas, keep = [], [], [], [], []
+    for a in args:
+        if isinstance(a, str):
+            arr = np.frombuffer(a.encode("utf-16-le"), dtype=np.uint16).copy()
+            cls.append(4)
+            d = [1, len(a)]
+        else:
+            arr = np.asfortranarray(np.atleast_2d(a) if np.ndim(a) < 2 else a)
+            cls.append(CLS[arr.dtype])
+            d = list(arr.shape)
+        keep.append(arr)
+        ndims.append(len(d))
+        dims += d
+        datas.append(arr.ctypes.data)
+    outs = [np.zeros(b // 8 + 1, np.float64) for b in out_bytes]
+    rc = lib.shim_call_mex_n(nlhs, len(args), (C.c_int * len(cls))(*cls),
+                             (C.c_int * len(ndims))(*ndims), (C.c_longlong * len(dims))(*dims),
+                             (C.c_void_p * len(datas))(*datas),
+                             (C.c_void_p * len(outs))(*[o.ctypes.data for o in outs]),
+                             (C.c_size_t * len(out_bytes))(*out_bytes))
+    return rc, outs
+
+
+@pytest.fixture(scope="module")
+def gw_interp():
+    return build_gateway("ba_interp2_mex.cpp", "mex_ba_interp2.so")
+
+
+@pytest.fixture(scope="module")
+def gw_aldic():
+    return build_gateway("aldic_mex.cpp", "mex_aldic.so")
+
+
+def _ref_error(args, nlhs=1):
+    import oracle
+    ref = oracle.ref()
+    ref.shim_last_error.restype = C.c_char_p
+    rc, _ = mex_call(ref, nlhs, args, [8])
+    return rc, ref.shim_last_error()
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference not compiled")
+@pytest.mark.parametrize("case", ["nargs", "class", "size", "nlhs"])
+def test_ba_interp2_gateway_errors_match_reference(gw_interp, case):
+    F = np.random.default_rng(0).random((6, 5))
+    X = np.ones((3, 1))
+    if case == "nargs":
+        args, nlhs = [F, X], 1
+    elif case == "class":
+        args, nlhs = [F, X.astype(np.float32), X], 1
+    elif case == "size":
+        args, nlhs = [F, X, np.ones((3, 1, 2))], 1
+    else:
+        args, nlhs = [F, X, X], 2
+    rc, _ = mex_call(gw_interp, nlhs, args, [8, 8])
+    rrc, rmsg = _ref_error(args, nlhs)
+    assert rc == rrc == -1
+    assert gw_interp.shim_last_error() == rmsg
+
+
+def test_aldic_gateway_usage_errors(gw_aldic):
+    rc, _ = mex_call(gw_aldic, 1, ["nosuch"], [8])
+    assert rc == -1 and b"unknown command" in gw_aldic.shim_last_error()
+    rc, _ = mex_call(gw_aldic, 1, ["icgn", np.zeros((2, 1))], [8])
+    assert rc == -1 and b"icgn takes 8 arguments" in gw_aldic.shim_last_error()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_ba_interp2_gateway_matches_reference(gw_interp, dt):
+    import oracle
+    rng = np.random.default_rng(3)
+    F = rng.uniform(0, 255, (40, 30, 2)).astype(dt)       # MATLAB M=40, N=30, P=2
+    X = rng.uniform(-2, 33, (50, 7)).astype(dt)
+    Y = rng.uniform(-2, 43, (50, 7)).astype(dt)
+    rc, outs = mex_call(gw_interp, 1, [F, X, Y, "cubic"], [F.itemsize * X.size * 2])
+    assert rc == 0
+    got = outs[0].view(dt)[:X.size * 2]
+    rref, ro = mex_call(oracle.ref(), 1, [F, X, Y], [F.itemsize * X.size * 2])
+    assert rref == 0
+    np.testing.assert_array_equal(got, ro[0].view(dt)[:X.size * 2])
+
+
+@pytest.mark.gpu
+def test_aldic_gateway_icgn_matches_oracle(gw_aldic, synth, oracle):
+    W, H = 140, 120
+    f = synth.speckle(W, H, 700, 31)
+    g = synth.warp(f, synth.uniform_affine(0.002, -0.001, 0.4, -0.3), 0.5, 31)
+    fn, _, _ = oracle.normalize(f)
+    gn, _, _ = oracle.normalize(g)
+    dx, dy = oracle.gradient(fn)
+    xs = np.arange(30.0, 111.0, 10.0)
+    X, Y = np.meshgrid(xs, np.arange(30.0, 91.0, 10.0))
+    coords = np.stack([X.ravel(), Y.ravel()], 1)
+    n = len(coords)
+    U0 = np.zeros(2 * n)
+    # MATLAB orientation: images W x H column-major == numpy (H, W) C order -> pass .T
+    args = ["icgn", U0[:, None], coords, dx[3:-3, 3:-3].T, dy[3:-3, 3:-3].T, fn.T, gn.T,
+            np.array([[20.0]]), np.array([[1e-3]])]
+    rc, outs = mex_call(gw_aldic, 4, args, [16 * n, 32 * n, 4 * n, 168 * n])
+    assert rc == 0, gw_aldic.shim_last_error()
+    U = outs[0][:2 * n]
+    it = outs[2].view(np.int32)[:n]
+    Uo, Fo, ito, Ho = oracle.icgn_batch(fn, gn, dx, dy, coords, U0, 20, 1e-3)
+    np.testing.assert_array_equal(it, ito)
+    np.testing.assert_allclose(U, Uo, atol=1e-8)
