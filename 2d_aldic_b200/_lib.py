@@ -37,6 +37,7 @@ _SIGS = {
     "aldic_subpb1": ([P, P, I64, P, P, P, P, P, I32, D, D, I32, P, P], I32),
     "aldic_subpb1_post": ([P, I32, I32, P, P, P], I32),
     "aldic_subpb2": ([P, I32, I32, D, D, D, P, P, P, P, P], I32),
+    "aldic_subpb2_noalloc": ([I32, I32, D, D, D, P, P, P, P, P, P], I32),
     "aldic_nodal_strain": ([P, I32, I32, D, P, P], I32),
     "aldic_gridfit_springs": ([P, I32, I32, I32, P, P], I32),
     "aldic_inpaint_springs": ([P, I32, I32, I32, P], I32),

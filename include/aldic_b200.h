@@ -155,6 +155,22 @@ ALDIC_API int aldic_subpb2(aldic_ctx *ctx, int M, int N, double step, double bet
                  const double *U, const double *F, const double *udual,
                  const double *vdual, double *Uhat);
 
+/* No counterpart in the reference.  Subproblem 2 as aldic_subpb2, for callers
+ * that cannot allocate device memory (a host framework that owns every
+ * device byte, a real-time loop that must not stall on an allocation, a
+ * process with audited or capped allocations).  All arrays are DEVICE
+ * pointers (U 2n, F 4n, udual 4n, vdual 2n in; Uhat 2n out, n = M*N); the
+ * solver's work vectors live in one fixed static device array of the library
+ * (about 8.4 MB, held on every GPU that loads the library until exit), so at
+ * most 65536 nodes are accepted -- larger grids return ALDIC_E_ARG.  The
+ * first call on a device looks up that array's device address (make it
+ * before any stream capture).  The array is shared by every call: calls whose
+ * GPU work overlaps (other streams or threads) race.  Returns after the
+ * solve (it reads the solver's status back).  stream: cudaStream_t. */
+ALDIC_API int aldic_subpb2_noalloc(int M, int N, double step, double beta, double mu,
+                                   const double *U, const double *F, const double *udual,
+                                   const double *vdual, double *Uhat, void *stream);
+
 /* funGlobal_NodalStrainAvg.m:1 on the uniform mesh (2x2 Gauss points,
  * extrapolation to the nodes, average over elements).  Output slots per node
  * are [du/dx du/dy dv/dx dv/dy], the order funGlobal_NodalStrainAvg.m:97,
