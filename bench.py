@@ -161,6 +161,28 @@ def icgn_bytes(iters: np.ndarray, winsize: int) -> float:
     return float((12 * N * active + 4 * N * k + 224 * active).sum())
 
 
+def icgn_traffic_from_profile():
+    """DRAM bytes (read + write) of one IC-GN launch from the committed ncu
+    summary of this workload (profiles/k_icgn_uniform2048.md), or None."""
+    import re
+    try:
+        text = open(os.path.join(ROOT, "profiles", "k_icgn_uniform2048.md")).read()
+    except OSError:
+        return None
+    sec = text.split("#### `k_icgn<float, 0>`", 1)
+    if len(sec) < 2:
+        return None
+    sec = sec[1].split("####", 1)[0]
+    tot = 0.0
+    for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+        m = re.search(r"`" + re.escape(key) + r"` \| ([0-9.]+) (\w+)", sec)
+        if not m:
+            return None
+        scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}.get(m.group(2), 1)
+        tot += float(m.group(1)) * scale
+    return tot
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -268,12 +290,7 @@ def main():
     b_icgn = icgn_bytes(iters, wl.winsize)
     t_icgn = statistics.mean(icgn_ms) / 1e3
     achieved = b_icgn / t_icgn / 1e9
-    traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "icgn_traffic.json")))
-        traffic = prof.get("bytes_per_launch")
-    except Exception:
-        pass
+    traffic = icgn_traffic_from_profile()
 
     # ---------------- end to end through the public API with host buffers
     e2e = None
