@@ -865,6 +865,7 @@ struct FrameBufs {
   double *sx, *sy, *su, *sv, *scc;   // search outputs (ny x nx)
   double *coords, *x0, *y0, *U0;
   double *U1, *F1, *H21, *U2, *F2, *udual, *vdual, *U2old, *U1old;
+  double *cache;                    // per-subset IC-GN setup constants (8 doubles)
   double *err;                      // [6] Err1, [6] Err2, misc
   double *beta;                     // [1]
   double *upd;                      // [2*16] update norms
@@ -1001,7 +1002,7 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   if ((rc = mark(c, 2))) return rc;
   const IcgnImages im = images_of(c);
   if ((rc = icgn(im, B.coords, n, B.U0, nullptr, p->winsize, p->tol, p->precision, B.U1, B.F1,
-                 B.it1, B.H21, c->queue.as<unsigned int>(), st)))
+                 B.it1, B.H21, c->queue.as<unsigned int>(), st, B.cache)))
     return rc;
   if ((rc = mark(c, 3))) return rc;
   if ((rc = icgn_flags(M, N, B.it1, B.bad, B.ints, B.meanit, B.ints + 1, st))) return rc;
@@ -1052,7 +1053,7 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   for (int a = 0; a < p->n_admm; ++a) {
     ALDIC_CUDA(cudaMemcpyAsync(B.U2old, B.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
     if ((rc = subpb1(im, B.coords, n, B.U2, B.F2, B.vdual, B.H21, nullptr, p->winsize, mu, p->tol,
-                     p->precision, B.U1, B.itb, c->queue.as<unsigned int>(), st)))
+                     p->precision, B.U1, B.itb, c->queue.as<unsigned int>(), st, B.cache)))
       return rc;
     if ((rc = gridfit_load(c->gw, M, N, 2, B.U1, 2, B.itb, st))) return rc;
     if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, 2, 0, 0, 1, lam2, kRtolFit, kMaxitFit, st))) return rc;
@@ -1109,7 +1110,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   const long long ny_nx = n;
   const size_t need = 256 * 40 + sizeof(double) * (5 * ny_nx + 2 * n + 2 * n + 2 * n + 2 * n + 4 * n +
                                                    21 * n + 2 * n + 4 * n + 4 * n + 2 * n + 2 * n +
-                                                   2 * n + 64 + 1024) +
+                                                   2 * n + 8 * n + 64 + 1024) +
                       sizeof(int) * (2 * n + 16) + n + 256;
   bool realloc = c->fr.cap < need;
   if ((rc = c->fr.ensure(need))) return rc;
@@ -1122,6 +1123,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   B.H21 = carve<double>(q, 21 * n); B.U2 = carve<double>(q, 2 * n); B.F2 = carve<double>(q, 4 * n);
   B.udual = carve<double>(q, 4 * n); B.vdual = carve<double>(q, 2 * n);
   B.U2old = carve<double>(q, 2 * n); B.U1old = carve<double>(q, 2 * n);
+  B.cache = carve<double>(q, 8 * n);
   B.err = carve<double>(q, 16); B.beta = carve<double>(q, 4); B.upd = carve<double>(q, 32);
   B.part = carve<double>(q, 1024); B.meanit = carve<double>(q, 4);
   B.it1 = carve<int>(q, n); B.itb = carve<int>(q, n); B.ints = carve<int>(q, 16);

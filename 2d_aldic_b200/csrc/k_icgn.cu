@@ -41,6 +41,9 @@ struct Args {
   double *U, *F, *H21out;
   int *iters;
   unsigned int *queue;
+  // per-subset setup constants (IC-GN writes, Subpb1 reads; may be null):
+  // [mean f, bf, S_f5, S_f6, S_5, S_6, w after growth, status 0/102/-1]
+  double *cache;
 };
 
 __device__ __forceinline__ double nan64() { return __longlong_as_double(0x7ff8000000000000ll); }
@@ -144,6 +147,7 @@ __device__ __forceinline__ Real sample(const Real *__restrict__ img, int W, int 
 template <bool SUB>
 __device__ __forceinline__ void fail_minus1(const Args &a, long long s, int lane) {
   if (lane == 0) {
+    if (!SUB && a.cache) a.cache[8 * s + 7] = -1.0;
     a.iters[s] = -1;
     a.U[2 * s] = nan64();
     a.U[2 * s + 1] = nan64();
@@ -158,6 +162,7 @@ __device__ __forceinline__ void fail_minus1(const Args &a, long long s, int lane
 template <bool SUB>
 __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
   if (lane == 0) {
+    if (!SUB && a.cache) a.cache[8 * s + 7] = 102.0;
     a.iters[s] = 102;
     a.U[2 * s] = a.U0[2 * s];
     a.U[2 * s + 1] = a.U0[2 * s + 1];
@@ -179,6 +184,21 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   const double x0 = a.coords[s], y0 = a.coords[a.n + s];
   int w = a.wins ? a.wins[s] : a.w;
   int xl, yl;
+  const bool cached = SUB && a.cache;
+  if (cached) {
+    // the IC-GN launch of this frame already ran the setup on the same
+    // reference image and window
+    const double stc = a.cache[8 * s + 7];
+    if (stc == -1.0) {
+      fail_minus1<SUB>(a, s, lane);
+      return;
+    }
+    if (stc == 102.0) {
+      done_102<SUB>(a, s, lane);
+      return;
+    }
+    w = (int)a.cache[8 * s + 6];
+  }
   bool ok = subset_ok(im, x0, y0, w, &xl, &yl);
   if (!ok) {
     fail_minus1<SUB>(a, s, lane);
@@ -196,7 +216,26 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   // subset grows (funICGN.m:57-65) and the pass runs again on the new window.
   int nw, npx, base;
   Real ox, oy;
-  double oxd, oyd, c0, A1, A2;
+  double oxd, oyd, c0 = 0, A1 = 0, A2 = 0;
+  double meanf, ssf;
+  if (cached) {
+    nw = w + 1;
+    npx = nw * nw;
+    oxd = (double)xl - x0;
+    oyd = (double)yl - y0;
+    ox = (Real)oxd;
+    oy = (Real)oyd;
+    base = (yl - 1) * W + (xl - 1);
+    meanf = a.cache[8 * s + 0];
+    const double bfc = a.cache[8 * s + 1];
+    ssf = bfc * bfc;
+    if (lane == 0) {
+      Sfs[4] = a.cache[8 * s + 2];
+      Sfs[5] = a.cache[8 * s + 3];
+      Sks[4] = a.cache[8 * s + 4];
+      Sks[5] = a.cache[8 * s + 5];
+    }
+  } else {
   for (int attempt = 0;; ++attempt) {
     nw = w + 1;
     npx = nw * nw;
@@ -286,12 +325,24 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     break;
   }
   const double dmc = A1 / (double)npx;  // mean(f) - c
-  const double meanf = c0 + dmc;
-  const double ssf = A2 - A1 * dmc;      // sum (f - mean f)^2
+  meanf = c0 + dmc;
+  ssf = A2 - A1 * dmc;                  // sum (f - mean f)^2
   if (lane == 0) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) Sfs[q] -= dmc * Sks[q];  // sum sd_k (f - mean f)
+    if (!SUB && a.cache) {
+      double *cc = a.cache + 8 * s;
+      cc[0] = meanf;
+      cc[1] = sqrt(ssf);
+      cc[2] = Sfs[4];
+      cc[3] = Sfs[5];
+      cc[4] = Sks[4];
+      cc[5] = Sks[5];
+      cc[6] = (double)w;
+      cc[7] = 0.0;
+    }
   }
+  }  // setup pass
   double P[6];
   if (SUB) {
     for (int q = 0; q < 4; ++q) P[q] = a.FOld[4 * s + q];
@@ -367,15 +418,17 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       Real s1 = 0, s2r = 0, t[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) t[q] = 0;
+      // pixel offsets X, Y and the image index k advance incrementally
       int iy = lane / nw, ix = lane - (lane / nw) * nw;
+      Real X = ox + (Real)ix, Y = oy + (Real)iy;
+      int k = base + iy * W + ix;
+      const Real c4 = p4 + fx0, c5 = p5 + fy0;
       for (int p = lane; p < npx; p += 32) {
-        const Real X = ox + (Real)ix, Y = oy + (Real)iy;
-        const Real ru = a11 * X + a12 * Y + p4 + fx0;
-        const Real rv = a21 * X + a22 * Y + p5 + fy0;
+        const Real ru = a11 * X + (a12 * Y + c4);
+        const Real rv = a21 * X + (a22 * Y + c5);
         const Real fu = floor(ru), fv = floor(rv);
         const int cx = xb + (int)fu - 1, cy = yb + (int)fv - 1;  // 0-based floor corner
         const Real gval = sample<Real>(gI, W, cx, cy, ru - fu, rv - fv);
-        const int k = base + iy * W + ix;
         const Real d = gval - cg;
         s1 += d;
         s2r += d * d;
@@ -390,9 +443,13 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
           t[3] += ay * Y;
         }
         ix += 32;
+        X += (Real)32;
+        k += 32;
         while (ix >= nw) {
           ix -= nw;
-          iy++;
+          X -= (Real)nw;
+          Y += (Real)1;
+          k += W - nw;
         }
       }
       sums[0] = warp_sum((double)s1);
@@ -498,9 +555,10 @@ int launch(const Args &a, cudaStream_t st) {
 
 int icgn(const IcgnImages &im, const double *coords, long long n, const double *U0,
          const int *wins, int w, double tol, int precision, double *U, double *F, int *iters,
-         double *H21, unsigned int *queue, cudaStream_t st) {
+         double *H21, unsigned int *queue, cudaStream_t st, double *cache) {
   if (n <= 0) return OK;
   Args a{};
+  a.cache = cache;
   a.im = im; a.coords = coords; a.n = n; a.U0 = U0; a.wins = wins; a.w = w; a.tol = tol;
   a.U = U; a.F = F; a.H21out = H21; a.iters = iters; a.queue = queue;
   return precision ? launch<double, false>(a, st) : launch<float, false>(a, st);
@@ -509,9 +567,10 @@ int icgn(const IcgnImages &im, const double *coords, long long n, const double *
 int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,
            const double *FOld, const double *vdual, const double *H21, const int *wins, int w,
            double mu, double tol, int precision, double *U, int *iters, unsigned int *queue,
-           cudaStream_t st) {
+           cudaStream_t st, const double *cache) {
   if (n <= 0) return OK;
   Args a{};
+  a.cache = const_cast<double *>(cache);
   a.im = im; a.coords = coords; a.n = n; a.U0 = UOld; a.FOld = FOld; a.vdual = vdual;
   a.H21in = H21; a.wins = wins; a.w = w; a.mu = mu; a.tol = tol; a.U = U; a.iters = iters;
   a.queue = queue;

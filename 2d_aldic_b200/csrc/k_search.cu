@@ -562,21 +562,30 @@ __global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f
     for (int ty = 0; ty < G.tw; ++ty) {
       const unsigned *trow = Tq + ty * L.tw4;
       const unsigned *dr = Dw + (b + ty) * L.dqw + wbase;
+      // windows of the word pair (w0, w1) shifted by 1..3 bytes; each step
+      // computes the shifts of (w1, w2) once and hands them to the next step
       unsigned w0 = dr[0], w1 = dr[1];
+      unsigned s1 = __funnelshift_r(w0, w1, 8), s2 = __funnelshift_r(w0, w1, 16),
+               s3 = __funnelshift_r(w0, w1, 24);
 #pragma unroll 3
       for (int jw = 0; jw < L.tw4; ++jw) {
         const unsigned t = trow[jw];
         const unsigned w2 = dr[jw + 2];
+        const unsigned n1 = __funnelshift_r(w1, w2, 8), n2 = __funnelshift_r(w1, w2, 16),
+                       n3 = __funnelshift_r(w1, w2, 24);
         acc[0] = __dp4a(t, w0, acc[0]);
-        acc[1] = __dp4a(t, __funnelshift_r(w0, w1, 8), acc[1]);
-        acc[2] = __dp4a(t, __funnelshift_r(w0, w1, 16), acc[2]);
-        acc[3] = __dp4a(t, __funnelshift_r(w0, w1, 24), acc[3]);
+        acc[1] = __dp4a(t, s1, acc[1]);
+        acc[2] = __dp4a(t, s2, acc[2]);
+        acc[3] = __dp4a(t, s3, acc[3]);
         acc[4] = __dp4a(t, w1, acc[4]);
-        acc[5] = __dp4a(t, __funnelshift_r(w1, w2, 8), acc[5]);
-        acc[6] = __dp4a(t, __funnelshift_r(w1, w2, 16), acc[6]);
-        acc[7] = __dp4a(t, __funnelshift_r(w1, w2, 24), acc[7]);
+        acc[5] = __dp4a(t, n1, acc[5]);
+        acc[6] = __dp4a(t, n2, acc[6]);
+        acc[7] = __dp4a(t, n3, acc[7]);
         w0 = w1;
         w1 = w2;
+        s1 = n1;
+        s2 = n2;
+        s3 = n3;
       }
     }
     const bool ring_b = (b == 0 || b == G.cc - 1);
@@ -585,12 +594,20 @@ __global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f
       const int a = a0 + k;
       if (a >= G.cr) break;
       const long long sd = CS[b * G.cr + a], sd2 = CS2[b * G.cr + a];
+      // Only the outermost ring of the cropped map overhangs the region, by
+      // one template column (a = 0: column 0; a = cr-1: column tw-1) and/or
+      // one template row (b = 0 / cc-1), so the padded part is O(1).
       int st_out = 0;
       long long n_out = 0;
-      // only the outermost ring of the cropped map overhangs the region
-      if (ring_b || a == 0 || a == G.cr - 1)
-        pad_terms<int>(G, a, b, colsum_s, rowsum_s,
-                       [&](int ty, int tx) { return (int)Tb[ty * G.tw + tx]; }, &st_out, &n_out);
+      if (ring_b || a == 0 || a == G.cr - 1) {
+        const int oc = a == 0 ? 0 : (a == G.cr - 1 ? G.tw - 1 : -1);
+        const int orow = b == 0 ? 0 : (b == G.cc - 1 ? G.tw - 1 : -1);
+        if (oc >= 0) st_out += colsum_s[oc];
+        if (orow >= 0) st_out += rowsum_s[orow];
+        if (oc >= 0 && orow >= 0) st_out -= Tb[orow * G.tw + oc];
+        const long long nco = oc >= 0, nro = orow >= 0;
+        n_out = nco * G.tw + nro * G.tw - nco * nro;
+      }
       map[b * G.cr + a] = ncc_combine(mn, st, st2, (long long)acc[k], sd, sd2, st_out, n_out, mu);
     }
   }

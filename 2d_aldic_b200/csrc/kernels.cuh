@@ -33,11 +33,11 @@ struct IcgnImages {
 };
 int icgn(const IcgnImages &im, const double *coords, long long n, const double *U0,
          const int *wins, int w, double tol, int precision, double *U, double *F, int *iters,
-         double *H21, unsigned int *queue, cudaStream_t st);
+         double *H21, unsigned int *queue, cudaStream_t st, double *cache = nullptr);
 int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,
            const double *FOld, const double *vdual, const double *H21, const int *wins, int w,
            double mu, double tol, int precision, double *U, int *iters, unsigned int *queue,
-           cudaStream_t st);
+           cudaStream_t st, const double *cache = nullptr);
 
 // ---- k_grid.cu: node-grid solvers and field kernels on the M x N mesh
 struct GridWork {
