@@ -5,14 +5,16 @@ this host package mirroring the reference MATLAB functions by name.
 The package directory is ``2d_aldic_b200``; import it with
 ``importlib.import_module("2d_aldic_b200")``.
 """
-from .api import (ALDIC, FP32, FP64, Context, IntegerSearch, Init, LocalICGN, MeshSetUp, Subpb1,
+from .api import (ALDIC, FP32, FP64, INIT_EXTRAP, INIT_GIVEN, INIT_PREV, INIT_SEARCH, INIT_ZERO,
+                  ALDICSequence, Context, IntegerSearch, Init, LocalICGN, MeshSetUp, Subpb1,
                   Subpb2, ba_interp2, default_context, funGlobal_NodalStrainAvg, funICGN,
                   funICGN_Subpb1, funImgGradient, funIntegerSearch, funNormalizeImg,
                   funSmoothDisp, funSmoothStrain, gridfit_springs, inpaint_nans, local_icgn)
 from ._lib import AldicError, exported_symbols
 from . import synth
 
-__all__ = ["ALDIC", "FP32", "FP64", "Context", "IntegerSearch", "Init", "LocalICGN", "MeshSetUp",
+__all__ = ["ALDIC", "ALDICSequence", "FP32", "FP64", "INIT_SEARCH", "INIT_PREV", "INIT_ZERO",
+           "INIT_EXTRAP", "INIT_GIVEN", "Context", "IntegerSearch", "Init", "LocalICGN", "MeshSetUp",
            "Subpb1", "Subpb2", "ba_interp2", "default_context", "funGlobal_NodalStrainAvg",
            "funICGN", "funICGN_Subpb1", "funImgGradient", "funIntegerSearch", "funNormalizeImg",
            "funSmoothDisp", "funSmoothStrain", "gridfit_springs", "inpaint_nans", "local_icgn",

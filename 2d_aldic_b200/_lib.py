@@ -44,13 +44,15 @@ _SIGS = {
     "aldic_smooth": ([P, I32, I32, I32, P], I32),
     "aldic_frame_dims": ([P, P, P, P], I32),
     "aldic_frame": ([P, P, P, P, P, P, P, P], I32),
+    "aldic_set_init": ([P, P, I64], I32),
 }
 
 
 class FrameParams(C.Structure):
     _fields_ = [("winsize", I32), ("step", I32), ("search", I32 * 2), ("gridx", I32 * 2),
                 ("gridy", I32 * 2), ("tol", D), ("mu", D), ("beta", D), ("n_admm", I32),
-                ("tol2", D), ("precision", I32), ("smooth", I32), ("use_graph", I32)]
+                ("tol2", D), ("precision", I32), ("smooth", I32), ("use_graph", I32),
+                ("init", I32)]
 
 
 class FrameStats(C.Structure):

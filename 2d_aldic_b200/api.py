@@ -32,6 +32,8 @@ except Exception:  # pragma: no cover
 
 U8, U16, F32, F64 = 0, 1, 2, 3
 FP32, FP64 = 0, 1
+# initial guess of a frame (ALDIC_INIT_* of the C ABI)
+INIT_SEARCH, INIT_PREV, INIT_ZERO, INIT_EXTRAP, INIT_GIVEN = 0, 1, 2, 3, 4
 _DT = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.float32): F32,
        np.dtype(np.float64): F64}
 
@@ -578,9 +580,18 @@ class ALDIC:
         call("aldic_frame_dims", self.ctx.h, C.byref(self.p), C.byref(M), C.byref(N))
         return M.value, N.value
 
-    def frame(self, out: dict | None = None, stats: bool = True, device_out: bool = False):
+    def set_init(self, U0):
+        """U0 (2n, interleaved) for frame(init=INIT_GIVEN)."""
+        a = _contig(U0) if _is_cuda(U0) else np.ascontiguousarray(U0, np.float64)
+        call("aldic_set_init", self.ctx.h, _ptr(a), int(a.numel() if _is_cuda(a) else a.size))
+
+    def frame(self, out: dict | None = None, stats: bool = True, device_out: bool = False,
+              init: int = INIT_SEARCH):
         """Run one frame.  With out (dict of preallocated arrays x0, y0, U, F,
-        iters -- numpy or CUDA tensors) the results are written there."""
+        iters -- numpy or CUDA tensors) the results are written there.  init
+        selects the initial guess (INIT_SEARCH, or a sequence mode: INIT_PREV,
+        INIT_ZERO, INIT_EXTRAP, INIT_GIVEN)."""
+        self.p.init = int(init)
         M, N = self.dims()
         n = M * N
         if out is None:
@@ -611,3 +622,79 @@ class ALDIC:
                                                     "section5", "admm", "frame"),
                                                    list(st.t_stage_ms)[:7]))}
         return res
+
+
+class ALDICSequence:
+    """The frame loop of main_ALDIC.m:53-147 over an image sequence, with
+    every image and all state on the device.
+
+        seq = ALDICSequence(inc_unit=10, winsize=32, step=16, search=24)
+        for res in seq.run(frames):      # frames[0] is the first reference
+            ...
+
+    Per frame ImgSeqNum = 2, 3, ... (1-based like the reference):
+      * ImgSeqNum < 2 + n_search (the reference: < 7): integer search
+        (NewFFTSearch = 1, main_ALDIC.m:69-75);
+      * else, when mod(ImgSeqNum - 2, inc_unit) == 0 (incremental mode): the
+        previous frame becomes the reference and U0 = 0 (main_ALDIC.m:118-126);
+      * else U0 from earlier results: the previous U for the first frame after
+        a reference change (main_ALDIC.m:130-131), later a constant-rate
+        extrapolation from the last two frames solved against the same
+        reference, standing in for the POD-GPR prediction of
+        main_ALDIC.m:133-146 (predictor="previous" keeps the previous U).
+    inc_unit=None is the accumulative mode (the reference never changes).
+    Each yielded dict holds the frame's U, F, iters (CUDA tensors), its
+    init mode, whether the reference was updated, and the device latency of
+    the frame in ms (CUDA events around set_def + frame on the context
+    stream)."""
+
+    def __init__(self, inc_unit: int | None = None, n_search: int = 5, predictor: str = "extrap",
+                 roi=None, mask=None, **frame_kw):
+        if predictor not in ("extrap", "previous"):
+            raise ValueError("predictor must be 'extrap' or 'previous'")
+        self.al = ALDIC(**frame_kw)
+        self.inc_unit = inc_unit
+        self.n_search = max(1, int(n_search))
+        self.predictor = predictor
+        self.roi, self.mask = roi, mask
+
+    def plan(self, n_frames: int):
+        """(ImgSeqNum, init mode, reference frame index (0-based), update)
+        for every deformed frame of an n_frames sequence."""
+        out, ref, same = [], 0, 0
+        for s in range(2, n_frames + 1):
+            upd = False
+            if s < 2 + self.n_search:
+                mode = INIT_SEARCH
+            elif self.inc_unit and (s - 2) % self.inc_unit == 0:
+                ref, upd, mode, same = s - 2, True, INIT_ZERO, 0
+            elif self.predictor == "extrap" and same >= 2:
+                mode = INIT_EXTRAP
+            else:
+                mode = INIT_PREV
+            out.append((s, mode, ref, upd))
+            same += 1
+        return out
+
+    def run(self, frames, stream=None):
+        if torch is None or not torch.cuda.is_available():
+            raise AldicError("ALDICSequence.run", -3, "a CUDA device is required")
+        dev = torch.device("cuda", self.al.ctx.device)
+        stream = stream or torch.cuda.Stream(dev)
+        self.al.ctx.set_stream(stream)
+        self.al.set_images(frames[0], roi=self.roi, mask=self.mask)
+        for s, mode, ref, upd in self.plan(len(frames)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                if upd:
+                    self.al.set_images(frames[ref], roi=self.roi, mask=self.mask)
+                self.al.ctx.set_def(frames[s - 1])
+                res = self.al.frame(device_out=True, init=mode, stats=False)
+                e1.record(stream)
+            e1.synchronize()
+            res.update(img_seq_num=s, init=mode, ref_index=ref, ref_updated=upd,
+                       latency_ms=e0.elapsed_time(e1))
+            yield res
+

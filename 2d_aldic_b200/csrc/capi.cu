@@ -3,6 +3,7 @@
 // captured frame pipeline of main_ALDIC.m Sections 3-6.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -112,11 +113,27 @@ struct aldic_ctx {
   // frame state
   DevBuf fr;  // one slab for all frame arrays
   long long fr_n = 0;
-  cudaGraphExec_t graph = nullptr;
-  int graph_kernels = -1;
+  // captured frame graphs, most recently used last (a sequence alternates
+  // between a few initial-guess modes, each its own graph)
+  struct FrameGraph {
+    std::string key;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = -1;
+  };
+  std::vector<FrameGraph> graphs;
   cudaEvent_t ev[8] = {};   // frame stage marks
-  std::string graph_key;
+  // sequence state: final U of the last two frames and the given U0
+  // (3 x 2n doubles: [U(k-1) | U(k-2) | given])
+  DevBuf hist;
+  long long hist_n = 0;
+  int hist_count = 0;
+  bool have_given = false;
   bool graph_failed = false;
+  void drop_graphs() {
+    for (auto &g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
 };
 
 namespace {
@@ -371,12 +388,13 @@ int aldic_ctx_destroy(aldic_ctx *c) {
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->drop_graphs();
   for (int k = 0; k < 8; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   DevBuf *bufs[] = {&c->f_raw, &c->g_raw, &c->f64, &c->g64, &c->f32, &c->g32, &c->gx64,
                     &c->gy64, &c->gx32, &c->gy32, &c->mask, &c->stats, &c->isums, &c->part,
-                    &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr};
+                    &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr,
+                    &c->hist};
   for (DevBuf *b : bufs) b->release();
   c->arena.release();
   if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -392,10 +410,7 @@ int aldic_ctx_set_stream(aldic_ctx *c, void *stream) {
   if (c->own_stream) cudaStreamDestroy(c->stream);
   c->stream = (cudaStream_t)stream;
   c->own_stream = false;
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  c->drop_graphs();
   return OK;
 }
 
@@ -893,6 +908,34 @@ __global__ void k_mesh_init(int M, int N, const double *sx, const double *sy, co
   }
 }
 
+// MeshSetUp node grid without a search: node (i, j) at XList(i) + w/2,
+// YList(j) + w/2 (funIntegerSearch.m:158-159)
+__global__ void k_mesh_grid(int M, int N, int gx1, int gy1, int step, double hw, double *coords,
+                            double *x0, double *y0) {
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    const double x = gx1 + (double)i * step + hw, y = gy1 + (double)j * step + hw;
+    coords[k] = x;
+    coords[n + k] = y;
+    x0[k] = x;
+    y0[k] = y;
+  }
+}
+
+// U0 of the sequence modes from the history [U(k-1) | U(k-2) | given]
+__global__ void k_init_hist(int mode, long long n2, const double *hist, double *U0) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+       k += (long long)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (mode == ALDIC_INIT_PREV) v = hist[k];
+    else if (mode == ALDIC_INIT_EXTRAP) v = 2.0 * hist[k] - hist[n2 + k];
+    else if (mode == ALDIC_INIT_GIVEN) v = hist[2 * n2 + k];
+    U0[k] = v;
+  }
+}
+
 __global__ void k_zero(double *a, long long n) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x)
@@ -947,12 +990,13 @@ T *carve(char *&p, long long count) {
   return r;
 }
 
-int frame_geometry(aldic_ctx *c, const aldic_frame_params *p, int gx[2], int gy[2], int *M, int *N) {
+int frame_geometry(aldic_ctx *c, const aldic_frame_params *p, int gx[2], int gy[2], int *M, int *N,
+                   int *gx1 = nullptr, int *gy1 = nullptr) {
   gx[0] = p->gridx[0]; gx[1] = p->gridx[1];
   gy[0] = p->gridy[0]; gy[1] = p->gridy[1];
   if (gx[0] == 0 && gx[1] == 0) { gx[0] = 1; gx[1] = c->W; }
   if (gy[0] == 0 && gy[1] == 0) { gy[0] = 1; gy[1] = c->H; }
-  int rc = search_dims(c->W, c->H, gx, gy, p->winsize, p->step, p->search, M, N, nullptr, nullptr);
+  int rc = search_dims(c->W, c->H, gx, gy, p->winsize, p->step, p->search, M, N, gx1, gy1);
   if (rc) {
     set_error("frame: winsize, step and search must be positive");
     return rc;
@@ -976,7 +1020,7 @@ int mark(aldic_ctx *c, int k) {
 }
 
 int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, int M, int N,
-                 const int gx[2], const int gy[2]) {
+                 const int gx[2], const int gy[2], int gx1, int gy1) {
   cudaStream_t st = c->stream;
   int rcm;
   if ((rcm = mark(c, 0))) return rcm;
@@ -989,15 +1033,23 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   // Section 2: normalise the deformed image (the reference's was done once)
   if (!c->prepared && (rc = prep_def(c))) return rc;
   if ((rc = mark(c, 1))) return rc;
-  // Section 3: integer search, MeshSetUp, Init (inpaint_nans of u, v)
-  if ((rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H, c->stats.as<double>() + 2, gx,
-                       gy, p->winsize, p->step, p->search, B.sx, B.sy, B.su, B.sv, B.scc, nullptr,
-                       nullptr, st)))
-    return rc;
-  k_mesh_init<<<nb, 256, 0, st>>>(M, N, B.sx, B.sy, B.su, B.sv, B.coords, B.x0, B.y0, B.U0);
-  if ((rc = inpaint_load(c->gw, M, N, 2, B.U0, 2, nullptr, st, 0))) return rc;
-  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 2, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st))) return rc;
-  if ((rc = inpaint_store(c->gw, M, N, 2, B.U0, 2, st, 0))) return rc;
+  double *hist = c->hist.as<double>();
+  if (p->init == ALDIC_INIT_SEARCH) {
+    // Section 3: integer search, MeshSetUp, Init (inpaint_nans of u, v)
+    if ((rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H, c->stats.as<double>() + 2,
+                         gx, gy, p->winsize, p->step, p->search, B.sx, B.sy, B.su, B.sv, B.scc,
+                         nullptr, nullptr, st)))
+      return rc;
+    k_mesh_init<<<nb, 256, 0, st>>>(M, N, B.sx, B.sy, B.su, B.sv, B.coords, B.x0, B.y0, B.U0);
+    if ((rc = inpaint_load(c->gw, M, N, 2, B.U0, 2, nullptr, st, 0))) return rc;
+    if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 2, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st)))
+      return rc;
+    if ((rc = inpaint_store(c->gw, M, N, 2, B.U0, 2, st, 0))) return rc;
+  } else {
+    // Section 3 of a later frame: the same mesh, U0 from the previous results
+    k_mesh_grid<<<nb, 256, 0, st>>>(M, N, gx1, gy1, p->step, 0.5 * p->winsize, B.coords, B.x0, B.y0);
+    k_init_hist<<<nb, 256, 0, st>>>(p->init, 2 * n, hist, B.U0);
+  }
   // Section 4: LocalICGN + post-processing
   if ((rc = mark(c, 2))) return rc;
   const IcgnImages im = images_of(c);
@@ -1078,6 +1130,9 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     if ((rc = vsub(B.F2, B.F1, B.udual, 4 * n, st))) return rc;
     if ((rc = vsub(B.U2, B.U1, B.vdual, 2 * n, st))) return rc;
   }
+  // sequence history: U(k-2) <- U(k-1) <- this frame's U
+  ALDIC_CUDA(cudaMemcpyAsync(hist + 2 * n, hist, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+  ALDIC_CUDA(cudaMemcpyAsync(hist, B.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
   if ((rc = mark(c, 6))) return rc;
   ALDIC_CUDA(cudaGetLastError());
   return OK;
@@ -1093,6 +1148,22 @@ int aldic_frame_dims(aldic_ctx *c, const aldic_frame_params *p, int *M, int *N) 
   return frame_geometry(c, p, gx, gy, M, N);
 }
 
+int aldic_set_init(aldic_ctx *c, const double *U0, long long n2) {
+  ALDIC_CHECK(c && U0 && n2 > 0 && n2 % 2 == 0, E_ARG, "set_init: bad arguments");
+  Guard g(c);
+  const long long n = n2 / 2;
+  int rc;
+  if (c->hist_n != n) {
+    if ((rc = c->hist.ensure(sizeof(double) * 6 * n))) return rc;
+    c->hist_n = n;
+    c->hist_count = 0;
+  }
+  ALDIC_CUDA(cudaMemcpyAsync(c->hist.as<double>() + 4 * n, U0, sizeof(double) * n2, cudaMemcpyDefault,
+                             c->stream));
+  c->have_given = true;
+  return finish(c, !is_device_ptr(U0));
+}
+
 int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y0, double *U,
                 double *F, int32_t *iters, aldic_frame_stats *stats) {
   ALDIC_CHECK(c && p, E_ARG, "frame: null argument");
@@ -1100,11 +1171,25 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   ALDIC_CHECK(p->n_admm >= 0 && p->n_admm <= 64, E_ARG, "frame: n_admm must be in [0, 64]");
   ALDIC_CHECK(p->tol > 0 && p->mu > 0, E_ARG, "frame: tol and mu must be positive");
   ALDIC_CHECK(p->tol2 <= 0, E_ARG, "frame: the tol2 early stop is not supported on this path; pass tol2 <= 0 and read update_y");
+  ALDIC_CHECK(p->init >= ALDIC_INIT_SEARCH && p->init <= ALDIC_INIT_GIVEN, E_ARG,
+              "frame: init must be one of ALDIC_INIT_SEARCH/PREV/ZERO/EXTRAP/GIVEN");
   Guard g(c);
-  int gx[2], gy[2], M, N;
-  int rc = frame_geometry(c, p, gx, gy, &M, &N);
+  int gx[2], gy[2], M, N, gx1, gy1;
+  int rc = frame_geometry(c, p, gx, gy, &M, &N, &gx1, &gy1);
   if (rc) return rc;
   const long long n = (long long)M * N;
+  if (c->hist_n != n) {
+    if ((rc = c->hist.ensure(sizeof(double) * 6 * n))) return rc;
+    c->hist_n = n;
+    c->hist_count = 0;
+    c->have_given = false;
+  }
+  ALDIC_CHECK(p->init != ALDIC_INIT_PREV || c->hist_count >= 1, E_STATE,
+              "frame: ALDIC_INIT_PREV needs a previous frame on this node grid");
+  ALDIC_CHECK(p->init != ALDIC_INIT_EXTRAP || c->hist_count >= 2, E_STATE,
+              "frame: ALDIC_INIT_EXTRAP needs two previous frames on this node grid");
+  ALDIC_CHECK(p->init != ALDIC_INIT_GIVEN || c->have_given, E_STATE,
+              "frame: ALDIC_INIT_GIVEN needs aldic_set_init on this node grid");
   if ((rc = ensure_grid_work(c, n))) return rc;
   // frame slab
   const long long ny_nx = n;
@@ -1128,25 +1213,38 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   B.part = carve<double>(q, 1024); B.meanit = carve<double>(q, 4);
   B.it1 = carve<int>(q, n); B.itb = carve<int>(q, n); B.ints = carve<int>(q, 16);
   B.bad = carve<unsigned char>(q, n);
-  // graph key: geometry and every parameter that changes the recorded work
+  // graph key: geometry, every parameter that changes the recorded work and
+  // the buffers the graph addresses
   char key[512];
-  snprintf(key, sizeof key, "%d %d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %.17g %d %d %d|%p %p %p",
-           c->W, c->H, c->dtype, (int)realloc, p->winsize, p->step, p->search[0], p->search[1],
-           gx[0], gx[1], gy[0], gy[1], p->tol, p->mu, p->beta, p->n_admm, p->precision, p->smooth,
-           c->fr.p, c->gw_vec.p, c->g_raw.p);
+  snprintf(key, sizeof key, "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p",
+           c->W, c->H, c->dtype, p->winsize, p->step, p->search[0], p->search[1], gx[0], gx[1],
+           gy[0], gy[1], p->tol, p->mu, p->beta, p->n_admm, p->precision, p->smooth, p->init,
+           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p);
+  if (realloc) c->drop_graphs();  // recorded against buffers that are gone
   const bool want_graph = p->use_graph && !c->graph_failed;
-  if (want_graph && c->graph && c->graph_key != key) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
+  aldic_ctx::FrameGraph *fg = nullptr;
+  if (want_graph) {
+    for (size_t k = 0; k < c->graphs.size(); ++k)
+      if (c->graphs[k].key == key) {
+        std::rotate(c->graphs.begin() + k, c->graphs.begin() + k + 1, c->graphs.end());
+        fg = &c->graphs.back();
+        break;
+      }
   }
-  if (want_graph && !c->graph) {
+  if (want_graph && !fg) {
+    constexpr size_t kMaxGraphs = 8;
+    if (c->graphs.size() >= kMaxGraphs) {
+      cudaGraphExecDestroy(c->graphs.front().exec);
+      c->graphs.erase(c->graphs.begin());
+    }
+    aldic_ctx::FrameGraph rec;
     cudaGraph_t gr = nullptr;
     bool okc = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (okc) {
-      int rc2 = frame_device(c, p, B, M, N, gx, gy);
+      int rc2 = frame_device(c, p, B, M, N, gx, gy, gx1, gy1);
       cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
       okc = rc2 == OK && e == cudaSuccess && gr;
-      if (okc) okc = cudaGraphInstantiate(&c->graph, gr, 0) == cudaSuccess;
+      if (okc) okc = cudaGraphInstantiate(&rec.exec, gr, 0) == cudaSuccess;
       if (okc) {
         size_t nn = 0;
         cudaGraphGetNodes(gr, nullptr, &nn);
@@ -1157,23 +1255,26 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
           cudaGraphNodeType t;
           if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kn++;
         }
-        c->graph_kernels = kn;
+        rec.kernels = kn;
       }
       if (gr) cudaGraphDestroy(gr);
     }
     cudaGetLastError();
     if (!okc) {
-      c->graph = nullptr;
+      if (rec.exec) cudaGraphExecDestroy(rec.exec);
       c->graph_failed = true;  // fall back to direct launches from now on
     } else {
-      c->graph_key = key;
+      rec.key = key;
+      c->graphs.push_back(rec);
+      fg = &c->graphs.back();
     }
   }
-  if (c->graph && want_graph) {
-    ALDIC_CUDA(cudaGraphLaunch(c->graph, c->stream));
+  if (fg) {
+    ALDIC_CUDA(cudaGraphLaunch(fg->exec, c->stream));
   } else {
-    if ((rc = frame_device(c, p, B, M, N, gx, gy))) return rc;
+    if ((rc = frame_device(c, p, B, M, N, gx, gy, gx1, gy1))) return rc;
   }
+  if (c->hist_count < 2) c->hist_count++;
   // outputs
   Arg<double> ax, ay, au, af;
   Arg<int32_t> ai;
@@ -1208,7 +1309,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     stats->converged_icgn = hs.ints[1];
     stats->beta = hs.beta;
     stats->mean_iters_icgn = hs.meanit;
-    stats->kernel_launches = (c->graph && want_graph) ? c->graph_kernels : -1;
+    stats->kernel_launches = fg ? fg->kernels : -1;
     stats->max_pcg_iters = hs.pcg_its;
     for (int k = 0; k < 6; ++k) {
       float ms = 0.f;

@@ -165,6 +165,169 @@ WORKLOADS = {
 }
 
 
+# ------------------------------------------------------ sequences (torch)
+# The 16-bit sequence is generated with torch (on the GPU when one is given)
+# from the same recipe: 50 frames of 4096^2 take seconds there instead of
+# minutes in numpy.
+
+def speckle_t(W: int, H: int, ndots: int, seed: int, device="cpu", bg: float = 20.0,
+              amp=(80.0, 200.0), radius=(2.0, 4.0), scale: float = 1.0):
+    """speckle() with the same draws, accumulated with torch; float64 (H, W)
+    before quantisation."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cx = rng.uniform(0, W, ndots)
+    cy = rng.uniform(0, H, ndots)
+    r = rng.uniform(radius[0], radius[1], ndots)
+    A = rng.uniform(amp[0], amp[1], ndots)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device=device)
+    cx, cy, r, A = t(cx), t(cy), t(r), t(A)
+    img = torch.zeros(H * W, dtype=torch.float64, device=device)
+    R = 12
+    off = torch.arange(-R, R + 1, device=device, dtype=torch.float64)
+    chunk = 8192
+    for s0 in range(0, ndots, chunk):
+        e = min(ndots, s0 + chunk)
+        px = torch.floor(cx[s0:e])[:, None, None] + off[None, None, :]
+        py = torch.floor(cy[s0:e])[:, None, None] + off[None, :, None]
+        d2 = (px - cx[s0:e, None, None]) ** 2 + (py - cy[s0:e, None, None]) ** 2
+        val = A[s0:e, None, None] * torch.exp(-d2 / (r[s0:e, None, None] ** 2))
+        ok = (px >= 0) & (px < W) & (py >= 0) & (py < H)
+        idx = (py * W + px).expand_as(val)[ok].long()
+        img.index_add_(0, idx, val[ok])
+    return (img.reshape(H, W) + bg) * scale
+
+
+def quantise_t(img, dtype):
+    import torch
+    info = np.iinfo(dtype)
+    tdt = {np.uint8: torch.uint8, np.uint16: torch.uint16}[dtype]
+    return torch.clamp(torch.round(img), info.min, info.max).to(torch.int32).to(tdt)
+
+
+def bicubic_sample_t(img, x, y):
+    """bicubic_sample() in torch (float64, 1-based coordinates)."""
+    import torch
+    H, W = img.shape
+    im = img.to(torch.float64).reshape(-1)
+    xf, yf = torch.floor(x), torch.floor(y)
+    wx = keys_weights(x - xf)
+    wy = keys_weights(y - yf)
+    xi = xf.long() - 1
+    yi = yf.long() - 1
+    out = torch.zeros_like(x)
+    for a in range(4):
+        rows = torch.clamp(yi - 1 + a, 0, H - 1) * W
+        acc = torch.zeros_like(x)
+        for b in range(4):
+            acc += wx[b] * im[rows + torch.clamp(xi - 1 + b, 0, W - 1)]
+        out += wy[a] * acc
+    return out
+
+
+def invert_t(field, x, y, tol=1e-10, maxit=200):
+    """X with X + u(X) = x (fixed-point iteration)."""
+    X, Y = x.clone(), y.clone()
+    for _ in range(maxit):
+        u, v = field(X, Y)
+        Xn, Yn = x - u, y - v
+        err = max(float((Xn - X).abs().max()), float((Yn - Y).abs().max()))
+        X, Y = Xn, Yn
+        if err < tol:
+            break
+    return X, Y
+
+
+@dataclasses.dataclass
+class SequenceWorkload:
+    """An image sequence: frame 0 is the speckle image, frame k (k >= 1) is it
+    under the field k below plus noise (seed + 1000 + k).
+
+    Field k (pixels, 1-based image coordinates, centre c):
+      u = k*exx*(X - cx) + amp*sin(2*pi*(Y + drift*k)/period)
+      v = k*eyy*(Y - cy) + amp*cos(2*pi*(X + drift*k)/period)
+    i.e. a uniaxial stretch of eyy per frame with lateral contraction exx,
+    plus a travelling sinusoid of amplitude amp."""
+    name: str
+    W: int
+    H: int
+    ndots: int
+    seed: int
+    n_frames: int
+    winsize: int
+    step: int
+    search: int
+    noise: float
+    inc_unit: int | None
+    exx: float = -0.0006
+    eyy: float = 0.002
+    amp: float = 0.5
+    period: float = 512.0
+    drift: float = 8.0
+    scale: float = 257.0
+    dtype: type = np.uint16
+    tol: float = 1e-2
+    n_admm: int = 3
+
+    def field(self, k: int) -> Field:
+        cx, cy = (self.W + 1) / 2.0, (self.H + 1) / 2.0
+
+        def f(X, Y):
+            xp = np if isinstance(X, np.ndarray) else __import__("torch")
+            if k == 0:
+                return 0.0 * X, 0.0 * Y
+            u = k * self.exx * (X - cx) + self.amp * xp.sin(2 * math.pi * (Y + self.drift * k) / self.period)
+            v = k * self.eyy * (Y - cy) + self.amp * xp.cos(2 * math.pi * (X + self.drift * k) / self.period)
+            return u, v
+        return f
+
+    def frames(self, device="cpu"):
+        """All frames as torch tensors of the integer type on device."""
+        import torch
+        f = speckle_t(self.W, self.H, self.ndots, self.seed, device=device, scale=self.scale)
+        out = [quantise_t(f, self.dtype)]
+        ys, xs = torch.meshgrid(torch.arange(1, self.H + 1, dtype=torch.float64, device=device),
+                                torch.arange(1, self.W + 1, dtype=torch.float64, device=device),
+                                indexing="ij")
+        fq = out[0].to(torch.float64)
+        for k in range(1, self.n_frames):
+            X, Y = invert_t(self.field(k), xs, ys)
+            g = bicubic_sample_t(fq, X, Y)
+            gen = torch.Generator(device=device).manual_seed(self.seed + 1000 + k)
+            g = g + self.noise * torch.randn(g.shape, generator=gen, dtype=torch.float64, device=device)
+            out.append(quantise_t(g, self.dtype))
+        return out
+
+    def truth(self, k: int, r: int, x, y):
+        """Displacement from frame r to frame k of the material points at
+        (x, y) in frame r (the incremental reference's coordinates)."""
+        import torch
+        x = torch.as_tensor(np.asarray(x, np.float64))
+        y = torch.as_tensor(np.asarray(y, np.float64))
+        X, Y = invert_t(self.field(r), x, y) if r > 0 else (x, y)
+        uk, vk = self.field(k)(X, Y)
+        return (X + uk - x).numpy(), (Y + vk - y).numpy()
+
+
+SEQUENCES = {
+    # 50 frames of 4096^2 uint16 (intensities x257), 0.2 %/frame stretch in y
+    # with 0.06 % lateral contraction, 0.5 px sinusoid, noise 30 grey levels;
+    # subset 32, step 16; reference updated every 10 frames
+    "sequence4096": SequenceWorkload("sequence4096", 4096, 4096, 520_000, 4, 50, 32, 16, 24, 30.0, 10),
+}
+
+
+def sequence(name: str, scale_down: int = 1, n_frames: int | None = None) -> SequenceWorkload:
+    w = dataclasses.replace(SEQUENCES[name])
+    if scale_down > 1:
+        w.W //= scale_down
+        w.H //= scale_down
+        w.ndots = max(1, w.ndots // (scale_down * scale_down))
+    if n_frames:
+        w.n_frames = n_frames
+    return w
+
+
 def workload(name: str, scale_down: int = 1) -> Workload:
     """A named workload; scale_down > 1 shrinks the image (same density) for
     quick parity runs."""

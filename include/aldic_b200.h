@@ -188,12 +188,30 @@ ALDIC_API int aldic_inpaint_springs(aldic_ctx *ctx, int M, int N, int nf, double
  * twice, on nf interleaved fields (stride nf). */
 ALDIC_API int aldic_smooth(aldic_ctx *ctx, int M, int N, int nf, double *vals);
 
-/* One frame of main_ALDIC.m Sections 3-6 (accumulative mode) on the images
- * set on the context: integer search, MeshSetUp/Init, LocalICGN and its
- * post-processing, beta selection, Subproblem 2, then n_admm ADMM iterations
- * (Subpb1 + post, Subpb2, nodal strain, dual update).  The device part is
- * recorded once as a CUDA graph and replayed on later calls with the same
- * geometry. */
+/* One frame of main_ALDIC.m Sections 3-6 on the images set on the context:
+ * the initial guess (integer search + MeshSetUp/Init, or one of the
+ * sequence modes below), LocalICGN and its post-processing, beta selection,
+ * Subproblem 2, then n_admm ADMM iterations (Subpb1 + post, Subpb2, nodal
+ * strain, dual update).  The device part is recorded once as a CUDA graph
+ * and replayed on later calls with the same geometry.
+ *
+ * Initial guess (main_ALDIC.m:60-151, Section 3 of each frame):
+ *   ALDIC_INIT_SEARCH  integer search + Init (NewFFTSearch = 1);
+ *   ALDIC_INIT_PREV    U of the previous frame on this context
+ *                      (U0 = ResultDisp{ImgSeqNum-2}.U, main_ALDIC.m:131);
+ *   ALDIC_INIT_ZERO    zeros (reference-image update, main_ALDIC.m:123);
+ *   ALDIC_INIT_EXTRAP  2 U(k-1) - U(k-2) from the last two frames, a
+ *                      constant-rate predictor standing in for the POD-GPR
+ *                      prediction of main_ALDIC.m:133-146;
+ *   ALDIC_INIT_GIVEN   the 2n values set by aldic_set_init.
+ * The node grid is the search grid of the same parameters in every mode.
+ * The context keeps the final U of its last two frames on the device; it is
+ * valid while the node grid does not change. */
+#define ALDIC_INIT_SEARCH 0
+#define ALDIC_INIT_PREV 1
+#define ALDIC_INIT_ZERO 2
+#define ALDIC_INIT_EXTRAP 3
+#define ALDIC_INIT_GIVEN 4
 typedef struct {
   int winsize, step;
   int search[2];
@@ -206,6 +224,7 @@ typedef struct {
   int precision;            /* ALDIC_FP32 or ALDIC_FP64 */
   int smooth;               /* 1: funSmoothDisp/funSmoothStrain as main_ALDIC */
   int use_graph;            /* 1: capture/replay the device work as a CUDA graph */
+  int init;                 /* ALDIC_INIT_* */
 } aldic_frame_params;
 
 typedef struct {
@@ -227,6 +246,9 @@ typedef struct {
 } aldic_frame_stats;
 
 ALDIC_API int aldic_frame_dims(aldic_ctx *ctx, const aldic_frame_params *p, int *M, int *N);
+/* Initial guess for ALDIC_INIT_GIVEN: U0 interleaved [u1 v1 u2 v2 ...] on the
+ * node grid of aldic_frame_dims (n2 = 2*M*N values, host or device). */
+ALDIC_API int aldic_set_init(aldic_ctx *ctx, const double *U0, long long n2);
 ALDIC_API int aldic_frame(aldic_ctx *ctx, const aldic_frame_params *p, double *x0, double *y0,
                 double *U, double *F, int32_t *iters, aldic_frame_stats *stats);
 

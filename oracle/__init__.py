@@ -315,7 +315,8 @@ class _FP(C.Structure):
     _fields_ = [("winsize", C.c_int), ("step", C.c_int), ("search", C.c_int * 2),
                 ("gridx", C.c_int * 2), ("gridy", C.c_int * 2), ("tol", C.c_double),
                 ("mu", C.c_double), ("beta", C.c_double), ("n_admm", C.c_int),
-                ("tol2", C.c_double), ("smooth", C.c_int)]
+                ("tol2", C.c_double), ("smooth", C.c_int),
+                ("init_U", C.POINTER(C.c_double))]
 
 
 class _FR(C.Structure):
@@ -330,8 +331,9 @@ class _FR(C.Structure):
 
 
 def frame(f_raw, g_raw, winsize, step, search, gridx=None, gridy=None, tol=1e-2, mu=1e-3,
-          beta=0.0, n_admm=3, tol2=0.0, smooth=False):
-    """One frame of the ADMM core (main_ALDIC.m Sections 3-6)."""
+          beta=0.0, n_admm=3, tol2=0.0, smooth=False, U0=None):
+    """One frame of the ADMM core (main_ALDIC.m Sections 3-6); U0 (2n) replaces
+    the integer search and Init for a later frame of a sequence."""
     f_raw = _c(f_raw)
     g_raw = _c(g_raw, f_raw.dtype)
     H, W = f_raw.shape
@@ -343,6 +345,9 @@ def frame(f_raw, g_raw, winsize, step, search, gridx=None, gridy=None, tol=1e-2,
     p.gridx[0], p.gridx[1] = gx
     p.gridy[0], p.gridy[1] = gy
     p.tol, p.mu, p.beta, p.n_admm, p.tol2, p.smooth = tol, mu, beta, n_admm, tol2, int(smooth)
+    if U0 is not None:
+        U0 = np.ascontiguousarray(U0, np.float64)
+        p.init_U = U0.ctypes.data_as(C.POINTER(C.c_double))
     r = _FR()
     rc = lib().orc_frame(_p(f_raw), _p(g_raw), _DT[f_raw.dtype], W, H, C.byref(p), C.byref(r))
     if rc:

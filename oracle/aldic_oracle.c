@@ -1440,8 +1440,22 @@ int orc_frame(const void *f_raw, const void *g_raw, int dtype, int W, int H,
   const int64_t n = (int64_t)M * N;
   double *sx = (double *)malloc(sizeof(double) * n * 5);
   double *sy = sx + n, *su = sy + n, *sv = su + n, *scc = sv + n;
-  orc_int_search(f_raw, g_raw, dtype, W, H, mg, p->gridx, p->gridy, p->winsize, p->step,
-                 p->search, sx, sy, su, sv, scc, NULL);
+  if (!p->init_U) {
+    orc_int_search(f_raw, g_raw, dtype, W, H, mg, p->gridx, p->gridy, p->winsize, p->step,
+                   p->search, sx, sy, su, sv, scc, NULL);
+  } else {
+    /* the node grid of the search (funIntegerSearch.m:158-159), no search */
+    int gx1, gy1;
+    orc_search_dims(W, H, p->gridx, p->gridy, p->winsize, p->step, p->search, &nx, &ny, &gx1, &gy1);
+    for (int i = 0; i < ny; ++i)
+      for (int j = 0; j < nx; ++j) {
+        const int64_t o = (int64_t)i + (int64_t)j * ny; /* ny x nx column-major */
+        const double ii = gx1 + (double)j * p->step, jj = gy1 + (double)i * p->step;
+        sx[o] = (ii + ii + p->winsize) / 2.0;
+        sy[o] = (jj + jj + p->winsize) / 2.0;
+        su[o] = sv[o] = scc[o] = 0.0;
+      }
+  }
   r->t_search = now_s() - ts;
   /* x (ny x nx) -> coordinatesFEM x-fastest; Init inpaints u,v (Init.m:13) */
   r->M = M; r->N = N;
@@ -1459,10 +1473,14 @@ int orc_frame(const void *f_raw, const void *g_raw, int dtype, int W, int H,
       ug[k] = su[src];
       vg[k] = sv[src];
     }
-  orc_inpaint_springs(M, N, ug);
-  orc_inpaint_springs(M, N, vg);
   double *U0 = (double *)malloc(sizeof(double) * 2 * n);
-  for (int64_t k = 0; k < n; ++k) { U0[2 * k] = ug[k]; U0[2 * k + 1] = vg[k]; }
+  if (!p->init_U) {
+    orc_inpaint_springs(M, N, ug);
+    orc_inpaint_springs(M, N, vg);
+    for (int64_t k = 0; k < n; ++k) { U0[2 * k] = ug[k]; U0[2 * k + 1] = vg[k]; }
+  } else {
+    memcpy(U0, p->init_U, sizeof(double) * 2 * n);
+  }
   /* Section 4: LocalICGN */
   double ti = now_s();
   double *U1 = (double *)malloc(sizeof(double) * 2 * n);

@@ -124,6 +124,9 @@ typedef struct {
   int n_admm;          /* ADMM iterations after step 1 (reference: 4) */
   double tol2;         /* ADMM stop (main_ALDIC.m:354); <= 0 disables */
   int smooth;          /* 1: funSmoothDisp/funSmoothStrain as main_ALDIC.m */
+  const double *init_U; /* NULL: integer search + Init; else U0 (2n) of a later
+                           frame of a sequence (main_ALDIC.m:118-147) on the
+                           same node grid */
 } orc_frame_params;
 
 typedef struct {
