@@ -45,6 +45,15 @@ _SIGS = {
     "aldic_frame_dims": ([P, P, P, P], I32),
     "aldic_frame": ([P, P, P, P, P, P, P, P], I32),
     "aldic_set_init": ([P, P, I64], I32),
+    "aldic_qt_mesh_generate": ([I32, P, I32, P, P, I32, I32, D, I32, P], I32),
+    "aldic_qt_mesh_create": ([I32, P, I32, P, I32, P, P], I32),
+    "aldic_qt_mesh_info": ([P, P, P, P], I32),
+    "aldic_qt_mesh_get": ([P, P, P, P], I32),
+    "aldic_qt_mesh_destroy": ([P], I32),
+    "aldic_qt_subpb2": ([P, P, D, D, P, P, P], I32),
+    "aldic_qt_nodal_strain": ([P, P, P, P], I32),
+    "aldic_qt_fill": ([P, P, I32, P, P], I32),
+    "aldic_icgn_flags": ([P, I64, P, D, P, P], I32),
 }
 
 

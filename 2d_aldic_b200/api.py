@@ -624,6 +624,266 @@ class ALDIC:
         return res
 
 
+# ------------------------------------------------------------------ quadtree
+class QuadtreeMesh:
+    """The DICmesh of main_ALDIC_Quadtree.m (func_quadtree/GenerateQuadtreeMesh.m):
+    coordinatesFEM (n x 2), elementsFEM (ne x 8, 1-based, slots 5-8 hanging
+    nodes, 0 = none) and dirichlet (markCoordHoleEdge), held by the library
+    (host data, device copies made on first use)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        n, ne, nd = C.c_int(), C.c_int(), C.c_int()
+        call("aldic_qt_mesh_info", self.h, C.byref(n), C.byref(ne), C.byref(nd))
+        self.n, self.ne, self.ndir = n.value, ne.value, nd.value
+        c = np.empty((2, self.n))
+        e = np.empty((8, self.ne), np.int32)
+        d = np.empty(max(1, self.ndir), np.int32)
+        call("aldic_qt_mesh_get", self.h, _ptr(c), _ptr(e), _ptr(d))
+        self.coordinatesFEM = c.T.copy()
+        self.elementsFEM = e.T.copy()
+        self.dirichlet = d[:self.ndir].copy()
+
+    @classmethod
+    def generate(cls, coordinatesFEM, elementsFEM, mask, winstepsize, elementMinSize=2):
+        """GenerateQuadtreeMesh.m on the uniform mesh of MeshSetUp (coordinates
+        n x 2, elements ne x 4) and ImgRefMask (H, W) array."""
+        c = np.asfortranarray(np.asarray(coordinatesFEM, np.float64))
+        e = np.asfortranarray(np.asarray(elementsFEM, np.int32)[:, :4])
+        m = np.ascontiguousarray(np.asarray(mask, np.float64))
+        H, W = m.shape
+        h = C.c_void_p()
+        call("aldic_qt_mesh_generate", len(c), _ptr(c), len(e), _ptr(e), _ptr(m), W, H,
+             float(winstepsize), int(elementMinSize), C.byref(h))
+        return cls(h)
+
+    @classmethod
+    def create(cls, coordinatesFEM, elementsFEM, dirichlet):
+        c = np.asfortranarray(np.asarray(coordinatesFEM, np.float64))
+        e8 = np.zeros((len(elementsFEM), 8), np.int32)
+        ea = np.asarray(elementsFEM, np.int32)
+        e8[:, :ea.shape[1]] = ea
+        e8 = np.asfortranarray(e8)
+        d = np.ascontiguousarray(np.asarray(dirichlet, np.int32).reshape(-1))
+        h = C.c_void_p()
+        call("aldic_qt_mesh_create", len(c), _ptr(c), len(e8), _ptr(e8), len(d),
+             _ptr(d) if len(d) else None, C.byref(h))
+        return cls(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().aldic_qt_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def GenerateQuadtreeMesh(DICmesh: dict, mask, winstepsize, elementMinSize=2) -> QuadtreeMesh:
+    """func_quadtree/GenerateQuadtreeMesh.m:17-115 (the mesh part; U0 is
+    interpolated separately)."""
+    return QuadtreeMesh.generate(DICmesh["coordinatesFEM"], DICmesh["elementsFEM"], mask,
+                                 winstepsize, elementMinSize)
+
+
+def Subpb2Quadtree(mesh: QuadtreeMesh, beta, mu, U, F, ctx: Context | None = None):
+    """func_quadtree/Subpb2Quadtree.m:1 (GaussPtOrder 2, alpha 0; the duals
+    are multiplied by zero in the reference and are not taken)."""
+    ctx = ctx or default_context()
+    Ua, Fa = _prep(U), _prep(F)
+    out = _empty(_first_cuda(Ua, Fa), (2 * mesh.n,))
+    call("aldic_qt_subpb2", ctx.h, mesh.h, float(beta), float(mu), _ptr(Ua), _ptr(Fa), _ptr(out))
+    return out
+
+
+def funGlobalNodalStrainQuadtree(mesh: QuadtreeMesh, U, ctx: Context | None = None):
+    """func_quadtree/funGlobalNodalStrainQuadtree.m:1 (nodal values by corner
+    extrapolation and averaging; the reference interpolates scattered
+    Gauss-point values)."""
+    ctx = ctx or default_context()
+    Ua = _prep(U)
+    out = _empty(_first_cuda(Ua), (4 * mesh.n,))
+    call("aldic_qt_nodal_strain", ctx.h, mesh.h, _ptr(Ua), _ptr(out))
+    return out
+
+
+def quadtree_fill(mesh: QuadtreeMesh, vals, bad, ctx: Context | None = None):
+    """Refill of the flagged nodes of nf interleaved fields (n x nf)."""
+    ctx = ctx or default_context()
+    v = _prep(vals)
+    v = v.clone() if _is_cuda(v) else v.copy()
+    nf = (v.numel() if _is_cuda(v) else v.size) // mesh.n
+    b = _prep(bad, np.uint8)
+    call("aldic_qt_fill", ctx.h, mesh.h, int(nf), _ptr(v), _ptr(b))
+    return v
+
+
+def icgn_flags(iters, floor=float("nan"), ctx: Context | None = None):
+    """Bad-subset flags on any node set (LocalICGN.m:117-131; floor 20 for
+    Subpb1Quadtree.m:172-181): (bad mask, bad-point count)."""
+    ctx = ctx or default_context()
+    it = _prep(iters, np.int32)
+    n = it.numel() if _is_cuda(it) else it.size
+    bad = _empty(_first_cuda(it), (n,), np.uint8) if _is_cuda(it) else np.empty(n, np.uint8)
+    nb = C.c_int()
+    call("aldic_icgn_flags", ctx.h, int(n), _ptr(it), float(floor), _ptr(bad), C.byref(nb))
+    return bad, nb.value
+
+
+def _interp_uniform(xs, ys, fields, pts):
+    # bilinear on the uniform node grid (stands in for scatteredInterpolant
+    # 'linear' of GenerateQuadtreeMesh.m:124-130)
+    x, y = pts[:, 0], pts[:, 1]
+    i = np.clip(np.searchsorted(xs, x, side="right") - 1, 0, len(xs) - 2)
+    j = np.clip(np.searchsorted(ys, y, side="right") - 1, 0, len(ys) - 2)
+    tx = (x - xs[i]) / (xs[i + 1] - xs[i])
+    ty = (y - ys[j]) / (ys[j + 1] - ys[j])
+    return np.stack([(1 - ty) * ((1 - tx) * f[j, i] + tx * f[j, i + 1]) +
+                     ty * ((1 - tx) * f[j + 1, i] + tx * f[j + 1, i + 1]) for f in fields], 1)
+
+
+def quadtree_subset_sizes(mesh: QuadtreeMesh, winsize, mode="uniform", lo=16, hi=64):
+    """Subset size per node: the reference's uniform winsize
+    (Subpb1Quadtree.m:50), or ("element") twice the smallest side of the
+    elements at the node, clipped to [lo, hi] and even."""
+    c, E = mesh.coordinatesFEM, mesh.elementsFEM
+    if mode == "uniform":
+        return np.full(mesh.n, int(winsize), np.int32)
+    if mode != "element":
+        raise ValueError("subsets must be 'uniform' or 'element'")
+    side = np.full(mesh.n, np.inf)
+    sz = np.abs(c[E[:, 2] - 1, 0] - c[E[:, 0] - 1, 0])
+    for k in range(8):
+        nz = E[:, k] > 0
+        np.minimum.at(side, E[nz, k] - 1, sz[nz])
+    side[~np.isfinite(side)] = winsize / 2
+    return (2 * np.round(np.clip(2 * side, lo, hi) / 2)).astype(np.int32)
+
+
+def _select_beta(betas, e1, e2):
+    # main_ALDIC_Quadtree.m:179-190
+    e1, e2 = np.asarray(e1), np.asarray(e2)
+    es = (e1 - e1.mean()) / e1.std(ddof=1) + (e2 - e2.mean()) / e2.std(ddof=1)
+    k = int(np.nanargmin(es))
+    if 1 <= k <= len(betas) - 2:
+        p = np.polyfit(np.log10(betas[k - 1:k + 2]), es[k - 1:k + 2], 2)
+        return 10 ** (-p[1] / 2 / p[0])
+    return betas[k]
+
+
+class ALDICQuadtree:
+    """One frame of main_ALDIC_Quadtree.m Sections 3-6 (first frame of a
+    sequence): integer search on the uniform grid and Init, the quadtree mesh
+    of GenerateQuadtreeMesh.m with the initial guess interpolated onto it,
+    LocalICGN on every quadtree node (+ flags and refill), the three-value
+    beta sweep, Subpb2Quadtree + nodal strain with the boundary strains kept,
+    then ADMM steps (Subpb1Quadtree, Subpb2Quadtree) until step 4 or an
+    update below tol2.  Left out: the interactive outlier removal
+    (funRemoveOutliersQuadtree) and the strain smoothing of
+    DICpara.StrainSmoothness (regularizeNd).
+
+        qt = ALDICQuadtree(winsize=32, step=16, search=16)
+        qt.set_images(f, g, mask)     # mask: ImgRefMask as an (H, W) array
+        res = qt.frame()              # coords, elems, U, F, ...
+    """
+
+    def __init__(self, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3, tol2=1e-2,
+                 min_size=2, precision=FP32, subsets="uniform", device=None,
+                 ctx: Context | None = None):
+        self.ctx = ctx or default_context(device)
+        self.w, self.step, self.search = int(winsize), int(step), int(search)
+        self.tol, self.mu, self.n_admm, self.tol2 = float(tol), float(mu), int(n_admm), float(tol2)
+        self.min_size, self.precision, self.subsets = int(min_size), int(precision), subsets
+        self.mesh = None
+
+    def set_images(self, f, g, mask):
+        self.f, self.g = f, g
+        self.mask = np.ascontiguousarray(np.asarray(mask, np.float64))
+
+    def frame(self):
+        ctx, w, step = self.ctx, self.w, self.step
+        f, g, mask = self.f, self.g, self.mask
+        H, W = f.shape
+        t0 = time.perf_counter()
+        # Section 3: integer search on the uniform grid, MeshSetUp, Init
+        x, y, u, v, _ = funIntegerSearch(f, g, self.search, (1, W), (1, H), w, step, 0, step,
+                                         qfactors=False, ctx=ctx)
+        xi, yi = np.asarray(x, int), np.asarray(y, int)
+        hole = mask[yi - 1, xi - 1] == 0                         # IntegerSearch.m:68-73
+        u = np.where(hole, np.nan, u)
+        v = np.where(hole, np.nan, v)
+        mesh0 = MeshSetUp(x, y, {"ImgSize": (W, H)})
+        U0u = Init(u, v, None, x, y, 0)
+        ny, nx = u.shape
+        ctx.set_ref(f, mask=mask)
+        ctx.set_def(g)
+        if self.mesh is not None:
+            self.mesh.close()
+        m = self.mesh = QuadtreeMesh.generate(mesh0["coordinatesFEM"], mesh0["elementsFEM"], mask,
+                                              step, self.min_size)
+        c, n = m.coordinatesFEM, m.n
+        U0 = _interp_uniform(np.asarray(x)[0], np.asarray(y)[:, 0],
+                             [U0u[0::2].reshape(ny, nx), U0u[1::2].reshape(ny, nx)], c).reshape(-1)
+        wins = quadtree_subset_sizes(m, w, self.subsets)
+        t_mesh = time.perf_counter()
+        # Section 4: LocalICGN + flags + refill
+        U1, F1, it, Hp = local_icgn(ctx, c, U0, wins, self.tol, self.precision)
+        bad, nbad = icgn_flags(it, ctx=ctx)
+        U1 = quadtree_fill(m, np.where(bad[:, None] != 0, 0.0, U1.reshape(n, 2)), bad, ctx).reshape(-1)
+        F1 = quadtree_fill(m, np.where(bad[:, None] != 0, 0.0, F1.reshape(n, 4)), bad, ctx).reshape(-1)
+        U_icgn = U1.copy()
+        # Section 5: beta sweep, Subpb2Quadtree, nodal strain
+        mu = self.mu
+        betas = np.array([1e-3, 1e-2, 1e-1]) * step * step * mu
+        e1, e2 = [], []
+        for b in betas:
+            U2 = Subpb2Quadtree(m, b, mu, U1, F1, ctx)
+            F2 = funGlobalNodalStrainQuadtree(m, U2, ctx)
+            e1.append(np.linalg.norm(U1 - U2))
+            e2.append(np.linalg.norm(F1 - F2))
+        beta = _select_beta(betas, e1, e2)
+        if abs(beta - betas[-1]) > np.finfo(float).eps:
+            U2 = Subpb2Quadtree(m, beta, mu, U1, F1, ctx)
+            F2 = funGlobalNodalStrainQuadtree(m, U2, ctx)
+        d = m.dirichlet
+        dd = np.repeat(4 * (d - 1), 4) + np.tile(np.arange(4), len(d))
+        F2[dd] = F1[dd]                                   # main_ALDIC_Quadtree.m:205-207
+        udual, vdual = F2 - F1, U2 - U1
+        # Section 6: ADMM
+        upd, upd2 = [], []
+        U1old = U1.copy()
+        Hc = np.ascontiguousarray(Hp.T)
+        cf = _coords_cm(c)
+        wa = _prep(wins, np.int32)
+        for _ in range(self.n_admm):
+            U2old = U2.copy()
+            U1 = np.empty(2 * n)
+            it1 = np.empty(n, np.int32)
+            call("aldic_subpb1", ctx.h, _ptr(cf), n, _ptr(_prep(U2)), _ptr(_prep(F2)),
+                 _ptr(_prep(vdual)), _ptr(Hc), _ptr(wa), 0, float(mu), self.tol, self.precision,
+                 _ptr(U1), _ptr(it1))
+            b1, _ = icgn_flags(it1, 20.0, ctx)
+            U1 = quadtree_fill(m, np.where(b1[:, None] != 0, 0.0, U1.reshape(n, 2)), b1, ctx).reshape(-1)
+            F1 = F2.copy()
+            U2 = Subpb2Quadtree(m, beta, mu, U1, F1, ctx)
+            F2 = funGlobalNodalStrainQuadtree(m, U2, ctx)
+            F2[dd] = F1[dd]
+            upd.append(float(np.linalg.norm(U2old - U2) / np.sqrt(2 * n)))
+            upd2.append(float(np.linalg.norm(U1old - U1) / np.sqrt(2 * n)))
+            U1old = U1.copy()
+            udual, vdual = F2 - F1, U2 - U1
+            if upd[-1] < self.tol2 or upd2[-1] < self.tol2:
+                break
+        t1 = time.perf_counter()
+        return {"coords": c, "elems": m.elementsFEM, "dirichlet": d, "U": U2, "F": F2,
+                "U_icgn": U_icgn, "iters_icgn": it, "bad_icgn": nbad, "beta": beta,
+                "update_y": upd, "update_y2": upd2, "wins": wins, "U0": U0,
+                "time_s": {"search_mesh": t_mesh - t0, "frame": t1 - t0}}
+
+
 class ALDICSequence:
     """The frame loop of main_ALDIC.m:53-147 over an image sequence, with
     every image and all state on the device.

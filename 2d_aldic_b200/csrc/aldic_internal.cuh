@@ -108,4 +108,30 @@ __device__ __forceinline__ void keys_w(double t, double w[4]) {
   w[3] = 0.5 * (t3 - t2);
 }
 
+// device buffer that grows on demand (contents are not kept on growth)
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMalloc of " + std::to_string(want) + " bytes failed");
+      return E_NOMEM;
+    }
+    cap = want;
+    return OK;
+  }
+  template <typename T> T *as() const { return (T *)p; }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
 }  // namespace aldic

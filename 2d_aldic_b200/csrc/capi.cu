@@ -14,38 +14,13 @@
 #include "../../include/aldic_b200.h"
 #include "aldic_internal.cuh"
 #include "kernels.cuh"
+#include "qt.cuh"
 
 namespace aldic {
 
 static thread_local std::string g_err;
 void set_error(const std::string &msg) { g_err = msg; }
 const char *last_error() { return g_err.c_str(); }
-
-// ------------------------------------------------------------------ buffers
-struct DevBuf {
-  void *p = nullptr;
-  size_t cap = 0;
-  int ensure(size_t bytes) {
-    if (bytes <= cap) return OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    size_t want = bytes < 256 ? 256 : bytes;
-    if (cudaMalloc(&p, want) != cudaSuccess) {
-      cudaGetLastError();
-      set_error("cudaMalloc of " + std::to_string(want) + " bytes failed");
-      return E_NOMEM;
-    }
-    cap = want;
-    return OK;
-  }
-  template <typename T> T *as() const { return (T *)p; }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-  }
-};
 
 // bump arena for staging host arguments (chunks persist, reset per call)
 struct Arena {
@@ -790,6 +765,136 @@ int aldic_subpb2(aldic_ctx *c, int M, int N, double step, double beta, double mu
   if ((rc = fe_store(c->gw, M, N, ao.dev, c->stream))) return rc;
   arg_back(c, ao);
   return check_grid_err(c);
+}
+
+int aldic_qt_mesh_generate(int n0, const double *coords, int ne0, const int32_t *elems,
+                           const double *mask, int W, int H, double step, int min_size,
+                           aldic_qt_mesh **out) {
+  ALDIC_CHECK(out, E_ARG, "qt_mesh_generate: null output");
+  *out = nullptr;
+  auto *m = new aldic_qt_mesh();
+  const int rc = qt_generate(n0, coords, ne0, elems, mask, W, H, step, min_size, *m);
+  if (rc) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return OK;
+}
+
+int aldic_qt_mesh_create(int n, const double *coords, int ne, const int32_t *elems, int ndir,
+                         const int32_t *dirichlet, aldic_qt_mesh **out) {
+  ALDIC_CHECK(out && n > 0 && ne > 0 && coords && elems && ndir >= 0 && (ndir == 0 || dirichlet),
+              E_ARG, "qt_mesh_create: bad arguments");
+  *out = nullptr;
+  for (long long k = 0; k < 8LL * ne; ++k)
+    ALDIC_CHECK(elems[k] >= 0 && elems[k] <= n && (k >= 4LL * ne || elems[k] >= 1), E_ARG,
+                "qt_mesh_create: element nodes must be 1..n (0 only in slots 5-8)");
+  for (int k = 0; k < ndir; ++k)
+    ALDIC_CHECK(dirichlet[k] >= 1 && dirichlet[k] <= n, E_ARG, "qt_mesh_create: Dirichlet node out of range");
+  auto *m = new aldic_qt_mesh();
+  m->n = n;
+  m->ne = ne;
+  m->coords.assign(coords, coords + 2LL * n);
+  m->elems.assign(elems, elems + 8LL * ne);
+  m->dirichlet.assign(dirichlet, dirichlet + ndir);
+  std::sort(m->dirichlet.begin(), m->dirichlet.end());
+  m->dirichlet.erase(std::unique(m->dirichlet.begin(), m->dirichlet.end()), m->dirichlet.end());
+  *out = m;
+  return OK;
+}
+
+int aldic_qt_mesh_info(const aldic_qt_mesh *m, int *n, int *ne, int *ndir) {
+  ALDIC_CHECK(m, E_ARG, "qt_mesh_info: null mesh");
+  if (n) *n = m->n;
+  if (ne) *ne = m->ne;
+  if (ndir) *ndir = (int)m->dirichlet.size();
+  return OK;
+}
+
+int aldic_qt_mesh_get(const aldic_qt_mesh *m, double *coords, int32_t *elems, int32_t *dirichlet) {
+  ALDIC_CHECK(m, E_ARG, "qt_mesh_get: null mesh");
+  if (coords) memcpy(coords, m->coords.data(), sizeof(double) * m->coords.size());
+  if (elems) memcpy(elems, m->elems.data(), sizeof(int32_t) * m->elems.size());
+  if (dirichlet && !m->dirichlet.empty())
+    memcpy(dirichlet, m->dirichlet.data(), sizeof(int32_t) * m->dirichlet.size());
+  return OK;
+}
+
+int aldic_qt_mesh_destroy(aldic_qt_mesh *m) {
+  if (!m) return OK;
+  if (m->device >= 0) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(m->device);
+    cudaDeviceSynchronize();
+    m->release();
+    cudaSetDevice(prev);
+  }
+  delete m;
+  return OK;
+}
+
+int aldic_qt_subpb2(aldic_ctx *c, aldic_qt_mesh *m, double beta, double mu, const double *U,
+                    const double *F, double *Uhat) {
+  ALDIC_CHECK(c && m && U && F && Uhat, E_ARG, "qt_subpb2: bad arguments");
+  Guard g(c);
+  const long long n = m->n;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> au, af, ao;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_in(c, F, 4 * n, af)) ||
+      (rc = arg_out(c, Uhat, 2 * n, ao)))
+    return rc;
+  if ((rc = qt_subpb2(*m, c->gw, beta, mu, au.dev, af.dev, ao.dev, c->stream))) return rc;
+  arg_back(c, ao);
+  return check_grid_err(c);
+}
+
+int aldic_qt_nodal_strain(aldic_ctx *c, aldic_qt_mesh *m, const double *U, double *F) {
+  ALDIC_CHECK(c && m && U && F, E_ARG, "qt_nodal_strain: bad arguments");
+  Guard g(c);
+  const long long n = m->n;
+  int rc;
+  Arg<double> au, af;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_out(c, F, 4 * n, af))) return rc;
+  if ((rc = qt_strain(*m, au.dev, af.dev, c->stream))) return rc;
+  arg_back(c, af);
+  return finish(c, af.staged || au.staged);
+}
+
+int aldic_qt_fill(aldic_ctx *c, aldic_qt_mesh *m, int nf, double *vals, const uint8_t *bad) {
+  ALDIC_CHECK(c && m && vals && bad && nf >= 1 && nf <= 6, E_ARG, "qt_fill: bad arguments");
+  Guard g(c);
+  const long long n = m->n;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> av;
+  Arg<unsigned char> ab;
+  if ((rc = arg_out(c, vals, nf * n, av, true)) || (rc = arg_in(c, bad, n, ab))) return rc;
+  if ((rc = qt_fill(*m, c->gw, nf, av.dev, ab.dev, c->stream))) return rc;
+  arg_back(c, av);
+  return check_grid_err(c);
+}
+
+int aldic_icgn_flags(aldic_ctx *c, long long n, const int32_t *iters, double floor, uint8_t *bad,
+                     int *nbad) {
+  ALDIC_CHECK(c && iters && bad && n > 0 && n < (1LL << 31), E_ARG, "icgn_flags: bad arguments");
+  Guard g(c);
+  int rc;
+  Arg<int32_t> ai;
+  Arg<unsigned char> ab;
+  if ((rc = arg_in(c, iters, n, ai)) || (rc = arg_out(c, bad, n, ab))) return rc;
+  int *ints = (int *)c->arena.get(64);
+  ALDIC_CHECK(ints, E_NOMEM, "staging buffer allocation failed");
+  double *mean = (double *)(ints + 4);
+  if ((rc = icgn_flags((int)n, 1, ai.dev, ab.dev, ints, mean, ints + 1, c->stream, floor))) return rc;
+  arg_back(c, ab);
+  int hv[2] = {0, 0};
+  ALDIC_CUDA(cudaMemcpyAsync(hv, ints, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  if (nbad) *nbad = hv[0];
+  return OK;
 }
 
 int aldic_nodal_strain(aldic_ctx *c, int M, int N, double step, const double *U, double *F) {

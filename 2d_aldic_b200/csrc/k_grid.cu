@@ -33,6 +33,7 @@ struct PcgArgs {
   const double *beta_ptr;  // if set, every right-hand side uses *beta_ptr
   GridSync gs;
   int *iters_out;
+  CsrOp csr;               // OP_CSR
 };
 
 // Scalar Q4 element matrices on a square element of size h with local nodes
@@ -61,6 +62,8 @@ __device__ __forceinline__ double op_diag(const PcgArgs &A, double beta, int i, 
   if (OP == OP_FE) {
     const double kc = beta * (4.0 / 6.0) + A.mu * A.h * A.h * (4.0 / 36.0);
     return ecnt(i, 0, M) * ecnt(j, 0, N) * kc;
+  } else if (OP == OP_CSR) {
+    return A.mask[(long long)f * M * N + k] ? A.csr.diag[k] : 1.0;
   } else if (OP == OP_GRIDFIT) {
     const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
     const int na = (i > 0) + (i < M - 1) + (j > 0) + (j < N - 1);
@@ -95,6 +98,16 @@ __device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i,
         const int t = (di != 0) + (dj != 0);
         y += (double)(ci * cj) * kap[t] * v[k + di + (long long)dj * M];
       }
+    }
+    return y;
+  } else if (OP == OP_CSR) {
+    const unsigned char *fr = A.mask + (long long)f * M * N;
+    if (!fr[k]) return v[k];
+    double y = 0.0;
+    const int p1 = A.csr.row[k + 1];
+    for (int p = A.csr.row[k]; p < p1; ++p) {
+      const int c = A.csr.col[p];
+      if (fr[c]) y += A.csr.val[p] * v[c];
     }
     return y;
   } else if (OP == OP_GRIDFIT) {
@@ -494,7 +507,7 @@ __global__ void k_inpaint_load(int M, int N, int nf, const double *__restrict__ 
 // ------------------------------------------------------------------ flags
 __global__ void k_icgn_flags(long long n, const int *__restrict__ it,
                              unsigned char *__restrict__ bad, int *badnum, double *meanit,
-                             int *nconv) {
+                             int *nconv, double floor) {
   __shared__ long long sh[32][3];
   __shared__ double shd[32];
   __shared__ double s_mean, s_thr;
@@ -539,7 +552,9 @@ __global__ void k_icgn_flags(long long n, const int *__restrict__ it,
     for (int w = 0; w < nw; ++w) t += shd[w];
     const double sd = ngood > 1 ? sqrt(t / (double)(ngood - 1))
                                 : (ngood == 1 ? 0.0 : __longlong_as_double(0x7ff8000000000000ll));
-    s_thr = m + 0.15 * sd;
+    // Subpb1Quadtree.m:180 raises the threshold to at least `floor`
+    // (MATLAB's max ignores a NaN); NaN floor = LocalICGN.m:128-131
+    s_thr = isnan(floor) ? m + 0.15 * sd : fmax(m + 0.15 * sd, floor);
   }
   __syncthreads();
   const double thr = s_thr;
@@ -675,6 +690,48 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
   A.gs.count = w.bar; A.gs.gen = w.bar + 1; A.gs.err = w.err;
   A.iters_out = w.iters_out;
   A.beta_ptr = beta_ptr;
+  A.csr = CsrOp{};
+  ALDIC_CUDA(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned int), st));
+  void *args[] = {&A};
+  ALDIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(PCG_THREADS), args, 0, st));
+  return OK;
+}
+
+int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, int maxit,
+            cudaStream_t st) {
+  ALDIC_CHECK(nrhs >= 1 && nrhs <= 6, E_ARG, "csr_pcg: 1..6 right-hand sides");
+  ALDIC_CHECK(n >= 1 && n < (1LL << 31), E_ARG, "csr_pcg: bad size");
+  int dev = 0, sms = 148;
+  ALDIC_CUDA(cudaGetDevice(&dev));
+  ALDIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  void *fn = nullptr;
+  switch (nrhs) {
+    case 1: fn = (void *)k_pcg<OP_CSR, 1>; break;
+    case 2: fn = (void *)k_pcg<OP_CSR, 2>; break;
+    case 3: case 4: fn = (void *)k_pcg<OP_CSR, 4>; break;
+    default: fn = (void *)k_pcg<OP_CSR, 6>; break;
+  }
+  const int nr_pad = nrhs <= 2 ? nrhs : (nrhs <= 4 ? 4 : 6);
+  long long blocks = sms;
+  const long long need = (n + PCG_THREADS - 1) / PCG_THREADS;
+  if (blocks > need) blocks = need;
+  if (blocks > w.max_blocks) blocks = w.max_blocks;
+  if (blocks < 1) blocks = 1;
+  PcgArgs A;
+  A.x = w.x; A.r = w.r; A.z = w.z; A.p0 = w.p; A.p1 = w.p + MAXRHS * n; A.q = w.q; A.b = w.b;
+  A.diag = w.diag; A.part = w.part; A.mask = w.mask;
+  if (nr_pad > nrhs) {
+    ALDIC_CUDA(cudaMemsetAsync(w.b + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
+    ALDIC_CUDA(cudaMemsetAsync(w.x + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
+    ALDIC_CUDA(cudaMemsetAsync(w.mask + nrhs * n, 0, (size_t)(nr_pad - nrhs) * n, st));
+  }
+  A.M = (int)n; A.N = 1; A.nrhs = nr_pad; A.maxit = maxit; A.blocks = (int)blocks;
+  for (int f = 0; f < MAXRHS; ++f) A.beta[f] = 0.0;
+  A.mu = 0; A.h = 1; A.lam2 = 0; A.rtol = rtol;
+  A.gs.count = w.bar; A.gs.gen = w.bar + 1; A.gs.err = w.err;
+  A.iters_out = w.iters_out;
+  A.beta_ptr = nullptr;
+  A.csr = op;
   ALDIC_CUDA(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned int), st));
   void *args[] = {&A};
   ALDIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(PCG_THREADS), args, 0, st));
@@ -738,9 +795,9 @@ int inpaint_store(const GridWork &w, int M, int N, int nf, double *vals, int str
 }
 
 int icgn_flags(int M, int N, const int *iters, unsigned char *badmask, int *d_badnum,
-               double *d_meaniters, int *d_nconv, cudaStream_t st) {
+               double *d_meaniters, int *d_nconv, cudaStream_t st, double floor) {
   k_icgn_flags<<<1, 1024, 0, st>>>((long long)M * N, iters, badmask, d_badnum, d_meaniters,
-                                   d_nconv);
+                                   d_nconv, floor);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

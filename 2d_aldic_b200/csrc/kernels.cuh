@@ -50,7 +50,18 @@ struct GridWork {
   int *iters_out;        // PCG iterations used
   int max_blocks;
 };
-enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2 };
+enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2, OP_CSR = 3 };
+
+// A symmetric sparse operator for the PCG: CSR rows of n nodes (sorted
+// columns), its diagonal, shared by every field.  Rows whose field mask is 0
+// are identity rows; columns whose mask is 0 are skipped (their values were
+// moved to the right-hand side).
+struct CsrOp {
+  const int *row, *col;
+  const double *val, *diag;
+};
+int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, int maxit,
+            cudaStream_t st);
 
 // solve op(x) = b for nrhs fields; b and x live in w.b / w.x (field-major)
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
@@ -76,7 +87,7 @@ int inpaint_store(const GridWork &w, int M, int N, int nf, double *vals, int str
                   cudaStream_t st, int f0 = 0);
 // LocalICGN.m:117-131 flags; writes badmask and the bad count to d_badnum
 int icgn_flags(int M, int N, const int *iters, unsigned char *badmask, int *d_badnum,
-               double *d_meaniters, int *d_nconv, cudaStream_t st);
+               double *d_meaniters, int *d_nconv, cudaStream_t st, double floor = __builtin_nan(""));
 // Subpb1.m:167-169 flags
 int subpb1_flags(int n, const int *iters, unsigned char *badmask, int *d_badnum,
                  cudaStream_t st);

@@ -1,0 +1,771 @@
+// qt.cu -- quadtree meshes: GenerateQuadtreeMesh.m on the host, and the
+// device operators of Subpb2Quadtree.m, funGlobalNodalStrainQuadtree.m and
+// the refill of flagged nodes on such a mesh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "qt.cuh"
+
+void aldic_qt_mesh::release() {
+  aldic::DevBuf *b[] = {&d_coords, &d_elems, &d_row, &d_col, &d_dpos, &d_iptr, &d_inc, &d_ipos,
+                        &d_kind, &d_val, &d_diag, &d_ke, &d_be, &d_es, &d_arow, &d_acol,
+                        &d_aval, &d_adiag, &d_icorner};
+  for (auto *x : b) x->release();
+  device = -1;
+}
+
+namespace aldic {
+
+namespace {
+
+// ------------------------------------------------------------------ host mesh
+struct HMesh {
+  std::vector<double> x, y;                  // node coordinates (0-based index)
+  std::vector<std::array<int, 4>> el;        // 1-based corners
+  std::vector<std::array<int, 3>> irr;       // sorted parent edge, hanging node
+};
+
+// element bounding box in whole pixels; false if not whole or out of the mask
+bool box(const HMesh &m, const std::array<int, 4> &e, int W, int H, int b[4]) {
+  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+  for (int c = 0; c < 4; ++c) {
+    const double x = m.x[e[c] - 1], y = m.y[e[c] - 1];
+    x0 = std::min(x0, x); x1 = std::max(x1, x);
+    y0 = std::min(y0, y); y1 = std::max(y1, y);
+  }
+  if (x0 != std::floor(x0) || x1 != std::floor(x1) || y0 != std::floor(y0) || y1 != std::floor(y1))
+    return false;
+  b[0] = (int)x0; b[1] = (int)x1; b[2] = (int)y0; b[3] = (int)y1;
+  return b[0] >= 1 && b[1] <= W && b[2] >= 1 && b[3] <= H;
+}
+
+// funMarkEdge.m: box straddles the mask edge and its smaller side > min_size
+int mark_edge(const HMesh &m, const double *mask, int W, int H, double min_size,
+              std::vector<int> &out) {
+  out.clear();
+  for (size_t e = 0; e < m.el.size(); ++e) {
+    int b[4];
+    if (!box(m, m.el[e], W, H, b)) return E_ARG;
+    double lo = 1e300, hi = -1e300;
+    for (int y = b[2]; y <= b[3]; ++y)
+      for (int x = b[0]; x <= b[1]; ++x) {
+        const double v = mask[(long long)(y - 1) * W + (x - 1)];
+        lo = std::min(lo, v);
+        hi = std::max(hi, v);
+      }
+    const double size = std::min(std::abs(b[1] - b[0]), std::abs(b[3] - b[2]));
+    if (hi - lo > 0 && size > min_size) out.push_back((int)e);
+  }
+  return OK;
+}
+
+// provideGeometricData.m: edges of the irregular triples (column by column)
+// then of the elements, sorted unique; inverse maps per triple / element
+struct Geo {
+  std::vector<std::array<int, 2>> e2n;
+  std::vector<std::array<int, 3>> irr2e;
+  std::vector<std::array<int, 4>> el2e;
+};
+
+void geometric(const HMesh &m, Geo &g) {
+  const size_t ni = m.irr.size(), ne = m.el.size(), n3 = 3 * ni;
+  std::vector<std::array<long long, 3>> ed;
+  ed.reserve(n3 + 4 * ne);
+  for (int c = 0; c < 3; ++c)
+    for (size_t r = 0; r < ni; ++r) {
+      const int a = m.irr[r][c], b = m.irr[r][(c + 1) % 3];
+      ed.push_back({std::min(a, b), std::max(a, b), (long long)(c * ni + r)});
+    }
+  for (int c = 0; c < 4; ++c)
+    for (size_t r = 0; r < ne; ++r) {
+      const int a = m.el[r][c], b = m.el[r][(c + 1) % 4];
+      ed.push_back({std::min(a, b), std::max(a, b), (long long)(n3 + c * ne + r)});
+    }
+  std::sort(ed.begin(), ed.end());
+  std::vector<int> ie(ed.size());
+  g.e2n.clear();
+  for (size_t k = 0; k < ed.size(); ++k) {
+    if (k == 0 || ed[k][0] != ed[k - 1][0] || ed[k][1] != ed[k - 1][1])
+      g.e2n.push_back({(int)ed[k][0], (int)ed[k][1]});
+    ie[ed[k][2]] = (int)g.e2n.size() - 1;
+  }
+  g.irr2e.assign(ni, {0, 0, 0});
+  g.el2e.assign(ne, {0, 0, 0, 0});
+  for (int c = 0; c < 3; ++c)
+    for (size_t r = 0; r < ni; ++r) g.irr2e[r][c] = ie[c * ni + r];
+  for (int c = 0; c < 4; ++c)
+    for (size_t r = 0; r < ne; ++r) g.el2e[r][c] = ie[n3 + c * ne + r];
+}
+
+// QrefineR.m: red refinement of the marked elements, closure by the
+// 1-irregular rule, new nodes on edges (sorted edge order) then at the
+// centres of refined elements (element order)
+void qrefine(HMesh &m, const std::vector<int> &marked) {
+  Geo g;
+  geometric(m, g);
+  const size_t nE = m.el.size(), ni = m.irr.size();
+  std::vector<long long> e2n(g.e2n.size(), 0);
+  for (int e : marked)
+    for (int c = 0; c < 4; ++c) e2n[g.el2e[e][c]] = 1;
+  for (size_t r = 0; r < ni; ++r) e2n[g.irr2e[r][0]] = 1;
+  bool first = true;
+  size_t nk = 0, nswap = 0;
+  std::vector<int> kdx;
+  while (first || nk || nswap) {
+    first = false;
+    kdx.clear();
+    for (size_t e = 0; e < nE; ++e) {
+      long long s = 0, mn = 1;
+      for (int c = 0; c < 4; ++c) {
+        const long long v = e2n[g.el2e[e][c]];
+        s += v < 0 ? -v : v;
+        mn = std::min(mn, v);
+      }
+      if (s < 4 && (s > 2 || mn < 0)) kdx.push_back((int)e);
+    }
+    for (int e : kdx)
+      for (int c = 0; c < 4; ++c)
+        if (e2n[g.el2e[e][c]] == 0) e2n[g.el2e[e][c]] = 1;
+    nk = kdx.size();
+    nswap = 0;
+    if (ni) {
+      std::vector<int> sw;
+      for (size_t r = 0; r < ni; ++r)
+        if (e2n[g.irr2e[r][1]] != 0 || e2n[g.irr2e[r][2]] != 0)
+          if (e2n[g.irr2e[r][0]] != -1) sw.push_back(g.irr2e[r][0]);
+      for (int ed : sw) e2n[ed] = -1;
+      nswap = sw.size();
+    }
+  }
+  for (size_t r = 0; r < ni; ++r) e2n[g.irr2e[r][0]] = -1;
+  long long next = (long long)m.x.size() + 1;
+  for (size_t ed = 0; ed < e2n.size(); ++ed)
+    if (e2n[ed] > 0) {
+      e2n[ed] = next++;
+      const int a = g.e2n[ed][0] - 1, b = g.e2n[ed][1] - 1;
+      m.x.push_back((m.x[a] + m.x[b]) / 2);
+      m.y.push_back((m.y[a] + m.y[b]) / 2);
+    }
+  for (size_t r = 0; r < ni; ++r) e2n[g.irr2e[r][0]] = m.irr[r][2];
+  std::vector<std::array<long long, 4>> nn(nE);
+  std::vector<int> reftyp(nE);
+  for (size_t e = 0; e < nE; ++e) {
+    int t = 0;
+    for (int c = 0; c < 4; ++c) {
+      nn[e][c] = e2n[g.el2e[e][c]];
+      if (nn[e][c] != 0) t |= 1 << c;
+    }
+    reftyp[e] = t;
+  }
+  std::vector<long long> mid(nE, 0);
+  for (size_t e = 0; e < nE; ++e)
+    if (reftyp[e] == 15) {
+      mid[e] = (long long)m.x.size() + 1;
+      const auto &q = m.el[e];
+      m.x.push_back((m.x[q[0] - 1] + m.x[q[1] - 1] + m.x[q[2] - 1] + m.x[q[3] - 1]) / 4);
+      m.y.push_back((m.y[q[0] - 1] + m.y[q[1] - 1] + m.y[q[2] - 1] + m.y[q[3] - 1]) / 4);
+    }
+  std::vector<std::array<int, 4>> nel;
+  nel.reserve(nE * 2);
+  for (size_t e = 0; e < nE; ++e) {
+    const auto &q = m.el[e];
+    if (reftyp[e] < 15) {
+      nel.push_back(q);
+    } else {
+      const int md = (int)mid[e];
+      const auto &w = nn[e];
+      nel.push_back({q[0], (int)w[0], md, (int)w[3]});
+      nel.push_back({q[1], (int)w[1], md, (int)w[0]});
+      nel.push_back({q[2], (int)w[2], md, (int)w[1]});
+      nel.push_back({q[3], (int)w[3], md, (int)w[2]});
+    }
+  }
+  // new irregularity data, in the column-major order of MATLAB's find()
+  std::vector<std::array<int, 3>> nirr;
+  for (int c = 0; c < 4; ++c)
+    for (size_t e = 0; e < nE; ++e)
+      if (reftyp[e] > 0 && reftyp[e] < 15 && nn[e][c] != 0) {
+        const auto &p = g.e2n[g.el2e[e][c]];
+        nirr.push_back({p[0], p[1], (int)nn[e][c]});
+      }
+  for (int c = 0; c < 2; ++c)
+    for (size_t r = 0; r < ni; ++r) {
+      const long long v1 = e2n[g.irr2e[r][1]], v2 = e2n[g.irr2e[r][2]];
+      if (v1 + v2 == 0) continue;
+      const long long v = c == 0 ? v1 : v2;
+      if (v != 0) {
+        const auto &p = g.e2n[g.irr2e[r][1 + c]];
+        nirr.push_back({p[0], p[1], (int)v});
+      }
+    }
+  m.el.swap(nel);
+  m.irr.swap(nirr);
+}
+
+}  // namespace
+
+int qt_generate(int n0, const double *coords, int ne0, const int32_t *elems, const double *mask,
+                int W, int H, double step, int min_size, aldic_qt_mesh &out) {
+  ALDIC_CHECK(n0 >= 4 && ne0 >= 1 && coords && elems && mask && W > 0 && H > 0 && step > 0 &&
+                  min_size >= 1,
+              E_ARG, "qt_mesh_generate: bad arguments");
+  HMesh m;
+  m.x.assign(coords, coords + n0);
+  m.y.assign(coords + n0, coords + 2 * n0);
+  m.el.resize(ne0);
+  for (int e = 0; e < ne0; ++e)
+    for (int c = 0; c < 4; ++c) {
+      const int v = elems[(long long)c * ne0 + e];
+      ALDIC_CHECK(v >= 1 && v <= n0, E_ARG, "qt_mesh_generate: element node out of range");
+      m.el[e][c] = v;
+    }
+  double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+  for (int k = 0; k < n0; ++k) {
+    xmin = std::min(xmin, m.x[k]); xmax = std::max(xmax, m.x[k]);
+    ymin = std::min(ymin, m.y[k]); ymax = std::max(ymax, m.y[k]);
+  }
+  std::vector<int> mk;
+  for (int pass = 0;; ++pass) {
+    ALDIC_CHECK(pass < 64, E_ARG, "qt_mesh_generate: refinement does not terminate");
+    if (mark_edge(m, mask, W, H, 2.0 * min_size, mk) != OK) {
+      set_error("qt_mesh_generate: element corners must be whole pixels inside the mask "
+                "(uniform step a power-of-two multiple of the minimum element size)");
+      return E_ARG;
+    }
+    qrefine(m, mk);
+    if (mk.empty()) break;
+  }
+  // hanging nodes into slots 5-8 (GenerateQuadtreeMesh.m:40-57): the first
+  // element whose edge (c1, c2), in either direction, is the parent edge
+  const size_t ne = m.el.size();
+  std::vector<std::array<int, 8>> E(ne);
+  for (size_t e = 0; e < ne; ++e) {
+    for (int c = 0; c < 4; ++c) E[e][c] = m.el[e][c];
+    for (int c = 4; c < 8; ++c) E[e][c] = 0;
+  }
+  static const int pairs[8][3] = {{0, 1, 7}, {1, 2, 4}, {2, 3, 5}, {3, 0, 6},
+                                  {1, 0, 7}, {2, 1, 4}, {3, 2, 5}, {0, 3, 6}};
+  std::map<std::tuple<int, int, int>, int> first;
+  for (int pi = 0; pi < 8; ++pi)
+    for (size_t e = ne; e-- > 0;)
+      first[std::make_tuple(m.el[e][pairs[pi][0]], m.el[e][pairs[pi][1]], pi)] = (int)e;
+  for (const auto &r : m.irr)
+    for (int pi = 0; pi < 8; ++pi) {
+      auto it = first.find(std::make_tuple(r[0], r[1], pi));
+      if (it != first.end()) E[it->second][pairs[pi][2]] = r[2];
+    }
+  // funMarkInside.m: drop elements less than half inside the mask
+  std::vector<std::array<int, 8>> K;
+  for (size_t e = 0; e < ne; ++e) {
+    int b[4];
+    if (!box(m, m.el[e], W, H, b)) return E_ARG;
+    double s = 0;
+    for (int y = b[2]; y <= b[3]; ++y)
+      for (int x = b[0]; x <= b[1]; ++x) s += mask[(long long)(y - 1) * W + (x - 1)];
+    if (!(s < 0.5 * (b[1] - b[0]) * (b[3] - b[2]))) K.push_back(E[e]);
+  }
+  // Dirichlet nodes (GenerateQuadtreeMesh.m:75-110): refined elements and
+  // elements at the ROI border, grown by two rings of neighbours
+  const size_t nk = K.size();
+  std::vector<char> sel(nk, 0);
+  for (size_t e = 0; e < nk; ++e) {
+    const int a = K[e][0] - 1, c = K[e][2] - 1;
+    const double d = std::hypot(m.x[a] - m.x[c], m.y[a] - m.y[c]);
+    sel[e] = d < 0.99 * std::sqrt(2.0) * step || m.x[a] < xmin + 1.01 * step ||
+             m.x[c] > xmax - 1.01 * step || m.y[a] < ymin + 1.01 * step ||
+             m.y[c] > ymax - 1.01 * step;
+  }
+  const size_t nn = m.x.size();
+  std::vector<char> mark(nn + 1, 0);
+  for (size_t e = 0; e < nk; ++e)
+    if (sel[e])
+      for (int s = 0; s < 8; ++s) mark[K[e][s]] = 1;
+  mark[0] = 0;
+  for (int it = 0; it < 2; ++it) {
+    std::vector<char> nm(nn + 1, 0);
+    for (size_t e = 0; e < nk; ++e) {
+      bool hit = false;
+      for (int s = 0; s < 8; ++s)
+        if (K[e][s] && mark[K[e][s]]) hit = true;
+      if (hit)
+        for (int s = 0; s < 8; ++s) nm[K[e][s]] = 1;
+    }
+    nm[0] = 0;
+    mark.swap(nm);
+  }
+  out.release();
+  out.n = (int)nn;
+  out.ne = (int)nk;
+  out.coords.resize(2 * nn);
+  for (size_t k = 0; k < nn; ++k) {
+    out.coords[k] = m.x[k];
+    out.coords[nn + k] = m.y[k];
+  }
+  out.elems.resize(8 * nk);
+  for (size_t e = 0; e < nk; ++e)
+    for (int s = 0; s < 8; ++s) out.elems[(size_t)s * nk + e] = K[e][s];
+  out.dirichlet.clear();
+  for (size_t k = 1; k <= nn; ++k)
+    if (mark[k]) out.dirichlet.push_back((int)k);
+  return OK;
+}
+
+// ------------------------------------------------------------------ device
+namespace {
+
+constexpr double kG = 0.57735026918962576451;  // 1/sqrt(3)
+
+__device__ __forceinline__ double sgn(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); }
+
+// N1..N8 and d/dksi, d/deta with hanging-node enrichment (Subpb2Quadtree.m
+// shape functions and the funDN* helpers); d[4] = presence of slots 5-8
+__device__ __forceinline__ void shape8(double ksi, double eta, const double d[4], double N[8],
+                                       double dk[8], double de[8]) {
+  const double ak = fabs(ksi), ae = fabs(eta);
+  N[4] = d[0] * 0.5 * (1 + ksi) * (1 - ae);
+  N[5] = d[1] * 0.5 * (1 + eta) * (1 - ak);
+  N[6] = d[2] * 0.5 * (1 - ksi) * (1 - ae);
+  N[7] = d[3] * 0.5 * (1 - eta) * (1 - ak);
+  N[0] = (1 - ksi) * (1 - eta) * 0.25 - 0.5 * (N[6] + N[7]);
+  N[1] = (1 + ksi) * (1 - eta) * 0.25 - 0.5 * (N[7] + N[4]);
+  N[2] = (1 + ksi) * (1 + eta) * 0.25 - 0.5 * (N[4] + N[5]);
+  N[3] = (1 - ksi) * (1 + eta) * 0.25 - 0.5 * (N[5] + N[6]);
+  dk[4] = d[0] * 0.5 * (1 - ae);
+  de[4] = d[0] * 0.5 * (1 + ksi) * sgn(-eta);
+  dk[5] = d[1] * 0.5 * (1 + eta) * sgn(-ksi);
+  de[5] = d[1] * 0.5 * (1 - ak);
+  dk[6] = d[2] * 0.5 * (-1) * (1 - ae);
+  de[6] = d[2] * 0.5 * (1 - ksi) * sgn(-eta);
+  dk[7] = d[3] * 0.5 * (1 - eta) * sgn(-ksi);
+  de[7] = d[3] * 0.5 * (-1) * (1 - ak);
+  dk[0] = -0.25 * (1 - eta) - 0.5 * (dk[6] + dk[7]);
+  de[0] = -0.25 * (1 - ksi) - 0.5 * (de[6] + de[7]);
+  dk[1] = 0.25 * (1 - eta) - 0.5 * (dk[7] + dk[4]);
+  de[1] = -0.25 * (1 + ksi) - 0.5 * (de[7] + de[4]);
+  dk[2] = 0.25 * (1 + eta) - 0.5 * (dk[4] + dk[5]);
+  de[2] = 0.25 * (1 + ksi) - 0.5 * (de[4] + de[5]);
+  dk[3] = -0.25 * (1 + eta) - 0.5 * (dk[5] + dk[6]);
+  de[3] = 0.25 * (1 - ksi) - 0.5 * (de[5] + de[6]);
+}
+
+// d/dx, d/dy and det J at (ksi, eta)
+__device__ __forceinline__ double grads(const double dk[8], const double de[8], const double px[8],
+                                        const double py[8], double dx[8], double dy[8]) {
+  double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    J11 += dk[s] * px[s];
+    J12 += dk[s] * py[s];
+    J21 += de[s] * px[s];
+    J22 += de[s] * py[s];
+  }
+  const double det = J11 * J22 - J12 * J21;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    dx[s] = (J22 * dk[s] - J12 * de[s]) / det;
+    dy[s] = (-J21 * dk[s] + J11 * de[s]) / det;
+  }
+  return det;
+}
+
+// one thread per (element, local row a): row a of the scalar 8x8 element
+// matrix sum_gp detJ (beta grad Na . grad Nb + mu Na Nb) and the row's
+// right-hand sides (the duals are multiplied by zero in the reference)
+__global__ void k_qt_elem(int ne, const int *__restrict__ E, const double *__restrict__ cx,
+                          const double *__restrict__ cy, double beta, double mu,
+                          const double *__restrict__ U, const double *__restrict__ F,
+                          double *__restrict__ ke, double *__restrict__ be) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 8LL * ne) return;
+  const int e = (int)(t >> 3), a = (int)(t & 7);
+  int nd[8];
+  double px[8], py[8], d[4];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    nd[s] = E[e * 8 + s];
+    px[s] = nd[s] >= 0 ? cx[nd[s]] : 0.0;
+    py[s] = nd[s] >= 0 ? cy[nd[s]] : 0.0;
+  }
+#pragma unroll
+  for (int s = 0; s < 4; ++s) d[s] = nd[4 + s] >= 0 ? 1.0 : 0.0;
+  double K[8] = {0, 0, 0, 0, 0, 0, 0, 0}, bu = 0, bv = 0;
+  if (nd[a] >= 0) {
+    const int ka = nd[a];
+    const double F0 = F[4 * ka], F1 = F[4 * ka + 1], F2 = F[4 * ka + 2], F3 = F[4 * ka + 3];
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+      const double ksi = (g & 1) ? kG : -kG, eta = (g & 2) ? kG : -kG;
+      double N[8], dk[8], de[8], dx[8], dy[8];
+      shape8(ksi, eta, d, N, dk, de);
+      const double J = grads(dk, de, px, py, dx, dy);
+      double uu = 0, vv = 0;
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+        if (nd[s] >= 0) {
+          uu += N[s] * U[2 * nd[s]];
+          vv += N[s] * U[2 * nd[s] + 1];
+        }
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+        if (nd[s] >= 0) K[s] += J * (beta * (dx[a] * dx[s] + dy[a] * dy[s]) + mu * N[a] * N[s]);
+      bu += J * (beta * (dx[a] * F0 + dy[a] * F2) + mu * N[a] * uu);
+      bv += J * (beta * (dx[a] * F1 + dy[a] * F3) + mu * N[a] * vv);
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < 8; ++s) ke[(long long)e * 64 + a * 8 + s] = K[s];
+  be[(long long)e * 16 + a] = bu;
+  be[(long long)e * 16 + 8 + a] = bv;
+}
+
+// one thread per node: its matrix row and right-hand sides, summed over the
+// incident elements in element order (deterministic)
+__global__ void k_qt_gather(int n, const int *__restrict__ iptr, const int *__restrict__ inc,
+                            const int *__restrict__ ipos, const int *__restrict__ row,
+                            const double *__restrict__ ke, const double *__restrict__ be,
+                            double *__restrict__ val, double *__restrict__ b) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  for (int p = row[a]; p < row[a + 1]; ++p) val[p] = 0.0;
+  double bu = 0, bv = 0;
+  for (int t = iptr[a]; t < iptr[a + 1]; ++t) {
+    const int ent = inc[t], e = ent >> 3, sa = ent & 7;
+    for (int sb = 0; sb < 8; ++sb) {
+      const int pos = ipos[8 * t + sb];
+      if (pos >= 0) val[pos] += ke[(long long)e * 64 + sa * 8 + sb];
+    }
+    bu += be[(long long)e * 16 + sa];
+    bv += be[(long long)e * 16 + 8 + sa];
+  }
+  b[a] = bu;
+  b[n + a] = bv;
+}
+
+// Dirichlet elimination: free rows move the fixed columns to the right-hand
+// side (start from U); Dirichlet rows keep U; nodes in no element get 0
+__global__ void k_qt_elim(int n, const int *__restrict__ row, const int *__restrict__ col,
+                          const double *__restrict__ val, const int *__restrict__ dpos,
+                          const unsigned char *__restrict__ kind, const double *__restrict__ U,
+                          double *__restrict__ b, double *__restrict__ x,
+                          unsigned char *__restrict__ mask, double *__restrict__ diag) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int kd = kind[a];
+  diag[a] = kd == 2 ? 1.0 : val[dpos[a]];
+  for (int f = 0; f < 2; ++f) {
+    const long long o = (long long)f * n + a;
+    if (kd == 0) {
+      double s = b[o];
+      for (int p = row[a]; p < row[a + 1]; ++p) {
+        const int c = col[p];
+        if (kind[c] == 1) s -= val[p] * U[2 * c + f];
+      }
+      b[o] = s;
+      x[o] = U[2 * a + f];
+      mask[o] = 1;
+    } else {
+      const double v = kd == 1 ? U[2 * a + f] : 0.0;
+      b[o] = v;
+      x[o] = v;
+      mask[o] = 0;
+    }
+  }
+}
+
+__global__ void k_qt_store(int n, const double *__restrict__ x, double *__restrict__ Uhat) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  Uhat[2 * a] = x[a];
+  Uhat[2 * a + 1] = x[n + a];
+}
+
+// Gauss-point strains of an element's Q4 corners (slots 5-8 ignored, as
+// funGlobalNodalStrainQuadtree.m:33 zeroes them), extrapolated to its
+// corners: es[e][corner][du/dx du/dy dv/dx dv/dy]
+__global__ void k_qt_strain_elem(int ne, const int *__restrict__ E, const double *__restrict__ cx,
+                                 const double *__restrict__ cy, const double *__restrict__ U,
+                                 double *__restrict__ es) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double px[8], py[8], u[4], v[4];
+  const double d[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const int k = E[e * 8 + s];
+    px[s] = cx[k];
+    py[s] = cy[k];
+    u[s] = U[2 * k];
+    v[s] = U[2 * k + 1];
+    px[4 + s] = py[4 + s] = 0.0;
+  }
+  double gv[4][4];
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    const double ksi = (g & 1) ? kG : -kG, eta = (g & 2) ? kG : -kG;
+    double N[8], dk[8], de[8], dx[8], dy[8];
+    shape8(ksi, eta, d, N, dk, de);
+    grads(dk, de, px, py, dx, dy);
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      a0 += dx[s] * u[s];
+      a1 += dy[s] * u[s];
+      a2 += dx[s] * v[s];
+      a3 += dy[s] * v[s];
+    }
+    gv[g][0] = a0; gv[g][1] = a1; gv[g][2] = a2; gv[g][3] = a3;
+  }
+  const double s3 = 1.7320508075688772935;  // corner / Gauss-point ratio
+  const double ck[4] = {-s3, s3, s3, -s3}, ce[4] = {-s3, -s3, s3, s3};
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const double k = ck[a], q = ce[a];
+    const double w0 = (1 - k) * (1 - q) * 0.25, w1 = (1 + k) * (1 - q) * 0.25,
+                 w2 = (1 - k) * (1 + q) * 0.25, w3 = (1 + k) * (1 + q) * 0.25;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      es[(long long)e * 16 + a * 4 + c] = w0 * gv[0][c] + w1 * gv[1][c] + w2 * gv[2][c] + w3 * gv[3][c];
+  }
+}
+
+__global__ void k_qt_strain_gather(int n, const int *__restrict__ iptr, const int *__restrict__ inc,
+                                   const double *__restrict__ es, double *__restrict__ F) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  double s[4] = {0, 0, 0, 0};
+  int cnt = 0;
+  for (int t = iptr[a]; t < iptr[a + 1]; ++t) {
+    const int ent = inc[t], e = ent >> 3, sa = ent & 7;
+    if (sa >= 4) continue;
+    for (int c = 0; c < 4; ++c) s[c] += es[(long long)e * 16 + sa * 4 + c];
+    cnt++;
+  }
+  for (int c = 0; c < 4; ++c) F[4 * a + c] = cnt ? s[c] / cnt : 0.0;
+}
+
+// refill: bad nodes are unknowns of (L + t I) x = sum of good neighbours
+__global__ void k_qt_fill_prep(int n, int nf, const double *__restrict__ vals,
+                               const unsigned char *__restrict__ bad, const int *__restrict__ row,
+                               const int *__restrict__ col, double *__restrict__ b,
+                               double *__restrict__ x, unsigned char *__restrict__ mask) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  for (int f = 0; f < nf; ++f) {
+    const long long o = (long long)f * n + a;
+    if (bad[a]) {
+      double s = 0.0;
+      for (int p = row[a]; p < row[a + 1]; ++p) {
+        const int c = col[p];
+        if (c != a && !bad[c]) s += vals[(long long)c * nf + f];
+      }
+      b[o] = s;
+      x[o] = 0.0;
+      mask[o] = 1;
+    } else {
+      const double v = vals[(long long)a * nf + f];
+      b[o] = v;
+      x[o] = v;
+      mask[o] = 0;
+    }
+  }
+}
+
+__global__ void k_qt_fill_store(int n, int nf, const double *__restrict__ x,
+                                const unsigned char *__restrict__ bad, double *__restrict__ vals) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n || !bad[a]) return;
+  for (int f = 0; f < nf; ++f) vals[(long long)a * nf + f] = x[(long long)f * n + a];
+}
+
+inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
+
+template <typename T>
+int put(DevBuf &b, const std::vector<T> &v) {
+  int rc = b.ensure(sizeof(T) * (v.empty() ? 1 : v.size()));
+  if (rc) return rc;
+  if (!v.empty()) ALDIC_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return OK;
+}
+
+}  // namespace
+
+int qt_upload(aldic_qt_mesh &m, cudaStream_t st) {
+  int dev = 0;
+  ALDIC_CUDA(cudaGetDevice(&dev));
+  if (m.device == dev) return OK;
+  m.release();
+  const int n = m.n, ne = m.ne;
+  std::vector<int> E(8 * (size_t)ne);
+  std::vector<unsigned char> kind(n, 2);
+  for (int e = 0; e < ne; ++e)
+    for (int s = 0; s < 8; ++s) {
+      const int v = m.elems[(size_t)s * ne + e];
+      ALDIC_CHECK(v >= 0 && v <= n, E_ARG, "quadtree mesh: element node out of range");
+      E[8 * e + s] = v - 1;
+      if (v) kind[v - 1] = 0;
+    }
+  ALDIC_CHECK(ne >= 1 && E[0] >= 0, E_ARG, "quadtree mesh: no elements");
+  for (int e = 0; e < ne; ++e)
+    for (int s = 0; s < 4; ++s) ALDIC_CHECK(E[8 * e + s] >= 0, E_ARG, "quadtree mesh: empty corner slot");
+  for (int d : m.dirichlet) {
+    ALDIC_CHECK(d >= 1 && d <= n, E_ARG, "quadtree mesh: Dirichlet node out of range");
+    if (kind[d - 1] == 0) kind[d - 1] = 1;
+  }
+  // FE pattern: node pairs sharing an element
+  std::vector<std::vector<int>> cols(n);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) {
+      const int na = E[8 * e + a];
+      if (na < 0) continue;
+      for (int b = 0; b < 8; ++b)
+        if (E[8 * e + b] >= 0) cols[na].push_back(E[8 * e + b]);
+    }
+  std::vector<int> row(n + 1, 0), col, dpos(n, 0);
+  for (int a = 0; a < n; ++a) {
+    auto &c = cols[a];
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    row[a + 1] = row[a] + (int)c.size();
+    for (size_t k = 0; k < c.size(); ++k)
+      if (c[k] == a) dpos[a] = row[a] + (int)k;
+    col.insert(col.end(), c.begin(), c.end());
+  }
+  // incidence (element order) and its scatter map into the rows
+  std::vector<std::vector<int>> incl(n);
+  for (int e = 0; e < ne; ++e)
+    for (int s = 0; s < 8; ++s)
+      if (E[8 * e + s] >= 0) incl[E[8 * e + s]].push_back(8 * e + s);
+  std::vector<int> iptr(n + 1, 0), inc, ipos;
+  for (int a = 0; a < n; ++a) {
+    iptr[a + 1] = iptr[a] + (int)incl[a].size();
+    for (int ent : incl[a]) {
+      inc.push_back(ent);
+      const int e = ent >> 3;
+      for (int sb = 0; sb < 8; ++sb) {
+        const int nb = E[8 * e + sb];
+        if (nb < 0) {
+          ipos.push_back(-1);
+        } else {
+          const auto it = std::lower_bound(col.begin() + row[a], col.begin() + row[a + 1], nb);
+          ipos.push_back((int)(it - col.begin()));
+        }
+      }
+    }
+  }
+  // refill graph: element boundary rings 1-8-2-5-3-6-4-7
+  static const int ring[8] = {0, 7, 1, 4, 2, 5, 3, 6};
+  std::vector<std::vector<int>> adj(n);
+  for (int e = 0; e < ne; ++e) {
+    int r[8], k = 0;
+    for (int q = 0; q < 8; ++q)
+      if (E[8 * e + ring[q]] >= 0) r[k++] = E[8 * e + ring[q]];
+    for (int q = 0; q < k; ++q) {
+      const int a = r[q], b = r[(q + 1) % k];
+      adj[a].push_back(b);
+      adj[b].push_back(a);
+    }
+  }
+  std::vector<int> arow(n + 1, 0), acol;
+  std::vector<double> aval, adiag(n);
+  for (int a = 0; a < n; ++a) {
+    auto &c = adj[a];
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    const double deg = (double)c.size();
+    bool diag_done = false;
+    for (int v : c) {
+      if (!diag_done && v > a) {
+        acol.push_back(a);
+        aval.push_back(deg + kQtFillTether);
+        diag_done = true;
+      }
+      acol.push_back(v);
+      aval.push_back(-1.0);
+    }
+    if (!diag_done) {
+      acol.push_back(a);
+      aval.push_back(deg + kQtFillTether);
+    }
+    adiag[a] = deg + kQtFillTether;
+    arow[a + 1] = (int)acol.size();
+  }
+  std::vector<int> icorner(n, 0);
+  int rc;
+  if ((rc = put(m.d_coords, m.coords)) || (rc = put(m.d_elems, E)) || (rc = put(m.d_row, row)) ||
+      (rc = put(m.d_col, col)) || (rc = put(m.d_dpos, dpos)) || (rc = put(m.d_iptr, iptr)) ||
+      (rc = put(m.d_inc, inc)) || (rc = put(m.d_ipos, ipos)) || (rc = put(m.d_kind, kind)) ||
+      (rc = put(m.d_arow, arow)) || (rc = put(m.d_acol, acol)) || (rc = put(m.d_aval, aval)) ||
+      (rc = put(m.d_adiag, adiag)))
+    return rc;
+  if ((rc = m.d_val.ensure(sizeof(double) * (col.size() + 1))) ||
+      (rc = m.d_diag.ensure(sizeof(double) * n)) || (rc = m.d_ke.ensure(sizeof(double) * 64 * ne)) ||
+      (rc = m.d_be.ensure(sizeof(double) * 16 * ne)) || (rc = m.d_es.ensure(sizeof(double) * 16 * ne)))
+    return rc;
+  m.nnz = (long long)col.size();
+  m.ninc = (long long)inc.size();
+  m.nadj = (long long)acol.size();
+  m.device = dev;
+  (void)st;
+  return OK;
+}
+
+constexpr double kQtRtol = 1e-11;
+constexpr int kQtMaxit = 50000;
+
+int qt_subpb2(aldic_qt_mesh &m, GridWork &w, double beta, double mu, const double *U,
+              const double *F, double *Uhat, cudaStream_t st) {
+  int rc;
+  if ((rc = qt_upload(m, st))) return rc;
+  const int n = m.n, ne = m.ne;
+  const double *cx = m.d_coords.as<double>(), *cy = cx + n;
+  k_qt_elem<<<nblk(8LL * ne), 256, 0, st>>>(ne, m.d_elems.as<int>(), cx, cy, beta, mu, U, F,
+                                            m.d_ke.as<double>(), m.d_be.as<double>());
+  k_qt_gather<<<nblk(n), 256, 0, st>>>(n, m.d_iptr.as<int>(), m.d_inc.as<int>(), m.d_ipos.as<int>(),
+                                       m.d_row.as<int>(), m.d_ke.as<double>(), m.d_be.as<double>(),
+                                       m.d_val.as<double>(), w.b);
+  k_qt_elim<<<nblk(n), 256, 0, st>>>(n, m.d_row.as<int>(), m.d_col.as<int>(), m.d_val.as<double>(),
+                                     m.d_dpos.as<int>(), m.d_kind.as<unsigned char>(), U, w.b, w.x,
+                                     w.mask, m.d_diag.as<double>());
+  ALDIC_CUDA(cudaGetLastError());
+  const CsrOp op{m.d_row.as<int>(), m.d_col.as<int>(), m.d_val.as<double>(), m.d_diag.as<double>()};
+  if ((rc = csr_pcg(w, op, n, 2, kQtRtol, kQtMaxit, st))) return rc;
+  k_qt_store<<<nblk(n), 256, 0, st>>>(n, w.x, Uhat);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int qt_strain(aldic_qt_mesh &m, const double *U, double *F, cudaStream_t st) {
+  int rc;
+  if ((rc = qt_upload(m, st))) return rc;
+  const int n = m.n, ne = m.ne;
+  const double *cx = m.d_coords.as<double>(), *cy = cx + n;
+  k_qt_strain_elem<<<nblk(ne), 256, 0, st>>>(ne, m.d_elems.as<int>(), cx, cy, U, m.d_es.as<double>());
+  k_qt_strain_gather<<<nblk(n), 256, 0, st>>>(n, m.d_iptr.as<int>(), m.d_inc.as<int>(),
+                                              m.d_es.as<double>(), F);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int qt_fill(aldic_qt_mesh &m, GridWork &w, int nf, double *vals, const unsigned char *bad,
+            cudaStream_t st) {
+  ALDIC_CHECK(nf >= 1 && nf <= 6, E_ARG, "qt_fill: 1..6 fields");
+  int rc;
+  if ((rc = qt_upload(m, st))) return rc;
+  const int n = m.n;
+  k_qt_fill_prep<<<nblk(n), 256, 0, st>>>(n, nf, vals, bad, m.d_arow.as<int>(), m.d_acol.as<int>(),
+                                          w.b, w.x, w.mask);
+  ALDIC_CUDA(cudaGetLastError());
+  const CsrOp op{m.d_arow.as<int>(), m.d_acol.as<int>(), m.d_aval.as<double>(), m.d_adiag.as<double>()};
+  if ((rc = csr_pcg(w, op, n, nf, kQtRtol, kQtMaxit, st))) return rc;
+  k_qt_fill_store<<<nblk(n), 256, 0, st>>>(n, nf, w.x, bad, vals);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace aldic

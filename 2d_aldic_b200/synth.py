@@ -123,6 +123,13 @@ class Workload:
     fp64: bool = False
     dtype: type = np.uint8
     scale: float = 1.0
+    hole: tuple | None = None      # (cx, cy, radius) of a circular hole
+
+    def mask(self):
+        """ImgRefMask (H, W): 1 on the specimen, 0 in the hole."""
+        if self.hole is None:
+            return np.ones((self.H, self.W))
+        return disk_mask(self.W, self.H, *self.hole)
 
     def images(self):
         f = speckle(self.W, self.H, self.ndots, self.seed, dtype=self.dtype,
@@ -156,12 +163,22 @@ def uniform_affine(ux, vy, u0=0.0, v0=0.0):
     return f
 
 
+def disk_mask(W, H, cx, cy, rad):
+    """ImgRefMask of a plate with a circular hole: 0 inside the disk."""
+    yy, xx = np.mgrid[1:H + 1, 1:W + 1]
+    return ((xx - cx) ** 2 + (yy - cy) ** 2 >= rad * rad).astype(np.float64)
+
+
 WORKLOADS = {
     # plain ALDIC, 512^2, 8000 dots, subset 20 / step 10, search +-20, FP64
     "plain512": Workload("plain512", 512, 512, 8000, 0, 20, 10, 20, 2.0, _affine_small,
                          tol=1e-3, fp64=True),
     # large uniform batch, 2048^2, 130k dots, subset 32 / step 8, sinusoidal
     "uniform2048": Workload("uniform2048", 2048, 2048, 130_000, 1, 32, 8, 16, 2.0, _sine),
+    # plate with a hole of radius 300 px at the centre, quadtree mesh from a
+    # 16 px grid, subset 32
+    "plate2048": Workload("plate2048", 2048, 2048, 130_000, 2, 32, 16, 16, 2.0,
+                          plate_hole(1024.0, 1024.0, 300.0), hole=(1024.0, 1024.0, 300.0)),
 }
 
 
@@ -336,6 +353,10 @@ def workload(name: str, scale_down: int = 1) -> Workload:
         w.W //= scale_down
         w.H //= scale_down
         w.ndots = max(1, w.ndots // (scale_down * scale_down))
+        if w.hole is not None:
+            cx, cy, r = (v / scale_down for v in w.hole)
+            w.hole = (cx, cy, r)
+            w.field = plate_hole(cx, cy, r)
     return w
 
 

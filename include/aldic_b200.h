@@ -188,6 +188,56 @@ ALDIC_API int aldic_inpaint_springs(aldic_ctx *ctx, int M, int N, int nf, double
  * twice, on nf interleaved fields (stride nf). */
 ALDIC_API int aldic_smooth(aldic_ctx *ctx, int M, int N, int nf, double *vals);
 
+/* ---- Quadtree meshes (func_quadtree/*) ----
+ * A mesh object: nodes (n x 2 column-major, like DICmesh.coordinatesFEM),
+ * elements (ne x 8 column-major int32, 1-based: corners 1-4, hanging nodes
+ * on edges 2-3, 3-4, 4-1, 1-2 in slots 5-8, 0 = none, like
+ * DICmesh.elementsFEM) and Dirichlet nodes (DICmesh.dirichlet).  Host data;
+ * device copies are made on first use. */
+typedef struct aldic_qt_mesh aldic_qt_mesh;
+/* GenerateQuadtreeMesh.m:17-115 from the uniform mesh of MeshSetUp.m
+ * (coords n0 x 2, elems ne0 x 4): refine elements whose box straddles the
+ * edge of mask (ImgRefMask, W x H doubles, Img(x,y) at (y-1)*W + x-1) until
+ * their smaller side is at most 2*min_size (QrefineR red refinement,
+ * 1-irregular), drop elements less than half inside the mask, mark the
+ * Dirichlet nodes (refined elements and the ROI border band, two rings
+ * wider).  Host computation. */
+ALDIC_API int aldic_qt_mesh_generate(int n0, const double *coords, int ne0, const int32_t *elems,
+                                     const double *mask, int W, int H, double step,
+                                     int min_size, aldic_qt_mesh **out);
+/* A mesh from the reference's own DICmesh arrays. */
+ALDIC_API int aldic_qt_mesh_create(int n, const double *coords, int ne, const int32_t *elems,
+                                   int ndir, const int32_t *dirichlet, aldic_qt_mesh **out);
+ALDIC_API int aldic_qt_mesh_info(const aldic_qt_mesh *m, int *n, int *ne, int *ndir);
+ALDIC_API int aldic_qt_mesh_get(const aldic_qt_mesh *m, double *coords, int32_t *elems,
+                                int32_t *dirichlet);
+ALDIC_API int aldic_qt_mesh_destroy(aldic_qt_mesh *m);
+/* Subpb2Quadtree.m:1 with GaussPtOrder 2 and alpha 0: the global step on the
+ * quadtree mesh (hanging-node shape functions, Dirichlet nodes keep U, nodes
+ * in no element get 0).  The reference multiplies udual and vdual by zero
+ * (Subpb2Quadtree.m:60-61), so they are not arguments.  U 2n, F 4n -> Uhat
+ * 2n; FP64 PCG to relative residual 1e-11 replaces the direct solve. */
+ALDIC_API int aldic_qt_subpb2(aldic_ctx *ctx, aldic_qt_mesh *m, double beta, double mu,
+                              const double *U, const double *F, double *Uhat);
+/* funGlobalNodalStrainQuadtree.m:1 Gauss-point strains (corners only, as the
+ * reference zeroes slots 5-8) extrapolated to the element corners and
+ * averaged per node (the reference interpolates them with
+ * scatteredInterpolant instead); output slots [du/dx du/dy dv/dx dv/dy]. */
+ALDIC_API int aldic_qt_nodal_strain(aldic_ctx *ctx, aldic_qt_mesh *m, const double *U, double *F);
+/* Refill of flagged nodes (bad[k] != 0) of nf interleaved fields in place:
+ * graph-Laplacian interpolation over the mesh edges with a 1e-6 tether to 0
+ * (the reference: scatteredInterpolant 'natural', LocalICGN.m:144-161,
+ * Subpb1Quadtree.m:194-199). */
+ALDIC_API int aldic_qt_fill(aldic_ctx *ctx, aldic_qt_mesh *m, int nf, double *vals,
+                            const uint8_t *bad);
+
+/* Bad-subset flags on any node set: status < 0 or > 99, or iterations above
+ * max(mean + 0.15 std over the good subsets, floor) -- LocalICGN.m:117-131
+ * with floor = NaN, Subpb1Quadtree.m:172-181 with floor = 20.  bad: n bytes;
+ * nbad: the reference's bad-point count (status 102 not counted). */
+ALDIC_API int aldic_icgn_flags(aldic_ctx *ctx, long long n, const int32_t *iters, double floor,
+                               uint8_t *bad, int *nbad);
+
 /* One frame of main_ALDIC.m Sections 3-6 on the images set on the context:
  * the initial guess (integer search + MeshSetUp/Init, or one of the
  * sequence modes below), LocalICGN and its post-processing, beta selection,
