@@ -183,6 +183,20 @@ def icgn_traffic_from_profile():
     return tot
 
 
+def aggregate(local_ms: float, local_units: float, world: int, device):
+    """Whole-job timing of independent replicas: the slowest rank's device
+    time and the units all ranks processed (the only collectives of a run;
+    none on the data path)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([local_ms], dtype=torch.float64, device=device)
+    u = torch.tensor([local_units], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
 def sequence_main(args, rank, world, local):
     """The 16-bit image-sequence workload: every frame through ALDICSequence
     (reference updated every inc_unit frames, all images and state on the
@@ -387,13 +401,8 @@ def main():
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
-    tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    csum = torch.tensor([float(sum(conv))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(csum, op=dist.ReduceOp.SUM)
-    total_ms = float(tmax.item())
-    value = float(csum.item()) / (total_ms / 1e3)
+    total_ms, units = aggregate(total_ms, float(sum(conv)), world, dev)
+    value = units / (total_ms / 1e3)
     frames_per_s = world * args.steps / (total_ms / 1e3)
     iters = out["iters"].cpu().numpy()
     kernels = r["stats"]["kernel_launches"]
