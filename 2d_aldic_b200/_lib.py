@@ -54,6 +54,7 @@ _SIGS = {
     "aldic_qt_nodal_strain": ([P, P, P, P], I32),
     "aldic_qt_fill": ([P, P, I32, P, P], I32),
     "aldic_icgn_flags": ([P, I64, P, D, P, P], I32),
+    "aldic_gemm_bf16": ([P, P, P, P, I32], I32),
 }
 
 
@@ -62,6 +63,17 @@ class FrameParams(C.Structure):
                 ("gridy", I32 * 2), ("tol", D), ("mu", D), ("beta", D), ("n_admm", I32),
                 ("tol2", D), ("precision", I32), ("smooth", I32), ("use_graph", I32),
                 ("init", I32)]
+
+
+class GemmOperand(C.Structure):
+    _fields_ = [("p", P), ("ld", I64), ("mode", I32), ("rows", I64), ("kdim", I64),
+                ("Hin", I32), ("Win", I32), ("C", I32), ("ps", I32)]
+
+
+class GemmOutput(C.Structure):
+    _fields_ = [("p", P), ("ld", I64), ("mode", I32), ("fp32", I32), ("bias", P), ("relu", I32),
+                ("mask", P), ("Hin", I32), ("Win", I32), ("C", I32), ("ps", I32), ("M", I64),
+                ("N", I64), ("split_stride", I64)]
 
 
 class FrameStats(C.Structure):

@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI of libaldic_b200.so (include/aldic_b200.h): context,
 // host/device argument staging, the per-function entry points and the
 // captured frame pipeline of main_ALDIC.m Sections 3-6.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -894,6 +895,40 @@ int aldic_icgn_flags(aldic_ctx *c, long long n, const int32_t *iters, double flo
   ALDIC_CUDA(cudaMemcpyAsync(hv, ints, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
   ALDIC_CUDA(cudaStreamSynchronize(c->stream));
   if (nbad) *nbad = hv[0];
+  return OK;
+}
+
+static GemmSrc gemm_src(const aldic_gemm_operand &o) {
+  GemmSrc s;
+  s.p = (const __nv_bfloat16 *)o.p;
+  s.ld = o.ld; s.mode = o.mode; s.rows = o.rows; s.kdim = o.kdim;
+  s.Hin = o.Hin; s.Win = o.Win; s.C = o.C; s.ps = o.ps;
+  return s;
+}
+
+int aldic_gemm_bf16(aldic_ctx *c, const aldic_gemm_operand *A, const aldic_gemm_operand *B,
+                    const aldic_gemm_output *D, int splits) {
+  ALDIC_CHECK(c && A && B && D, E_ARG, "gemm: null argument");
+  ALDIC_CHECK(A->mode >= 0 && A->mode <= 3 && B->mode >= 0 && B->mode <= 3 &&
+                  (D->mode == 0 || D->mode == 1),
+              E_ARG, "gemm: bad mode");
+  Guard g(c);
+  int rc;
+  if ((rc = ensure_grid_work(c, 1))) return rc;
+  GemmDst d;
+  d.p = D->p; d.ld = D->ld; d.mode = D->mode; d.fp32 = D->fp32; d.bias = D->bias; d.relu = D->relu;
+  d.mask = (const __nv_bfloat16 *)D->mask;
+  d.Hin = D->Hin; d.Win = D->Win; d.C = D->C; d.ps = D->ps; d.M = D->M; d.N = D->N;
+  d.split_stride = D->split_stride;
+  if ((rc = gemm_bf16(gemm_src(*A), gemm_src(*B), d, splits, c->gw.err, c->stream))) return rc;
+  int err = 0;
+  ALDIC_CUDA(cudaMemcpyAsync(&err, c->gw.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  ALDIC_CUDA(cudaStreamSynchronize(c->stream));
+  if (err) {
+    cudaMemsetAsync(c->gw.err, 0, sizeof(int), c->stream);
+    set_error("gemm: a tensor-core wait timed out");
+    return E_TIMEOUT;
+  }
   return OK;
 }
 

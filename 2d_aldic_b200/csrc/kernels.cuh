@@ -1,5 +1,6 @@
 // kernels.cuh -- launchers of the sm_100a kernels (called by capi.cu).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,6 +63,40 @@ struct CsrOp {
 };
 int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, int maxit,
             cudaStream_t st);
+
+// ---- BF16 tensor-core GEMM (k_gemm.cu): D = A . B^T over K
+enum GemmMode { GEMM_ROW = 0, GEMM_PATCH = 1, GEMM_TRANS = 2, GEMM_PATCHT = 3 };
+// An operand of `rows` x `kdim` bf16 values read from p:
+//   ROW    (r, k) at p[r * ld + k]
+//   PATCH  (r, k) = im2col of an NHWC tensor [*, Hin, Win, C] with
+//          non-overlapping ps x ps patches: r = (b, i, j) output position,
+//          k = (di, dj, c) in that order
+//   TRANS  (r, k) at p[k * ld + r]          (a ROW source read transposed)
+//   PATCHT (r, k) = PATCH element (k, r)    (im2col read transposed)
+struct GemmSrc {
+  const __nv_bfloat16 *p;
+  long long ld;
+  int mode;
+  long long rows, kdim;
+  int Hin, Win, C, ps;
+};
+// Output: ROW (m, n) at p[m * ld + n], or PATCH scatter of (m, n) into the
+// NHWC tensor the PATCH operand reads; x = acc (+ bias[n]) (ReLU) and zeroed
+// where mask (same layout as the output, bf16) is not positive.
+struct GemmDst {
+  void *p;
+  long long ld;
+  int mode;
+  int fp32;
+  const float *bias;
+  int relu;
+  const __nv_bfloat16 *mask;
+  int Hin, Win, C, ps;
+  long long M, N;
+  long long split_stride;  // elements between the partial products of split-K
+};
+int gemm_bf16(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, int *err,
+              cudaStream_t st);
 
 // solve op(x) = b for nrhs fields; b and x live in w.b / w.x (field-major)
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,

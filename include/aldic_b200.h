@@ -238,6 +238,42 @@ ALDIC_API int aldic_qt_fill(aldic_ctx *ctx, aldic_qt_mesh *m, int nf, double *va
 ALDIC_API int aldic_icgn_flags(aldic_ctx *ctx, long long n, const int32_t *iters, double floor,
                                uint8_t *bad, int *nbad);
 
+/* ---- BF16 tensor-core GEMM (the learned initial guess's layers; no
+ * counterpart in the reference) ----
+ * D[M x N] = A[M x K] . B[N x K]^T in FP32 on the tcgen05 tensor cores.
+ * Operands are bf16 device arrays read in one of four ways (mode):
+ *   0 rows     (r, k) at p[r * ld + k]
+ *   1 patches  im2col of an NHWC tensor [*, Hin, Win, C] with
+ *              non-overlapping ps x ps patches (row = output position, column =
+ *              (di, dj, c)); ps * C must be a multiple of 8
+ *   2 rows read transposed   (r, k) at p[k * ld + r]
+ *   3 patches read transposed (r, k) = patch element (k, r)
+ * Output: rows (ld) or (mode 1) scattered back into the NHWC tensor a patch
+ * operand reads; x (+ bias[n]) (ReLU), zeroed where mask <= 0 (bf16, output
+ * layout); FP32 or bf16.  splits > 1 splits K, split s writing its partial
+ * product at p + s * split_stride.  Device pointers, 16-byte aligned. */
+typedef struct {
+  const void *p;
+  long long ld;
+  int mode;
+  long long rows, kdim;
+  int Hin, Win, C, ps;
+} aldic_gemm_operand;
+typedef struct {
+  void *p;
+  long long ld;
+  int mode;
+  int fp32;
+  const float *bias;
+  int relu;
+  const void *mask;
+  int Hin, Win, C, ps;
+  long long M, N;
+  long long split_stride;
+} aldic_gemm_output;
+ALDIC_API int aldic_gemm_bf16(aldic_ctx *ctx, const aldic_gemm_operand *A,
+                              const aldic_gemm_operand *B, const aldic_gemm_output *D, int splits);
+
 /* One frame of main_ALDIC.m Sections 3-6 on the images set on the context:
  * the initial guess (integer search + MeshSetUp/Init, or one of the
  * sequence modes below), LocalICGN and its post-processing, beta selection,
