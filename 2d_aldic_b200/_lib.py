@@ -55,6 +55,15 @@ _SIGS = {
     "aldic_qt_fill": ([P, P, I32, P, P], I32),
     "aldic_icgn_flags": ([P, I64, P, D, P, P], I32),
     "aldic_gemm_bf16": ([P, P, P, P, I32], I32),
+    "aldic_cnn_create": ([I32, C.c_uint64, P], I32),
+    "aldic_cnn_destroy": ([P], I32),
+    "aldic_cnn_num_params": ([], I64),
+    "aldic_cnn_get_params": ([P, P], I32),
+    "aldic_cnn_set_params": ([P, P], I32),
+    "aldic_cnn_train_step": ([P, P, I32, P, I32, C.c_float, P, P, P, P], I32),
+    "aldic_cnn_predict": ([P, P, I32, I32, P, P], I32),
+    "aldic_cnn_patches": ([P, P, I64, I32, P], I32),
+    "aldic_cnn_to_init": ([P, P, I64, P, P, P], I32),
 }
 
 

@@ -884,6 +884,87 @@ class ALDICQuadtree:
                 "time_s": {"search_mesh": t_mesh - t0, "frame": t1 - t0}}
 
 
+# ------------------------------------------------------------------ learned init
+class InitNet:
+    """The learned initial guess's network (aldic_cnn_*): 64 x 64 reference /
+    deformed patch pairs -> [u/16, v/16, 20 du/dx, 20 dv/dx, 20 du/dy,
+    20 dv/dy, confidence logit, 0], trained and run on the GPU by the
+    library's own tcgen05 forward and backward kernels."""
+
+    TSCALE, GSCALE = 16.0, 20.0
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        call("aldic_cnn_create", int(device), C.c_uint64(seed), C.byref(h))
+        self.h, self.device = h, device
+        self.n_params = int(_lib.lib().aldic_cnn_num_params())
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().aldic_cnn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.n_params, np.float32)
+        call("aldic_cnn_get_params", self.h, _ptr(p))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(np.asarray(p, np.float32))
+        call("aldic_cnn_set_params", self.h, _ptr(p))
+
+    def save(self, path):
+        np.savez_compressed(path, params=self.get_params())
+
+    def load(self, path):
+        self.set_params(np.load(path)["params"])
+
+    @staticmethod
+    def _x(x):
+        bf = _is_cuda(x) and x.dtype == torch.bfloat16
+        return (x.contiguous() if _is_cuda(x) else np.ascontiguousarray(x, np.float32)), int(bf)
+
+    def train_step(self, x, targets, lr, stream=None, grads=False, outputs=False):
+        """One step on a batch; returns (loss, grads or None, outputs or None)."""
+        xx, bf = self._x(x)
+        B = xx.shape[0]
+        t = targets.contiguous() if _is_cuda(targets) else np.ascontiguousarray(targets, np.float32)
+        loss = C.c_double()
+        g = np.empty(self.n_params, np.float32) if grads else None
+        o = np.empty((B, 8), np.float32) if outputs else None
+        sh = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        call("aldic_cnn_train_step", self.h, _ptr(xx), bf, _ptr(t), B, float(lr), C.c_void_p(sh),
+             C.byref(loss), _ptr(g), _ptr(o))
+        return loss.value, g, o
+
+    def predict(self, x, stream=None, out=None):
+        xx, bf = self._x(x)
+        B = xx.shape[0]
+        if out is None:
+            out = (torch.empty((B, 8), dtype=torch.float32, device=xx.device) if _is_cuda(xx)
+                   else np.empty((B, 8), np.float32))
+        sh = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        call("aldic_cnn_predict", self.h, _ptr(xx), bf, B, C.c_void_p(sh), _ptr(out))
+        return out
+
+
+def cnn_patches(ctx: Context, coords, bf16=True):
+    """64 x 64 normalised patch pairs around the nodes (coords n x 2) from the
+    images set on ctx: a CUDA tensor n x 64 x 64 x 2."""
+    cf = _coords_cm(coords)
+    n = cf.shape[-1]
+    out = torch.empty((n, 64, 64, 2), dtype=torch.bfloat16 if bf16 else torch.float32,
+                      device=torch.device("cuda", ctx.device))
+    call("aldic_cnn_patches", ctx.h, _ptr(cf), n, int(bf16), _ptr(out))
+    return out
+
+
 class ALDICSequence:
     """The frame loop of main_ALDIC.m:53-147 over an image sequence, with
     every image and all state on the device.

@@ -932,6 +932,29 @@ int aldic_gemm_bf16(aldic_ctx *c, const aldic_gemm_operand *A, const aldic_gemm_
   return OK;
 }
 
+int aldic_cnn_patches(aldic_ctx *c, const double *coords, long long n, int bf16, void *out) {
+  ALDIC_CHECK(c && coords && out && n > 0, E_ARG, "cnn_patches: bad arguments");
+  ALDIC_CHECK(c->have_ref && c->have_def, E_STATE, "cnn_patches: set both images first");
+  ALDIC_CHECK(is_device_ptr(out), E_ARG, "cnn_patches: out must be device memory");
+  Guard g(c);
+  int rc;
+  Arg<double> ac;
+  if ((rc = arg_in(c, coords, 2 * n, ac))) return rc;
+  if ((rc = cnn_patches(c->f32.as<float>(), c->g32.as<float>(), c->W, c->H, ac.dev, n,
+                        bf16 ? out : nullptr, bf16 ? nullptr : (float *)out, c->stream)))
+    return rc;
+  return finish(c, ac.staged);
+}
+
+int aldic_cnn_to_init(aldic_ctx *c, const float *out, long long n, double *U0, double *F0,
+                      float *conf) {
+  ALDIC_CHECK(c && out && n > 0, E_ARG, "cnn_to_init: bad arguments");
+  Guard g(c);
+  int rc;
+  if ((rc = cnn_to_init(out, n, U0, F0, conf, c->stream))) return rc;
+  return finish(c, false);
+}
+
 int aldic_nodal_strain(aldic_ctx *c, int M, int N, double step, const double *U, double *F) {
   ALDIC_CHECK(c && U && F && M > 1 && N > 1 && step > 0, E_ARG, "nodal_strain: bad arguments");
   Guard g(c);

@@ -97,6 +97,10 @@ struct GemmDst {
 };
 int gemm_bf16(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, int *err,
               cudaStream_t st);
+// learned initial guess (cnn.cu)
+int cnn_patches(const float *f, const float *g, int W, int H, const double *coords, long long n,
+                void *bf16_out, float *f32_out, cudaStream_t st);
+int cnn_to_init(const float *out, long long n, double *U0, double *F0, float *conf, cudaStream_t st);
 
 // solve op(x) = b for nrhs fields; b and x live in w.b / w.x (field-major)
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,

@@ -274,6 +274,42 @@ typedef struct {
 ALDIC_API int aldic_gemm_bf16(aldic_ctx *ctx, const aldic_gemm_operand *A,
                               const aldic_gemm_operand *B, const aldic_gemm_output *D, int splits);
 
+/* ---- Learned initial guess (no counterpart in the reference; its
+ * data-driven guess is POD-GPR over earlier frames) ----
+ * A patch network on a reference / deformed 64 x 64 patch pair: 4x4, 2x2,
+ * 2x2 non-overlapping patch layers (64, 128, 256 channels), a 4096 -> 256
+ * dense layer (all bf16 on the tcgen05 GEMM, FP32 accumulation, ReLU) and a
+ * 256 -> 8 FP32 output: [u/16, v/16, 20 du/dx, 20 dv/dx, 20 du/dy,
+ * 20 dv/dy, confidence logit, 0].  Inputs x: B x 64 x 64 x 2 (channel 0 the
+ * reference patch, 1 the deformed one), FP32 (host or device) or bf16
+ * (device).  Parameters: 1 217 224 FP32 values, blocks W1 b1 .. W5 b5, Wl
+ * row-major [out x in] with the patch index order (di, dj, c). */
+typedef struct aldic_cnn aldic_cnn;
+ALDIC_API int aldic_cnn_create(int device, unsigned long long seed, aldic_cnn **out);
+ALDIC_API int aldic_cnn_destroy(aldic_cnn *net);
+ALDIC_API long long aldic_cnn_num_params(void);
+ALDIC_API int aldic_cnn_get_params(aldic_cnn *net, float *params);
+ALDIC_API int aldic_cnn_set_params(aldic_cnn *net, const float *params);
+/* One training step on B pairs with targets (B x 6, the first six outputs'
+ * scaling): forward, loss (squared error + confidence cross-entropy against
+ * "translation within 0.5 px"), backward, and an Adam step when lr > 0.
+ * Optional outputs: loss, grads (n_params), out (B x 8). */
+ALDIC_API int aldic_cnn_train_step(aldic_cnn *net, const void *x, int x_bf16, const float *targets,
+                                   int B, float lr, void *stream, double *loss, float *grads,
+                                   float *out);
+ALDIC_API int aldic_cnn_predict(aldic_cnn *net, const void *x, int x_bf16, int B, void *stream,
+                                float *out);
+/* 64 x 64 patch pairs around n nodes (coords n x 2 column-major, 1-based)
+ * from the context's normalised images, each patch normalised to zero mean
+ * and unit deviation; out: n x 64 x 64 x 2, bf16 (bf16 = 1) or FP32 device
+ * array. */
+ALDIC_API int aldic_cnn_patches(aldic_ctx *ctx, const double *coords, long long n, int bf16,
+                                void *out);
+/* U0 (2n), F0 (4n, [F11 F21 F12 F22]) and confidence (n) from network
+ * outputs (n x 8); any output may be NULL.  Device arrays. */
+ALDIC_API int aldic_cnn_to_init(aldic_ctx *ctx, const float *out, long long n, double *U0,
+                                double *F0, float *conf);
+
 /* One frame of main_ALDIC.m Sections 3-6 on the images set on the context:
  * the initial guess (integer search + MeshSetUp/Init, or one of the
  * sequence modes below), LocalICGN and its post-processing, beta selection,
