@@ -336,7 +336,10 @@ int aldic_ctx_create(int device, aldic_ctx **out) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // a blocking stream: ordered with the legacy default stream, so device
+  // arrays produced there (by the caller's other libraries) are complete
+  // before the context reads them, and vice versa
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess) {
     cudaSetDevice(prev);
     delete c;
     set_error("ctx_create: stream creation failed");

@@ -72,7 +72,10 @@ ALDIC_API int aldic_ba_interp2_f32(const float *F, int64_t M, int64_t N, int64_t
                          void *stream);
 
 /* Context: device-resident images, gradients and work buffers that persist
- * across calls (the MEX side keeps one per MATLAB session: mexLock/mexAtExit). */
+ * across calls (the MEX side keeps one per MATLAB session: mexLock/mexAtExit).
+ * Its own stream is a blocking stream (ordered with the legacy default
+ * stream); callers that produce or consume device arrays on other streams
+ * pass their stream with aldic_ctx_set_stream. */
 ALDIC_API int aldic_ctx_create(int device, aldic_ctx **out);
 ALDIC_API int aldic_ctx_destroy(aldic_ctx *ctx);
 ALDIC_API int aldic_ctx_set_stream(aldic_ctx *ctx, void *stream);
