@@ -54,6 +54,8 @@ _SIGS = {
     "aldic_qt_nodal_strain": ([P, P, P, P], I32),
     "aldic_qt_fill": ([P, P, I32, P, P], I32),
     "aldic_icgn_flags": ([P, I64, P, D, P, P], I32),
+    "aldic_subpb2_fd": ([P, I32, I32, D, D, D, P, P, P, P, P], I32),
+    "aldic_fd_strain": ([P, I32, I32, D, P, P], I32),
     "aldic_gemm_bf16": ([P, P, P, P, I32], I32),
     "aldic_cnn_create": ([I32, C.c_uint64, P], I32),
     "aldic_cnn_destroy": ([P], I32),
@@ -71,7 +73,7 @@ class FrameParams(C.Structure):
     _fields_ = [("winsize", I32), ("step", I32), ("search", I32 * 2), ("gridx", I32 * 2),
                 ("gridy", I32 * 2), ("tol", D), ("mu", D), ("beta", D), ("n_admm", I32),
                 ("tol2", D), ("precision", I32), ("smooth", I32), ("use_graph", I32),
-                ("init", I32)]
+                ("init", I32), ("subpb2_fd", I32)]
 
 
 class GemmOperand(C.Structure):

@@ -496,6 +496,27 @@ def Subpb2(DICmesh, beta, mu, U, F, udual, vdual, alpha=0, GaussPtOrder=2):
     return out
 
 
+def subpb2_fd(M, N, winstepsize, beta, mu, U, F, udual, vdual, ctx: Context | None = None):
+    """The finite-difference Subproblem 2 of main_ALDIC.m:243-259 (interior
+    nodes solve (beta D'D + mu I) x = beta D'(F - udual) + mu (U - vdual),
+    D = funDerivativeOp of the interior grid; border nodes keep U)."""
+    ctx = ctx or _ctx_for(U)
+    Ua, Fa, ua, va = _prep(U), _prep(F), _prep(udual), _prep(vdual)
+    out = _empty(_first_cuda(Ua), (2 * M * N,))
+    call("aldic_subpb2_fd", ctx.h, int(M), int(N), float(winstepsize), float(beta), float(mu),
+         _ptr(Ua), _ptr(Fa), _ptr(ua), _ptr(va), _ptr(out))
+    return out
+
+
+def fd_strain(M, N, winstepsize, U, ctx: Context | None = None):
+    """F = funDerivativeOp(M, N, winstepsize) * U (main_ALDIC.m:259)."""
+    ctx = ctx or _ctx_for(U)
+    Ua = _prep(U)
+    out = _empty(_first_cuda(Ua), (4 * M * N,))
+    call("aldic_fd_strain", ctx.h, int(M), int(N), float(winstepsize), _ptr(Ua), _ptr(out))
+    return out
+
+
 def funGlobal_NodalStrainAvg(coordinatesFEM, elementsFEM, U, GaussPtOrder=2):
     """StrainNodalPt = funGlobal_NodalStrainAvg(coordinatesFEM,elementsFEM,U,
     GaussPtOrder) -- funGlobal_NodalStrainAvg.m:1 on the uniform mesh."""
@@ -556,7 +577,7 @@ class ALDIC:
 
     def __init__(self, winsize, step, search, tol=1e-2, mu=1e-3, beta=0.0, n_admm=3,
                  precision=FP32, smooth=False, gridx=(0, 0), gridy=(0, 0), use_graph=True,
-                 device=None, ctx: Context | None = None):
+                 device=None, ctx: Context | None = None, subpb2: str = "fe"):
         self.ctx = ctx or default_context(device)
         p = FrameParams()
         p.winsize, p.step = int(winsize), int(step)
@@ -567,6 +588,9 @@ class ALDIC:
         p.tol, p.mu, p.beta, p.n_admm = float(tol), float(mu), float(beta), int(n_admm)
         p.tol2 = 0.0
         p.precision, p.smooth, p.use_graph = int(precision), int(bool(smooth)), int(bool(use_graph))
+        if subpb2 not in ("fe", "fd"):
+            raise ValueError("subpb2 must be 'fe' (Subpb2.m) or 'fd' (finite differences)")
+        p.subpb2_fd = int(subpb2 == "fd")
         self.p = p
 
     def set_images(self, f=None, g=None, roi=None, mask=None):

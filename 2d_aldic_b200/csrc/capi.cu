@@ -958,6 +958,40 @@ int aldic_cnn_to_init(aldic_ctx *c, const float *out, long long n, double *U0, d
   return finish(c, false);
 }
 
+int aldic_subpb2_fd(aldic_ctx *c, int M, int N, double step, double beta, double mu,
+                    const double *U, const double *F, const double *udual, const double *vdual,
+                    double *Uhat) {
+  ALDIC_CHECK(c && U && F && udual && vdual && Uhat && M >= 4 && N >= 4 && step > 0, E_ARG,
+              "subpb2_fd: bad arguments (the node grid needs at least 4 x 4 nodes)");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  if ((rc = ensure_grid_work(c, n))) return rc;
+  Arg<double> au, af, aud, avd, ao;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_in(c, F, 4 * n, af)) ||
+      (rc = arg_in(c, udual, 4 * n, aud)) || (rc = arg_in(c, vdual, 2 * n, avd)) ||
+      (rc = arg_out(c, Uhat, 2 * n, ao)))
+    return rc;
+  if ((rc = fd_rhs(c->gw, M, N, step, beta, mu, au.dev, af.dev, aud.dev, avd.dev, c->stream)) ||
+      (rc = grid_pcg(c->gw, OP_FD, M - 2, N - 2, 2, beta, mu, step, 0, kRtolFE, kMaxitFE, c->stream)) ||
+      (rc = fd_store(c->gw, M, N, au.dev, ao.dev, c->stream)))
+    return rc;
+  arg_back(c, ao);
+  return check_grid_err(c);
+}
+
+int aldic_fd_strain(aldic_ctx *c, int M, int N, double step, const double *U, double *F) {
+  ALDIC_CHECK(c && U && F && M >= 2 && N >= 2 && step > 0, E_ARG, "fd_strain: bad arguments");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  Arg<double> au, af;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_out(c, F, 4 * n, af))) return rc;
+  if ((rc = fd_strain(M, N, step, au.dev, af.dev, c->stream))) return rc;
+  arg_back(c, af);
+  return finish(c, af.staged || au.staged);
+}
+
 int aldic_nodal_strain(aldic_ctx *c, int M, int N, double step, const double *U, double *F) {
   ALDIC_CHECK(c && U && F && M > 1 && N > 1 && step > 0, E_ARG, "nodal_strain: bad arguments");
   Guard g(c);
@@ -1114,7 +1148,10 @@ __global__ void k_scale_store(const double *src, double *dst, double s) { *dst =
 
 // main_ALDIC.m:285-301: beta from the sweep (device-side so the frame stays
 // capturable); err[0..5] = Err1, err[6..11] = Err2, betas on the fly
-__global__ void k_beta_select(const double *err, double base, double *beta_out) {
+// beta from the sweep: FE (fd_h = 0) the normalised error sum of
+// main_ALDIC.m:293-301, FD (fd_h = step) Err1 + Err2 step^2 of :262-269; then
+// the three-point parabola vertex in log10(beta)
+__global__ void k_beta_select(const double *err, double base, double *beta_out, double fd_h) {
   const double bl[6] = {1e-3, 3.1622776601683795e-3, 1e-2, 3.1622776601683794e-2, 1e-1,
                         3.1622776601683794e-1};
   double bs[6], e1[6], e2[6];
@@ -1132,7 +1169,7 @@ __global__ void k_beta_select(const double *err, double base, double *beta_out) 
   double es[6];
   int ib = 0;
   for (int k = 0; k < 6; ++k) {
-    es[k] = (e1[k] - m1) / v1 + (e2[k] - m2) / v2;
+    es[k] = fd_h > 0 ? e1[k] + e2[k] * fd_h * fd_h : (e1[k] - m1) / v1 + (e2[k] - m2) / v2;
     if (es[k] < es[ib]) ib = k;
   }
   double beta;
@@ -1234,6 +1271,31 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F1))) return rc;
   k_zero<<<nb, 256, 0, st>>>(B.udual, 4 * n);
   k_zero<<<nb, 256, 0, st>>>(B.vdual, 2 * n);
+  // Subproblem 2 on the FE mesh (Subpb2.m) or by finite differences on the
+  // interior nodes (main_ALDIC.m:243-278): solve into fields f0, f0 + 1,
+  // store U2, strain F2
+  const bool fd = p->subpb2_fd != 0;
+  auto rhs = [&](double beta, const double *beta_ptr, int f0) {
+    return fd ? fd_rhs(c->gw, M, N, h, beta, mu, B.U1, B.F1, B.udual, B.vdual, st, beta_ptr, f0)
+              : fe_rhs(c->gw, M, N, h, beta, mu, B.U1, B.F1, B.udual, B.vdual, st, beta_ptr, f0);
+  };
+  auto pcg = [&](int nr, const double *beta_ptr, const double *beta_each) {
+    return fd ? grid_pcg(c->gw, OP_FD, M - 2, N - 2, nr, 0, mu, h, 0, kRtolFE, kMaxitFE, st,
+                         beta_ptr, beta_each)
+              : grid_pcg(c->gw, OP_FE, M, N, nr, 0, mu, h, 0, kRtolFE, kMaxitFE, st, beta_ptr,
+                         beta_each);
+  };
+  auto store = [&](int f0) {
+    return fd ? fd_store(c->gw, M, N, B.U1, B.U2, st, f0) : fe_store(c->gw, M, N, B.U2, st, f0);
+  };
+  auto strain = [&]() {
+    return fd ? fd_strain(M, N, h, B.U2, B.F2, st) : nodal_strain(M, N, h, B.U2, B.F2, st);
+  };
+  auto dual = [&](int accumulate) {
+    if (fd) return fd_dual(M, N, B.F2, B.F1, B.U2, B.U1, B.udual, B.vdual, accumulate, st);
+    int r = vsub(B.F2, B.F1, B.udual, 4 * n, st);
+    return r ? r : vsub(B.U2, B.U1, B.vdual, 2 * n, st);
+  };
   if (p->beta > 0) {
     k_set1<<<1, 1, 0, st>>>(B.beta, p->beta);
   } else {
@@ -1242,28 +1304,22 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     double be[12];
     for (int k = 0; k < 6; ++k) {
       be[2 * k] = be[2 * k + 1] = bl[k] * base;
-      if ((rc = fe_rhs(c->gw, M, N, h, bl[k] * base, mu, B.U1, B.F1, B.udual, B.vdual, st,
-                       nullptr, 2 * k)))
-        return rc;
+      if ((rc = rhs(bl[k] * base, nullptr, 2 * k))) return rc;
     }
     // the six systems of the sweep in one launch (12 right-hand sides)
-    if ((rc = grid_pcg(c->gw, OP_FE, M, N, 12, 0, mu, h, 0, kRtolFE, kMaxitFE, st, nullptr, be)))
-      return rc;
+    if ((rc = pcg(12, nullptr, be))) return rc;
     for (int k = 0; k < 6; ++k) {
-      if ((rc = fe_store(c->gw, M, N, B.U2, st, 2 * k))) return rc;
-      if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
+      if ((rc = store(2 * k))) return rc;
+      if ((rc = strain())) return rc;
       if ((rc = vdiffnorm(B.U1, B.U2, 2 * n, B.part, B.err + k, st))) return rc;
       if ((rc = vdiffnorm(B.F1, B.F2, 4 * n, B.part, B.err + 6 + k, st))) return rc;
     }
-    k_beta_select<<<1, 1, 0, st>>>(B.err, base, B.beta);
+    k_beta_select<<<1, 1, 0, st>>>(B.err, base, B.beta, fd ? h : 0.0);
   }
-  if ((rc = fe_rhs(c->gw, M, N, h, 0, mu, B.U1, B.F1, B.udual, B.vdual, st, B.beta))) return rc;
-  if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, 0, mu, h, 0, kRtolFE, kMaxitFE, st, B.beta))) return rc;
-  if ((rc = fe_store(c->gw, M, N, B.U2, st))) return rc;
-  if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
+  if ((rc = rhs(0, B.beta, 0)) || (rc = pcg(2, B.beta, nullptr)) || (rc = store(0)) || (rc = strain()))
+    return rc;
   if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F2))) return rc;
-  if ((rc = vsub(B.F2, B.F1, B.udual, 4 * n, st))) return rc;
-  if ((rc = vsub(B.U2, B.U1, B.vdual, 2 * n, st))) return rc;
+  if ((rc = dual(0))) return rc;
   ALDIC_CUDA(cudaMemcpyAsync(B.U1old, B.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
   // Section 6: ADMM iterations
   if ((rc = mark(c, 5))) return rc;
@@ -1283,18 +1339,15 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     }
     ALDIC_CUDA(cudaMemcpyAsync(B.U1old, B.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
     if (p->smooth && (rc = smooth_dev(c, M, N, 2, B.U1))) return rc;
-    if ((rc = fe_rhs(c->gw, M, N, h, 0, mu, B.U1, B.F1, B.udual, B.vdual, st, B.beta))) return rc;
-    if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, 0, mu, h, 0, kRtolFE, kMaxitFE, st, B.beta))) return rc;
-    if ((rc = fe_store(c->gw, M, N, B.U2, st))) return rc;
+    if ((rc = rhs(0, B.beta, 0)) || (rc = pcg(2, B.beta, nullptr)) || (rc = store(0))) return rc;
     if (p->smooth && (rc = smooth_dev(c, M, N, 2, B.U2))) return rc;
-    if ((rc = nodal_strain(M, N, h, B.U2, B.F2, st))) return rc;
+    if ((rc = strain())) return rc;
     if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F2))) return rc;
     if (a < 16) {
       if ((rc = vdiffnorm(B.U2old, B.U2, 2 * n, B.part, B.upd + a, st))) return rc;
       k_scale_store<<<1, 1, 0, st>>>(B.upd + a, B.upd + a, inv);
     }
-    if ((rc = vsub(B.F2, B.F1, B.udual, 4 * n, st))) return rc;
-    if ((rc = vsub(B.U2, B.U1, B.vdual, 2 * n, st))) return rc;
+    if ((rc = dual(1))) return rc;   // FE resets the duals, FD accumulates (main_ALDIC.m:434-441)
   }
   // sequence history: U(k-2) <- U(k-1) <- this frame's U
   ALDIC_CUDA(cudaMemcpyAsync(hist + 2 * n, hist, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
@@ -1384,7 +1437,8 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   char key[512];
   snprintf(key, sizeof key, "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p",
            c->W, c->H, c->dtype, p->winsize, p->step, p->search[0], p->search[1], gx[0], gx[1],
-           gy[0], gy[1], p->tol, p->mu, p->beta, p->n_admm, p->precision, p->smooth, p->init,
+           gy[0], gy[1], p->tol, p->mu, p->beta, p->n_admm, p->precision, p->smooth,
+           p->init * 2 + (p->subpb2_fd != 0),
            c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p);
   if (realloc) c->drop_graphs();  // recorded against buffers that are gone
   const bool want_graph = p->use_graph && !c->graph_failed;

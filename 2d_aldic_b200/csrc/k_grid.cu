@@ -55,6 +55,48 @@ __device__ __forceinline__ int ecnt(int i, int di, int M) {
   return di == 0 ? (i >= 1) + (i <= M - 2) : (di > 0 ? (i <= M - 2) : (i >= 1));
 }
 
+// funDerivativeOp.m:25-35 along one line of n nodes: 2h times the weight of
+// x_s in the difference at t (central inside, one-sided doubled at the ends)
+__device__ __forceinline__ double fdc(int t, int s, int n) {
+  if (t == 0) return s == 1 ? 2.0 : (s == 0 ? -2.0 : 0.0);
+  if (t == n - 1) return s == n - 1 ? 2.0 : (s == n - 2 ? -2.0 : 0.0);
+  return s == t + 1 ? 1.0 : (s == t - 1 ? -1.0 : 0.0);
+}
+
+// (D'D v) along one line through node index c of a line with n nodes,
+// stride st between line neighbours (scaled by 4 h^2)
+__device__ __forceinline__ double fd_dtd(const double *__restrict__ v, long long k, int c, int n,
+                                         long long st) {
+  double y = 0.0;
+#pragma unroll
+  for (int dt = -1; dt <= 1; ++dt) {
+    const int t = c + dt;
+    if (t < 0 || t >= n) continue;
+    const double w = fdc(t, c, n);
+    if (w == 0.0) continue;
+    double d = 0.0;
+#pragma unroll
+    for (int ds = -1; ds <= 1; ++ds) {
+      const int s = t + ds;
+      if (s < 0 || s >= n) continue;
+      const double ws = fdc(t, s, n);
+      if (ws != 0.0) d += ws * v[k + (long long)(s - c) * st];
+    }
+    y += w * d;
+  }
+  return y;
+}
+
+__device__ __forceinline__ double fd_diag1(int c, int n) {
+  double y = 0.0;
+  for (int t = c - 1; t <= c + 1; ++t)
+    if (t >= 0 && t < n) {
+      const double w = fdc(t, c, n);
+      y += w * w;
+    }
+  return y;
+}
+
 template <int OP>
 __device__ __forceinline__ double op_diag(const PcgArgs &A, double beta, int i, int j,
                                           long long k, int f) {
@@ -62,6 +104,8 @@ __device__ __forceinline__ double op_diag(const PcgArgs &A, double beta, int i, 
   if (OP == OP_FE) {
     const double kc = beta * (4.0 / 6.0) + A.mu * A.h * A.h * (4.0 / 36.0);
     return ecnt(i, 0, M) * ecnt(j, 0, N) * kc;
+  } else if (OP == OP_FD) {
+    return beta * (fd_diag1(i, M) + fd_diag1(j, N)) / (4.0 * A.h * A.h) + A.mu;
   } else if (OP == OP_CSR) {
     return A.mask[(long long)f * M * N + k] ? A.csr.diag[k] : 1.0;
   } else if (OP == OP_GRIDFIT) {
@@ -100,6 +144,8 @@ __device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i,
       }
     }
     return y;
+  } else if (OP == OP_FD) {
+    return beta * (fd_dtd(v, k, i, M, 1) + fd_dtd(v, k, j, N, M)) / (4.0 * A.h * A.h) + A.mu * v[k];
   } else if (OP == OP_CSR) {
     const unsigned char *fr = A.mask + (long long)f * M * N;
     if (!fr[k]) return v[k];
@@ -370,6 +416,115 @@ __global__ void k_fe_rhs(int M, int N, double h, double beta, const double *beta
       }
     b[k] = bu;
     b[n + k] = bv;
+  }
+}
+
+// beta D'a + mu b on the interior grid (Mi = M - 2, Ni = N - 2); a = F - udual,
+// b = U - vdual at the interior nodes of the full M x N grid; x starts at U
+__global__ void k_fd_rhs(int M, int N, double h, double beta, const double *beta_ptr, double mu,
+                         const double *__restrict__ U, const double *__restrict__ F,
+                         const double *__restrict__ ud, const double *__restrict__ vd,
+                         double *__restrict__ b, double *__restrict__ x,
+                         unsigned char *__restrict__ mask) {
+  if (beta_ptr) beta = *beta_ptr;
+  const int Mi = M - 2, Ni = N - 2;
+  const long long ni = (long long)Mi * Ni;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ni;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % Mi), j = (int)(k / Mi);
+    // D' a: x-differences of the F11 / F21 slots, y-differences of F12 / F22
+    double au = 0.0, av = 0.0;
+    for (int t = i - 1; t <= i + 1; ++t) {
+      if (t < 0 || t >= Mi) continue;
+      const double w = fdc(t, i, Mi);
+      if (w == 0.0) continue;
+      const long long q = (long long)(j + 1) * M + (t + 1);
+      au += w * (F[4 * q + 0] - ud[4 * q + 0]);
+      av += w * (F[4 * q + 1] - ud[4 * q + 1]);
+    }
+    for (int t = j - 1; t <= j + 1; ++t) {
+      if (t < 0 || t >= Ni) continue;
+      const double w = fdc(t, j, Ni);
+      if (w == 0.0) continue;
+      const long long q = (long long)(t + 1) * M + (i + 1);
+      au += w * (F[4 * q + 2] - ud[4 * q + 2]);
+      av += w * (F[4 * q + 3] - ud[4 * q + 3]);
+    }
+    const long long q = (long long)(j + 1) * M + (i + 1);
+    b[k] = beta * au / (2.0 * h) + mu * (U[2 * q] - vd[2 * q]);
+    b[ni + k] = beta * av / (2.0 * h) + mu * (U[2 * q + 1] - vd[2 * q + 1]);
+    x[k] = U[2 * q];
+    x[ni + k] = U[2 * q + 1];
+    mask[k] = 1;
+    mask[ni + k] = 1;
+  }
+}
+
+__global__ void k_fd_store(int M, int N, const double *__restrict__ x, const double *__restrict__ U1,
+                           double *__restrict__ U2) {
+  const long long n = (long long)M * N, ni = (long long)(M - 2) * (N - 2);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    if (i >= 1 && i <= M - 2 && j >= 1 && j <= N - 2) {
+      const long long q = (long long)(j - 1) * (M - 2) + (i - 1);
+      U2[2 * k] = x[q];
+      U2[2 * k + 1] = x[ni + q];
+    } else {
+      U2[2 * k] = U1[2 * k];
+      U2[2 * k + 1] = U1[2 * k + 1];
+    }
+  }
+}
+
+// F = D2 U (funDerivativeOp(M, N, h) * U): [du/dx dv/dx du/dy dv/dy]
+__global__ void k_fd_strain(int M, int N, double h, const double *__restrict__ U,
+                            double *__restrict__ F) {
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    double ux = 0, vx = 0, uy = 0, vy = 0;
+    for (int s = i - 1; s <= i + 1; ++s) {
+      if (s < 0 || s >= M) continue;
+      const double w = fdc(i, s, M);
+      if (w == 0.0) continue;
+      const long long q = (long long)j * M + s;
+      ux += w * U[2 * q];
+      vx += w * U[2 * q + 1];
+    }
+    for (int s = j - 1; s <= j + 1; ++s) {
+      if (s < 0 || s >= N) continue;
+      const double w = fdc(j, s, N);
+      if (w == 0.0) continue;
+      const long long q = (long long)s * M + i;
+      uy += w * U[2 * q];
+      vy += w * U[2 * q + 1];
+    }
+    const double c = 1.0 / (2.0 * h);
+    F[4 * k + 0] = ux * c;
+    F[4 * k + 1] = vx * c;
+    F[4 * k + 2] = uy * c;
+    F[4 * k + 3] = vy * c;
+  }
+}
+
+__global__ void k_fd_dual(int M, int N, const double *__restrict__ F2, const double *__restrict__ F1,
+                          const double *__restrict__ U2, const double *__restrict__ U1,
+                          double *__restrict__ ud, double *__restrict__ vd, int accumulate) {
+  const long long n = (long long)M * N;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    const bool in = i >= 1 && i <= M - 2 && j >= 1 && j <= N - 2;
+    for (int c = 0; c < 4; ++c) {
+      const double d = in ? F2[4 * k + c] - F1[4 * k + c] : 0.0;
+      ud[4 * k + c] = accumulate ? ud[4 * k + c] + d : d;
+    }
+    for (int c = 0; c < 2; ++c) {
+      const double d = in ? U2[2 * k + c] - U1[2 * k + c] : 0.0;
+      vd[2 * k + c] = accumulate ? vd[2 * k + c] + d : d;
+    }
   }
 }
 
@@ -664,6 +819,7 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
     default: fn = (void *)k_pcg<OPV, 12>; break;                                  \
   }
   if (op == OP_FE) { ALDIC_PCG_FN(OP_FE) }
+  else if (op == OP_FD) { ALDIC_PCG_FN(OP_FD) }
   else if (op == OP_GRIDFIT) { ALDIC_PCG_FN(OP_GRIDFIT) }
   else { ALDIC_PCG_FN(OP_INPAINT) }
 #undef ALDIC_PCG_FN
@@ -745,6 +901,38 @@ int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const do
   k_fe_rhs<<<blocks_for(n), 256, 0, st>>>(M, N, h, beta, beta_ptr, mu, U, F, udual, vdual,
                                           w.b + f0 * n);
   k_fe_init<<<blocks_for(2 * n), 256, 0, st>>>(2 * n, w.x + f0 * n, w.mask + f0 * n);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int fd_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
+           const double *F, const double *udual, const double *vdual, cudaStream_t st,
+           const double *beta_ptr, int f0) {
+  ALDIC_CHECK(M >= 4 && N >= 4, E_ARG, "FD Subpb2: the node grid needs at least 4 x 4 nodes");
+  const long long ni = (long long)(M - 2) * (N - 2);
+  k_fd_rhs<<<blocks_for(ni), 256, 0, st>>>(M, N, h, beta, beta_ptr, mu, U, F, udual, vdual,
+                                          w.b + f0 * ni, w.x + f0 * ni, w.mask + f0 * ni);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int fd_store(const GridWork &w, int M, int N, const double *U1, double *U2, cudaStream_t st, int f0) {
+  const long long ni = (long long)(M - 2) * (N - 2);
+  k_fd_store<<<blocks_for((long long)M * N), 256, 0, st>>>(M, N, w.x + f0 * ni, U1, U2);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int fd_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st) {
+  k_fd_strain<<<blocks_for((long long)M * N), 256, 0, st>>>(M, N, h, U, F);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int fd_dual(int M, int N, const double *F2, const double *F1, const double *U2, const double *U1,
+            double *udual, double *vdual, int accumulate, cudaStream_t st) {
+  k_fd_dual<<<blocks_for((long long)M * N), 256, 0, st>>>(M, N, F2, F1, U2, U1, udual, vdual,
+                                                         accumulate);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

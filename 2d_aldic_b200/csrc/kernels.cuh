@@ -51,7 +51,23 @@ struct GridWork {
   int *iters_out;        // PCG iterations used
   int max_blocks;
 };
-enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2, OP_CSR = 3 };
+enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2, OP_CSR = 3, OP_FD = 4 };
+
+// Finite-difference Subproblem 2 (funDerivativeOp.m, main_ALDIC.m:243-278):
+// (beta D'D + mu I) x = beta D' a + mu b on the interior (M-2) x (N-2) nodes,
+// D central differences with the reference's one-sided borders.
+int fd_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
+           const double *F, const double *udual, const double *vdual, cudaStream_t st,
+           const double *beta_ptr = nullptr, int f0 = 0);
+// U2 = U1 with the interior replaced by the solution of fields f0, f0 + 1
+int fd_store(const GridWork &w, int M, int N, const double *U1, double *U2, cudaStream_t st,
+             int f0 = 0);
+// F = D2 U on the full M x N grid, slots [du/dx dv/dx du/dy dv/dy]
+int fd_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st);
+// FD dual update on the interior nodes (main_ALDIC.m:334-338, 434-438):
+// reset (accumulate = 0: zero elsewhere) or accumulate
+int fd_dual(int M, int N, const double *F2, const double *F1, const double *U2, const double *U1,
+            double *udual, double *vdual, int accumulate, cudaStream_t st);
 
 // A symmetric sparse operator for the PCG: CSR rows of n nodes (sorted
 // columns), its diagonal, shared by every field.  Rows whose field mask is 0

@@ -174,6 +174,17 @@ ALDIC_API int aldic_subpb2_noalloc(int M, int N, double step, double beta, doubl
                                    const double *U, const double *F, const double *udual,
                                    const double *vdual, double *Uhat, void *stream);
 
+/* Finite-difference Subproblem 2 (main_ALDIC.m:243-278, funDerivativeOp.m):
+ * the interior (M-2) x (N-2) nodes solve (beta D'D + mu I) x = beta D'(F -
+ * udual) + mu (U - vdual) with D the central differences of
+ * funDerivativeOp.m (one-sided at the interior grid's edges); the border
+ * nodes keep U.  PCG to relative residual 1e-11 replaces the direct solve. */
+ALDIC_API int aldic_subpb2_fd(aldic_ctx *ctx, int M, int N, double step, double beta, double mu,
+                              const double *U, const double *F, const double *udual,
+                              const double *vdual, double *Uhat);
+/* F = funDerivativeOp(M, N, step) * U: [du/dx dv/dx du/dy dv/dy] per node. */
+ALDIC_API int aldic_fd_strain(aldic_ctx *ctx, int M, int N, double step, const double *U, double *F);
+
 /* funGlobal_NodalStrainAvg.m:1 on the uniform mesh (2x2 Gauss points,
  * extrapolation to the nodes, average over elements).  Output slots per node
  * are [du/dx du/dy dv/dx dv/dy], the order funGlobal_NodalStrainAvg.m:97,
@@ -350,6 +361,7 @@ typedef struct {
   int smooth;               /* 1: funSmoothDisp/funSmoothStrain as main_ALDIC */
   int use_graph;            /* 1: capture/replay the device work as a CUDA graph */
   int init;                 /* ALDIC_INIT_* */
+  int subpb2_fd;            /* 1: finite-difference Subproblem 2 (DICpara.Subpb2FDOrFEM = 1) */
 } aldic_frame_params;
 
 typedef struct {
