@@ -56,7 +56,7 @@ _SIGS = {
     "aldic_icgn_flags": ([P, I64, P, D, P, P], I32),
     "aldic_subpb2_fd": ([P, I32, I32, D, D, D, P, P, P, P, P], I32),
     "aldic_fd_strain": ([P, I32, I32, D, P, P], I32),
-    "aldic_gemm_bf16": ([P, P, P, P, I32], I32),
+    "aldic_gemm_bf16": ([P, P, P, P, I32, I32], I32),
     "aldic_cnn_create": ([I32, C.c_uint64, P], I32),
     "aldic_cnn_destroy": ([P], I32),
     "aldic_cnn_num_params": ([], I64),
@@ -78,13 +78,13 @@ class FrameParams(C.Structure):
 
 class GemmOperand(C.Structure):
     _fields_ = [("p", P), ("ld", I64), ("mode", I32), ("rows", I64), ("kdim", I64),
-                ("Hin", I32), ("Win", I32), ("C", I32), ("ps", I32)]
+                ("Hin", I32), ("Win", I32), ("C", I32), ("ps", I32), ("bstride", I64)]
 
 
 class GemmOutput(C.Structure):
     _fields_ = [("p", P), ("ld", I64), ("mode", I32), ("fp32", I32), ("bias", P), ("relu", I32),
                 ("mask", P), ("Hin", I32), ("Win", I32), ("C", I32), ("ps", I32), ("M", I64),
-                ("N", I64), ("split_stride", I64)]
+                ("N", I64), ("split_stride", I64), ("scale", C.c_float), ("bstride", I64)]
 
 
 class FrameStats(C.Structure):

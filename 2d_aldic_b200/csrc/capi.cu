@@ -906,11 +906,12 @@ static GemmSrc gemm_src(const aldic_gemm_operand &o) {
   s.p = (const __nv_bfloat16 *)o.p;
   s.ld = o.ld; s.mode = o.mode; s.rows = o.rows; s.kdim = o.kdim;
   s.Hin = o.Hin; s.Win = o.Win; s.C = o.C; s.ps = o.ps;
+  s.bstride = o.bstride;
   return s;
 }
 
 int aldic_gemm_bf16(aldic_ctx *c, const aldic_gemm_operand *A, const aldic_gemm_operand *B,
-                    const aldic_gemm_output *D, int splits) {
+                    const aldic_gemm_output *D, int splits, int batches) {
   ALDIC_CHECK(c && A && B && D, E_ARG, "gemm: null argument");
   ALDIC_CHECK(A->mode >= 0 && A->mode <= 3 && B->mode >= 0 && B->mode <= 3 &&
                   (D->mode == 0 || D->mode == 1),
@@ -923,7 +924,9 @@ int aldic_gemm_bf16(aldic_ctx *c, const aldic_gemm_operand *A, const aldic_gemm_
   d.mask = (const __nv_bfloat16 *)D->mask;
   d.Hin = D->Hin; d.Win = D->Win; d.C = D->C; d.ps = D->ps; d.M = D->M; d.N = D->N;
   d.split_stride = D->split_stride;
-  if ((rc = gemm_bf16(gemm_src(*A), gemm_src(*B), d, splits, c->gw.err, c->stream))) return rc;
+  d.scale = D->scale == 0.f ? 1.f : D->scale;
+  d.bstride = D->bstride;
+  if ((rc = gemm_bf16(gemm_src(*A), gemm_src(*B), d, splits, c->gw.err, c->stream, batches))) return rc;
   int err = 0;
   ALDIC_CUDA(cudaMemcpyAsync(&err, c->gw.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   ALDIC_CUDA(cudaStreamSynchronize(c->stream));

@@ -1,19 +1,21 @@
-// cnn.cu -- the learned initial guess: a patch network that maps a
+// cnn.cu -- the learned initial guess: a Siamese patch network that maps a
 // reference / deformed 64 x 64 patch pair to the six affine warp parameters
 // of the subset at its centre plus a confidence logit.  No counterpart in the
 // reference (its data-driven guess is POD-GPR over earlier frames).
 //
-//   x0  [B, 64, 64, 2]   f and g patches, each normalised to zero mean and
-//                        unit deviation (bf16)
-//   L1  4x4 patches -> 64   (K = 32)    y1 [B, 16, 16, 64]   ReLU
-//   L2  2x2 patches -> 128  (K = 256)   y2 [B, 8, 8, 128]    ReLU
-//   L3  2x2 patches -> 256  (K = 512)   y3 [B, 4, 4, 256]    ReLU
-//   L4  dense 4096 -> 256               y4 [B, 256]          ReLU
-//   L5  dense 256 -> 8 (FP32)           out [B, 8]: u/16, v/16,
+//   x   [2B, 64, 64, 1]  the B reference patches, then the B deformed ones,
+//                        each normalised to zero mean and unit deviation
+//   E1  8x8 patches -> 128 (K = 64), ReLU      e1 [2B, 8, 8, 128]
+//   E2  1x1 -> 128 (linear)                    e2 [2B, 8, 8, 128]
+//   C   all-pairs cell correlation of the two patches' features,
+//       corr[b][i][j] = e2_f[b][i] . e2_g[b][j] / sqrt(128)   [B, 64 x 64]
+//   L3  dense 4096 -> 256, ReLU                y3 [B, 256]
+//   L4  dense 256 -> 8 (FP32)                  out [B, 8]: u/16, v/16,
 //        20 du/dx, 20 dv/dx, 20 du/dy, 20 dv/dy, confidence logit, 0
-// L1-L4 run on the tcgen05 GEMM (bf16 operands, FP32 accumulation, bias and
-// ReLU in the epilogue); their backward products are the same GEMM with
-// transposed / patch-transposed operands and a ReLU-masked patch scatter.
+// E1, E2, C and L3 run on the tcgen05 GEMM (bf16 operands, FP32
+// accumulation; C as B independent 64 x 64 x 128 products); their backward
+// products are the same GEMM with transposed operands.  The encoder sees
+// both patches as one batch of 2B, so its weight gradients sum over both.
 // Parameters are FP32 masters updated by Adam; bf16 copies feed the GEMMs.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -29,17 +31,18 @@
 namespace aldic {
 namespace cnn {
 
-constexpr int P = 64, CIN = 2, C1 = 64, C2 = 128, C3 = 256, F4 = 256, NOUT = 8;
-constexpr int K1 = 4 * 4 * CIN, K2 = 2 * 2 * C1, K3 = 2 * 2 * C2, K4 = 4 * 4 * C3, K5 = F4;
+constexpr int P = 64, PS = 8, CELLS = (P / PS) * (P / PS), C1 = 128, C2 = 128, F3 = 256, NOUT = 8;
+constexpr int K1 = PS * PS, K2 = C1, K3 = CELLS * CELLS, K5 = F3;
 constexpr float TSCALE = 16.f, GSCALE = 20.f;
-// parameter blocks: W1 b1 W2 b2 W3 b3 W4 b4 W5 b5
-constexpr long long NW[5] = {(long long)C1 * K1, (long long)C2 * K2, (long long)C3 * K3,
-                             (long long)F4 * K4, (long long)NOUT * K5};
-constexpr long long NB[5] = {C1, C2, C3, F4, NOUT};
+constexpr int NL = 4;
+// parameter blocks: W1 b1 W2 b2 W3 b3 W4 b4 (E1, E2, L3, L4)
+constexpr long long NW[NL] = {(long long)C1 * K1, (long long)C2 * K2, (long long)F3 * K3,
+                              (long long)NOUT * K5};
+constexpr long long NB[NL] = {C1, C2, F3, NOUT};
 
 long long n_params() {
   long long s = 0;
-  for (int l = 0; l < 5; ++l) s += NW[l] + NB[l];
+  for (int l = 0; l < NL; ++l) s += NW[l] + NB[l];
   return s;
 }
 
@@ -95,13 +98,24 @@ __global__ void k_patches(const float *__restrict__ f, const float *__restrict__
     }
 }
 
+// pairs [B, 64, 64, 2] -> the encoder batch [2B, 64, 64]: reference patches
+// first, deformed patches after them
+__global__ void k_split(const bf16 *__restrict__ pairs, long long B, bf16 *__restrict__ x) {
+  const long long n = B * cnn::P * cnn::P;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    x[k] = pairs[2 * k];
+    x[n + k] = pairs[2 * k + 1];
+  }
+}
+
 __global__ void k_f2bf(const float *__restrict__ a, bf16 *__restrict__ b, long long n) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x)
     b[k] = __float2bfloat16_rn(a[k]);
 }
 
-// out[b][o] = y4[b] . W5[o] + b5[o]
+// out[b][o] = y[b] . W[o] + bias[o] (the FP32 output layer)
 __global__ void k_fc5(const bf16 *__restrict__ y4, const float *__restrict__ W5,
                       const float *__restrict__ b5, float *__restrict__ out, int B) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -139,7 +153,7 @@ __global__ void k_loss(const float *__restrict__ out, const float *__restrict__ 
   if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l / B);
 }
 
-// L5 backward: dW5, db5 (thread per (o, k) / o), dz4 = (dout . W5) * (y4 > 0)
+// output-layer backward: dW, db (thread per (o, k) / o), dz = (dout . W) * (y > 0)
 __global__ void k_fc5_back(const float *__restrict__ dout, const bf16 *__restrict__ y4,
                            const float *__restrict__ W5, int B, float *__restrict__ gW5,
                            float *__restrict__ gb5, bf16 *__restrict__ dz4) {
@@ -234,8 +248,8 @@ struct aldic_cnn {
   int device = 0;
   int maxB = 0;
   long long steps = 0;
-  DevBuf prm, grad, adm, adv, wbf;  // packed FP32 parameters, gradients, Adam moments; bf16 W1-W4
-  DevBuf x0, y1, y2, y3, y4, out, dout, dz1, dz2, dz3, dz4, part, err, loss, tgt;
+  DevBuf prm, grad, adm, adv, wbf;  // packed FP32 parameters, gradients, Adam moments; bf16 W1-W3
+  DevBuf xin, x0, e1, e2, corr, y3, out, dout, dz3, dcorr, de2, dz1, part, err, loss, tgt;
   float *W(int l) const { return prm.as<float>() + off_w(l); }
   float *Bv(int l) const { return prm.as<float>() + off_w(l) + cnn::NW[l]; }
   float *gW(int l) const { return grad.as<float>() + off_w(l); }
@@ -256,64 +270,74 @@ namespace aldic {
 namespace {
 
 GemmSrc src(const void *p, int mode, long long rows, long long kdim, long long ld, int Hin = 0,
-            int Win = 0, int C = 0, int ps = 0) {
+            int Win = 0, int C = 0, int ps = 0, long long bstride = 0) {
   GemmSrc s;
   s.p = (const bf16 *)p; s.mode = mode; s.rows = rows; s.kdim = kdim; s.ld = ld;
-  s.Hin = Hin; s.Win = Win; s.C = C; s.ps = ps;
+  s.Hin = Hin; s.Win = Win; s.C = C; s.ps = ps; s.bstride = bstride;
   return s;
 }
 
 GemmDst dst(void *p, long long M, long long N, long long ld, int fp32, const float *bias, int relu,
-            int mode = GEMM_ROW, const void *mask = nullptr, int Hin = 0, int Win = 0, int C = 0,
-            int ps = 0) {
+            int mode = GEMM_ROW, const void *mask = nullptr) {
   GemmDst d;
   d.p = p; d.M = M; d.N = N; d.ld = ld; d.fp32 = fp32; d.bias = bias; d.relu = relu; d.mode = mode;
-  d.mask = (const bf16 *)mask; d.Hin = Hin; d.Win = Win; d.C = C; d.ps = ps; d.split_stride = 0;
+  d.mask = (const bf16 *)mask; d.Hin = d.Win = d.C = d.ps = 0; d.split_stride = 0;
   return d;
 }
 
 int ensure(aldic_cnn *c, int B) {
   if (B <= c->maxB) return OK;
-  const long long b = B;
+  const long long b = B, cells = 2 * b * cnn::CELLS;
   int rc;
-  if ((rc = c->x0.ensure(2 * b * cnn::P * cnn::P * cnn::CIN)) ||
-      (rc = c->y1.ensure(2 * b * 256 * cnn::C1)) || (rc = c->y2.ensure(2 * b * 64 * cnn::C2)) ||
-      (rc = c->y3.ensure(2 * b * 16 * cnn::C3)) || (rc = c->y4.ensure(2 * b * cnn::F4)) ||
+  if ((rc = c->xin.ensure(2 * b * cnn::P * cnn::P * 2)) || (rc = c->x0.ensure(2 * 2 * b * cnn::P * cnn::P)) ||
+      (rc = c->e1.ensure(2 * cells * cnn::C1)) || (rc = c->e2.ensure(2 * cells * cnn::C2)) ||
+      (rc = c->corr.ensure(2 * b * cnn::K3)) || (rc = c->y3.ensure(2 * b * cnn::F3)) ||
       (rc = c->out.ensure(4 * b * cnn::NOUT)) || (rc = c->dout.ensure(4 * b * cnn::NOUT)) ||
-      (rc = c->dz1.ensure(2 * b * 256 * cnn::C1)) || (rc = c->dz2.ensure(2 * b * 64 * cnn::C2)) ||
-      (rc = c->dz3.ensure(2 * b * 16 * cnn::C3)) || (rc = c->dz4.ensure(2 * b * cnn::F4)) ||
+      (rc = c->dz3.ensure(2 * b * cnn::F3)) || (rc = c->dcorr.ensure(2 * b * cnn::K3)) ||
+      (rc = c->de2.ensure(2 * cells * cnn::C2)) || (rc = c->dz1.ensure(2 * cells * cnn::C1)) ||
       (rc = c->tgt.ensure(4 * b * 6)))
     return rc;
   c->maxB = B;
   return OK;
 }
 
+constexpr float kCorrScale = 0.08838834764831845f;  // 1 / sqrt(128)
+
 int forward(aldic_cnn *c, int B, cudaStream_t st) {
   int *err = c->err.as<int>();
   int rc;
-  const long long b = B;
-  if ((rc = gemm_bf16(src(c->x0.p, GEMM_PATCH, b * 256, cnn::K1, 0, 64, 64, cnn::CIN, 4),
+  const long long b = B, cells = 2 * b * cnn::CELLS, fs = (long long)cnn::CELLS * cnn::C2;
+  k_split<<<nblk(b * cnn::P * cnn::P), 256, 0, st>>>(c->xin.as<bf16>(), b, c->x0.as<bf16>());
+  ALDIC_CUDA(cudaGetLastError());
+  // E1: 8x8 patch embedding of both patches
+  if ((rc = gemm_bf16(src(c->x0.p, GEMM_PATCH, cells, cnn::K1, 0, cnn::P, cnn::P, 1, cnn::PS),
                       src(c->Wb(0), GEMM_ROW, cnn::C1, cnn::K1, cnn::K1),
-                      dst(c->y1.p, b * 256, cnn::C1, cnn::C1, 0, c->Bv(0), 1), 1, err, st)))
+                      dst(c->e1.p, cells, cnn::C1, cnn::C1, 0, c->Bv(0), 1), 1, err, st)))
     return rc;
-  if ((rc = gemm_bf16(src(c->y1.p, GEMM_PATCH, b * 64, cnn::K2, 0, 16, 16, cnn::C1, 2),
+  // E2: 1x1 (linear)
+  if ((rc = gemm_bf16(src(c->e1.p, GEMM_ROW, cells, cnn::K2, cnn::C1),
                       src(c->Wb(1), GEMM_ROW, cnn::C2, cnn::K2, cnn::K2),
-                      dst(c->y2.p, b * 64, cnn::C2, cnn::C2, 0, c->Bv(1), 1), 1, err, st)))
+                      dst(c->e2.p, cells, cnn::C2, cnn::C2, 0, c->Bv(1), 0), 1, err, st)))
     return rc;
-  if ((rc = gemm_bf16(src(c->y2.p, GEMM_PATCH, b * 16, cnn::K3, 0, 8, 8, cnn::C2, 2),
-                      src(c->Wb(2), GEMM_ROW, cnn::C3, cnn::K3, cnn::K3),
-                      dst(c->y3.p, b * 16, cnn::C3, cnn::C3, 0, c->Bv(2), 1), 1, err, st)))
+  // C: per pair, reference cells x deformed cells
+  GemmDst dc = dst(c->corr.p, cnn::CELLS, cnn::CELLS, cnn::CELLS, 0, nullptr, 0);
+  dc.scale = kCorrScale;
+  dc.bstride = cnn::K3;
+  if ((rc = gemm_bf16(src(c->e2.p, GEMM_ROW, cnn::CELLS, cnn::C2, cnn::C2, 0, 0, 0, 0, fs),
+                      src(c->e2.as<bf16>() + b * fs, GEMM_ROW, cnn::CELLS, cnn::C2, cnn::C2, 0, 0, 0, 0, fs),
+                      dc, 1, err, st, B)))
     return rc;
-  if ((rc = gemm_bf16(src(c->y3.p, GEMM_ROW, b, cnn::K4, cnn::K4),
-                      src(c->Wb(3), GEMM_ROW, cnn::F4, cnn::K4, cnn::K4),
-                      dst(c->y4.p, b, cnn::F4, cnn::F4, 0, c->Bv(3), 1), 1, err, st)))
+  // L3
+  if ((rc = gemm_bf16(src(c->corr.p, GEMM_ROW, b, cnn::K3, cnn::K3),
+                      src(c->Wb(2), GEMM_ROW, cnn::F3, cnn::K3, cnn::K3),
+                      dst(c->y3.p, b, cnn::F3, cnn::F3, 0, c->Bv(2), 1), 1, err, st)))
     return rc;
-  k_fc5<<<nblk(b * cnn::NOUT), 256, 0, st>>>(c->y4.as<bf16>(), c->W(4), c->Bv(4), c->out.as<float>(), B);
+  k_fc5<<<nblk(b * cnn::NOUT), 256, 0, st>>>(c->y3.as<bf16>(), c->W(3), c->Bv(3), c->out.as<float>(), B);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
 
-// dW = A^T-style product with split-K, summed into g
+// dW = A . B^T product with split-K, summed into g
 int weight_grad(aldic_cnn *c, const GemmSrc &A, const GemmSrc &Bm, float *g, cudaStream_t st) {
   const long long kt = (A.kdim + 63) / 64;
   int splits = (int)(kt / 8);
@@ -331,51 +355,52 @@ int weight_grad(aldic_cnn *c, const GemmSrc &A, const GemmSrc &Bm, float *g, cud
 
 int backward(aldic_cnn *c, int B, cudaStream_t st) {
   int *err = c->err.as<int>();
-  const long long b = B;
+  const long long b = B, cells = 2 * b * cnn::CELLS, fs = (long long)cnn::CELLS * cnn::C2;
   int rc;
   const long long t5 = (long long)cnn::NOUT * cnn::K5 + cnn::NOUT + b * cnn::K5;
-  k_fc5_back<<<(unsigned)((t5 + 255) / 256), 256, 0, st>>>(c->dout.as<float>(), c->y4.as<bf16>(),
-                                                           c->W(4), B, c->gW(4), c->gB(4),
-                                                           c->dz4.as<bf16>());
+  k_fc5_back<<<(unsigned)((t5 + 255) / 256), 256, 0, st>>>(c->dout.as<float>(), c->y3.as<bf16>(),
+                                                           c->W(3), B, c->gW(3), c->gB(3),
+                                                           c->dz3.as<bf16>());
   ALDIC_CUDA(cudaGetLastError());
-  // L4
-  if ((rc = weight_grad(c, src(c->dz4.p, GEMM_TRANS, cnn::F4, b, cnn::F4),
-                        src(c->y3.p, GEMM_TRANS, cnn::K4, b, cnn::K4), c->gW(3), st)))
+  // L3
+  if ((rc = weight_grad(c, src(c->dz3.p, GEMM_TRANS, cnn::F3, b, cnn::F3),
+                        src(c->corr.p, GEMM_TRANS, cnn::K3, b, cnn::K3), c->gW(2), st)))
     return rc;
-  k_colsum<<<cnn::F4, 256, 0, st>>>(c->dz4.as<bf16>(), b, cnn::F4, c->gB(3));
-  if ((rc = gemm_bf16(src(c->dz4.p, GEMM_ROW, b, cnn::F4, cnn::F4),
-                      src(c->Wb(3), GEMM_TRANS, cnn::K4, cnn::F4, cnn::K4),
-                      dst(c->dz3.p, b, cnn::K4, cnn::K4, 0, nullptr, 0, GEMM_ROW, c->y3.p), 1, err,
+  k_colsum<<<cnn::F3, 256, 0, st>>>(c->dz3.as<bf16>(), b, cnn::F3, c->gB(2));
+  if ((rc = gemm_bf16(src(c->dz3.p, GEMM_ROW, b, cnn::F3, cnn::F3),
+                      src(c->Wb(2), GEMM_TRANS, cnn::K3, cnn::F3, cnn::K3),
+                      dst(c->dcorr.p, b, cnn::K3, cnn::K3, 0, nullptr, 0), 1, err, st)))
+    return rc;
+  // C: d e2_f = s dcorr . e2_g,  d e2_g = s dcorr^T . e2_f  (one product per pair)
+  GemmDst df = dst(c->de2.p, cnn::CELLS, cnn::C2, cnn::C2, 0, nullptr, 0);
+  df.scale = kCorrScale;
+  df.bstride = fs;
+  if ((rc = gemm_bf16(src(c->dcorr.p, GEMM_ROW, cnn::CELLS, cnn::CELLS, cnn::CELLS, 0, 0, 0, 0, cnn::K3),
+                      src(c->e2.as<bf16>() + b * fs, GEMM_TRANS, cnn::C2, cnn::CELLS, cnn::C2, 0, 0, 0, 0, fs),
+                      df, 1, err, st, B)))
+    return rc;
+  GemmDst dg = df;
+  dg.p = c->de2.as<bf16>() + b * fs;
+  if ((rc = gemm_bf16(src(c->dcorr.p, GEMM_TRANS, cnn::CELLS, cnn::CELLS, cnn::CELLS, 0, 0, 0, 0, cnn::K3),
+                      src(c->e2.p, GEMM_TRANS, cnn::C2, cnn::CELLS, cnn::C2, 0, 0, 0, 0, fs),
+                      dg, 1, err, st, B)))
+    return rc;
+  // E2 (linear)
+  if ((rc = weight_grad(c, src(c->de2.p, GEMM_TRANS, cnn::C2, cells, cnn::C2),
+                        src(c->e1.p, GEMM_TRANS, cnn::K2, cells, cnn::C1), c->gW(1), st)))
+    return rc;
+  k_colsum<<<cnn::C2, 256, 0, st>>>(c->de2.as<bf16>(), cells, cnn::C2, c->gB(1));
+  if ((rc = gemm_bf16(src(c->de2.p, GEMM_ROW, cells, cnn::C2, cnn::C2),
+                      src(c->Wb(1), GEMM_TRANS, cnn::K2, cnn::C2, cnn::K2),
+                      dst(c->dz1.p, cells, cnn::C1, cnn::C1, 0, nullptr, 0, GEMM_ROW, c->e1.p), 1, err,
                       st)))
     return rc;
-  // L3
-  if ((rc = weight_grad(c, src(c->dz3.p, GEMM_TRANS, cnn::C3, b * 16, cnn::C3),
-                        src(c->y2.p, GEMM_PATCHT, cnn::K3, b * 16, 0, 8, 8, cnn::C2, 2), c->gW(2), st)))
+  // E1
+  if ((rc = weight_grad(c, src(c->dz1.p, GEMM_TRANS, cnn::C1, cells, cnn::C1),
+                        src(c->x0.p, GEMM_PATCHT, cnn::K1, cells, 0, cnn::P, cnn::P, 1, cnn::PS),
+                        c->gW(0), st)))
     return rc;
-  k_colsum<<<cnn::C3, 256, 0, st>>>(c->dz3.as<bf16>(), b * 16, cnn::C3, c->gB(2));
-  if ((rc = gemm_bf16(src(c->dz3.p, GEMM_ROW, b * 16, cnn::C3, cnn::C3),
-                      src(c->Wb(2), GEMM_TRANS, cnn::K3, cnn::C3, cnn::K3),
-                      dst(c->dz2.p, b * 16, cnn::K3, 0, 0, nullptr, 0, GEMM_PATCH, c->y2.p, 8, 8,
-                          cnn::C2, 2),
-                      1, err, st)))
-    return rc;
-  // L2
-  if ((rc = weight_grad(c, src(c->dz2.p, GEMM_TRANS, cnn::C2, b * 64, cnn::C2),
-                        src(c->y1.p, GEMM_PATCHT, cnn::K2, b * 64, 0, 16, 16, cnn::C1, 2), c->gW(1), st)))
-    return rc;
-  k_colsum<<<cnn::C2, 256, 0, st>>>(c->dz2.as<bf16>(), b * 64, cnn::C2, c->gB(1));
-  if ((rc = gemm_bf16(src(c->dz2.p, GEMM_ROW, b * 64, cnn::C2, cnn::C2),
-                      src(c->Wb(1), GEMM_TRANS, cnn::K2, cnn::C2, cnn::K2),
-                      dst(c->dz1.p, b * 64, cnn::K2, 0, 0, nullptr, 0, GEMM_PATCH, c->y1.p, 16, 16,
-                          cnn::C1, 2),
-                      1, err, st)))
-    return rc;
-  // L1
-  if ((rc = weight_grad(c, src(c->dz1.p, GEMM_TRANS, cnn::C1, b * 256, cnn::C1),
-                        src(c->x0.p, GEMM_PATCHT, cnn::K1, b * 256, 0, 64, 64, cnn::CIN, 4), c->gW(0),
-                        st)))
-    return rc;
-  k_colsum<<<cnn::C1, 256, 0, st>>>(c->dz1.as<bf16>(), b * 256, cnn::C1, c->gB(0));
+  k_colsum<<<cnn::C1, 256, 0, st>>>(c->dz1.as<bf16>(), cells, cnn::C1, c->gB(0));
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
@@ -384,13 +409,13 @@ int adam(aldic_cnn *c, float lr, cudaStream_t st) {
   c->steps++;
   const float c1 = 1.f / (1.f - powf(0.9f, (float)c->steps));
   const float c2 = 1.f / (1.f - powf(0.999f, (float)c->steps));
-  for (int l = 0; l < 5; ++l) {
+  for (int l = 0; l < cnn::NL; ++l) {
     const long long o = aldic_cnn::off_w(l), n = cnn::NW[l] + cnn::NB[l];
     float *w = c->prm.as<float>() + o;
-    // weights (bf16 copy for L1-L4), then biases
+    // weights (bf16 copy for the tensor-core layers), then biases
     k_adam<<<nblk(cnn::NW[l]), 256, 0, st>>>(w, c->grad.as<float>() + o, c->adm.as<float>() + o,
                                              c->adv.as<float>() + o, cnn::NW[l], lr, c1, c2,
-                                             l < 4 ? c->Wb(l) : nullptr);
+                                             l < cnn::NL - 1 ? c->Wb(l) : nullptr);
     k_adam<<<1, 256, 0, st>>>(w + cnn::NW[l], c->grad.as<float>() + o + cnn::NW[l],
                               c->adm.as<float>() + o + cnn::NW[l], c->adv.as<float>() + o + cnn::NW[l],
                               n - cnn::NW[l], lr, c1, c2, nullptr);
@@ -400,7 +425,7 @@ int adam(aldic_cnn *c, float lr, cudaStream_t st) {
 }
 
 int sync_bf16(aldic_cnn *c, cudaStream_t st) {
-  for (int l = 0; l < 4; ++l)
+  for (int l = 0; l < cnn::NL - 1; ++l)
     k_f2bf<<<nblk(cnn::NW[l]), 256, 0, st>>>(c->W(l), c->Wb(l), cnn::NW[l]);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
@@ -420,9 +445,9 @@ int check_err(aldic_cnn *c, cudaStream_t st) {
 
 // network input: fp32 (host or device) or bf16 (device) patches
 int load_input(aldic_cnn *c, const void *x, int x_bf16, int B, cudaStream_t st) {
-  const long long n = (long long)B * cnn::P * cnn::P * cnn::CIN;
+  const long long n = (long long)B * cnn::P * cnn::P * 2;
   if (x_bf16) {
-    ALDIC_CUDA(cudaMemcpyAsync(c->x0.p, x, 2 * n, cudaMemcpyDefault, st));
+    ALDIC_CUDA(cudaMemcpyAsync(c->xin.p, x, 2 * n, cudaMemcpyDefault, st));
     return OK;
   }
   DevBuf tmp;
@@ -437,7 +462,7 @@ int load_input(aldic_cnn *c, const void *x, int x_bf16, int B, cudaStream_t st) 
     ALDIC_CUDA(cudaMemcpyAsync(tmp.p, x, 4 * n, cudaMemcpyHostToDevice, st));
     xd = tmp.as<float>();
   }
-  k_f2bf<<<nblk(n), 256, 0, st>>>(xd, c->x0.as<bf16>(), n);
+  k_f2bf<<<nblk(n), 256, 0, st>>>(xd, c->xin.as<bf16>(), n);
   ALDIC_CUDA(cudaGetLastError());
   if (!dev) {
     ALDIC_CUDA(cudaStreamSynchronize(st));
@@ -461,7 +486,7 @@ int aldic_cnn_create(int device, unsigned long long seed, aldic_cnn **out) {
   c->device = device;
   const long long np = cnn::n_params();
   long long nwb = 0;
-  for (int l = 0; l < 4; ++l) nwb += cnn::NW[l];
+  for (int l = 0; l < cnn::NL - 1; ++l) nwb += cnn::NW[l];
   int rc;
   if ((rc = c->prm.ensure(4 * np)) || (rc = c->grad.ensure(4 * np)) || (rc = c->adm.ensure(4 * np)) ||
       (rc = c->adv.ensure(4 * np)) || (rc = c->wbf.ensure(2 * nwb)) || (rc = c->err.ensure(64)) ||
@@ -473,10 +498,10 @@ int aldic_cnn_create(int device, unsigned long long seed, aldic_cnn **out) {
   // He-normal weights (std sqrt(2 / fan_in)), zero biases, seeded
   std::vector<float> h(np, 0.f);
   std::mt19937_64 rng(seed);
-  for (int l = 0; l < 5; ++l) {
+  for (int l = 0; l < cnn::NL; ++l) {
     const long long fan_in = cnn::NW[l] / cnn::NB[l];
-    std::normal_distribution<float> nd(0.f, l == 4 ? (float)std::sqrt(1.0 / fan_in)
-                                                    : (float)std::sqrt(2.0 / fan_in));
+    std::normal_distribution<float> nd(0.f, l == 1 || l == cnn::NL - 1 ? (float)std::sqrt(1.0 / fan_in)
+                                                                       : (float)std::sqrt(2.0 / fan_in));
     float *w = h.data() + aldic_cnn::off_w(l);
     for (long long k = 0; k < cnn::NW[l]; ++k) w[k] = nd(rng);
   }
@@ -502,9 +527,9 @@ int aldic_cnn_destroy(aldic_cnn *c) {
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
-  DevBuf *b[] = {&c->prm, &c->grad, &c->adm, &c->adv, &c->wbf, &c->x0, &c->y1, &c->y2, &c->y3,
-                 &c->y4, &c->out, &c->dout, &c->dz1, &c->dz2, &c->dz3, &c->dz4, &c->part, &c->err,
-                 &c->loss, &c->tgt};
+  DevBuf *b[] = {&c->prm, &c->grad, &c->adm, &c->adv, &c->wbf, &c->xin, &c->x0, &c->e1, &c->e2,
+                 &c->corr, &c->y3, &c->out, &c->dout, &c->dz3, &c->dcorr, &c->de2, &c->dz1,
+                 &c->part, &c->err, &c->loss, &c->tgt};
   for (auto *x : b) x->release();
   cudaSetDevice(prev);
   delete c;

@@ -159,7 +159,7 @@ __device__ __forceinline__ long long dst_off(const GemmDst &D, long long m, long
 
 template <int BN>
 __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, GemmDst D, int kt_per,
-                                                      int *err) {
+                                                      int batched, int *err) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   constexpr int A_BYTES = BM * 128, STAGE = A_BYTES + BN * 128;
@@ -169,7 +169,14 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, Gem
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long m0 = (long long)blockIdx.x * BM, n0 = (long long)blockIdx.y * BN;
   const int kt_total = (int)((A.kdim + BK - 1) / BK);
-  const int kt0 = blockIdx.z * kt_per;
+  if (batched) {  // grid z = product index
+    A.p += blockIdx.z * A.bstride;
+    B.p += blockIdx.z * B.bstride;
+    if (D.fp32) D.p = reinterpret_cast<float *>(D.p) + blockIdx.z * D.bstride;
+    else D.p = reinterpret_cast<__nv_bfloat16 *>(D.p) + blockIdx.z * D.bstride;
+    if (D.mask) D.mask += blockIdx.z * D.bstride;
+  }
+  const int kt0 = batched ? 0 : blockIdx.z * kt_per;
   const int kt1 = min(kt0 + kt_per, kt_total);
   const int nk = kt1 > kt0 ? kt1 - kt0 : 0;
 
@@ -226,7 +233,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, Gem
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
   __syncthreads();
-  if (D.split_stride) {  // split-K: each split writes its own partial product
+  if (D.split_stride && !batched) {  // split-K: each split writes its own partial product
     if (D.fp32) D.p = reinterpret_cast<float *>(D.p) + blockIdx.z * D.split_stride;
     else D.p = reinterpret_cast<__nv_bfloat16 *>(D.p) + blockIdx.z * D.split_stride;
   }
@@ -248,7 +255,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, Gem
       for (int i = 0; i < 16; ++i) {
         const long long n = n0 + c0 + i;
         if (n >= D.N) continue;
-        float x = v[i];
+        float x = v[i] * D.scale;
         if (D.bias) x += D.bias[n];
         if (D.relu) x = fmaxf(x, 0.f);
         const long long o = dst_off(D, m, n);
@@ -265,14 +272,15 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, Gem
 }
 
 template <int BN>
-int launch_gemm(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, int *err,
-                cudaStream_t st) {
+int launch_gemm(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, int batches,
+                int *err, cudaStream_t st) {
   const size_t smem = 2 * (size_t)(BM * 128 + BN * 128) + 1024;
   ALDIC_CUDA(cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int kt_total = (int)((A.kdim + BK - 1) / BK);
   const int kt_per = (kt_total + splits - 1) / splits;
-  dim3 grid((unsigned)((A.rows + BM - 1) / BM), (unsigned)((B.rows + BN - 1) / BN), (unsigned)splits);
-  k_gemm<BN><<<grid, GEMM_THREADS, smem, st>>>(A, B, D, kt_per < 1 ? 1 : kt_per, err);
+  dim3 grid((unsigned)((A.rows + BM - 1) / BM), (unsigned)((B.rows + BN - 1) / BN),
+            (unsigned)(batches > 1 ? batches : splits));
+  k_gemm<BN><<<grid, GEMM_THREADS, smem, st>>>(A, B, D, kt_per < 1 ? 1 : kt_per, batches > 1, err);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
@@ -290,7 +298,7 @@ bool src_ok(const GemmSrc &S) {
 }  // namespace
 
 int gemm_bf16(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, int *err,
-              cudaStream_t st) {
+              cudaStream_t st, int batches) {
   ALDIC_CHECK(src_ok(A) && src_ok(B), E_ARG,
               "gemm: operands must be 16-byte aligned with rows of whole 16-byte chunks");
   ALDIC_CHECK(A.kdim == B.kdim, E_ARG, "gemm: A and B disagree on K");
@@ -300,10 +308,14 @@ int gemm_bf16(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, 
   ALDIC_CHECK(A.kdim % 8 == 0, E_ARG, "gemm: K must be a multiple of 8");
   ALDIC_CHECK(D.p && D.M <= A.rows && D.N <= B.rows && splits >= 1 && err, E_ARG, "gemm: bad output");
   ALDIC_CHECK(splits == 1 || D.split_stride > 0, E_ARG, "gemm: split-K needs a partial-product stride");
+  ALDIC_CHECK(batches >= 1 && batches <= 65535 && (batches == 1 || splits == 1), E_ARG,
+              "gemm: 1..65535 batched products, without split-K");
+  ALDIC_CHECK(batches == 1 || (A.bstride % 8 == 0 && B.bstride % 8 == 0), E_ARG,
+              "gemm: batch strides must keep 16-byte alignment");
   ALDIC_CHECK(D.mode == GEMM_ROW || (D.ps > 0 && D.C > 0), E_ARG, "gemm: bad output geometry");
-  if (B.rows <= 64) return launch_gemm<64>(A, B, D, splits, err, st);
-  if (B.rows <= 128) return launch_gemm<128>(A, B, D, splits, err, st);
-  return launch_gemm<256>(A, B, D, splits, err, st);
+  if (B.rows <= 64) return launch_gemm<64>(A, B, D, splits, batches, err, st);
+  if (B.rows <= 128) return launch_gemm<128>(A, B, D, splits, batches, err, st);
+  return launch_gemm<256>(A, B, D, splits, batches, err, st);
 }
 
 }  // namespace aldic

@@ -95,6 +95,7 @@ struct GemmSrc {
   int mode;
   long long rows, kdim;
   int Hin, Win, C, ps;
+  long long bstride = 0;   // elements between the operands of a batch of products
 };
 // Output: ROW (m, n) at p[m * ld + n], or PATCH scatter of (m, n) into the
 // NHWC tensor the PATCH operand reads; x = acc (+ bias[n]) (ReLU) and zeroed
@@ -110,9 +111,13 @@ struct GemmDst {
   int Hin, Win, C, ps;
   long long M, N;
   long long split_stride;  // elements between the partial products of split-K
+  float scale = 1.f;       // x = scale * acc (+ bias ...)
+  long long bstride = 0;   // elements between the outputs of a batch of products
 };
+// splits > 1: split-K; batches > 1: independent products (operand and output
+// strides bstride), one per grid z
 int gemm_bf16(const GemmSrc &A, const GemmSrc &B, const GemmDst &D, int splits, int *err,
-              cudaStream_t st);
+              cudaStream_t st, int batches = 1);
 // learned initial guess (cnn.cu)
 int cnn_patches(const float *f, const float *g, int W, int H, const double *coords, long long n,
                 void *bf16_out, float *f32_out, cudaStream_t st);

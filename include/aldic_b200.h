@@ -272,6 +272,7 @@ typedef struct {
   int mode;
   long long rows, kdim;
   int Hin, Win, C, ps;
+  long long bstride;        /* batches > 1: elements between the products' operands */
 } aldic_gemm_operand;
 typedef struct {
   void *p;
@@ -284,20 +285,26 @@ typedef struct {
   int Hin, Win, C, ps;
   long long M, N;
   long long split_stride;
+  float scale;              /* x = scale * acc (+ bias); 0 is read as 1 */
+  long long bstride;        /* batches > 1: elements between the products' outputs */
 } aldic_gemm_output;
+/* batches > 1 runs that many independent products (strides bstride). */
 ALDIC_API int aldic_gemm_bf16(aldic_ctx *ctx, const aldic_gemm_operand *A,
-                              const aldic_gemm_operand *B, const aldic_gemm_output *D, int splits);
+                              const aldic_gemm_operand *B, const aldic_gemm_output *D, int splits,
+                              int batches);
 
 /* ---- Learned initial guess (no counterpart in the reference; its
  * data-driven guess is POD-GPR over earlier frames) ----
- * A patch network on a reference / deformed 64 x 64 patch pair: 4x4, 2x2,
- * 2x2 non-overlapping patch layers (64, 128, 256 channels), a 4096 -> 256
- * dense layer (all bf16 on the tcgen05 GEMM, FP32 accumulation, ReLU) and a
- * 256 -> 8 FP32 output: [u/16, v/16, 20 du/dx, 20 dv/dx, 20 du/dy,
- * 20 dv/dy, confidence logit, 0].  Inputs x: B x 64 x 64 x 2 (channel 0 the
- * reference patch, 1 the deformed one), FP32 (host or device) or bf16
- * (device).  Parameters: 1 217 224 FP32 values, blocks W1 b1 .. W5 b5, Wl
- * row-major [out x in] with the patch index order (di, dj, c). */
+ * A Siamese patch network on a reference / deformed 64 x 64 patch pair: a
+ * shared encoder (8x8 patch embedding to 128 channels with ReLU, then a
+ * linear 1x1 layer to 128), the all-pairs correlation of the two patches'
+ * 8 x 8 cell features (64 x 64 / sqrt(128)), a 4096 -> 256 dense layer with
+ * ReLU (all bf16 on the tcgen05 GEMM, FP32 accumulation) and a 256 -> 8 FP32
+ * output: [u/16, v/16, 20 du/dx, 20 dv/dx, 20 du/dy, 20 dv/dy, confidence
+ * logit, 0].  Inputs x: B x 64 x 64 x 2 (channel 0 the reference patch, 1 the
+ * deformed one), FP32 (host or device) or bf16 (device).  Parameters:
+ * 1 075 720 FP32 values, blocks W1 b1 .. W4 b4, Wl row-major [out x in],
+ * W1's inputs in the patch order (dy, dx). */
 typedef struct aldic_cnn aldic_cnn;
 ALDIC_API int aldic_cnn_create(int device, unsigned long long seed, aldic_cnn **out);
 ALDIC_API int aldic_cnn_destroy(aldic_cnn *net);

@@ -2,7 +2,7 @@
 learned-initial-guess network of the library (2d_aldic_b200/csrc/cnn.cu),
 used to check the GPU's outputs and gradients.  With rounding=True the bf16
 roundings of the GPU path are applied at the same points (input, weights of
-the four tensor-core layers, every stored activation and back-propagated
+the tensor-core layers, every stored activation and back-propagated
 activation gradient); with rounding=False everything is FP64, which the
 finite-difference test uses to check this restatement's own backward pass.
 The network has no counterpart in the reference.
@@ -11,9 +11,10 @@ from __future__ import annotations
 
 import numpy as np
 
-P, CIN, C1, C2, C3, F4, NOUT = 64, 2, 64, 128, 256, 256, 8
-K = [4 * 4 * CIN, 2 * 2 * C1, 2 * 2 * C2, 4 * 4 * C3, F4]
-COUT = [C1, C2, C3, F4, NOUT]
+P, PS, CELLS, C1, C2, F3, NOUT = 64, 8, 64, 128, 128, 256, 8
+K = [PS * PS, C1, CELLS * CELLS, F3]
+COUT = [C1, C2, F3, NOUT]
+CORR_SCALE = 1.0 / np.sqrt(128.0)
 TSCALE, GSCALE = 16.0, 20.0
 
 
@@ -47,28 +48,27 @@ def im2col(x, ps):
             .reshape(B * (H // ps) * (W // ps), ps * ps * C))
 
 
-def col2im(y, shape, ps):
-    B, H, W, C = shape
-    return (y.reshape(B, H // ps, W // ps, ps, ps, C).transpose(0, 1, 3, 2, 4, 5)
-            .reshape(B, H, W, C))
-
-
 def _r(x, rounding):
     return bf16(x).astype(np.float64) if rounding else np.asarray(x, np.float64)
 
 
 def forward(params, x, rounding=True):
-    """Network outputs (B x 8) and the stored activations."""
+    """Network outputs (B x 8) and the stored activations.  x: B x 64 x 64 x 2
+    (reference, deformed)."""
     L = unpack(np.asarray(params, np.float64))
     B = x.shape[0]
-    x0 = _r(x, rounding)
-    Wb = [_r(W, rounding) if l < 4 else np.asarray(W, np.float64) for l, (W, _) in enumerate(L)]
-    y1 = _r(np.maximum(im2col(x0, 4) @ Wb[0].T + L[0][1], 0), rounding).reshape(B, 16, 16, C1)
-    y2 = _r(np.maximum(im2col(y1, 2) @ Wb[1].T + L[1][1], 0), rounding).reshape(B, 8, 8, C2)
-    y3 = _r(np.maximum(im2col(y2, 2) @ Wb[2].T + L[2][1], 0), rounding).reshape(B, 4, 4, C3)
-    y4 = _r(np.maximum(y3.reshape(B, -1) @ Wb[3].T + L[3][1], 0), rounding)
-    out = y4 @ Wb[4].T + L[4][1]
-    return out, dict(x0=x0, y1=y1, y2=y2, y3=y3, y4=y4, Wb=Wb)
+    xin = _r(x, rounding)
+    X = np.concatenate([xin[..., 0], xin[..., 1]], 0)[..., None]       # encoder batch of 2B
+    Wb = [_r(W, rounding) for W, _ in L[:3]] + [np.asarray(L[3][0], np.float64)]
+    cols = im2col(X, PS)
+    e1 = _r(np.maximum(cols @ Wb[0].T + L[0][1], 0), rounding)
+    e2 = _r(e1 @ Wb[1].T + L[1][1], rounding)
+    ef = e2[:B * CELLS].reshape(B, CELLS, C2)
+    eg = e2[B * CELLS:].reshape(B, CELLS, C2)
+    corr = _r(CORR_SCALE * (ef @ eg.transpose(0, 2, 1)), rounding).reshape(B, CELLS * CELLS)
+    y3 = _r(np.maximum(corr @ Wb[2].T + L[2][1], 0), rounding)
+    out = y3 @ Wb[3].T + L[3][1]
+    return out, dict(cols=cols, e1=e1, e2=e2, ef=ef, eg=eg, corr=corr, y3=y3, Wb=Wb)
 
 
 def loss_grad(out, tgt):
@@ -92,21 +92,19 @@ def backward(params, x, tgt, rounding=True):
     """(loss, packed gradients, outputs)."""
     out, A = forward(params, x, rounding)
     loss, dout = loss_grad(out, np.asarray(tgt, np.float64))
-    L = unpack(np.asarray(params, np.float64))
     B = x.shape[0]
     Wb = A["Wb"]
-    g = [None] * 5
-    y4, y3, y2, y1, x0 = A["y4"], A["y3"].reshape(B, -1), A["y2"], A["y1"], A["x0"]
-    g[4] = (dout.T @ y4, dout.sum(0))
-    dz4 = _r((dout @ Wb[4]) * (y4 > 0), rounding)
-    g[3] = (dz4.T @ y3, dz4.sum(0))
-    dz3 = _r((dz4 @ Wb[3]) * (y3 > 0), rounding).reshape(B * 16, C3)
-    g[2] = (dz3.T @ im2col(y2, 2), dz3.sum(0))
-    dz2 = _r(col2im(dz3 @ Wb[2], y2.shape, 2) * (y2 > 0), rounding)
-    dz2r = dz2.reshape(B * 64, C2)
-    g[1] = (dz2r.T @ im2col(y1, 2), dz2r.sum(0))
-    dz1 = _r(col2im(dz2r @ Wb[1], y1.shape, 2) * (y1 > 0), rounding)
-    dz1r = dz1.reshape(B * 256, C1)
-    g[0] = (dz1r.T @ im2col(x0, 4), dz1r.sum(0))
+    g = [None] * 4
+    y3, corr, e1, ef, eg = A["y3"], A["corr"], A["e1"], A["ef"], A["eg"]
+    g[3] = (dout.T @ y3, dout.sum(0))
+    dz3 = _r((dout @ Wb[3]) * (y3 > 0), rounding)
+    g[2] = (dz3.T @ corr, dz3.sum(0))
+    dcorr = _r(dz3 @ Wb[2], rounding).reshape(B, CELLS, CELLS)
+    def_ = _r(CORR_SCALE * (dcorr @ eg), rounding)
+    deg = _r(CORR_SCALE * (dcorr.transpose(0, 2, 1) @ ef), rounding)
+    de2 = np.concatenate([def_.reshape(B * CELLS, C2), deg.reshape(B * CELLS, C2)])
+    g[1] = (de2.T @ e1, de2.sum(0))
+    dz1 = _r((de2 @ Wb[1]) * (e1 > 0), rounding)
+    g[0] = (dz1.T @ A["cols"], dz1.sum(0))
     flat = np.concatenate([np.concatenate([gw.reshape(-1), gb]) for gw, gb in g])
     return loss, flat, out

@@ -8,7 +8,7 @@ from oracle import cnn as N
 
 
 def test_param_count():
-    assert N.n_params() == 1_217_224
+    assert N.n_params() == 1_075_720
 
 
 def test_backward_matches_finite_differences():

@@ -2,7 +2,7 @@
 reference of the same product (inputs rounded to bf16 first, so only the
 accumulation order differs): plain, ragged, bias/ReLU/bf16 epilogue, several
 N tiles, transposed and patch (im2col) operands, patch scatter with a ReLU
-mask, and split-K."""
+mask, split-K, and batches of scaled products."""
 import ctypes as C
 
 import numpy as np
@@ -18,28 +18,28 @@ def env(aldic):
     return aldic, aldic.Context(0), torch
 
 
-def _op(L, t, mode, rows, kdim, ld=0, geo=(0, 0, 0, 0)):
+def _op(L, t, mode, rows, kdim, ld=0, geo=(0, 0, 0, 0), bstride=0):
     o = L.GemmOperand()
-    o.p, o.ld, o.mode, o.rows, o.kdim = t.data_ptr(), ld, mode, rows, kdim
+    o.p, o.ld, o.mode, o.rows, o.kdim, o.bstride = t.data_ptr(), ld, mode, rows, kdim, bstride
     o.Hin, o.Win, o.C, o.ps = geo
     return o
 
 
 def _out(L, t, M, N, ld=0, fp32=1, bias=None, relu=0, mode=0, mask=None, geo=(0, 0, 0, 0),
-         split_stride=0):
+         split_stride=0, scale=1.0, bstride=0):
     d = L.GemmOutput()
     d.p, d.ld, d.mode, d.fp32 = t.data_ptr(), ld, mode, fp32
     d.bias = bias.data_ptr() if bias is not None else None
     d.relu = relu
     d.mask = mask.data_ptr() if mask is not None else None
     d.Hin, d.Win, d.C, d.ps = geo
-    d.M, d.N, d.split_stride = M, N, split_stride
+    d.M, d.N, d.split_stride, d.scale, d.bstride = M, N, split_stride, scale, bstride
     return d
 
 
-def _gemm(env, A, B, D, splits=1):
+def _gemm(env, A, B, D, splits=1, batches=1):
     aldic, ctx, torch = env
-    aldic._lib.call("aldic_gemm_bf16", ctx.h, C.byref(A), C.byref(B), C.byref(D), splits)
+    aldic._lib.call("aldic_gemm_bf16", ctx.h, C.byref(A), C.byref(B), C.byref(D), splits, batches)
     torch.cuda.synchronize()
 
 
@@ -143,3 +143,23 @@ def test_gemm_rejects_misaligned(env):
     D = torch.empty((128, 64), device="cuda")
     with pytest.raises(aldic.AldicError):
         _gemm(env, _op(L, A, 0, 128, 70, 70), _op(L, A, 0, 64, 70, 70), _out(L, D, 128, 64, 64))
+
+
+def test_gemm_batched_scaled(env):
+    aldic, ctx, torch = env
+    L = aldic._lib
+    nb, M, N, K = 37, 64, 64, 128
+    A = _rand(torch, nb, M, K, seed=14)
+    B = _rand(torch, nb, N, K, seed=15)
+    D = torch.empty((nb, M, N), device="cuda")
+    _gemm(env, _op(L, A, 0, M, K, K, bstride=M * K), _op(L, B, 0, N, K, K, bstride=N * K),
+          _out(L, D, M, N, N, scale=0.125, bstride=M * N), batches=nb)
+    ref = torch.bmm(A.float(), B.float().transpose(1, 2)) * 0.125
+    torch.testing.assert_close(D, ref, rtol=1e-4, atol=1e-4)
+    # transposed operands inside a batch (the correlation's backward products)
+    At = _rand(torch, nb, K, M, seed=16)
+    D2 = torch.empty((nb, M, N), device="cuda")
+    _gemm(env, _op(L, At, 2, M, K, M, bstride=M * K), _op(L, B, 0, N, K, K, bstride=N * K),
+          _out(L, D2, M, N, N, bstride=M * N), batches=nb)
+    torch.testing.assert_close(D2, torch.bmm(At.float().transpose(1, 2), B.float().transpose(1, 2)),
+                               rtol=1e-4, atol=1e-4)
