@@ -989,6 +989,18 @@ def cnn_patches(ctx: Context, coords, bf16=True):
     return out
 
 
+def cnn_to_init(ctx: Context, out):
+    """U0 (2n), F0 (4n) and confidence (n) from network outputs (n x 8 CUDA
+    tensor), on the device."""
+    n = out.shape[0]
+    dev = out.device
+    U0 = torch.empty(2 * n, dtype=torch.float64, device=dev)
+    F0 = torch.empty(4 * n, dtype=torch.float64, device=dev)
+    conf = torch.empty(n, dtype=torch.float32, device=dev)
+    call("aldic_cnn_to_init", ctx.h, _ptr(out.contiguous()), n, _ptr(U0), _ptr(F0), _ptr(conf))
+    return U0, F0, conf
+
+
 class ALDICSequence:
     """The frame loop of main_ALDIC.m:53-147 over an image sequence, with
     every image and all state on the device.

@@ -146,6 +146,10 @@ def _sine(X, Y):
     return 2.0 * np.sin(2 * np.pi * Y / 256.0), 1.5 * np.cos(2 * np.pi * X / 256.0)
 
 
+def _smooth_large(X, Y):
+    return 6.0 + 5.0 * np.sin(2 * np.pi * Y / 2048.0), -4.0 + 5.0 * np.cos(2 * np.pi * X / 2048.0)
+
+
 def plate_hole(cx=1024.0, cy=1024.0, rad=300.0):
     def f(X, Y):
         dx, dy = X - cx, Y - cy
@@ -175,6 +179,10 @@ WORKLOADS = {
                          tol=1e-3, fp64=True),
     # large uniform batch, 2048^2, 130k dots, subset 32 / step 8, sinusoidal
     "uniform2048": Workload("uniform2048", 2048, 2048, 130_000, 1, 32, 8, 16, 2.0, _sine),
+    # learned-initial-guess evaluation frame: 4096^2, displacements up to
+    # +-11 px with gradients up to 0.015 (inside the training distribution),
+    # subset 32, step 16
+    "learned4096": Workload("learned4096", 4096, 4096, 520_000, 5, 32, 16, 16, 2.0, _smooth_large),
     # plate with a hole of radius 300 px at the centre, quadtree mesh from a
     # 16 px grid, subset 32
     "plate2048": Workload("plate2048", 2048, 2048, 130_000, 2, 32, 16, 16, 2.0,

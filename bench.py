@@ -319,6 +319,94 @@ def quadtree_main(args, rank, world, local):
         }), flush=True)
 
 
+def learned_main(args, rank, world, local):
+    """Configuration 4: train the learned initial guess on the GPU (200 k
+    affine speckle pairs labelled by IC-GN), then run the 4096^2 frame from the
+    integer-search guess and from the network's guess (patches + network +
+    frame inside the timed region), reporting time, IC-GN iterations,
+    convergence and accuracy of both."""
+    import torch
+    aldic = importlib.import_module("2d_aldic_b200")
+    learned = importlib.import_module("2d_aldic_b200.learned")
+    synth = importlib.import_module("2d_aldic_b200.synth")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    data = learned.make_pairs(200_000, seed=3, device=local)
+    val = learned.make_pairs(5000, seed=13, device=local)
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    net = learned.train(data, epochs=30, lr=3e-4, device=local)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    ev = learned.evaluate(net, val)
+    del data
+    wl = synth.workload("learned4096")
+    f, g = wl.images()
+    stream = torch.cuda.Stream(device=dev)
+    ctx = aldic.Context(local)
+    ctx.set_stream(stream)
+    al = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=wl.n_admm,
+                     precision=aldic.FP32, ctx=ctx)
+    al.set_images(torch.from_numpy(f).to(dev), torch.from_numpy(g).to(dev))
+    r0 = al.frame(device_out=True)
+    coords = torch.stack([r0["x0"], r0["y0"]], 1)
+    n = coords.shape[0]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def run(mode, k):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            if mode == "learned":
+                x = aldic.cnn_patches(ctx, coords)
+                out = net.predict(x, stream=stream)
+                U0, _, conf = aldic.cnn_to_init(ctx, out)
+                al.set_init(U0)
+                r = al.frame(device_out=True, init=aldic.INIT_GIVEN)
+            else:
+                r = al.frame(device_out=True)
+            b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b), r
+
+    res = {}
+    for mode in ("search", "learned"):
+        for k in range(args.warmup):
+            run(mode, k)
+        ms, r = [], None
+        for k in range(args.steps):
+            t, r = run(mode, k)
+            ms.append(t)
+        U = r["U"].cpu().numpy()
+        ut, vt = synth.truth(wl, r["x0"].cpu().numpy(), r["y0"].cpu().numpy())
+        st = r["stats"]
+        res[mode] = {"ms_per_frame": statistics.mean(ms),
+                     "mean_iters_icgn": st["mean_iters_icgn"],
+                     "converged_icgn": st["converged_icgn"], "bad_icgn": st["bad_icgn"],
+                     "rms_px_vs_truth": float(np.sqrt(np.mean(np.r_[U[0::2] - ut, U[1::2] - vt] ** 2)))}
+    if rank == 0:
+        s, l = res["search"], res["learned"]
+        print(json.dumps({
+            "metric": METRIC, "value": l["converged_icgn"] / (l["ms_per_frame"] / 1e3), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": l["ms_per_frame"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 network (FP32 accumulate); f32 sampling, f64 sums+solves", "data": "synthetic",
+            "learned_vs_search": {"search_init": s, "learned_init": l,
+                                  "frame_time_ratio": s["ms_per_frame"] / l["ms_per_frame"],
+                                  "iteration_ratio": s["mean_iters_icgn"] / l["mean_iters_icgn"]},
+            "network": {"train_pairs": 200_000, "epochs": 30, "train_s": t_train, "pair_gen_s": t_gen,
+                        "held_out": ev},
+            "config": {"workload": f"{wl.name}: 4096x4096 u8 speckle (seed {wl.seed}), "
+                                   "u=6+5sin(2pi y/2048), v=-4+5cos(2pi x/2048), noise 2; subset 32, "
+                                   "step 16, search 16", "subsets": n,
+                       "l2": "flushed between frames (256 MB write)"},
+        }), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -329,6 +417,9 @@ def main():
         return
     if args.workload.startswith("sequence"):
         sequence_main(args, rank, world, local)
+        return
+    if args.workload.startswith("learned"):
+        learned_main(args, rank, world, local)
         return
     if args.workload.startswith("plate"):
         quadtree_main(args, rank, world, local)
