@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, Gem
   } else {
     // epilogue: row r = 32 * warp + lane of the tile
     const long long m = m0 + 32 * warp + lane;
+    const bool base_aligned = ((uintptr_t)D.p & 15) == 0 && ((uintptr_t)D.mask & 15) == 0;
     for (int c0 = 0; c0 < BN; c0 += 16) {
       float v[16];
       if (nk > 0) {
@@ -251,9 +252,53 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_gemm(GemmSrc A, GemmSrc B, Gem
         for (int i = 0; i < 16; ++i) v[i] = 0.f;
       }
       if (m >= D.M) continue;
+      const long long nf = n0 + c0;
+      // 16 contiguous, 16-byte aligned destination elements: vector stores
+      if (nf + 16 <= D.N) {
+        const long long o0 = dst_off(D, m, nf);
+        const int seg = D.ps * D.C;
+        const bool contig = D.mode == GEMM_ROW || (nf % seg) + 16 <= seg;
+        const bool aligned = (o0 & 7) == 0 && base_aligned;
+        if (contig && aligned) {
+          float x[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            x[i] = v[i] * D.scale;
+            if (D.bias) x[i] += D.bias[nf + i];
+            if (D.relu) x[i] = fmaxf(x[i], 0.f);
+          }
+          if (D.mask) {
+            const uint4 *mp = reinterpret_cast<const uint4 *>(D.mask + o0);
+            const uint4 q0 = mp[0], q1 = mp[1];
+            const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&q0);
+            const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&q1);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              if (!(__bfloat162float(mb0[i]) > 0.f)) x[i] = 0.f;
+              if (!(__bfloat162float(mb1[i]) > 0.f)) x[8 + i] = 0.f;
+            }
+          }
+          if (D.fp32) {
+            float4 *dp = reinterpret_cast<float4 *>(reinterpret_cast<float *>(D.p) + o0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dp[i] = make_float4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+          } else {
+            uint32_t pk[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+              pk[i] = *reinterpret_cast<uint32_t *>(&h);
+            }
+            uint4 *dp = reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(D.p) + o0);
+            dp[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            dp[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          }
+          continue;
+        }
+      }
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const long long n = n0 + c0 + i;
+        const long long n = nf + i;
         if (n >= D.N) continue;
         float x = v[i] * D.scale;
         if (D.bias) x += D.bias[n];

@@ -388,6 +388,22 @@ def learned_main(args, rank, world, local):
                      "mean_iters_icgn": st["mean_iters_icgn"],
                      "converged_icgn": st["converged_icgn"], "bad_icgn": st["bad_icgn"],
                      "rms_px_vs_truth": float(np.sqrt(np.mean(np.r_[U[0::2] - ut, U[1::2] - vt] ** 2)))}
+    # the network alone (patch extraction + forward pass over every subset)
+    net_ms = []
+    for k in range(max(2, args.steps)):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            x = aldic.cnn_patches(ctx, coords)
+            net.predict(x, stream=stream)
+            b.record(stream)
+        b.synchronize()
+        net_ms.append(a.elapsed_time(b))
+    res["learned"]["network_ms"] = statistics.mean(net_ms[1:])
+    # forward flops: E1 + E2 on both patches, correlation, L3, output layer
+    fl = 2.0 * n * (2 * 64 * (64 * 128 + 128 * 128) + 64 * 64 * 128 + 4096 * 256 + 256 * 8)
+    res["learned"]["network_tflops"] = fl / (res["learned"]["network_ms"] / 1e3) / 1e12
     if rank == 0:
         s, l = res["search"], res["learned"]
         print(json.dumps({
