@@ -496,6 +496,35 @@ def Subpb2(DICmesh, beta, mu, U, F, udual, vdual, alpha=0, GaussPtOrder=2):
     return out
 
 
+def ComputeStrain(ULocal, FLocal, DICmesh, DICpara, ctx: Context | None = None):
+    """ComputeStrain.m: strains on the uniform mesh.  DICpara keys
+    MethodToComputeStrain (0 solved F, 1 central differences, 2 plane
+    fitting, 3 finite elements; default 3), StrainType (0 infinitesimal,
+    1 Eulerian, 2 Green-Lagrangian; default 0) and, for method 2, PlaneFitRad
+    (the half window the reference asks for interactively).  Returns a dict
+    with FStrain and FStrainFinite (4n, [F11 F21 F12 F22]) and FStrainWorld
+    (the nodes inside the Rad ring, the F21 and F12 slots negated for the
+    upward y axis).  Method 3 keeps funGlobal_NodalStrainAvg's slot order
+    [du/dx du/dy dv/dx dv/dy], which ComputeStrain.m then reads as
+    [F11 F21 F12 F22], as the reference does."""
+    ctx = ctx or default_context()
+    method = int(DICpara.get("MethodToComputeStrain", 3))
+    stype = int(DICpara.get("StrainType", 0))
+    rad = {0: 0, 1: 1, 2: int(DICpara.get("PlaneFitRad", 2)), 3: 1}[method]
+    M, N = int(DICmesh["M"]), int(DICmesh["N"])
+    h = float(np.mean(DICpara["winstepsize"]))
+    U = np.ascontiguousarray(ULocal, np.float64) if ULocal is not None else None
+    F = np.ascontiguousarray(FLocal, np.float64) if FLocal is not None else None
+    fs = np.empty(4 * M * N)
+    ff = np.empty(4 * M * N)
+    call("aldic_compute_strain", ctx.h, M, N, h, method, rad, stype, _ptr(U), _ptr(F), _ptr(fs), _ptr(ff))
+    i, j = np.meshgrid(np.arange(M), np.arange(N))
+    k = (j * M + i)[rad:N - rad, rad:M - rad].reshape(-1)
+    world = ff.reshape(-1, 4)[k].copy()
+    world[:, 1:3] *= -1
+    return {"FStrain": fs, "FStrainFinite": ff, "FStrainWorld": world.reshape(-1)}
+
+
 def subpb2_fd(M, N, winstepsize, beta, mu, U, F, udual, vdual, ctx: Context | None = None):
     """The finite-difference Subproblem 2 of main_ALDIC.m:243-259 (interior
     nodes solve (beta D'D + mu I) x = beta D'(F - udual) + mu (U - vdual),

@@ -983,6 +983,39 @@ int aldic_subpb2_fd(aldic_ctx *c, int M, int N, double step, double beta, double
   return check_grid_err(c);
 }
 
+int aldic_compute_strain(aldic_ctx *c, int M, int N, double step, int method, int rad,
+                         int strain_type, const double *U, const double *F, double *strain,
+                         double *finite) {
+  ALDIC_CHECK(c && finite && M >= 2 && N >= 2 && step > 0, E_ARG, "compute_strain: bad arguments");
+  ALDIC_CHECK(method >= 0 && method <= 3, E_ARG, "compute_strain: method must be 0..3");
+  ALDIC_CHECK(strain_type >= 0 && strain_type <= 2, E_ARG, "compute_strain: strain_type must be 0..2");
+  ALDIC_CHECK(method == 0 ? F != nullptr : U != nullptr, E_ARG,
+              "compute_strain: method 0 needs F, the others U");
+  ALDIC_CHECK(method != 2 || (rad >= 1 && 2 * rad < M && 2 * rad < N), E_ARG,
+              "compute_strain: plane fitting needs 1 <= rad < min(M, N) / 2");
+  Guard g(c);
+  const long long n = (long long)M * N;
+  int rc;
+  Arg<double> au, af, as, ao;
+  if ((rc = arg_in(c, U, 2 * n, au)) || (rc = arg_in(c, F, 4 * n, af)) ||
+      (rc = arg_out(c, strain, 4 * n, as)) || (rc = arg_out(c, finite, 4 * n, ao)))
+    return rc;
+  double *fs = as.dev ? as.dev : (double *)c->arena.get(sizeof(double) * 4 * n);
+  ALDIC_CHECK(fs, E_NOMEM, "staging buffer allocation failed");
+  if (method == 0) {
+    ALDIC_CUDA(cudaMemcpyAsync(fs, af.dev, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, c->stream));
+  } else if (method == 3) {
+    if ((rc = nodal_strain(M, N, step, au.dev, fs, c->stream))) return rc;
+  } else {
+    if ((rc = fd_strain(M, N, step, au.dev, fs, c->stream))) return rc;
+    if (method == 2 && (rc = plane_fit(M, N, step, rad, au.dev, fs, c->stream))) return rc;
+  }
+  if ((rc = finite_strain(n, strain_type, fs, ao.dev, c->stream))) return rc;
+  arg_back(c, as);
+  arg_back(c, ao);
+  return finish(c, as.staged || ao.staged);
+}
+
 int aldic_fd_strain(aldic_ctx *c, int M, int N, double step, const double *U, double *F) {
   ALDIC_CHECK(c && U && F && M >= 2 && N >= 2 && step > 0, E_ARG, "fd_strain: bad arguments");
   Guard g(c);

@@ -937,6 +937,73 @@ int fd_dual(int M, int N, const double *F2, const double *F1, const double *U2, 
   return OK;
 }
 
+// PlaneFit2.m on the symmetric (2 rad + 1)^2 window: the least-squares plane
+// a + b (i h) + c (j h) has b = sum(i u) / (h (2r+1) sum i^2) and c likewise
+// (the window's sums of i, j and i j vanish)
+__global__ void k_plane_fit(int M, int N, double h, int rad, const double *__restrict__ U,
+                            double *__restrict__ F) {
+  const long long n = (long long)M * N;
+  double s2 = 0.0;
+  for (int t = -rad; t <= rad; ++t) s2 += (double)t * t;
+  const double den = h * (2 * rad + 1) * s2;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    if (i < rad || i >= M - rad || j < rad || j >= N - rad) continue;
+    double ux = 0, vx = 0, uy = 0, vy = 0;
+    for (int tj = -rad; tj <= rad; ++tj)
+      for (int ti = -rad; ti <= rad; ++ti) {
+        const long long q = (long long)(j + tj) * M + (i + ti);
+        const double u = U[2 * q], v = U[2 * q + 1];
+        ux += ti * u;
+        vx += ti * v;
+        uy += tj * u;
+        vy += tj * v;
+      }
+    F[4 * k + 0] = ux / den;
+    F[4 * k + 1] = vx / den;
+    F[4 * k + 2] = uy / den;
+    F[4 * k + 3] = vy / den;
+  }
+}
+
+// ComputeStrain.m:105-129 on [du/dx dv/dx du/dy dv/dy] per node
+__global__ void k_finite_strain(long long n, int type, const double *__restrict__ F,
+                                double *__restrict__ out) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const double ux = F[4 * k], vx = F[4 * k + 1], uy = F[4 * k + 2], vy = F[4 * k + 3];
+    double o0 = ux, o1 = vx, o2 = uy, o3 = vy;
+    if (type == 1) {         // Eulerian
+      o0 = 1.0 / (1.0 - ux) - 1.0;
+      o3 = 1.0 / (1.0 - vy) - 1.0;
+      o2 = uy / (1.0 - vy);
+      o1 = vx / (1.0 - ux);
+    } else if (type == 2) {  // Green-Lagrangian, E = (C - I) / 2
+      o0 = 0.5 * (ux * 2 - ux * ux - vx * vx);
+      o3 = 0.5 * (vy * 2 - uy * uy - vy * vy);
+      o2 = 0.5 * (uy + vx - ux * uy - vx * vy);
+      o1 = 0.5 * (vx + uy - uy * ux - vy * vx);
+    }
+    out[4 * k] = o0;
+    out[4 * k + 1] = o1;
+    out[4 * k + 2] = o2;
+    out[4 * k + 3] = o3;
+  }
+}
+
+int plane_fit(int M, int N, double h, int rad, const double *U, double *F, cudaStream_t st) {
+  k_plane_fit<<<blocks_for((long long)M * N), 256, 0, st>>>(M, N, h, rad, U, F);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int finite_strain(long long n, int type, const double *F, double *out, cudaStream_t st) {
+  k_finite_strain<<<blocks_for(n), 256, 0, st>>>(n, type, F, out);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
 int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int f0) {
   const long long n = (long long)M * N;
   k_fe_store<<<blocks_for(n), 256, 0, st>>>(n, w.x + f0 * n, Uhat);

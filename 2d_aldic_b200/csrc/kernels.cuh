@@ -68,6 +68,11 @@ int fd_strain(int M, int N, double h, const double *U, double *F, cudaStream_t s
 // reset (accumulate = 0: zero elsewhere) or accumulate
 int fd_dual(int M, int N, const double *F2, const double *F1, const double *U2, const double *U1,
             double *udual, double *vdual, int accumulate, cudaStream_t st);
+// ComputeStrain.m: plane-fit gradients on the interior (PlaneFit2.m, window
+// (2 rad + 1)^2) written over F; finite-strain conversion of F (type 1
+// Eulerian, 2 Green-Lagrangian) into out
+int plane_fit(int M, int N, double h, int rad, const double *U, double *F, cudaStream_t st);
+int finite_strain(long long n, int type, const double *F, double *out, cudaStream_t st);
 
 // A symmetric sparse operator for the PCG: CSR rows of n nodes (sorted
 // columns), its diagonal, shared by every field.  Rows whose field mask is 0

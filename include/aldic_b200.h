@@ -185,6 +185,18 @@ ALDIC_API int aldic_subpb2_fd(aldic_ctx *ctx, int M, int N, double step, double 
 /* F = funDerivativeOp(M, N, step) * U: [du/dx dv/dx du/dy dv/dy] per node. */
 ALDIC_API int aldic_fd_strain(aldic_ctx *ctx, int M, int N, double step, const double *U, double *F);
 
+/* ComputeStrain.m (Section 8 of main_ALDIC.m) on the uniform M x N grid:
+ * method 0 the solved F, 1 central differences (funDerivativeOp), 2 plane
+ * fitting over a (2 rad + 1)^2 window on the interior (PlaneFit2.m; the
+ * border keeps the differences), 3 finite-element nodal strains
+ * (funGlobal_NodalStrainAvg); strain_type 0 infinitesimal, 1 Eulerian, 2
+ * Green-Lagrangian.  F (4n) is read by method 0 only; strain (4n, may be
+ * NULL) receives FStrain, finite (4n) FStrainFinite, both full-grid
+ * [F11 F21 F12 F22] slots as the reference fills them. */
+ALDIC_API int aldic_compute_strain(aldic_ctx *ctx, int M, int N, double step, int method, int rad,
+                                   int strain_type, const double *U, const double *F,
+                                   double *strain, double *finite);
+
 /* funGlobal_NodalStrainAvg.m:1 on the uniform mesh (2x2 Gauss points,
  * extrapolation to the nodes, average over elements).  Output slots per node
  * are [du/dx du/dy dv/dx dv/dy], the order funGlobal_NodalStrainAvg.m:97,
