@@ -24,4 +24,5 @@ def test_compute_strain_matches_oracle(aldic, method, stype):
     w = r["FStrainWorld"].reshape(-1, 4)
     assert len(w) == (M - 2 * rad) * (N - 2 * rad)
     k = rad * M + rad
-    np.testing.assert_array_equal(w[0], ff.reshape(-1, 4)[k] * [1, -1, -1, 1])
+    # the world-frame copy is the finite strain itself, interior ring removed, slots 1, 2 negated
+    np.testing.assert_array_equal(w[0], r["FStrainFinite"].reshape(-1, 4)[k] * [1, -1, -1, 1])
