@@ -32,6 +32,7 @@ _SIGS = {
     "aldic_get_images": ([P, P, P, P, P, P], I32),
     "aldic_search_dims": ([I32, I32, P, P, I32, I32, P, P, P], I32),
     "aldic_int_search": ([P, P, P, I32, I32, P, P, P, P, P, P, P], I32),
+    "aldic_int_search_mg": ([P, P, P, I32, I32, P, P, I64, P, P, P, P, P, P, P], I32),
     "aldic_icgn": ([P, P, I64, P, P, I32, D, I32, P, P, P, P], I32),
     "aldic_localicgn_post": ([P, I32, I32, P, P, P, P], I32),
     "aldic_subpb1": ([P, P, I64, P, P, P, P, P, I32, D, D, I32, P, P], I32),
@@ -74,7 +75,7 @@ class FrameParams(C.Structure):
     _fields_ = [("winsize", I32), ("step", I32), ("search", I32 * 2), ("gridx", I32 * 2),
                 ("gridy", I32 * 2), ("tol", D), ("mu", D), ("beta", D), ("n_admm", I32),
                 ("tol2", D), ("precision", I32), ("smooth", I32), ("use_graph", I32),
-                ("init", I32), ("subpb2_fd", I32)]
+                ("init", I32), ("subpb2_fd", I32), ("node_grid", D * 4)]
 
 
 class GemmOperand(C.Structure):
@@ -92,7 +93,8 @@ class FrameStats(C.Structure):
     _fields_ = [("M", I32), ("N", I32), ("admm_steps", I32), ("bad_icgn", I32),
                 ("converged_icgn", I32), ("beta", D), ("update_y", D * 16),
                 ("update_y2", D * 16), ("mean_iters_icgn", D), ("kernel_launches", I32),
-                ("t_stage_ms", D * 8), ("max_pcg_iters", I32)]
+                ("t_stage_ms", D * 8), ("max_pcg_iters", I32), ("node_grid", D * 4),
+                ("t_search_mg_ms", D)]
 
 
 class AldicError(RuntimeError):

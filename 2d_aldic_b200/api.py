@@ -33,7 +33,7 @@ except Exception:  # pragma: no cover
 U8, U16, F32, F64 = 0, 1, 2, 3
 FP32, FP64 = 0, 1
 # initial guess of a frame (ALDIC_INIT_* of the C ABI)
-INIT_SEARCH, INIT_PREV, INIT_ZERO, INIT_EXTRAP, INIT_GIVEN = 0, 1, 2, 3, 4
+INIT_SEARCH, INIT_PREV, INIT_ZERO, INIT_EXTRAP, INIT_GIVEN, INIT_SEARCH_MG = 0, 1, 2, 3, 4, 5
 _DT = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.float32): F32,
        np.dtype(np.float64): F64}
 
@@ -285,6 +285,52 @@ def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winste
     return x, y, u, v, cc
 
 
+def funIntegerSearchMg(f, g, gridx, gridy, winsize, winstepsize, *varargin,
+                       ctx: Context | None = None, info: dict | None = None):
+    """[xGrid,yGrid,uGrid,vGrid,cc] = funIntegerSearchMg(f,g,gridx,gridy,
+    winsize,winstepsize,winstepsize) -- funIntegerSearchMg.m:1, the multigrid
+    search of IntegerSearch.m:117-120 for large displacements.
+
+    f, g: images (H, W).  Returns x, y, u, v as ny x nx arrays on the node
+    grid gridx(1):step:gridx(2) (its borders follow the displacements of the
+    outermost regions) and cc = {'max': ny x nx, 'qfactors': (nx*ny) x 2 in
+    column-major grid order, as cc.qfactors = [qf_1Grid(:), qf_2Grid(:)]}.
+    info, when given, receives the level count, the last-level region count,
+    the regions whose correlation raised and the level-1 (whole ROI) shift."""
+    ctx = ctx or _ctx_for(f, g)
+    H, W = f.shape
+    if _dtype_code(f) in (U8, U16):
+        ctx.set_ref(f)
+        ctx.set_def(g)
+    else:
+        ctx.set_fields(_prep(f), _prep(g), _zeros_like_img(f), _zeros_like_img(f))
+    gxa = (C.c_int * 2)(int(gridx[0]), int(gridx[-1]))
+    gya = (C.c_int * 2)(int(gridy[0]), int(gridy[-1]))
+    step = int(winstepsize if np.ndim(winstepsize) == 0 else winstepsize[0])
+    cap = (W // step + 1) * (H // step + 1)
+    like = _first_cuda(f, g)
+    outs = [_empty(like, (cap,)) for _ in range(5)]
+    q = _empty(like, (2, cap))
+    nx, ny = C.c_int(), C.c_int()
+    inf = np.zeros(10)
+    call("aldic_int_search_mg", ctx.h, gxa, gya, int(winsize), step, C.byref(nx), C.byref(ny), cap,
+         *[_ptr(o) for o in outs], _ptr(q), _ptr(inf))
+    nx, ny = nx.value, ny.value
+    n = nx * ny
+    x, y, u, v, cmax = (o[:n].reshape(ny, nx) for o in outs)
+    qs = q.reshape(-1)[:2 * n].reshape(2, ny, nx)
+    if _is_cuda(qs):
+        qf = torch.stack([qs[0].T.reshape(-1), qs[1].T.reshape(-1)], 1)
+    else:
+        qf = np.stack([qs[0].T.reshape(-1), qs[1].T.reshape(-1)], 1)
+    if info is not None:
+        info.update(levels=int(inf[0]), regions=int(inf[1]), failed=int(inf[2]),
+                    level1_u=float(inf[3]), level1_v=float(inf[4]), level1_cc=float(inf[5]),
+                    ms_level1=float(inf[6]), ms_levels=float(inf[7]), ms_last_level=float(inf[8]),
+                    ms_gridfit=float(inf[9]))
+    return x, y, u, v, {"max": cmax, "qfactors": qf, "A": []}
+
+
 def _zeros_like_img(f):
     if _is_cuda(f):
         return torch.zeros(f.shape, dtype=torch.float64, device=f.device)
@@ -293,19 +339,31 @@ def _zeros_like_img(f):
 
 def IntegerSearch(ImgRef, ImgDef, file_name, DICpara):
     """[DICpara,x0,y0,u,v,cc] = IntegerSearch(ImgRef,ImgDef,file_name,DICpara)
-    -- IntegerSearch.m:1, non-interactive: the search zone comes from
-    DICpara['SizeOfFFTSearchRegion'] instead of input() and only the whole-
-    field method (InitFFTSearchMethod = 1) is available."""
-    s = DICpara.get("SizeOfFFTSearchRegion")
-    if s is None:
-        raise ValueError("DICpara['SizeOfFFTSearchRegion'] is required (the reference asks "
-                         "for it interactively)")
+    -- IntegerSearch.m:1, non-interactive.  DICpara['InitFFTSearchMethod']
+    (default 1) picks the whole-field search, whose zone comes from
+    DICpara['SizeOfFFTSearchRegion'] instead of input(), or -- for any value
+    other than 1 and 2 -- the multigrid search funIntegerSearchMg
+    (IntegerSearch.m:117-120).  The seed-point method 2 is interactive in the
+    reference (ginput) and is not available."""
+    method = DICpara.get("InitFFTSearchMethod", 1)
     roi = DICpara["gridxyROIRange"]
-    x0, y0, u, v, cc = funIntegerSearch(ImgRef, ImgDef, s, roi["gridx"], roi["gridy"],
-                                        DICpara["winsize"], DICpara["winstepsize"], 0,
-                                        DICpara["winstepsize"])
+    if method == 2:
+        raise NotImplementedError("InitFFTSearchMethod = 2 picks seed points with ginput")
+    if method == 1:
+        s = DICpara.get("SizeOfFFTSearchRegion")
+        if s is None:
+            raise ValueError("DICpara['SizeOfFFTSearchRegion'] is required (the reference asks "
+                             "for it interactively)")
+        x0, y0, u, v, cc = funIntegerSearch(ImgRef, ImgDef, s, roi["gridx"], roi["gridy"],
+                                            DICpara["winsize"], DICpara["winstepsize"], 0,
+                                            DICpara["winstepsize"])
+    else:
+        x0, y0, u, v, cc = funIntegerSearchMg(ImgRef, ImgDef, roi["gridx"], roi["gridy"],
+                                              DICpara["winsize"], DICpara["winstepsize"],
+                                              DICpara["winstepsize"])
+    DICpara = dict(DICpara, InitFFTSearchMethod=method)
     mask = DICpara.get("ImgRefMask")
-    if mask is not None:  # IntegerSearch.m:68-73
+    if mask is not None:  # IntegerSearch.m:68-73, :125-131
         xi = np.asarray(x0, int).ravel() - 1
         yi = np.asarray(y0, int).ravel() - 1
         hole = np.asarray(mask)[yi, xi].reshape(np.shape(x0)).astype(float)
@@ -621,10 +679,13 @@ class ALDIC:
             raise ValueError("subpb2 must be 'fe' (Subpb2.m) or 'fd' (finite differences)")
         p.subpb2_fd = int(subpb2 == "fd")
         self.p = p
+        self.node_grid = None   # grid of the last multigrid-search frame
+        self.shape = None
 
     def set_images(self, f=None, g=None, roi=None, mask=None):
         if f is not None:
             self.ctx.set_ref(f, roi=roi, mask=mask)
+            self.shape = tuple(f.shape)
         if g is not None:
             self.ctx.set_def(g)
 
@@ -642,11 +703,26 @@ class ALDIC:
               init: int = INIT_SEARCH):
         """Run one frame.  With out (dict of preallocated arrays x0, y0, U, F,
         iters -- numpy or CUDA tensors) the results are written there.  init
-        selects the initial guess (INIT_SEARCH, or a sequence mode: INIT_PREV,
-        INIT_ZERO, INIT_EXTRAP, INIT_GIVEN)."""
+        selects the initial guess (INIT_SEARCH, INIT_SEARCH_MG -- the
+        multigrid search, which also decides the node grid -- or a sequence
+        mode: INIT_PREV, INIT_ZERO, INIT_EXTRAP, INIT_GIVEN).  The sequence
+        modes run on the grid of the last INIT_SEARCH_MG frame, if any since
+        the last INIT_SEARCH frame."""
         self.p.init = int(init)
-        M, N = self.dims()
-        n = M * N
+        mg = init == INIT_SEARCH_MG
+        if init == INIT_SEARCH:
+            self.node_grid = None
+        for k in range(4):
+            self.p.node_grid[k] = 0.0 if (mg or self.node_grid is None) else self.node_grid[k]
+        if mg:
+            if self.shape is None:
+                raise AldicError("ALDIC.frame", -2, "set the reference image first")
+            H, W = self.shape
+            n = (W // self.p.step + 1) * (H // self.p.step + 1)   # capacity; the grid follows
+            stats = True
+        else:
+            M, N = self.dims()
+            n = M * N
         if out is None:
             if device_out:
                 dev = torch.device("cuda", self.ctx.device)
@@ -662,7 +738,14 @@ class ALDIC:
         call("aldic_frame", self.ctx.h, C.byref(self.p), _ptr(out["x0"]), _ptr(out["y0"]),
              _ptr(out["U"]), _ptr(out["F"]), _ptr(out["iters"]), C.byref(st) if stats else None)
         res = dict(out)
+        if mg:
+            self.node_grid = tuple(st.node_grid)
+            M, N = int(st.node_grid[2]), int(st.node_grid[3])
+            n = M * N
+            for k, m in (("x0", 1), ("y0", 1), ("U", 2), ("F", 4), ("iters", 1)):
+                res[k] = out[k][:m * n]
         res["M"], res["N"] = M, N
+        res["node_grid"] = tuple(st.node_grid) if stats else self.node_grid
         if stats:
             res["stats"] = {"beta": st.beta, "bad_icgn": st.bad_icgn,
                             "converged_icgn": st.converged_icgn,
@@ -671,6 +754,7 @@ class ALDIC:
                             "update_y2": list(st.update_y2)[:st.admm_steps],
                             "kernel_launches": st.kernel_launches,
                             "max_pcg_iters": st.max_pcg_iters,
+                            "t_search_mg_ms": st.t_search_mg_ms,
                             "t_stage_ms": dict(zip(("normalize", "search", "icgn", "icgn_post",
                                                     "section5", "admm", "frame"),
                                                    list(st.t_stage_ms)[:7]))}
@@ -1055,9 +1139,13 @@ class ALDICSequence:
     stream)."""
 
     def __init__(self, inc_unit: int | None = None, n_search: int = 5, predictor: str = "extrap",
-                 roi=None, mask=None, **frame_kw):
+                 roi=None, mask=None, search_method: str = "whole", **frame_kw):
         if predictor not in ("extrap", "previous"):
             raise ValueError("predictor must be 'extrap' or 'previous'")
+        if search_method not in ("whole", "multigrid"):
+            raise ValueError("search_method must be 'whole' (InitFFTSearchMethod = 1) or "
+                             "'multigrid' (funIntegerSearchMg)")
+        self.search_mode = INIT_SEARCH if search_method == "whole" else INIT_SEARCH_MG
         self.al = ALDIC(**frame_kw)
         self.inc_unit = inc_unit
         self.n_search = max(1, int(n_search))
@@ -1071,7 +1159,7 @@ class ALDICSequence:
         for s in range(2, n_frames + 1):
             upd = False
             if s < 2 + self.n_search:
-                mode = INIT_SEARCH
+                mode = getattr(self, "search_mode", INIT_SEARCH)
             elif self.inc_unit and (s - 2) % self.inc_unit == 0:
                 ref, upd, mode, same = s - 2, True, INIT_ZERO, 0
             elif self.predictor == "extrap" and same >= 2:

@@ -19,7 +19,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libaldic_b200.so")
 ROOT = os.path.dirname(HERE)
 
-SOURCES = ["k_image.cu", "k_search.cu", "k_icgn.cu", "k_grid.cu", "qt.cu", "k_gemm.cu", "cnn.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["k_image.cu", "k_search.cu", "k_searchmg.cu", "k_icgn.cu", "k_grid.cu", "qt.cu", "k_gemm.cu", "cnn.cu", "capi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]

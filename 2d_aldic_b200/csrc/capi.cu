@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -101,6 +102,7 @@ struct aldic_ctx {
   // sequence state: final U of the last two frames and the given U0
   // (3 x 2n doubles: [U(k-1) | U(k-2) | given])
   DevBuf hist;
+  MgWork mg;  // multigrid search work
   long long hist_n = 0;
   int hist_count = 0;
   bool have_given = false;
@@ -197,10 +199,10 @@ int ensure_grid_work(aldic_ctx *c, long long n) {
   if (n <= c->gw_n && c->gw.x) return OK;
   const long long R = 12;
   int rc;
-  // x r z p(2 buffers) q b diag -> 8 * R * n doubles
-  if ((rc = c->gw_vec.ensure(sizeof(double) * 8 * R * n))) return rc;
+  // x r z p(2 buffers) q b diag zz qq ss pp -> 12 * R * n doubles
+  if ((rc = c->gw_vec.ensure(sizeof(double) * 12 * R * n))) return rc;
   c->gw.max_blocks = 148 * 8;
-  if ((rc = c->gw_part.ensure(sizeof(double) * 4 * R * c->gw.max_blocks))) return rc;
+  if ((rc = c->gw_part.ensure(sizeof(double) * 2 * 4 * R * c->gw.max_blocks))) return rc;
   if ((rc = c->gw_mask.ensure(R * n))) return rc;
   if ((rc = c->gw_misc.ensure(64))) return rc;
   double *v = c->gw_vec.as<double>();
@@ -211,6 +213,10 @@ int ensure_grid_work(aldic_ctx *c, long long n) {
   c->gw.q = v + 5 * R * n;
   c->gw.b = v + 6 * R * n;
   c->gw.diag = v + 7 * R * n;
+  c->gw.zz = v + 8 * R * n;
+  c->gw.qq = v + 9 * R * n;
+  c->gw.ss = v + 10 * R * n;
+  c->gw.pp = v + 11 * R * n;
   c->gw.part = c->gw_part.as<double>();
   c->gw.mask = c->gw_mask.as<unsigned char>();
   unsigned int *misc = c->gw_misc.as<unsigned int>();
@@ -375,6 +381,7 @@ int aldic_ctx_destroy(aldic_ctx *c) {
                     &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr,
                     &c->hist};
   for (DevBuf *b : bufs) b->release();
+  c->mg.release();
   c->arena.release();
   if (c->own_stream) cudaStreamDestroy(c->stream);
   cudaSetDevice(prev);
@@ -632,6 +639,67 @@ int aldic_int_search(aldic_ctx *c, const int gridx[2], const int gridy[2], int w
     ALDIC_CUDA(cudaStreamSynchronize(c->stream));
   }
   return finish(c, ax.staged || qfactors);
+}
+
+// Multigrid search shared by aldic_int_search_mg and the frame's
+// ALDIC_INIT_SEARCH_MG: levels, node grid, gridfit.  fit receives the five
+// fitted fields (u v Phi q1 q2, x fastest) in context memory.
+static int run_search_mg(aldic_ctx *c, const int gridx[2], const int gridy[2], int winsize, int step,
+                  int nfields, MgData &d, MgGrid &G, double **fit) {
+  int rc = search_mg_levels(c->mg, c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H,
+                            c->stats.as<double>() + 2, gridx, gridy, winsize, nfields > 3, d,
+                            c->stream);
+  if (rc) return rc;
+  ALDIC_CHECK(search_mg_grid(d, winsize, step, c->W, c->H, G), E_ARG,
+              "multigrid search: fewer than 2 x 2 grid points after the border trim");
+  const long long ng = (long long)G.nx * G.ny;
+  if ((rc = ensure_grid_work(c, ng))) return rc;
+  *fit = (double *)c->arena.get(sizeof(double) * 5 * ng);
+  ALDIC_CHECK(*fit, E_NOMEM, "staging buffer allocation failed");
+  if ((rc = search_mg_fit(c->gw, c->mg, d, G, nfields, *fit, c->stream))) return rc;
+  return check_grid_err(c);
+}
+
+int aldic_int_search_mg(aldic_ctx *c, const int gridx[2], const int gridy[2], int winsize, int step,
+                        int *nx, int *ny, int64_t cap, double *x, double *y, double *u, double *v,
+                        double *ccmax, double *qfactors, double *info) {
+  ALDIC_CHECK(c && c->have_ref && c->have_def, E_STATE, "int_search_mg: set both images first");
+  ALDIC_CHECK(gridx && gridy && nx && ny, E_ARG, "int_search_mg: null argument");
+  ALDIC_CHECK(winsize > 0 && step > 0, E_ARG, "int_search_mg: winsize and step must be positive");
+  Guard g(c);
+  MgData d;
+  MgGrid G;
+  double *fit = nullptr;
+  int rc = run_search_mg(c, gridx, gridy, winsize, step, qfactors ? 5 : 3, d, G, &fit);
+  if (rc) return rc;
+  *nx = G.nx;
+  *ny = G.ny;
+  if (info) {
+    info[0] = d.levels;
+    info[1] = (double)d.tx.size();
+    info[2] = d.failed;
+    info[3] = d.l1_u;
+    info[4] = d.l1_v;
+    info[5] = d.l1_cc;
+    for (int k = 0; k < 4; ++k) info[6 + k] = d.t_ms[k];
+  }
+  const long long ng = (long long)G.nx * G.ny;
+  ALDIC_CHECK(cap >= ng, E_ARG, "int_search_mg: the output arrays hold fewer than nx * ny values");
+  ALDIC_CHECK(x && y && u && v && ccmax, E_ARG, "int_search_mg: null output");
+  std::vector<double> hx(ng), hy(ng);
+  for (long long k = 0; k < ng; ++k) {
+    hx[k] = G.x0 + (double)(k % G.nx) * G.step;
+    hy[k] = G.y0 + (double)(k / G.nx) * G.step;
+  }
+  ALDIC_CUDA(cudaMemcpyAsync(x, hx.data(), sizeof(double) * ng, cudaMemcpyDefault, c->stream));
+  ALDIC_CUDA(cudaMemcpyAsync(y, hy.data(), sizeof(double) * ng, cudaMemcpyDefault, c->stream));
+  ALDIC_CUDA(cudaMemcpyAsync(u, fit, sizeof(double) * ng, cudaMemcpyDefault, c->stream));
+  ALDIC_CUDA(cudaMemcpyAsync(v, fit + ng, sizeof(double) * ng, cudaMemcpyDefault, c->stream));
+  ALDIC_CUDA(cudaMemcpyAsync(ccmax, fit + 2 * ng, sizeof(double) * ng, cudaMemcpyDefault, c->stream));
+  if (qfactors)
+    ALDIC_CUDA(cudaMemcpyAsync(qfactors, fit + 3 * ng, sizeof(double) * 2 * ng, cudaMemcpyDefault,
+                               c->stream));
+  return finish(c, true);
 }
 
 int aldic_icgn(aldic_ctx *c, const double *coords, int64_t n, const double *U0,
@@ -1146,17 +1214,27 @@ __global__ void k_mesh_init(int M, int N, const double *sx, const double *sy, co
 
 // MeshSetUp node grid without a search: node (i, j) at XList(i) + w/2,
 // YList(j) + w/2 (funIntegerSearch.m:158-159)
-__global__ void k_mesh_grid(int M, int N, int gx1, int gy1, int step, double hw, double *coords,
+__global__ void k_mesh_grid(int M, int N, double xf, double yf, int step, double *coords,
                             double *x0, double *y0) {
   const long long n = (long long)M * N;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k % M), j = (int)(k / M);
-    const double x = gx1 + (double)i * step + hw, y = gy1 + (double)j * step + hw;
+    const double x = xf + (double)i * step, y = yf + (double)j * step;
     coords[k] = x;
     coords[n + k] = y;
     x0[k] = x;
     y0[k] = y;
+  }
+}
+
+// U0 = [u1 v1 u2 v2 ...] from the multigrid search's fitted u, v fields
+__global__ void k_interleave2(long long n, const double *__restrict__ u, const double *__restrict__ v,
+                              double *__restrict__ U) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    U[2 * k] = u[k];
+    U[2 * k + 1] = v[k];
   }
 }
 
@@ -1259,7 +1337,7 @@ int mark(aldic_ctx *c, int k) {
 }
 
 int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, int M, int N,
-                 const int gx[2], const int gy[2], int gx1, int gy1) {
+                 const int gx[2], const int gy[2], const double node0[2]) {
   cudaStream_t st = c->stream;
   int rcm;
   if ((rcm = mark(c, 0))) return rcm;
@@ -1286,7 +1364,7 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     if ((rc = inpaint_store(c->gw, M, N, 2, B.U0, 2, st, 0))) return rc;
   } else {
     // Section 3 of a later frame: the same mesh, U0 from the previous results
-    k_mesh_grid<<<nb, 256, 0, st>>>(M, N, gx1, gy1, p->step, 0.5 * p->winsize, B.coords, B.x0, B.y0);
+    k_mesh_grid<<<nb, 256, 0, st>>>(M, N, node0[0], node0[1], p->step, B.coords, B.x0, B.y0);
     k_init_hist<<<nb, 256, 0, st>>>(p->init, 2 * n, hist, B.U0);
   }
   // Section 4: LocalICGN + post-processing
@@ -1399,6 +1477,13 @@ extern "C" {
 
 int aldic_frame_dims(aldic_ctx *c, const aldic_frame_params *p, int *M, int *N) {
   ALDIC_CHECK(c && p && M && N && c->have_ref, E_ARG, "frame_dims: bad arguments");
+  ALDIC_CHECK(p->init != ALDIC_INIT_SEARCH_MG, E_ARG,
+              "frame_dims: the multigrid search decides the node grid (see aldic_frame_stats.node_grid)");
+  if (p->node_grid[2] > 0) {
+    *M = (int)p->node_grid[2];
+    *N = (int)p->node_grid[3];
+    return OK;
+  }
   int gx[2], gy[2];
   return frame_geometry(c, p, gx, gy, M, N);
 }
@@ -1426,12 +1511,49 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   ALDIC_CHECK(p->n_admm >= 0 && p->n_admm <= 64, E_ARG, "frame: n_admm must be in [0, 64]");
   ALDIC_CHECK(p->tol > 0 && p->mu > 0, E_ARG, "frame: tol and mu must be positive");
   ALDIC_CHECK(p->tol2 <= 0, E_ARG, "frame: the tol2 early stop is not supported on this path; pass tol2 <= 0 and read update_y");
-  ALDIC_CHECK(p->init >= ALDIC_INIT_SEARCH && p->init <= ALDIC_INIT_GIVEN, E_ARG,
-              "frame: init must be one of ALDIC_INIT_SEARCH/PREV/ZERO/EXTRAP/GIVEN");
+  ALDIC_CHECK(p->init >= ALDIC_INIT_SEARCH && p->init <= ALDIC_INIT_SEARCH_MG, E_ARG,
+              "frame: init must be one of ALDIC_INIT_SEARCH/PREV/ZERO/EXTRAP/GIVEN/SEARCH_MG");
   Guard g(c);
-  int gx[2], gy[2], M, N, gx1, gy1;
-  int rc = frame_geometry(c, p, gx, gy, &M, &N, &gx1, &gy1);
-  if (rc) return rc;
+  int gx[2], gy[2], M, N;
+  int rc;
+  aldic_frame_params qp = *p;  // the parameters the device work sees
+  double node0[2];            // first node of the grid
+  double *mg_fit = nullptr;
+  double t_mg = 0.0;
+  if (p->init == ALDIC_INIT_SEARCH_MG) {
+    // IntegerSearch.m:117-120 + MeshSetUp + Init: the multigrid search decides
+    // the node grid; the rest of the frame runs as with a given U0
+    gx[0] = p->gridx[0]; gx[1] = p->gridx[1];
+    gy[0] = p->gridy[0]; gy[1] = p->gridy[1];
+    if (gx[0] == 0 && gx[1] == 0) { gx[0] = 1; gx[1] = c->W; }
+    if (gy[0] == 0 && gy[1] == 0) { gy[0] = 1; gy[1] = c->H; }
+    MgData d;
+    MgGrid G;
+    const auto t0 = std::chrono::steady_clock::now();
+    // u and v only: Init (index 0) uses neither Phi nor the q-factors
+    if ((rc = run_search_mg(c, gx, gy, p->winsize, p->step, 2, d, G, &mg_fit))) return rc;
+    t_mg = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    M = G.nx;
+    N = G.ny;
+    node0[0] = G.x0;
+    node0[1] = G.y0;
+    qp.init = ALDIC_INIT_GIVEN;
+  } else if (p->node_grid[2] > 0) {
+    ALDIC_CHECK(p->init != ALDIC_INIT_SEARCH, E_ARG,
+                "frame: an explicit node grid takes a U0 that is not searched (PREV/ZERO/EXTRAP/GIVEN)");
+    M = (int)p->node_grid[2];
+    N = (int)p->node_grid[3];
+    ALDIC_CHECK(M >= 2 && N >= 2 && M == p->node_grid[2] && N == p->node_grid[3], E_ARG,
+                "frame: node_grid needs whole M, N >= 2");
+    node0[0] = p->node_grid[0];
+    node0[1] = p->node_grid[1];
+    gx[0] = gx[1] = gy[0] = gy[1] = 0;
+  } else {
+    int gx1, gy1;
+    if ((rc = frame_geometry(c, p, gx, gy, &M, &N, &gx1, &gy1))) return rc;
+    node0[0] = gx1 + 0.5 * p->winsize;  // MeshSetUp: (ii + ii + w) / 2
+    node0[1] = gy1 + 0.5 * p->winsize;
+  }
   const long long n = (long long)M * N;
   if (c->hist_n != n) {
     if ((rc = c->hist.ensure(sizeof(double) * 6 * n))) return rc;
@@ -1439,11 +1561,17 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     c->hist_count = 0;
     c->have_given = false;
   }
-  ALDIC_CHECK(p->init != ALDIC_INIT_PREV || c->hist_count >= 1, E_STATE,
+  if (mg_fit) {
+    k_interleave2<<<(unsigned)std::min<long long>((n + 255) / 256, 1184), 256, 0, c->stream>>>(
+        n, mg_fit, mg_fit + n, c->hist.as<double>() + 4 * n);
+    ALDIC_CUDA(cudaGetLastError());
+    c->have_given = true;
+  }
+  ALDIC_CHECK(qp.init != ALDIC_INIT_PREV || c->hist_count >= 1, E_STATE,
               "frame: ALDIC_INIT_PREV needs a previous frame on this node grid");
-  ALDIC_CHECK(p->init != ALDIC_INIT_EXTRAP || c->hist_count >= 2, E_STATE,
+  ALDIC_CHECK(qp.init != ALDIC_INIT_EXTRAP || c->hist_count >= 2, E_STATE,
               "frame: ALDIC_INIT_EXTRAP needs two previous frames on this node grid");
-  ALDIC_CHECK(p->init != ALDIC_INIT_GIVEN || c->have_given, E_STATE,
+  ALDIC_CHECK(qp.init != ALDIC_INIT_GIVEN || c->have_given, E_STATE,
               "frame: ALDIC_INIT_GIVEN needs aldic_set_init on this node grid");
   if ((rc = ensure_grid_work(c, n))) return rc;
   // frame slab
@@ -1471,10 +1599,11 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   // graph key: geometry, every parameter that changes the recorded work and
   // the buffers the graph addresses
   char key[512];
-  snprintf(key, sizeof key, "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p",
+  snprintf(key, sizeof key,
+           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p",
            c->W, c->H, c->dtype, p->winsize, p->step, p->search[0], p->search[1], gx[0], gx[1],
-           gy[0], gy[1], p->tol, p->mu, p->beta, p->n_admm, p->precision, p->smooth,
-           p->init * 2 + (p->subpb2_fd != 0),
+           gy[0], gy[1], node0[0], node0[1], M, N, p->tol, p->mu, p->beta, p->n_admm, p->precision,
+           p->smooth, qp.init * 2 + (p->subpb2_fd != 0),
            c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p);
   if (realloc) c->drop_graphs();  // recorded against buffers that are gone
   const bool want_graph = p->use_graph && !c->graph_failed;
@@ -1497,7 +1626,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     cudaGraph_t gr = nullptr;
     bool okc = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (okc) {
-      int rc2 = frame_device(c, p, B, M, N, gx, gy, gx1, gy1);
+      int rc2 = frame_device(c, &qp, B, M, N, gx, gy, node0);
       cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
       okc = rc2 == OK && e == cudaSuccess && gr;
       if (okc) okc = cudaGraphInstantiate(&rec.exec, gr, 0) == cudaSuccess;
@@ -1528,7 +1657,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   if (fg) {
     ALDIC_CUDA(cudaGraphLaunch(fg->exec, c->stream));
   } else {
-    if ((rc = frame_device(c, p, B, M, N, gx, gy, gx1, gy1))) return rc;
+    if ((rc = frame_device(c, &qp, B, M, N, gx, gy, node0))) return rc;
   }
   if (c->hist_count < 2) c->hist_count++;
   // outputs
@@ -1567,6 +1696,11 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     stats->mean_iters_icgn = hs.meanit;
     stats->kernel_launches = fg ? fg->kernels : -1;
     stats->max_pcg_iters = hs.pcg_its;
+    stats->node_grid[0] = node0[0];
+    stats->node_grid[1] = node0[1];
+    stats->node_grid[2] = M;
+    stats->node_grid[3] = N;
+    stats->t_search_mg_ms = t_mg;
     for (int k = 0; k < 6; ++k) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]) == cudaSuccess) stats->t_stage_ms[k] = ms;

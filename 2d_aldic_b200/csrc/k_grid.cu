@@ -26,6 +26,7 @@ constexpr int MAXRHS = 12;
 
 struct PcgArgs {
   double *x, *r, *z, *p0, *p1, *q, *b, *diag, *part;
+  double *zz, *qq, *ss, *pp;  // pipelined-CG directions
   const unsigned char *mask;
   int M, N, nrhs, maxit, blocks;
   double mu, h, lam2, rtol;
@@ -34,6 +35,7 @@ struct PcgArgs {
   GridSync gs;
   int *iters_out;
   CsrOp csr;               // OP_CSR
+  const double *ata;       // OP_GRIDFIT with scattered data: A'A, 9 coefficients per node
 };
 
 // Scalar Q4 element matrices on a square element of size h with local nodes
@@ -109,7 +111,7 @@ __device__ __forceinline__ double op_diag(const PcgArgs &A, double beta, int i, 
   } else if (OP == OP_CSR) {
     return A.mask[(long long)f * M * N + k] ? A.csr.diag[k] : 1.0;
   } else if (OP == OP_GRIDFIT) {
-    const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
+    const double w = A.ata ? A.ata[9 * k + 4] : (A.mask[(long long)f * M * N + k] ? 1.0 : 0.0);
     const int na = (i > 0) + (i < M - 1) + (j > 0) + (j < N - 1);
     const int nd = (i > 0 && j > 0) + (i < M - 1 && j > 0) + (i > 0 && j < N - 1) +
                    (i < M - 1 && j < N - 1);
@@ -167,8 +169,26 @@ __device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i,
     if (i < M - 1 && j > 0) sd += xk - v[k - M + 1];
     if (i > 0 && j < N - 1) sd += xk - v[k + M - 1];
     if (i < M - 1 && j < N - 1) sd += xk - v[k + M + 1];
-    const double w = A.mask[(long long)f * M * N + k] ? 1.0 : 0.0;
-    return w * xk + A.lam2 * (s + 0.5 * sd);
+    double dterm;
+    if (A.ata) {  // scattered data: the 9-point A'A stencil of the triangle interpolation
+      const double *c = A.ata + 9 * k;
+      dterm = c[4] * xk;
+      if (i > 0) dterm += c[3] * v[k - 1];
+      if (i < M - 1) dterm += c[5] * v[k + 1];
+      if (j > 0) {
+        dterm += c[1] * v[k - M];
+        if (i > 0) dterm += c[0] * v[k - M - 1];
+        if (i < M - 1) dterm += c[2] * v[k - M + 1];
+      }
+      if (j < N - 1) {
+        dterm += c[7] * v[k + M];
+        if (i > 0) dterm += c[6] * v[k + M - 1];
+        if (i < M - 1) dterm += c[8] * v[k + M + 1];
+      }
+    } else {
+      dterm = (A.mask[(long long)f * M * N + k] ? 1.0 : 0.0) * xk;
+    }
+    return dterm + A.lam2 * (s + 0.5 * sd);
   } else {
     const unsigned char *unk = A.mask + (long long)f * M * N;
     const double xk = v[k];
@@ -227,13 +247,21 @@ __device__ void global_sums(PcgShared &S, const double *part, int cnt, int block
   __syncthreads();
 }
 
-// Preconditioned CG in the Chronopoulos-Gear arrangement: one mat-vec per
-// iteration on the preconditioned residual u (w = A u), the recurrences
-// p = u + beta p, s = w + beta s (s = A p), and the three dot products
-// (r,u), (w,u), (r,r) reduced together -- two grid barriers per iteration.
-// Fields are processed one after another inside each phase (few live
-// registers); per-field scalars live in shared memory.
-// Buffers: x, r, u (= z slot), w (= q slot), p (p0), s (p1), 1/diag.
+// Pipelined preconditioned CG (Ghysels and Vanroose, "Hiding global
+// synchronization latency in the preconditioned Conjugate Gradient
+// algorithm", Parallel Computing 40, 2014): with u = M^-1 r, w = A u,
+// m = M^-1 w, n = A m the recurrences
+//   z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
+//   x += alpha p, r -= alpha s, u -= alpha q, w -= alpha z
+// need the dot products (r,u), (w,u) of the current vectors and one mat-vec
+// n = A m, so an iteration is ONE sweep (the mat-vec and updates of a node,
+// then its next dot-product terms and m = w / diag) and ONE grid barrier
+// (the dot products' block partials, and every m, complete).  m and the
+// partials alternate between two buffers, so a block that runs ahead never
+// overwrites what a slower block still reads.  Jacobi preconditioner M =
+// diag(A); convergence on the recursive residual, |r| <= rtol |b|.
+// Buffers: x, r, u (= z slot), w (= q slot), m (p0 / p1), the directions
+// zz, qq, ss, pp, 1/diag.
 template <int OP, int NR>
 __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
   __shared__ PcgShared S;
@@ -246,9 +274,11 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
   const int M = A.M;
   const long long tid0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  double *const X = A.x, *const R = A.r, *const Uv = A.z, *const Wv = A.q, *const Pv = A.p0,
-               *const Sv = A.p1, *const Di = A.diag;
-  // ---- r = b - A x, u = D^-1 r, p = s = 0
+  double *const X = A.x, *const R = A.r, *const Uv = A.z, *const Wv = A.q, *const Di = A.diag;
+  double *const Zd = A.zz, *const Qd = A.qq, *const Sd = A.ss, *const Pd = A.pp;
+  double *Mv[2] = {A.p0, A.p1};
+  const long long pstride = (long long)4 * MAXRHS * A.blocks;  // second partials buffer
+  // ---- r = b - A x, u = D^-1 r, directions 0
 #pragma unroll 1
   for (int f = 0; f < NR; ++f) {
     const double bt = A.beta[f];
@@ -260,12 +290,14 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
       R[o] = rv;
       Uv[o] = rv * dinv;
       Di[o] = dinv;
-      Pv[o] = 0.0;
-      Sv[o] = 0.0;
+      Zd[o] = 0.0;
+      Qd[o] = 0.0;
+      Sd[o] = 0.0;
+      Pd[o] = 0.0;
     }
   }
   if (!grid_sync(A.gs, A.blocks)) return;
-  // ---- w = A u; partials (r,u) (w,u) (r,r) (b,b)
+  // ---- w = A u, m = D^-1 w; partials (r,u) (w,u) (r,r) (b,b)
 #pragma unroll 1
   for (int f = 0; f < NR; ++f) {
     const double bt = A.beta[f];
@@ -275,6 +307,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
       const long long o = f * n + k;
       const double wv = op_apply<OP>(A, bt, i, j, k, f, Uv + f * n);
       Wv[o] = wv;
+      Mv[0][o] = wv * Di[o];
       const double rv = R[o], uv = Uv[o], bv = A.b[o];
       a0 += rv * uv;
       a1 += wv * uv;
@@ -304,36 +337,35 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
 #pragma unroll
     for (int f = 0; f < NR; ++f) all &= (S.done[f] != 0);
     if (all) break;
-    // ---- p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = D^-1 r
-#pragma unroll 1
-    for (int f = 0; f < NR; ++f) {
-      if (S.done[f]) continue;
-      const double al = S.alpha[f], be = S.beta[f];
-      for (long long k = tid0; k < n; k += stride) {
-        const long long o = f * n + k;
-        const double pv = Uv[o] + be * Pv[o];
-        const double sv = Wv[o] + be * Sv[o];
-        Pv[o] = pv;
-        Sv[o] = sv;
-        X[o] += al * pv;
-        const double rv = R[o] - al * sv;
-        R[o] = rv;
-        Uv[o] = rv * Di[o];
-      }
-    }
-    if (!grid_sync(A.gs, A.blocks)) return;
-    // ---- w = A u and the three dot products
+    const double *Mo = Mv[it & 1];
+    double *Mn = Mv[(it + 1) & 1];
+    double *part = A.part + ((it + 1) & 1) * pstride;
+    // ---- n = A m; directions and iterates; next partials and m
 #pragma unroll 1
     for (int f = 0; f < NR; ++f) {
       double a0 = 0.0, a1 = 0.0, a2 = 0.0;
       if (!S.done[f]) {
-        const double bt = A.beta[f];
+        const double bt = A.beta[f], al = S.alpha[f], be = S.beta[f];
         for (long long k = tid0; k < n; k += stride) {
           const int i = (int)(k % M), j = (int)(k / M);
           const long long o = f * n + k;
-          const double wv = op_apply<OP>(A, bt, i, j, k, f, Uv + f * n);
+          const double nv = op_apply<OP>(A, bt, i, j, k, f, Mo + f * n);
+          const double zv = nv + be * Zd[o];
+          const double qv = Mo[o] + be * Qd[o];
+          const double sv = Wv[o] + be * Sd[o];
+          const double pv = Uv[o] + be * Pd[o];
+          Zd[o] = zv;
+          Qd[o] = qv;
+          Sd[o] = sv;
+          Pd[o] = pv;
+          X[o] += al * pv;
+          const double rv = R[o] - al * sv;
+          const double uv = Uv[o] - al * qv;
+          const double wv = Wv[o] - al * zv;
+          R[o] = rv;
+          Uv[o] = uv;
           Wv[o] = wv;
-          const double rv = R[o], uv = Uv[o];
+          Mn[o] = wv * Di[o];
           a0 += rv * uv;
           a1 += wv * uv;
           a2 += rv * rv;
@@ -343,9 +375,9 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
       warp_stage(S, NR + f, a1);
       warp_stage(S, 2 * NR + f, a2);
     }
-    block_partials(S, 3 * NR, A.part, A.blocks);
+    block_partials(S, 3 * NR, part, A.blocks);
     if (!grid_sync(A.gs, A.blocks)) return;
-    global_sums(S, A.part, 3 * NR, A.blocks);
+    global_sums(S, part, 3 * NR, A.blocks);
     if (threadIdx.x < NR) {
       const int f = threadIdx.x;
       if (!S.done[f]) {
@@ -809,7 +841,7 @@ inline int blocks_for(long long n, int threads = 256) {
 
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
              double lam2, double rtol, int maxit, cudaStream_t st, const double *beta_ptr,
-             const double *beta_each) {
+             const double *beta_each, const double *ata) {
   ALDIC_CHECK(nrhs >= 1 && nrhs <= MAXRHS, E_ARG, "grid_pcg: 1..12 right-hand sides");
   const long long n = (long long)M * N;
   int dev = 0, sms = 148, per = 1;
@@ -841,6 +873,7 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
   PcgArgs A;
   A.x = w.x; A.r = w.r; A.z = w.z; A.p0 = w.p; A.p1 = w.p + MAXRHS * n; A.q = w.q; A.b = w.b;
   A.diag = w.diag; A.part = w.part; A.mask = w.mask;
+  A.zz = w.zz; A.qq = w.qq; A.ss = w.ss; A.pp = w.pp;
   if (nr_pad > nrhs) {  // padded right-hand sides: b = x = 0 converge at once
     ALDIC_CUDA(cudaMemsetAsync(w.b + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
     ALDIC_CUDA(cudaMemsetAsync(w.x + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
@@ -853,6 +886,7 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
   A.iters_out = w.iters_out;
   A.beta_ptr = beta_ptr;
   A.csr = CsrOp{};
+  A.ata = op == OP_GRIDFIT ? ata : nullptr;
   ALDIC_CUDA(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned int), st));
   void *args[] = {&A};
   ALDIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(PCG_THREADS), args, 0, st));
@@ -882,6 +916,7 @@ int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, in
   PcgArgs A;
   A.x = w.x; A.r = w.r; A.z = w.z; A.p0 = w.p; A.p1 = w.p + MAXRHS * n; A.q = w.q; A.b = w.b;
   A.diag = w.diag; A.part = w.part; A.mask = w.mask;
+  A.zz = w.zz; A.qq = w.qq; A.ss = w.ss; A.pp = w.pp;
   if (nr_pad > nrhs) {
     ALDIC_CUDA(cudaMemsetAsync(w.b + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
     ALDIC_CUDA(cudaMemsetAsync(w.x + nrhs * n, 0, sizeof(double) * (nr_pad - nrhs) * n, st));
@@ -894,6 +929,7 @@ int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, in
   A.iters_out = w.iters_out;
   A.beta_ptr = nullptr;
   A.csr = op;
+  A.ata = nullptr;
   ALDIC_CUDA(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned int), st));
   void *args[] = {&A};
   ALDIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3((unsigned)blocks), dim3(PCG_THREADS), args, 0, st));

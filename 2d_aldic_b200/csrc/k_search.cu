@@ -14,13 +14,13 @@
 // sub-pixel peak bit-identical to it.
 #include "aldic_internal.cuh"
 #include "kernels.cuh"
+#include "ncc.cuh"
 
 namespace aldic {
 
 namespace {
 
 constexpr int KX = 8;
-constexpr double kSqrtEps = 1.4901161193847656e-08;  // sqrt(DBL_EPSILON) = 2^-26
 
 template <typename T> struct SearchTraits;
 template <> struct SearchTraits<uint8_t> {
@@ -75,88 +75,6 @@ struct SmemLayout {
     total = o;
   }
 };
-
-// NCC at one cropped-map entry from the exact partial sums (same arithmetic
-// as the CPU restatement's ncc_at).
-__device__ __forceinline__ double ncc_combine(long long mn, long long st, long long st2,
-                                              long long stdv, long long sd, long long sd2,
-                                              long long st_pad, long long n_pad, double mu) {
-  const double denT = (double)(mn * st2 - st * st);
-  const double A = (double)(mn * stdv - st * sd);
-  const double C0 = (double)(mn * sd2 - sd * sd);
-  double B = 0.0, Cc = 0.0;
-  if (n_pad > 0) {
-    B = __dmul_rn(mu, (double)(mn * st_pad - st * n_pad));
-    Cc = __dmul_rn(mu, __dsub_rn(__dmul_rn((double)(n_pad * (mn - n_pad)), mu),
-                                 __dmul_rn(2.0, (double)(sd * n_pad))));
-  }
-  const double num = __dadd_rn(A, B);
-  const double den = __dadd_rn(C0, Cc);
-  if (!(den > 0.0)) return 0.0;
-  double r = __ddiv_rn(num, __dsqrt_rn(__dmul_rn(denT, den)));
-  if (__dsub_rn(fabs(r), 1.0) > kSqrtEps) r = 0.0;
-  return r;
-}
-
-__device__ __forceinline__ double ncc_combine_f(double mn, double st, double st2, double stdv,
-                                                double sd, double sd2, double st_pad,
-                                                double n_pad, double mu) {
-  const double denT = mn * st2 - st * st;
-  const double A = mn * stdv - st * sd;
-  const double C0 = mn * sd2 - sd * sd;
-  double B = 0.0, Cc = 0.0;
-  if (n_pad > 0) {
-    B = mu * (mn * st_pad - st * n_pad);
-    Cc = mu * ((n_pad * (mn - n_pad)) * mu - 2.0 * (sd * n_pad));
-  }
-  const double num = A + B, den = C0 + Cc;
-  if (!(den > 0.0)) return 0.0;
-  double r = num / sqrt(denT * den);
-  if (fabs(r) - 1.0 > kSqrtEps) r = 0.0;
-  return r;
-}
-
-// findpeak.m:27-66 with the closed-form 3x3 quadratic fit (same operation
-// order as the CPU restatement).
-__device__ void findpeak_fit(const double *map, int nr, int nc, int im, double *row_pk,
-                             double *col_pk, double *max_f) {
-  const int r = im % nr, c = im / nr;
-  *row_pk = r + 1;
-  *col_pk = c + 1;
-  *max_f = map[im];
-  if (r == 0 || r == nr - 1 || c == 0 || c == nc - 1) return;
-  double s0 = 0, sxu = 0, syu = 0, sxyu = 0, sxxu = 0, syyu = 0;
-  for (int dc = -1; dc <= 1; ++dc)
-    for (int dr = -1; dr <= 1; ++dr) {
-      const double u = map[(c + dc) * nr + (r + dr)];
-      s0 = __dadd_rn(s0, u);
-      sxu = __dadd_rn(sxu, __dmul_rn((double)dc, u));
-      syu = __dadd_rn(syu, __dmul_rn((double)dr, u));
-      sxyu = __dadd_rn(sxyu, __dmul_rn((double)(dc * dr), u));
-      sxxu = __dadd_rn(sxxu, __dmul_rn((double)(dc * dc), u));
-      syyu = __dadd_rn(syyu, __dmul_rn((double)(dr * dr), u));
-    }
-  const double A2 = __ddiv_rn(sxu, 6.0), A3 = __ddiv_rn(syu, 6.0), A4 = __ddiv_rn(sxyu, 4.0);
-  const double p = __dsub_rn(__dmul_rn(0.5, __dadd_rn(sxxu, syyu)), __dmul_rn(2.0 / 3.0, s0));
-  const double q = __dmul_rn(0.5, __dsub_rn(sxxu, syyu));
-  const double A5 = __dmul_rn(0.5, __dadd_rn(p, q)), A6 = __dmul_rn(0.5, __dsub_rn(p, q));
-  const double A1 = __ddiv_rn(__dsub_rn(s0, __dmul_rn(6.0, p)), 9.0);
-  const double den = __dsub_rn(__dmul_rn(A4, A4), __dmul_rn(__dmul_rn(4.0, A5), A6));
-  double xo = __ddiv_rn(__dadd_rn(__dmul_rn(-A3, A4), __dmul_rn(__dmul_rn(2.0, A6), A2)), den);
-  double yo = __dmul_rn(__ddiv_rn(-1.0, den),
-                        __dsub_rn(__dmul_rn(A4, A2), __dmul_rn(__dmul_rn(2.0, A5), A3)));
-  if (fabs(xo) > 1.0 || fabs(yo) > 1.0) return;
-  xo = __ddiv_rn(round(__dmul_rn(1000.0, xo)), 1000.0);
-  yo = __ddiv_rn(round(__dmul_rn(1000.0, yo)), 1000.0);
-  *col_pk = __dadd_rn((double)(c + 1), xo);
-  *row_pk = __dadd_rn((double)(r + 1), yo);
-  double m = __dadd_rn(A1, __dmul_rn(A2, xo));
-  m = __dadd_rn(m, __dmul_rn(A3, yo));
-  m = __dadd_rn(m, __dmul_rn(A4, __dmul_rn(xo, yo)));
-  m = __dadd_rn(m, __dmul_rn(A5, __dmul_rn(xo, xo)));
-  m = __dadd_rn(m, __dmul_rn(A6, __dmul_rn(yo, yo)));
-  *max_f = m;
-}
 
 // Argmax of the cropped map (first maximum in column-major order, as
 // MATLAB's max), the sub-pixel fit of findpeak.m and the outputs of

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace aldic {
 
 // ---- k_image.cu
@@ -42,9 +44,11 @@ int subpb1(const IcgnImages &im, const double *coords, long long n, const double
 
 // ---- k_grid.cu: node-grid solvers and field kernels on the M x N mesh
 struct GridWork {
-  // PCG vectors for up to 12 right-hand sides of M*N (x fastest) each
+  // PCG vectors for up to 12 right-hand sides of M*N (x fastest) each; p is
+  // two vectors (the second 12*M*N after the first)
   double *x, *r, *z, *p, *q, *b, *diag;
-  double *part;          // per-block partial sums: [3][nrhs][blocks]
+  double *zz, *qq, *ss, *pp;  // pipelined-CG directions
+  double *part;          // per-block partial sums: 2 buffers of [4][nrhs][blocks]
   unsigned char *mask;   // per node flags (data present / unknown)
   unsigned int *bar;     // grid barrier {count, gen}
   int *err;              // barrier / solver error flag
@@ -129,9 +133,12 @@ int cnn_patches(const float *f, const float *g, int W, int H, const double *coor
 int cnn_to_init(const float *out, long long n, double *U0, double *F0, float *conf, cudaStream_t st);
 
 // solve op(x) = b for nrhs fields; b and x live in w.b / w.x (field-major)
+// ata (OP_GRIDFIT only, may be NULL): scattered-data A'A as 9 coefficients per
+// node (offsets (di, dj) in row-major 3 x 3 order); the mask is then unused
 int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu, double h,
              double lam2, double rtol, int maxit, cudaStream_t st,
-             const double *beta_ptr = nullptr, const double *beta_each = nullptr);
+             const double *beta_ptr = nullptr, const double *beta_each = nullptr,
+             const double *ata = nullptr);
 // Subpb2 right-hand side (Subpb2.m:76-159) into w.b (2 fields: u, v)
 int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
            const double *F, const double *udual, const double *vdual, cudaStream_t st,
@@ -163,5 +170,39 @@ int vsub(const double *a, const double *b, double *out, long long n, cudaStream_
 // ||a - b||_2 into *res (deterministic)
 int vdiffnorm(const double *a, const double *b, long long n, double *part, double *res,
               cudaStream_t st);
+
+// ---- multigrid integer search (k_searchmg.cu, funIntegerSearchMg.m)
+struct MgWork {
+  DevBuf sat, tot;         // summed-area tables of f, f^2, g, g^2 and column-chunk totals
+  DevBuf fft, tw, part;    // level-1 transforms, twiddles, argmax partials
+  DevBuf regs, acc, res;   // per-level region descriptors, crop products, results
+  DevBuf csr;              // gridfit normal equations
+  void release() {
+    for (DevBuf *b : {&sat, &tot, &fft, &tw, &part, &regs, &acc, &res, &csr}) b->release();
+  }
+};
+// last level of the search: region centres and their results (NaN where the
+// correlation raised; Phi 0 there), normalised q-factors, the trimmed ROI
+struct MgData {
+  std::vector<double> tx, ty, u, v, phi, q1, q2;
+  int gridx[2] = {0, 0}, gridy[2] = {0, 0};
+  int levels = 0, failed = 0;
+  double l1_u = 0, l1_v = 0, l1_cc = 0;  // level-1 (whole ROI) shift and peak
+  double t_ms[4] = {0, 0, 0, 0};         // host time: tables + level 1, levels 2.., last level, fit
+};
+struct MgGrid {
+  double x0 = 0, y0 = 0;  // first node (xList(1), yList(1))
+  int nx = 0, ny = 0, step = 1;
+};
+// qfactors: compute the last level's full maps and compute_qFactor (else
+// only the 13 x 14 crops, q1/q2 NaN)
+int search_mg_levels(MgWork &w, const void *f, const void *g, int dtype, int W, int H,
+                     const double *mu_g, const int gridx[2], const int gridy[2], int winsize,
+                     bool qfactors, MgData &out, cudaStream_t st);
+bool search_mg_grid(const MgData &d, int winsize, int step, int W, int H, MgGrid &grid);
+// out: the first nfields of (u v Phi q1 q2), nx*ny values each, x fastest;
+// gw sized for nx*ny
+int search_mg_fit(GridWork &gw, MgWork &w, MgData &d, const MgGrid &grid, int nfields,
+                  double *out, cudaStream_t st);
 
 }  // namespace aldic

@@ -21,11 +21,12 @@
 namespace aldic {
 namespace {
 
-// 2 displacement fields x 8 PCG vectors per node, for at most this many nodes
+// 2 displacement fields x 12 PCG vectors per node, for at most this many nodes
 constexpr long long kNoAllocMaxNodes = 65536;  // e.g. a 256 x 256 node grid
 constexpr int kNoAllocMaxBlocks = 192;         // cooperative grid: one block per SM
-constexpr long long kVecDoubles = 8 * 2 * kNoAllocMaxNodes;
-constexpr long long kPartDoubles = 4 * 2 * kNoAllocMaxBlocks;
+constexpr long long kVecDoubles = 12 * 2 * kNoAllocMaxNodes;
+// two buffers of block partials, laid out for up to 12 right-hand sides
+constexpr long long kPartDoubles = 2 * 4 * 12 * kNoAllocMaxBlocks;
 
 struct NoAllocScratch {
   double vec[kVecDoubles];
@@ -34,7 +35,7 @@ struct NoAllocScratch {
   unsigned int ctl[16];  // barrier count/generation, error flag, iteration count
 };
 
-// The scratch (~8.4 MB).  Host code must not use &g_scratch as a device
+// The scratch (~12.7 MB).  Host code must not use &g_scratch as a device
 // address: it is a host-side stand-in; the device address comes from
 // cudaGetSymbolAddress below.
 static __device__ __align__(256) NoAllocScratch g_scratch;
@@ -82,8 +83,8 @@ extern "C" int aldic_subpb2_noalloc(int M, int N, double step, double beta, doub
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   // PCG vectors for two right-hand sides, 2n values each, packed for this n.
-  // grid_pcg keeps its second search-direction buffer 12n after the first,
-  // so p0 sits at 0, p1 at 12n, and the other six vectors fill the gap.
+  // grid_pcg keeps its second m buffer 12n after the first, so p0 sits at
+  // 0, p1 at 12n, five vectors fill the gap and the rest follow.
   double *v = S->vec;
   GridWork w{};
   w.p = v;
@@ -93,6 +94,10 @@ extern "C" int aldic_subpb2_noalloc(int M, int N, double step, double beta, doub
   w.q = v + 8 * n;
   w.b = v + 10 * n;
   w.diag = v + 14 * n;
+  w.zz = v + 16 * n;
+  w.qq = v + 18 * n;
+  w.ss = v + 20 * n;
+  w.pp = v + 22 * n;
   w.part = S->part;
   w.mask = S->mask;
   w.bar = S->ctl;

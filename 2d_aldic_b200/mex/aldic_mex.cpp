@@ -14,6 +14,12 @@
 //       Subpb2.m on the uniform mesh of MeshSetUp.m
 //   F = aldic_mex('strain', M, N, winstepsize, U)
 //       funGlobal_NodalStrainAvg.m on the uniform mesh
+//   [x0,y0,u,v,ccmax] = aldic_mex('searchmg', ImgRef, ImgDef, gridx, gridy, winsize,
+//                                 winstepsize)
+//       funIntegerSearchMg.m (IntegerSearch.m:117-120), ny x nx outputs
+//   [FStrain,FStrainFinite] = aldic_mex('computestrain', M, N, winstepsize, method, rad,
+//                                       straintype, U, F)
+//       ComputeStrain.m Section 8 (F is read by method 0 only; pass [] otherwise)
 // ImgRef/ImgDef are the normalised W x H doubles; DfDx/DfDy are the reference's
 // (W-6) x (H-6) Df.DfDx/Df.DfDy.  The GPU context persists across calls
 // (mexLock), images and gradients are re-uploaded on every icgn/subpb1 call.
@@ -120,6 +126,51 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
     plhs[0] = mxCreateDoubleMatrix(4 * (size_t)M * N, 1, mxREAL);
     check(aldic_nodal_strain(ctx(), M, N, mxGetScalar(prhs[3]), dbl(prhs[4], "U"),
                              mxGetPr(plhs[0])));
+  } else if (c == "searchmg") {
+    if (nrhs != 7) mexErrMsgIdAndTxt("aldic:usage", "searchmg takes 6 arguments");
+    const size_t W = mxGetM(prhs[1]), H = mxGetN(prhs[1]);
+    if (mxGetM(prhs[2]) != W || mxGetN(prhs[2]) != H)
+      mexErrMsgIdAndTxt("aldic:size", "ImgRef/ImgDef differ");
+    if (mxGetNumberOfElements(prhs[3]) != 2 || mxGetNumberOfElements(prhs[4]) != 2)
+      mexErrMsgIdAndTxt("aldic:size", "gridx and gridy are [first last]");
+    std::vector<double> zeros(W * H, 0.0);  // gradients: not used by the search
+    check(aldic_set_fields(ctx(), dbl(prhs[1], "ImgRef"), dbl(prhs[2], "ImgDef"), zeros.data(),
+                           zeros.data(), (int)W, (int)H));
+    const double *gxd = dbl(prhs[3], "gridx"), *gyd = dbl(prhs[4], "gridy");
+    const int gx[2] = {(int)gxd[0], (int)gxd[1]}, gy[2] = {(int)gyd[0], (int)gyd[1]};
+    const int step = (int)mxGetScalar(prhs[6]);
+    if (step <= 0) mexErrMsgIdAndTxt("aldic:usage", "winstepsize must be positive");
+    const int64_t cap = (int64_t)(W / step + 1) * (int64_t)(H / step + 1);
+    std::vector<double> buf(5 * (size_t)cap);
+    int nx = 0, ny = 0;
+    check(aldic_int_search_mg(ctx(), gx, gy, (int)mxGetScalar(prhs[5]), step, &nx, &ny, cap,
+                              &buf[0], &buf[cap], &buf[2 * cap], &buf[3 * cap], &buf[4 * cap],
+                              nullptr, nullptr));
+    // library order x fastest -> MATLAB ny x nx column-major
+    for (int o = 0; o < 5 && o < (nlhs > 0 ? nlhs : 1); ++o) {
+      plhs[o] = mxCreateDoubleMatrix((size_t)ny, (size_t)nx, mxREAL);
+      double *dst = mxGetPr(plhs[o]);
+      for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix)
+          dst[iy + (size_t)ix * ny] = buf[(size_t)o * cap + (size_t)iy * nx + ix];
+    }
+  } else if (c == "computestrain") {
+    if (nrhs != 9) mexErrMsgIdAndTxt("aldic:usage", "computestrain takes 8 arguments");
+    const int M = (int)mxGetScalar(prhs[1]), N = (int)mxGetScalar(prhs[2]);
+    const int method = (int)mxGetScalar(prhs[4]);
+    const size_t n = (size_t)M * N;
+    if (mxGetNumberOfElements(prhs[7]) != 2 * n) mexErrMsgIdAndTxt("aldic:size", "U is 2*M*N");
+    const double *F = nullptr;
+    if (method == 0) {
+      if (mxGetNumberOfElements(prhs[8]) != 4 * n) mexErrMsgIdAndTxt("aldic:size", "F is 4*M*N");
+      F = dbl(prhs[8], "F");
+    }
+    plhs[0] = mxCreateDoubleMatrix(4 * n, 1, mxREAL);
+    mxArray *fin = mxCreateDoubleMatrix(4 * n, 1, mxREAL);
+    check(aldic_compute_strain(ctx(), M, N, mxGetScalar(prhs[3]), method, (int)mxGetScalar(prhs[5]),
+                               (int)mxGetScalar(prhs[6]), dbl(prhs[7], "U"), F, mxGetPr(plhs[0]),
+                               mxGetPr(fin)));
+    if (nlhs > 1) plhs[1] = fin; else mxDestroyArray(fin);
   } else {
     mexErrMsgIdAndTxt("aldic:usage", "unknown command '%s'", cmd);
   }

@@ -137,6 +137,23 @@ class Workload:
         g = warp(f, self.field, self.noise * self.scale, self.seed)
         return f, g
 
+    def images_t(self, device="cpu"):
+        """images() generated with torch (on the GPU when one is given): the
+        same speckle draws and warp recipe, noise from torch's generator;
+        fields must accept torch tensors."""
+        import torch
+        f = quantise_t(speckle_t(self.W, self.H, self.ndots, self.seed, device=device,
+                                 scale=self.scale), self.dtype)
+        ys, xs = torch.meshgrid(torch.arange(1, self.H + 1, dtype=torch.float64, device=device),
+                                torch.arange(1, self.W + 1, dtype=torch.float64, device=device),
+                                indexing="ij")
+        X, Y = invert_t(self.field, xs, ys)
+        g = bicubic_sample_t(f.to(torch.float64), X, Y)
+        gen = torch.Generator(device=device).manual_seed(self.seed + 1000)
+        g = g + self.noise * self.scale * torch.randn(g.shape, generator=gen, dtype=torch.float64,
+                                                      device=device)
+        return f, quantise_t(g, self.dtype)
+
 
 def _affine_small(X, Y):
     return 0.5 + 0.01 * X, -0.3 + 0.005 * Y
@@ -148,6 +165,14 @@ def _sine(X, Y):
 
 def _smooth_large(X, Y):
     return 6.0 + 5.0 * np.sin(2 * np.pi * Y / 2048.0), -4.0 + 5.0 * np.cos(2 * np.pi * X / 2048.0)
+
+
+def _large_shift(X, Y):
+    """Displacements larger than a subset: 34-46 px in x, -24..-36 px in y,
+    gradients up to 0.018 (numpy or torch arrays)."""
+    xp = np if isinstance(X, np.ndarray) else __import__("torch")
+    return (40.0 + 6.0 * xp.sin(2 * np.pi * Y / 2048.0),
+            -30.0 + 6.0 * xp.cos(2 * np.pi * X / 2048.0))
 
 
 def plate_hole(cx=1024.0, cy=1024.0, rad=300.0):
@@ -187,6 +212,11 @@ WORKLOADS = {
     # 16 px grid, subset 32
     "plate2048": Workload("plate2048", 2048, 2048, 130_000, 2, 32, 16, 16, 2.0,
                           plate_hole(1024.0, 1024.0, 300.0), hole=(1024.0, 1024.0, 300.0)),
+    # displacements larger than the subset (up to 46 px): the multigrid
+    # search (funIntegerSearchMg) initialises the frame; subset 32, step 16;
+    # search 48 is the whole-field search radius that would cover the field
+    "largeshift4096": Workload("largeshift4096", 4096, 4096, 520_000, 6, 32, 16, 48, 2.0,
+                               _large_shift),
 }
 
 

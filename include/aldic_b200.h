@@ -125,6 +125,29 @@ ALDIC_API int aldic_int_search(aldic_ctx *ctx, const int gridx[2], const int gri
                      double *y, double *u, double *v, double *ccmax,
                      double *qfactors);
 
+/* Multigrid integer search -- funIntegerSearchMg.m:1, the search that
+ * IntegerSearch.m:117-120 runs when DICpara.InitFFTSearchMethod is neither 1
+ * nor 2 (large displacements): a whole-ROI normxcorr2 for one global shift,
+ * then regions halved level by level (x, y or both by their aspect ratio,
+ * while wider than winsize), each searched within +-5 px of its parent's
+ * shift, and gridfit 'springs' of the last level onto
+ * xList = gridx(1):step:gridx(2), yList likewise, with borders from the
+ * extreme regions' displacements (funIntegerSearchMg.m:210-244).
+ * The node grid is data dependent: *nx, *ny receive numel(xList),
+ * numel(yList); x, y, u, v, ccmax (cc.max) receive nx*ny values each
+ * (x fastest: the ny x nx arrays of the reference in row-major order) and
+ * qfactors (may be NULL) the two normalised q-factor grids, 2*nx*ny values.
+ * cap = capacity of each output in values; (W/step+1)*(H/step+1) always
+ * suffices; a smaller cap than nx*ny returns ALDIC_E_ARG with *nx, *ny set.
+ * info (may be NULL, else 10 values): {levels, last-level regions, regions
+ * whose correlation raised (NaN), level-1 u, level-1 v, level-1 peak, host
+ * ms of: tables + level 1, levels 2 .. last-1, last level, gridfit}.  The whole ROI must fit
+ * an 8192-point transform per side (ROI <= 4096 px). */
+ALDIC_API int aldic_int_search_mg(aldic_ctx *ctx, const int gridx[2], const int gridy[2],
+                                  int winsize, int step, int *nx, int *ny, int64_t cap, double *x,
+                                  double *y, double *u, double *v, double *ccmax, double *qfactors,
+                                  double *info);
+
 /* Local IC-GN -- funICGN.m:1 for every node (the loop of LocalICGN.m:64-81,
  * one launch): 6-DOF affine inverse-compositional Gauss-Newton with the
  * ZNSSD residual.  winsize_arr (n subsets, may be NULL) overrides winsize
@@ -164,7 +187,7 @@ ALDIC_API int aldic_subpb2(aldic_ctx *ctx, int M, int N, double step, double bet
  * process with audited or capped allocations).  All arrays are DEVICE
  * pointers (U 2n, F 4n, udual 4n, vdual 2n in; Uhat 2n out, n = M*N); the
  * solver's work vectors live in one fixed static device array of the library
- * (about 8.4 MB, held on every GPU that loads the library until exit), so at
+ * (about 12.7 MB, held on every GPU that loads the library until exit), so at
  * most 65536 nodes are accepted -- larger grids return ALDIC_E_ARG.  The
  * first call on a device looks up that array's device address (make it
  * before any stream capture).  The array is shared by every call: calls whose
@@ -358,15 +381,23 @@ ALDIC_API int aldic_cnn_to_init(aldic_ctx *ctx, const float *out, long long n, d
  *   ALDIC_INIT_EXTRAP  2 U(k-1) - U(k-2) from the last two frames, a
  *                      constant-rate predictor standing in for the POD-GPR
  *                      prediction of main_ALDIC.m:133-146;
- *   ALDIC_INIT_GIVEN   the 2n values set by aldic_set_init.
- * The node grid is the search grid of the same parameters in every mode.
- * The context keeps the final U of its last two frames on the device; it is
- * valid while the node grid does not change. */
+ *   ALDIC_INIT_GIVEN   the 2n values set by aldic_set_init;
+ *   ALDIC_INIT_SEARCH_MG  the multigrid search (aldic_int_search_mg,
+ *                      InitFFTSearchMethod other than 1 and 2) + Init: the
+ *                      search decides the node grid, which the frame
+ *                      reports in aldic_frame_stats.node_grid; the output
+ *                      arrays must then hold (W/step+1)*(H/step+1) nodes.
+ * The node grid is the whole-field search grid of the same parameters, or
+ * node_grid when its M is set (for the frames after a multigrid-search
+ * frame, pass the grid that frame reported).  The context keeps the final U
+ * of its last two frames on the device; it is valid while the node grid does
+ * not change. */
 #define ALDIC_INIT_SEARCH 0
 #define ALDIC_INIT_PREV 1
 #define ALDIC_INIT_ZERO 2
 #define ALDIC_INIT_EXTRAP 3
 #define ALDIC_INIT_GIVEN 4
+#define ALDIC_INIT_SEARCH_MG 5
 typedef struct {
   int winsize, step;
   int search[2];
@@ -381,6 +412,9 @@ typedef struct {
   int use_graph;            /* 1: capture/replay the device work as a CUDA graph */
   int init;                 /* ALDIC_INIT_* */
   int subpb2_fd;            /* 1: finite-difference Subproblem 2 (DICpara.Subpb2FDOrFEM = 1) */
+  double node_grid[4];      /* {x, y of the first node, M, N}: an explicit node grid
+                               (step apart) for the modes that do not search;
+                               M = 0: the whole-field search grid */
 } aldic_frame_params;
 
 typedef struct {
@@ -399,6 +433,8 @@ typedef struct {
    * (beta, Subpb2, nodal strain), 5 ADMM iterations, 6 whole frame */
   double t_stage_ms[8];
   int max_pcg_iters;        /* most PCG iterations taken by one node-grid solve */
+  double node_grid[4];      /* the node grid used: {x, y of the first node, M, N} */
+  double t_search_mg_ms;    /* host time of the multigrid search (ALDIC_INIT_SEARCH_MG) */
 } aldic_frame_stats;
 
 ALDIC_API int aldic_frame_dims(aldic_ctx *ctx, const aldic_frame_params *p, int *M, int *N);

@@ -528,6 +528,71 @@ int orc_int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H
 }
 
 /* ======================================================================
+ * Multigrid search primitives (func/funIntegerSearchMg.m): normxcorr2 of an
+ * arbitrary template rectangle of f against a region rectangle of g, at a
+ * rectangle of offsets; findpeak and compute_qFactor on a given map.
+ * ==================================================================== */
+int orc_ncc_map(const void *f_raw, const void *g_raw, int dtype, int W, int H, double mu_g,
+                const int trect[4], const int drect[4], int ox0, int ox1, int oy0, int oy1,
+                double *out) {
+  const int tw = trect[1] - trect[0] + 1, th = trect[3] - trect[2] + 1;
+  const int dw = drect[1] - drect[0] + 1, dh = drect[3] - drect[2] + 1;
+  if (tw < 1 || th < 1 || dw < 1 || dh < 1) return -1;
+  if (trect[0] < 1 || trect[1] > W || trect[2] < 1 || trect[3] > H) return -1;
+  if (drect[0] < 1 || drect[1] > W || drect[2] < 1 || drect[3] > H) return -1;
+  const int integer = dtype <= 1;
+  int64_t *T = (int64_t *)malloc(sizeof(int64_t) * tw * th);
+  int64_t *D = (int64_t *)malloc(sizeof(int64_t) * dw * dh);
+  double *Tf = (double *)malloc(sizeof(double) * tw * th);
+  double *Df = (double *)malloc(sizeof(double) * dw * dh);
+  int64_t st = 0, st2 = 0;
+  double stf = 0, st2f = 0;
+  for (int ty = 0; ty < th; ++ty)
+    for (int tx = 0; tx < tw; ++tx) {
+      const double v = px_value(f_raw, dtype, (int64_t)(trect[2] - 1 + ty) * W + (trect[0] - 1 + tx));
+      Tf[ty * tw + tx] = v;
+      T[ty * tw + tx] = (int64_t)v;
+      st += (int64_t)v;
+      st2 += (int64_t)v * (int64_t)v;
+      stf += v;
+      st2f += v * v;
+    }
+  for (int dy = 0; dy < dh; ++dy)
+    for (int dx = 0; dx < dw; ++dx) {
+      const double v = px_value(g_raw, dtype, (int64_t)(drect[2] - 1 + dy) * W + (drect[0] - 1 + dx));
+      Df[dy * dw + dx] = v;
+      D[dy * dw + dx] = (int64_t)v;
+    }
+  int flat;
+  if (integer) {
+    flat = ((int64_t)tw * th * st2 - st * st) == 0;
+  } else {
+    double m = stf / ((double)tw * th), q = 0;
+    for (int i = 0; i < tw * th; ++i) q += (Tf[i] - m) * (Tf[i] - m);
+    flat = !(q > 0);
+  }
+  if (!flat) {
+    ncc_ctx c;
+    memset(&c, 0, sizeof(c));
+    c.tw = tw; c.th = th; c.dw = dw; c.dh = dh; c.integer = integer;
+    c.T = T; c.D = D; c.Tf = Tf; c.Df = Df;
+    c.st = st; c.st2 = st2; c.stf = stf; c.st2f = st2f;
+    const int nr = ox1 - ox0 + 1, nc = oy1 - oy0 + 1;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nc; ++b)
+      for (int a = 0; a < nr; ++a) out[(int64_t)b * nr + a] = ncc_at(&c, ox0 + a, oy0 + b, mu_g);
+  }
+  free(T); free(D); free(Tf); free(Df);
+  return flat ? 1 : 0;
+}
+
+void orc_findpeak(const double *map, int nr, int nc, double out[3]) {
+  findpeak_restated(map, nr, nc, &out[0], &out[1], &out[2]);
+}
+
+void orc_qfactor(const double *cc, int n, double out[2]) { qfactor(cc, n, &out[0], &out[1]); }
+
+/* ======================================================================
  * a6: MeshSetUp.m:23-39.
  * ==================================================================== */
 void orc_mesh(int M, int N, const double *xlist, const double *ylist, double *coords,

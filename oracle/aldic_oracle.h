@@ -145,6 +145,21 @@ int orc_frame(const void *f_raw, const void *g_raw, int dtype, int W, int H,
               const orc_frame_params *p, orc_frame_result *r);
 void orc_frame_free(orc_frame_result *r);
 
+/* Multigrid search primitives (func/funIntegerSearchMg.m).  orc_ncc_map:
+ * normxcorr2(C, D) for C = f(trect[0]:trect[1], trect[2]:trect[3]) and
+ * D = g(drect[0]:drect[1], drect[2]:drect[3]) (1-based, inclusive, inside the
+ * W x H image), at the 0-based D offsets [ox0, ox1] x [oy0, oy1] of C's first
+ * pixel; out is column-major with rows = x offsets.  D is padded with mu_g
+ * (zero in normalised units).  Returns 1 for a constant template (normxcorr2
+ * raises), -1 for a bad rectangle, else 0.  orc_findpeak: findpeak.m on an
+ * nr x nc column-major map -> (row, col, max_f), 1-based.  orc_qfactor:
+ * compute_qFactor -> (PCE, 1/entropy). */
+int orc_ncc_map(const void *f_raw, const void *g_raw, int dtype, int W, int H, double mu_g,
+                const int trect[4], const int drect[4], int ox0, int ox1, int oy0, int oy1,
+                double *out);
+void orc_findpeak(const double *map, int nr, int nc, double out[3]);
+void orc_qfactor(const double *cc, int n, double out[2]);
+
 /* thread count used by OpenMP regions (0 = default) */
 void orc_set_threads(int n);
 int orc_get_threads(void);

@@ -140,3 +140,38 @@ def test_aldic_gateway_icgn_matches_oracle(gw_aldic, synth, oracle):
     Uo, Fo, ito, Ho = oracle.icgn_batch(fn, gn, dx, dy, coords, U0, 20, 1e-3)
     np.testing.assert_array_equal(it, ito)
     np.testing.assert_allclose(U, Uo, atol=1e-8)
+
+
+@pytest.mark.gpu
+def test_aldic_gateway_searchmg_and_computestrain(gw_aldic, synth, oracle, aldic):
+    """'searchmg' on the normalised images as MATLAB holds them equals the
+    library's funIntegerSearchMg on the raw images (normalisation is affine,
+    the correlation does not see it); 'computestrain' equals ComputeStrain."""
+    W, H = 192, 160
+    f = synth.speckle(W, H, 900, 33)
+    g = synth.warp(f, synth.uniform_affine(0.004, -0.003, 14.6, -9.2), 2.0, 33)
+    fn, _, _ = oracle.normalize(f)
+    gn, _, _ = oracle.normalize(g)
+    cap = (W // 8 + 1) * (H // 8 + 1)
+    args = ["searchmg", fn.T, gn.T, np.array([[1.0, W]]), np.array([[1.0, H]]),
+            np.array([[16.0]]), np.array([[8.0]])]
+    rc, outs = mex_call(gw_aldic, 5, args, [8 * cap] * 5)
+    assert rc == 0, gw_aldic.shim_last_error()
+    x, y, u, v, cc = aldic.funIntegerSearchMg(f, g, [1, W], [1, H], 16, 8, 8)
+    ny, nx = u.shape
+    for got, ref in zip(outs, (x, y, u, v, cc["max"])):
+        m = got[:nx * ny].reshape(nx, ny).T                 # MATLAB ny x nx column-major
+        np.testing.assert_allclose(m, ref, rtol=0, atol=1e-6)
+    # ComputeStrain, plane fitting, Green-Lagrangian
+    M, N = nx, ny
+    U = np.empty(2 * M * N)
+    U[0::2], U[1::2] = u.reshape(-1), v.reshape(-1)
+    args = ["computestrain", np.array([[float(M)]]), np.array([[float(N)]]), np.array([[8.0]]),
+            np.array([[2.0]]), np.array([[2.0]]), np.array([[2.0]]), U[:, None], np.zeros((0, 0))]
+    rc, outs = mex_call(gw_aldic, 2, args, [32 * M * N, 32 * M * N])
+    assert rc == 0, gw_aldic.shim_last_error()
+    r = aldic.ComputeStrain(U, None, {"M": M, "N": N},
+                            {"MethodToComputeStrain": 2, "StrainType": 2, "PlaneFitRad": 2,
+                             "winstepsize": 8})
+    np.testing.assert_array_equal(outs[0][:4 * M * N], r["FStrain"])
+    np.testing.assert_array_equal(outs[1][:4 * M * N], r["FStrainFinite"])
