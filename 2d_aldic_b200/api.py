@@ -955,6 +955,7 @@ class ALDICQuadtree:
         mesh0 = MeshSetUp(x, y, {"ImgSize": (W, H)})
         U0u = Init(u, v, None, x, y, 0)
         ny, nx = u.shape
+        t_search = time.perf_counter()
         ctx.set_ref(f, mask=mask)
         ctx.set_def(g)
         if self.mesh is not None:
@@ -972,6 +973,7 @@ class ALDICQuadtree:
         U1 = quadtree_fill(m, np.where(bad[:, None] != 0, 0.0, U1.reshape(n, 2)), bad, ctx).reshape(-1)
         F1 = quadtree_fill(m, np.where(bad[:, None] != 0, 0.0, F1.reshape(n, 4)), bad, ctx).reshape(-1)
         U_icgn = U1.copy()
+        t_icgn = time.perf_counter()
         # Section 5: beta sweep, Subpb2Quadtree, nodal strain
         mu = self.mu
         betas = np.array([1e-3, 1e-2, 1e-1]) * step * step * mu
@@ -989,6 +991,7 @@ class ALDICQuadtree:
         dd = np.repeat(4 * (d - 1), 4) + np.tile(np.arange(4), len(d))
         F2[dd] = F1[dd]                                   # main_ALDIC_Quadtree.m:205-207
         udual, vdual = F2 - F1, U2 - U1
+        t_s5 = time.perf_counter()
         # Section 6: ADMM
         upd, upd2 = [], []
         U1old = U1.copy()
@@ -1018,7 +1021,9 @@ class ALDICQuadtree:
         return {"coords": c, "elems": m.elementsFEM, "dirichlet": d, "U": U2, "F": F2,
                 "U_icgn": U_icgn, "iters_icgn": it, "bad_icgn": nbad, "beta": beta,
                 "update_y": upd, "update_y2": upd2, "wins": wins, "U0": U0,
-                "time_s": {"search_mesh": t_mesh - t0, "frame": t1 - t0}}
+                "time_s": {"search": t_search - t0, "mesh": t_mesh - t_search,
+                           "search_mesh": t_mesh - t0, "icgn": t_icgn - t_mesh,
+                           "section5": t_s5 - t_icgn, "admm": t1 - t_s5, "frame": t1 - t0}}
 
 
 # ------------------------------------------------------------------ learned init

@@ -340,40 +340,72 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
     const double *Mo = Mv[it & 1];
     double *Mn = Mv[(it + 1) & 1];
     double *part = A.part + ((it + 1) & 1) * pstride;
-    // ---- n = A m; directions and iterates; next partials and m
+    // ---- n = A m; directions and iterates; next partials and m.  Fields
+    // go in pairs, every load of a pair before any store, so the two fields'
+    // memory round trips overlap.
 #pragma unroll 1
-    for (int f = 0; f < NR; ++f) {
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-      if (!S.done[f]) {
-        const double bt = A.beta[f], al = S.alpha[f], be = S.beta[f];
+    for (int f0 = 0; f0 < NR; f0 += 2) {
+      constexpr int G2 = NR >= 2 ? 2 : 1;
+      double a0[G2], a1[G2], a2[G2], al[G2], be[G2], bt[G2];
+      bool live[G2];
+#pragma unroll
+      for (int q = 0; q < G2; ++q) {
+        a0[q] = a1[q] = a2[q] = 0.0;
+        const int f = f0 + q;
+        live[q] = f < NR && !S.done[f];
+        bt[q] = f < NR ? A.beta[f] : 0.0;
+        al[q] = f < NR ? S.alpha[f] : 0.0;
+        be[q] = f < NR ? S.beta[f] : 0.0;
+      }
+      if (live[0] || (G2 > 1 && live[G2 - 1])) {
         for (long long k = tid0; k < n; k += stride) {
           const int i = (int)(k % M), j = (int)(k / M);
-          const long long o = f * n + k;
-          const double nv = op_apply<OP>(A, bt, i, j, k, f, Mo + f * n);
-          const double zv = nv + be * Zd[o];
-          const double qv = Mo[o] + be * Qd[o];
-          const double sv = Wv[o] + be * Sd[o];
-          const double pv = Uv[o] + be * Pd[o];
-          Zd[o] = zv;
-          Qd[o] = qv;
-          Sd[o] = sv;
-          Pd[o] = pv;
-          X[o] += al * pv;
-          const double rv = R[o] - al * sv;
-          const double uv = Uv[o] - al * qv;
-          const double wv = Wv[o] - al * zv;
-          R[o] = rv;
-          Uv[o] = uv;
-          Wv[o] = wv;
-          Mn[o] = wv * Di[o];
-          a0 += rv * uv;
-          a1 += wv * uv;
-          a2 += rv * rv;
+          double nv[G2], zo[G2], qo[G2], so[G2], po[G2], mo[G2], wo[G2], uo[G2], ro[G2], xo[G2],
+              di[G2];
+#pragma unroll
+          for (int q = 0; q < G2; ++q) {
+            if (!live[q]) continue;
+            const int f = f0 + q;
+            const long long o = f * n + k;
+            nv[q] = op_apply<OP>(A, bt[q], i, j, k, f, Mo + f * n);
+            zo[q] = Zd[o]; qo[q] = Qd[o]; so[q] = Sd[o]; po[q] = Pd[o];
+            mo[q] = Mo[o]; wo[q] = Wv[o]; uo[q] = Uv[o]; ro[q] = R[o]; xo[q] = X[o]; di[q] = Di[o];
+          }
+#pragma unroll
+          for (int q = 0; q < G2; ++q) {
+            if (!live[q]) continue;
+            const long long o = (f0 + q) * n + k;
+            const double zv = nv[q] + be[q] * zo[q];
+            const double qv = mo[q] + be[q] * qo[q];
+            const double sv = wo[q] + be[q] * so[q];
+            const double pv = uo[q] + be[q] * po[q];
+            Zd[o] = zv;
+            Qd[o] = qv;
+            Sd[o] = sv;
+            Pd[o] = pv;
+            X[o] = xo[q] + al[q] * pv;
+            const double rv = ro[q] - al[q] * sv;
+            const double uv = uo[q] - al[q] * qv;
+            const double wv = wo[q] - al[q] * zv;
+            R[o] = rv;
+            Uv[o] = uv;
+            Wv[o] = wv;
+            Mn[o] = wv * di[q];
+            a0[q] += rv * uv;
+            a1[q] += wv * uv;
+            a2[q] += rv * rv;
+          }
         }
       }
-      warp_stage(S, f, a0);
-      warp_stage(S, NR + f, a1);
-      warp_stage(S, 2 * NR + f, a2);
+#pragma unroll
+      for (int q = 0; q < G2; ++q) {
+        const int f = f0 + q;
+        if (f < NR) {
+          warp_stage(S, f, a0[q]);
+          warp_stage(S, NR + f, a1[q]);
+          warp_stage(S, 2 * NR + f, a2[q]);
+        }
+      }
     }
     block_partials(S, 3 * NR, part, A.blocks);
     if (!grid_sync(A.gs, A.blocks)) return;

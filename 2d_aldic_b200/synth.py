@@ -159,12 +159,18 @@ def _affine_small(X, Y):
     return 0.5 + 0.01 * X, -0.3 + 0.005 * Y
 
 
+def _xp(X):
+    return np if isinstance(X, np.ndarray) else __import__("torch")
+
+
 def _sine(X, Y):
-    return 2.0 * np.sin(2 * np.pi * Y / 256.0), 1.5 * np.cos(2 * np.pi * X / 256.0)
+    xp = _xp(X)
+    return 2.0 * xp.sin(2 * np.pi * Y / 256.0), 1.5 * xp.cos(2 * np.pi * X / 256.0)
 
 
 def _smooth_large(X, Y):
-    return 6.0 + 5.0 * np.sin(2 * np.pi * Y / 2048.0), -4.0 + 5.0 * np.cos(2 * np.pi * X / 2048.0)
+    xp = _xp(X)
+    return 6.0 + 5.0 * xp.sin(2 * np.pi * Y / 2048.0), -4.0 + 5.0 * xp.cos(2 * np.pi * X / 2048.0)
 
 
 def _large_shift(X, Y):

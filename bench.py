@@ -316,7 +316,8 @@ def quadtree_main(args, rank, world, local):
                                    f"{wl.step} px grid, element-sized subsets",
                        "nodes": len(c), "elements": int(len(r["elems"])),
                        "subset_sizes": {int(k): int(v) for k, v in zip(sizes, counts)},
-                       "admm_steps": len(r["update_y"]), "beta": r["beta"]},
+                       "admm_steps": len(r["update_y"]), "beta": r["beta"],
+                       "host_time_ms": {k: round(v * 1e3, 2) for k, v in r["time_s"].items()}},
             "clocks": clk,
         }), flush=True)
 
