@@ -6,8 +6,8 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
-#include <map>
-#include <tuple>
+#include <cstring>
+#include <unordered_map>
 #include <vector>
 
 #include "qt.cuh"
@@ -15,8 +15,12 @@
 void aldic_qt_mesh::release() {
   aldic::DevBuf *b[] = {&d_coords, &d_elems, &d_row, &d_col, &d_dpos, &d_iptr, &d_inc, &d_ipos,
                         &d_kind, &d_val, &d_diag, &d_ke, &d_be, &d_es, &d_arow, &d_acol,
-                        &d_aval, &d_adiag, &d_icorner};
-  for (auto *x : b) x->release();
+                        &d_aval, &d_adiag};
+  for (auto *x : b) {  // views into the slab
+    x->p = nullptr;
+    x->cap = 0;
+  }
+  slab.release();
   device = -1;
 }
 
@@ -45,13 +49,73 @@ bool box(const HMesh &m, const std::array<int, 4> &e, int W, int H, int b[4]) {
   return b[0] >= 1 && b[1] <= W && b[2] >= 1 && b[3] <= H;
 }
 
-// funMarkEdge.m: box straddles the mask edge and its smaller side > min_size
-int mark_edge(const HMesh &m, const double *mask, int W, int H, double min_size,
-              std::vector<int> &out) {
-  out.clear();
-  for (size_t e = 0; e < m.el.size(); ++e) {
-    int b[4];
-    if (!box(m, m.el[e], W, H, b)) return E_ARG;
+// Mask box queries.  A mask of zeros and ones (the usual ImgRefMask) is
+// answered exactly from a summed-area table of pixel counts: a box straddles
+// the edge iff 0 < count < area, and its sum is the count.  Other masks scan
+// the box.
+struct MaskTable {
+  std::vector<int32_t> sat;  // (W+1) x (H+1) counts of ones
+  int W = 0, H = 0;
+  uint64_t hash = 0;         // of the mask it was built from
+  bool binary = false;
+};
+
+struct MaskQ {
+  const double *mask;
+  int W, H;
+  bool binary;
+  std::vector<int32_t> &sat;
+  static MaskTable &table() {
+    // kept across calls: a quadtree frame regenerates its mesh on every
+    // search frame of a sequence, with the same mask
+    static thread_local MaskTable t;
+    return t;
+  }
+  MaskQ(const double *m, int w, int h) : mask(m), W(w), H(h), binary(true), sat(table().sat) {
+    MaskTable &t = table();
+    const long long n = (long long)W * H;
+    uint64_t hs = 1469598103934665603ull;  // FNV-1a over the 64-bit words
+    for (long long k = 0; k < n; ++k) {
+      uint64_t bits;
+      std::memcpy(&bits, m + k, 8);
+      hs = (hs ^ bits) * 1099511628211ull;
+    }
+    if (t.W == W && t.H == H && t.hash == hs && !t.sat.empty()) {
+      binary = t.binary;
+      return;
+    }
+    for (long long k = 0; k < n && binary; ++k) binary = m[k] == 0.0 || m[k] == 1.0;
+    t.W = W;
+    t.H = H;
+    t.hash = hs;
+    t.binary = binary;
+    if (!binary) {
+      t.sat.clear();
+      t.W = 0;
+      return;
+    }
+    const size_t W1 = (size_t)W + 1;
+    if (sat.size() < W1 * (H + 1)) sat.resize(W1 * (H + 1));
+    for (size_t x = 0; x < W1; ++x) sat[x] = 0;
+    for (int y = 1; y <= H; ++y) {
+      int32_t row = 0;
+      sat[(size_t)y * W1] = 0;
+      for (int x = 1; x <= W; ++x) {
+        row += m[(long long)(y - 1) * W + (x - 1)] != 0.0;
+        sat[(size_t)y * W1 + x] = sat[(size_t)(y - 1) * W1 + x] + row;
+      }
+    }
+  }
+  int64_t count(const int b[4]) const {  // ones in [b0, b1] x [b2, b3], 1-based inclusive
+    const size_t W1 = W + 1;
+    return sat[(size_t)b[3] * W1 + b[1]] - sat[(size_t)(b[2] - 1) * W1 + b[1]] -
+           sat[(size_t)b[3] * W1 + (b[0] - 1)] + sat[(size_t)(b[2] - 1) * W1 + (b[0] - 1)];
+  }
+  bool straddles(const int b[4]) const {
+    if (binary) {
+      const int64_t c = count(b), area = (int64_t)(b[1] - b[0] + 1) * (b[3] - b[2] + 1);
+      return c > 0 && c < area;
+    }
     double lo = 1e300, hi = -1e300;
     for (int y = b[2]; y <= b[3]; ++y)
       for (int x = b[0]; x <= b[1]; ++x) {
@@ -59,8 +123,25 @@ int mark_edge(const HMesh &m, const double *mask, int W, int H, double min_size,
         lo = std::min(lo, v);
         hi = std::max(hi, v);
       }
+    return hi - lo > 0;
+  }
+  double sum(const int b[4]) const {
+    if (binary) return (double)count(b);
+    double s = 0;
+    for (int y = b[2]; y <= b[3]; ++y)
+      for (int x = b[0]; x <= b[1]; ++x) s += mask[(long long)(y - 1) * W + (x - 1)];
+    return s;
+  }
+};
+
+// funMarkEdge.m: box straddles the mask edge and its smaller side > min_size
+int mark_edge(const HMesh &m, const MaskQ &mq, double min_size, std::vector<int> &out) {
+  out.clear();
+  for (size_t e = 0; e < m.el.size(); ++e) {
+    int b[4];
+    if (!box(m, m.el[e], mq.W, mq.H, b)) return E_ARG;
     const double size = std::min(std::abs(b[1] - b[0]), std::abs(b[3] - b[2]));
-    if (hi - lo > 0 && size > min_size) out.push_back((int)e);
+    if (size > min_size && mq.straddles(b)) out.push_back((int)e);
   }
   return OK;
 }
@@ -75,25 +156,25 @@ struct Geo {
 
 void geometric(const HMesh &m, Geo &g) {
   const size_t ni = m.irr.size(), ne = m.el.size(), n3 = 3 * ni;
-  std::vector<std::array<long long, 3>> ed;
+  // (sorted node pair as one 64-bit key, occurrence index), sorted
+  std::vector<std::pair<uint64_t, int>> ed;
   ed.reserve(n3 + 4 * ne);
+  auto k2 = [](int a, int b) {
+    return ((uint64_t)(uint32_t)std::min(a, b) << 32) | (uint64_t)(uint32_t)std::max(a, b);
+  };
   for (int c = 0; c < 3; ++c)
-    for (size_t r = 0; r < ni; ++r) {
-      const int a = m.irr[r][c], b = m.irr[r][(c + 1) % 3];
-      ed.push_back({std::min(a, b), std::max(a, b), (long long)(c * ni + r)});
-    }
+    for (size_t r = 0; r < ni; ++r)
+      ed.push_back({k2(m.irr[r][c], m.irr[r][(c + 1) % 3]), (int)(c * ni + r)});
   for (int c = 0; c < 4; ++c)
-    for (size_t r = 0; r < ne; ++r) {
-      const int a = m.el[r][c], b = m.el[r][(c + 1) % 4];
-      ed.push_back({std::min(a, b), std::max(a, b), (long long)(n3 + c * ne + r)});
-    }
+    for (size_t r = 0; r < ne; ++r)
+      ed.push_back({k2(m.el[r][c], m.el[r][(c + 1) % 4]), (int)(n3 + c * ne + r)});
   std::sort(ed.begin(), ed.end());
   std::vector<int> ie(ed.size());
   g.e2n.clear();
   for (size_t k = 0; k < ed.size(); ++k) {
-    if (k == 0 || ed[k][0] != ed[k - 1][0] || ed[k][1] != ed[k - 1][1])
-      g.e2n.push_back({(int)ed[k][0], (int)ed[k][1]});
-    ie[ed[k][2]] = (int)g.e2n.size() - 1;
+    if (k == 0 || ed[k].first != ed[k - 1].first)
+      g.e2n.push_back({(int)(ed[k].first >> 32), (int)(ed[k].first & 0xffffffffu)});
+    ie[ed[k].second] = (int)g.e2n.size() - 1;
   }
   g.irr2e.assign(ni, {0, 0, 0});
   g.el2e.assign(ne, {0, 0, 0, 0});
@@ -230,10 +311,11 @@ int qt_generate(int n0, const double *coords, int ne0, const int32_t *elems, con
     xmin = std::min(xmin, m.x[k]); xmax = std::max(xmax, m.x[k]);
     ymin = std::min(ymin, m.y[k]); ymax = std::max(ymax, m.y[k]);
   }
+  const MaskQ mq(mask, W, H);
   std::vector<int> mk;
   for (int pass = 0;; ++pass) {
     ALDIC_CHECK(pass < 64, E_ARG, "qt_mesh_generate: refinement does not terminate");
-    if (mark_edge(m, mask, W, H, 2.0 * min_size, mk) != OK) {
+    if (mark_edge(m, mq, 2.0 * min_size, mk) != OK) {
       set_error("qt_mesh_generate: element corners must be whole pixels inside the mask "
                 "(uniform step a power-of-two multiple of the minimum element size)");
       return E_ARG;
@@ -251,23 +333,32 @@ int qt_generate(int n0, const double *coords, int ne0, const int32_t *elems, con
   }
   static const int pairs[8][3] = {{0, 1, 7}, {1, 2, 4}, {2, 3, 5}, {3, 0, 6},
                                   {1, 0, 7}, {2, 1, 4}, {3, 2, 5}, {0, 3, 6}};
-  std::map<std::tuple<int, int, int>, int> first;
+  // (corner a, corner b, pair) -> first element: only the pairs that are
+  // parent edges of hanging nodes are looked up, so only those are recorded
+  auto key = [](int a, int b, int pi) -> unsigned long long {
+    return ((unsigned long long)(unsigned)a << 35) ^ ((unsigned long long)(unsigned)b << 3) ^
+           (unsigned long long)pi;
+  };
+  std::unordered_map<unsigned long long, int> first;
+  first.reserve(8 * m.irr.size() + 16);
+  for (const auto &r : m.irr)
+    for (int pi = 0; pi < 8; ++pi) first.emplace(key(r[0], r[1], pi), -1);
   for (int pi = 0; pi < 8; ++pi)
-    for (size_t e = ne; e-- > 0;)
-      first[std::make_tuple(m.el[e][pairs[pi][0]], m.el[e][pairs[pi][1]], pi)] = (int)e;
+    for (size_t e = 0; e < ne; ++e) {
+      auto it = first.find(key(m.el[e][pairs[pi][0]], m.el[e][pairs[pi][1]], pi));
+      if (it != first.end() && it->second < 0) it->second = (int)e;
+    }
   for (const auto &r : m.irr)
     for (int pi = 0; pi < 8; ++pi) {
-      auto it = first.find(std::make_tuple(r[0], r[1], pi));
-      if (it != first.end()) E[it->second][pairs[pi][2]] = r[2];
+      const int e = first[key(r[0], r[1], pi)];
+      if (e >= 0) E[e][pairs[pi][2]] = r[2];
     }
   // funMarkInside.m: drop elements less than half inside the mask
   std::vector<std::array<int, 8>> K;
   for (size_t e = 0; e < ne; ++e) {
     int b[4];
     if (!box(m, m.el[e], W, H, b)) return E_ARG;
-    double s = 0;
-    for (int y = b[2]; y <= b[3]; ++y)
-      for (int x = b[0]; x <= b[1]; ++x) s += mask[(long long)(y - 1) * W + (x - 1)];
+    const double s = mq.sum(b);
     if (!(s < 0.5 * (b[1] - b[0]) * (b[3] - b[2]))) K.push_back(E[e]);
   }
   // Dirichlet nodes (GenerateQuadtreeMesh.m:75-110): refined elements and
@@ -585,13 +676,6 @@ __global__ void k_qt_fill_store(int n, int nf, const double *__restrict__ x,
 
 inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
 
-template <typename T>
-int put(DevBuf &b, const std::vector<T> &v) {
-  int rc = b.ensure(sizeof(T) * (v.empty() ? 1 : v.size()));
-  if (rc) return rc;
-  if (!v.empty()) ALDIC_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
-  return OK;
-}
 
 }  // namespace
 
@@ -617,69 +701,82 @@ int qt_upload(aldic_qt_mesh &m, cudaStream_t st) {
     ALDIC_CHECK(d >= 1 && d <= n, E_ARG, "quadtree mesh: Dirichlet node out of range");
     if (kind[d - 1] == 0) kind[d - 1] = 1;
   }
-  // FE pattern: node pairs sharing an element
-  std::vector<std::vector<int>> cols(n);
-  for (int e = 0; e < ne; ++e)
-    for (int a = 0; a < 8; ++a) {
-      const int na = E[8 * e + a];
-      if (na < 0) continue;
-      for (int b = 0; b < 8; ++b)
-        if (E[8 * e + b] >= 0) cols[na].push_back(E[8 * e + b]);
-    }
-  std::vector<int> row(n + 1, 0), col, dpos(n, 0);
-  for (int a = 0; a < n; ++a) {
-    auto &c = cols[a];
-    std::sort(c.begin(), c.end());
-    c.erase(std::unique(c.begin(), c.end()), c.end());
-    row[a + 1] = row[a] + (int)c.size();
-    for (size_t k = 0; k < c.size(); ++k)
-      if (c[k] == a) dpos[a] = row[a] + (int)k;
-    col.insert(col.end(), c.begin(), c.end());
+  // incidence node -> (element * 8 + slot) in element order (counting sort)
+  std::vector<int> iptr(n + 1, 0), inc;
+  for (int k = 0; k < 8 * ne; ++k)
+    if (E[k] >= 0) iptr[E[k] + 1]++;
+  for (int a = 0; a < n; ++a) iptr[a + 1] += iptr[a];
+  inc.resize(iptr[n]);
+  {
+    std::vector<int> fill(iptr.begin(), iptr.end() - 1);
+    for (int k = 0; k < 8 * ne; ++k)
+      if (E[k] >= 0) inc[fill[E[k]]++] = k;
   }
-  // incidence (element order) and its scatter map into the rows
-  std::vector<std::vector<int>> incl(n);
-  for (int e = 0; e < ne; ++e)
-    for (int s = 0; s < 8; ++s)
-      if (E[8 * e + s] >= 0) incl[E[8 * e + s]].push_back(8 * e + s);
-  std::vector<int> iptr(n + 1, 0), inc, ipos;
+  // FE pattern: node pairs sharing an element, each row sorted
+  std::vector<int> row(n + 1, 0), col, dpos(n, 0), buf;
+  col.reserve((size_t)iptr[n] * 4);
   for (int a = 0; a < n; ++a) {
-    iptr[a + 1] = iptr[a] + (int)incl[a].size();
-    for (int ent : incl[a]) {
-      inc.push_back(ent);
-      const int e = ent >> 3;
+    buf.clear();
+    for (int t = iptr[a]; t < iptr[a + 1]; ++t) {
+      const int e = inc[t] >> 3;
+      for (int b = 0; b < 8; ++b)
+        if (E[8 * e + b] >= 0) buf.push_back(E[8 * e + b]);
+    }
+    std::sort(buf.begin(), buf.end());
+    buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+    row[a + 1] = row[a] + (int)buf.size();
+    for (size_t k = 0; k < buf.size(); ++k)
+      if (buf[k] == a) dpos[a] = row[a] + (int)k;
+    col.insert(col.end(), buf.begin(), buf.end());
+  }
+  // scatter map of each incidence into its row
+  std::vector<int> ipos((size_t)8 * inc.size());
+  for (int a = 0; a < n; ++a)
+    for (int t = iptr[a]; t < iptr[a + 1]; ++t) {
+      const int e = inc[t] >> 3;
       for (int sb = 0; sb < 8; ++sb) {
         const int nb = E[8 * e + sb];
-        if (nb < 0) {
-          ipos.push_back(-1);
-        } else {
-          const auto it = std::lower_bound(col.begin() + row[a], col.begin() + row[a + 1], nb);
-          ipos.push_back((int)(it - col.begin()));
-        }
+        ipos[(size_t)8 * t + sb] =
+            nb < 0 ? -1
+                   : (int)(std::lower_bound(col.begin() + row[a], col.begin() + row[a + 1], nb) -
+                           col.begin());
       }
     }
-  }
-  // refill graph: element boundary rings 1-8-2-5-3-6-4-7
+  // refill graph: element boundary rings 1-8-2-5-3-6-4-7 (edge list, then
+  // grouped per node by a counting sort)
   static const int ring[8] = {0, 7, 1, 4, 2, 5, 3, 6};
-  std::vector<std::vector<int>> adj(n);
+  std::vector<int> ea, eb;
+  ea.reserve((size_t)16 * ne);
+  eb.reserve((size_t)16 * ne);
   for (int e = 0; e < ne; ++e) {
     int r[8], k = 0;
     for (int q = 0; q < 8; ++q)
       if (E[8 * e + ring[q]] >= 0) r[k++] = E[8 * e + ring[q]];
     for (int q = 0; q < k; ++q) {
       const int a = r[q], b = r[(q + 1) % k];
-      adj[a].push_back(b);
-      adj[b].push_back(a);
+      ea.push_back(a); eb.push_back(b);
+      ea.push_back(b); eb.push_back(a);
     }
+  }
+  std::vector<int> aptr(n + 1, 0), anb(ea.size());
+  for (int a : ea) aptr[a + 1]++;
+  for (int a = 0; a < n; ++a) aptr[a + 1] += aptr[a];
+  {
+    std::vector<int> fill(aptr.begin(), aptr.end() - 1);
+    for (size_t k = 0; k < ea.size(); ++k) anb[fill[ea[k]]++] = eb[k];
   }
   std::vector<int> arow(n + 1, 0), acol;
   std::vector<double> aval, adiag(n);
+  acol.reserve(anb.size() + n);
+  aval.reserve(anb.size() + n);
   for (int a = 0; a < n; ++a) {
-    auto &c = adj[a];
-    std::sort(c.begin(), c.end());
-    c.erase(std::unique(c.begin(), c.end()), c.end());
-    const double deg = (double)c.size();
+    auto b0 = anb.begin() + aptr[a], b1 = anb.begin() + aptr[a + 1];
+    std::sort(b0, b1);
+    b1 = std::unique(b0, b1);
+    const double deg = (double)(b1 - b0);
     bool diag_done = false;
-    for (int v : c) {
+    for (auto it = b0; it != b1; ++it) {
+      const int v = *it;
       if (!diag_done && v > a) {
         acol.push_back(a);
         aval.push_back(deg + kQtFillTether);
@@ -695,18 +792,50 @@ int qt_upload(aldic_qt_mesh &m, cudaStream_t st) {
     adiag[a] = deg + kQtFillTether;
     arow[a + 1] = (int)acol.size();
   }
-  std::vector<int> icorner(n, 0);
+  // one device slab: the arrays above, then the work arrays
+  struct Part {
+    DevBuf *b;
+    const void *src;
+    size_t bytes;
+  };
+  const Part parts[] = {
+      {&m.d_coords, m.coords.data(), sizeof(double) * m.coords.size()},
+      {&m.d_elems, E.data(), sizeof(int) * E.size()},
+      {&m.d_row, row.data(), sizeof(int) * row.size()},
+      {&m.d_col, col.data(), sizeof(int) * col.size()},
+      {&m.d_dpos, dpos.data(), sizeof(int) * dpos.size()},
+      {&m.d_iptr, iptr.data(), sizeof(int) * iptr.size()},
+      {&m.d_inc, inc.data(), sizeof(int) * inc.size()},
+      {&m.d_ipos, ipos.data(), sizeof(int) * ipos.size()},
+      {&m.d_kind, kind.data(), kind.size()},
+      {&m.d_arow, arow.data(), sizeof(int) * arow.size()},
+      {&m.d_acol, acol.data(), sizeof(int) * acol.size()},
+      {&m.d_aval, aval.data(), sizeof(double) * aval.size()},
+      {&m.d_adiag, adiag.data(), sizeof(double) * adiag.size()},
+      {&m.d_val, nullptr, sizeof(double) * (col.size() + 1)},
+      {&m.d_diag, nullptr, sizeof(double) * n},
+      {&m.d_ke, nullptr, sizeof(double) * 64 * ne},
+      {&m.d_be, nullptr, sizeof(double) * 16 * ne},
+      {&m.d_es, nullptr, sizeof(double) * 16 * ne},
+  };
+  size_t off = 0, upload = 0;
+  for (const Part &q : parts) {
+    off = (off + 255) & ~(size_t)255;
+    if (q.src) upload = off + q.bytes;
+    off += q.bytes > 0 ? q.bytes : 1;
+  }
   int rc;
-  if ((rc = put(m.d_coords, m.coords)) || (rc = put(m.d_elems, E)) || (rc = put(m.d_row, row)) ||
-      (rc = put(m.d_col, col)) || (rc = put(m.d_dpos, dpos)) || (rc = put(m.d_iptr, iptr)) ||
-      (rc = put(m.d_inc, inc)) || (rc = put(m.d_ipos, ipos)) || (rc = put(m.d_kind, kind)) ||
-      (rc = put(m.d_arow, arow)) || (rc = put(m.d_acol, acol)) || (rc = put(m.d_aval, aval)) ||
-      (rc = put(m.d_adiag, adiag)))
-    return rc;
-  if ((rc = m.d_val.ensure(sizeof(double) * (col.size() + 1))) ||
-      (rc = m.d_diag.ensure(sizeof(double) * n)) || (rc = m.d_ke.ensure(sizeof(double) * 64 * ne)) ||
-      (rc = m.d_be.ensure(sizeof(double) * 16 * ne)) || (rc = m.d_es.ensure(sizeof(double) * 16 * ne)))
-    return rc;
+  if ((rc = m.slab.ensure(off))) return rc;
+  std::vector<unsigned char> host(upload, 0);
+  off = 0;
+  for (const Part &q : parts) {
+    off = (off + 255) & ~(size_t)255;
+    q.b->p = m.slab.as<unsigned char>() + off;
+    q.b->cap = 0;  // a view: never grown or freed on its own
+    if (q.src && q.bytes) std::memcpy(host.data() + off, q.src, q.bytes);
+    off += q.bytes > 0 ? q.bytes : 1;
+  }
+  ALDIC_CUDA(cudaMemcpy(m.slab.p, host.data(), upload, cudaMemcpyHostToDevice));
   m.nnz = (long long)col.size();
   m.ninc = (long long)inc.size();
   m.nadj = (long long)acol.size();

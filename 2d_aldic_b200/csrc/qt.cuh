@@ -29,7 +29,7 @@ struct aldic_qt_mesh {
   aldic::DevBuf d_kind;          // 0 free, 1 Dirichlet, 2 in no element
   aldic::DevBuf d_val, d_diag, d_ke, d_be, d_es;
   aldic::DevBuf d_arow, d_acol, d_aval, d_adiag;  // refill graph Laplacian
-  aldic::DevBuf d_icorner;       // per node: corner incidences
+  aldic::DevBuf slab;            // one allocation; the arrays above are views into it
   void release();
 };
 
