@@ -102,7 +102,8 @@ struct aldic_ctx {
   // sequence state: final U of the last two frames and the given U0
   // (3 x 2n doubles: [U(k-1) | U(k-2) | given])
   DevBuf hist;
-  MgWork mg;  // multigrid search work
+  MgWork mg;      // multigrid search work
+  SearchWork sw;  // tiled 8-bit search work
   long long hist_n = 0;
   int hist_count = 0;
   bool have_given = false;
@@ -382,6 +383,7 @@ int aldic_ctx_destroy(aldic_ctx *c) {
                     &c->hist};
   for (DevBuf *b : bufs) b->release();
   c->mg.release();
+  c->sw.release();
   c->arena.release();
   if (c->own_stream) cudaStreamDestroy(c->stream);
   cudaSetDevice(prev);
@@ -618,7 +620,7 @@ int aldic_int_search(aldic_ctx *c, const int gridx[2], const int gridy[2], int w
   }
   rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H, c->stats.as<double>() + 2, gridx,
                   gridy, winsize, step, search, ax.dev, ay.dev, au.dev, av.dev, ac.dev, pce, ppe,
-                  c->stream);
+                  c->stream, &c->sw);
   if (rc) return rc;
   arg_back(c, ax); arg_back(c, ay); arg_back(c, au); arg_back(c, av); arg_back(c, ac);
   if (qfactors) {
@@ -1355,7 +1357,7 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     // Section 3: integer search, MeshSetUp, Init (inpaint_nans of u, v)
     if ((rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, c->W, c->H, c->stats.as<double>() + 2,
                          gx, gy, p->winsize, p->step, p->search, B.sx, B.sy, B.su, B.sv, B.scc,
-                         nullptr, nullptr, st)))
+                         nullptr, nullptr, st, &c->sw)))
       return rc;
     k_mesh_init<<<nb, 256, 0, st>>>(M, N, B.sx, B.sy, B.su, B.sv, B.coords, B.x0, B.y0, B.U0);
     if ((rc = inpaint_load(c->gw, M, N, 2, B.U0, 2, nullptr, st, 0))) return rc;
@@ -1574,6 +1576,8 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   ALDIC_CHECK(qp.init != ALDIC_INIT_GIVEN || c->have_given, E_STATE,
               "frame: ALDIC_INIT_GIVEN needs aldic_set_init on this node grid");
   if ((rc = ensure_grid_work(c, n))) return rc;
+  // search work before any capture (a graph records its addresses)
+  if (qp.init == ALDIC_INIT_SEARCH && (rc = search_work_ensure(c->sw, c->W, c->H, n))) return rc;
   // frame slab
   const long long ny_nx = n;
   const size_t need = 256 * 40 + sizeof(double) * (5 * ny_nx + 2 * n + 2 * n + 2 * n + 2 * n + 4 * n +
@@ -1600,11 +1604,11 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   // the buffers the graph addresses
   char key[512];
   snprintf(key, sizeof key,
-           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p",
+           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p %p",
            c->W, c->H, c->dtype, p->winsize, p->step, p->search[0], p->search[1], gx[0], gx[1],
            gy[0], gy[1], node0[0], node0[1], M, N, p->tol, p->mu, p->beta, p->n_admm, p->precision,
            p->smooth, qp.init * 2 + (p->subpb2_fd != 0),
-           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p);
+           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p, c->sw.buf.p);
   if (realloc) c->drop_graphs();  // recorded against buffers that are gone
   const bool want_graph = p->use_graph && !c->graph_failed;
   aldic_ctx::FrameGraph *fg = nullptr;

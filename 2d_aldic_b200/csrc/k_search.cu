@@ -12,6 +12,8 @@
 // integers with a fixed FP64 formula (explicit rounding, no contraction)
 // shared with the CPU restatement, which makes argmax and the 1e-3-rounded
 // sub-pixel peak bit-identical to it.
+#include <algorithm>
+
 #include "aldic_internal.cuh"
 #include "kernels.cuh"
 #include "ncc.cuh"
@@ -342,13 +344,12 @@ struct U8Layout {
   }
 };
 
-__global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f,
-                                                   const uint8_t *__restrict__ g, SearchGeom G,
-                                                   double *__restrict__ ox,
-                                                   double *__restrict__ oy,
-                                                   double *__restrict__ ou,
-                                                   double *__restrict__ ov,
-                                                   double *__restrict__ occ) {
+__device__ __forceinline__ void search_point_u8(const uint8_t *__restrict__ f,
+                                                const uint8_t *__restrict__ g,
+                                                const SearchGeom &G, const int pt,
+                                                double *__restrict__ ox, double *__restrict__ oy,
+                                                double *__restrict__ ou, double *__restrict__ ov,
+                                                double *__restrict__ occ) {
   extern __shared__ __align__(16) unsigned char smem[];
   const U8Layout L(G);
   uint8_t *Tb = smem + L.tb;                 // template bytes, tw x tw
@@ -365,7 +366,6 @@ __global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f
   __shared__ long long s_st, s_st2;
   __shared__ int colsum_s[72], rowsum_s[72];
   const double mu = *G.mu;
-  const int pt = blockIdx.x;
   const int ix = pt % G.nx, iy = pt / G.nx;
   const int ii = G.gx1 + ix * G.step, jj = G.gy1 + iy * G.step;  // 1-based
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -533,6 +533,713 @@ __global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f
   peak_epilogue(map, G, ii, jj, out_idx, redv, redi, ox, oy, ou, ov, occ);
 }
 
+__global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f,
+                                                   const uint8_t *__restrict__ g, SearchGeom G,
+                                                   double *__restrict__ ox,
+                                                   double *__restrict__ oy,
+                                                   double *__restrict__ ou,
+                                                   double *__restrict__ ov,
+                                                   double *__restrict__ occ) {
+  search_point_u8(f, g, G, blockIdx.x, ox, oy, ou, ov, occ);
+}
+
+// The same over a device-side list of grid points (list[0] entries from
+// list[1]): the points the tiled search hands back.
+__global__ void __launch_bounds__(512) k_search_u8_list(const uint8_t *__restrict__ f,
+                                                        const uint8_t *__restrict__ g,
+                                                        SearchGeom G, const int *__restrict__ list,
+                                                        double *__restrict__ ox,
+                                                        double *__restrict__ oy,
+                                                        double *__restrict__ ou,
+                                                        double *__restrict__ ov,
+                                                        double *__restrict__ occ) {
+  const int n = list[0];
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    search_point_u8(f, g, G, list[1 + i], ox, oy, ou, ov, occ);
+    __syncthreads();
+  }
+}
+
+// ---- 8-bit images, tiled: step a multiple of 4 that divides the subset size.
+// Neighbouring subsets overlap (step 8 of a 33 px window: every pixel lies in
+// 16 windows), so the per-point kernel above recomputes each product
+// f(q) g(q + d) up to 16 times.  Here one CTA takes a TSX x TSY tile of grid
+// points and every shift d = (a, b) of the cropped map once: a thread walks
+// the tile's rows for its shift, forms each 4-pixel group product once
+// (dp4a on word-aligned views of g, no funnel shifts) and assembles the
+// windows from step x step block sums:
+//   window(ix, iy) = blocks iy .. iy+QB-1 (all rows) + row 0 of block iy+QB,
+//   each block row = groups GS*ix .. GS*ix+Q-1 + the first pixel of group
+//   GS*ix+Q,
+// with the pixels whose partner lies beyond the search region (the outer
+// ring of the map) left out exactly.  All sums are exact 32-bit integers, the
+// same ones the per-point kernel forms.
+//
+// Peak search without an FP64 division per entry: each entry's NCC is first
+// estimated in FP32 from the exact integers (interior entries from a
+// per-image table of window sums and 1/sqrt of the window variance term, ring
+// entries from the same FP64 numerator and denominator as ncc_combine),
+// |estimate - FP64 value| < kTileEps.  A per-point lower bound lb on the
+// maximum (max of estimate - eps) grows as the tile's shifts are processed;
+// entries with estimate + eps >= lb are kept with their exact correlation
+// sum, and only those (and the 3 x 3 neighbourhood of the winner) are
+// evaluated with ncc_combine.  Every entry that can be the maximum (or tie
+// with it) is kept, so argmax and findpeak's fit are those of the full map.
+// A point with more than kTileCap kept entries (near-ties, flat search
+// regions), or whose kept maximum falls below lb, is handed to the per-point
+// kernel.
+constexpr int kTileCap = 24;
+constexpr float kTileEps = 1e-5f;
+constexpr int kTileThreads = 256;
+
+struct TileSub {
+  int st, st2, cs0, csL, rs0, rsL, c00, cL0, c0L, cLL;
+  float invT;     // 1 / sqrt(mn st2 - st^2)
+  unsigned lb;    // ordered key of the lower bound on the maximum
+  int cnt;        // kept entries
+  int state;      // 0 searched, 1 constant template (NaN), 2 beyond the grid
+  int pad[2];
+};
+
+struct TileArgs {
+  const uint8_t *f, *g;
+  const unsigned *sat1, *sat2;  // (W+1) x (H+1) summed-area tables of g, g^2 (mod 2^32)
+  const uint2 *tab;             // W x H: (window sum, bits of 1/sqrt(C0)) of full windows
+  const double *mu;
+  double *ox, *oy, *ou, *ov, *occ;
+  int *fb;                      // fb[0] count, fb[1 ..] grid points for the per-point kernel
+  int W, H, px1, py1, nx, ny, w, sx, sy, cr, cc;
+  int tsy, ndy, nbatch, pitch, rows_g, pb;
+  long long mn;
+  int off_g, off_sub, off_cand;
+};
+
+__device__ __forceinline__ unsigned fkey(float x) {  // order-preserving float -> unsigned
+  const unsigned u = __float_as_uint(x);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+__device__ __forceinline__ long long sat_rect(const unsigned *__restrict__ s, long long W1, int x0,
+                                              int x1, int y0, int y1) {
+  // wrapping 32-bit arithmetic: exact whenever the rectangle's sum is < 2^32
+  return (long long)(unsigned)(s[y1 * W1 + x1] - s[y0 * W1 + x1] - s[y1 * W1 + x0] +
+                               s[y0 * W1 + x0]);
+}
+
+// template pixels of entry (a, b) whose partner lies beyond the search region
+__device__ __forceinline__ void tile_pad(const TileSub &S, int a, int b, int cr, int cc, int tw,
+                                         long long *st_out, long long *n_out) {
+  const int nco = (a == 0) || (a == cr - 1), nro = (b == 0) || (b == cc - 1);
+  long long so = 0;
+  if (a == 0) so += S.cs0;
+  if (a == cr - 1) so += S.csL;
+  if (b == 0) so += S.rs0;
+  if (b == cc - 1) so += S.rsL;
+  if (nco && nro) so -= (b == 0) ? (a == 0 ? S.c00 : S.cL0) : (a == 0 ? S.c0L : S.cLL);
+  *st_out = so;
+  *n_out = (long long)nco * tw + (long long)nro * tw - (long long)nco * nro;
+}
+
+// FP64 NCC of entry (a, b) of tile point s from its exact correlation sum
+__device__ __forceinline__ double tile_exact(const TileArgs &A, const TileSub &S, int px, int py,
+                                             int tw, int a, int b, unsigned acc, double mu) {
+  const int qx = px + a - 1 - A.sx, qy = py + b - 1 - A.sy;
+  const int x0 = qx + (a == 0), x1 = qx + tw - (a == A.cr - 1);
+  const int y0 = qy + (b == 0), y1 = qy + tw - (b == A.cc - 1);
+  const long long W1 = A.W + 1;
+  const long long sd = sat_rect(A.sat1, W1, x0, x1, y0, y1);
+  const long long sd2 = sat_rect(A.sat2, W1, x0, x1, y0, y1);
+  long long st_out, n_out;
+  tile_pad(S, a, b, A.cr, A.cc, tw, &st_out, &n_out);
+  return ncc_combine(A.mn, S.st, S.st2, (long long)acc, sd, sd2, st_out, n_out, mu);
+}
+
+template <int STEP, int WS, int TSX>
+struct TileShape {
+  static constexpr int TW = WS + 1, Q = WS / 4, GS = STEP / 4, QB = WS / STEP;
+  static constexpr int NG = GS * (TSX - 1) + Q + 1;  // 4-pixel groups of a tile row
+  static constexpr int NE = TSX + QB;                // groups whose first pixel is kept apart
+  static constexpr int NGP = (NG + 3) & ~3;          // words per staged f row
+};
+
+// exact correlation sum of entry (a, b) of tile point (ix, iy), by one warp
+template <int STEP, int WS, int TSX>
+__device__ __forceinline__ unsigned tile_direct(const uint32_t *Fw, const uint32_t *Gw, int pitch,
+                                                int ix, int iy, int a, int b, int cr, int cc) {
+  using T = TileShape<STEP, WS, TSX>;
+  const int lane = threadIdx.x & 31;
+  unsigned sum = 0;
+  for (int ty = lane; ty < T::TW; ty += 32) {
+    if ((b == 0 && ty == 0) || (b == cc - 1 && ty == T::TW - 1)) continue;
+    const int y = iy * STEP + ty;
+    const uint32_t *fr = Fw + y * T::NGP + T::GS * ix;
+    const uint32_t *gr = Gw + (y + b) * pitch + ix * STEP + a;
+#pragma unroll
+    for (int k = 0; k < T::Q; ++k) {
+      uint32_t fw = fr[k];
+      if (k == 0 && a == 0) fw &= 0xFFFFFF00u;
+      sum = __dp4a(fw, gr[4 * k], sum);
+    }
+    if (a != cr - 1) sum = __dp4a(fr[T::Q] & 0xFFu, gr[4 * T::Q], sum);
+  }
+  return __reduce_add_sync(0xffffffffu, sum);
+}
+
+// one tile row for shift (a, b): group products into acc, first pixels into accE
+template <int STEP, int WS, int TSX>
+__device__ __forceinline__ void tile_row(const uint32_t *__restrict__ frow,
+                                         const uint32_t *__restrict__ grow,
+                                         unsigned (&acc)[TileShape<STEP, WS, TSX>::NG],
+                                         unsigned (&accE)[TileShape<STEP, WS, TSX>::NE]) {
+  using T = TileShape<STEP, WS, TSX>;
+  uint32_t fw[T::NGP];
+#pragma unroll
+  for (int k4 = 0; k4 < T::NGP / 4; ++k4) {
+    const uint4 v = reinterpret_cast<const uint4 *>(frow)[k4];
+    fw[4 * k4] = v.x;
+    fw[4 * k4 + 1] = v.y;
+    fw[4 * k4 + 2] = v.z;
+    fw[4 * k4 + 3] = v.w;
+  }
+#pragma unroll
+  for (int k = 0; k < T::NG; ++k) {
+    const uint32_t gw = grow[4 * k];
+    if (k < T::NG - 1) acc[k] = __dp4a(fw[k], gw, acc[k]);
+    if (k % T::GS == 0) accE[k / T::GS] = __dp4a(fw[k] & 0xFFu, gw, accE[k / T::GS]);
+  }
+}
+
+// the TSX horizontal window sums of the rows accumulated in acc / accE
+template <int STEP, int WS, int TSX>
+__device__ __forceinline__ void tile_hsum(const unsigned (&acc)[TileShape<STEP, WS, TSX>::NG],
+                                          const unsigned (&accE)[TileShape<STEP, WS, TSX>::NE],
+                                          unsigned cF, unsigned cL, unsigned (&S)[TSX]) {
+  using T = TileShape<STEP, WS, TSX>;
+  unsigned run = 0;
+#pragma unroll
+  for (int k = 0; k < T::Q; ++k) run += acc[k];
+#pragma unroll
+  for (int ix = 0; ix < TSX; ++ix) {
+    S[ix] = run + cL * accE[ix + T::QB] - cF * accE[ix];
+    if (ix + 1 < TSX) {
+#pragma unroll
+      for (int k = 0; k < T::GS; ++k) run += acc[T::GS * ix + T::Q + k] - acc[T::GS * ix + k];
+    }
+  }
+}
+
+template <int STEP, int WS, int TSX>
+__global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) {
+  using T = TileShape<STEP, WS, TSX>;
+  constexpr int TW = T::TW, NG = T::NG, NE = T::NE, NGP = T::NGP, QB = T::QB;
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t *Fw = reinterpret_cast<uint32_t *>(smem);
+  uint32_t *Gw = reinterpret_cast<uint32_t *>(smem + A.off_g);
+  TileSub *sub = reinterpret_cast<TileSub *>(smem + A.off_sub);
+  uint2 *cand = reinterpret_cast<uint2 *>(smem + A.off_cand);
+  uint8_t *tmp = smem + A.off_cand;  // g bytes while staging (the candidates come later)
+  const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nth >> 5;
+  const int TSY = A.tsy, NS = TSX * TSY, RYf = (TSY - 1) * STEP + TW;
+  const int cr = A.cr, cc = A.cc, pitch = A.pitch;
+  const int tx0 = blockIdx.x * TSX, ty0 = blockIdx.y * TSY;       // first grid point
+  const int px0 = A.px1 + tx0 * STEP, py0 = A.py1 + ty0 * STEP;   // its 0-based corner
+  const int gx0 = px0 - A.sx - 1, gy0 = py0 - A.sy - 1;           // corner of the g tile
+
+  // ---- stage f (4 pixels a word) and g (word m of a row = bytes m .. m+3)
+  for (int i = tid; i < RYf * NGP; i += nth) {
+    const int y = i / NGP, k = i - y * NGP;
+    unsigned v = 0;
+    if (py0 + y < A.H) {
+      const uint8_t *row = A.f + (long long)(py0 + y) * A.W;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int x = px0 + 4 * k + j;
+        if (x < A.W) v |= (unsigned)row[x] << (8 * j);
+      }
+    }
+    Fw[i] = v;
+  }
+  for (int i = tid; i < A.rows_g * A.pb; i += nth) {
+    const int r = i / A.pb, x = i - r * A.pb;
+    const int yy = gy0 + r, xx = gx0 + x;
+    tmp[i] = (yy < A.H && xx < A.W) ? A.g[(long long)yy * A.W + xx] : (uint8_t)0;
+  }
+  __syncthreads();
+  for (int i = tid; i < A.rows_g * pitch; i += nth) {
+    const int r = i / pitch, m = i - r * pitch;
+    const uint32_t *tw = reinterpret_cast<const uint32_t *>(tmp + r * A.pb);
+    Gw[i] = __funnelshift_r(tw[m >> 2], tw[(m >> 2) + 1], 8 * (m & 3));
+  }
+  // ---- template sums of every point (a warp per point, lanes over rows)
+  for (int s = wid; s < NS; s += nw) {
+    const int ix = s % TSX, iy = s / TSX;
+    const bool valid = tx0 + ix < A.nx && ty0 + iy < A.ny;
+    int v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // st st2 cs0 csL rs0 rsL c00 cL0 c0L cLL
+    if (valid)
+      for (int ty = lane; ty < TW; ty += 32) {
+        const uint32_t *fr = Fw + (iy * STEP + ty) * NGP + T::GS * ix;
+        unsigned rs = 0, rq = 0;
+#pragma unroll
+        for (int k = 0; k < T::Q; ++k) {
+          rs = __dp4a(fr[k], 0x01010101u, rs);
+          rq = __dp4a(fr[k], fr[k], rq);
+        }
+        const int first = fr[0] & 0xFF, last = fr[T::Q] & 0xFF;
+        rs += last;
+        rq += last * last;
+        v[0] += rs;
+        v[1] += rq;
+        v[2] += first;
+        v[3] += last;
+        if (ty == 0) { v[4] = rs; v[6] = first; v[7] = last; }
+        if (ty == TW - 1) { v[5] = rs; v[8] = first; v[9] = last; }
+      }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) v[k] = __reduce_add_sync(0xffffffffu, v[k]);
+    if (lane == 0) {
+      TileSub &S = sub[s];
+      S.st = v[0]; S.st2 = v[1]; S.cs0 = v[2]; S.csL = v[3]; S.rs0 = v[4]; S.rsL = v[5];
+      S.c00 = v[6]; S.cL0 = v[7]; S.c0L = v[8]; S.cLL = v[9];
+      const long long denT = A.mn * v[1] - (long long)v[0] * v[0];
+      S.state = !valid ? 2 : (denT == 0 ? 1 : 0);
+      S.invT = denT > 0 ? (float)(1.0 / sqrt((double)denT)) : 0.f;
+      S.lb = 0u;
+      S.cnt = 0;
+    }
+  }
+  __syncthreads();
+  const double mu = *A.mu;
+
+  // ---- every shift of the cropped map, ndy map columns per batch
+  for (int bt = 0; bt < A.nbatch; ++bt) {
+    int a = tid % cr, b = bt * A.ndy + tid / cr;
+    const bool active = tid < cr * A.ndy && b < cc;
+    if (!active) a = b = 0;  // in-bounds work whose results are dropped
+    const unsigned cF = (a == 0), cL = (a != cr - 1), cRF = (b == 0), cRL = (b != cc - 1);
+    const bool ring = (a == 0) || (a == cr - 1) || (b == 0) || (b == cc - 1);
+    const uint32_t *gbase = Gw + b * pitch + a;
+    unsigned win[QB][TSX];
+    unsigned acc[NG], accE[NE], S[TSX];
+    for (int j0 = 0; j0 < TSY + QB; j0 += QB) {
+#pragma unroll
+      for (int sl = 0; sl < QB; ++sl) {
+        const int j = j0 + sl;
+        if (j >= TSY + QB) break;
+#pragma unroll
+        for (int k = 0; k < NG; ++k) acc[k] = 0;
+#pragma unroll
+        for (int k = 0; k < NE; ++k) accE[k] = 0;
+        tile_row<STEP, WS, TSX>(Fw + j * STEP * NGP, gbase + j * STEP * pitch, acc, accE);
+        tile_hsum<STEP, WS, TSX>(acc, accE, cF, cL, S);
+        if (j >= QB) {
+          // ---- the windows of point row iy are complete: screen them
+          const int iy = j - QB;
+          float rlo[TSX], rhi[TSX];
+#pragma unroll
+          for (int ix = 0; ix < TSX; ++ix) {
+            const unsigned C = win[sl][ix] + cRL * S[ix];
+            win[sl][ix] = C;
+            const TileSub &P = sub[iy * TSX + ix];
+            rlo[ix] = -INFINITY;
+            rhi[ix] = -INFINITY;
+            if (active && P.state == 0) {
+              const int px = px0 + ix * STEP, py = py0 + iy * STEP;
+              const int qx = px + a - 1 - A.sx, qy = py + b - 1 - A.sy;
+              float r;
+              if (!ring) {
+                const uint2 e = A.tab[(long long)qy * A.W + qx];
+                const long long num = A.mn * (long long)C - (long long)P.st * (int)e.x;
+                r = (float)num * P.invT * __uint_as_float(e.y);
+              } else {
+                const long long W1 = A.W + 1;
+                const int x0 = qx + (a == 0), x1 = qx + TW - (a == cr - 1);
+                const int y0 = qy + (b == 0), y1 = qy + TW - (b == cc - 1);
+                const long long sd = sat_rect(A.sat1, W1, x0, x1, y0, y1);
+                const long long sd2 = sat_rect(A.sat2, W1, x0, x1, y0, y1);
+                long long st_out, n_out;
+                tile_pad(P, a, b, cr, cc, TW, &st_out, &n_out);
+                double num, den;
+                ncc_parts(A.mn, P.st, (long long)C, sd, sd2, st_out, n_out, mu, &num, &den);
+                r = den > 0.0 ? (float)num * P.invT * rsqrtf((float)den) : 0.f;
+              }
+              rlo[ix] = r - kTileEps;
+              rhi[ix] = r + kTileEps;
+            }
+          }
+#pragma unroll
+          for (int ix = 0; ix < TSX; ++ix) {
+            const unsigned kmax = __reduce_max_sync(0xffffffffu, fkey(rlo[ix]));
+            if (lane == 0) atomicMax(&sub[iy * TSX + ix].lb, kmax);
+          }
+          __syncthreads();
+#pragma unroll
+          for (int ix = 0; ix < TSX; ++ix) {
+            const int s = iy * TSX + ix;
+            if (rhi[ix] != -INFINITY && fkey(rhi[ix]) >= sub[s].lb) {
+              const int pos = atomicAdd(&sub[s].cnt, 1);
+              if (pos < kTileCap) cand[s * kTileCap + pos] = make_uint2(b * cr + a, win[sl][ix]);
+            }
+          }
+        }
+        if (j < TSY) {
+#pragma unroll
+          for (int ix = 0; ix < TSX; ++ix) win[sl][ix] = 0u - cRF * S[ix];
+        }
+        if (j < TSY + QB - 1) {
+          for (int rr = 1; rr < STEP; ++rr)
+            tile_row<STEP, WS, TSX>(Fw + (j * STEP + rr) * NGP, gbase + (j * STEP + rr) * pitch,
+                                    acc, accE);
+          tile_hsum<STEP, WS, TSX>(acc, accE, cF, cL, S);
+          // the open windows: point rows j-QB+1 .. j, one per slot
+#pragma unroll
+          for (int s2 = 0; s2 < QB; ++s2) {
+            const int iy = j - ((sl - s2 + QB) % QB);
+            if (iy >= 0 && iy < TSY) {
+#pragma unroll
+              for (int ix = 0; ix < TSX; ++ix) win[s2][ix] += S[ix];
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- exact FP64 values of the kept entries, argmax, findpeak (a warp a point)
+  for (int s = wid; s < NS; s += nw) {
+    const TileSub &P = sub[s];
+    if (P.state == 2) continue;
+    const int ix = s % TSX, iy = s / TSX;
+    const int gix = tx0 + ix, giy = ty0 + iy;
+    const long long out_idx = (long long)giy + (long long)gix * A.ny;
+    const int px = px0 + ix * STEP, py = py0 + iy * STEP;
+    const int ii = px + 1, jj = py + 1;  // 1-based
+    if (P.state == 1) {
+      if (lane == 0) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        A.ox[out_idx] = (ii + ii + A.w) / 2.0;
+        A.oy[out_idx] = (jj + jj + A.w) / 2.0;
+        A.ou[out_idx] = nan;
+        A.ov[out_idx] = nan;
+        A.occ[out_idx] = nan;
+      }
+      continue;
+    }
+    const int n = P.cnt;
+    bool hand_back = n > kTileCap;
+    double best = -INFINITY;
+    int bi = 0x7fffffff;
+    if (!hand_back) {
+      if (lane < n) {
+        const uint2 e = cand[s * kTileCap + lane];
+        bi = (int)e.x;
+        best = tile_exact(A, P, px, py, TW, bi % cr, bi / cr, e.y, mu);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      // the bound must hold for the kept maximum (it can only fail where an
+      // estimate met ncc_combine's clamp of |r| > 1)
+      hand_back = !(best >= (double)fkey_inv(P.lb));
+    }
+    if (hand_back) {
+      if (lane == 0) {
+        const int pos = atomicAdd(A.fb, 1);
+        A.fb[1 + pos] = giy * A.nx + gix;
+      }
+      continue;
+    }
+    const int am = bi % cr, bm = bi / cr;
+    double rpk = am + 1, cpk = bm + 1, mf = best;
+    if (am > 0 && am < cr - 1 && bm > 0 && bm < cc - 1) {
+      unsigned my_acc = 0;
+      int my_a = am, my_b = bm;
+      for (int k = 0; k < 9; ++k) {
+        if (k == 4) continue;
+        const int na = am + k % 3 - 1, nb = bm + k / 3 - 1;
+        const unsigned c = tile_direct<STEP, WS, TSX>(Fw, Gw, pitch, ix, iy, na, nb, cr, cc);
+        if (lane == k) {
+          my_acc = c;
+          my_a = na;
+          my_b = nb;
+        }
+      }
+      double r = best;
+      if (lane < 9 && lane != 4) r = tile_exact(A, P, px, py, TW, my_a, my_b, my_acc, mu);
+      double u9[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) u9[k] = __shfl_sync(0xffffffffu, r, k);
+      if (lane == 0) findpeak_fit9(u9, am, bm, &rpk, &cpk, &mf);
+    }
+    if (lane == 0) {
+      A.ox[out_idx] = (ii + ii + A.w) / 2.0;
+      A.oy[out_idx] = (jj + jj + A.w) / 2.0;
+      A.ou[out_idx] = __dsub_rn(rpk, (double)(A.sx + 2));
+      A.ov[out_idx] = __dsub_rn(cpk, (double)(A.sy + 2));
+      A.occ[out_idx] = mf;
+    }
+  }
+}
+
+// ---- summed-area tables of g and g^2 (wrapping 32-bit), (W+1) x (H+1)
+// rows: a block per image row, 8 pixels a thread, block scan
+__global__ void __launch_bounds__(256) k_sat_rows_u8(const uint8_t *__restrict__ g, int W, int H,
+                                                     unsigned *__restrict__ s1,
+                                                     unsigned *__restrict__ s2) {
+  const int y = blockIdx.x;
+  const long long W1 = W + 1;
+  unsigned *r1 = s1 + (y + 1) * W1, *r2 = s2 + (y + 1) * W1;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  __shared__ unsigned w1[8], w2[8];
+  if (y == 0)
+    for (int x = tid; x <= W; x += 256) s1[x] = s2[x] = 0u;
+  if (tid == 0) r1[0] = r2[0] = 0u;
+  unsigned carry1 = 0, carry2 = 0;
+  const uint8_t *row = g + (long long)y * W;
+  for (int x0 = 0; x0 < W; x0 += 256 * 8) {
+    const int xb = x0 + 8 * tid;
+    unsigned p1[8], p2[8], t1 = 0, t2 = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const unsigned v = xb + j < W ? row[xb + j] : 0u;
+      t1 += v;
+      t2 += v * v;
+      p1[j] = t1;
+      p2[j] = t2;
+    }
+    unsigned i1 = t1, i2 = t2;  // inclusive scan of the thread totals
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned u1 = __shfl_up_sync(0xffffffffu, i1, o), u2 = __shfl_up_sync(0xffffffffu, i2, o);
+      if (lane >= o) {
+        i1 += u1;
+        i2 += u2;
+      }
+    }
+    if (lane == 31) {
+      w1[wid] = i1;
+      w2[wid] = i2;
+    }
+    __syncthreads();
+    unsigned b1 = carry1 + i1 - t1, b2 = carry2 + i2 - t2;
+    for (int k = 0; k < wid; ++k) {
+      b1 += w1[k];
+      b2 += w2[k];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (xb + j < W) {
+        r1[xb + j + 1] = b1 + p1[j];
+        r2[xb + j + 1] = b2 + p2[j];
+      }
+    for (int k = 0; k < 8; ++k) {
+      carry1 += w1[k];
+      carry2 += w2[k];
+    }
+    __syncthreads();
+  }
+}
+
+constexpr int kSatRows = 64;  // rows per column chunk
+
+// columns: in-place prefix within chunks of kSatRows table rows, chunk totals
+__global__ void k_sat_cols_u8(unsigned *__restrict__ s1, unsigned *__restrict__ s2, int W, int H,
+                              unsigned *__restrict__ tot) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, ch = blockIdx.y;
+  const long long W1 = W + 1;
+  if (x > W) return;
+  const int y0 = 1 + ch * kSatRows, y1 = min(H + 1, y0 + kSatRows);
+  unsigned a1 = 0, a2 = 0;
+  for (int y = y0; y < y1; ++y) {
+    a1 += s1[y * W1 + x];
+    a2 += s2[y * W1 + x];
+    s1[y * W1 + x] = a1;
+    s2[y * W1 + x] = a2;
+  }
+  tot[2 * (ch * W1 + x)] = a1;
+  tot[2 * (ch * W1 + x) + 1] = a2;
+}
+
+// box table of the full windows with top-left corners [x0, x1] x [y0, y1]
+__global__ void k_box_tab(const unsigned *__restrict__ s1, const unsigned *__restrict__ s2, int W,
+                          int tw, long long mn, int x0, int x1, int y0, uint2 *__restrict__ tab) {
+  const int x = x0 + blockIdx.x * blockDim.x + threadIdx.x, y = y0 + blockIdx.y;
+  if (x > x1) return;
+  const long long W1 = W + 1;
+  const long long sd = sat_rect(s1, W1, x, x + tw, y, y + tw);
+  const long long sd2 = sat_rect(s2, W1, x, x + tw, y, y + tw);
+  const long long c0 = mn * sd2 - sd * sd;
+  tab[(long long)y * W + x] =
+      make_uint2((unsigned)sd, c0 > 0 ? __float_as_uint(rsqrtf((float)c0)) : 0u);
+}
+
+// add the totals of the chunks above to every chunk but the first
+__global__ void k_sat_fix_u8(unsigned *__restrict__ s1, unsigned *__restrict__ s2, int W, int H,
+                             const unsigned *__restrict__ tot) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, ch = blockIdx.y + 1;
+  const long long W1 = W + 1;
+  if (x > W) return;
+  unsigned o1 = 0, o2 = 0;
+  for (int c = 0; c < ch; ++c) {
+    o1 += tot[2 * (c * W1 + x)];
+    o2 += tot[2 * (c * W1 + x) + 1];
+  }
+  const int y0 = 1 + ch * kSatRows, y1 = min(H + 1, y0 + kSatRows);
+  for (int y = y0; y < y1; ++y) {
+    s1[y * W1 + x] += o1;
+    s2[y * W1 + x] += o2;
+  }
+}
+
+constexpr int kTileTSX = 8;  // grid points per tile row
+
+struct TilePlan {
+  int tsy = 0, ndy = 0, nbatch = 0, pitch = 0, rows_g = 0, pb = 0, threads = 0;
+  int off_g = 0, off_sub = 0, off_cand = 0, total = 0;
+};
+
+// tile rows, thread batches and the shared-memory layout; the largest tile
+// (up to 8 point rows) that lets two CTAs share an SM, else one
+template <int STEP, int WS>
+bool tile_plan(int sx, int sy, TilePlan &P) {
+  using T = TileShape<STEP, WS, kTileTSX>;
+  const int cr = 2 * sx + 3, cc = 2 * sy + 3;
+  if (cr > kTileThreads) return false;
+  P.ndy = std::min(cc, kTileThreads / cr);
+  P.nbatch = (cc + P.ndy - 1) / P.ndy;
+  P.threads = (cr * P.ndy + 31) / 32 * 32;
+  // odd rows of a warp continue the bank sequence of the row before
+  const int minp = cr + 4 * T::NG - 4;
+  P.pitch = minp + (((cr - minp) % 32) + 32) % 32;
+  P.pb = (int)align16(4 * ((P.pitch - 1) / 4 + 2));
+  for (const size_t limit : {(size_t)113 * 1024, (size_t)227 * 1024})
+    for (int tsy = 8; tsy >= 1; --tsy) {
+      const int ryf = (tsy - 1) * STEP + T::TW, rows_g = ryf + cc - 1, ns = kTileTSX * tsy;
+      size_t o = align16((size_t)ryf * T::NGP * 4);
+      const size_t og = o;
+      o += align16((size_t)rows_g * P.pitch * 4);
+      const size_t os = o;
+      o += align16((size_t)ns * sizeof(TileSub));
+      const size_t oc = o;
+      o += align16(std::max((size_t)ns * kTileCap * sizeof(uint2), (size_t)rows_g * P.pb));
+      if (o <= limit) {
+        P.tsy = tsy;
+        P.rows_g = rows_g;
+        P.off_g = (int)og;
+        P.off_sub = (int)os;
+        P.off_cand = (int)oc;
+        P.total = (int)o;
+        return true;
+      }
+    }
+  return false;
+}
+
+template <int STEP, int WS>
+int tile_launch(TileArgs A, const TilePlan &P, cudaStream_t st) {
+  A.tsy = P.tsy; A.ndy = P.ndy; A.nbatch = P.nbatch; A.pitch = P.pitch;
+  A.rows_g = P.rows_g; A.pb = P.pb;
+  A.off_g = P.off_g; A.off_sub = P.off_sub; A.off_cand = P.off_cand;
+  auto kern = k_search_tile<STEP, WS, kTileTSX>;
+  ALDIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, P.total));
+  const dim3 grid((A.nx + kTileTSX - 1) / kTileTSX, (A.ny + P.tsy - 1) / P.tsy);
+  kern<<<grid, P.threads, P.total, st>>>(A);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+// (step, winsize) pairs with a tiled kernel
+#define ALDIC_TILE_SHAPES(X) X(4, 16) X(8, 16) X(8, 24) X(8, 32) X(16, 32)
+
+bool tile_shape(int step, int w, int sx, int sy, TilePlan &P) {
+#define ALDIC_TILE_PLAN(S, Wd) \
+  if (step == S && w == Wd) return tile_plan<S, Wd>(sx, sy, P);
+  ALDIC_TILE_SHAPES(ALDIC_TILE_PLAN)
+#undef ALDIC_TILE_PLAN
+  return false;
+}
+
+int tile_dispatch(const TileArgs &A, const TilePlan &P, int step, cudaStream_t st) {
+#define ALDIC_TILE_GO(S, Wd) \
+  if (step == S && A.w == Wd) return tile_launch<S, Wd>(A, P, st);
+  ALDIC_TILE_SHAPES(ALDIC_TILE_GO)
+#undef ALDIC_TILE_GO
+  return E_ARG;
+}
+
+struct TileBufs {
+  unsigned *sat1, *sat2, *tot;
+  uint2 *tab;
+  int *fb;
+  size_t bytes;
+};
+TileBufs tile_bufs(void *base, int W, int H, long long npts) {
+  const size_t W1 = W + 1, H1 = H + 1, nch = (H + kSatRows - 1) / kSatRows;
+  TileBufs b;
+  size_t o = 0;
+  const size_t o_s1 = o; o += align16(W1 * H1 * 4);
+  const size_t o_s2 = o; o += align16(W1 * H1 * 4);
+  const size_t o_t = o; o += align16(2 * W1 * nch * 4);
+  const size_t o_tab = o; o += align16((size_t)W * H * 8);
+  const size_t o_fb = o; o += align16((size_t)(npts + 1) * 4);
+  char *p = (char *)base;
+  b.sat1 = (unsigned *)(p + o_s1);
+  b.sat2 = (unsigned *)(p + o_s2);
+  b.tot = (unsigned *)(p + o_t);
+  b.tab = (uint2 *)(p + o_tab);
+  b.fb = (int *)(p + o_fb);
+  b.bytes = o;
+  return b;
+}
+
+// tiled 8-bit search; false in *used when the geometry has no tiled kernel
+int tile_search(const uint8_t *f, const uint8_t *g, const SearchGeom &G, SearchWork &sw,
+                double *x, double *y, double *u, double *v, double *cc, int threads_pt,
+                size_t smem_pt, cudaStream_t st, bool *used) {
+  *used = false;
+  TilePlan P;
+  if (G.step % 4 || G.w % G.step || !tile_shape(G.step, G.w, G.sx, G.sy, P)) return OK;
+  const int px1 = G.gx1 - 1, py1 = G.gy1 - 1;
+  if (px1 - G.sx - 1 < 0 || py1 - G.sy - 1 < 0) return OK;
+  const long long npts = (long long)G.nx * G.ny;
+  int rc = search_work_ensure(sw, G.W, G.H, npts);
+  if (rc) return rc;
+  const TileBufs B = tile_bufs(sw.buf.p, G.W, G.H, npts);
+  const int W1 = G.W + 1, nch = (G.H + kSatRows - 1) / kSatRows;
+  const long long mn = (long long)G.tw * G.tw;
+  k_sat_rows_u8<<<G.H, 256, 0, st>>>(g, G.W, G.H, B.sat1, B.sat2);
+  k_sat_cols_u8<<<dim3((W1 + 255) / 256, nch), 256, 0, st>>>(B.sat1, B.sat2, G.W, G.H, B.tot);
+  if (nch > 1)
+    k_sat_fix_u8<<<dim3((W1 + 255) / 256, nch - 1), 256, 0, st>>>(B.sat1, B.sat2, G.W, G.H,
+                                                                   B.tot);
+  // full windows of the interior entries: corners px1 - sx .. last + sx
+  const int x0 = px1 - G.sx, x1 = px1 + (G.nx - 1) * G.step + G.sx;
+  const int y0 = py1 - G.sy, y1 = py1 + (G.ny - 1) * G.step + G.sy;
+  k_box_tab<<<dim3((x1 - x0 + 256) / 256, y1 - y0 + 1), 256, 0, st>>>(B.sat1, B.sat2, G.W, G.tw,
+                                                                      mn, x0, x1, y0, B.tab);
+  ALDIC_CUDA(cudaMemsetAsync(B.fb, 0, sizeof(int), st));
+  TileArgs A{};
+  A.f = f; A.g = g; A.sat1 = B.sat1; A.sat2 = B.sat2; A.tab = B.tab; A.mu = G.mu;
+  A.ox = x; A.oy = y; A.ou = u; A.ov = v; A.occ = cc; A.fb = B.fb;
+  A.W = G.W; A.H = G.H; A.px1 = px1; A.py1 = py1; A.nx = G.nx; A.ny = G.ny; A.w = G.w;
+  A.sx = G.sx; A.sy = G.sy; A.cr = G.cr; A.cc = G.cc; A.mn = mn;
+  if ((rc = tile_dispatch(A, P, G.step, st))) return rc;
+  // the points handed back: per-point kernel over the device-side list
+  const int nb = (int)std::min<long long>(npts, 296);
+  k_search_u8_list<<<nb, threads_pt, smem_pt, st>>>(f, g, G, B.fb, x, y, u, v, cc);
+  ALDIC_CUDA(cudaGetLastError());
+  *used = true;
+  return OK;
+}
+
 // ---- q-factors over the full (2w+2s+1)^2 map (optional, direct sums)
 template <typename T>
 __global__ void k_qfactor(const T *__restrict__ f, const T *__restrict__ g, SearchGeom G,
@@ -652,7 +1359,8 @@ __global__ void k_qfactor(const T *__restrict__ f, const T *__restrict__ g, Sear
 
 template <typename T>
 int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, double *y,
-                  double *u, double *v, double *cc, double *pce, double *ppe, cudaStream_t st) {
+                  double *u, double *v, double *cc, double *pce, double *ppe, cudaStream_t st,
+                  SearchWork *sw) {
   using Tr = SearchTraits<T>;
   using V = typename Tr::V;
   using S = typename SumT<Tr::integer>::type;
@@ -668,8 +1376,17 @@ int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, 
                 "integer search: window/search size too large for shared memory");
     ALDIC_CUDA(cudaFuncSetAttribute(k_search_u8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)L.total));
-    k_search_u8<<<npts, threads, L.total, st>>>((const uint8_t *)f, (const uint8_t *)g, G, x, y,
-                                                 u, v, cc);
+    ALDIC_CUDA(cudaFuncSetAttribute(k_search_u8_list,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    bool tiled = false;
+    if (sw) {
+      const int rc = tile_search((const uint8_t *)f, (const uint8_t *)g, G, *sw, x, y, u, v, cc,
+                                 threads, L.total, st, &tiled);
+      if (rc) return rc;
+    }
+    if (!tiled)
+      k_search_u8<<<npts, threads, L.total, st>>>((const uint8_t *)f, (const uint8_t *)g, G, x,
+                                                   y, u, v, cc);
   } else {
     SmemLayout<V, S> L(G);
     ALDIC_CHECK(L.total <= 227 * 1024, E_ARG,
@@ -709,10 +1426,14 @@ int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsiz
   return OK;
 }
 
+int search_work_ensure(SearchWork &w, int W, int H, long long npts) {
+  return w.buf.ensure(tile_bufs(nullptr, W, H, npts).bytes);
+}
+
 int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,
                const int gridx[2], const int gridy[2], int winsize, int step,
                const int search[2], double *x, double *y, double *u, double *v, double *cc,
-               double *pce, double *ppe, cudaStream_t st) {
+               double *pce, double *ppe, cudaStream_t st, SearchWork *sw) {
   SearchGeom G;
   int rc = search_dims(W, H, gridx, gridy, winsize, step, search, &G.nx, &G.ny, &G.gx1, &G.gy1);
   if (rc) return rc;
@@ -729,10 +1450,10 @@ int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, co
   G.dph = G.dh + 2;
   G.mu = mu_g;
   switch (dtype) {
-    case 0: return launch_search<uint8_t>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st);
-    case 1: return launch_search<uint16_t>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st);
-    case 2: return launch_search<float>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st);
-    default: return launch_search<double>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st);
+    case 0: return launch_search<uint8_t>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st, sw);
+    case 1: return launch_search<uint16_t>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st, sw);
+    case 2: return launch_search<float>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st, sw);
+    default: return launch_search<double>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st, sw);
   }
 }
 

@@ -10,12 +10,12 @@ namespace aldic {
 
 constexpr double kSqrtEps = 1.4901161193847656e-08;  // sqrt(DBL_EPSILON) = 2^-26
 
-// NCC at one cropped-map entry from the exact partial sums (same arithmetic
-// as the CPU restatement's ncc_at).
-__device__ __forceinline__ double ncc_combine(long long mn, long long st, long long st2,
-                                              long long stdv, long long sd, long long sd2,
-                                              long long st_pad, long long n_pad, double mu) {
-  const double denT = (double)(mn * st2 - st * st);
+// Numerator and window part of the denominator of one cropped-map entry:
+// the template is correlated with the window whose n_pad pixels beyond the
+// search region read as mu (the mean the padding stands for).
+__device__ __forceinline__ void ncc_parts(long long mn, long long st, long long stdv,
+                                          long long sd, long long sd2, long long st_pad,
+                                          long long n_pad, double mu, double *num, double *den) {
   const double A = (double)(mn * stdv - st * sd);
   const double C0 = (double)(mn * sd2 - sd * sd);
   double B = 0.0, Cc = 0.0;
@@ -24,8 +24,18 @@ __device__ __forceinline__ double ncc_combine(long long mn, long long st, long l
     Cc = __dmul_rn(mu, __dsub_rn(__dmul_rn((double)(n_pad * (mn - n_pad)), mu),
                                  __dmul_rn(2.0, (double)(sd * n_pad))));
   }
-  const double num = __dadd_rn(A, B);
-  const double den = __dadd_rn(C0, Cc);
+  *num = __dadd_rn(A, B);
+  *den = __dadd_rn(C0, Cc);
+}
+
+// NCC at one cropped-map entry from the exact partial sums (same arithmetic
+// as the CPU restatement's ncc_at).
+__device__ __forceinline__ double ncc_combine(long long mn, long long st, long long st2,
+                                              long long stdv, long long sd, long long sd2,
+                                              long long st_pad, long long n_pad, double mu) {
+  const double denT = (double)(mn * st2 - st * st);
+  double num, den;
+  ncc_parts(mn, st, stdv, sd, sd2, st_pad, n_pad, mu, &num, &den);
   if (!(den > 0.0)) return 0.0;
   double r = __ddiv_rn(num, __dsqrt_rn(__dmul_rn(denT, den)));
   if (__dsub_rn(fabs(r), 1.0) > kSqrtEps) r = 0.0;
