@@ -1577,7 +1577,9 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
               "frame: ALDIC_INIT_GIVEN needs aldic_set_init on this node grid");
   if ((rc = ensure_grid_work(c, n))) return rc;
   // search work before any capture (a graph records its addresses)
-  if (qp.init == ALDIC_INIT_SEARCH && (rc = search_work_ensure(c->sw, c->W, c->H, n))) return rc;
+  if (qp.init == ALDIC_INIT_SEARCH &&
+      (rc = search_work_ensure(c->sw, c->W, c->H, M, N, p->search)))
+    return rc;
   // frame slab
   const long long ny_nx = n;
   const size_t need = 256 * 40 + sizeof(double) * (5 * ny_nx + 2 * n + 2 * n + 2 * n + 2 * n + 4 * n +

@@ -575,22 +575,29 @@ __global__ void __launch_bounds__(512) k_search_u8_list(const uint8_t *__restric
 // ring of the map) left out exactly.  All sums are exact 32-bit integers, the
 // same ones the per-point kernel forms.
 //
-// Peak search without an FP64 division per entry: each entry's NCC is first
-// estimated in FP32 from the exact integers (interior entries from a
-// per-image table of window sums and 1/sqrt of the window variance term, ring
-// entries from the same FP64 numerator and denominator as ncc_combine),
-// |estimate - FP64 value| < kTileEps.  A per-point lower bound lb on the
-// maximum (max of estimate - eps) grows as the tile's shifts are processed;
-// entries with estimate + eps >= lb are kept with their exact correlation
-// sum, and only those (and the 3 x 3 neighbourhood of the winner) are
-// evaluated with ncc_combine.  Every entry that can be the maximum (or tie
-// with it) is kept, so argmax and findpeak's fit are those of the full map.
-// A point with more than kTileCap kept entries (near-ties, flat search
-// regions), or whose kept maximum falls below lb, is handed to the per-point
-// kernel.
+// Peak search without an FP64 division per interior entry: each interior
+// entry's NCC is first estimated in FP32 from the exact integers (the window
+// sum and 1/sqrt of the window variance term), |estimate - FP64 value| <
+// kTileEps.  A per-point lower bound lb on the interior maximum (max of
+// estimate - eps) grows as the tile's shifts are processed; entries with
+// estimate + eps >= lb are kept with their exact correlation sum.  The exact
+// sums of the map's outer ring (2 (cr + cc) - 4 entries a point, whose
+// padded windows need the FP64 form) go to a scratch array.  At the end a
+// warp a point evaluates its ring and its kept entries with ncc_combine, and
+// the 3 x 3 neighbourhood of the winner for findpeak.  Every entry that can
+// be the maximum (or tie with it) is evaluated, so argmax and findpeak's fit
+// are those of the full map.  A point with more than kTileCap kept entries
+// (near-ties, flat search regions), or whose evaluated maximum falls below
+// lb, is handed to the per-point kernel.
+//
+// The window sums of every shift of the tile live in shared memory: the
+// full windows (sum, sum of squares, 1/sqrt(C0)) copied from a per-image
+// table, the windows of the outer ring (one column and/or row left out)
+// formed from the staged g.
 constexpr int kTileCap = 24;
 constexpr float kTileEps = 1e-5f;
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 512;
+constexpr int kTileTSX = 8;  // grid points per tile row
 
 struct TileSub {
   int st, st2, cs0, csL, rs0, rsL, c00, cL0, c0L, cLL;
@@ -603,15 +610,15 @@ struct TileSub {
 
 struct TileArgs {
   const uint8_t *f, *g;
-  const unsigned *sat1, *sat2;  // (W+1) x (H+1) summed-area tables of g, g^2 (mod 2^32)
-  const uint2 *tab;             // W x H: (window sum, bits of 1/sqrt(C0)) of full windows
+  const uint4 *tab;  // W x H: (sum, sum of squares, bits of 1/sqrt(C0), 0) of full windows
   const double *mu;
   double *ox, *oy, *ou, *ov, *occ;
-  int *fb;                      // fb[0] count, fb[1 ..] grid points for the per-point kernel
-  int W, H, px1, py1, nx, ny, w, sx, sy, cr, cc;
-  int tsy, ndy, nbatch, pitch, rows_g, pb;
+  int *fb;           // fb[0] count, fb[1 ..] grid points for the per-point kernel
+  unsigned *ringc;   // exact sums of the outer ring, nring a point, tile by tile
+  int W, H, px1, py1, nx, ny, w, sx, sy, cr, cc, nring;
+  int tsy, ndy, nbatch, pitch, rows_g, pb, qxn, qyn;
   long long mn;
-  int off_g, off_sub, off_cand;
+  int off_g, off_ti, off_ra, off_rb, off_rc, off_sub, off_cand;
 };
 
 __device__ __forceinline__ unsigned fkey(float x) {  // order-preserving float -> unsigned
@@ -620,12 +627,6 @@ __device__ __forceinline__ unsigned fkey(float x) {  // order-preserving float -
 }
 __device__ __forceinline__ float fkey_inv(unsigned k) {
   return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
-}
-__device__ __forceinline__ long long sat_rect(const unsigned *__restrict__ s, long long W1, int x0,
-                                              int x1, int y0, int y1) {
-  // wrapping 32-bit arithmetic: exact whenever the rectangle's sum is < 2^32
-  return (long long)(unsigned)(s[y1 * W1 + x1] - s[y0 * W1 + x1] - s[y1 * W1 + x0] +
-                               s[y0 * W1 + x0]);
 }
 
 // template pixels of entry (a, b) whose partner lies beyond the search region
@@ -642,20 +643,6 @@ __device__ __forceinline__ void tile_pad(const TileSub &S, int a, int b, int cr,
   *n_out = (long long)nco * tw + (long long)nro * tw - (long long)nco * nro;
 }
 
-// FP64 NCC of entry (a, b) of tile point s from its exact correlation sum
-__device__ __forceinline__ double tile_exact(const TileArgs &A, const TileSub &S, int px, int py,
-                                             int tw, int a, int b, unsigned acc, double mu) {
-  const int qx = px + a - 1 - A.sx, qy = py + b - 1 - A.sy;
-  const int x0 = qx + (a == 0), x1 = qx + tw - (a == A.cr - 1);
-  const int y0 = qy + (b == 0), y1 = qy + tw - (b == A.cc - 1);
-  const long long W1 = A.W + 1;
-  const long long sd = sat_rect(A.sat1, W1, x0, x1, y0, y1);
-  const long long sd2 = sat_rect(A.sat2, W1, x0, x1, y0, y1);
-  long long st_out, n_out;
-  tile_pad(S, a, b, A.cr, A.cc, tw, &st_out, &n_out);
-  return ncc_combine(A.mn, S.st, S.st2, (long long)acc, sd, sd2, st_out, n_out, mu);
-}
-
 template <int STEP, int WS, int TSX>
 struct TileShape {
   static constexpr int TW = WS + 1, Q = WS / 4, GS = STEP / 4, QB = WS / STEP;
@@ -664,25 +651,76 @@ struct TileShape {
   static constexpr int NGP = (NG + 3) & ~3;          // words per staged f row
 };
 
+// shared-memory views of one tile
+struct TileMem {
+  const uint32_t *Fw, *Gw;
+  const int *tis, *tis2;   // full windows at tile position (qxi, qyi): sums of g, g^2
+  const float *tii;        // and 1 / sqrt(mn sum g^2 - (sum g)^2) (0 where that is <= 0)
+  const uint2 *ra, *rb, *rc;
+  int pitch, qxn, qyn, tsy;
+};
+
+// (sum g, sum g^2) over the part of entry (a, b)'s window inside the search region
+template <int STEP>
+__device__ __forceinline__ uint2 tile_wsum(const TileMem &M, int ix, int iy, int a, int b,
+                                           int cr, int cc) {
+  const bool ra = a == 0 || a == cr - 1, rb = b == 0 || b == cc - 1;
+  const int qxi = ix * STEP + a, qyi = iy * STEP + b;
+  if (!ra && !rb) {
+    const int i = qyi * M.qxn + qxi;
+    return make_uint2((unsigned)M.tis[i], (unsigned)M.tis2[i]);
+  }
+  if (!rb) return M.ra[((a != 0) * kTileTSX + ix) * M.qyn + qyi];
+  if (!ra) return M.rb[((b != 0) * M.tsy + iy) * M.qxn + qxi];
+  return M.rc[(iy * kTileTSX + ix) * 4 + (a != 0) + 2 * (b != 0)];
+}
+
+// the outer ring of the cropped map, k in [0, 2 (cr + cc) - 4): columns a = 0
+// and cr-1 (all b), then rows b = 0 and cc-1 (a = 1 .. cr-2)
+__device__ __forceinline__ void ring_pos(int k, int cr, int cc, int *a, int *b) {
+  if (k < 2 * cc) {
+    *a = k < cc ? 0 : cr - 1;
+    *b = k < cc ? k : k - cc;
+  } else {
+    const int m = k - 2 * cc;
+    *a = 1 + (m < cr - 2 ? m : m - (cr - 2));
+    *b = m < cr - 2 ? 0 : cc - 1;
+  }
+}
+__device__ __forceinline__ int ring_index(int a, int b, int cr, int cc) {
+  if (a == 0) return b;
+  if (a == cr - 1) return cc + b;
+  return 2 * cc + (a - 1) + (b == 0 ? 0 : cr - 2);
+}
+
+// FP64 NCC of entry (a, b) of tile point (ix, iy) from its exact correlation sum
+template <int STEP>
+__device__ __forceinline__ double tile_exact(const TileArgs &A, const TileMem &M, const TileSub &S,
+                                             int ix, int iy, int tw, int a, int b, unsigned acc,
+                                             double mu) {
+  const uint2 w = tile_wsum<STEP>(M, ix, iy, a, b, A.cr, A.cc);
+  long long st_out, n_out;
+  tile_pad(S, a, b, A.cr, A.cc, tw, &st_out, &n_out);
+  return ncc_combine(A.mn, S.st, S.st2, (long long)acc, (long long)w.x, (long long)w.y, st_out,
+                     n_out, mu);
+}
+
 // exact correlation sum of entry (a, b) of tile point (ix, iy), by one warp
 template <int STEP, int WS, int TSX>
 __device__ __forceinline__ unsigned tile_direct(const uint32_t *Fw, const uint32_t *Gw, int pitch,
                                                 int ix, int iy, int a, int b, int cr, int cc) {
   using T = TileShape<STEP, WS, TSX>;
+  constexpr int NW = T::Q + 1;  // words of a template row (the last holds one pixel)
   const int lane = threadIdx.x & 31;
   unsigned sum = 0;
-  for (int ty = lane; ty < T::TW; ty += 32) {
+  for (int p = lane; p < T::TW * NW; p += 32) {  // lanes over (row, word) pairs
+    const int ty = p / NW, k = p - ty * NW;
     if ((b == 0 && ty == 0) || (b == cc - 1 && ty == T::TW - 1)) continue;
     const int y = iy * STEP + ty;
-    const uint32_t *fr = Fw + y * T::NGP + T::GS * ix;
-    const uint32_t *gr = Gw + (y + b) * pitch + ix * STEP + a;
-#pragma unroll
-    for (int k = 0; k < T::Q; ++k) {
-      uint32_t fw = fr[k];
-      if (k == 0 && a == 0) fw &= 0xFFFFFF00u;
-      sum = __dp4a(fw, gr[4 * k], sum);
-    }
-    if (a != cr - 1) sum = __dp4a(fr[T::Q] & 0xFFu, gr[4 * T::Q], sum);
+    uint32_t fw = Fw[y * T::NGP + T::GS * ix + k];
+    if (k == 0 && a == 0) fw &= 0xFFFFFF00u;
+    if (k == T::Q) fw = a != cr - 1 ? fw & 0xFFu : 0u;
+    sum = __dp4a(fw, Gw[(y + b) * pitch + ix * STEP + a + 4 * k], sum);
   }
   return __reduce_add_sync(0xffffffffu, sum);
 }
@@ -731,21 +769,29 @@ __device__ __forceinline__ void tile_hsum(const unsigned (&acc)[TileShape<STEP, 
 }
 
 template <int STEP, int WS, int TSX>
-__global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) {
+__global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs A) {
   using T = TileShape<STEP, WS, TSX>;
   constexpr int TW = T::TW, NG = T::NG, NE = T::NE, NGP = T::NGP, QB = T::QB;
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t *Fw = reinterpret_cast<uint32_t *>(smem);
   uint32_t *Gw = reinterpret_cast<uint32_t *>(smem + A.off_g);
+  int *tis = reinterpret_cast<int *>(smem + A.off_ti);
+  int *tis2 = tis + A.qxn * A.qyn;
+  float *tii = reinterpret_cast<float *>(tis2 + A.qxn * A.qyn);
+  uint2 *ra = reinterpret_cast<uint2 *>(smem + A.off_ra);
+  uint2 *rb = reinterpret_cast<uint2 *>(smem + A.off_rb);
+  uint2 *rc = reinterpret_cast<uint2 *>(smem + A.off_rc);
   TileSub *sub = reinterpret_cast<TileSub *>(smem + A.off_sub);
   uint2 *cand = reinterpret_cast<uint2 *>(smem + A.off_cand);
-  uint8_t *tmp = smem + A.off_cand;  // g bytes while staging (the candidates come later)
+  uint8_t *tmp = smem + A.off_ti;  // g bytes while staging (the window tables come later)
   const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nth >> 5;
   const int TSY = A.tsy, NS = TSX * TSY, RYf = (TSY - 1) * STEP + TW;
-  const int cr = A.cr, cc = A.cc, pitch = A.pitch;
+  const int cr = A.cr, cc = A.cc, pitch = A.pitch, qxn = A.qxn, qyn = A.qyn;
   const int tx0 = blockIdx.x * TSX, ty0 = blockIdx.y * TSY;       // first grid point
   const int px0 = A.px1 + tx0 * STEP, py0 = A.py1 + ty0 * STEP;   // its 0-based corner
   const int gx0 = px0 - A.sx - 1, gy0 = py0 - A.sy - 1;           // corner of the g tile
+  const TileMem M{Fw, Gw, tis, tis2, tii, ra, rb, rc, pitch, qxn, qyn, TSY};
+  unsigned *ringc = A.ringc + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * NS * A.nring;
 
   // ---- stage f (4 pixels a word) and g (word m of a row = bytes m .. m+3)
   for (int i = tid; i < RYf * NGP; i += nth) {
@@ -771,6 +817,68 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
     const int r = i / pitch, m = i - r * pitch;
     const uint32_t *tw = reinterpret_cast<const uint32_t *>(tmp + r * A.pb);
     Gw[i] = __funnelshift_r(tw[m >> 2], tw[(m >> 2) + 1], 8 * (m & 3));
+  }
+  __syncthreads();
+  // ---- full windows at every tile position (positions beyond the image: 0)
+  const int tabw = A.W - TW, tabh = A.H - TW;
+  for (int i = tid; i < qxn * qyn; i += nth) {
+    const int qyi = i / qxn, qxi = i - qyi * qxn;
+    const int xx = gx0 + qxi, yy = gy0 + qyi;
+    uint4 e = make_uint4(0, 0, 0, 0);
+    if (xx <= tabw && yy <= tabh) e = A.tab[(long long)yy * A.W + xx];
+    tis[i] = (int)e.x;
+    tis2[i] = (int)e.y;
+    tii[i] = __uint_as_float(e.z);
+  }
+  __syncthreads();
+  // ---- the outer ring's windows: full window minus a column and/or a row
+  const uint8_t *gb = reinterpret_cast<const uint8_t *>(Gw);  // byte 0 of word c = g(c)
+  auto colsum = [&](int col, int r0, unsigned &s1, unsigned &s2) {
+    s1 = s2 = 0;
+    for (int r = r0; r < r0 + TW; ++r) {
+      const unsigned v = gb[(r * pitch + col) * 4];
+      s1 += v;
+      s2 += v * v;
+    }
+  };
+  auto rowsum = [&](int row, int c0, unsigned &s1, unsigned &s2) {
+    const uint32_t *w = Gw + row * pitch + c0;
+    s1 = s2 = 0;
+#pragma unroll
+    for (int k = 0; k < T::Q; ++k) {
+      s1 = __dp4a(w[4 * k], 0x01010101u, s1);
+      s2 = __dp4a(w[4 * k], w[4 * k], s2);
+    }
+    const unsigned v = w[4 * T::Q] & 0xFFu;
+    s1 += v;
+    s2 += v * v;
+  };
+  for (int i = tid; i < 2 * TSX * qyn; i += nth) {
+    const int side = i / (TSX * qyn), r = i - side * TSX * qyn, ix = r / qyn, qyi = r - ix * qyn;
+    const int qxi = ix * STEP + (side ? cr - 1 : 0), col = side ? qxi + TW - 1 : qxi;
+    unsigned c1, c2;
+    colsum(col, qyi, c1, c2);
+    const int j = qyi * qxn + qxi;
+    ra[i] = make_uint2((unsigned)tis[j] - c1, (unsigned)tis2[j] - c2);
+  }
+  for (int i = tid; i < 2 * TSY * qxn; i += nth) {
+    const int side = i / (TSY * qxn), r = i - side * TSY * qxn, iy = r / qxn, qxi = r - iy * qxn;
+    const int qyi = iy * STEP + (side ? cc - 1 : 0), row = side ? qyi + TW - 1 : qyi;
+    unsigned r1, r2;
+    rowsum(row, qxi, r1, r2);
+    const int j = qyi * qxn + qxi;
+    rb[i] = make_uint2((unsigned)tis[j] - r1, (unsigned)tis2[j] - r2);
+  }
+  for (int i = tid; i < NS * 4; i += nth) {
+    const int s = i >> 2, as = i & 1, bs = (i >> 1) & 1, ix = s % TSX, iy = s / TSX;
+    const int qxi = ix * STEP + (as ? cr - 1 : 0), qyi = iy * STEP + (bs ? cc - 1 : 0);
+    const int col = as ? qxi + TW - 1 : qxi, row = bs ? qyi + TW - 1 : qyi;
+    unsigned c1, c2, r1, r2;
+    colsum(col, qyi, c1, c2);
+    rowsum(row, qxi, r1, r2);
+    const unsigned v = gb[(row * pitch + col) * 4];
+    const int j = qyi * qxn + qxi;
+    rc[i] = make_uint2((unsigned)tis[j] - c1 - r1 + v, (unsigned)tis2[j] - c2 - r2 + v * v);
   }
   // ---- template sums of every point (a warp per point, lanes over rows)
   for (int s = wid; s < NS; s += nw) {
@@ -812,11 +920,26 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
   __syncthreads();
   const double mu = *A.mu;
 
-  // ---- every shift of the cropped map, ndy map columns per batch
+  // ---- every shift of the cropped map, ndy map columns per batch; the two
+  // ring shifts (a = 0, cr-1) of each column take the first lanes
   for (int bt = 0; bt < A.nbatch; ++bt) {
-    int a = tid % cr, b = bt * A.ndy + tid / cr;
-    const bool active = tid < cr * A.ndy && b < cc;
-    if (!active) a = b = 0;  // in-bounds work whose results are dropped
+    const int b0 = bt * A.ndy, nbr = min(A.ndy, cc - b0);
+    int a, b;
+    bool active;
+    if (tid < 2 * nbr) {
+      a = (tid & 1) ? cr - 1 : 0;
+      b = b0 + (tid >> 1);
+      active = true;
+    } else {
+      const int u = tid - 2 * nbr;
+      a = 1 + u % (cr - 2);
+      b = b0 + u / (cr - 2);
+      active = b < b0 + nbr;
+      if (!active) {  // in-bounds work whose results are dropped
+        a = 1;
+        b = b0;
+      }
+    }
     const unsigned cF = (a == 0), cL = (a != cr - 1), cRF = (b == 0), cRL = (b != cc - 1);
     const bool ring = (a == 0) || (a == cr - 1) || (b == 0) || (b == cc - 1);
     const uint32_t *gbase = Gw + b * pitch + a;
@@ -845,39 +968,31 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
             rlo[ix] = -INFINITY;
             rhi[ix] = -INFINITY;
             if (active && P.state == 0) {
-              const int px = px0 + ix * STEP, py = py0 + iy * STEP;
-              const int qx = px + a - 1 - A.sx, qy = py + b - 1 - A.sy;
-              float r;
               if (!ring) {
-                const uint2 e = A.tab[(long long)qy * A.W + qx];
-                const long long num = A.mn * (long long)C - (long long)P.st * (int)e.x;
-                r = (float)num * P.invT * __uint_as_float(e.y);
+                const int i = (iy * STEP + b) * qxn + ix * STEP + a;
+                const long long num = A.mn * (long long)C - (long long)P.st * tis[i];
+                const float r = (float)num * P.invT * tii[i];
+                rlo[ix] = r - kTileEps;
+                rhi[ix] = r + kTileEps;
               } else {
-                const long long W1 = A.W + 1;
-                const int x0 = qx + (a == 0), x1 = qx + TW - (a == cr - 1);
-                const int y0 = qy + (b == 0), y1 = qy + TW - (b == cc - 1);
-                const long long sd = sat_rect(A.sat1, W1, x0, x1, y0, y1);
-                const long long sd2 = sat_rect(A.sat2, W1, x0, x1, y0, y1);
-                long long st_out, n_out;
-                tile_pad(P, a, b, cr, cc, TW, &st_out, &n_out);
-                double num, den;
-                ncc_parts(A.mn, P.st, (long long)C, sd, sd2, st_out, n_out, mu, &num, &den);
-                r = den > 0.0 ? (float)num * P.invT * rsqrtf((float)den) : 0.f;
+                ringc[(iy * TSX + ix) * A.nring + ring_index(a, b, cr, cc)] = C;
               }
-              rlo[ix] = r - kTileEps;
-              rhi[ix] = r + kTileEps;
             }
           }
+          // raise the bound by this warp's maximum, then keep what can still
+          // reach it; no barrier: a bound read before other warps raised it
+          // only keeps a few more entries (it never exceeds the final one)
 #pragma unroll
           for (int ix = 0; ix < TSX; ++ix) {
             const unsigned kmax = __reduce_max_sync(0xffffffffu, fkey(rlo[ix]));
             if (lane == 0) atomicMax(&sub[iy * TSX + ix].lb, kmax);
           }
-          __syncthreads();
+          __syncwarp();
 #pragma unroll
           for (int ix = 0; ix < TSX; ++ix) {
             const int s = iy * TSX + ix;
-            if (rhi[ix] != -INFINITY && fkey(rhi[ix]) >= sub[s].lb) {
+            const unsigned lbs = *reinterpret_cast<volatile unsigned *>(&sub[s].lb);
+            if (rhi[ix] != -INFINITY && fkey(rhi[ix]) >= lbs) {
               const int pos = atomicAdd(&sub[s].cnt, 1);
               if (pos < kTileCap) cand[s * kTileCap + pos] = make_uint2(b * cr + a, win[sl][ix]);
             }
@@ -914,8 +1029,7 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
     const int ix = s % TSX, iy = s / TSX;
     const int gix = tx0 + ix, giy = ty0 + iy;
     const long long out_idx = (long long)giy + (long long)gix * A.ny;
-    const int px = px0 + ix * STEP, py = py0 + iy * STEP;
-    const int ii = px + 1, jj = py + 1;  // 1-based
+    const int ii = px0 + ix * STEP + 1, jj = py0 + iy * STEP + 1;  // 1-based
     if (P.state == 1) {
       if (lane == 0) {
         const double nan = __longlong_as_double(0x7ff8000000000000ll);
@@ -932,10 +1046,24 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
     double best = -INFINITY;
     int bi = 0x7fffffff;
     if (!hand_back) {
+      for (int k = lane; k < A.nring; k += 32) {
+        int ra_, rb_;
+        ring_pos(k, cr, cc, &ra_, &rb_);
+        const double r =
+            tile_exact<STEP>(A, M, P, ix, iy, TW, ra_, rb_, ringc[s * A.nring + k], mu);
+        const int idx = rb_ * cr + ra_;
+        if (r > best || (r == best && idx < bi)) {
+          best = r;
+          bi = idx;
+        }
+      }
       if (lane < n) {
         const uint2 e = cand[s * kTileCap + lane];
-        bi = (int)e.x;
-        best = tile_exact(A, P, px, py, TW, bi % cr, bi / cr, e.y, mu);
+        const double r = tile_exact<STEP>(A, M, P, ix, iy, TW, e.x % cr, e.x / cr, e.y, mu);
+        if (r > best || (r == best && (int)e.x < bi)) {
+          best = r;
+          bi = (int)e.x;
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -946,8 +1074,8 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
           bi = oi;
         }
       }
-      // the bound must hold for the kept maximum (it can only fail where an
-      // estimate met ncc_combine's clamp of |r| > 1)
+      // the bound must hold for the evaluated maximum (it can only fail where
+      // an estimate met ncc_combine's clamp of |r| > 1)
       hand_back = !(best >= (double)fkey_inv(P.lb));
     }
     if (hand_back) {
@@ -973,7 +1101,7 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
         }
       }
       double r = best;
-      if (lane < 9 && lane != 4) r = tile_exact(A, P, px, py, TW, my_a, my_b, my_acc, mu);
+      if (lane < 9 && lane != 4) r = tile_exact<STEP>(A, M, P, ix, iy, TW, my_a, my_b, my_acc, mu);
       double u9[9];
 #pragma unroll
       for (int k = 0; k < 9; ++k) u9[k] = __shfl_sync(0xffffffffu, r, k);
@@ -989,169 +1117,146 @@ __global__ void __launch_bounds__(kTileThreads) k_search_tile(const TileArgs A) 
   }
 }
 
-// ---- summed-area tables of g and g^2 (wrapping 32-bit), (W+1) x (H+1)
-// rows: a block per image row, 8 pixels a thread, block scan
-__global__ void __launch_bounds__(256) k_sat_rows_u8(const uint8_t *__restrict__ g, int W, int H,
-                                                     unsigned *__restrict__ s1,
-                                                     unsigned *__restrict__ s2) {
-  const int y = blockIdx.x;
-  const long long W1 = W + 1;
-  unsigned *r1 = s1 + (y + 1) * W1, *r2 = s2 + (y + 1) * W1;
+// ---- per-image table of the full tw x tw windows of g: (sum, sum of
+// squares, 1/sqrt(mn sum^2 - sum^2) or 0) at every top-left corner in
+// [x0, x1] x [y0, y1].  A block per kTabX x kTabY corners: the bytes in
+// shared memory, vertical sums per column, a prefix sum per row.
+constexpr int kTabX = 128, kTabY = 32;
+
+__global__ void __launch_bounds__(256) k_box_tab(const uint8_t *__restrict__ g, int W, int H,
+                                                 int tw, long long mn, int x0, int x1, int y0,
+                                                 int y1, uint4 *__restrict__ tab) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int bx = x0 + blockIdx.x * kTabX, by = y0 + blockIdx.y * kTabY;
+  const int nc = kTabX + tw - 1, nr = kTabY + tw - 1, np = nc + 1;
+  uint8_t *G = sm;
+  unsigned *P1 = reinterpret_cast<unsigned *>(sm + align16((size_t)nr * nc));
+  unsigned *P2 = P1 + kTabY * np;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  __shared__ unsigned w1[8], w2[8];
-  if (y == 0)
-    for (int x = tid; x <= W; x += 256) s1[x] = s2[x] = 0u;
-  if (tid == 0) r1[0] = r2[0] = 0u;
-  unsigned carry1 = 0, carry2 = 0;
-  const uint8_t *row = g + (long long)y * W;
-  for (int x0 = 0; x0 < W; x0 += 256 * 8) {
-    const int xb = x0 + 8 * tid;
-    unsigned p1[8], p2[8], t1 = 0, t2 = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const unsigned v = xb + j < W ? row[xb + j] : 0u;
-      t1 += v;
-      t2 += v * v;
-      p1[j] = t1;
-      p2[j] = t2;
+  for (int i = tid; i < nr * nc; i += 256) {
+    const int r = i / nc, c = i - r * nc, yy = by + r, xx = bx + c;
+    G[i] = (yy < H && xx < W) ? g[(long long)yy * W + xx] : (uint8_t)0;
+  }
+  __syncthreads();
+  for (int c = tid; c < nc; c += 256) {  // vertical sums, column c, rows oy .. oy+tw-1
+    unsigned s1 = 0, s2 = 0;
+    for (int r = 0; r < tw; ++r) {
+      const unsigned v = G[r * nc + c];
+      s1 += v;
+      s2 += v * v;
     }
-    unsigned i1 = t1, i2 = t2;  // inclusive scan of the thread totals
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned u1 = __shfl_up_sync(0xffffffffu, i1, o), u2 = __shfl_up_sync(0xffffffffu, i2, o);
-      if (lane >= o) {
-        i1 += u1;
-        i2 += u2;
+    for (int oy = 0; oy < kTabY; ++oy) {
+      P1[oy * np + c + 1] = s1;
+      P2[oy * np + c + 1] = s2;
+      if (oy + 1 < kTabY) {
+        const unsigned vo = G[oy * nc + c], vi = G[(oy + tw) * nc + c];
+        s1 += vi - vo;
+        s2 += vi * vi - vo * vo;
       }
     }
-    if (lane == 31) {
-      w1[wid] = i1;
-      w2[wid] = i2;
-    }
-    __syncthreads();
-    unsigned b1 = carry1 + i1 - t1, b2 = carry2 + i2 - t2;
-    for (int k = 0; k < wid; ++k) {
-      b1 += w1[k];
-      b2 += w2[k];
-    }
+  }
+  __syncthreads();
+  for (int oy = wid; oy < kTabY; oy += 8) {  // prefix sums along each row, a warp a row
+    unsigned *q1 = P1 + oy * np, *q2 = P2 + oy * np;
+    if (lane == 0) q1[0] = q2[0] = 0;
+    unsigned c1 = 0, c2 = 0;
+    for (int c0 = 1; c0 <= nc; c0 += 32) {
+      const int c = c0 + lane;
+      unsigned v1 = c <= nc ? q1[c] : 0u, v2 = c <= nc ? q2[c] : 0u;
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-      if (xb + j < W) {
-        r1[xb + j + 1] = b1 + p1[j];
-        r2[xb + j + 1] = b2 + p2[j];
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t1 = __shfl_up_sync(0xffffffffu, v1, o), t2 = __shfl_up_sync(0xffffffffu, v2, o);
+        if (lane >= o) {
+          v1 += t1;
+          v2 += t2;
+        }
       }
-    for (int k = 0; k < 8; ++k) {
-      carry1 += w1[k];
-      carry2 += w2[k];
+      if (c <= nc) {
+        q1[c] = c1 + v1;
+        q2[c] = c2 + v2;
+      }
+      c1 += __shfl_sync(0xffffffffu, v1, 31);
+      c2 += __shfl_sync(0xffffffffu, v2, 31);
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  for (int i = tid; i < kTabX * kTabY; i += 256) {
+    const int oy = i / kTabX, ox = i - oy * kTabX, x = bx + ox, y = by + oy;
+    if (x > x1 || y > y1) continue;
+    const unsigned s1 = P1[oy * np + ox + tw] - P1[oy * np + ox];
+    const unsigned s2 = P2[oy * np + ox + tw] - P2[oy * np + ox];
+    const long long c0 = mn * (long long)s2 - (long long)s1 * s1;
+    tab[(long long)y * W + x] =
+        make_uint4(s1, s2, c0 > 0 ? __float_as_uint(rsqrtf((float)c0)) : 0u, 0u);
   }
 }
-
-constexpr int kSatRows = 64;  // rows per column chunk
-
-// columns: in-place prefix within chunks of kSatRows table rows, chunk totals
-__global__ void k_sat_cols_u8(unsigned *__restrict__ s1, unsigned *__restrict__ s2, int W, int H,
-                              unsigned *__restrict__ tot) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, ch = blockIdx.y;
-  const long long W1 = W + 1;
-  if (x > W) return;
-  const int y0 = 1 + ch * kSatRows, y1 = min(H + 1, y0 + kSatRows);
-  unsigned a1 = 0, a2 = 0;
-  for (int y = y0; y < y1; ++y) {
-    a1 += s1[y * W1 + x];
-    a2 += s2[y * W1 + x];
-    s1[y * W1 + x] = a1;
-    s2[y * W1 + x] = a2;
-  }
-  tot[2 * (ch * W1 + x)] = a1;
-  tot[2 * (ch * W1 + x) + 1] = a2;
-}
-
-// box table of the full windows with top-left corners [x0, x1] x [y0, y1]
-__global__ void k_box_tab(const unsigned *__restrict__ s1, const unsigned *__restrict__ s2, int W,
-                          int tw, long long mn, int x0, int x1, int y0, uint2 *__restrict__ tab) {
-  const int x = x0 + blockIdx.x * blockDim.x + threadIdx.x, y = y0 + blockIdx.y;
-  if (x > x1) return;
-  const long long W1 = W + 1;
-  const long long sd = sat_rect(s1, W1, x, x + tw, y, y + tw);
-  const long long sd2 = sat_rect(s2, W1, x, x + tw, y, y + tw);
-  const long long c0 = mn * sd2 - sd * sd;
-  tab[(long long)y * W + x] =
-      make_uint2((unsigned)sd, c0 > 0 ? __float_as_uint(rsqrtf((float)c0)) : 0u);
-}
-
-// add the totals of the chunks above to every chunk but the first
-__global__ void k_sat_fix_u8(unsigned *__restrict__ s1, unsigned *__restrict__ s2, int W, int H,
-                             const unsigned *__restrict__ tot) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, ch = blockIdx.y + 1;
-  const long long W1 = W + 1;
-  if (x > W) return;
-  unsigned o1 = 0, o2 = 0;
-  for (int c = 0; c < ch; ++c) {
-    o1 += tot[2 * (c * W1 + x)];
-    o2 += tot[2 * (c * W1 + x) + 1];
-  }
-  const int y0 = 1 + ch * kSatRows, y1 = min(H + 1, y0 + kSatRows);
-  for (int y = y0; y < y1; ++y) {
-    s1[y * W1 + x] += o1;
-    s2[y * W1 + x] += o2;
-  }
-}
-
-constexpr int kTileTSX = 8;  // grid points per tile row
 
 struct TilePlan {
-  int tsy = 0, ndy = 0, nbatch = 0, pitch = 0, rows_g = 0, pb = 0, threads = 0;
-  int off_g = 0, off_sub = 0, off_cand = 0, total = 0;
+  int tsy = 0, ndy = 0, nbatch = 0, pitch = 0, rows_g = 0, pb = 0, qxn = 0, qyn = 0;
+  int off_g = 0, off_ti = 0, off_ra = 0, off_rb = 0, off_rc = 0, off_sub = 0, off_cand = 0;
+  int total = 0;
 };
 
-// tile rows, thread batches and the shared-memory layout; the largest tile
-// (up to 8 point rows) that lets two CTAs share an SM, else one
+// tile rows, thread batches and the shared-memory layout: the largest tile
+// (up to 8 point rows) that fits one CTA per SM
 template <int STEP, int WS>
 bool tile_plan(int sx, int sy, TilePlan &P) {
   using T = TileShape<STEP, WS, kTileTSX>;
   const int cr = 2 * sx + 3, cc = 2 * sy + 3;
   if (cr > kTileThreads) return false;
-  P.ndy = std::min(cc, kTileThreads / cr);
-  P.nbatch = (cc + P.ndy - 1) / P.ndy;
-  P.threads = (cr * P.ndy + 31) / 32 * 32;
-  // odd rows of a warp continue the bank sequence of the row before
+  P.nbatch = (cc + kTileThreads / cr - 1) / (kTileThreads / cr);
+  P.ndy = (cc + P.nbatch - 1) / P.nbatch;
+  // the interior lanes of a warp continue the bank sequence across rows
   const int minp = cr + 4 * T::NG - 4;
-  P.pitch = minp + (((cr - minp) % 32) + 32) % 32;
+  P.pitch = minp + (((cr - 2 - minp) % 32) + 32) % 32;
   P.pb = (int)align16(4 * ((P.pitch - 1) / 4 + 2));
-  for (const size_t limit : {(size_t)113 * 1024, (size_t)227 * 1024})
-    for (int tsy = 8; tsy >= 1; --tsy) {
-      const int ryf = (tsy - 1) * STEP + T::TW, rows_g = ryf + cc - 1, ns = kTileTSX * tsy;
-      size_t o = align16((size_t)ryf * T::NGP * 4);
-      const size_t og = o;
-      o += align16((size_t)rows_g * P.pitch * 4);
-      const size_t os = o;
-      o += align16((size_t)ns * sizeof(TileSub));
-      const size_t oc = o;
-      o += align16(std::max((size_t)ns * kTileCap * sizeof(uint2), (size_t)rows_g * P.pb));
-      if (o <= limit) {
-        P.tsy = tsy;
-        P.rows_g = rows_g;
-        P.off_g = (int)og;
-        P.off_sub = (int)os;
-        P.off_cand = (int)oc;
-        P.total = (int)o;
-        return true;
-      }
+  P.qxn = (kTileTSX - 1) * STEP + cr;
+  for (int tsy = 8; tsy >= 1; --tsy) {
+    const int ryf = (tsy - 1) * STEP + T::TW, rows_g = ryf + cc - 1, ns = kTileTSX * tsy;
+    const int qyn = (tsy - 1) * STEP + cc;
+    size_t o = align16((size_t)ryf * T::NGP * 4);
+    const size_t og = o;
+    o += align16((size_t)rows_g * P.pitch * 4);
+    const size_t oti = o;
+    o += align16(std::max((size_t)3 * P.qxn * qyn * 4, (size_t)rows_g * P.pb));
+    const size_t ora = o;
+    o += align16((size_t)2 * kTileTSX * qyn * sizeof(uint2));
+    const size_t orb = o;
+    o += align16((size_t)2 * tsy * P.qxn * sizeof(uint2));
+    const size_t orc = o;
+    o += align16((size_t)ns * 4 * sizeof(uint2));
+    const size_t os = o;
+    o += align16((size_t)ns * sizeof(TileSub));
+    const size_t oc = o;
+    o += align16((size_t)ns * kTileCap * sizeof(uint2));
+    if (o <= (size_t)227 * 1024) {
+      P.tsy = tsy;
+      P.rows_g = rows_g;
+      P.qyn = qyn;
+      P.off_g = (int)og;
+      P.off_ti = (int)oti;
+      P.off_ra = (int)ora;
+      P.off_rb = (int)orb;
+      P.off_rc = (int)orc;
+      P.off_sub = (int)os;
+      P.off_cand = (int)oc;
+      P.total = (int)o;
+      return true;
     }
+  }
   return false;
 }
 
 template <int STEP, int WS>
 int tile_launch(TileArgs A, const TilePlan &P, cudaStream_t st) {
   A.tsy = P.tsy; A.ndy = P.ndy; A.nbatch = P.nbatch; A.pitch = P.pitch;
-  A.rows_g = P.rows_g; A.pb = P.pb;
-  A.off_g = P.off_g; A.off_sub = P.off_sub; A.off_cand = P.off_cand;
+  A.rows_g = P.rows_g; A.pb = P.pb; A.qxn = P.qxn; A.qyn = P.qyn;
+  A.off_g = P.off_g; A.off_ti = P.off_ti; A.off_ra = P.off_ra; A.off_rb = P.off_rb;
+  A.off_rc = P.off_rc; A.off_sub = P.off_sub; A.off_cand = P.off_cand;
   auto kern = k_search_tile<STEP, WS, kTileTSX>;
   ALDIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, P.total));
   const dim3 grid((A.nx + kTileTSX - 1) / kTileTSX, (A.ny + P.tsy - 1) / P.tsy);
-  kern<<<grid, P.threads, P.total, st>>>(A);
+  kern<<<grid, kTileThreads, P.total, st>>>(A);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
@@ -1175,29 +1280,16 @@ int tile_dispatch(const TileArgs &A, const TilePlan &P, int step, cudaStream_t s
   return E_ARG;
 }
 
-struct TileBufs {
-  unsigned *sat1, *sat2, *tot;
-  uint2 *tab;
-  int *fb;
-  size_t bytes;
-};
-TileBufs tile_bufs(void *base, int W, int H, long long npts) {
-  const size_t W1 = W + 1, H1 = H + 1, nch = (H + kSatRows - 1) / kSatRows;
-  TileBufs b;
-  size_t o = 0;
-  const size_t o_s1 = o; o += align16(W1 * H1 * 4);
-  const size_t o_s2 = o; o += align16(W1 * H1 * 4);
-  const size_t o_t = o; o += align16(2 * W1 * nch * 4);
-  const size_t o_tab = o; o += align16((size_t)W * H * 8);
-  const size_t o_fb = o; o += align16((size_t)(npts + 1) * 4);
-  char *p = (char *)base;
-  b.sat1 = (unsigned *)(p + o_s1);
-  b.sat2 = (unsigned *)(p + o_s2);
-  b.tot = (unsigned *)(p + o_t);
-  b.tab = (uint2 *)(p + o_tab);
-  b.fb = (int *)(p + o_fb);
-  b.bytes = o;
-  return b;
+// work slab: the window table (16 B per pixel), the hand-back list and the
+// ring sums (tiles hold at most 8 x 8 points, so (nx + 7) (ny + 7) bounds them)
+size_t tile_ring_bytes(int nx, int ny, const int search[2]) {
+  const long long nring = 2ll * (2 * search[0] + 3 + 2 * search[1] + 3) - 4;
+  return (size_t)(nx + 7) * (ny + 7) * nring * sizeof(unsigned);
+}
+size_t tile_bytes(int W, int H, int nx, int ny, const int search[2]) {
+  return align16((size_t)W * H * sizeof(uint4)) +
+         align16((size_t)((long long)nx * ny + 1) * sizeof(int)) +
+         align16(tile_ring_bytes(nx, ny, search));
 }
 
 // tiled 8-bit search; false in *used when the geometry has no tiled kernel
@@ -1210,31 +1302,35 @@ int tile_search(const uint8_t *f, const uint8_t *g, const SearchGeom &G, SearchW
   const int px1 = G.gx1 - 1, py1 = G.gy1 - 1;
   if (px1 - G.sx - 1 < 0 || py1 - G.sy - 1 < 0) return OK;
   const long long npts = (long long)G.nx * G.ny;
-  int rc = search_work_ensure(sw, G.W, G.H, npts);
+  const int srch[2] = {G.sx, G.sy};
+  int rc = search_work_ensure(sw, G.W, G.H, G.nx, G.ny, srch);
   if (rc) return rc;
-  const TileBufs B = tile_bufs(sw.buf.p, G.W, G.H, npts);
-  const int W1 = G.W + 1, nch = (G.H + kSatRows - 1) / kSatRows;
+  char *wb = sw.buf.as<char>();
+  uint4 *tab = reinterpret_cast<uint4 *>(wb);
+  wb += align16((size_t)G.W * G.H * sizeof(uint4));
+  int *fb = reinterpret_cast<int *>(wb);
+  wb += align16((size_t)(npts + 1) * sizeof(int));
+  unsigned *ringc = reinterpret_cast<unsigned *>(wb);
   const long long mn = (long long)G.tw * G.tw;
-  k_sat_rows_u8<<<G.H, 256, 0, st>>>(g, G.W, G.H, B.sat1, B.sat2);
-  k_sat_cols_u8<<<dim3((W1 + 255) / 256, nch), 256, 0, st>>>(B.sat1, B.sat2, G.W, G.H, B.tot);
-  if (nch > 1)
-    k_sat_fix_u8<<<dim3((W1 + 255) / 256, nch - 1), 256, 0, st>>>(B.sat1, B.sat2, G.W, G.H,
-                                                                   B.tot);
-  // full windows of the interior entries: corners px1 - sx .. last + sx
-  const int x0 = px1 - G.sx, x1 = px1 + (G.nx - 1) * G.step + G.sx;
-  const int y0 = py1 - G.sy, y1 = py1 + (G.ny - 1) * G.step + G.sy;
-  k_box_tab<<<dim3((x1 - x0 + 256) / 256, y1 - y0 + 1), 256, 0, st>>>(B.sat1, B.sat2, G.W, G.tw,
-                                                                      mn, x0, x1, y0, B.tab);
-  ALDIC_CUDA(cudaMemsetAsync(B.fb, 0, sizeof(int), st));
+  // full windows of every shift of every point (outer ring included)
+  const int x0 = px1 - G.sx - 1, x1 = px1 + (G.nx - 1) * G.step + G.sx + 1;
+  const int y0 = py1 - G.sy - 1, y1 = py1 + (G.ny - 1) * G.step + G.sy + 1;
+  const size_t smt = align16((size_t)(kTabY + G.tw - 1) * (kTabX + G.tw - 1)) +
+                     2 * sizeof(unsigned) * kTabY * (kTabX + G.tw);
+  ALDIC_CUDA(cudaFuncSetAttribute(k_box_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt));
+  k_box_tab<<<dim3((x1 - x0 + kTabX) / kTabX, (y1 - y0 + kTabY) / kTabY), 256, smt, st>>>(
+      g, G.W, G.H, G.tw, mn, x0, x1, y0, y1, tab);
+  ALDIC_CUDA(cudaMemsetAsync(fb, 0, sizeof(int), st));
   TileArgs A{};
-  A.f = f; A.g = g; A.sat1 = B.sat1; A.sat2 = B.sat2; A.tab = B.tab; A.mu = G.mu;
-  A.ox = x; A.oy = y; A.ou = u; A.ov = v; A.occ = cc; A.fb = B.fb;
+  A.f = f; A.g = g; A.tab = tab; A.mu = G.mu;
+  A.ox = x; A.oy = y; A.ou = u; A.ov = v; A.occ = cc; A.fb = fb; A.ringc = ringc;
   A.W = G.W; A.H = G.H; A.px1 = px1; A.py1 = py1; A.nx = G.nx; A.ny = G.ny; A.w = G.w;
   A.sx = G.sx; A.sy = G.sy; A.cr = G.cr; A.cc = G.cc; A.mn = mn;
+  A.nring = 2 * (G.cr + G.cc) - 4;
   if ((rc = tile_dispatch(A, P, G.step, st))) return rc;
   // the points handed back: per-point kernel over the device-side list
   const int nb = (int)std::min<long long>(npts, 296);
-  k_search_u8_list<<<nb, threads_pt, smem_pt, st>>>(f, g, G, B.fb, x, y, u, v, cc);
+  k_search_u8_list<<<nb, threads_pt, smem_pt, st>>>(f, g, G, fb, x, y, u, v, cc);
   ALDIC_CUDA(cudaGetLastError());
   *used = true;
   return OK;
@@ -1426,8 +1522,8 @@ int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsiz
   return OK;
 }
 
-int search_work_ensure(SearchWork &w, int W, int H, long long npts) {
-  return w.buf.ensure(tile_bufs(nullptr, W, H, npts).bytes);
+int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2]) {
+  return w.buf.ensure(tile_bytes(W, H, nx, ny, search));
 }
 
 int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,

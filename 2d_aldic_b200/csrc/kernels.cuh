@@ -21,13 +21,13 @@ int interp_f32(const float *F, long long M, long long N, long long P, const floa
                const float *Y, long long n, float *Z, cudaStream_t st);
 
 // ---- k_search.cu
-// work of the tiled 8-bit search: summed-area tables and the window table of
-// the deformed image, the list of points handed to the per-point kernel
+// work of the tiled 8-bit search: the window table of the deformed image, the
+// list of points handed to the per-point kernel and the outer-ring sums
 struct SearchWork {
   DevBuf buf;
   void release() { buf.release(); }
 };
-int search_work_ensure(SearchWork &w, int W, int H, long long npts);
+int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2]);
 int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsize, int step,
                 const int search[2], int *nx, int *ny, int *gx1, int *gy1);
 int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,
