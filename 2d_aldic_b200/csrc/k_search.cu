@@ -575,50 +575,46 @@ __global__ void __launch_bounds__(512) k_search_u8_list(const uint8_t *__restric
 // ring of the map) left out exactly.  All sums are exact 32-bit integers, the
 // same ones the per-point kernel forms.
 //
-// Peak search without an FP64 division per interior entry: each interior
-// entry's NCC is first estimated in FP32 from the exact integers (the window
-// sum and 1/sqrt of the window variance term), |estimate - FP64 value| <
-// kTileEps.  A per-point lower bound lb on the interior maximum (max of
-// estimate - eps) grows as the tile's shifts are processed; entries with
-// estimate + eps >= lb are kept with their exact correlation sum.  The exact
-// sums of the map's outer ring (2 (cr + cc) - 4 entries a point, whose
-// padded windows need the FP64 form) go to a scratch array.  At the end a
-// warp a point evaluates its ring and its kept entries with ncc_combine, and
-// the 3 x 3 neighbourhood of the winner for findpeak.  Every entry that can
-// be the maximum (or tie with it) is evaluated, so argmax and findpeak's fit
-// are those of the full map.  A point with more than kTileCap kept entries
-// (near-ties, flat search regions), or whose evaluated maximum falls below
-// lb, is handed to the per-point kernel.
+// The exact sums of every shift go to a per-point map in global memory (a
+// tile's maps, 64 points x (2s+3)^2 words, stay in L2 while the tile runs).
+// Peak search without an FP64 division per entry: at the end a warp a point
+// estimates each entry's NCC in FP32 from the exact integers (interior
+// entries from the window sum and 1/sqrt of the window variance term, the
+// outer ring from ncc_combine's own FP64 numerator and denominator), with
+// |estimate - ncc_combine| < kTileEps.  A running bound T = max(estimate -
+// eps) grows over the map; entries with estimate + eps >= T are queued and,
+// once T is final, those still within reach are evaluated with ncc_combine
+// (lanes in parallel), as is the 3 x 3 neighbourhood of the winner for
+// findpeak.  Every entry that can be the maximum (or tie with it) is
+// evaluated, so argmax and findpeak's fit are those of the full map.  A point
+// with more than kTileQueue queued entries (near-ties, flat search regions),
+// or whose evaluated maximum falls below T, is handed to the per-point kernel.
 //
 // The window sums of every shift of the tile live in shared memory: the
 // full windows (sum, sum of squares, 1/sqrt(C0)) copied from a per-image
 // table, the windows of the outer ring (one column and/or row left out)
 // formed from the staged g.
-constexpr int kTileCap = 24;
 constexpr float kTileEps = 1e-5f;
 constexpr int kTileThreads = 512;
-constexpr int kTileTSX = 8;  // grid points per tile row
+constexpr int kTileQueue = 64;  // queued entries a point (a warp's shared-memory queue)
+constexpr int kTileTSX = 8;     // grid points per tile row
 
 struct TileSub {
   int st, st2, cs0, csL, rs0, rsL, c00, cL0, c0L, cLL;
   float invT;     // 1 / sqrt(mn st2 - st^2)
-  unsigned lb;    // ordered key of the lower bound on the maximum
-  int cnt;        // kept entries
   int state;      // 0 searched, 1 constant template (NaN), 2 beyond the grid
-  int pad[2];
 };
 
 struct TileArgs {
   const uint8_t *f, *g;
   const uint4 *tab;  // W x H: (sum, sum of squares, bits of 1/sqrt(C0), 0) of full windows
-  const double *mu;
-  double *ox, *oy, *ou, *ov, *occ;
-  int *fb;           // fb[0] count, fb[1 ..] grid points for the per-point kernel
-  unsigned *ringc;   // exact sums of the outer ring, nring a point, tile by tile
-  int W, H, px1, py1, nx, ny, w, sx, sy, cr, cc, nring;
+  unsigned *cmap;    // exact correlation sums, cr * cc a point (b * cr + a), tile by tile
+  TileSub *subs;     // template sums of every point, tile by tile
+  uint2 *ringw;      // window sums of every point's outer ring, ring order
+  int W, H, px1, py1, nx, ny, w, sx, sy, cr, cc;
   int tsy, ndy, nbatch, pitch, rows_g, pb, qxn, qyn;
   long long mn;
-  int off_g, off_ti, off_ra, off_rb, off_rc, off_sub, off_cand;
+  int off_g, off_ti, off_ra, off_rb, off_rc, off_sub;
 };
 
 __device__ __forceinline__ unsigned fkey(float x) {  // order-preserving float -> unsigned
@@ -655,7 +651,6 @@ struct TileShape {
 struct TileMem {
   const uint32_t *Fw, *Gw;
   const int *tis, *tis2;   // full windows at tile position (qxi, qyi): sums of g, g^2
-  const float *tii;        // and 1 / sqrt(mn sum g^2 - (sum g)^2) (0 where that is <= 0)
   const uint2 *ra, *rb, *rc;
   int pitch, qxn, qyn, tsy;
 };
@@ -675,14 +670,14 @@ __device__ __forceinline__ uint2 tile_wsum(const TileMem &M, int ix, int iy, int
   return M.rc[(iy * kTileTSX + ix) * 4 + (a != 0) + 2 * (b != 0)];
 }
 
-// the outer ring of the cropped map, k in [0, 2 (cr + cc) - 4): columns a = 0
+// the outer ring of the cropped map, r in [0, 2 (cr + cc) - 4): columns a = 0
 // and cr-1 (all b), then rows b = 0 and cc-1 (a = 1 .. cr-2)
-__device__ __forceinline__ void ring_pos(int k, int cr, int cc, int *a, int *b) {
-  if (k < 2 * cc) {
-    *a = k < cc ? 0 : cr - 1;
-    *b = k < cc ? k : k - cc;
+__device__ __forceinline__ void ring_pos(int r, int cr, int cc, int *a, int *b) {
+  if (r < 2 * cc) {
+    *a = r < cc ? 0 : cr - 1;
+    *b = r < cc ? r : r - cc;
   } else {
-    const int m = k - 2 * cc;
+    const int m = r - 2 * cc;
     *a = 1 + (m < cr - 2 ? m : m - (cr - 2));
     *b = m < cr - 2 ? 0 : cc - 1;
   }
@@ -691,38 +686,6 @@ __device__ __forceinline__ int ring_index(int a, int b, int cr, int cc) {
   if (a == 0) return b;
   if (a == cr - 1) return cc + b;
   return 2 * cc + (a - 1) + (b == 0 ? 0 : cr - 2);
-}
-
-// FP64 NCC of entry (a, b) of tile point (ix, iy) from its exact correlation sum
-template <int STEP>
-__device__ __forceinline__ double tile_exact(const TileArgs &A, const TileMem &M, const TileSub &S,
-                                             int ix, int iy, int tw, int a, int b, unsigned acc,
-                                             double mu) {
-  const uint2 w = tile_wsum<STEP>(M, ix, iy, a, b, A.cr, A.cc);
-  long long st_out, n_out;
-  tile_pad(S, a, b, A.cr, A.cc, tw, &st_out, &n_out);
-  return ncc_combine(A.mn, S.st, S.st2, (long long)acc, (long long)w.x, (long long)w.y, st_out,
-                     n_out, mu);
-}
-
-// exact correlation sum of entry (a, b) of tile point (ix, iy), by one warp
-template <int STEP, int WS, int TSX>
-__device__ __forceinline__ unsigned tile_direct(const uint32_t *Fw, const uint32_t *Gw, int pitch,
-                                                int ix, int iy, int a, int b, int cr, int cc) {
-  using T = TileShape<STEP, WS, TSX>;
-  constexpr int NW = T::Q + 1;  // words of a template row (the last holds one pixel)
-  const int lane = threadIdx.x & 31;
-  unsigned sum = 0;
-  for (int p = lane; p < T::TW * NW; p += 32) {  // lanes over (row, word) pairs
-    const int ty = p / NW, k = p - ty * NW;
-    if ((b == 0 && ty == 0) || (b == cc - 1 && ty == T::TW - 1)) continue;
-    const int y = iy * STEP + ty;
-    uint32_t fw = Fw[y * T::NGP + T::GS * ix + k];
-    if (k == 0 && a == 0) fw &= 0xFFFFFF00u;
-    if (k == T::Q) fw = a != cr - 1 ? fw & 0xFFu : 0u;
-    sum = __dp4a(fw, Gw[(y + b) * pitch + ix * STEP + a + 4 * k], sum);
-  }
-  return __reduce_add_sync(0xffffffffu, sum);
 }
 
 // one tile row for shift (a, b): group products into acc, first pixels into accE
@@ -777,12 +740,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
   uint32_t *Gw = reinterpret_cast<uint32_t *>(smem + A.off_g);
   int *tis = reinterpret_cast<int *>(smem + A.off_ti);
   int *tis2 = tis + A.qxn * A.qyn;
-  float *tii = reinterpret_cast<float *>(tis2 + A.qxn * A.qyn);
   uint2 *ra = reinterpret_cast<uint2 *>(smem + A.off_ra);
   uint2 *rb = reinterpret_cast<uint2 *>(smem + A.off_rb);
   uint2 *rc = reinterpret_cast<uint2 *>(smem + A.off_rc);
   TileSub *sub = reinterpret_cast<TileSub *>(smem + A.off_sub);
-  uint2 *cand = reinterpret_cast<uint2 *>(smem + A.off_cand);
   uint8_t *tmp = smem + A.off_ti;  // g bytes while staging (the window tables come later)
   const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nth >> 5;
   const int TSY = A.tsy, NS = TSX * TSY, RYf = (TSY - 1) * STEP + TW;
@@ -790,8 +751,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
   const int tx0 = blockIdx.x * TSX, ty0 = blockIdx.y * TSY;       // first grid point
   const int px0 = A.px1 + tx0 * STEP, py0 = A.py1 + ty0 * STEP;   // its 0-based corner
   const int gx0 = px0 - A.sx - 1, gy0 = py0 - A.sy - 1;           // corner of the g tile
-  const TileMem M{Fw, Gw, tis, tis2, tii, ra, rb, rc, pitch, qxn, qyn, TSY};
-  unsigned *ringc = A.ringc + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * NS * A.nring;
+  const TileMem M{Fw, Gw, tis, tis2, ra, rb, rc, pitch, qxn, qyn, TSY};
+  const int nmap = cr * cc;
+  unsigned *cmap = A.cmap + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * NS * nmap;
 
   // ---- stage f (4 pixels a word) and g (word m of a row = bytes m .. m+3)
   for (int i = tid; i < RYf * NGP; i += nth) {
@@ -828,7 +790,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
     if (xx <= tabw && yy <= tabh) e = A.tab[(long long)yy * A.W + xx];
     tis[i] = (int)e.x;
     tis2[i] = (int)e.y;
-    tii[i] = __uint_as_float(e.z);
   }
   __syncthreads();
   // ---- the outer ring's windows: full window minus a column and/or a row
@@ -913,15 +874,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
       const long long denT = A.mn * v[1] - (long long)v[0] * v[0];
       S.state = !valid ? 2 : (denT == 0 ? 1 : 0);
       S.invT = denT > 0 ? (float)(1.0 / sqrt((double)denT)) : 0.f;
-      S.lb = 0u;
-      S.cnt = 0;
     }
   }
   __syncthreads();
-  const double mu = *A.mu;
 
   // ---- every shift of the cropped map, ndy map columns per batch; the two
-  // ring shifts (a = 0, cr-1) of each column take the first lanes
+  // ring shifts (a = 0, cr-1) of each column take the first lanes, so the
+  // interior shifts of a warp run along a in one bank sequence
   for (int bt = 0; bt < A.nbatch; ++bt) {
     const int b0 = bt * A.ndy, nbr = min(A.ndy, cc - b0);
     int a, b;
@@ -941,7 +900,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
       }
     }
     const unsigned cF = (a == 0), cL = (a != cr - 1), cRF = (b == 0), cRL = (b != cc - 1);
-    const bool ring = (a == 0) || (a == cr - 1) || (b == 0) || (b == cc - 1);
     const uint32_t *gbase = Gw + b * pitch + a;
     unsigned win[QB][TSX];
     unsigned acc[NG], accE[NE], S[TSX];
@@ -957,45 +915,12 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
         tile_row<STEP, WS, TSX>(Fw + j * STEP * NGP, gbase + j * STEP * pitch, acc, accE);
         tile_hsum<STEP, WS, TSX>(acc, accE, cF, cL, S);
         if (j >= QB) {
-          // ---- the windows of point row iy are complete: screen them
+          // ---- the windows of point row iy are complete: to the maps
           const int iy = j - QB;
-          float rlo[TSX], rhi[TSX];
-#pragma unroll
-          for (int ix = 0; ix < TSX; ++ix) {
-            const unsigned C = win[sl][ix] + cRL * S[ix];
-            win[sl][ix] = C;
-            const TileSub &P = sub[iy * TSX + ix];
-            rlo[ix] = -INFINITY;
-            rhi[ix] = -INFINITY;
-            if (active && P.state == 0) {
-              if (!ring) {
-                const int i = (iy * STEP + b) * qxn + ix * STEP + a;
-                const long long num = A.mn * (long long)C - (long long)P.st * tis[i];
-                const float r = (float)num * P.invT * tii[i];
-                rlo[ix] = r - kTileEps;
-                rhi[ix] = r + kTileEps;
-              } else {
-                ringc[(iy * TSX + ix) * A.nring + ring_index(a, b, cr, cc)] = C;
-              }
-            }
-          }
-          // raise the bound by this warp's maximum, then keep what can still
-          // reach it; no barrier: a bound read before other warps raised it
-          // only keeps a few more entries (it never exceeds the final one)
-#pragma unroll
-          for (int ix = 0; ix < TSX; ++ix) {
-            const unsigned kmax = __reduce_max_sync(0xffffffffu, fkey(rlo[ix]));
-            if (lane == 0) atomicMax(&sub[iy * TSX + ix].lb, kmax);
-          }
-          __syncwarp();
 #pragma unroll
           for (int ix = 0; ix < TSX; ++ix) {
             const int s = iy * TSX + ix;
-            const unsigned lbs = *reinterpret_cast<volatile unsigned *>(&sub[s].lb);
-            if (rhi[ix] != -INFINITY && fkey(rhi[ix]) >= lbs) {
-              const int pos = atomicAdd(&sub[s].cnt, 1);
-              if (pos < kTileCap) cand[s * kTileCap + pos] = make_uint2(b * cr + a, win[sl][ix]);
-            }
+            if (active && sub[s].state == 0) cmap[(size_t)s * nmap + b * cr + a] = win[sl][ix] + cRL * S[ix];
           }
         }
         if (j < TSY) {
@@ -1022,97 +947,19 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_search_tile(const TileArgs 
   }
   __syncthreads();
 
-  // ---- exact FP64 values of the kept entries, argmax, findpeak (a warp a point)
+  // ---- export: each point's template sums and the window sums of its outer
+  // ring (the peak kernel reads them with the maps)
+  const size_t tile0 = (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * NS;
+  const int nring = 2 * (cr + cc) - 4;
   for (int s = wid; s < NS; s += nw) {
-    const TileSub &P = sub[s];
-    if (P.state == 2) continue;
+    if (lane == 0) A.subs[tile0 + s] = sub[s];
+    if (sub[s].state != 0) continue;
     const int ix = s % TSX, iy = s / TSX;
-    const int gix = tx0 + ix, giy = ty0 + iy;
-    const long long out_idx = (long long)giy + (long long)gix * A.ny;
-    const int ii = px0 + ix * STEP + 1, jj = py0 + iy * STEP + 1;  // 1-based
-    if (P.state == 1) {
-      if (lane == 0) {
-        const double nan = __longlong_as_double(0x7ff8000000000000ll);
-        A.ox[out_idx] = (ii + ii + A.w) / 2.0;
-        A.oy[out_idx] = (jj + jj + A.w) / 2.0;
-        A.ou[out_idx] = nan;
-        A.ov[out_idx] = nan;
-        A.occ[out_idx] = nan;
-      }
-      continue;
-    }
-    const int n = P.cnt;
-    bool hand_back = n > kTileCap;
-    double best = -INFINITY;
-    int bi = 0x7fffffff;
-    if (!hand_back) {
-      for (int k = lane; k < A.nring; k += 32) {
-        int ra_, rb_;
-        ring_pos(k, cr, cc, &ra_, &rb_);
-        const double r =
-            tile_exact<STEP>(A, M, P, ix, iy, TW, ra_, rb_, ringc[s * A.nring + k], mu);
-        const int idx = rb_ * cr + ra_;
-        if (r > best || (r == best && idx < bi)) {
-          best = r;
-          bi = idx;
-        }
-      }
-      if (lane < n) {
-        const uint2 e = cand[s * kTileCap + lane];
-        const double r = tile_exact<STEP>(A, M, P, ix, iy, TW, e.x % cr, e.x / cr, e.y, mu);
-        if (r > best || (r == best && (int)e.x < bi)) {
-          best = r;
-          bi = (int)e.x;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      // the bound must hold for the evaluated maximum (it can only fail where
-      // an estimate met ncc_combine's clamp of |r| > 1)
-      hand_back = !(best >= (double)fkey_inv(P.lb));
-    }
-    if (hand_back) {
-      if (lane == 0) {
-        const int pos = atomicAdd(A.fb, 1);
-        A.fb[1 + pos] = giy * A.nx + gix;
-      }
-      continue;
-    }
-    const int am = bi % cr, bm = bi / cr;
-    double rpk = am + 1, cpk = bm + 1, mf = best;
-    if (am > 0 && am < cr - 1 && bm > 0 && bm < cc - 1) {
-      unsigned my_acc = 0;
-      int my_a = am, my_b = bm;
-      for (int k = 0; k < 9; ++k) {
-        if (k == 4) continue;
-        const int na = am + k % 3 - 1, nb = bm + k / 3 - 1;
-        const unsigned c = tile_direct<STEP, WS, TSX>(Fw, Gw, pitch, ix, iy, na, nb, cr, cc);
-        if (lane == k) {
-          my_acc = c;
-          my_a = na;
-          my_b = nb;
-        }
-      }
-      double r = best;
-      if (lane < 9 && lane != 4) r = tile_exact<STEP>(A, M, P, ix, iy, TW, my_a, my_b, my_acc, mu);
-      double u9[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) u9[k] = __shfl_sync(0xffffffffu, r, k);
-      if (lane == 0) findpeak_fit9(u9, am, bm, &rpk, &cpk, &mf);
-    }
-    if (lane == 0) {
-      A.ox[out_idx] = (ii + ii + A.w) / 2.0;
-      A.oy[out_idx] = (jj + jj + A.w) / 2.0;
-      A.ou[out_idx] = __dsub_rn(rpk, (double)(A.sx + 2));
-      A.ov[out_idx] = __dsub_rn(cpk, (double)(A.sy + 2));
-      A.occ[out_idx] = mf;
+    uint2 *rw = A.ringw + (tile0 + s) * nring;
+    for (int r = lane; r < nring; r += 32) {
+      int ra, rb;
+      ring_pos(r, cr, cc, &ra, &rb);
+      rw[r] = tile_wsum<STEP>(M, ix, iy, ra, rb, cr, cc);
     }
   }
 }
@@ -1191,9 +1038,220 @@ __global__ void __launch_bounds__(256) k_box_tab(const uint8_t *__restrict__ g, 
   }
 }
 
+// ---- peak search of every grid point from its exact correlation map (a
+// warp a point, full occupancy): FP32 estimates over the map, the entries
+// within reach of the running bound T = max(estimate - eps) queued in shared
+// memory, ncc_combine on those still within reach of the final T (lanes in
+// parallel), argmax (first in map order on ties), findpeak's 3 x 3 fit from
+// the neighbours' exact values; outputs of funIntegerSearch.m:148-159.
+constexpr int kPeakWarps = 8;
+
+struct PeakArgs {
+  const unsigned *cmap;   // exact correlation sums, tile by tile
+  const uint2 *ringw;     // window sums of the outer ring, ring order
+  const TileSub *subs;    // template sums
+  const uint4 *tab;       // W x H full-window table (sum, sum of squares, 1/sqrt(C0))
+  const double *mu;
+  double *ox, *oy, *ou, *ov, *occ;
+  int *fb;                // fb[0] count, fb[1 ..] grid points for the per-point kernel
+  int W, px1, py1, nx, ny, step, w, tw, sx, sy, cr, cc, tsy, tiles_x;
+  long long mn;
+};
+
+__global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakArgs A) {
+  __shared__ uint3 qbuf[kPeakWarps][kTileQueue];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint3 *queue = qbuf[wid];
+  const double mu = *A.mu;
+  const int cr = A.cr, cc = A.cc, ci = cr - 2, ni = ci * (cc - 2), nring = 2 * (cr + cc) - 4;
+  const int nmap = cr * cc, NS = kTileTSX * A.tsy;
+  const long long npts = (long long)A.nx * A.ny;
+  for (long long pt = (long long)blockIdx.x * kPeakWarps + wid; pt < npts;
+       pt += (long long)gridDim.x * kPeakWarps) {
+    const int gix = (int)(pt % A.nx), giy = (int)(pt / A.nx);
+    const size_t ps = (size_t)((giy / A.tsy) * A.tiles_x + gix / kTileTSX) * NS +
+                      (giy % A.tsy) * kTileTSX + gix % kTileTSX;
+    const TileSub P = A.subs[ps];
+    const long long out_idx = (long long)giy + (long long)gix * A.ny;
+    const int px = A.px1 + gix * A.step, py = A.py1 + giy * A.step;
+    const int ii = px + 1, jj = py + 1;  // 1-based
+    if (P.state != 0) {  // constant template: normxcorr2 raises (funIntegerSearch.m:153-157)
+      if (lane == 0) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        A.ox[out_idx] = (ii + ii + A.w) / 2.0;
+        A.oy[out_idx] = (jj + jj + A.w) / 2.0;
+        A.ou[out_idx] = nan;
+        A.ov[out_idx] = nan;
+        A.occ[out_idx] = nan;
+      }
+      continue;
+    }
+    const unsigned *cm = A.cmap + ps * nmap;
+    const uint2 *rw = A.ringw + ps * nring;
+    const uint4 *tb = A.tab + (long long)(py - 1 - A.sy) * A.W + (px - 1 - A.sx);  // entry (a, b): tb[b W + a]
+    auto exact = [&](int a, int b, unsigned C) -> double {
+      uint2 w;
+      if (a == 0 || a == cr - 1 || b == 0 || b == cc - 1) {
+        w = rw[ring_index(a, b, cr, cc)];
+      } else {
+        const uint4 t = tb[(long long)b * A.W + a];
+        w = make_uint2(t.x, t.y);
+      }
+      long long st_out, n_out;
+      tile_pad(P, a, b, cr, cc, A.tw, &st_out, &n_out);
+      return ncc_combine(A.mn, P.st, P.st2, (long long)C, (long long)w.x, (long long)w.y, st_out,
+                         n_out, mu);
+    };
+    unsigned tkey = 0u;  // ordered key of the running bound
+    int nq = 0;          // queued entries (the same in every lane)
+    // 4 entries a lane at a time: the loads first, one bound update, then the
+    // queue (ballot order keeps it dense)
+    auto screen4 = [&](const bool (&valid)[4], const int (&k)[4], const unsigned (&C)[4],
+                       const float (&e)[4]) {
+      float mx = -INFINITY;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (valid[j]) mx = fmaxf(mx, e[j] - kTileEps);
+      tkey = max(tkey, __reduce_max_sync(0xffffffffu, fkey(mx)));
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool keep = valid[j] && fkey(e[j] + kTileEps) >= tkey;
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int pos = nq + __popc(bal & ((1u << lane) - 1u));
+          if (pos < kTileQueue) queue[pos] = make_uint3((unsigned)k[j], C[j], __float_as_uint(e[j]));
+        }
+        nq += __popc(bal);
+      }
+    };
+    // interior entries (a, b in 1 .. cr-2, 1 .. cc-2), lanes along a
+    int a = 1 + lane, b = 1;
+    while (a > ci) {
+      a -= ci;
+      ++b;
+    }
+    for (int k0 = 0; k0 < ni; k0 += 128) {
+      bool valid[4];
+      int k[4];
+      unsigned C[4];
+      uint4 t[4];
+      float e[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        valid[j] = k0 + 32 * j + lane < ni;
+        k[j] = b * cr + a;
+        C[j] = 0u;
+        t[j] = make_uint4(0, 0, 0, 0);
+        if (valid[j]) {
+          C[j] = cm[k[j]];
+          t[j] = tb[(long long)b * A.W + a];
+        }
+        a += 32;
+        while (a > ci) {
+          a -= ci;
+          ++b;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const long long num = A.mn * (long long)C[j] - (long long)P.st * (int)t[j].x;
+        e[j] = (float)num * P.invT * __uint_as_float(t[j].z);
+      }
+      screen4(valid, k, C, e);
+    }
+    // the outer ring, from ncc_combine's own FP64 numerator and denominator
+    for (int k0 = 0; k0 < nring; k0 += 128) {
+      bool valid[4];
+      int k[4], ra[4], rb[4];
+      unsigned C[4];
+      uint2 w[4];
+      float e[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = k0 + 32 * j + lane;
+        valid[j] = r < nring;
+        ring_pos(valid[j] ? r : 0, cr, cc, &ra[j], &rb[j]);
+        k[j] = rb[j] * cr + ra[j];
+        C[j] = valid[j] ? cm[k[j]] : 0u;
+        w[j] = valid[j] ? rw[r] : make_uint2(0, 0);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        e[j] = 0.f;
+        if (valid[j]) {
+          long long st_out, n_out;
+          tile_pad(P, ra[j], rb[j], cr, cc, A.tw, &st_out, &n_out);
+          double num, den;
+          ncc_parts(A.mn, P.st, (long long)C[j], (long long)w[j].x, (long long)w[j].y, st_out,
+                    n_out, mu, &num, &den);
+          e[j] = den > 0.0 ? (float)num * P.invT * rsqrtf((float)den) : 0.f;
+        }
+      }
+      screen4(valid, k, C, e);
+    }
+    __syncwarp();
+    bool hand_back = nq > kTileQueue;
+    double best = -INFINITY;
+    int bi = 0x7fffffff;
+    if (!hand_back) {
+      for (int q = lane; q < nq; q += 32) {
+        const uint3 e = queue[q];
+        if (fkey(__uint_as_float(e.z) + kTileEps) >= tkey) {
+          const double r = exact((int)e.x % cr, (int)e.x / cr, e.y);
+          if (r > best || (r == best && (int)e.x < bi)) {
+            best = r;
+            bi = (int)e.x;
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      // the bound must hold for the evaluated maximum (it can only fail where
+      // an estimate met ncc_combine's clamp of |r| > 1)
+      hand_back = !(best >= (double)fkey_inv(tkey));
+    }
+    __syncwarp();  // the queue is the next point's
+    if (hand_back) {
+      if (lane == 0) {
+        const int pos = atomicAdd(A.fb, 1);
+        A.fb[1 + pos] = giy * A.nx + gix;
+      }
+      continue;
+    }
+    const int am = bi % cr, bm = bi / cr;
+    double rpk = am + 1, cpk = bm + 1, mf = best;
+    if (am > 0 && am < cr - 1 && bm > 0 && bm < cc - 1) {
+      // the 3 x 3 neighbourhood, lane k = (dc + 1) * 3 + dr + 1
+      double r = best;
+      if (lane < 9 && lane != 4) {
+        const int na = am + lane % 3 - 1, nb = bm + lane / 3 - 1;
+        r = exact(na, nb, cm[nb * cr + na]);
+      }
+      double u9[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) u9[k] = __shfl_sync(0xffffffffu, r, k);
+      if (lane == 0) findpeak_fit9(u9, am, bm, &rpk, &cpk, &mf);
+    }
+    if (lane == 0) {
+      A.ox[out_idx] = (ii + ii + A.w) / 2.0;
+      A.oy[out_idx] = (jj + jj + A.w) / 2.0;
+      A.ou[out_idx] = __dsub_rn(rpk, (double)(A.sx + 2));
+      A.ov[out_idx] = __dsub_rn(cpk, (double)(A.sy + 2));
+      A.occ[out_idx] = mf;
+    }
+  }
+}
+
 struct TilePlan {
   int tsy = 0, ndy = 0, nbatch = 0, pitch = 0, rows_g = 0, pb = 0, qxn = 0, qyn = 0;
-  int off_g = 0, off_ti = 0, off_ra = 0, off_rb = 0, off_rc = 0, off_sub = 0, off_cand = 0;
+  int off_g = 0, off_ti = 0, off_ra = 0, off_rb = 0, off_rc = 0, off_sub = 0;
   int total = 0;
 };
 
@@ -1218,7 +1276,7 @@ bool tile_plan(int sx, int sy, TilePlan &P) {
     const size_t og = o;
     o += align16((size_t)rows_g * P.pitch * 4);
     const size_t oti = o;
-    o += align16(std::max((size_t)3 * P.qxn * qyn * 4, (size_t)rows_g * P.pb));
+    o += align16(std::max((size_t)2 * P.qxn * qyn * 4, (size_t)rows_g * P.pb));
     const size_t ora = o;
     o += align16((size_t)2 * kTileTSX * qyn * sizeof(uint2));
     const size_t orb = o;
@@ -1227,8 +1285,6 @@ bool tile_plan(int sx, int sy, TilePlan &P) {
     o += align16((size_t)ns * 4 * sizeof(uint2));
     const size_t os = o;
     o += align16((size_t)ns * sizeof(TileSub));
-    const size_t oc = o;
-    o += align16((size_t)ns * kTileCap * sizeof(uint2));
     if (o <= (size_t)227 * 1024) {
       P.tsy = tsy;
       P.rows_g = rows_g;
@@ -1239,7 +1295,6 @@ bool tile_plan(int sx, int sy, TilePlan &P) {
       P.off_rb = (int)orb;
       P.off_rc = (int)orc;
       P.off_sub = (int)os;
-      P.off_cand = (int)oc;
       P.total = (int)o;
       return true;
     }
@@ -1252,7 +1307,7 @@ int tile_launch(TileArgs A, const TilePlan &P, cudaStream_t st) {
   A.tsy = P.tsy; A.ndy = P.ndy; A.nbatch = P.nbatch; A.pitch = P.pitch;
   A.rows_g = P.rows_g; A.pb = P.pb; A.qxn = P.qxn; A.qyn = P.qyn;
   A.off_g = P.off_g; A.off_ti = P.off_ti; A.off_ra = P.off_ra; A.off_rb = P.off_rb;
-  A.off_rc = P.off_rc; A.off_sub = P.off_sub; A.off_cand = P.off_cand;
+  A.off_rc = P.off_rc; A.off_sub = P.off_sub;
   auto kern = k_search_tile<STEP, WS, kTileTSX>;
   ALDIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, P.total));
   const dim3 grid((A.nx + kTileTSX - 1) / kTileTSX, (A.ny + P.tsy - 1) / P.tsy);
@@ -1280,16 +1335,34 @@ int tile_dispatch(const TileArgs &A, const TilePlan &P, int step, cudaStream_t s
   return E_ARG;
 }
 
-// work slab: the window table (16 B per pixel), the hand-back list and the
-// ring sums (tiles hold at most 8 x 8 points, so (nx + 7) (ny + 7) bounds them)
-size_t tile_ring_bytes(int nx, int ny, const int search[2]) {
-  const long long nring = 2ll * (2 * search[0] + 3 + 2 * search[1] + 3) - 4;
-  return (size_t)(nx + 7) * (ny + 7) * nring * sizeof(unsigned);
-}
-size_t tile_bytes(int W, int H, int nx, int ny, const int search[2]) {
-  return align16((size_t)W * H * sizeof(uint4)) +
-         align16((size_t)((long long)nx * ny + 1) * sizeof(int)) +
-         align16(tile_ring_bytes(nx, ny, search));
+// work slab: the window table (16 B per pixel), the hand-back list, then
+// per tile point (tiles hold at most 8 x 8 points, so (nx + 7) (ny + 7)
+// bounds them) the correlation map (4 B per entry of the (2s+3)^2 map), the
+// template sums and the outer ring's window sums
+struct TileBufs {
+  uint4 *tab;
+  int *fb;
+  unsigned *cmap;
+  TileSub *subs;
+  uint2 *ringw;
+  size_t bytes;
+};
+TileBufs tile_bufs(char *base, int W, int H, int nx, int ny, const int search[2]) {
+  const size_t cr = 2 * search[0] + 3, cc = 2 * search[1] + 3, slots = (size_t)(nx + 7) * (ny + 7);
+  TileBufs B;
+  size_t o = 0;
+  B.tab = reinterpret_cast<uint4 *>(base + o);
+  o += align16((size_t)W * H * sizeof(uint4));
+  B.fb = reinterpret_cast<int *>(base + o);
+  o += align16((size_t)((long long)nx * ny + 1) * sizeof(int));
+  B.cmap = reinterpret_cast<unsigned *>(base + o);
+  o += align16(slots * cr * cc * sizeof(unsigned));
+  B.subs = reinterpret_cast<TileSub *>(base + o);
+  o += align16(slots * sizeof(TileSub));
+  B.ringw = reinterpret_cast<uint2 *>(base + o);
+  o += align16(slots * (2 * (cr + cc) - 4) * sizeof(uint2));
+  B.bytes = o;
+  return B;
 }
 
 // tiled 8-bit search; false in *used when the geometry has no tiled kernel
@@ -1305,12 +1378,9 @@ int tile_search(const uint8_t *f, const uint8_t *g, const SearchGeom &G, SearchW
   const int srch[2] = {G.sx, G.sy};
   int rc = search_work_ensure(sw, G.W, G.H, G.nx, G.ny, srch);
   if (rc) return rc;
-  char *wb = sw.buf.as<char>();
-  uint4 *tab = reinterpret_cast<uint4 *>(wb);
-  wb += align16((size_t)G.W * G.H * sizeof(uint4));
-  int *fb = reinterpret_cast<int *>(wb);
-  wb += align16((size_t)(npts + 1) * sizeof(int));
-  unsigned *ringc = reinterpret_cast<unsigned *>(wb);
+  const TileBufs B = tile_bufs(sw.buf.as<char>(), G.W, G.H, G.nx, G.ny, srch);
+  uint4 *tab = B.tab;
+  int *fb = B.fb;
   const long long mn = (long long)G.tw * G.tw;
   // full windows of every shift of every point (outer ring included)
   const int x0 = px1 - G.sx - 1, x1 = px1 + (G.nx - 1) * G.step + G.sx + 1;
@@ -1322,12 +1392,19 @@ int tile_search(const uint8_t *f, const uint8_t *g, const SearchGeom &G, SearchW
       g, G.W, G.H, G.tw, mn, x0, x1, y0, y1, tab);
   ALDIC_CUDA(cudaMemsetAsync(fb, 0, sizeof(int), st));
   TileArgs A{};
-  A.f = f; A.g = g; A.tab = tab; A.mu = G.mu;
-  A.ox = x; A.oy = y; A.ou = u; A.ov = v; A.occ = cc; A.fb = fb; A.ringc = ringc;
+  A.f = f; A.g = g; A.tab = tab; A.cmap = B.cmap; A.subs = B.subs; A.ringw = B.ringw;
   A.W = G.W; A.H = G.H; A.px1 = px1; A.py1 = py1; A.nx = G.nx; A.ny = G.ny; A.w = G.w;
   A.sx = G.sx; A.sy = G.sy; A.cr = G.cr; A.cc = G.cc; A.mn = mn;
-  A.nring = 2 * (G.cr + G.cc) - 4;
   if ((rc = tile_dispatch(A, P, G.step, st))) return rc;
+  PeakArgs K{};
+  K.cmap = B.cmap; K.ringw = B.ringw; K.subs = B.subs; K.tab = tab; K.mu = G.mu;
+  K.ox = x; K.oy = y; K.ou = u; K.ov = v; K.occ = cc; K.fb = fb;
+  K.W = G.W; K.px1 = px1; K.py1 = py1; K.nx = G.nx; K.ny = G.ny; K.step = G.step; K.w = G.w;
+  K.tw = G.tw; K.sx = G.sx; K.sy = G.sy; K.cr = G.cr; K.cc = G.cc; K.tsy = P.tsy;
+  K.tiles_x = (G.nx + kTileTSX - 1) / kTileTSX; K.mn = mn;
+  const int pb = (int)std::min<long long>((npts + kPeakWarps - 1) / kPeakWarps, 148 * 16);
+  k_search_peak<<<pb, kPeakWarps * 32, 0, st>>>(K);
+  ALDIC_CUDA(cudaGetLastError());
   // the points handed back: per-point kernel over the device-side list
   const int nb = (int)std::min<long long>(npts, 296);
   k_search_u8_list<<<nb, threads_pt, smem_pt, st>>>(f, g, G, fb, x, y, u, v, cc);
@@ -1523,7 +1600,7 @@ int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsiz
 }
 
 int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2]) {
-  return w.buf.ensure(tile_bytes(W, H, nx, ny, search));
+  return w.buf.ensure(tile_bufs(nullptr, W, H, nx, ny, search).bytes);
 }
 
 int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,

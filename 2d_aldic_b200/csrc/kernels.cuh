@@ -22,7 +22,7 @@ int interp_f32(const float *F, long long M, long long N, long long P, const floa
 
 // ---- k_search.cu
 // work of the tiled 8-bit search: the window table of the deformed image, the
-// list of points handed to the per-point kernel and the outer-ring sums
+// list of points handed to the per-point kernel and the correlation maps
 struct SearchWork {
   DevBuf buf;
   void release() { buf.release(); }

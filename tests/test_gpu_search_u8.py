@@ -4,8 +4,7 @@ cc.max.  Steps that are multiples of 4 dividing the subset size run the
 tiled kernel (every tile shape built: 16/4, 16/8, 24/8, 32/8, 32/16), step 10
 the per-point kernel; grid rows of every length, a constant template patch
 (normxcorr2 raises -> NaN) and a constant patch of the deformed image whose
-maps are all ties (the tiled kernel hands those points to the per-point
-kernel)."""
+maps hold dozens of exact ties."""
 import numpy as np
 import pytest
 
@@ -38,8 +37,8 @@ def test_search_flat_deformed_patch(aldic, oracle, synth):
     """A constant region of g larger than the search windows: the interior
     entries of those maps are all 0 and each side of the outer ring holds
     cc - 2 = 33 identical values (the padded pixels read as the mean), so the
-    maximum sits on the ring among more exact ties than the tiled kernel
-    keeps, and those points go to the per-point kernel."""
+    maximum sits on the ring among dozens of exact ties, all of which the
+    tiled kernel evaluates exactly (the first in map order wins)."""
     W, H = 300, 260
     f = synth.speckle(W, H, 1500, 43)
     g = synth.warp(f, lambda X, Y: (1.7 + 0 * X, -2.4 + 0 * Y), 2.0, 43)
