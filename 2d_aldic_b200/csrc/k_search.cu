@@ -1045,6 +1045,7 @@ __global__ void __launch_bounds__(256) k_box_tab(const uint8_t *__restrict__ g, 
 // parallel), argmax (first in map order on ties), findpeak's 3 x 3 fit from
 // the neighbours' exact values; outputs of funIntegerSearch.m:148-159.
 constexpr int kPeakWarps = 8;
+constexpr int kPeakUnroll = 4;  // map entries a lane has in flight
 
 struct PeakArgs {
   const unsigned *cmap;   // exact correlation sums, tile by tile
@@ -1104,17 +1105,17 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
     };
     unsigned tkey = 0u;  // ordered key of the running bound
     int nq = 0;          // queued entries (the same in every lane)
-    // 4 entries a lane at a time: the loads first, one bound update, then the
-    // queue (ballot order keeps it dense)
-    auto screen4 = [&](const bool (&valid)[4], const int (&k)[4], const unsigned (&C)[4],
-                       const float (&e)[4]) {
+    // kPeakUnroll entries a lane at a time: the loads first, one bound update,
+    // then the queue (ballot order keeps it dense)
+    auto screen = [&](const bool (&valid)[kPeakUnroll], const int (&k)[kPeakUnroll],
+                      const unsigned (&C)[kPeakUnroll], const float (&e)[kPeakUnroll]) {
       float mx = -INFINITY;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < kPeakUnroll; ++j)
         if (valid[j]) mx = fmaxf(mx, e[j] - kTileEps);
       tkey = max(tkey, __reduce_max_sync(0xffffffffu, fkey(mx)));
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kPeakUnroll; ++j) {
         const bool keep = valid[j] && fkey(e[j] + kTileEps) >= tkey;
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
         if (keep) {
@@ -1124,50 +1125,56 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
         nq += __popc(bal);
       }
     };
-    // interior entries (a, b in 1 .. cr-2, 1 .. cc-2), lanes along a
+    // interior entries (a, b in 1 .. cr-2, 1 .. cc-2), lanes along a; the
+    // lane's map index and table entry advance with it
     int a = 1 + lane, b = 1;
     while (a > ci) {
       a -= ci;
       ++b;
     }
-    for (int k0 = 0; k0 < ni; k0 += 128) {
-      bool valid[4];
-      int k[4];
-      unsigned C[4];
-      uint4 t[4];
-      float e[4];
+    int km = b * cr + a;
+    const uint4 *tp = tb + (long long)b * A.W + a;
+    for (int k0 = 0; k0 < ni; k0 += 32 * kPeakUnroll) {
+      bool valid[kPeakUnroll];
+      int k[kPeakUnroll];
+      unsigned C[kPeakUnroll];
+      uint4 t[kPeakUnroll];
+      float e[kPeakUnroll];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kPeakUnroll; ++j) {
         valid[j] = k0 + 32 * j + lane < ni;
-        k[j] = b * cr + a;
+        k[j] = km;
         C[j] = 0u;
         t[j] = make_uint4(0, 0, 0, 0);
         if (valid[j]) {
-          C[j] = cm[k[j]];
-          t[j] = tb[(long long)b * A.W + a];
+          C[j] = cm[km];
+          t[j] = *tp;
         }
         a += 32;
+        km += 32;
+        tp += 32;
         while (a > ci) {
           a -= ci;
-          ++b;
+          km += cr - ci;
+          tp += A.W - ci;
         }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kPeakUnroll; ++j) {
         const long long num = A.mn * (long long)C[j] - (long long)P.st * (int)t[j].x;
         e[j] = (float)num * P.invT * __uint_as_float(t[j].z);
       }
-      screen4(valid, k, C, e);
+      screen(valid, k, C, e);
     }
     // the outer ring, from ncc_combine's own FP64 numerator and denominator
-    for (int k0 = 0; k0 < nring; k0 += 128) {
-      bool valid[4];
-      int k[4], ra[4], rb[4];
-      unsigned C[4];
-      uint2 w[4];
-      float e[4];
+    for (int k0 = 0; k0 < nring; k0 += 32 * kPeakUnroll) {
+      bool valid[kPeakUnroll];
+      int k[kPeakUnroll], ra[kPeakUnroll], rb[kPeakUnroll];
+      unsigned C[kPeakUnroll];
+      uint2 w[kPeakUnroll];
+      float e[kPeakUnroll];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kPeakUnroll; ++j) {
         const int r = k0 + 32 * j + lane;
         valid[j] = r < nring;
         ring_pos(valid[j] ? r : 0, cr, cc, &ra[j], &rb[j]);
@@ -1176,7 +1183,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
         w[j] = valid[j] ? rw[r] : make_uint2(0, 0);
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < kPeakUnroll; ++j) {
         e[j] = 0.f;
         if (valid[j]) {
           long long st_out, n_out;
@@ -1187,7 +1194,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
           e[j] = den > 0.0 ? (float)num * P.invT * rsqrtf((float)den) : 0.f;
         }
       }
-      screen4(valid, k, C, e);
+      screen(valid, k, C, e);
     }
     __syncwarp();
     bool hand_back = nq > kTileQueue;
