@@ -362,9 +362,16 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
           const int i = (int)(k % M), j = (int)(k / M);
           double nv[G2], zo[G2], qo[G2], so[G2], po[G2], mo[G2], wo[G2], uo[G2], ro[G2], xo[G2],
               di[G2];
+          // inpainting: a known entry is an identity row whose r, u, w, m and
+          // directions are 0 after the set-up sweeps and stay 0, and no
+          // unknown row reads it -- skip it (its dot-product terms are 0)
+          bool act[G2];
+#pragma unroll
+          for (int q = 0; q < G2; ++q)
+            act[q] = live[q] && (OP != OP_INPAINT || A.mask[(long long)(f0 + q) * n + k]);
 #pragma unroll
           for (int q = 0; q < G2; ++q) {
-            if (!live[q]) continue;
+            if (!act[q]) continue;
             const int f = f0 + q;
             const long long o = f * n + k;
             nv[q] = op_apply<OP>(A, bt[q], i, j, k, f, Mo + f * n);
@@ -373,7 +380,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
           }
 #pragma unroll
           for (int q = 0; q < G2; ++q) {
-            if (!live[q]) continue;
+            if (!act[q]) continue;
             const long long o = (f0 + q) * n + k;
             const double zv = nv[q] + be[q] * zo[q];
             const double qv = mo[q] + be[q] * qo[q];
