@@ -79,6 +79,7 @@ struct aldic_ctx {
   bool have_ref = false, have_def = false;
   bool prepared = false;  // fields given by aldic_set_fields (no normalisation)
   DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
+  DevBuf g4;  // row runs of g32 (float4 per pixel) read by the FP32 IC-GN sampler
   DevBuf stats;   // double[4]: mean_f std_f mean_g std_g
   DevBuf isums;   // u64[2]
   DevBuf part;    // double[1024]
@@ -249,6 +250,7 @@ int check_grid_err(aldic_ctx *c) {
 IcgnImages images_of(aldic_ctx *c) {
   IcgnImages im;
   im.f32 = c->f32.as<float>(); im.g32 = c->g32.as<float>();
+  im.g4 = c->g4.as<float4>();
   im.gx32 = c->gx32.as<float>(); im.gy32 = c->gy32.as<float>();
   im.f64 = c->f64.as<double>(); im.g64 = c->g64.as<double>();
   im.gx64 = c->gx64.as<double>(); im.gy64 = c->gy64.as<double>();
@@ -378,7 +380,7 @@ int aldic_ctx_destroy(aldic_ctx *c) {
   for (int k = 0; k < 8; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   DevBuf *bufs[] = {&c->f_raw, &c->g_raw, &c->f64, &c->g64, &c->f32, &c->g32, &c->gx64,
-                    &c->gy64, &c->gx32, &c->gy32, &c->mask, &c->stats, &c->isums, &c->part,
+                    &c->gy64, &c->gx32, &c->gy32, &c->g4, &c->mask, &c->stats, &c->isums, &c->part,
                     &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr,
                     &c->hist};
   for (DevBuf *b : bufs) b->release();
@@ -417,6 +419,7 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     if ((rc = b->ensure(sizeof(double) * n))) return rc;
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
+  if ((rc = c->g4.ensure(sizeof(float4) * n))) return rc;
   if ((rc = c->f_raw.ensure(es * n))) return rc;
   if ((rc = c->g_raw.ensure(es * n))) return rc;
   if (c->dtype != dtype || c->W != W || c->H != H) c->have_def = false;
@@ -458,8 +461,10 @@ static int prep_def(aldic_ctx *c) {
   int rc = roi_stats(c->g_raw.p, c->dtype, c->W, c->roi, st + 2, c->isums.as<unsigned long long>(),
                      c->part.as<double>(), c->stream);
   if (rc) return rc;
-  return normalize(c->g_raw.p, c->dtype, (long long)c->W * c->H, st + 2, c->g64.as<double>(),
-                   c->g32.as<float>(), c->stream);
+  if ((rc = normalize(c->g_raw.p, c->dtype, (long long)c->W * c->H, st + 2, c->g64.as<double>(),
+                      c->g32.as<float>(), c->stream)))
+    return rc;
+  return row_runs(c->g32.as<float>(), c->W, c->H, c->g4.as<float4>(), c->stream);
 }
 
 int aldic_set_def(aldic_ctx *c, const void *img, int dtype) {
@@ -548,6 +553,7 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     if ((rc = b->ensure(bytes))) return rc;
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
+  if ((rc = c->g4.ensure(sizeof(float4) * n))) return rc;
   if (first) c->have_def = false;
   c->W = W; c->H = H; c->dtype = 3;
   c->prepared = true;
@@ -560,6 +566,7 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     ALDIC_CUDA(cudaMemcpyAsync(d64[k]->p, src[k], bytes, cudaMemcpyDefault, c->stream));
     k_to_f32<<<1184, 256, 0, c->stream>>>(d64[k]->as<double>(), d32[k]->as<float>(), n);
   }
+  if (gimg && (rc = row_runs(c->g32.as<float>(), W, H, c->g4.as<float4>(), c->stream))) return rc;
   if (f) ALDIC_CUDA(cudaMemcpyAsync(c->f_raw.p, c->f64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
   if (gimg) ALDIC_CUDA(cudaMemcpyAsync(c->g_raw.p, c->g64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
   // the normalised fields have mean 0 in the units the search pads with

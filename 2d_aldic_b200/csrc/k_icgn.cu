@@ -72,8 +72,9 @@ template <> struct Img<double> {
   static __device__ __forceinline__ const double *gy(const IcgnImages &m) { return m.gy64; }
 };
 
-// Cholesky of the 6x6 SPD matrix (lower, packed row-wise in L[21]).
-__device__ bool chol6(const double H[36], double L[21]) {
+// Cholesky of the 6x6 SPD matrix (lower, packed row-wise in L[21]); inv[i]
+// = 1 / L(i,i), so that the solves multiply instead of dividing.
+__device__ bool chol6(const double H[36], double L[21], double inv[6]) {
   int idx = 0;
   for (int i = 0; i < 6; ++i)
     for (int j = 0; j <= i; ++j) {
@@ -82,24 +83,29 @@ __device__ bool chol6(const double H[36], double L[21]) {
       if (i == j) {
         if (!(s > 0.0)) return false;
         L[idx++] = sqrt(s);
+        inv[i] = 1.0 / L[idx - 1];
       } else {
-        L[idx++] = s / L[j * (j + 1) / 2 + j];
+        L[idx++] = s * inv[j];
       }
     }
   return true;
 }
 
-__device__ void chol6_solve(const double *L, const double b[6], double x[6]) {
+__device__ void chol6_solve(const double *L, const double *inv, const double b[6], double x[6]) {
   double y[6];
+#pragma unroll
   for (int i = 0; i < 6; ++i) {
     double t = b[i];
+#pragma unroll
     for (int k = 0; k < i; ++k) t -= L[i * (i + 1) / 2 + k] * y[k];
-    y[i] = t / L[i * (i + 1) / 2 + i];
+    y[i] = t * inv[i];
   }
+#pragma unroll
   for (int i = 5; i >= 0; --i) {
     double t = y[i];
+#pragma unroll
     for (int k = i + 1; k < 6; ++k) t -= L[k * (k + 1) / 2 + i] * x[k];
-    x[i] = t / L[i * (i + 1) / 2 + i];
+    x[i] = t * inv[i];
   }
 }
 
@@ -107,12 +113,13 @@ __device__ void chol6_solve(const double *L, const double b[6], double x[6]) {
 __device__ __forceinline__ bool ic_compose(double P[6], const double d[6]) {
   const double det = (1 + d[0]) * (1 + d[3]) - d[1] * d[2];
   if (!(det != 0.0)) return false;
-  const double t1 = (-d[0] - d[0] * d[3] + d[1] * d[2]) / det;
-  const double t2 = -d[1] / det;
-  const double t3 = -d[2] / det;
-  const double t4 = (-d[3] - d[0] * d[3] + d[1] * d[2]) / det;
-  const double t5 = (-d[4] - d[3] * d[4] + d[2] * d[5]) / det;
-  const double t6 = (-d[5] - d[0] * d[5] + d[1] * d[4]) / det;
+  const double id = 1.0 / det;
+  const double t1 = (-d[0] - d[0] * d[3] + d[1] * d[2]) * id;
+  const double t2 = -d[1] * id;
+  const double t3 = -d[2] * id;
+  const double t4 = (-d[3] - d[0] * d[3] + d[1] * d[2]) * id;
+  const double t5 = (-d[4] - d[3] * d[4] + d[2] * d[5]) * id;
+  const double t6 = (-d[5] - d[0] * d[5] + d[1] * d[4]) * id;
   const double a11 = 1 + P[0], a12 = P[2], a13 = P[4];
   const double a21 = P[1], a22 = 1 + P[3], a23 = P[5];
   P[0] = a11 * (1 + t1) + a12 * t2 - 1;
@@ -142,6 +149,28 @@ __device__ __forceinline__ Real sample(const Real *__restrict__ img, int W, int 
   }
   return acc;
 }
+
+// The same sample from the row runs of img (q[i] = img[i .. i+3]): each
+// stencil row is one aligned 16-byte load, with the arithmetic of sample().
+__device__ __forceinline__ float sample(const float4 *__restrict__ q, int W, int cx, int cy,
+                                        float tu, float tv) {
+  float wu[4], wv[4];
+  keys_w(tu, wu);
+  keys_w(tv, wv);
+  const float4 *p = q + ((cy - 1) * W + (cx - 1));
+  float acc = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float4 t = __ldg(p + r * W);
+    const float s = wu[0] * t.x + wu[1] * t.y + wu[2] * t.z + wu[3] * t.w;
+    acc += wv[r] * s;
+  }
+  return acc;
+}
+
+// the FP32 path samples the row runs, the FP64 path the image itself
+__device__ __forceinline__ const float4 *sample_src(const IcgnImages &m, float) { return m.g4; }
+__device__ __forceinline__ const double *sample_src(const IcgnImages &m, double) { return m.g64; }
 
 // MATLAB's catch branch (LocalICGN.m:75-80, Subpb1.m:89-92): -1 and NaN
 template <bool SUB>
@@ -174,12 +203,13 @@ __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
 }
 
 // ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
-// S_f[6] at 57 and S[6] at 63 (kept out of registers to raise occupancy)
-constexpr int WS = 72;
+// S_f[6] at 57, S[6] at 63 and 1 / diag(L) at 69 (kept out of registers to
+// raise occupancy)
+constexpr int WS = 76;
 
 template <typename Real, bool SUB>
 __device__ void process(const Args &a, long long s, int lane, double *ws) {
-  double *Lsh = ws + 36, *Sfs = ws + 57, *Sks = ws + 63;
+  double *Lsh = ws + 36, *Sfs = ws + 57, *Sks = ws + 63, *Linv = ws + 69;
   const IcgnImages &im = a.im;
   const double x0 = a.coords[s], y0 = a.coords[a.n + s];
   int w = a.wins ? a.wins[s] : a.w;
@@ -205,7 +235,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     return;
   }
   const Real *fI = Img<Real>::f(im);
-  const Real *gI = Img<Real>::g(im);
+  const auto *gI = sample_src(im, Real(0));
   const Real *gxI = Img<Real>::gx(im);
   const Real *gyI = Img<Real>::gy(im);
   const int W = im.W;
@@ -356,7 +386,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   // ---- Hessian factor (IC-GN) or the damped 2x2 system (Subpb1)
   double *Hm = ws;
   bool spd = true;
-  double s2 = 0, Ha = 0, Hb = 0, Hd = 0;
+  double s2 = 0, l11i = 0, l21 = 0, l22i = 0;
   if (!SUB) {
     if (lane == 0) {
       // H of funICGN.m:67-79 from its 18 distinct sums (index map)
@@ -366,7 +396,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       double q[18];
       for (int k = 0; k < 18; ++k) q[k] = ws[k];
       for (int k = 0; k < 36; ++k) Hm[k] = q[map[k]];
-      spd = chol6(Hm, Lsh);
+      spd = chol6(Hm, Lsh, Linv);
     }
     spd = __shfl_sync(0xffffffffu, (int)spd, 0);
     __syncwarp();
@@ -378,9 +408,12 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
                  h66 = a.H21in[20 * a.n + s];
     const double H2a = h55 * s2 + a.mu, H2b = h65 * s2, H2d = h66 * s2 + a.mu;
     const double dmax = H2a > H2d ? H2a : H2d;
-    Ha = H2a + 1e-3 * dmax;
-    Hb = H2b;
-    Hd = H2d + 1e-3 * dmax;
+    // the damped 2x2 matrix is fixed for the subset: factor it once
+    const double Ha = H2a + 1e-3 * dmax, Hd = H2d + 1e-3 * dmax;
+    const double l11 = sqrt(Ha);
+    l11i = 1.0 / l11;
+    l21 = H2b * l11i;
+    l22i = 1.0 / sqrt(Hd - l21 * l21);
   }
 
   // ---- iterations (funICGN.m:107-294 / funICGN_Subpb1.m:94-337)
@@ -428,7 +461,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         const Real rv = a21 * X + (a22 * Y + c5);
         const Real fu = floor(ru), fv = floor(rv);
         const int cx = xb + (int)fu - 1, cy = yb + (int)fv - 1;  // 0-based floor corner
-        const Real gval = sample<Real>(gI, W, cx, cy, ru - fu, rv - fv);
+        const Real gval = sample(gI, W, cx, cy, ru - fu, rv - fv);
         const Real d = gval - cg;
         s1 += d;
         s2r += d * d;
@@ -464,17 +497,19 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     const double gm = sums[0] / n;                 // mean(g) - c
     const double ssg = sums[1] - sums[0] * gm;     // sum (g - gbar)^2
     const double bg = sqrt(ssg);
+    // b_k = bf (S_fk / bf - (T_k - gm S_k) / bg) = S_fk - (bf / bg)(T_k - gm S_k)
+    // (a flat reference subset, bf = 0, stays NaN as the division gives it)
+    const double rfg = bf > 0.0 ? bf / bg : nan64();
     double b[6], nb = 0;
     if (!SUB) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const double b2 = Sfs[q] / bf - (sums[2 + q] - gm * Sks[q]) / bg;
-        b[q] = bf * b2;
+        b[q] = Sfs[q] - rfg * (sums[2 + q] - gm * Sks[q]);
         nb += b[q] * b[q];
       }
     } else {
-      const double b5 = bf * (Sfs[4] / bf - (sums[6] - gm * Sks[4]) / bg);
-      const double b6 = bf * (Sfs[5] / bf - (sums[7] - gm * Sks[5]) / bg);
+      const double b5 = Sfs[4] - rfg * (sums[6] - gm * Sks[4]);
+      const double b6 = Sfs[5] - rfg * (sums[7] - gm * Sks[5]);
       b[4] = b5 * s2 + a.mu * (P[4] - a.U0[2 * s] - a.vdual[2 * s]);
       b[5] = b6 * s2 + a.mu * (P[5] - a.U0[2 * s + 1] - a.vdual[2 * s + 1]);
       nb = b[4] * b[4] + b[5] * b[5];
@@ -488,7 +523,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     double dP[6] = {0, 0, 0, 0, 0, 0};
     if (!SUB) {
       if (spd) {
-        chol6_solve(Lsh, b, dP);
+        chol6_solve(Lsh, Linv, b, dP);
 #pragma unroll
         for (int q = 0; q < 6; ++q) dP[q] = -dP[q];
       } else {
@@ -496,10 +531,9 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         for (int q = 0; q < 6; ++q) dP[q] = nan64();
       }
     } else {
-      // 2x2 SPD solve by Cholesky
-      const double l11 = sqrt(Ha), l21 = Hb / l11, l22 = sqrt(Hd - l21 * l21);
-      const double y1 = b[4] / l11, y2 = (b[5] - l21 * y1) / l22;
-      const double x2 = y2 / l22, x1 = (y1 - l21 * x2) / l11;
+      // 2x2 SPD solve with the Cholesky factor of the damped matrix
+      const double y1 = b[4] * l11i, y2 = (b[5] - l21 * y1) * l22i;
+      const double x2 = y2 * l22i, x1 = (y1 - l21 * x2) * l11i;
       dP[4] = -x1;
       dP[5] = -x2;
     }
@@ -521,7 +555,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 }
 
 template <typename Real, bool SUB>
-__global__ void __launch_bounds__(WARPS * 32, sizeof(Real) == 4 ? 3 : 2) k_icgn(Args a) {
+__global__ void __launch_bounds__(WARPS * 32, sizeof(Real) == 4 ? (SUB ? 4 : 3) : 2) k_icgn(Args a) {
   __shared__ double Lsh[WARPS][WS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   while (true) {

@@ -132,6 +132,29 @@ int normalize(const void *img, int dtype, long long n, const double *d_stats, do
   return OK;
 }
 
+// ------------------------------------------------------------------ row runs
+// q[y W + x] = (g[x], g[x+1], g[x+2], g[x+3]) of row y (0 past the row's
+// end): one aligned 16-byte load then gives a whole row of a bicubic stencil.
+__global__ void k_row_runs(const float *__restrict__ g, int W, long long n,
+                           float4 *__restrict__ q) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % W);
+    float4 t;
+    t.x = g[i];
+    t.y = x + 1 < W ? g[i + 1] : 0.f;
+    t.z = x + 2 < W ? g[i + 2] : 0.f;
+    t.w = x + 3 < W ? g[i + 3] : 0.f;
+    q[i] = t;
+  }
+}
+
+int row_runs(const float *g, int W, int H, float4 *q, cudaStream_t st) {
+  k_row_runs<<<1184, 256, 0, st>>>(g, W, (long long)W * H, q);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
 // ------------------------------------------------------------------ gradient
 __device__ __forceinline__ double grad7(const double *f, long long i, long long s) {
   const double c1 = 0.75, c2 = 3.0 / 20.0, c3 = 1.0 / 60.0;
