@@ -150,13 +150,25 @@ __device__ __forceinline__ Real sample(const Real *__restrict__ img, int W, int 
   return acc;
 }
 
+// Twice the Keys weights of keys_w (the same expressions without the final
+// multiplication by 1/2, which is exact in binary floating point).
+__device__ __forceinline__ void keys_w2(float t, float w[4]) {
+  const float t2 = t * t, t3 = t2 * t;
+  w[0] = fmaf(2.0f, t2, -t) - t3;
+  w[1] = fmaf(3.0f, t3, fmaf(-5.0f, t2, 2.0f));
+  w[2] = fmaf(-3.0f, t3, fmaf(4.0f, t2, t));
+  w[3] = t3 - t2;
+}
+
 // The same sample from the row runs of img (q[i] = img[i .. i+3]): each
-// stencil row is one aligned 16-byte load, with the arithmetic of sample().
-__device__ __forceinline__ float sample(const float4 *__restrict__ q, int W, int cx, int cy,
-                                        float tu, float tv) {
+// stencil row is one aligned 16-byte load.  With both weight sets doubled
+// every product and partial sum is exactly 2x or 4x that of sample(), so the
+// returned 4x sample scaled by 1/4 is bit-identical to sample().
+__device__ __forceinline__ float sample4x(const float4 *__restrict__ q, int W, int cx, int cy,
+                                          float tu, float tv) {
   float wu[4], wv[4];
-  keys_w(tu, wu);
-  keys_w(tv, wv);
+  keys_w2(tu, wu);
+  keys_w2(tv, wv);
   const float4 *p = q + ((cy - 1) * W + (cx - 1));
   float acc = 0;
 #pragma unroll
@@ -166,6 +178,17 @@ __device__ __forceinline__ float sample(const float4 *__restrict__ q, int W, int
     acc += wv[r] * s;
   }
   return acc;
+}
+
+// sample - c: one FMA of the exact 1/4 scaling (FP32 row runs), or the
+// FP64 sample minus c
+__device__ __forceinline__ float sample_minus(const float4 *q, int W, int cx, int cy, float tu,
+                                              float tv, float c) {
+  return fmaf(sample4x(q, W, cx, cy, tu, tv), 0.25f, -c);
+}
+__device__ __forceinline__ double sample_minus(const double *img, int W, int cx, int cy,
+                                               double tu, double tv, double c) {
+  return sample<double>(img, W, cx, cy, tu, tv) - c;
 }
 
 // the FP32 path samples the row runs, the FP64 path the image itself
@@ -461,8 +484,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         const Real rv = a21 * X + (a22 * Y + c5);
         const Real fu = floor(ru), fv = floor(rv);
         const int cx = xb + (int)fu - 1, cy = yb + (int)fv - 1;  // 0-based floor corner
-        const Real gval = sample(gI, W, cx, cy, ru - fu, rv - fv);
-        const Real d = gval - cg;
+        const Real d = sample_minus(gI, W, cx, cy, ru - fu, rv - fv, cg);
         s1 += d;
         s2r += d * d;
         const Real fx = gxI[k], fy = gyI[k];
