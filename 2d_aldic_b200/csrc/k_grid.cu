@@ -864,10 +864,19 @@ __global__ void k_diffnorm_part(const double *a, const double *b, long long n, d
   }
 }
 
+// one 256-thread block: strided partial sums, then a fixed-order tree
 __global__ void k_diffnorm_final(const double *part, int np, double *res) {
   double t = 0.0;
-  for (int k = 0; k < np; ++k) t += part[k];
-  *res = sqrt(t);
+  for (int k = threadIdx.x; k < np; k += blockDim.x) t += part[k];
+  t = warp_sum(t);
+  __shared__ double sh[32];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) u += sh[w];
+    *res = sqrt(u);
+  }
 }
 
 inline int blocks_for(long long n, int threads = 256) {
@@ -1162,7 +1171,7 @@ int vdiffnorm(const double *a, const double *b, long long n, double *part, doubl
               cudaStream_t st) {
   const int nb = 148;
   k_diffnorm_part<<<nb, 256, 0, st>>>(a, b, n, part);
-  k_diffnorm_final<<<1, 1, 0, st>>>(part, nb, res);
+  k_diffnorm_final<<<1, 256, 0, st>>>(part, nb, res);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

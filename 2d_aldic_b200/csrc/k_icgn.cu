@@ -225,6 +225,27 @@ __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
   }
 }
 
+// Pixel p of an nw x nw subset (x fastest): its column and row as exact
+// small integers in Real, and its offset row * W + column from the subset's
+// top-left pixel.  Branch-free, so the lanes of a warp (which wrap to the
+// next row at different p) stay converged.  row = floor((p + 1/2) / nw) is
+// exact: (p + 1/2) / nw lies at least 1/(2 nw) from an integer, and the two
+// FP32 roundings err by at most (p / nw) 2^-23, far less for p < 2^20.
+template <typename Real> struct PixelMap {
+  Real fnw, inw;
+  int W;
+  __device__ __forceinline__ PixelMap(int nw, int W_)
+      : fnw((Real)nw), inw((Real)1 / (Real)nw), W(W_) {}
+  __device__ __forceinline__ int at(int p, Real *col, Real *row) const {
+    const Real fp = (Real)p;
+    const Real r = floor((fp + (Real)0.5) * inw);
+    const Real c = fp - r * fnw;
+    *col = c;
+    *row = r;
+    return (int)r * W + (int)c;
+  }
+};
+
 // ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
 // S_f[6] at 57, S[6] at 63 and 1 / diag(L) at 69 (kept out of registers to
 // raise occupancy)
@@ -305,9 +326,10 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     for (int q = 0; q < 6; ++q) sk[q] = sfk[q] = 0;
 #pragma unroll
     for (int q = 0; q < 18; ++q) hh[q] = 0;
-    int iy = lane / nw, ix = lane - iy * nw;
+    const PixelMap<Real> pm(nw, W);
     for (int p = lane; p < npx; p += 32) {
-      const int k = base + iy * W + ix;
+      Real rx, ry;
+      const int k = base + pm.at(p, &rx, &ry);
       const Real fx = gxI[k], fy = gyI[k];
       const Real d = fI[k] - c;
       cnt += fx == (Real)0;
@@ -317,7 +339,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         sk[4] += fx; sk[5] += fy;
         sfk[4] += fx * d; sfk[5] += fy * d;
       } else {
-        const Real X = ox + (Real)ix, Y = oy + (Real)iy;
+        const Real X = ox + rx, Y = oy + ry;
         const Real sd[6] = {fx * X, fy * X, fx * Y, fy * Y, fx, fy};
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
@@ -331,11 +353,6 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         hh[8] += X * fyy;   hh[9] += YY * fxx;  hh[10] += YY * fxy; hh[11] += Y * fxx;
         hh[12] += Y * fxy;  hh[13] += YY * fyy; hh[14] += Y * fyy;  hh[15] += fxx;
         hh[16] += fxy;      hh[17] += fyy;
-      }
-      ix += 32;
-      while (ix >= nw) {
-        ix -= nw;
-        iy++;
       }
     }
 #pragma unroll
@@ -474,12 +491,15 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       Real s1 = 0, s2r = 0, t[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) t[q] = 0;
-      // pixel offsets X, Y and the image index k advance incrementally
-      int iy = lane / nw, ix = lane - (lane / nw) * nw;
-      Real X = ox + (Real)ix, Y = oy + (Real)iy;
-      int k = base + iy * W + ix;
+      const PixelMap<Real> pm(nw, W);
       const Real c4 = p4 + fx0, c5 = p5 + fy0;
+      // two pixels per trip pay off in the lighter Subpb1 loop only
+      constexpr int kUnroll = SUB ? 2 : 1;
+#pragma unroll kUnroll
       for (int p = lane; p < npx; p += 32) {
+        Real rx, ry;
+        const int k = base + pm.at(p, &rx, &ry);
+        const Real X = ox + rx, Y = oy + ry;
         const Real ru = a11 * X + (a12 * Y + c4);
         const Real rv = a21 * X + (a22 * Y + c5);
         const Real fu = floor(ru), fv = floor(rv);
@@ -496,15 +516,6 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
           t[1] += ay * X;
           t[2] += ax * Y;
           t[3] += ay * Y;
-        }
-        ix += 32;
-        X += (Real)32;
-        k += 32;
-        while (ix >= nw) {
-          ix -= nw;
-          X -= (Real)nw;
-          Y += (Real)1;
-          k += W - nw;
         }
       }
       sums[0] = warp_sum((double)s1);
