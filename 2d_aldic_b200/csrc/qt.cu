@@ -7,7 +7,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
-#include <unordered_map>
+#include <thread>
 #include <vector>
 
 #include "qt.cuh"
@@ -60,6 +60,52 @@ struct MaskTable {
   bool binary = false;
 };
 
+// FNV-1a over the words of m[0, n) in 8 interleaved lanes (independent
+// multiply chains), the lanes folded by one more FNV round each
+uint64_t fnv8(const double *m, long long n) {
+  uint64_t lane[8];
+  for (int j = 0; j < 8; ++j) lane[j] = 1469598103934665603ull + (uint64_t)j;
+  long long k = 0;
+  for (; k + 8 <= n; k += 8) {
+    uint64_t bits[8];
+    std::memcpy(bits, m + k, 64);
+    for (int j = 0; j < 8; ++j) lane[j] = (lane[j] ^ bits[j]) * 1099511628211ull;
+  }
+  for (; k < n; ++k) {
+    uint64_t bits;
+    std::memcpy(&bits, m + k, 8);
+    lane[0] = (lane[0] ^ bits) * 1099511628211ull;
+  }
+  uint64_t h = 1469598103934665603ull;
+  for (int j = 0; j < 8; ++j) h = (h ^ lane[j]) * 1099511628211ull;
+  return h;
+}
+
+// Hash of a whole mask: fixed chunks hashed on up to 8 host threads (the
+// scan is bound by one core's memory bandwidth), folded in chunk order, so
+// the value does not depend on the thread count.
+uint64_t mask_hash(const double *m, long long n) {
+  constexpr int kChunks = 8;
+  uint64_t part[kChunks];
+  const long long per = (n + kChunks - 1) / kChunks;
+  auto run = [&](int c) {
+    const long long a = std::min(n, c * per), b = std::min(n, a + per);
+    part[c] = fnv8(m + a, b - a);
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  if (n < (1LL << 20) || hw < 2) {
+    for (int c = 0; c < kChunks; ++c) run(c);
+  } else {
+    std::vector<std::thread> th;
+    for (int c = 1; c < kChunks; ++c) th.emplace_back(run, c);
+    run(0);
+    for (auto &t : th) t.join();
+  }
+  uint64_t h = 1469598103934665603ull;
+  for (int c = 0; c < kChunks; ++c) h = (h ^ part[c]) * 1099511628211ull;
+  return h;
+}
+
 struct MaskQ {
   const double *mask;
   int W, H;
@@ -74,12 +120,7 @@ struct MaskQ {
   MaskQ(const double *m, int w, int h) : mask(m), W(w), H(h), binary(true), sat(table().sat) {
     MaskTable &t = table();
     const long long n = (long long)W * H;
-    uint64_t hs = 1469598103934665603ull;  // FNV-1a over the 64-bit words
-    for (long long k = 0; k < n; ++k) {
-      uint64_t bits;
-      std::memcpy(&bits, m + k, 8);
-      hs = (hs ^ bits) * 1099511628211ull;
-    }
+    const uint64_t hs = mask_hash(m, n);
     if (t.W == W && t.H == H && t.hash == hs && !t.sat.empty()) {
       binary = t.binary;
       return;
@@ -146,6 +187,32 @@ int mark_edge(const HMesh &m, const MaskQ &mq, double min_size, std::vector<int>
   return OK;
 }
 
+// Sort (edge key, occurrence) pairs by key, ties in occurrence order: the
+// pairs arrive in occurrence order, so a stable LSD radix sort on the two
+// node numbers (each below nn + 1) gives the order of sorting the pairs.
+void sort_edges(std::vector<std::pair<uint64_t, int>> &ed, size_t nn) {
+  int bits = 1;
+  while (((size_t)1 << bits) <= nn + 1) ++bits;
+  const int digit = 11, R = 1 << digit;
+  std::vector<std::pair<uint64_t, int>> tmp(ed.size());
+  std::vector<size_t> cnt(R);
+  // low node (bits 0..31) then high node (bits 32..63), digit by digit
+  for (int half = 0; half < 2; ++half)
+    for (int lo = 0; lo < bits; lo += digit) {
+      const int sh = 32 * half + lo;
+      std::fill(cnt.begin(), cnt.end(), 0);
+      for (const auto &v : ed) ++cnt[(v.first >> sh) & (R - 1)];
+      size_t sum = 0;
+      for (int d = 0; d < R; ++d) {
+        const size_t c = cnt[d];
+        cnt[d] = sum;
+        sum += c;
+      }
+      for (const auto &v : ed) tmp[cnt[(v.first >> sh) & (R - 1)]++] = v;
+      ed.swap(tmp);
+    }
+}
+
 // provideGeometricData.m: edges of the irregular triples (column by column)
 // then of the elements, sorted unique; inverse maps per triple / element
 struct Geo {
@@ -168,7 +235,7 @@ void geometric(const HMesh &m, Geo &g) {
   for (int c = 0; c < 4; ++c)
     for (size_t r = 0; r < ne; ++r)
       ed.push_back({k2(m.el[r][c], m.el[r][(c + 1) % 4]), (int)(n3 + c * ne + r)});
-  std::sort(ed.begin(), ed.end());
+  sort_edges(ed, m.x.size());
   std::vector<int> ie(ed.size());
   g.e2n.clear();
   for (size_t k = 0; k < ed.size(); ++k) {
@@ -291,6 +358,42 @@ void qrefine(HMesh &m, const std::vector<int> &marked) {
 
 }  // namespace
 
+// Open-addressing table of nonzero 64-bit keys -> int (initially -1), for the
+// hanging-node lookups of qt_generate (a few thousand keys, ~10^5 probes).
+struct FlatMap {
+  std::vector<uint64_t> k;
+  std::vector<int> v;
+  size_t mask;
+  explicit FlatMap(size_t n) {
+    size_t cap = 16;
+    while (cap < 2 * n + 16) cap <<= 1;
+    k.assign(cap, 0);
+    v.assign(cap, -1);
+    mask = cap - 1;
+  }
+  static size_t mix(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    return (size_t)x;
+  }
+  void insert(uint64_t key) {
+    for (size_t i = mix(key) & mask;; i = (i + 1) & mask) {
+      if (k[i] == key) return;
+      if (k[i] == 0) {
+        k[i] = key;
+        return;
+      }
+    }
+  }
+  int *find(uint64_t key) {
+    for (size_t i = mix(key) & mask;; i = (i + 1) & mask) {
+      if (k[i] == key) return &v[i];
+      if (k[i] == 0) return nullptr;
+    }
+  }
+};
+
 int qt_generate(int n0, const double *coords, int ne0, const int32_t *elems, const double *mask,
                 int W, int H, double step, int min_size, aldic_qt_mesh &out) {
   ALDIC_CHECK(n0 >= 4 && ne0 >= 1 && coords && elems && mask && W > 0 && H > 0 && step > 0 &&
@@ -339,18 +442,17 @@ int qt_generate(int n0, const double *coords, int ne0, const int32_t *elems, con
     return ((unsigned long long)(unsigned)a << 35) ^ ((unsigned long long)(unsigned)b << 3) ^
            (unsigned long long)pi;
   };
-  std::unordered_map<unsigned long long, int> first;
-  first.reserve(8 * m.irr.size() + 16);
+  FlatMap first(8 * m.irr.size());
   for (const auto &r : m.irr)
-    for (int pi = 0; pi < 8; ++pi) first.emplace(key(r[0], r[1], pi), -1);
+    for (int pi = 0; pi < 8; ++pi) first.insert(key(r[0], r[1], pi));
   for (int pi = 0; pi < 8; ++pi)
     for (size_t e = 0; e < ne; ++e) {
-      auto it = first.find(key(m.el[e][pairs[pi][0]], m.el[e][pairs[pi][1]], pi));
-      if (it != first.end() && it->second < 0) it->second = (int)e;
+      int *v = first.find(key(m.el[e][pairs[pi][0]], m.el[e][pairs[pi][1]], pi));
+      if (v && *v < 0) *v = (int)e;
     }
   for (const auto &r : m.irr)
     for (int pi = 0; pi < 8; ++pi) {
-      const int e = first[key(r[0], r[1], pi)];
+      const int e = *first.find(key(r[0], r[1], pi));
       if (e >= 0) E[e][pairs[pi][2]] = r[2];
     }
   // funMarkInside.m: drop elements less than half inside the mask
