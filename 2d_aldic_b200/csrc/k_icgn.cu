@@ -588,7 +588,9 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 }
 
 template <typename Real, bool SUB>
-__global__ void __launch_bounds__(WARPS * 32, sizeof(Real) == 4 ? (SUB ? 4 : 3) : 2) k_icgn(Args a) {
+// FP32: 64 registers (4 CTAs, 32 warps per SM) -- the extra resident warps
+// hide more gather latency than the register spills cost
+__global__ void __launch_bounds__(WARPS * 32, sizeof(Real) == 4 ? 4 : 2) k_icgn(Args a) {
   __shared__ double Lsh[WARPS][WS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   while (true) {
