@@ -190,6 +190,31 @@ def test_subpb1_matches_oracle(aldic, ctx, oracle, plain, prec):
     assert du < (1e-8 if prec == "fp64" else 1e-3), du
 
 
+def test_icgn_fp32_same_through_set_fields(aldic, ctx, oracle, plain):
+    """The FP64-field route of the MATLAB-signature wrappers (aldic_set_fields,
+    as LocalICGN/funICGN/Subpb1 load ImgRef, ImgDef and Df) feeds the FP32
+    IC-GN the same images as aldic_set_ref/aldic_set_def: given the context's
+    own normalised images and gradients, the results are bit-identical, also
+    after a second call that replaces only the deformed image."""
+    wl = plain["wl"]
+    coords, U0, nx, ny = _mesh(oracle, plain)
+    ctx.set_ref(plain["f"])
+    ctx.set_def(plain["g"])
+    H, W = plain["f"].shape
+    fn, gn, dx, dy, _ = ctx.get_images(W, H)
+    U, F, it, _ = aldic.local_icgn(ctx, coords, U0, wl.winsize, wl.tol, aldic.FP32)
+    c2 = aldic.Context(0)
+    try:
+        c2.set_fields(fn, fn, dx, dy)   # deformed image first set to the reference
+        c2.set_fields(g=gn)             # then replaced on its own
+        U2, F2, it2, _ = aldic.local_icgn(c2, coords, U0, wl.winsize, wl.tol, aldic.FP32)
+    finally:
+        c2.close()
+    np.testing.assert_array_equal(it2, it)
+    np.testing.assert_array_equal(U2, U)
+    np.testing.assert_array_equal(F2, F)
+
+
 # ------------------------------------------------------------------ post + grid solvers
 def test_grid_kernels_match_oracle(aldic, ctx, oracle):
     import ctypes as C
