@@ -721,17 +721,20 @@ __global__ void k_inpaint_load(int M, int N, int nf, const double *__restrict__ 
       const bool kn = known(k);
       mask[f * n + k] = !kn;
       double bv;
+      int kc = 0;  // known neighbours of an unknown entry
       if (kn) {
         bv = vals[k * stride + f];
       } else {
         bv = 0.0;
-        if (i > 0 && known(k - 1)) bv += vals[(k - 1) * stride + f];
-        if (i < M - 1 && known(k + 1)) bv += vals[(k + 1) * stride + f];
-        if (j > 0 && known(k - M)) bv += vals[(k - M) * stride + f];
-        if (j < N - 1 && known(k + M)) bv += vals[(k + M) * stride + f];
+        if (i > 0 && known(k - 1)) { bv += vals[(k - 1) * stride + f]; ++kc; }
+        if (i < M - 1 && known(k + 1)) { bv += vals[(k + 1) * stride + f]; ++kc; }
+        if (j > 0 && known(k - M)) { bv += vals[(k - M) * stride + f]; ++kc; }
+        if (j < N - 1 && known(k + M)) { bv += vals[(k + M) * stride + f]; ++kc; }
       }
       b[f * n + k] = bv;
-      x[f * n + k] = kn ? bv : 0.0;
+      // an unknown entry starts from the mean of its known neighbours (the
+      // solution itself for an isolated one), else from 0
+      x[f * n + k] = kn ? bv : (kc > 0 ? bv / kc : 0.0);
     }
   }
 }
