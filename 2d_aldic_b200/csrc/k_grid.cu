@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
   for (int f = 0; f < NR; ++f) {
     const double bt = A.beta[f];
     for (long long k = tid0; k < n; k += stride) {
-      const int i = (int)(k % M), j = (int)(k / M);
+      const int j = (int)k / M, i = (int)k - j * M;  // n < 2^31 (checked at launch)
       const long long o = f * n + k;
       const double rv = A.b[o] - op_apply<OP>(A, bt, i, j, k, f, X + f * n);
       const double dinv = 1.0 / op_diag<OP>(A, bt, i, j, k, f);
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
     const double bt = A.beta[f];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     for (long long k = tid0; k < n; k += stride) {
-      const int i = (int)(k % M), j = (int)(k / M);
+      const int j = (int)k / M, i = (int)k - j * M;  // n < 2^31 (checked at launch)
       const long long o = f * n + k;
       const double wv = op_apply<OP>(A, bt, i, j, k, f, Uv + f * n);
       Wv[o] = wv;
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
       }
       if (live[0] || (G2 > 1 && live[G2 - 1])) {
         for (long long k = tid0; k < n; k += stride) {
-          const int i = (int)(k % M), j = (int)(k / M);
+          const int j = (int)k / M, i = (int)k - j * M;  // n < 2^31 (checked at launch)
           double nv[G2], zo[G2], qo[G2], so[G2], po[G2], mo[G2], wo[G2], uo[G2], ro[G2], xo[G2],
               di[G2];
           // inpainting: a known entry is an identity row whose r, u, w, m and
@@ -895,6 +895,7 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
              const double *beta_each, const double *ata) {
   ALDIC_CHECK(nrhs >= 1 && nrhs <= MAXRHS, E_ARG, "grid_pcg: 1..12 right-hand sides");
   const long long n = (long long)M * N;
+  ALDIC_CHECK(n < (1LL << 31), E_ARG, "grid_pcg: more than 2^31 nodes");
   int dev = 0, sms = 148, per = 1;
   ALDIC_CUDA(cudaGetDevice(&dev));
   ALDIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
