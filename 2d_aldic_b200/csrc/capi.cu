@@ -80,6 +80,7 @@ struct aldic_ctx {
   bool prepared = false;  // fields given by aldic_set_fields (no normalisation)
   DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
   DevBuf g4;  // row runs of g32 (float4 per pixel) read by the FP32 IC-GN sampler
+  DevBuf gxy;  // (gx32, gy32) pairs (float2 per pixel) read by the FP32 IC-GN
   DevBuf stats;   // double[4]: mean_f std_f mean_g std_g
   DevBuf isums;   // u64[2]
   DevBuf part;    // double[1024]
@@ -251,6 +252,7 @@ IcgnImages images_of(aldic_ctx *c) {
   IcgnImages im;
   im.f32 = c->f32.as<float>(); im.g32 = c->g32.as<float>();
   im.g4 = c->g4.as<float4>();
+  im.gxy = c->gxy.as<float2>();
   im.gx32 = c->gx32.as<float>(); im.gy32 = c->gy32.as<float>();
   im.f64 = c->f64.as<double>(); im.g64 = c->g64.as<double>();
   im.gx64 = c->gx64.as<double>(); im.gy64 = c->gy64.as<double>();
@@ -380,7 +382,7 @@ int aldic_ctx_destroy(aldic_ctx *c) {
   for (int k = 0; k < 8; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   DevBuf *bufs[] = {&c->f_raw, &c->g_raw, &c->f64, &c->g64, &c->f32, &c->g32, &c->gx64,
-                    &c->gy64, &c->gx32, &c->gy32, &c->g4, &c->mask, &c->stats, &c->isums, &c->part,
+                    &c->gy64, &c->gx32, &c->gy32, &c->g4, &c->gxy, &c->mask, &c->stats, &c->isums, &c->part,
                     &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr,
                     &c->hist};
   for (DevBuf *b : bufs) b->release();
@@ -420,6 +422,7 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
   if ((rc = c->g4.ensure(sizeof(float4) * n))) return rc;
+  if ((rc = c->gxy.ensure(sizeof(float2) * n))) return rc;
   if ((rc = c->f_raw.ensure(es * n))) return rc;
   if ((rc = c->g_raw.ensure(es * n))) return rc;
   if (c->dtype != dtype || c->W != W || c->H != H) c->have_def = false;
@@ -451,6 +454,8 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     return rc;
   if ((rc = gradient(c->f64.as<double>(), dmask, W, H, c->gx64.as<double>(), c->gy64.as<double>(),
                      c->gx32.as<float>(), c->gy32.as<float>(), c->stream)))
+    return rc;
+  if ((rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
     return rc;
   c->have_ref = true;
   return finish(c, true);
@@ -554,6 +559,7 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
   if ((rc = c->g4.ensure(sizeof(float4) * n))) return rc;
+  if ((rc = c->gxy.ensure(sizeof(float2) * n))) return rc;
   if (first) c->have_def = false;
   c->W = W; c->H = H; c->dtype = 3;
   c->prepared = true;
@@ -567,6 +573,9 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     k_to_f32<<<1184, 256, 0, c->stream>>>(d64[k]->as<double>(), d32[k]->as<float>(), n);
   }
   if (gimg && (rc = row_runs(c->g32.as<float>(), W, H, c->g4.as<float4>(), c->stream))) return rc;
+  if ((dfdx || dfdy) &&
+      (rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
+    return rc;
   if (f) ALDIC_CUDA(cudaMemcpyAsync(c->f_raw.p, c->f64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
   if (gimg) ALDIC_CUDA(cudaMemcpyAsync(c->g_raw.p, c->g64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
   // the normalised fields have mean 0 in the units the search pads with

@@ -61,15 +61,36 @@ __device__ __forceinline__ bool subset_ok(const IcgnImages &im, double x0, doubl
 template <typename Real> struct Img;
 template <> struct Img<float> {
   static __device__ __forceinline__ const float *f(const IcgnImages &m) { return m.f32; }
-  static __device__ __forceinline__ const float *g(const IcgnImages &m) { return m.g32; }
-  static __device__ __forceinline__ const float *gx(const IcgnImages &m) { return m.gx32; }
-  static __device__ __forceinline__ const float *gy(const IcgnImages &m) { return m.gy32; }
 };
 template <> struct Img<double> {
   static __device__ __forceinline__ const double *f(const IcgnImages &m) { return m.f64; }
-  static __device__ __forceinline__ const double *g(const IcgnImages &m) { return m.g64; }
-  static __device__ __forceinline__ const double *gx(const IcgnImages &m) { return m.gx64; }
-  static __device__ __forceinline__ const double *gy(const IcgnImages &m) { return m.gy64; }
+};
+
+// The reference gradients of a pixel.  FP32 Subpb1 reads the (gx, gy) pair
+// in one 8-byte load (its loop is L1-throughput bound); FP32 IC-GN (measured
+// faster with two 4-byte loads) and FP64 read the two fields.
+template <typename Real, bool PAIR> struct Grad;
+template <> struct Grad<float, true> {
+  const float2 *p;
+  __device__ __forceinline__ explicit Grad(const IcgnImages &m) : p(m.gxy) {}
+  __device__ __forceinline__ void at(int k, float *fx, float *fy) const {
+    const float2 t = __ldg(p + k);
+    *fx = t.x;
+    *fy = t.y;
+  }
+};
+template <typename Real> struct GradFields {
+  const Real *x, *y;
+  __device__ __forceinline__ void at(int k, Real *fx, Real *fy) const {
+    *fx = x[k];
+    *fy = y[k];
+  }
+};
+template <> struct Grad<float, false> : GradFields<float> {
+  __device__ __forceinline__ explicit Grad(const IcgnImages &m) : GradFields<float>{m.gx32, m.gy32} {}
+};
+template <bool PAIR> struct Grad<double, PAIR> : GradFields<double> {
+  __device__ __forceinline__ explicit Grad(const IcgnImages &m) : GradFields<double>{m.gx64, m.gy64} {}
 };
 
 // Cholesky of the 6x6 SPD matrix (lower, packed row-wise in L[21]); inv[i]
@@ -280,8 +301,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   }
   const Real *fI = Img<Real>::f(im);
   const auto *gI = sample_src(im, Real(0));
-  const Real *gxI = Img<Real>::gx(im);
-  const Real *gyI = Img<Real>::gy(im);
+  const Grad<Real, SUB> grad(im);
   const int W = im.W;
   // One fused pass over the subset: the masked-pixel count of funICGN.m:54,
   // the Hessian sums of :67-79, and -- with a shift c (the subset's centre
@@ -330,7 +350,8 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     for (int p = lane; p < npx; p += 32) {
       Real rx, ry;
       const int k = base + pm.at(p, &rx, &ry);
-      const Real fx = gxI[k], fy = gyI[k];
+      Real fx, fy;
+      grad.at(k, &fx, &fy);
       const Real d = fI[k] - c;
       cnt += fx == (Real)0;
       a1 += d;
@@ -507,7 +528,8 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         const Real d = sample_minus(gI, W, cx, cy, ru - fu, rv - fv, cg);
         s1 += d;
         s2r += d * d;
-        const Real fx = gxI[k], fy = gyI[k];
+        Real fx, fy;
+        grad.at(k, &fx, &fy);
         const Real ax = fx * d, ay = fy * d;
         t[4] += ax;
         t[5] += ay;

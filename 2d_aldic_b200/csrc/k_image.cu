@@ -155,6 +155,20 @@ int row_runs(const float *g, int W, int H, float4 *q, cudaStream_t st) {
   return OK;
 }
 
+// q[i] = (gx[i], gy[i]): the two FP32 gradients of a pixel in one 8-byte load
+__global__ void k_pair(const float *__restrict__ gx, const float *__restrict__ gy, long long n,
+                       float2 *__restrict__ q) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    q[i] = make_float2(gx[i], gy[i]);
+}
+
+int grad_pairs(const float *gx, const float *gy, long long n, float2 *q, cudaStream_t st) {
+  k_pair<<<1184, 256, 0, st>>>(gx, gy, n, q);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
 // ------------------------------------------------------------------ gradient
 __device__ __forceinline__ double grad7(const double *f, long long i, long long s) {
   const double c1 = 0.75, c2 = 3.0 / 20.0, c3 = 1.0 / 60.0;

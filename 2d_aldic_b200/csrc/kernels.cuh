@@ -17,6 +17,8 @@ int gradient(const double *f, const double *mask, int W, int H, double *gx64, do
              float *gx32, float *gy32, cudaStream_t st);
 // q[i] = g[i .. i+3] within the row (zero past its end), W*H float4
 int row_runs(const float *g, int W, int H, float4 *q, cudaStream_t st);
+// q[i] = (gx[i], gy[i]), n float2
+int grad_pairs(const float *gx, const float *gy, long long n, float2 *q, cudaStream_t st);
 int interp_f64(const double *F, long long M, long long N, long long P, const double *X,
                const double *Y, long long n, double *Z, cudaStream_t st);
 int interp_f32(const float *F, long long M, long long N, long long P, const float *X,
@@ -41,6 +43,7 @@ int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, co
 struct IcgnImages {
   const float *f32, *g32, *gx32, *gy32;
   const float4 *g4;  // row runs of g32 (row_runs): the FP32 sampler's stencil rows
+  const float2 *gxy;  // (gx32, gy32) pairs (grad_pairs) read by the FP32 IC-GN
   const double *f64, *g64, *gx64, *gy64;
   int W, H;
 };
