@@ -264,7 +264,9 @@ def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winste
     ctx = ctx or _ctx_for(f, g)
     H, W = f.shape
     if _dtype_code(f) in (U8, U16):
-        ctx.set_ref(f)
+        # the reference searches images normalised over gridxyROIRange (main_ALDIC.m
+        # Section 2): the ROI statistics set the value the correlation pads with
+        ctx.set_ref(f, roi=(int(gridx[0]), int(gridx[-1]), int(gridy[0]), int(gridy[-1])))
         ctx.set_def(g)
     else:
         ctx.set_fields(_prep(f), _prep(g), _zeros_like_img(f), _zeros_like_img(f))
@@ -300,7 +302,9 @@ def funIntegerSearchMg(f, g, gridx, gridy, winsize, winstepsize, *varargin,
     ctx = ctx or _ctx_for(f, g)
     H, W = f.shape
     if _dtype_code(f) in (U8, U16):
-        ctx.set_ref(f)
+        # the reference searches images normalised over gridxyROIRange (main_ALDIC.m
+        # Section 2): the ROI statistics set the value the correlation pads with
+        ctx.set_ref(f, roi=(int(gridx[0]), int(gridx[-1]), int(gridy[0]), int(gridy[-1])))
         ctx.set_def(g)
     else:
         ctx.set_fields(_prep(f), _prep(g), _zeros_like_img(f), _zeros_like_img(f))
@@ -929,9 +933,11 @@ class ALDICQuadtree:
 
     def __init__(self, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3, tol2=1e-2,
                  min_size=2, precision=FP32, subsets="uniform", device=None,
-                 ctx: Context | None = None):
+                 ctx: Context | None = None, gridx=None, gridy=None):
         self.ctx = ctx or default_context(device)
         self.w, self.step, self.search = int(winsize), int(step), int(search)
+        self.gridx = None if gridx is None else (int(gridx[0]), int(gridx[-1]))
+        self.gridy = None if gridy is None else (int(gridy[0]), int(gridy[-1]))
         self.tol, self.mu, self.n_admm, self.tol2 = float(tol), float(mu), int(n_admm), float(tol2)
         self.min_size, self.precision, self.subsets = int(min_size), int(precision), subsets
         self.mesh = None
@@ -944,9 +950,11 @@ class ALDICQuadtree:
         ctx, w, step = self.ctx, self.w, self.step
         f, g, mask = self.f, self.g, self.mask
         H, W = f.shape
+        gx = self.gridx or (1, W)                 # DICpara.gridxyROIRange
+        gy = self.gridy or (1, H)
         t0 = time.perf_counter()
         # Section 3: integer search on the uniform grid, MeshSetUp, Init
-        x, y, u, v, _ = funIntegerSearch(f, g, self.search, (1, W), (1, H), w, step, 0, step,
+        x, y, u, v, _ = funIntegerSearch(f, g, self.search, gx, gy, w, step, 0, step,
                                          qfactors=False, ctx=ctx)
         xi, yi = np.asarray(x, int), np.asarray(y, int)
         hole = mask[yi - 1, xi - 1] == 0                         # IntegerSearch.m:68-73
@@ -956,7 +964,7 @@ class ALDICQuadtree:
         U0u = Init(u, v, None, x, y, 0)
         ny, nx = u.shape
         t_search = time.perf_counter()
-        ctx.set_ref(f, mask=mask)
+        ctx.set_ref(f, roi=(gx[0], gx[1], gy[0], gy[1]), mask=mask)
         ctx.set_def(g)
         if self.mesh is not None:
             self.mesh.close()

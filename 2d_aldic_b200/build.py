@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -19,7 +20,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libaldic_b200.so")
 ROOT = os.path.dirname(HERE)
 
-SOURCES = ["k_image.cu", "k_search.cu", "k_searchmg.cu", "k_icgn.cu", "k_grid.cu", "qt.cu", "k_gemm.cu", "cnn.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["k_image.cu", "k_search.cu", "k_searchmg.cu", "k_icgn.cu", "k_grid.cu", "fdm.cu", "qt.cu", "k_gemm.cu", "cnn.cu", "capi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]
@@ -44,16 +45,23 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
     os.makedirs(OBJ, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".cuh")]
     headers.append(os.path.join(ROOT, "include", "aldic_b200.h"))
-    objs = []
+    objs, jobs = [], []
     for s in SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(OBJ, s.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [src] + headers + [__file__]):
-            cmd = [nvcc(), *ARCH, *FLAGS, *(extra or []), "-c", src, "-o", obj]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            jobs.append([nvcc(), *ARCH, *FLAGS, *(extra or []), "-c", src, "-o", obj])
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    # one nvcc per translation unit, as many at once as there are host cores
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(run, c) for c in jobs]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-lpthread",
                "-ldl"]

@@ -41,8 +41,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="uniform2048")
-    ap.add_argument("--cpu-crop", type=int, default=1536,
-                    help="side of the image crop the CPU baseline runs on")
+    ap.add_argument("--cpu-crop", type=int, default=0,
+                    help="side of a top-left image crop for the CPU baseline and the reference "
+                         "arm (0: the whole workload image, the default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--mg-only", action="store_true",
@@ -109,19 +110,25 @@ class Clocks:
 # ------------------------------------------------------------------ reference arm
 def oracle_sample(wl, crop: int):
     f, g = wl.images()
+    if crop <= 0 or crop >= max(wl.W, wl.H):
+        return f, g, None
     c = min(crop, wl.W, wl.H)
     return f[:c, :c].copy(), g[:c, :c].copy(), c
 
 
-def run_oracle_frames(oracle, wl, f, g, k):
-    times, conv = [], 0
+def sample_name(wl, c):
+    return f"the whole {wl.W}x{wl.H} frame" if c is None else f"a {c}x{c} top-left crop"
+
+
+def run_oracle_frames(oracle, wl, f, g, k, keep=False):
+    times, conv, r = [], 0, None
     for _ in range(k):
         t0 = time.perf_counter()
         r = oracle.frame(f, g, wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=wl.n_admm)
         times.append(time.perf_counter() - t0)
         it = r["iters_icgn"]
         conv = int(((it >= 1) & (it <= 100)).sum())
-    return times, conv
+    return (times, conv, r) if keep else (times, conv)
 
 
 def reference_arm(args, rank):
@@ -136,14 +143,15 @@ def reference_arm(args, rank):
     times, conv = run_oracle_frames(oracle, wl, f, g, args.steps)
     tot = sum(times)
     value = conv * args.steps / tot
-    sample = (f"{c}x{c} top-left crop of the {args.workload} workload ({conv} converged subsets "
+    sample = (f"{sample_name(wl, c)} of the {args.workload} workload ({conv} converged subsets "
               f"per frame), full frame pipeline of the FP64 CPU restatement per step")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "frames_per_s": args.steps / tot,
-        "config": {"workload": f"{args.workload} (CPU sample {c}x{c})", "threads": oracle.get_threads()},
+        "config": {"workload": args.workload if c is None else f"{args.workload} (CPU sample {c}x{c})",
+                   "threads": oracle.get_threads()},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -163,13 +171,34 @@ def icgn_bytes(iters: np.ndarray, winsize: int) -> float:
     return float((12 * N * active + 4 * N * k + 224 * active).sum())
 
 
+ICGN_SOURCES = ("2d_aldic_b200/csrc/k_icgn.cu", "2d_aldic_b200/csrc/kernels.cuh",
+                "2d_aldic_b200/csrc/aldic_internal.cuh")
+
+
+def icgn_source_digest() -> str:
+    """sha1 over the IC-GN kernel's source files: the ncu summary records the
+    digest of the build it measured, so a summary of an older kernel is not
+    reported as this one's traffic."""
+    import hashlib
+    h = hashlib.sha1()
+    for rel in ICGN_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:12]
+
+
 def icgn_traffic_from_profile():
     """DRAM bytes (read + write) of one IC-GN launch from the committed ncu
-    summary of this workload (profiles/k_icgn_uniform2048.md), or None."""
+    summary of this workload (profiles/k_icgn_uniform2048.md) when the
+    summary's "source digest" line matches the kernel sources being run;
+    otherwise None (the traffic of this build is unmeasured)."""
     import re
     try:
         text = open(os.path.join(ROOT, "profiles", "k_icgn_uniform2048.md")).read()
     except OSError:
+        return None
+    m = re.search(r"source digest: `([0-9a-f]+)`", text)
+    if not m or m.group(1) != icgn_source_digest():
         return None
     sec = text.split("#### `k_icgn<float, 0>`", 1)
     if len(sec) < 2:
@@ -684,15 +713,22 @@ def main():
 
     # ---------------- CPU baseline (rank 0, N = 1 only)
     cpu = None
+    acc_oracle = {}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         oracle.set_threads(host_cores())
         fs, gs, c = oracle_sample(wl, args.cpu_crop)
-        times, cconv = run_oracle_frames(oracle, wl, fs, gs, 1)
+        times, cconv, ro = run_oracle_frames(oracle, wl, fs, gs, 1, keep=True)
         cpu = {"value": cconv / times[0], "unit": UNIT, "cores": oracle.get_threads(),
                "kind": "port",
-               "sample": f"one frame of the FP64 CPU restatement on a {c}x{c} crop of the "
+               "sample": f"one frame of the FP64 CPU restatement on {sample_name(wl, c)} of the "
                          f"workload ({cconv} converged subsets, {times[0]:.1f} s)"}
+        if c is None:
+            # the metric's accuracy: the timed FP32 frame against the FP64 oracle frame
+            dU = U32 - ro["U"]
+            acc_oracle = {"rms_px_vs_fp64_oracle": float(np.sqrt(np.mean(dU ** 2))),
+                          "max_px_vs_fp64_oracle": float(np.abs(dU).max()),
+                          "fp64_gpu_max_px_vs_oracle": float(np.abs(r64["U"] - ro["U"]).max())}
 
     if rank == 0:
         mst = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
@@ -702,7 +738,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 sampling/residuals, f64 sums+solves", "data": "synthetic",
             "frames_per_s": frames_per_s,
-            "accuracy": {"rms_px_vs_fp64_pipeline": rms_fp64, "rms_px_vs_truth": rms_truth,
+            "accuracy": {**acc_oracle, "rms_px_vs_fp64_pipeline": rms_fp64,
+                         "rms_px_vs_truth": rms_truth,
                          "fp64_frame_ms": r64["stats"]["t_stage_ms"]["frame"]},
             "config": {"workload": "uniform2048: 2048x2048 u8 speckle, 130k dots (seed 1), "
                                    "u=2sin(2pi y/256), v=1.5cos(2pi x/256), noise 2; subset 32, "

@@ -10,7 +10,8 @@ library's FD path.
     interior (M-2) x (N-2) nodes (funFDNeumannBCInd.m), border nodes keep U;
     scipy's sparse direct solve stands in for MATLAB's backslash
   * frame_fd       one frame of main_ALDIC.m with DICpara.Subpb2FDOrFEM = 1,
-    built from the C oracle's search / IC-GN / Subpb1 pieces (smoothing off)
+    built from the C oracle's search / IC-GN / Subpb1 pieces, with the
+    reference's ROI and (optionally) its in-loop smoothing
 """
 from __future__ import annotations
 
@@ -77,15 +78,23 @@ def _select_beta_fd(betas, e1, e2, h):
     return betas[k]
 
 
-def frame_fd(f_raw, g_raw, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3):
-    """main_ALDIC.m Sections 3-6 with the FD Subproblem 2 (smoothing off)."""
+def frame_fd(f_raw, g_raw, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3, gridx=None,
+             gridy=None, smooth=False):
+    """main_ALDIC.m Sections 3-6 with the FD Subproblem 2.  gridx/gridy is
+    DICpara.gridxyROIRange (funNormalizeImg statistics and the search grid);
+    smooth=True adds the reference's funSmoothDisp/funSmoothStrain calls
+    (main_ALDIC.m:233 on FSubpb1, :321 on FSubpb2, and in every ADMM step
+    :381 on USubpb1 after its save, :400 on USubpb2, :408 on FSubpb2)."""
     import oracle as O
     f_raw, g_raw = np.asarray(f_raw), np.asarray(g_raw)
     H, W = f_raw.shape
-    fn, _, _ = O.normalize(f_raw)
-    gn, mg, _ = O.normalize(g_raw)
+    gx = tuple(gridx) if gridx is not None else (1, W)
+    gy = tuple(gridy) if gridy is not None else (1, H)
+    roi = (gx[0], gx[1], gy[0], gy[1])
+    fn, _, _ = O.normalize(f_raw, roi)
+    gn, mg, _ = O.normalize(g_raw, roi)
     dfdx, dfdy = O.gradient(fn)
-    x, y, u, v, cc, _ = O.int_search(f_raw, g_raw, mg, (1, W), (1, H), winsize, step, (search, search))
+    x, y, u, v, cc, _ = O.int_search(f_raw, g_raw, mg, gx, gy, winsize, step, (search, search))
     N, M = u.shape
     coords = np.stack([x.reshape(-1), y.reshape(-1)], 1)
     ug = O.inpaint_springs(M, N, u.reshape(-1))
@@ -93,8 +102,13 @@ def frame_fd(f_raw, g_raw, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3):
     U0 = np.empty(2 * M * N)
     U0[0::2], U0[1::2] = ug, vg
     U1, F1, it, H21 = O.icgn_batch(fn, gn, dfdx, dfdy, coords, U0, winsize, tol)
-    U1, F1, _ = O.localicgn_post(M, N, it, U1, F1)
+    U1, F1, nbad = O.localicgn_post(M, N, it, U1, F1)
     n = M * N
+
+    def sm(a, nf):
+        return O.smooth_fields(M, N, a, nf) if smooth else a
+
+    F1 = sm(F1, 4)
     ud, vd = np.zeros(4 * n), np.zeros(2 * n)
     betas = np.array([1e-3, np.sqrt(1e-5), 1e-2, np.sqrt(1e-3), 1e-1, np.sqrt(1e-1)]) * step * step * mu
     e1, e2 = [], []
@@ -105,7 +119,7 @@ def frame_fd(f_raw, g_raw, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3):
         e2.append(np.linalg.norm(F1 - F2))
     beta = _select_beta_fd(betas, e1, e2, step)
     U2 = subpb2_fd(M, N, step, beta, mu, U1, F1, ud, vd)
-    F2 = fd_strain(M, N, step, U2)
+    F2 = sm(fd_strain(M, N, step, U2), 4)
     iF, iU = interior(M, N)
     ud = np.zeros(4 * n)
     vd = np.zeros(2 * n)
@@ -120,9 +134,11 @@ def frame_fd(f_raw, g_raw, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3):
         F1 = F2.copy()
         upd2.append(np.linalg.norm(U1old - U1) / np.sqrt(2 * n))
         U1old = U1.copy()
-        U2 = subpb2_fd(M, N, step, beta, mu, U1, F1, ud, vd)
-        F2 = fd_strain(M, N, step, U2)
+        U1 = sm(U1, 2)
+        U2 = sm(subpb2_fd(M, N, step, beta, mu, U1, F1, ud, vd), 2)
+        F2 = sm(fd_strain(M, N, step, U2), 4)
         upd.append(np.linalg.norm(U2old - U2) / np.sqrt(2 * n))
         ud[iF] += (F2 - F1)[iF]
         vd[iU] += (U2 - U1)[iU]
-    return dict(M=M, N=N, U=U2, F=F2, beta=beta, update_y=upd, update_y2=upd2, iters_icgn=it)
+    return dict(M=M, N=N, U=U2, F=F2, beta=beta, update_y=upd, update_y2=upd2, iters_icgn=it,
+                bad_icgn=nbad)

@@ -429,7 +429,7 @@ def select_beta(betas, e1, e2):
 
 
 def frame(f_raw, g_raw, mask, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3, tol2=1e-2,
-          min_size=2, subsets="uniform"):
+          min_size=2, subsets="uniform", gridx=None, gridy=None):
     """One frame of main_ALDIC_Quadtree.m Sections 3-6 (ImgSeqNum 2) with
     the interactive outlier removal and the strain smoothing
     (DICpara.StrainSmoothness, regularizeNd) left out."""
@@ -437,10 +437,13 @@ def frame(f_raw, g_raw, mask, winsize, step, search, tol=1e-2, mu=1e-3, n_admm=3
     f_raw, g_raw = np.asarray(f_raw), np.asarray(g_raw)
     H, W = f_raw.shape
     mask = np.asarray(mask, np.float64)
-    fn, _, _ = O.normalize(f_raw)
-    gn, mg, _ = O.normalize(g_raw)
+    gx = tuple(gridx) if gridx is not None else (1, W)
+    gy = tuple(gridy) if gridy is not None else (1, H)
+    roi = (gx[0], gx[1], gy[0], gy[1])
+    fn, _, _ = O.normalize(f_raw, roi)                    # funNormalizeImg(Img, gridxyROIRange)
+    gn, mg, _ = O.normalize(g_raw, roi)
     dfdx, dfdy = O.gradient(fn, mask)
-    x, y, u, v, cc, _ = O.int_search(f_raw, g_raw, mg, (1, W), (1, H), winsize, step, (search, search))
+    x, y, u, v, cc, _ = O.int_search(f_raw, g_raw, mg, gx, gy, winsize, step, (search, search))
     hole = mask[y.astype(int) - 1, x.astype(int) - 1] == 0        # IntegerSearch.m:68-73
     u, v = np.where(hole, np.nan, u), np.where(hole, np.nan, v)
     ny, nx = u.shape
