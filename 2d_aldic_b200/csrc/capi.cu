@@ -88,6 +88,7 @@ struct aldic_ctx {
   DevBuf gw_vec, gw_part, gw_mask, gw_misc;
   long long gw_n = 0;
   GridWork gw{};
+  FdmBasis fdm;  // eigenbases of the uniform-grid Subproblem 2 operator (fdm.cu)
   DevBuf queue;
   // frame state
   DevBuf fr;  // one slab for all frame arrays
@@ -280,8 +281,8 @@ double springs_lam2(int M, int N) {
 }
 
 // PCG tolerances of the node-grid solves
-constexpr double kRtolFE = 1e-11, kRtolFit = 1e-11, kRtolInpaint = 1e-11;
-constexpr int kMaxitFE = 4000, kMaxitFit = 8000, kMaxitInpaint = 50000;
+constexpr double kRtolFit = 1e-11, kRtolInpaint = 1e-11;
+constexpr int kMaxitFit = 8000, kMaxitInpaint = 50000;
 
 }  // namespace
 
@@ -388,6 +389,7 @@ int aldic_ctx_destroy(aldic_ctx *c) {
   for (DevBuf *b : bufs) b->release();
   c->mg.release();
   c->sw.release();
+  c->fdm.release();
   c->arena.release();
   if (c->own_stream) cudaStreamDestroy(c->stream);
   cudaSetDevice(prev);
@@ -848,9 +850,10 @@ int aldic_subpb2(aldic_ctx *c, int M, int N, double step, double beta, double mu
       (rc = arg_in(c, udual, 4 * n, aud)) || (rc = arg_in(c, vdual, 2 * n, avd)) ||
       (rc = arg_out(c, Uhat, 2 * n, ao)))
     return rc;
+  if ((rc = fdm_ensure(c->fdm, FDM_FE, M, N, step, c->stream))) return rc;
   if ((rc = fe_rhs(c->gw, M, N, step, beta, mu, au.dev, af.dev, aud.dev, avd.dev, c->stream)))
     return rc;
-  if ((rc = grid_pcg(c->gw, OP_FE, M, N, 2, beta, mu, step, 0, kRtolFE, kMaxitFE, c->stream)))
+  if ((rc = fdm_solve(c->fdm, 2, c->gw.b, c->gw.x, c->gw.r, mu, beta, nullptr, nullptr, c->stream)))
     return rc;
   if ((rc = fe_store(c->gw, M, N, ao.dev, c->stream))) return rc;
   arg_back(c, ao);
@@ -1061,8 +1064,9 @@ int aldic_subpb2_fd(aldic_ctx *c, int M, int N, double step, double beta, double
       (rc = arg_in(c, udual, 4 * n, aud)) || (rc = arg_in(c, vdual, 2 * n, avd)) ||
       (rc = arg_out(c, Uhat, 2 * n, ao)))
     return rc;
+  if ((rc = fdm_ensure(c->fdm, FDM_FD, M - 2, N - 2, step, c->stream))) return rc;
   if ((rc = fd_rhs(c->gw, M, N, step, beta, mu, au.dev, af.dev, aud.dev, avd.dev, c->stream)) ||
-      (rc = grid_pcg(c->gw, OP_FD, M - 2, N - 2, 2, beta, mu, step, 0, kRtolFE, kMaxitFE, c->stream)) ||
+      (rc = fdm_solve(c->fdm, 2, c->gw.b, c->gw.x, c->gw.r, mu, beta, nullptr, nullptr, c->stream)) ||
       (rc = fd_store(c->gw, M, N, au.dev, ao.dev, c->stream)))
     return rc;
   arg_back(c, ao);
@@ -1411,11 +1415,9 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     return fd ? fd_rhs(c->gw, M, N, h, beta, mu, B.U1, B.F1, B.udual, B.vdual, st, beta_ptr, f0)
               : fe_rhs(c->gw, M, N, h, beta, mu, B.U1, B.F1, B.udual, B.vdual, st, beta_ptr, f0);
   };
+  // the direct fast-diagonalisation solve (fdm.cu; bases set up before capture)
   auto pcg = [&](int nr, const double *beta_ptr, const double *beta_each) {
-    return fd ? grid_pcg(c->gw, OP_FD, M - 2, N - 2, nr, 0, mu, h, 0, kRtolFE, kMaxitFE, st,
-                         beta_ptr, beta_each)
-              : grid_pcg(c->gw, OP_FE, M, N, nr, 0, mu, h, 0, kRtolFE, kMaxitFE, st, beta_ptr,
-                         beta_each);
+    return fdm_solve(c->fdm, nr, c->gw.b, c->gw.x, c->gw.r, mu, 0.0, beta_each, beta_ptr, st);
   };
   auto store = [&](int f0) {
     return fd ? fd_store(c->gw, M, N, B.U1, B.U2, st, f0) : fe_store(c->gw, M, N, B.U2, st, f0);
@@ -1592,6 +1594,10 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   ALDIC_CHECK(qp.init != ALDIC_INIT_GIVEN || c->have_given, E_STATE,
               "frame: ALDIC_INIT_GIVEN needs aldic_set_init on this node grid");
   if ((rc = ensure_grid_work(c, n))) return rc;
+  // Subproblem 2 eigenbases (host work, synchronises: before any capture)
+  if ((rc = p->subpb2_fd ? fdm_ensure(c->fdm, FDM_FD, M - 2, N - 2, (double)p->step, c->stream)
+                         : fdm_ensure(c->fdm, FDM_FE, M, N, (double)p->step, c->stream)))
+    return rc;
   // search work before any capture (a graph records its addresses)
   if (qp.init == ALDIC_INIT_SEARCH &&
       (rc = search_work_ensure(c->sw, c->W, c->H, M, N, p->search)))
@@ -1622,11 +1628,11 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   // the buffers the graph addresses
   char key[512];
   snprintf(key, sizeof key,
-           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p %p",
+           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p %p %p",
            c->W, c->H, c->dtype, p->winsize, p->step, p->search[0], p->search[1], gx[0], gx[1],
            gy[0], gy[1], node0[0], node0[1], M, N, p->tol, p->mu, p->beta, p->n_admm, p->precision,
            p->smooth, qp.init * 2 + (p->subpb2_fd != 0),
-           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p, c->sw.buf.p);
+           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p, c->sw.buf.p, c->fdm.buf.p);
   if (realloc) c->drop_graphs();  // recorded against buffers that are gone
   const bool want_graph = p->use_graph && !c->graph_failed;
   aldic_ctx::FrameGraph *fg = nullptr;

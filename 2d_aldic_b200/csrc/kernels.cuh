@@ -70,6 +70,31 @@ struct GridWork {
 };
 enum GridOp { OP_FE = 0, OP_GRIDFIT = 1, OP_INPAINT = 2, OP_CSR = 3, OP_FD = 4 };
 
+// ---- fdm.cu: direct Subproblem 2 solves on the uniform node grid by fast
+// diagonalisation (the FE and FD operators are Kronecker sums of 1-D ones)
+enum { FDM_FE = 0, FDM_FD = 1 };
+struct FdmBasis {
+  int type = -1, M = 0, N = 0;
+  double h = 0.0;
+  DevBuf buf;  // Vx (M x M), Vy (N x N), lx (M), ly (N)
+  double *Vx = nullptr, *Vy = nullptr, *lx = nullptr, *ly = nullptr;
+  void release() {
+    buf.release();
+    type = -1;
+  }
+};
+// 1-D eigenbasis (row-major V, column p = eigenvector p, V' M V = I) and
+// eigenvalues of the FE (stiffness, mass) or FD (d'd, I) pencil of n nodes
+int fdm_basis_1d(int type, int n, double h, double *V, double *lam);
+// the bases of an M x N grid on the device (host work once per geometry;
+// synchronises the stream, so never inside a capture)
+int fdm_ensure(FdmBasis &B, int type, int M, int N, double h, cudaStream_t st);
+// x_f = A_f^-1 b_f for the nrhs fields of M*N values (x fastest) at b, x;
+// A_f = beta_f (Kx (+) Ky) + mu Mx (x) My with beta_f = *beta_ptr if given,
+// else beta_each[f] if given, else beta; tmp: nrhs*M*N doubles
+int fdm_solve(const FdmBasis &B, int nrhs, const double *b, double *x, double *tmp, double mu,
+              double beta, const double *beta_each, const double *beta_ptr, cudaStream_t st);
+
 // Finite-difference Subproblem 2 (funDerivativeOp.m, main_ALDIC.m:243-278):
 // (beta D'D + mu I) x = beta D' a + mu b on the interior (M-2) x (N-2) nodes,
 // D central differences with the reference's one-sided borders.

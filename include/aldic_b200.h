@@ -175,8 +175,11 @@ ALDIC_API int aldic_subpb1_post(aldic_ctx *ctx, int M, int N, const int32_t *ite
                       int *bad_num);
 
 /* ADMM global step -- Subpb2.m:1 on the uniform Q4 mesh of MeshSetUp.m
- * (M x N nodes, spacing step, no Dirichlet/Neumann nodes): assembles
- * beta*DN'DN + mu*N'N with 3x3 Gauss points matrix-free and solves by PCG. */
+ * (M x N nodes, spacing step, no Dirichlet/Neumann nodes): the right-hand
+ * side of the 3x3 Gauss rule of Subpb2.m:100-149 per node, then the direct
+ * solve of beta*DN'DN + mu*N'N (the reference's A\b, Subpb2.m:195) by fast
+ * diagonalisation -- the operator is a Kronecker sum of 1-D linear-element
+ * stiffness and mass matrices (see aldic_fdm_basis). */
 ALDIC_API int aldic_subpb2(aldic_ctx *ctx, int M, int N, double step, double beta, double mu,
                  const double *U, const double *F, const double *udual,
                  const double *vdual, double *Uhat);
@@ -190,18 +193,33 @@ ALDIC_API int aldic_subpb2(aldic_ctx *ctx, int M, int N, double step, double bet
  * (about 12.7 MB, held on every GPU that loads the library until exit), so at
  * most 65536 nodes are accepted -- larger grids return ALDIC_E_ARG.  The
  * first call on a device looks up that array's device address (make it
- * before any stream capture).  The array is shared by every call: calls whose
- * GPU work overlaps (other streams or threads) race.  Returns after the
- * solve (it reads the solver's status back).  stream: cudaStream_t. */
+ * before any stream capture) and keeps it for the process; a cudaDeviceReset
+ * of that device invalidates it, so do not call this entry point on a device
+ * after resetting it.  The array is shared by every call: calls whose GPU
+ * work overlaps (other streams or threads) race.  Every call synchronises
+ * the stream before it returns (it reads the solver's status back).  The
+ * solve is iterative (PCG to relative residual 1e-11), where aldic_subpb2
+ * solves directly.  stream: cudaStream_t. */
 ALDIC_API int aldic_subpb2_noalloc(int M, int N, double step, double beta, double mu,
                                    const double *U, const double *F, const double *udual,
                                    const double *vdual, double *Uhat, void *stream);
+
+/* The 1-D eigenbasis behind the direct Subproblem 2 solves (host only, no
+ * device work; exposed for testing and for callers that want the basis):
+ * type ALDIC_FDM_FE -- the linear-element stiffness K and mass M of n nodes
+ * at spacing h (the 1-D factors of Subpb2.m's operator), type ALDIC_FDM_FD --
+ * G = d'd with d the 1-D difference of funDerivativeOp.m and M = I.  On
+ * return K V = M V diag(lam) and V' M V = I; V is n x n row-major (column p
+ * is eigenvector p). */
+#define ALDIC_FDM_FE 0
+#define ALDIC_FDM_FD 1
+ALDIC_API int aldic_fdm_basis(int type, int n, double h, double *V, double *lam);
 
 /* Finite-difference Subproblem 2 (main_ALDIC.m:243-278, funDerivativeOp.m):
  * the interior (M-2) x (N-2) nodes solve (beta D'D + mu I) x = beta D'(F -
  * udual) + mu (U - vdual) with D the central differences of
  * funDerivativeOp.m (one-sided at the interior grid's edges); the border
- * nodes keep U.  PCG to relative residual 1e-11 replaces the direct solve. */
+ * nodes keep U.  Direct solve by fast diagonalisation, as aldic_subpb2. */
 ALDIC_API int aldic_subpb2_fd(aldic_ctx *ctx, int M, int N, double step, double beta, double mu,
                               const double *U, const double *F, const double *udual,
                               const double *vdual, double *Uhat);

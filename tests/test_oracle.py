@@ -219,6 +219,13 @@ def test_subpb1_pulls_to_penalty(oracle, synth):
 # ------------------------------------------------------------------ a10/a11
 def _subpb2_scipy(M, N, h, beta, mu, U, F, ud, vd):
     """Independent restatement of Subpb2.m:76-195 with scipy sparse."""
+    A, b = subpb2_system(M, N, h, beta, mu, U, F, ud, vd)
+    return spla.spsolve(A.tocsc(), b)
+
+
+def subpb2_system(M, N, h, beta, mu, U, F, ud, vd):
+    """The sparse matrix (2n x 2n, DOFs [u1 v1 u2 v2 ...]) and right-hand side
+    Subpb2.m:76-163 assembles on the uniform M x N mesh."""
     n = M * N
     gp = [-np.sqrt(3 / 5), 0, np.sqrt(3 / 5)]
     gw = [5 / 9, 8 / 9, 5 / 9]
@@ -259,7 +266,7 @@ def _subpb2_scipy(M, N, h, beta, mu, U, F, ud, vd):
                 for q in range(8):
                     rows.append(idx[r]); cols.append(idx[q]); vals.append(A8[r, q])
     A = sp.csr_matrix((vals, (rows, cols)), shape=(2 * n, 2 * n))
-    return spla.spsolve(A.tocsc(), b)
+    return A, b
 
 
 def test_subpb2_matches_sparse_restatement(oracle):

@@ -3,9 +3,10 @@ device memory (a host framework that owns every device byte, a real-time loop
 that must not stall on an allocation, a process with audited or capped
 allocations).  Its work vectors live in the library's fixed static device
 array, so the test checks, through the C ABI, that two calls in a row give
-the same Uhat as the allocating entry point aldic_subpb2 (PCG tolerance
-1e-11 relative; results compared to 1e-8) and that oversize grids are
-refused.  Kept in its own file that pytest collects last."""
+the same Uhat as the allocating entry point aldic_subpb2 (which solves
+directly; this entry point's PCG stops at 1e-11 relative residual; results
+compared to 1e-8) and that oversize grids are refused.  Kept in its own file
+that pytest collects last."""
 import ctypes as C
 
 import numpy as np
