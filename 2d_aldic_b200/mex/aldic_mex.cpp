@@ -20,6 +20,27 @@
 //   [FStrain,FStrainFinite] = aldic_mex('computestrain', M, N, winstepsize, method, rad,
 //                                       straintype, U, F)
 //       ComputeStrain.m Section 8 (F is read by method 0 only; pass [] otherwise)
+//   [x,y,u,v,ccmax,qfactors] = aldic_mex('intsearch', f, g, tempSizeOfSearchRegion, gridx,
+//                                        gridy, winsize, winstepsize)
+//       funIntegerSearch.m:3 whole field (the call of IntegerSearch.m:54 with
+//       tempNoOfInitPt = 0): x, y, u, v, ccmax are ny x nx, qfactors n x 2
+//       (cc.max and cc.qfactors of the reference's cc struct).  f, g: W x H
+//       double (normalised, as IntegerSearch passes them) or uint8/uint16 raw
+//       images (exact integer correlation, statistics over gridx x gridy)
+//   Uhat = aldic_mex('subpb2qt', coordinatesFEM, elementsFEM, dirichlet, beta, mu, U, F)
+//       Subpb2Quadtree.m:1 (GaussPtOrder 2, alpha 0) on a DICmesh of the
+//       quadtree path: coordinatesFEM n x 2, elementsFEM ne x 8 (hanging nodes
+//       in columns 5-8, 0 = none), dirichlet the node list
+//   [x0,y0,U,F,ConvItPerEle,stats] = aldic_mex('frame', ImgRef, ImgDef, winsize,
+//        winstepsize, tempSizeOfSearchRegion, gridx, gridy, tol, nADMM, Subpb2FDOrFEM,
+//        smooth)
+//       one frame of main_ALDIC.m Sections 3-6 (whole-field search, LocalICGN,
+//       beta sweep, nADMM ADMM steps; Subpb2FDOrFEM 1 = FD, 2 = FE; smooth 1 =
+//       the funSmoothDisp/funSmoothStrain calls): x0, y0 M x N, U 2MN, F 4MN,
+//       ConvItPerEle MN x 1; stats = [beta, LocalICGNBadPtNum, UpdateY of each
+//       ADMM step] (all nADMM steps run: compare UpdateY with tol2 = 1e-4 of
+//       main_ALDIC.m:354 to see where the reference would have stopped).
+//       ImgRef/ImgDef raw uint8/uint16 or double W x H
 // ImgRef/ImgDef are the normalised W x H doubles; DfDx/DfDy are the reference's
 // (W-6) x (H-6) Df.DfDx/Df.DfDy.  The GPU context persists across calls
 // (mexLock), images and gradients are re-uploaded on every icgn/subpb1 call.
@@ -65,6 +86,33 @@ static std::vector<double> expand_df(const mxArray *d, size_t W, size_t H) {
   for (size_t y = 0; y < H - 6; ++y)
     std::memcpy(&out[(y + 3) * W + 3], s + y * (W - 6), sizeof(double) * (W - 6));
   return out;
+}
+
+// uint8 / uint16 / double image class -> library dtype
+static int img_dtype(const mxArray *a, const char *what) {
+  if (mxIsUint8(a)) return ALDIC_U8;
+  if (mxIsUint16(a)) return ALDIC_U16;
+  if (mxIsDouble(a)) return ALDIC_F64;
+  mexErrMsgIdAndTxt("aldic:type", "%s must be uint8, uint16 or double", what);
+  return -1;
+}
+
+static void pair2(const mxArray *a, const char *what, int out[2]) {
+  if (!mxIsDouble(a) || mxGetNumberOfElements(a) < 1 || mxGetNumberOfElements(a) > 2)
+    mexErrMsgIdAndTxt("aldic:size", "%s is a double scalar or [a b]", what);
+  const double *d = (const double *)mxGetData(a);
+  out[0] = (int)d[0];
+  out[1] = (int)d[mxGetNumberOfElements(a) - 1];
+}
+
+// hand the first max(nlhs, 1) of k arrays to MATLAB and free the rest
+// (plhs has room for max(nlhs, 1) entries only)
+static void give_outputs(mxArray **o, int k, int nlhs, mxArray *plhs[]) {
+  const int keep = nlhs > 1 ? nlhs : 1;
+  for (int i = 0; i < k; ++i) {
+    if (i < keep) plhs[i] = o[i];
+    else mxDestroyArray(o[i]);
+  }
 }
 
 static void load_fields(const mxArray *DfDx, const mxArray *DfDy, const mxArray *f,
@@ -171,6 +219,110 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
                                (int)mxGetScalar(prhs[6]), dbl(prhs[7], "U"), F, mxGetPr(plhs[0]),
                                mxGetPr(fin)));
     if (nlhs > 1) plhs[1] = fin; else mxDestroyArray(fin);
+  } else if (c == "intsearch") {
+    if (nrhs != 8) mexErrMsgIdAndTxt("aldic:usage", "intsearch takes 7 arguments");
+    const size_t W = mxGetM(prhs[1]), H = mxGetN(prhs[1]);
+    if (mxGetM(prhs[2]) != W || mxGetN(prhs[2]) != H || mxGetClassID(prhs[1]) != mxGetClassID(prhs[2]))
+      mexErrMsgIdAndTxt("aldic:size", "f and g differ in size or class");
+    int s[2], gx[2], gy[2];
+    pair2(prhs[3], "tempSizeOfSearchRegion", s);
+    pair2(prhs[4], "gridx", gx);
+    pair2(prhs[5], "gridy", gy);
+    const int w = (int)mxGetScalar(prhs[6]), step = (int)mxGetScalar(prhs[7]);
+    const int dt = img_dtype(prhs[1], "f");
+    if (dt == ALDIC_F64) {
+      std::vector<double> zeros(W * H, 0.0);  // gradients: not used by the search
+      check(aldic_set_fields(ctx(), dbl(prhs[1], "f"), dbl(prhs[2], "g"), zeros.data(),
+                             zeros.data(), (int)W, (int)H));
+    } else {
+      const int roi[4] = {gx[0], gx[1], gy[0], gy[1]};
+      check(aldic_set_ref(ctx(), mxGetData(prhs[1]), dt, (int)W, (int)H, roi, nullptr));
+      check(aldic_set_def(ctx(), mxGetData(prhs[2]), dt));
+    }
+    int nx = 0, ny = 0;
+    check(aldic_search_dims((int)W, (int)H, gx, gy, w, step, s, &nx, &ny));
+    const size_t n = (size_t)nx * ny;
+    // the library writes MATLAB's ny x nx column-major arrays directly
+    mxArray *o[6];
+    for (int k = 0; k < 5; ++k) o[k] = mxCreateDoubleMatrix((size_t)ny, (size_t)nx, mxREAL);
+    o[5] = mxCreateDoubleMatrix(n, 2, mxREAL);
+    const int rc = aldic_int_search(ctx(), gx, gy, w, step, s, mxGetPr(o[0]), mxGetPr(o[1]),
+                                    mxGetPr(o[2]), mxGetPr(o[3]), mxGetPr(o[4]),
+                                    nlhs > 5 ? mxGetPr(o[5]) : nullptr);
+    give_outputs(o, 6, nlhs, plhs);
+    check(rc);
+  } else if (c == "subpb2qt") {
+    if (nrhs != 8) mexErrMsgIdAndTxt("aldic:usage", "subpb2qt takes 7 arguments");
+    const size_t n = mxGetM(prhs[1]), ne = mxGetM(prhs[2]), nd = mxGetNumberOfElements(prhs[3]);
+    if (mxGetN(prhs[1]) != 2 || mxGetN(prhs[2]) != 8)
+      mexErrMsgIdAndTxt("aldic:size", "coordinatesFEM is n x 2 and elementsFEM ne x 8");
+    if (mxGetNumberOfElements(prhs[6]) != 2 * n || mxGetNumberOfElements(prhs[7]) != 4 * n)
+      mexErrMsgIdAndTxt("aldic:size", "U is 2n and F is 4n");
+    // MATLAB column-major n x 2 / ne x 8 -> row-major pairs / 8-tuples
+    const double *cs = dbl(prhs[1], "coordinatesFEM"), *es = dbl(prhs[2], "elementsFEM");
+    const double *ds = dbl(prhs[3], "dirichlet");
+    std::vector<double> coords(2 * n);
+    std::vector<int32_t> el(8 * ne), dir(nd);
+    for (size_t k = 0; k < n; ++k) { coords[2 * k] = cs[k]; coords[2 * k + 1] = cs[n + k]; }
+    for (size_t k = 0; k < ne; ++k)
+      for (int j = 0; j < 8; ++j) el[8 * k + j] = (int32_t)es[k + (size_t)j * ne];
+    for (size_t k = 0; k < nd; ++k) dir[k] = (int32_t)ds[k];
+    aldic_qt_mesh *m = nullptr;
+    check(aldic_qt_mesh_create((int)n, coords.data(), (int)ne, el.data(), (int)nd, dir.data(), &m));
+    plhs[0] = mxCreateDoubleMatrix(2 * n, 1, mxREAL);
+    const int rc = aldic_qt_subpb2(ctx(), m, mxGetScalar(prhs[4]), mxGetScalar(prhs[5]),
+                                   dbl(prhs[6], "U"), dbl(prhs[7], "F"), mxGetPr(plhs[0]));
+    aldic_qt_mesh_destroy(m);
+    check(rc);
+  } else if (c == "frame") {
+    if (nrhs != 12) mexErrMsgIdAndTxt("aldic:usage", "frame takes 11 arguments");
+    const size_t W = mxGetM(prhs[1]), H = mxGetN(prhs[1]);
+    if (mxGetM(prhs[2]) != W || mxGetN(prhs[2]) != H || mxGetClassID(prhs[1]) != mxGetClassID(prhs[2]))
+      mexErrMsgIdAndTxt("aldic:size", "ImgRef and ImgDef differ in size or class");
+    aldic_frame_params p;
+    std::memset(&p, 0, sizeof p);
+    p.winsize = (int)mxGetScalar(prhs[3]);
+    p.step = (int)mxGetScalar(prhs[4]);
+    pair2(prhs[5], "tempSizeOfSearchRegion", p.search);
+    pair2(prhs[6], "gridx", p.gridx);
+    pair2(prhs[7], "gridy", p.gridy);
+    p.tol = mxGetScalar(prhs[8]);
+    p.mu = 1e-3;
+    p.beta = 0.0;
+    p.n_admm = (int)mxGetScalar(prhs[9]);
+    p.tol2 = 0.0;  // every one of the nADMM steps runs; stats holds UpdateY of each
+    p.precision = ALDIC_FP64;
+    p.subpb2_fd = mxGetScalar(prhs[10]) == 1.0;
+    p.smooth = mxGetScalar(prhs[11]) != 0.0;
+    p.use_graph = 1;
+    p.init = ALDIC_INIT_SEARCH;
+    const int dt = img_dtype(prhs[1], "ImgRef");
+    const int roi[4] = {p.gridx[0], p.gridx[1], p.gridy[0], p.gridy[1]};
+    check(aldic_set_ref(ctx(), mxGetData(prhs[1]), dt, (int)W, (int)H, roi, nullptr));
+    check(aldic_set_def(ctx(), mxGetData(prhs[2]), dt));
+    int M = 0, N = 0;
+    check(aldic_frame_dims(ctx(), &p, &M, &N));
+    const size_t n = (size_t)M * N;
+    // x0, y0 as MeshSetUp.m's M x N arrays (x index first: node k = i + M j,
+    // the library's x-fastest order)
+    mxArray *o[6];
+    o[0] = mxCreateDoubleMatrix((size_t)M, (size_t)N, mxREAL);
+    o[1] = mxCreateDoubleMatrix((size_t)M, (size_t)N, mxREAL);
+    o[2] = mxCreateDoubleMatrix(2 * n, 1, mxREAL);
+    o[3] = mxCreateDoubleMatrix(4 * n, 1, mxREAL);
+    mwSize d1[2] = {n, 1};
+    o[4] = mxCreateNumericArray(2, d1, mxINT32_CLASS, mxREAL);
+    aldic_frame_stats st;
+    std::memset(&st, 0, sizeof st);
+    const int rc = aldic_frame(ctx(), &p, mxGetPr(o[0]), mxGetPr(o[1]), mxGetPr(o[2]),
+                               mxGetPr(o[3]), (int32_t *)mxGetData(o[4]), &st);
+    o[5] = mxCreateDoubleMatrix(1, 2 + (size_t)st.admm_steps, mxREAL);
+    double *sv = mxGetPr(o[5]);
+    sv[0] = st.beta;
+    sv[1] = st.bad_icgn;
+    for (int a = 0; a < st.admm_steps; ++a) sv[2 + a] = st.update_y[a];
+    give_outputs(o, 6, nlhs, plhs);
+    check(rc);
   } else {
     mexErrMsgIdAndTxt("aldic:usage", "unknown command '%s'", cmd);
   }

@@ -12,7 +12,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BUILD = os.path.join(ROOT, "tests", "_build")
 SHIM = os.path.join(ROOT, "oracle", "mex_shim")
-CLS = {np.dtype(np.float64): 6, np.dtype(np.float32): 7, np.dtype(np.int32): 12}
+CLS = {np.dtype(np.float64): 6, np.dtype(np.float32): 7, np.dtype(np.int32): 12,
+       np.dtype(np.uint8): 9, np.dtype(np.uint16): 11}
 
 
 def build_gateway(src_name, out_name):
@@ -175,3 +176,89 @@ def test_aldic_gateway_searchmg_and_computestrain(gw_aldic, synth, oracle, aldic
                              "winstepsize": 8})
     np.testing.assert_array_equal(outs[0][:4 * M * N], r["FStrain"])
     np.testing.assert_array_equal(outs[1][:4 * M * N], r["FStrainFinite"])
+
+
+def test_aldic_gateway_new_command_usage(gw_aldic):
+    for cmd, msg in (("intsearch", b"intsearch takes 7 arguments"),
+                     ("subpb2qt", b"subpb2qt takes 7 arguments"),
+                     ("frame", b"frame takes 11 arguments")):
+        rc, _ = mex_call(gw_aldic, 1, [cmd, np.zeros((2, 1))], [8])
+        assert rc == -1 and msg in gw_aldic.shim_last_error()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["uint8", "double"])
+def test_aldic_gateway_intsearch_matches_oracle(gw_aldic, synth, oracle, kind):
+    """funIntegerSearch through the gateway as IntegerSearch.m:54 calls it:
+    [x,y,u,v,cc] = funIntegerSearch(f,g,searchSize,gridx,gridy,winsize,step,0,step)
+    -- on raw 8-bit images (exact integer correlation) and on the normalised
+    doubles MATLAB passes; peaks equal the oracle's."""
+    W, H = 200, 170
+    f = synth.speckle(W, H, 1100, 41)
+    g = synth.warp(f, synth.uniform_affine(0.003, -0.002, 2.6, -1.7), 2.0, 41)
+    roi = (11, 190, 6, 161)
+    if kind == "uint8":
+        fa, ga = f.T, g.T
+    else:
+        fa, ga = oracle.normalize(f, roi)[0].T, oracle.normalize(g, roi)[0].T
+    args = ["intsearch", fa, ga, np.array([[6.0, 6.0]]), np.array([[11.0, 190.0]]),
+            np.array([[6.0, 161.0]]), np.array([[20.0]]), np.array([[10.0]])]
+    nx, ny, _, _ = oracle.search_dims(W, H, (11, 190), (6, 161), 20, 10, (6, 6))
+    n = nx * ny
+    rc, outs = mex_call(gw_aldic, 6, args, [8 * n] * 5 + [16 * n])
+    assert rc == 0, gw_aldic.shim_last_error()
+    mg = oracle.normalize(g, roi)[1]
+    xo, yo, uo, vo, co, qo = oracle.int_search(f, g, mg, (11, 190), (6, 161), 20, 10, (6, 6), True)
+    for got, ref in zip(outs[:5], (xo, yo, uo, vo, co)):
+        m = got[:n].reshape(nx, ny).T                        # ny x nx column-major
+        if kind == "uint8":
+            np.testing.assert_array_equal(m, ref)
+        else:
+            np.testing.assert_allclose(m, ref, rtol=0, atol=1e-9)
+    q = outs[5][:2 * n].reshape(2, n).T
+    qo = np.asarray(qo)
+    np.testing.assert_allclose(q, qo.T if qo.shape[0] == 2 else qo, rtol=1e-9, equal_nan=True)
+
+
+@pytest.mark.gpu
+def test_aldic_gateway_subpb2qt_matches_oracle(gw_aldic, oracle):
+    """Subpb2Quadtree.m through the gateway on the reference's own Sample12
+    mesh (MATLAB's column-major DICmesh arrays) against the oracle's sparse
+    direct restatement."""
+    from oracle import quadtree as Q
+    from test_reference_pins import sample12
+    z = sample12()
+    c, E, d = z["coordinatesFEM"], z["elementsFEM"], z["dirichlet"]
+    n = len(c)
+    rng = np.random.default_rng(5)
+    U = rng.standard_normal(2 * n)
+    F = 0.01 * rng.standard_normal(4 * n)
+    beta, mu = 2.56e-4, 1e-3
+    args = ["subpb2qt", c, E.astype(np.float64), d.astype(np.float64)[:, None], np.array([[beta]]),
+            np.array([[mu]]), U[:, None], F[:, None]]
+    rc, outs = mex_call(gw_aldic, 1, args, [16 * n])
+    assert rc == 0, gw_aldic.shim_last_error()
+    ref = Q.subpb2_quadtree(c, E, d, beta, mu, U, F)
+    np.testing.assert_allclose(outs[0][:2 * n], ref, rtol=1e-8, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_aldic_gateway_frame_matches_oracle(gw_aldic, synth, oracle):
+    """The whole frame (main_ALDIC.m Sections 3-6) through the gateway on raw
+    8-bit images: the FP64 oracle frame within 1e-4 px, the mesh exact."""
+    wl = synth.workload("plain512", scale_down=2)
+    f, g = wl.images()
+    H, W = f.shape
+    args = ["frame", f.T, g.T, np.array([[float(wl.winsize)]]), np.array([[float(wl.step)]]),
+            np.array([[float(wl.search)]]), np.array([[1.0, W]]), np.array([[1.0, H]]),
+            np.array([[wl.tol]]), np.array([[2.0]]), np.array([[2.0]]), np.array([[0.0]])]
+    nx, ny, _, _ = oracle.search_dims(W, H, (1, W), (1, H), wl.winsize, wl.step,
+                                      (wl.search, wl.search))
+    n = nx * ny
+    rc, outs = mex_call(gw_aldic, 6, args, [8 * n, 8 * n, 16 * n, 32 * n, 4 * n, 8 * 8])
+    assert rc == 0, gw_aldic.shim_last_error()
+    ro = oracle.frame(f, g, wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=2)
+    np.testing.assert_array_equal(outs[0][:n], ro["x0"])
+    np.testing.assert_array_equal(outs[1][:n], ro["y0"])
+    assert np.abs(outs[2][:2 * n] - ro["U"]).max() < 1e-4
+    assert abs(outs[5][0] - ro["beta"]) < 1e-9 * ro["beta"]
