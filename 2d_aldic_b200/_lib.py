@@ -59,6 +59,7 @@ _SIGS = {
     "aldic_fd_strain": ([P, I32, I32, D, P, P], I32),
     "aldic_compute_strain": ([P, I32, I32, D, I32, I32, I32, P, P, P, P], I32),
     "aldic_fdm_basis": ([I32, I32, D, P, P], I32),
+    "aldic_set_stats": ([P, P], I32),
     "aldic_gemm_bf16": ([P, P, P, P, I32, I32], I32),
     "aldic_cnn_create": ([I32, C.c_uint64, P], I32),
     "aldic_cnn_destroy": ([P], I32),

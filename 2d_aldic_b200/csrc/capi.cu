@@ -78,6 +78,7 @@ struct aldic_ctx {
   int W = 0, H = 0, dtype = -1, roi[4] = {0, 0, 0, 0};
   bool have_ref = false, have_def = false;
   bool prepared = false;  // fields given by aldic_set_fields (no normalisation)
+  bool has_mask = false;  // the last aldic_set_ref had an ImgRefMask
   DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
   DevBuf g4;  // row runs of g32 (float4 per pixel) read by the FP32 IC-GN sampler
   DevBuf gxy;  // (gx32, gy32) pairs (float2 per pixel) read by the FP32 IC-GN
@@ -448,6 +449,7 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     ALDIC_CUDA(cudaMemcpyAsync(c->mask.p, mask, sizeof(double) * n, cudaMemcpyDefault, c->stream));
     dmask = c->mask.as<double>();
   }
+  c->has_mask = dmask != nullptr;
   double *st = c->stats.as<double>();
   if ((rc = roi_stats(c->f_raw.p, dtype, W, r, st, c->isums.as<unsigned long long>(),
                       c->part.as<double>(), c->stream)))
@@ -485,6 +487,32 @@ int aldic_set_def(aldic_ctx *c, const void *img, int dtype) {
   if (rc) return rc;
   c->have_def = true;
   return finish(c, !is_device_ptr(img));
+}
+
+int aldic_set_stats(aldic_ctx *c, const double stats[4]) {
+  ALDIC_CHECK(c && stats, E_ARG, "set_stats: null argument");
+  ALDIC_CHECK(c->have_ref && c->have_def && !c->prepared, E_STATE,
+              "set_stats: set the reference and deformed images (aldic_set_ref/aldic_set_def) first");
+  ALDIC_CHECK(stats[1] > 0 && stats[3] > 0, E_ARG, "set_stats: standard deviations must be positive");
+  Guard g(c);
+  const long long n = (long long)c->W * c->H;
+  double *st = c->stats.as<double>();
+  ALDIC_CUDA(cudaMemcpyAsync(st, stats, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc;
+  if ((rc = normalize(c->f_raw.p, c->dtype, n, st, c->f64.as<double>(), c->f32.as<float>(), c->stream)))
+    return rc;
+  if ((rc = gradient(c->f64.as<double>(), c->has_mask ? c->mask.as<double>() : nullptr, c->W, c->H,
+                     c->gx64.as<double>(), c->gy64.as<double>(), c->gx32.as<float>(),
+                     c->gy32.as<float>(), c->stream)))
+    return rc;
+  if ((rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
+    return rc;
+  // the deformed image with stats[2..3] (not prep_def, which takes them from the ROI)
+  if ((rc = normalize(c->g_raw.p, c->dtype, n, st + 2, c->g64.as<double>(), c->g32.as<float>(),
+                      c->stream)) ||
+      (rc = row_runs(c->g32.as<float>(), c->W, c->H, c->g4.as<float4>(), c->stream)))
+    return rc;
+  return finish(c, true);
 }
 
 int aldic_normalize(aldic_ctx *c, const void *img, int dtype, int W, int H, const int roi[4],

@@ -111,6 +111,15 @@ ALDIC_API int aldic_set_fields(aldic_ctx *ctx, const double *f, const double *g,
 ALDIC_API int aldic_get_images(aldic_ctx *ctx, double *f, double *g, double *dfdx,
                      double *dfdy, double stats[4]);
 
+/* Normalisation statistics given from outside instead of the ROI of the
+ * images held (funNormalizeImg.m's mean and sample standard deviation of
+ * the ROI, {mean_f, std_f, mean_g, std_g}): for a context that holds only a
+ * band of the images (a frame split across GPUs), whose ROI statistics are
+ * summed over the ranks.  Renormalises both images and the gradients; a
+ * later aldic_set_ref/aldic_set_def or aldic_frame takes the statistics from
+ * the ROI again. */
+ALDIC_API int aldic_set_stats(aldic_ctx *ctx, const double stats[4]);
+
 /* Integer search -- funIntegerSearch.m:3 (whole field, tempNoOfInitPt = 0):
  * grid trimming of :14-25, then per grid point the normalised cross-
  * correlation of the (w+1)^2 template against the (w+1+2s)^2 region and the
