@@ -60,6 +60,9 @@ _SIGS = {
     "aldic_compute_strain": ([P, I32, I32, D, I32, I32, I32, P, P, P, P], I32),
     "aldic_fdm_basis": ([I32, I32, D, P, P], I32),
     "aldic_set_stats": ([P, P], I32),
+    "aldic_set_init_gated": ([P, P, P, P, D, I64], I32),
+    "aldic_icgn_autotune": ([I32], I32),
+    "aldic_icgn_shape": ([I32, I32, I32, C.c_longlong, P, P, P, P], I32),
     "aldic_gemm_bf16": ([P, P, P, P, I32, I32], I32),
     "aldic_cnn_create": ([I32, C.c_uint64, P], I32),
     "aldic_cnn_destroy": ([P], I32),
@@ -96,7 +99,7 @@ class FrameStats(C.Structure):
                 ("converged_icgn", I32), ("beta", D), ("update_y", D * 16),
                 ("update_y2", D * 16), ("mean_iters_icgn", D), ("kernel_launches", I32),
                 ("t_stage_ms", D * 8), ("max_pcg_iters", I32), ("node_grid", D * 4),
-                ("t_search_mg_ms", D)]
+                ("t_search_mg_ms", D), ("gated_init", I32)]
 
 
 class AldicError(RuntimeError):

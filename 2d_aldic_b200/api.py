@@ -33,7 +33,7 @@ except Exception:  # pragma: no cover
 U8, U16, F32, F64 = 0, 1, 2, 3
 FP32, FP64 = 0, 1
 # initial guess of a frame (ALDIC_INIT_* of the C ABI)
-INIT_SEARCH, INIT_PREV, INIT_ZERO, INIT_EXTRAP, INIT_GIVEN, INIT_SEARCH_MG = 0, 1, 2, 3, 4, 5
+INIT_SEARCH, INIT_PREV, INIT_ZERO, INIT_EXTRAP, INIT_GIVEN, INIT_SEARCH_MG, INIT_GATED = 0, 1, 2, 3, 4, 5, 6
 _DT = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.float32): F32,
        np.dtype(np.float64): F64}
 
@@ -703,6 +703,18 @@ class ALDIC:
         a = _contig(U0) if _is_cuda(U0) else np.ascontiguousarray(U0, np.float64)
         call("aldic_set_init", self.ctx.h, _ptr(a), int(a.numel() if _is_cuda(a) else a.size))
 
+    def set_init_gated(self, U0, F0=None, conf=None, conf_min=0.5):
+        """An external guess for frame(init=INIT_GATED): U0 (2n), F0 (4n or
+        None) and a confidence per node (n, float32, or None); nodes with
+        conf >= conf_min start IC-GN from (U0, F0), the others from the
+        integer search."""
+        a = _contig(U0) if _is_cuda(U0) else np.ascontiguousarray(U0, np.float64)
+        n = int(a.numel() if _is_cuda(a) else a.size) // 2
+        fa = None if F0 is None else (_contig(F0) if _is_cuda(F0) else np.ascontiguousarray(F0, np.float64))
+        ca = None if conf is None else (_contig(conf) if _is_cuda(conf)
+                                        else np.ascontiguousarray(conf, np.float32))
+        call("aldic_set_init_gated", self.ctx.h, _ptr(a), _ptr(fa), _ptr(ca), float(conf_min), n)
+
     def frame(self, out: dict | None = None, stats: bool = True, device_out: bool = False,
               init: int = INIT_SEARCH):
         """Run one frame.  With out (dict of preallocated arrays x0, y0, U, F,
@@ -759,6 +771,7 @@ class ALDIC:
                             "kernel_launches": st.kernel_launches,
                             "max_pcg_iters": st.max_pcg_iters,
                             "t_search_mg_ms": st.t_search_mg_ms,
+                            "gated_init": st.gated_init,
                             "t_stage_ms": dict(zip(("normalize", "search", "icgn", "icgn_post",
                                                     "section5", "admm", "frame"),
                                                    list(st.t_stage_ms)[:7]))}

@@ -12,12 +12,28 @@
 // forms b, the convergence test and dP = -H\b with the FP64 Cholesky factor
 // of H, and applies the inverse-compositional update in FP64.
 //
+// FP32 evaluations sample two horizontally adjacent pixels (A, B) of a subset
+// row per lane and trip with the packed FP32 instructions of sm_100
+// (__ffma2_rn & co., two IEEE single-precision operations per instruction):
+// B's stencil is A's shifted one column whenever B's floor corner is A's
+// corner + (1, 0), and the pair runs gp (g[i], g[i+1], g[i+1], g[i+2]) then
+// hold the (A, B) tap pairs of a stencil row in two 16-byte loads -- the
+// weights, the 16 row products, the combination and the residual sums all
+// run on (A, B) pairs.  A pair whose B corner differs (the fraction of B
+// wrapped: about |F11| + |F21| of the pairs) drops B from the packed sums
+// and queues it in shared memory; the warp samples the queued pixels
+// together afterwards, one per lane, so the rare case costs no divergence.
+//
 // ZNSSD residual (funICGN.m:238): r = (f - fbar)/bf - (g - gbar)/bg.  With
 // sd_k the steepest-descent images,
 //   b2_k = S_fk/bf - (T_k - gm S_k)/bg,
 // where S_fk = sum sd_k (f - fbar), S_k = sum sd_k are fixed per subset and
 // T_k = sum sd_k (g - c), gm = mean(g) - c are accumulated per iteration with
 // the shift c = fbar (which keeps the one-pass variance well conditioned).
+#include <map>
+#include <mutex>
+#include <vector>
+
 #include "aldic_internal.cuh"
 #include "kernels.cuh"
 
@@ -25,13 +41,13 @@ namespace aldic {
 
 namespace {
 
-constexpr int WARPS = 8;  // warps per CTA
 
 struct Args {
   IcgnImages im;
   const double *coords;
   long long n;
   const double *U0;     // IC-GN: U0; Subpb1: UOld
+  const double *F0;     // IC-GN: initial deformation gradient [F11 F21 F12 F22] per subset, or null (0)
   const double *FOld;   // Subpb1
   const double *vdual;  // Subpb1
   const double *H21in;  // Subpb1
@@ -212,6 +228,166 @@ __device__ __forceinline__ double sample_minus(const double *img, int W, int cx,
   return sample<double>(img, W, cx, cy, tu, tv) - c;
 }
 
+// Packed (A, B) arithmetic: two IEEE FP32 operations per instruction on sm_100.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// keys_w2 of the two fractions in t (A, B)
+__device__ __forceinline__ void keys_w2x2(float2 t, float2 w[4]) {
+  const float2 t2 = __fmul2_rn(t, t), t3 = __fmul2_rn(t2, t);
+  const float2 nt = __fmul2_rn(t, f2(-1.f));
+  w[0] = __ffma2_rn(t3, f2(-1.f), __ffma2_rn(t2, f2(2.f), nt));     // 2t^2 - t - t^3
+  w[1] = __ffma2_rn(t3, f2(3.f), __ffma2_rn(t2, f2(-5.f), f2(2.f)));  // 3t^3 - 5t^2 + 2
+  w[2] = __ffma2_rn(t3, f2(-3.f), __ffma2_rn(t2, f2(4.f), t));        // -3t^3 + 4t^2 + t
+  w[3] = __ffma2_rn(t2, f2(-1.f), t3);                                // t^3 - t^2
+}
+
+// Both 4x samples of a pixel pair whose B stencil is A's shifted one column:
+// p points at A's stencil origin in the pair runs.
+__device__ __forceinline__ float2 sample4x_pair(const float4 *__restrict__ p, int W, float2 tu,
+                                                float2 tv) {
+  float2 wu[4], wv[4];
+  keys_w2x2(tu, wu);
+  keys_w2x2(tv, wv);
+  float2 acc = f2(0.f);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float4 a = __ldg(p + r * W), b = __ldg(p + r * W + 2);
+    float2 s = __fmul2_rn(wu[0], f2(a.x, a.y));
+    s = __ffma2_rn(wu[1], f2(a.z, a.w), s);
+    s = __ffma2_rn(wu[2], f2(b.x, b.y), s);
+    s = __ffma2_rn(wu[3], f2(b.z, b.w), s);
+    acc = r == 0 ? __fmul2_rn(wv[0], s) : __ffma2_rn(wv[r], s, acc);
+  }
+  return acc;
+}
+
+// Residual sums of one FP32 evaluation over the subset's pixel pairs.  Pair
+// q of a row of nw pixels covers columns 2j, 2j+1 (j = q mod ppr, ppr =
+// ceil(nw / 2)); for odd nw the last pair's B lies outside the subset and
+// counts zero.  Queued B pixels (see the file header) are sampled by the
+// whole warp in fq_flush.  Per lane, acc holds (A, B) partial sums of
+// [d, d^2, fx d X, fy d X, fx d Y, fy d Y, fx d, fy d] with d = g - c at the
+// warped pixel (SUB: only d, d^2, fx d, fy d).
+struct PairEval {
+  const float4 *gp, *gxyp;
+  int W, nw, base, xb, yb;
+  float ox, oy, a11, a12, a21, a22, c4, c5, cg;
+};
+
+template <bool SUB>
+__device__ __forceinline__ void add_terms(float2 d, float2 X, float Y, float4 G, float2 acc[8]) {
+  acc[0] = __fadd2_rn(acc[0], d);
+  acc[1] = __ffma2_rn(d, d, acc[1]);
+  const float2 ax = __fmul2_rn(f2(G.x, G.y), d), ay = __fmul2_rn(f2(G.z, G.w), d);
+  acc[6] = __fadd2_rn(acc[6], ax);
+  acc[7] = __fadd2_rn(acc[7], ay);
+  if (!SUB) {
+    acc[2] = __ffma2_rn(ax, X, acc[2]);
+    acc[3] = __ffma2_rn(ay, X, acc[3]);
+    acc[4] = __ffma2_rn(ax, f2(Y), acc[4]);
+    acc[5] = __ffma2_rn(ay, f2(Y), acc[5]);
+  }
+}
+
+// one queued B pixel (pair index q) sampled by a single lane with its own
+// stencil (two pair-run loads a row give its four taps), accumulated into
+// the B half of the lane's sums
+template <bool SUB>
+__device__ __forceinline__ void b_pixel(const PairEval &e, int ppr, int q, float2 acc[8]) {
+  const float rq = floor(((float)q + 0.5f) * (1.0f / (float)ppr));
+  const int row = (int)rq, colA = 2 * (q - row * ppr);
+  const float X = e.ox + (float)(colA + 1), Y = e.oy + rq;
+  const float ru = fmaf(e.a11, X, fmaf(e.a12, Y, e.c4));
+  const float rv = fmaf(e.a21, X, fmaf(e.a22, Y, e.c5));
+  const float fu = floor(ru), fv = floor(rv);
+  const int cx = e.xb + (int)fu - 1, cy = e.yb + (int)fv - 1;
+  float wu[4], wv[4];
+  keys_w2(ru - fu, wu);
+  keys_w2(rv - fv, wv);
+  const float4 *p = e.gp + ((cy - 1) * e.W + (cx - 1));
+  float a4 = 0.f;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float4 u = __ldg(p + r * e.W), v = __ldg(p + r * e.W + 2);
+    const float t = wu[0] * u.x + wu[1] * u.y + wu[2] * v.x + wu[3] * v.y;
+    a4 += wv[r] * t;
+  }
+  const float d = fmaf(a4, 0.25f, -e.cg);
+  const float4 G = __ldg(e.gxyp + (e.base + row * e.W + colA));  // B's gradients: .y, .w
+  const float ax = G.y * d, ay = G.w * d;
+  acc[0].y += d;
+  acc[1].y = fmaf(d, d, acc[1].y);
+  acc[6].y += ax;
+  acc[7].y += ay;
+  if (!SUB) {
+    acc[2].y = fmaf(ax, X, acc[2].y);
+    acc[3].y = fmaf(ay, X, acc[3].y);
+    acc[4].y = fmaf(ax, Y, acc[4].y);
+    acc[5].y = fmaf(ay, Y, acc[5].y);
+  }
+}
+
+constexpr int FQ = 128;  // per-warp queue of B pixels
+
+template <bool SUB>
+__device__ __noinline__ void fq_flush(const PairEval &e, int ppr, const unsigned short *fq, int cnt,
+                                      int lane, float2 acc[8]) {
+  __syncwarp();
+  for (int i = lane; i < cnt; i += 32) b_pixel<SUB>(e, ppr, fq[i], acc);
+  __syncwarp();
+}
+
+template <bool SUB>
+__device__ __forceinline__ void eval_pairs(const PairEval &e, int lane, unsigned short *fq,
+                                           float out[8]) {
+  const int nw = e.nw, ppr = (nw + 1) >> 1, npairs = nw * ppr;
+  const float fppr = (float)ppr, ippr = 1.0f / fppr;
+  float2 acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc[k] = f2(0.f);
+  int qn = 0;  // queued B pixels (warp-uniform)
+  for (int q0 = 0; q0 < npairs; q0 += 32) {
+    const int q = q0 + lane;
+    bool queue = false;
+    if (q < npairs) {
+      const float rq = floor(((float)q + 0.5f) * ippr);
+      const float cj = (float)q - rq * fppr;
+      const int row = (int)rq, colA = 2 * (int)cj;
+      const float XA = fmaf(2.f, cj, e.ox);
+      const float2 X = f2(XA, XA + 1.f);
+      const float Y = e.oy + rq;
+      const float2 ru = __ffma2_rn(f2(e.a11), X, f2(fmaf(e.a12, Y, e.c4)));
+      const float2 rv = __ffma2_rn(f2(e.a21), X, f2(fmaf(e.a22, Y, e.c5)));
+      const float fu = floor(ru.x), fv = floor(rv.x);
+      const float2 tu = __fadd2_rn(ru, f2(-fu, -fu - 1.f));
+      const float2 tv = __fadd2_rn(rv, f2(-fv));
+      const int cx = e.xb + (int)fu - 1, cy = e.yb + (int)fv - 1;
+      const float2 a4 = sample4x_pair(e.gp + ((cy - 1) * e.W + (cx - 1)), e.W, tu, tv);
+      float2 d = __ffma2_rn(a4, f2(0.25f), f2(-e.cg));
+      const bool hasB = colA + 1 < nw;
+      const bool okB = tu.y >= 0.f && tu.y < 1.f && tv.y >= 0.f && tv.y < 1.f;
+      queue = hasB && !okB;
+      if (!(hasB && okB)) d.y = 0.f;
+      add_terms<SUB>(d, X, Y, __ldg(e.gxyp + (e.base + row * e.W + colA)), acc);
+    }
+    // queue the B pixels whose stencil is not A's shifted one column
+    const unsigned bal = __ballot_sync(0xffffffffu, queue);
+    if (bal) {
+      const int nb = __popc(bal);
+      if (qn + nb > FQ) {
+        fq_flush<SUB>(e, ppr, fq, qn, lane, acc);
+        qn = 0;
+      }
+      if (queue) fq[qn + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)q;
+      qn += nb;
+    }
+  }
+  if (qn) fq_flush<SUB>(e, ppr, fq, qn, lane, acc);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) out[k] = acc[k].x + acc[k].y;
+}
+
 // the FP32 path samples the row runs, the FP64 path the image itself
 __device__ __forceinline__ const float4 *sample_src(const IcgnImages &m, float) { return m.g4; }
 __device__ __forceinline__ const double *sample_src(const IcgnImages &m, double) { return m.g64; }
@@ -273,7 +449,7 @@ template <typename Real> struct PixelMap {
 constexpr int WS = 76;
 
 template <typename Real, bool SUB>
-__device__ void process(const Args &a, long long s, int lane, double *ws) {
+__device__ void process(const Args &a, long long s, int lane, double *ws, unsigned short *fq) {
   double *Lsh = ws + 36, *Sfs = ws + 57, *Sks = ws + 63, *Linv = ws + 69;
   const IcgnImages &im = a.im;
   const double x0 = a.coords[s], y0 = a.coords[a.n + s];
@@ -438,7 +614,9 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   if (SUB) {
     for (int q = 0; q < 4; ++q) P[q] = a.FOld[4 * s + q];
   } else {
-    P[0] = P[1] = P[2] = P[3] = 0.0;
+    // funICGN.m:39 starts from P = [0 0 0 0 u v]; an external guess may give
+    // the gradient terms too
+    for (int q = 0; q < 4; ++q) P[q] = a.F0 ? a.F0[4 * s + q] : 0.0;
   }
   P[4] = a.U0[2 * s];
   P[5] = a.U0[2 * s + 1];
@@ -506,7 +684,18 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) pfin &= isfinite(P[q]);
     double sums[8];
-    if (pfin) {
+    if (pfin && sizeof(Real) == 4) {
+      PairEval e;
+      e.gp = im.gp; e.gxyp = im.gxyp;
+      e.W = W; e.nw = nw; e.base = base; e.xb = xb; e.yb = yb;
+      e.ox = (float)ox; e.oy = (float)oy;
+      e.a11 = (float)(1 + P[0]); e.a12 = (float)P[2]; e.a21 = (float)P[1]; e.a22 = (float)(1 + P[3]);
+      e.c4 = (float)P[4] + (float)fx0; e.c5 = (float)P[5] + (float)fy0; e.cg = (float)cg;
+      float o[8];
+      eval_pairs<SUB>(e, lane, fq, o);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sums[q] = (SUB && q >= 2 && q < 6) ? 0.0 : warp_sum((double)o[q]);
+    } else if (pfin) {
       const Real a11 = (Real)(1 + P[0]), a12 = (Real)P[2], a21 = (Real)P[1],
                  a22 = (Real)(1 + P[3]), p4 = (Real)P[4], p5 = (Real)P[5];
       Real s1 = 0, s2r = 0, t[6];
@@ -609,36 +798,142 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   }
 }
 
-template <typename Real, bool SUB>
-// FP32: 64 registers (4 CTAs, 32 warps per SM) -- the extra resident warps
-// hide more gather latency than the register spills cost
-__global__ void __launch_bounds__(WARPS * 32, sizeof(Real) == 4 ? 4 : 2) k_icgn(Args a) {
-  __shared__ double Lsh[WARPS][WS];
+// Launch shapes the autotuner chooses from: NW warps per CTA and MINB
+// resident CTAs per SM in the launch bounds (NW * 32 * MINB threads share
+// the SM's 64 K registers, so MINB sets the register cap: 8 x 4 and 4 x 8 ->
+// 64 registers, 8 x 3 -> 80, 8 x 2 -> 128, 4 x 6 -> 80, 16 x 2 -> 64; FP64:
+// 8 x 2 -> 128, 4 x 3 -> 168).  Every shape runs the same per-subset code,
+// so the results are bit-identical and only the time differs.
+template <typename Real, bool SUB, int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_icgn(Args a) {
+  __shared__ double Lsh[NW][WS];
+  __shared__ unsigned short Fq[NW][FQ];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   while (true) {
     unsigned int s = 0;
     if (lane == 0) s = atomicAdd(a.queue, 1u);
     s = __shfl_sync(0xffffffffu, s, 0);
     if ((long long)s >= a.n) break;
-    process<Real, SUB>(a, (long long)s, lane, Lsh[wid]);
+    process<Real, SUB>(a, (long long)s, lane, Lsh[wid], Fq[wid]);
     __syncwarp();
   }
 }
 
+struct Shape {
+  int nw, minb;
+  const void *fn;
+};
+
 template <typename Real, bool SUB>
-int launch(const Args &a, cudaStream_t st) {
+std::vector<Shape> make_shapes() {
+  if constexpr (sizeof(Real) == 4)
+    return {{8, 4, (const void *)k_icgn<Real, SUB, 8, 4>},
+            {8, 3, (const void *)k_icgn<Real, SUB, 8, 3>},
+            {8, 2, (const void *)k_icgn<Real, SUB, 8, 2>},
+            {4, 8, (const void *)k_icgn<Real, SUB, 4, 8>},
+            {4, 6, (const void *)k_icgn<Real, SUB, 4, 6>},
+            {16, 2, (const void *)k_icgn<Real, SUB, 16, 2>}};
+  else
+    return {{8, 2, (const void *)k_icgn<Real, SUB, 8, 2>},
+            {4, 3, (const void *)k_icgn<Real, SUB, 4, 3>}};
+}
+
+template <typename Real, bool SUB>
+const std::vector<Shape> &shapes() {
+  static const std::vector<Shape> v = make_shapes<Real, SUB>();
+  return v;
+}
+
+int launch_shape(const Shape &sh, const Args &a, cudaStream_t st) {
   int dev = 0, sms = 148, per = 1;
   ALDIC_CUDA(cudaGetDevice(&dev));
   ALDIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  ALDIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icgn<Real, SUB>, WARPS * 32, 0));
+  ALDIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sh.fn, sh.nw * 32, 0));
   if (per < 1) per = 1;
-  long long blocks = (long long)sms * per;
-  const long long need = (a.n + WARPS - 1) / WARPS;
+  long long blocks = (long long)sms * per;  // persistent: every resident CTA, one wave
+  const long long need = (a.n + sh.nw - 1) / sh.nw;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
   ALDIC_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned int), st));
-  k_icgn<Real, SUB><<<(int)blocks, WARPS * 32, 0, st>>>(a);
-  ALDIC_CUDA(cudaGetLastError());
+  Args arg = a;
+  void *args[] = {&arg};
+  ALDIC_CUDA(cudaLaunchKernel(sh.fn, dim3((unsigned)blocks), dim3(sh.nw * 32), args, 0, st));
+  return OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+// The launch shape per (precision, instance, device, subset size, log2 of
+// the subset count) is picked by timed trials on the first launch that may
+// synchronise (not inside a stream capture): every shape runs twice on the
+// call's own data and the faster second run wins.  The choice is kept for
+// the process; a launch inside a capture before any trial uses shape 0.
+struct TuneKey {
+  int prec, sub, dev, w, nlog;
+  bool operator<(const TuneKey &o) const {
+    if (prec != o.prec) return prec < o.prec;
+    if (sub != o.sub) return sub < o.sub;
+    if (dev != o.dev) return dev < o.dev;
+    if (w != o.w) return w < o.w;
+    return nlog < o.nlog;
+  }
+};
+struct TuneVal {
+  int shape;
+  float ms[8];
+  int count;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+bool g_tune_on = true;
+
+TuneKey tune_key(int prec, bool sub, int w, long long n) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int nl = 0;
+  while ((1LL << (nl + 1)) <= n) ++nl;
+  return TuneKey{prec, sub ? 1 : 0, dev, w, nl};
+}
+
+template <typename Real, bool SUB>
+int launch(const Args &a, cudaStream_t st) {
+  const auto &sv = shapes<Real, SUB>();
+  const TuneKey key = tune_key(sizeof(Real) == 8, SUB, a.wins ? -1 : a.w, a.n);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return launch_shape(sv[it->second.shape], a, st);
+    if (!g_tune_on) return launch_shape(sv[0], a, st);
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ALDIC_CUDA(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone || a.n < 2048) return launch_shape(sv[0], a, st);
+  cudaEvent_t e0, e1;
+  ALDIC_CUDA(cudaEventCreate(&e0));
+  ALDIC_CUDA(cudaEventCreate(&e1));
+  TuneVal tv{};
+  tv.count = (int)sv.size();
+  int rc = OK;
+  for (size_t k = 0; k < sv.size() && rc == OK; ++k) {
+    float ms = 0.f;
+    for (int rep = 0; rep < 2 && rc == OK; ++rep) {
+      cudaEventRecord(e0, st);
+      rc = launch_shape(sv[k], a, st);
+      cudaEventRecord(e1, st);
+      if (rc == OK && (cudaEventSynchronize(e1) != cudaSuccess ||
+                       cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)) {
+        set_error("icgn autotune: timing failed");
+        rc = E_CUDA;
+      }
+    }
+    tv.ms[k] = ms;
+    if (ms < tv.ms[tv.shape]) tv.shape = (int)k;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  // the outputs of the last trial stand (every shape computes the same)
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = tv;
   return OK;
 }
 
@@ -646,13 +941,42 @@ int launch(const Args &a, cudaStream_t st) {
 
 int icgn(const IcgnImages &im, const double *coords, long long n, const double *U0,
          const int *wins, int w, double tol, int precision, double *U, double *F, int *iters,
-         double *H21, unsigned int *queue, cudaStream_t st, double *cache) {
+         double *H21, unsigned int *queue, cudaStream_t st, double *cache, const double *F0) {
   if (n <= 0) return OK;
   Args a{};
   a.cache = cache;
+  a.F0 = F0;
   a.im = im; a.coords = coords; a.n = n; a.U0 = U0; a.wins = wins; a.w = w; a.tol = tol;
   a.U = U; a.F = F; a.H21out = H21; a.iters = iters; a.queue = queue;
   return precision ? launch<double, false>(a, st) : launch<float, false>(a, st);
+}
+
+bool icgn_tuned(int precision, bool sub, int w, long long n) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (!g_tune_on || n < 2048) return true;
+  return g_tune.count(tune_key(precision ? 1 : 0, sub, w, n)) != 0;
+}
+
+void icgn_autotune(bool on) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_on = on;
+  if (!on) g_tune.clear();
+}
+
+int icgn_tuned_shape(int precision, bool sub, int w, long long n, int *nwarps, int *minb,
+                     float ms[8], int *count) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(precision ? 1 : 0, sub, w, n));
+  if (it == g_tune.end()) return E_STATE;
+  const auto &sv = precision ? (sub ? shapes<double, true>() : shapes<double, false>())
+                             : (sub ? shapes<float, true>() : shapes<float, false>());
+  const Shape &sh = sv[it->second.shape];
+  if (nwarps) *nwarps = sh.nw;
+  if (minb) *minb = sh.minb;
+  if (count) *count = it->second.count;
+  if (ms)
+    for (int k = 0; k < 8; ++k) ms[k] = k < it->second.count ? it->second.ms[k] : 0.f;
+  return OK;
 }
 
 int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,

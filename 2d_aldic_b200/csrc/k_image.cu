@@ -169,6 +169,41 @@ int grad_pairs(const float *gx, const float *gy, long long n, float2 *q, cudaStr
   return OK;
 }
 
+// Pixel-pair runs for the packed FP32 sampler: with pixel A's stencil
+// column c, q[c + 2j] = (g[c+2j], g[c+2j+1], g[c+2j+1], g[c+2j+2]) holds
+// taps 2j and 2j+1 of A and of its right neighbour B (whose stencil starts
+// one column later) as two (A, B) register pairs.
+__global__ void k_pair_runs(const float *__restrict__ g, int W, long long n,
+                            float4 *__restrict__ q) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % W);
+    const float g1 = x + 1 < W ? g[i + 1] : 0.f;
+    q[i] = make_float4(g[i], g1, g1, x + 2 < W ? g[i + 2] : 0.f);
+  }
+}
+
+int pair_runs(const float *g, int W, int H, float4 *q, cudaStream_t st) {
+  k_pair_runs<<<1184, 256, 0, st>>>(g, W, (long long)W * H, q);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+__global__ void k_grad_pair_runs(const float *__restrict__ gx, const float *__restrict__ gy, int W,
+                                 long long n, float4 *__restrict__ q) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool in = (int)(i % W) + 1 < W;
+    q[i] = make_float4(gx[i], in ? gx[i + 1] : 0.f, gy[i], in ? gy[i + 1] : 0.f);
+  }
+}
+
+int grad_pair_runs(const float *gx, const float *gy, int W, int H, float4 *q, cudaStream_t st) {
+  k_grad_pair_runs<<<1184, 256, 0, st>>>(gx, gy, W, (long long)W * H, q);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
 // ------------------------------------------------------------------ gradient
 __device__ __forceinline__ double grad7(const double *f, long long i, long long s) {
   const double c1 = 0.75, c2 = 3.0 / 20.0, c3 = 1.0 / 60.0;

@@ -19,6 +19,10 @@ int gradient(const double *f, const double *mask, int W, int H, double *gx64, do
 int row_runs(const float *g, int W, int H, float4 *q, cudaStream_t st);
 // q[i] = (gx[i], gy[i]), n float2
 int grad_pairs(const float *gx, const float *gy, long long n, float2 *q, cudaStream_t st);
+// q[i] = (g[i], g[i+1], g[i+1], g[i+2]) within the row, W*H float4
+int pair_runs(const float *g, int W, int H, float4 *q, cudaStream_t st);
+// q[i] = (gx[i], gx[i+1], gy[i], gy[i+1]) within the row, W*H float4
+int grad_pair_runs(const float *gx, const float *gy, int W, int H, float4 *q, cudaStream_t st);
 int interp_f64(const double *F, long long M, long long N, long long P, const double *X,
                const double *Y, long long n, double *Z, cudaStream_t st);
 int interp_f32(const float *F, long long M, long long N, long long P, const float *X,
@@ -44,12 +48,23 @@ struct IcgnImages {
   const float *f32, *g32, *gx32, *gy32;
   const float4 *g4;  // row runs of g32 (row_runs): the FP32 sampler's stencil rows
   const float2 *gxy;  // (gx32, gy32) pairs (grad_pairs) read by the FP32 IC-GN
+  // pixel-pair runs read by the FP32 evaluation loop, which samples two
+  // horizontally adjacent pixels at once: gp[i] = (g[i], g[i+1], g[i+1],
+  // g[i+2]) (pair_runs) and gxyp[i] = (gx[i], gx[i+1], gy[i], gy[i+1])
+  // (grad_pair_runs), zero past the row's end
+  const float4 *gp, *gxyp;
   const double *f64, *g64, *gx64, *gy64;
   int W, H;
 };
 int icgn(const IcgnImages &im, const double *coords, long long n, const double *U0,
          const int *wins, int w, double tol, int precision, double *U, double *F, int *iters,
-         double *H21, unsigned int *queue, cudaStream_t st, double *cache = nullptr);
+         double *H21, unsigned int *queue, cudaStream_t st, double *cache = nullptr,
+         const double *F0 = nullptr);
+// launch-shape autotuner of the IC-GN / Subpb1 kernels (k_icgn.cu)
+bool icgn_tuned(int precision, bool sub, int w, long long n);
+void icgn_autotune(bool on);
+int icgn_tuned_shape(int precision, bool sub, int w, long long n, int *nwarps, int *minb,
+                     float ms[8], int *count);
 int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,
            const double *FOld, const double *vdual, const double *H21, const int *wins, int w,
            double mu, double tol, int precision, double *U, int *iters, unsigned int *queue,

@@ -409,6 +409,10 @@ ALDIC_API int aldic_cnn_to_init(aldic_ctx *ctx, const float *out, long long n, d
  *                      constant-rate predictor standing in for the POD-GPR
  *                      prediction of main_ALDIC.m:133-146;
  *   ALDIC_INIT_GIVEN   the 2n values set by aldic_set_init;
+ *   ALDIC_INIT_GATED   the integer search + Init, then every node whose
+ *                      confidence set by aldic_set_init_gated reaches its
+ *                      threshold starts IC-GN from the given U0 and F0 instead
+ *                      (a learned guess with the search as its fallback);
  *   ALDIC_INIT_SEARCH_MG  the multigrid search (aldic_int_search_mg,
  *                      InitFFTSearchMethod other than 1 and 2) + Init: the
  *                      search decides the node grid, which the frame
@@ -425,6 +429,7 @@ ALDIC_API int aldic_cnn_to_init(aldic_ctx *ctx, const float *out, long long n, d
 #define ALDIC_INIT_EXTRAP 3
 #define ALDIC_INIT_GIVEN 4
 #define ALDIC_INIT_SEARCH_MG 5
+#define ALDIC_INIT_GATED 6
 typedef struct {
   int winsize, step;
   int search[2];
@@ -462,12 +467,36 @@ typedef struct {
   int max_pcg_iters;        /* most PCG iterations taken by one node-grid solve */
   double node_grid[4];      /* the node grid used: {x, y of the first node, M, N} */
   double t_search_mg_ms;    /* host time of the multigrid search (ALDIC_INIT_SEARCH_MG) */
+  int gated_init;           /* ALDIC_INIT_GATED: nodes started from the given guess */
 } aldic_frame_stats;
+
+/* Launch-shape autotuner of the IC-GN and Subpb1 kernels (no counterpart
+ * in the reference, whose funICGN runs one subset per call): the first
+ * launch of a geometry that may synchronise times every launch shape (warps
+ * per CTA x register cap, each computing bit-identical results) on its own
+ * data and keeps the fastest for the process; aldic_frame runs one eager
+ * frame before its first capture of a geometry for that.  enable = 0 turns
+ * the trials off (and forgets the choices): the default shape is used. */
+ALDIC_API int aldic_icgn_autotune(int enable);
+/* The shape chosen for (precision, subpb1 0/1, winsize -- -1 for per-subset
+ * sizes --, n subsets): warps per CTA, resident CTAs per SM in the launch
+ * bounds, and the trial time of each candidate shape (ms[count], count <= 8).
+ * ALDIC_E_STATE if that geometry has not been tuned. */
+ALDIC_API int aldic_icgn_shape(int precision, int subpb1, int winsize, long long n, int *nwarps,
+                               int *minb, float *ms, int *count);
 
 ALDIC_API int aldic_frame_dims(aldic_ctx *ctx, const aldic_frame_params *p, int *M, int *N);
 /* Initial guess for ALDIC_INIT_GIVEN: U0 interleaved [u1 v1 u2 v2 ...] on the
  * node grid of aldic_frame_dims (n2 = 2*M*N values, host or device). */
 ALDIC_API int aldic_set_init(aldic_ctx *ctx, const double *U0, long long n2);
+/* No counterpart in the reference (its data-driven guess is POD-GPR,
+ * main_ALDIC.m:133-146): an external initial guess for ALDIC_INIT_GATED
+ * frames -- U0 (2n), F0 (4n, [F11 F21 F12 F22] per node; NULL = 0, as
+ * funICGN.m:39 starts) and a confidence per node (n floats, NULL = all
+ * pass); nodes with conf >= conf_min take (U0, F0) as their IC-GN start,
+ * the others the integer search's.  Host or device arrays. */
+ALDIC_API int aldic_set_init_gated(aldic_ctx *ctx, const double *U0, const double *F0,
+                                   const float *conf, double conf_min, long long n);
 ALDIC_API int aldic_frame(aldic_ctx *ctx, const aldic_frame_params *p, double *x0, double *y0,
                 double *U, double *F, int32_t *iters, aldic_frame_stats *stats);
 
