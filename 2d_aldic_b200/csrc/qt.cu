@@ -10,7 +10,29 @@
 #include <thread>
 #include <vector>
 
+#include <mutex>
+
 #include "qt.cuh"
+
+namespace {
+// Device slabs of released meshes, kept for the next mesh of the same device:
+// a quadtree frame replaces its mesh on every search frame, and a free plus a
+// fresh allocation of the slab each time would put cudaFree's device
+// synchronisation and the allocator's page mapping on the frame's path.
+struct SlabCache {
+  std::mutex mu;
+  struct Entry {
+    int device;
+    aldic::DevBuf buf;
+  };
+  std::vector<Entry> free;
+  static constexpr size_t kMax = 4;
+};
+SlabCache &slab_cache() {
+  static SlabCache c;
+  return c;
+}
+}  // namespace
 
 void aldic_qt_mesh::release() {
   aldic::DevBuf *b[] = {&d_coords, &d_elems, &d_row, &d_col, &d_dpos, &d_iptr, &d_inc, &d_ipos,
@@ -20,8 +42,32 @@ void aldic_qt_mesh::release() {
     x->p = nullptr;
     x->cap = 0;
   }
+  if (slab.p && device >= 0) {
+    SlabCache &c = slab_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.free.size() < SlabCache::kMax) {
+      c.free.push_back({device, slab});
+      slab.p = nullptr;
+      slab.cap = 0;
+    }
+  }
   slab.release();
   device = -1;
+}
+
+// a cached slab of this device with at least `bytes`, the smallest that fits
+static void take_cached_slab(aldic::DevBuf &slab, int dev, size_t bytes) {
+  SlabCache &c = slab_cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  int best = -1;
+  for (size_t k = 0; k < c.free.size(); ++k)
+    if (c.free[k].device == dev && c.free[k].buf.cap >= bytes &&
+        (best < 0 || c.free[k].buf.cap < c.free[(size_t)best].buf.cap))
+      best = (int)k;
+  if (best < 0) return;
+  slab.release();
+  slab = c.free[(size_t)best].buf;
+  c.free.erase(c.free.begin() + best);
 }
 
 namespace aldic {
@@ -927,6 +973,7 @@ int qt_upload(aldic_qt_mesh &m, cudaStream_t st) {
     off += q.bytes > 0 ? q.bytes : 1;
   }
   int rc;
+  take_cached_slab(m.slab, dev, off);
   if ((rc = m.slab.ensure(off))) return rc;
   std::vector<unsigned char> host(upload, 0);
   off = 0;
