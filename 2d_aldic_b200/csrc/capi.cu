@@ -1718,7 +1718,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     return rc;
   // search work before any capture (a graph records its addresses)
   if ((qp.init == ALDIC_INIT_SEARCH || qp.init == ALDIC_INIT_GATED) &&
-      (rc = search_work_ensure(c->sw, c->W, c->H, M, N, p->search)))
+      (rc = search_work_ensure(c->sw, c->W, c->H, M, N, p->search, p->winsize, c->dtype)))
     return rc;
   // frame slab
   const long long ny_nx = n;
@@ -1747,11 +1747,11 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
   // the buffers the graph addresses
   char key[512];
   snprintf(key, sizeof key,
-           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p %p %p",
+           "%d %d %d|%d %d %d %d %d %d %d %d|%.17g %.17g %d %d|%.17g %.17g %.17g %d %d %d %d|%p %p %p %p %p %p %p",
            c->W, c->H, c->dtype, p->winsize, p->step, p->search[0], p->search[1], gx[0], gx[1],
            gy[0], gy[1], node0[0], node0[1], M, N, p->tol, p->mu, p->beta, p->n_admm, p->precision,
            p->smooth, qp.init * 2 + (p->subpb2_fd != 0),
-           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p, c->sw.buf.p, c->fdm.buf.p);
+           c->fr.p, c->gw_vec.p, c->g_raw.p, c->hist.p, c->sw.buf.p, c->fdm.buf.p, c->sw.big.p);
   if (realloc) c->drop_graphs();  // recorded against buffers that are gone
   const bool want_graph = p->use_graph && !c->graph_failed;
   aldic_ctx::FrameGraph *fg = nullptr;

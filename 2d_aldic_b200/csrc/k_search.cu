@@ -61,18 +61,34 @@ struct SearchGeom {
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
+// Shared-memory layout of the per-point kernel.  With big = true (search
+// regions whose window row sums and correlation map exceed the 227 KB of
+// shared memory a CTA may have) the row sums RS, RS2 and the map live in a
+// per-CTA slot of global work memory instead (`slot` bytes each, offsets
+// g_rs, g_rs2, g_map) and shared memory holds the template and the region.
 template <typename V, typename S>
 struct SmemLayout {
   size_t tp, dp, rs, rs2, colsum, rowsum, map, red, total;
-  __host__ __device__ SmemLayout(const SearchGeom &g) {
+  size_t g_rs, g_rs2, g_map, slot;
+  __host__ __device__ SmemLayout(const SearchGeom &g, bool big = false) {
     size_t o = 0;
     tp = o; o = align16(o + sizeof(V) * g.tw * g.twp);
     dp = o; o = align16(o + sizeof(V) * g.dph * g.dpw);
-    rs = o; o = align16(o + sizeof(S) * g.dph * g.cr);
-    rs2 = o; o = align16(o + sizeof(S) * g.dph * g.cr);
+    const size_t brs = align16(sizeof(S) * g.dph * g.cr), bmap = align16(sizeof(double) * g.cr * g.cc);
+    g_rs = 0;
+    g_rs2 = brs;
+    g_map = 2 * brs;
+    slot = (2 * brs + bmap + 255) & ~size_t(255);
+    rs = rs2 = map = 0;
+    if (!big) {
+      rs = o; o += brs;
+      rs2 = o; o += brs;
+    }
     colsum = o; o = align16(o + sizeof(S) * g.tw);
     rowsum = o; o = align16(o + sizeof(S) * g.tw);
-    map = o; o = align16(o + sizeof(double) * g.cr * g.cc);
+    if (!big) {
+      map = o; o += bmap;
+    }
     red = o; o = align16(o + (sizeof(double) + sizeof(int)) * 32 + 64);
     total = o;
   }
@@ -152,30 +168,35 @@ __device__ __forceinline__ void pad_terms(const SearchGeom &G, int a, int b, con
   *n_out = nco * G.tw + nro * G.tw - nco * nro;
 }
 
-template <typename T>
+// One CTA per grid point at a time, looping over the points (grid-stride):
+// with BIG the row sums and the map of the CTA's current point are in its
+// slot of the global work memory `work` (SmemLayout).
+template <typename T, bool BIG>
 __global__ void __launch_bounds__(512) k_search(const T *__restrict__ f, const T *__restrict__ g,
                                                 SearchGeom G, double *__restrict__ ox,
                                                 double *__restrict__ oy, double *__restrict__ ou,
-                                                double *__restrict__ ov, double *__restrict__ occ) {
+                                                double *__restrict__ ov, double *__restrict__ occ,
+                                                unsigned char *__restrict__ work) {
   using Tr = SearchTraits<T>;
   using V = typename Tr::V;
   using RowAcc = typename Tr::RowAcc;
   using S = typename SumT<Tr::integer>::type;
   extern __shared__ __align__(16) unsigned char smem[];
-  const SmemLayout<V, S> L(G);
+  const SmemLayout<V, S> L(G, BIG);
+  unsigned char *wk = BIG ? work + (size_t)blockIdx.x * L.slot : nullptr;
   V *Tp = (V *)(smem + L.tp);
   V *Dp = (V *)(smem + L.dp);
-  S *RS = (S *)(smem + L.rs);
-  S *RS2 = (S *)(smem + L.rs2);
+  S *RS = BIG ? (S *)(wk + L.g_rs) : (S *)(smem + L.rs);
+  S *RS2 = BIG ? (S *)(wk + L.g_rs2) : (S *)(smem + L.rs2);
   S *colsum = (S *)(smem + L.colsum);
   S *rowsum = (S *)(smem + L.rowsum);
-  double *map = (double *)(smem + L.map);
+  double *map = BIG ? (double *)(wk + L.g_map) : (double *)(smem + L.map);
   double *redv = (double *)(smem + L.red);
   int *redi = (int *)(redv + 32);
   __shared__ S s_st, s_st2;
   const double mu = *G.mu;
 
-  const int pt = blockIdx.x;
+  for (int pt = blockIdx.x; pt < G.nx * G.ny; pt += gridDim.x) {
   const int ix = pt % G.nx, iy = pt / G.nx;
   const int ii = G.gx1 + ix * G.step, jj = G.gy1 + iy * G.step;  // 1-based
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -251,7 +272,8 @@ __global__ void __launch_bounds__(512) k_search(const T *__restrict__ f, const T
       ov[out_idx] = nan;
       occ[out_idx] = nan;
     }
-    return;
+    __syncthreads();  // the next point restages the template
+    continue;
   }
 
   // ---- correlation strips
@@ -308,6 +330,8 @@ __global__ void __launch_bounds__(512) k_search(const T *__restrict__ f, const T
   }
   __syncthreads();
   peak_epilogue(map, G, ii, jj, out_idx, redv, redi, ox, oy, ou, ov, occ);
+  __syncthreads();  // the next point overwrites the staging and the map
+  }
 }
 
 // ---- 8-bit images: byte-packed correlation with __dp4a (exact int32).
@@ -1537,6 +1561,45 @@ __global__ void k_qfactor(const T *__restrict__ f, const T *__restrict__ g, Sear
   }
 }
 
+constexpr size_t kSmemMax = 227 * 1024;
+constexpr int kBigBlocks = 296;  // CTAs (and global work slots) of the big-region search
+
+// Search regions too large for shared memory: the per-point kernel with its
+// row sums and map in global work slots, one per CTA, kBigBlocks CTAs
+// looping over the points.  The slots are in SearchWork::big, sized before
+// any capture by search_work_ensure (or here, outside a capture).
+template <typename T>
+int launch_big(const void *f, const void *g, const SearchGeom &G, double *x, double *y, double *u,
+               double *v, double *cc, cudaStream_t st, SearchWork *sw) {
+  using Tr = SearchTraits<T>;
+  using V = typename Tr::V;
+  using S = typename SumT<Tr::integer>::type;
+  const SmemLayout<V, S> L(G, true);
+  ALDIC_CHECK(L.total <= kSmemMax, E_ARG,
+              "integer search: window/search size too large even with the map in global memory");
+  const int npts = G.nx * G.ny;
+  const int blocks = npts < kBigBlocks ? npts : kBigBlocks;
+  const size_t need = L.slot * (size_t)blocks;
+  ALDIC_CHECK(sw != nullptr, E_ARG, "integer search: this search region needs the context's work memory");
+  if (sw->big.cap < need) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    ALDIC_CUDA(cudaStreamIsCapturing(st, &cs));
+    ALDIC_CHECK(cs == cudaStreamCaptureStatusNone, E_STATE,
+                "integer search: work memory for this search region was not set up before capture");
+    int rc = sw->big.ensure(need);
+    if (rc) return rc;
+  }
+  int threads = ((G.cc * G.nsx + 31) / 32) * 32;
+  if (threads < 64) threads = 64;
+  if (threads > 512) threads = 512;
+  ALDIC_CUDA(cudaFuncSetAttribute(k_search<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)L.total));
+  k_search<T, true><<<blocks, threads, L.total, st>>>((const T *)f, (const T *)g, G, x, y, u, v, cc,
+                                                      sw->big.as<unsigned char>());
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
 template <typename T>
 int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, double *y,
                   double *u, double *v, double *cc, double *pce, double *ppe, cudaStream_t st,
@@ -1550,10 +1613,11 @@ int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, 
   if (threads > 512) threads = 512;
   const int npts = G.nx * G.ny;
   if (npts == 0) return OK;
-  if (sizeof(T) == 1) {
+  if (sizeof(T) == 1 && !(U8Layout(G).total <= kSmemMax && G.tw <= 72)) {
+    const int rc = launch_big<T>(f, g, G, x, y, u, v, cc, st, sw);
+    if (rc) return rc;
+  } else if (sizeof(T) == 1) {
     U8Layout L(G);
-    ALDIC_CHECK(L.total <= 227 * 1024 && G.tw <= 72, E_ARG,
-                "integer search: window/search size too large for shared memory");
     ALDIC_CUDA(cudaFuncSetAttribute(k_search_u8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)L.total));
     ALDIC_CUDA(cudaFuncSetAttribute(k_search_u8_list,
@@ -1569,11 +1633,15 @@ int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, 
                                                    y, u, v, cc);
   } else {
     SmemLayout<V, S> L(G);
-    ALDIC_CHECK(L.total <= 227 * 1024, E_ARG,
-                "integer search: window/search size too large for shared memory");
-    ALDIC_CUDA(cudaFuncSetAttribute(k_search<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)L.total));
-    k_search<T><<<npts, threads, L.total, st>>>((const T *)f, (const T *)g, G, x, y, u, v, cc);
+    if (L.total > kSmemMax) {
+      const int rc = launch_big<T>(f, g, G, x, y, u, v, cc, st, sw);
+      if (rc) return rc;
+    } else {
+      ALDIC_CUDA(cudaFuncSetAttribute(k_search<T, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+      k_search<T, false><<<npts, threads, L.total, st>>>((const T *)f, (const T *)g, G, x, y, u, v,
+                                                         cc, nullptr);
+    }
   }
   ALDIC_CUDA(cudaGetLastError());
   if (pce) {
@@ -1606,18 +1674,9 @@ int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsiz
   return OK;
 }
 
-int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2]) {
-  return w.buf.ensure(tile_bufs(nullptr, W, H, nx, ny, search).bytes);
-}
-
-int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,
-               const int gridx[2], const int gridy[2], int winsize, int step,
-               const int search[2], double *x, double *y, double *u, double *v, double *cc,
-               double *pce, double *ppe, cudaStream_t st, SearchWork *sw) {
-  SearchGeom G;
-  int rc = search_dims(W, H, gridx, gridy, winsize, step, search, &G.nx, &G.ny, &G.gx1, &G.gy1);
-  if (rc) return rc;
-  G.W = W; G.H = H; G.step = step; G.w = winsize; G.sx = search[0]; G.sy = search[1];
+// the window / region / map extents of a search geometry (funIntegerSearch.m:121-134)
+void geom_sizes(SearchGeom &G, int winsize, const int search[2]) {
+  G.w = winsize; G.sx = search[0]; G.sy = search[1];
   G.tw = winsize + 1;
   G.twp = (G.tw + KX - 1) / KX * KX;
   G.dw = G.tw + 2 * G.sx;
@@ -1628,6 +1687,41 @@ int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, co
   G.dpw = G.nsx * KX + G.twp - 1;
   if (G.dpw < G.dw + 2) G.dpw = G.dw + 2;
   G.dph = G.dh + 2;
+}
+
+template <typename T>
+size_t big_bytes(const SearchGeom &G) {
+  using Tr = SearchTraits<T>;
+  using S = typename SumT<Tr::integer>::type;
+  const bool small = sizeof(T) == 1 ? (U8Layout(G).total <= kSmemMax && G.tw <= 72)
+                                    : SmemLayout<typename Tr::V, S>(G).total <= kSmemMax;
+  if (small) return 0;
+  const int npts = G.nx * G.ny;
+  return SmemLayout<typename Tr::V, S>(G, true).slot * (size_t)(npts < kBigBlocks ? npts : kBigBlocks);
+}
+
+int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2], int winsize,
+                       int dtype) {
+  int rc = w.buf.ensure(tile_bufs(nullptr, W, H, nx, ny, search).bytes);
+  if (rc || winsize <= 0) return rc;
+  SearchGeom G{};
+  G.nx = nx;
+  G.ny = ny;
+  geom_sizes(G, winsize, search);
+  const size_t b = dtype == 0 ? big_bytes<uint8_t>(G) : dtype == 1 ? big_bytes<uint16_t>(G)
+                 : dtype == 2 ? big_bytes<float>(G) : big_bytes<double>(G);
+  return b ? w.big.ensure(b) : OK;
+}
+
+int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,
+               const int gridx[2], const int gridy[2], int winsize, int step,
+               const int search[2], double *x, double *y, double *u, double *v, double *cc,
+               double *pce, double *ppe, cudaStream_t st, SearchWork *sw) {
+  SearchGeom G;
+  int rc = search_dims(W, H, gridx, gridy, winsize, step, search, &G.nx, &G.ny, &G.gx1, &G.gy1);
+  if (rc) return rc;
+  G.W = W; G.H = H; G.step = step;
+  geom_sizes(G, winsize, search);
   G.mu = mu_g;
   switch (dtype) {
     case 0: return launch_search<uint8_t>(f_raw, g_raw, G, x, y, u, v, cc, pce, ppe, st, sw);

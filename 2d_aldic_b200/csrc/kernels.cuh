@@ -33,9 +33,16 @@ int interp_f32(const float *F, long long M, long long N, long long P, const floa
 // list of points handed to the per-point kernel and the correlation maps
 struct SearchWork {
   DevBuf buf;
-  void release() { buf.release(); }
+  DevBuf big;  // per-CTA row sums and maps of search regions too large for shared memory
+  void release() {
+    buf.release();
+    big.release();
+  }
 };
-int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2]);
+// work memory of a search geometry (with winsize > 0 and the image dtype also
+// the big-region slots), allocated ahead of any stream capture
+int search_work_ensure(SearchWork &w, int W, int H, int nx, int ny, const int search[2],
+                       int winsize = 0, int dtype = -1);
 int search_dims(int W, int H, const int gridx[2], const int gridy[2], int winsize, int step,
                 const int search[2], int *nx, int *ny, int *gx1, int *gy1);
 int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, const double *mu_g,

@@ -93,6 +93,25 @@ def test_int_search_bit_exact(aldic, oracle, plain, scale):
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("scale", [1, 257])
+def test_int_search_large_region_bit_exact(aldic, oracle, plain, scale):
+    """A search radius whose window row sums and correlation map exceed
+    shared memory (the reference manual's search zone of 60 px with subset
+    20): the per-point kernel keeps them in global work slots; u, v and
+    cc.max stay bit-exact with the oracle (8- and 16-bit images)."""
+    f, g = plain["f"], plain["g"]
+    if scale > 1:
+        f = (f.astype(np.uint32) * scale).astype(np.uint16)
+        g = (g.astype(np.uint32) * scale).astype(np.uint16)
+    H, W = f.shape
+    x, y, u, v, cc = aldic.funIntegerSearch(f, g, 60, [1, W], [1, H], 20, 10, 0, qfactors=False)
+    mg = g.astype(np.float64).mean()
+    xo, yo, uo, vo, co, _ = oracle.int_search(f, g, mg, [1, W], [1, H], 20, 10, [60, 60])
+    assert u.size > 100
+    for a, b in ((x, xo), (y, yo), (u, uo), (v, vo), (cc["max"], co)):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_int_search_qfactors_and_edges(aldic, oracle, synth):
     W = H = 160
     f = synth.speckle(W, H, 800, 21)
