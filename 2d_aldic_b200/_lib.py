@@ -60,6 +60,8 @@ _SIGS = {
     "aldic_compute_strain": ([P, I32, I32, D, I32, I32, I32, P, P, P, P], I32),
     "aldic_fdm_basis": ([I32, I32, D, P, P], I32),
     "aldic_set_stats": ([P, P], I32),
+    "aldic_qt_frame": ([P, P, P, P], I32),
+    "aldic_qt_frame_get": ([P, P, P, P, P, P, P], I32),
     "aldic_set_init_gated": ([P, P, P, P, D, I64], I32),
     "aldic_icgn_autotune": ([I32], I32),
     "aldic_icgn_shape": ([I32, I32, I32, C.c_longlong, P, P, P, P], I32),
@@ -100,6 +102,18 @@ class FrameStats(C.Structure):
                 ("update_y2", D * 16), ("mean_iters_icgn", D), ("kernel_launches", I32),
                 ("t_stage_ms", D * 8), ("max_pcg_iters", I32), ("node_grid", D * 4),
                 ("t_search_mg_ms", D), ("gated_init", I32)]
+
+
+class QtFrameParams(C.Structure):
+    _fields_ = [("winsize", I32), ("step", I32), ("search", I32), ("gridx", I32 * 2),
+                ("gridy", I32 * 2), ("tol", D), ("mu", D), ("tol2", D), ("n_admm", I32),
+                ("min_size", I32), ("precision", I32), ("subsets", I32)]
+
+
+class QtFrameStats(C.Structure):
+    _fields_ = [("n", I32), ("ne", I32), ("ndir", I32), ("bad_icgn", I32), ("admm_steps", I32),
+                ("mesh_reused", I32), ("beta", D), ("update_y", D * 16), ("update_y2", D * 16),
+                ("t_ms", D * 6)]
 
 
 class AldicError(RuntimeError):

@@ -23,7 +23,7 @@ from typing import Any
 import numpy as np
 
 from . import _lib
-from ._lib import AldicError, FrameParams, FrameStats, call
+from ._lib import AldicError, FrameParams, FrameStats, QtFrameParams, QtFrameStats, call
 
 try:  # torch is optional for host callers
     import torch
@@ -785,8 +785,9 @@ class QuadtreeMesh:
     nodes, 0 = none) and dirichlet (markCoordHoleEdge), held by the library
     (host data, device copies made on first use)."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, owned=True):
         self.h = handle
+        self.owned = owned   # False: a context's frame mesh, freed by the library
         n, ne, nd = C.c_int(), C.c_int(), C.c_int()
         call("aldic_qt_mesh_info", self.h, C.byref(n), C.byref(ne), C.byref(nd))
         self.n, self.ne, self.ndir = n.value, ne.value, nd.value
@@ -826,7 +827,8 @@ class QuadtreeMesh:
 
     def close(self):
         if getattr(self, "h", None):
-            _lib.lib().aldic_qt_mesh_destroy(self.h)
+            if getattr(self, "owned", True):
+                _lib.lib().aldic_qt_mesh_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -957,94 +959,53 @@ class ALDICQuadtree:
 
     def set_images(self, f, g, mask):
         self.f, self.g = f, g
+        self._mask_in = mask
         self.mask = np.ascontiguousarray(np.asarray(mask, np.float64))
+        self._mask_key = None
 
     def frame(self):
-        ctx, w, step = self.ctx, self.w, self.step
+        """One frame through aldic_qt_frame (all arrays on the device; the
+        mesh is regenerated when the search grid or the mask changes)."""
+        ctx = self.ctx
         f, g, mask = self.f, self.g, self.mask
         H, W = f.shape
         gx = self.gridx or (1, W)                 # DICpara.gridxyROIRange
         gy = self.gridy or (1, H)
         t0 = time.perf_counter()
-        # Section 3: integer search on the uniform grid, MeshSetUp, Init
-        x, y, u, v, _ = funIntegerSearch(f, g, self.search, gx, gy, w, step, 0, step,
-                                         qfactors=False, ctx=ctx)
-        xi, yi = np.asarray(x, int), np.asarray(y, int)
-        hole = mask[yi - 1, xi - 1] == 0                         # IntegerSearch.m:68-73
-        u = np.where(hole, np.nan, u)
-        v = np.where(hole, np.nan, v)
-        mesh0 = MeshSetUp(x, y, {"ImgSize": (W, H)})
-        U0u = Init(u, v, None, x, y, 0)
-        ny, nx = u.shape
-        t_search = time.perf_counter()
-        ctx.set_ref(f, roi=(gx[0], gx[1], gy[0], gy[1]), mask=mask)
+        if self._mask_key != (id(self._mask_in), id(f), gx, gy):
+            ctx.set_ref(f, roi=(gx[0], gx[1], gy[0], gy[1]), mask=mask)
+            self._mask_key = (id(self._mask_in), id(f), gx, gy)
         ctx.set_def(g)
-        if self.mesh is not None:
-            self.mesh.close()
-        m = self.mesh = QuadtreeMesh.generate(mesh0["coordinatesFEM"], mesh0["elementsFEM"], mask,
-                                              step, self.min_size)
-        c, n = m.coordinatesFEM, m.n
-        U0 = _interp_uniform(np.asarray(x)[0], np.asarray(y)[:, 0],
-                             [U0u[0::2].reshape(ny, nx), U0u[1::2].reshape(ny, nx)], c).reshape(-1)
-        wins = quadtree_subset_sizes(m, w, self.subsets)
-        t_mesh = time.perf_counter()
-        # Section 4: LocalICGN + flags + refill
-        U1, F1, it, Hp = local_icgn(ctx, c, U0, wins, self.tol, self.precision)
-        bad, nbad = icgn_flags(it, ctx=ctx)
-        U1 = quadtree_fill(m, np.where(bad[:, None] != 0, 0.0, U1.reshape(n, 2)), bad, ctx).reshape(-1)
-        F1 = quadtree_fill(m, np.where(bad[:, None] != 0, 0.0, F1.reshape(n, 4)), bad, ctx).reshape(-1)
-        U_icgn = U1.copy()
-        t_icgn = time.perf_counter()
-        # Section 5: beta sweep, Subpb2Quadtree, nodal strain
-        mu = self.mu
-        betas = np.array([1e-3, 1e-2, 1e-1]) * step * step * mu
-        e1, e2 = [], []
-        for b in betas:
-            U2 = Subpb2Quadtree(m, b, mu, U1, F1, ctx)
-            F2 = funGlobalNodalStrainQuadtree(m, U2, ctx)
-            e1.append(np.linalg.norm(U1 - U2))
-            e2.append(np.linalg.norm(F1 - F2))
-        beta = _select_beta(betas, e1, e2)
-        if abs(beta - betas[-1]) > np.finfo(float).eps:
-            U2 = Subpb2Quadtree(m, beta, mu, U1, F1, ctx)
-            F2 = funGlobalNodalStrainQuadtree(m, U2, ctx)
-        d = m.dirichlet
-        dd = np.repeat(4 * (d - 1), 4) + np.tile(np.arange(4), len(d))
-        F2[dd] = F1[dd]                                   # main_ALDIC_Quadtree.m:205-207
-        udual, vdual = F2 - F1, U2 - U1
-        t_s5 = time.perf_counter()
-        # Section 6: ADMM
-        upd, upd2 = [], []
-        U1old = U1.copy()
-        Hc = np.ascontiguousarray(Hp.T)
-        cf = _coords_cm(c)
-        wa = _prep(wins, np.int32)
-        for _ in range(self.n_admm):
-            U2old = U2.copy()
-            U1 = np.empty(2 * n)
-            it1 = np.empty(n, np.int32)
-            call("aldic_subpb1", ctx.h, _ptr(cf), n, _ptr(_prep(U2)), _ptr(_prep(F2)),
-                 _ptr(_prep(vdual)), _ptr(Hc), _ptr(wa), 0, float(mu), self.tol, self.precision,
-                 _ptr(U1), _ptr(it1))
-            b1, _ = icgn_flags(it1, 20.0, ctx)
-            U1 = quadtree_fill(m, np.where(b1[:, None] != 0, 0.0, U1.reshape(n, 2)), b1, ctx).reshape(-1)
-            F1 = F2.copy()
-            U2 = Subpb2Quadtree(m, beta, mu, U1, F1, ctx)
-            F2 = funGlobalNodalStrainQuadtree(m, U2, ctx)
-            F2[dd] = F1[dd]
-            upd.append(float(np.linalg.norm(U2old - U2) / np.sqrt(2 * n)))
-            upd2.append(float(np.linalg.norm(U1old - U1) / np.sqrt(2 * n)))
-            U1old = U1.copy()
-            udual, vdual = F2 - F1, U2 - U1
-            if upd[-1] < self.tol2 or upd2[-1] < self.tol2:
-                break
+        p = QtFrameParams()
+        p.winsize, p.step, p.search = self.w, self.step, self.search
+        p.gridx[0], p.gridx[1] = gx
+        p.gridy[0], p.gridy[1] = gy
+        p.tol, p.mu, p.tol2, p.n_admm = self.tol, self.mu, self.tol2, self.n_admm
+        p.min_size, p.precision = self.min_size, self.precision
+        if self.subsets not in ("uniform", "element"):
+            raise ValueError("subsets must be 'uniform' or 'element'")
+        p.subsets = 1 if self.subsets == "element" else 0
+        mh = C.c_void_p()
+        st = QtFrameStats()
+        call("aldic_qt_frame", ctx.h, C.byref(p), C.byref(mh), C.byref(st))
+        if self.mesh is None or not st.mesh_reused:
+            self.mesh = QuadtreeMesh(mh.value, owned=False)
+        m = self.mesh
+        n = st.n
+        U0, Ui, U, F = np.empty(2 * n), np.empty(2 * n), np.empty(2 * n), np.empty(4 * n)
+        it, wins = np.empty(n, np.int32), np.empty(n, np.int32)
+        call("aldic_qt_frame_get", ctx.h, _ptr(U0), _ptr(Ui), _ptr(U), _ptr(F), _ptr(it), _ptr(wins))
         t1 = time.perf_counter()
-        return {"coords": c, "elems": m.elementsFEM, "dirichlet": d, "U": U2, "F": F2,
-                "U_icgn": U_icgn, "iters_icgn": it, "bad_icgn": nbad, "beta": beta,
-                "update_y": upd, "update_y2": upd2, "wins": wins, "U0": U0,
-                "time_s": {"search": t_search - t0, "mesh": t_mesh - t_search,
-                           "search_mesh": t_mesh - t0, "icgn": t_icgn - t_mesh,
-                           "section5": t_s5 - t_icgn, "admm": t1 - t_s5, "frame": t1 - t0}}
+        k = st.admm_steps
+        tm = list(st.t_ms)
+        return {"coords": m.coordinatesFEM, "elems": m.elementsFEM, "dirichlet": m.dirichlet,
+                "U": U, "F": F, "U_icgn": Ui, "iters_icgn": it, "bad_icgn": st.bad_icgn,
+                "beta": st.beta, "update_y": list(st.update_y)[:k],
+                "update_y2": list(st.update_y2)[:k], "wins": wins, "U0": U0,
+                "mesh_reused": bool(st.mesh_reused),
+                "time_s": {"search": tm[0] / 1e3, "mesh": tm[1] / 1e3, "search_mesh": (tm[0] + tm[1]) / 1e3,
+                           "icgn": tm[2] / 1e3, "section5": tm[3] / 1e3, "admm": tm[4] / 1e3,
+                           "frame": t1 - t0}}
 
 
 # ------------------------------------------------------------------ learned init

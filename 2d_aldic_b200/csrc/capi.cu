@@ -79,6 +79,21 @@ struct aldic_ctx {
   bool have_ref = false, have_def = false;
   bool prepared = false;  // fields given by aldic_set_fields (no normalisation)
   bool has_mask = false;  // the last aldic_set_ref had an ImgRefMask
+  std::vector<double> mask_host;  // its host copy (quadtree mesh generation)
+  long long mask_version = 0;     // bumped by every aldic_set_ref with a mask
+  // aldic_qt_frame: the mesh of the last frame (reused while the search grid
+  // and the mask are unchanged), its subset sizes and the frame's arrays
+  struct QtFrame {
+    aldic_qt_mesh *mesh = nullptr;
+    long long key[9] = {};
+    DevBuf wins, slab, ugrid;
+    int n = 0;
+    double *U0 = nullptr, *U1 = nullptr, *F1 = nullptr, *U2 = nullptr, *F2 = nullptr;
+    double *ud = nullptr, *vd = nullptr, *U2old = nullptr, *U1old = nullptr, *H21 = nullptr;
+    double *norms = nullptr, *Uicgn = nullptr;
+    int *it1 = nullptr, *itb = nullptr, *ints = nullptr;
+    unsigned char *bad = nullptr;
+  } qtf;
   DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
   DevBuf g4;  // row runs of g32 (float4 per pixel) read by the FP32 IC-GN sampler
   DevBuf gxy;  // (gx32, gy32) pairs (float2 per pixel) read by the FP32 IC-GN
@@ -398,6 +413,13 @@ int aldic_ctx_destroy(aldic_ctx *c) {
   c->sw.release();
   c->fdm.release();
   c->given.release();
+  c->qtf.wins.release();
+  c->qtf.slab.release();
+  c->qtf.ugrid.release();
+  if (c->qtf.mesh) {
+    c->qtf.mesh->release();
+    delete c->qtf.mesh;
+  }
   c->arena.release();
   if (c->own_stream) cudaStreamDestroy(c->stream);
   cudaSetDevice(prev);
@@ -457,6 +479,10 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     if ((rc = c->mask.ensure(sizeof(double) * n))) return rc;
     ALDIC_CUDA(cudaMemcpyAsync(c->mask.p, mask, sizeof(double) * n, cudaMemcpyDefault, c->stream));
     dmask = c->mask.as<double>();
+    c->mask_host.resize((size_t)n);
+    ALDIC_CUDA(cudaMemcpyAsync(c->mask_host.data(), mask, sizeof(double) * n, cudaMemcpyDefault,
+                               c->stream));
+    c->mask_version++;
   }
   c->has_mask = dmask != nullptr;
   double *st = c->stats.as<double>();
@@ -1571,9 +1597,332 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   return OK;
 }
 
+// ---------------------------------------------------------------- quadtree frame
+// IntegerSearch.m:68-73: search results at nodes inside the mask's hole are NaN
+__global__ void k_qt_hole(long long n, const double *sx, const double *sy, double *su, double *sv,
+                          const double *mask, int W) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long xi = (long long)sx[k], yi = (long long)sy[k];
+    if (mask[(yi - 1) * W + (xi - 1)] == 0.0) {
+      su[k] = __longlong_as_double(0x7ff8000000000000ll);
+      sv[k] = su[k];
+    }
+  }
+}
+
+// U0 on the quadtree nodes: bilinear on the uniform node grid (x0 + i step,
+// y0 + j step; cell clamped to the grid), standing in for scatteredInterpolant
+// 'linear' of GenerateQuadtreeMesh.m:124-130
+__global__ void k_qt_interp(long long n, const double *qc, double x0, double y0, double step,
+                            int nx, int ny, const double *U0u, double *U0q) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const double x = qc[k], y = qc[n + k];
+    int i = (int)floor((x - x0) / step), j = (int)floor((y - y0) / step);
+    i = i < 0 ? 0 : (i > nx - 2 ? nx - 2 : i);
+    j = j < 0 ? 0 : (j > ny - 2 ? ny - 2 : j);
+    const double xi = x0 + i * step, yj = y0 + j * step;
+    const double tx = (x - xi) / ((x0 + (i + 1) * step) - xi);
+    const double ty = (y - yj) / ((y0 + (j + 1) * step) - yj);
+    for (int f = 0; f < 2; ++f) {
+      const double a = U0u[2 * ((long long)j * nx + i) + f], b = U0u[2 * ((long long)j * nx + i + 1) + f];
+      const double c = U0u[2 * ((long long)(j + 1) * nx + i) + f],
+                   d = U0u[2 * ((long long)(j + 1) * nx + i + 1) + f];
+      U0q[2 * k + f] = (1 - ty) * ((1 - tx) * a + tx * b) + ty * ((1 - tx) * c + tx * d);
+    }
+  }
+}
+
+// flagged nodes start the refill from 0 (nf interleaved fields)
+__global__ void k_zero_bad(long long n, int nf, double *v, const unsigned char *bad) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    if (bad[k])
+      for (int f = 0; f < nf; ++f) v[nf * k + f] = 0.0;
+}
+
+// main_ALDIC_Quadtree.m:205-207: the Dirichlet nodes keep Subproblem 1's strains
+__global__ void k_qt_keep_dirichlet(long long n, const unsigned char *kind, const double *F1,
+                                    double *F2) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    if (kind[k] == 1)
+      for (int q = 0; q < 4; ++q) F2[4 * k + q] = F1[4 * k + q];
+}
+
+// main_ALDIC_Quadtree.m:179-190: normalised error sum over the beta sweep,
+// the parabola vertex in log10(beta) around its minimum (or the minimising
+// beta at either end)
+double qt_select_beta(const double *b, const double *e1, const double *e2, int nb) {
+  double m1 = 0, m2 = 0;
+  for (int k = 0; k < nb; ++k) { m1 += e1[k]; m2 += e2[k]; }
+  m1 /= nb; m2 /= nb;
+  double v1 = 0, v2 = 0;
+  for (int k = 0; k < nb; ++k) { v1 += (e1[k] - m1) * (e1[k] - m1); v2 += (e2[k] - m2) * (e2[k] - m2); }
+  v1 = std::sqrt(v1 / (nb - 1)); v2 = std::sqrt(v2 / (nb - 1));
+  double es[8];
+  int ib = 0;
+  for (int k = 0; k < nb; ++k) {
+    es[k] = (e1[k] - m1) / v1 + (e2[k] - m2) / v2;
+    if (es[k] < es[ib]) ib = k;
+  }
+  if (ib >= 1 && ib <= nb - 2) {
+    const double x0 = std::log10(b[ib - 1]), x1 = std::log10(b[ib]), x2 = std::log10(b[ib + 1]);
+    const double d01 = (es[ib] - es[ib - 1]) / (x1 - x0), d12 = (es[ib + 1] - es[ib]) / (x2 - x1);
+    const double p1 = (d12 - d01) / (x2 - x0), p2 = d01 - p1 * (x0 + x1);
+    return std::pow(10.0, -p2 / 2.0 / p1);
+  }
+  return b[ib];
+}
+
 }  // namespace
 
 extern "C" {
+
+int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh **mesh_out,
+                   aldic_qt_frame_stats *stats) {
+  ALDIC_CHECK(c && p && mesh_out, E_ARG, "qt_frame: null argument");
+  ALDIC_CHECK(c->have_ref && c->have_def && c->has_mask && !c->prepared, E_STATE,
+              "qt_frame: set the reference image with its ImgRefMask (aldic_set_ref) and the "
+              "deformed image first");
+  ALDIC_CHECK(p->winsize > 0 && p->step > 0 && p->search >= 0 && p->tol > 0 && p->mu > 0 &&
+                  p->n_admm >= 0 && p->n_admm <= 16 && p->min_size >= 1,
+              E_ARG, "qt_frame: bad parameters");
+  Guard g(c);
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  cudaStream_t st = c->stream;
+  const int W = c->W, H = c->H, w = p->winsize, step = p->step;
+  const int gx[2] = {p->gridx[1] > 0 ? p->gridx[0] : 1, p->gridx[1] > 0 ? p->gridx[1] : W};
+  const int gy[2] = {p->gridy[1] > 0 ? p->gridy[0] : 1, p->gridy[1] > 0 ? p->gridy[1] : H};
+  const int srch[2] = {p->search, p->search};
+  int nx = 0, ny = 0, gx1 = 0, gy1 = 0, rc;
+  if ((rc = search_dims(W, H, gx, gy, w, step, srch, &nx, &ny, &gx1, &gy1))) return rc;
+  ALDIC_CHECK(nx >= 2 && ny >= 2, E_ARG, "qt_frame: the search grid needs 2 x 2 nodes");
+  const long long n0 = (long long)nx * ny;
+  // ---- Section 3: whole-field search on the uniform grid, holes, Init
+  if ((rc = search_work_ensure(c->sw, W, H, nx, ny, srch, w, c->dtype))) return rc;
+  auto &Q = c->qtf;
+  if ((rc = Q.ugrid.ensure(sizeof(double) * (11 * n0 + 1024)))) return rc;
+  double *sx = Q.ugrid.as<double>(), *sy = sx + n0, *su = sy + n0, *sv = su + n0, *scc = sv + n0;
+  double *ucoords = scc + n0, *ux0 = ucoords + 2 * n0, *uy0 = ux0 + n0, *U0u = uy0 + n0;
+  if ((rc = int_search(c->f_raw.p, c->g_raw.p, c->dtype, W, H, c->stats.as<double>() + 2, gx, gy, w,
+                       step, srch, sx, sy, su, sv, scc, nullptr, nullptr, st, &c->sw)))
+    return rc;
+  const int nb0 = (int)((n0 + 255) / 256 > 1184 ? 1184 : (n0 + 255) / 256);
+  k_qt_hole<<<nb0, 256, 0, st>>>(n0, sx, sy, su, sv, c->mask.as<double>(), W);
+  k_mesh_init<<<nb0, 256, 0, st>>>(nx, ny, sx, sy, su, sv, ucoords, ux0, uy0, U0u);
+  if ((rc = ensure_grid_work(c, n0))) return rc;
+  if ((rc = inpaint_load(c->gw, nx, ny, 2, U0u, 2, nullptr, st, 0)) ||
+      (rc = grid_pcg(c->gw, OP_INPAINT, nx, ny, 2, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st)) ||
+      (rc = inpaint_store(c->gw, nx, ny, 2, U0u, 2, st, 0)))
+    return rc;
+  ALDIC_CUDA(cudaStreamSynchronize(st));
+  const auto t1 = clk::now();
+  // ---- the quadtree mesh of GenerateQuadtreeMesh.m (kept while the grid and mask stay)
+  const double xf = gx1 + w / 2.0, yf = gy1 + w / 2.0;  // first node, funIntegerSearch.m:158-159
+  const long long key[9] = {W, H, c->mask_version, gx1, gy1, nx, ny, step,
+                            (long long)p->min_size * 4 + p->subsets};
+  bool reused = Q.mesh && std::equal(key, key + 9, Q.key);
+  if (!reused) {
+    if (Q.mesh) {
+      Q.mesh->release();
+      delete Q.mesh;
+      Q.mesh = nullptr;
+    }
+    std::vector<double> cu(2 * n0);
+    std::vector<int32_t> eu(4 * (size_t)(nx - 1) * (ny - 1));
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        cu[(size_t)j * nx + i] = xf + (double)i * step;
+        cu[n0 + (size_t)j * nx + i] = yf + (double)j * step;
+      }
+    const long long ne0 = (long long)(nx - 1) * (ny - 1);  // MeshSetUp.m:37, counter-clockwise
+    long long e = 0;
+    for (int j = 1; j < ny; ++j)
+      for (int i = 1; i < nx; ++i, ++e) {
+        eu[e] = (j - 1) * nx + i;
+        eu[ne0 + e] = (j - 1) * nx + i + 1;
+        eu[2 * ne0 + e] = j * nx + i + 1;
+        eu[3 * ne0 + e] = j * nx + i;
+      }
+    auto *m = new aldic_qt_mesh();
+    rc = qt_generate((int)n0, cu.data(), (int)ne0, eu.data(), c->mask_host.data(), W, H, (double)step,
+                     p->min_size, *m);
+    if (rc) {
+      delete m;
+      return rc;
+    }
+    if ((rc = qt_upload(*m, st))) {
+      delete m;
+      return rc;
+    }
+    Q.mesh = m;
+    std::copy(key, key + 9, Q.key);
+    // subset size per node: the reference's uniform winsize (Subpb1Quadtree.m:50)
+    // or twice the smallest side of the node's elements, in [16, 64], even
+    const int n = m->n, ne = m->ne;
+    std::vector<int32_t> wv((size_t)n, w);
+    if (p->subsets == 1) {
+      std::vector<double> side((size_t)n, INFINITY);
+      for (int k = 0; k < ne; ++k) {
+        const int a = m->elems[k] - 1, b = m->elems[2 * (size_t)ne + k] - 1;
+        const double sz = std::fabs(m->coords[b] - m->coords[a]);
+        for (int q = 0; q < 8; ++q) {
+          const int v = m->elems[(size_t)q * ne + k];
+          if (v > 0) side[v - 1] = std::min(side[v - 1], sz);
+        }
+      }
+      for (int k = 0; k < n; ++k) {
+        const double sd = std::isfinite(side[k]) ? side[k] : w / 2.0;
+        const double cl = std::min(64.0, std::max(16.0, 2.0 * sd));
+        wv[k] = (int32_t)(2.0 * std::nearbyint(cl / 2.0));
+      }
+    }
+    if ((rc = Q.wins.ensure(sizeof(int32_t) * n))) return rc;
+    ALDIC_CUDA(cudaMemcpyAsync(Q.wins.p, wv.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    ALDIC_CUDA(cudaStreamSynchronize(st));
+  }
+  aldic_qt_mesh &m = *Q.mesh;
+  const long long n = m.n;
+  const int nb = (int)((n + 255) / 256 > 1184 ? 1184 : (n + 255) / 256);
+  if ((rc = Q.slab.ensure(sizeof(double) * (49 * n + 2048) + sizeof(int) * (2 * n + 16) + n + 512)))
+    return rc;
+  {
+    char *q = (char *)Q.slab.p;
+    Q.U0 = carve<double>(q, 2 * n); Q.U1 = carve<double>(q, 2 * n); Q.F1 = carve<double>(q, 4 * n);
+    Q.U2 = carve<double>(q, 2 * n); Q.F2 = carve<double>(q, 4 * n); Q.ud = carve<double>(q, 4 * n);
+    Q.vd = carve<double>(q, 2 * n); Q.U2old = carve<double>(q, 2 * n); Q.U1old = carve<double>(q, 2 * n);
+    Q.H21 = carve<double>(q, 21 * n); Q.norms = carve<double>(q, 2048); Q.Uicgn = carve<double>(q, 2 * n);
+    Q.it1 = carve<int>(q, n); Q.itb = carve<int>(q, n); Q.ints = carve<int>(q, 16);
+    Q.bad = carve<unsigned char>(q, n);
+    Q.n = (int)n;
+  }
+  double *part = Q.norms + 1024, *nrm = Q.norms;  // nrm: [0,8) sweep, [8,40) ADMM
+  k_qt_interp<<<nb, 256, 0, st>>>(n, m.d_coords.as<double>(), xf, yf, (double)step, nx, ny, U0u, Q.U0);
+  ALDIC_CUDA(cudaGetLastError());
+  if ((rc = ensure_grid_work(c, n > n0 ? n : n0))) return rc;
+  const auto t2 = clk::now();
+  // ---- Section 4: LocalICGN on every quadtree node, flags, refill
+  const IcgnImages im = images_of(c);
+  const double *qcoords = m.d_coords.as<double>();
+  const int *wins = Q.wins.as<int>();
+  if ((rc = icgn(im, qcoords, n, Q.U0, wins, w, p->tol, p->precision, Q.U1, Q.F1, Q.it1, Q.H21,
+                 c->queue.as<unsigned int>(), st, nullptr)))
+    return rc;
+  double *mean = (double *)(Q.ints + 8);
+  if ((rc = icgn_flags((int)n, 1, Q.it1, Q.bad, Q.ints, mean, Q.ints + 1, st))) return rc;
+  k_zero_bad<<<nb, 256, 0, st>>>(n, 2, Q.U1, Q.bad);
+  k_zero_bad<<<nb, 256, 0, st>>>(n, 4, Q.F1, Q.bad);
+  if ((rc = qt_fill(m, c->gw, 2, Q.U1, Q.bad, st)) || (rc = qt_fill(m, c->gw, 4, Q.F1, Q.bad, st)))
+    return rc;
+  ALDIC_CUDA(cudaMemcpyAsync(Q.Uicgn, Q.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+  int nbad = 0;
+  ALDIC_CUDA(cudaMemcpyAsync(&nbad, Q.ints, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ALDIC_CUDA(cudaStreamSynchronize(st));
+  if ((rc = check_grid_err(c))) return rc;
+  const auto t3 = clk::now();
+  // ---- Section 5: beta sweep, Subpb2Quadtree, nodal strain (main_ALDIC_Quadtree.m:175-207)
+  const double mu = p->mu;
+  const double betas[3] = {1e-3 * step * step * mu, 1e-2 * step * step * mu, 1e-1 * step * step * mu};
+  for (int k = 0; k < 3; ++k) {
+    if ((rc = qt_subpb2(m, c->gw, betas[k], mu, Q.U1, Q.F1, Q.U2, st)) ||
+        (rc = qt_strain(m, Q.U2, Q.F2, st)) ||
+        (rc = vdiffnorm(Q.U1, Q.U2, 2 * n, part, nrm + k, st)) ||
+        (rc = vdiffnorm(Q.F1, Q.F2, 4 * n, part, nrm + 4 + k, st)))
+      return rc;
+  }
+  double hn[8];
+  ALDIC_CUDA(cudaMemcpyAsync(hn, nrm, sizeof(hn), cudaMemcpyDeviceToHost, st));
+  ALDIC_CUDA(cudaStreamSynchronize(st));
+  if ((rc = check_grid_err(c))) return rc;
+  const double beta = qt_select_beta(betas, hn, hn + 4, 3);
+  if (std::fabs(beta - betas[2]) > 2.220446049250313e-16) {
+    if ((rc = qt_subpb2(m, c->gw, beta, mu, Q.U1, Q.F1, Q.U2, st)) || (rc = qt_strain(m, Q.U2, Q.F2, st)))
+      return rc;
+  }
+  const unsigned char *kind = m.d_kind.as<unsigned char>();
+  k_qt_keep_dirichlet<<<nb, 256, 0, st>>>(n, kind, Q.F1, Q.F2);
+  if ((rc = vsub(Q.F2, Q.F1, Q.ud, 4 * n, st)) || (rc = vsub(Q.U2, Q.U1, Q.vd, 2 * n, st))) return rc;
+  ALDIC_CUDA(cudaMemcpyAsync(Q.U1old, Q.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+  ALDIC_CUDA(cudaStreamSynchronize(st));
+  const auto t4 = clk::now();
+  // ---- Section 6: ADMM until step 4 or an update below tol2 (main_ALDIC_Quadtree.m:213-320)
+  double upd[16] = {}, upd2[16] = {};
+  int steps = 0;
+  const double inv = 1.0 / std::sqrt((double)(2 * n));
+  for (int a = 0; a < p->n_admm; ++a) {
+    ALDIC_CUDA(cudaMemcpyAsync(Q.U2old, Q.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    if ((rc = subpb1(im, qcoords, n, Q.U2, Q.F2, Q.vd, Q.H21, wins, w, mu, p->tol, p->precision, Q.U1,
+                     Q.itb, c->queue.as<unsigned int>(), st, nullptr)))
+      return rc;
+    if ((rc = icgn_flags((int)n, 1, Q.itb, Q.bad, Q.ints + 4, mean, Q.ints + 5, st, 20.0))) return rc;
+    k_zero_bad<<<nb, 256, 0, st>>>(n, 2, Q.U1, Q.bad);
+    if ((rc = qt_fill(m, c->gw, 2, Q.U1, Q.bad, st))) return rc;
+    ALDIC_CUDA(cudaMemcpyAsync(Q.F1, Q.F2, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, st));
+    if ((rc = qt_subpb2(m, c->gw, beta, mu, Q.U1, Q.F1, Q.U2, st)) || (rc = qt_strain(m, Q.U2, Q.F2, st)))
+      return rc;
+    k_qt_keep_dirichlet<<<nb, 256, 0, st>>>(n, kind, Q.F1, Q.F2);
+    if ((rc = vdiffnorm(Q.U2old, Q.U2, 2 * n, part, nrm + 8, st)) ||
+        (rc = vdiffnorm(Q.U1old, Q.U1, 2 * n, part, nrm + 9, st)))
+      return rc;
+    ALDIC_CUDA(cudaMemcpyAsync(Q.U1old, Q.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    if ((rc = vsub(Q.F2, Q.F1, Q.ud, 4 * n, st)) || (rc = vsub(Q.U2, Q.U1, Q.vd, 2 * n, st))) return rc;
+    double hv[2];
+    ALDIC_CUDA(cudaMemcpyAsync(hv, nrm + 8, sizeof(hv), cudaMemcpyDeviceToHost, st));
+    ALDIC_CUDA(cudaStreamSynchronize(st));  // the stop test needs the two norms
+    if ((rc = check_grid_err(c))) return rc;
+    upd[a] = hv[0] * inv;
+    upd2[a] = hv[1] * inv;
+    steps++;
+    if (p->tol2 > 0 && (upd[a] < p->tol2 || upd2[a] < p->tol2)) break;
+  }
+  ALDIC_CUDA(cudaGetLastError());
+  const auto t5 = clk::now();
+  *mesh_out = Q.mesh;
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->n = (int)n;
+    stats->ne = m.ne;
+    stats->ndir = (int)m.dirichlet.size();
+    stats->bad_icgn = nbad;
+    stats->admm_steps = steps;
+    stats->mesh_reused = reused ? 1 : 0;
+    stats->beta = beta;
+    for (int a = 0; a < 16; ++a) {
+      stats->update_y[a] = upd[a];
+      stats->update_y2[a] = upd2[a];
+    }
+    auto ms = [](clk::time_point a, clk::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    stats->t_ms[0] = ms(t0, t1);
+    stats->t_ms[1] = ms(t1, t2);
+    stats->t_ms[2] = ms(t2, t3);
+    stats->t_ms[3] = ms(t3, t4);
+    stats->t_ms[4] = ms(t4, t5);
+    stats->t_ms[5] = ms(t0, t5);
+  }
+  return OK;
+}
+
+int aldic_qt_frame_get(aldic_ctx *c, double *U0, double *U_icgn, double *U, double *F, int32_t *iters,
+                       int32_t *wins) {
+  ALDIC_CHECK(c && c->qtf.mesh && c->qtf.n > 0, E_STATE, "qt_frame_get: no quadtree frame on this context");
+  Guard g(c);
+  const long long n = c->qtf.n;
+  auto &Q = c->qtf;
+  cudaStream_t st = c->stream;
+  if (U0) ALDIC_CUDA(cudaMemcpyAsync(U0, Q.U0, sizeof(double) * 2 * n, cudaMemcpyDefault, st));
+  if (U_icgn) ALDIC_CUDA(cudaMemcpyAsync(U_icgn, Q.Uicgn, sizeof(double) * 2 * n, cudaMemcpyDefault, st));
+  if (U) ALDIC_CUDA(cudaMemcpyAsync(U, Q.U2, sizeof(double) * 2 * n, cudaMemcpyDefault, st));
+  if (F) ALDIC_CUDA(cudaMemcpyAsync(F, Q.F2, sizeof(double) * 4 * n, cudaMemcpyDefault, st));
+  if (iters) ALDIC_CUDA(cudaMemcpyAsync(iters, Q.it1, sizeof(int32_t) * n, cudaMemcpyDefault, st));
+  if (wins) ALDIC_CUDA(cudaMemcpyAsync(wins, Q.wins.p, sizeof(int32_t) * n, cudaMemcpyDefault, st));
+  ALDIC_CUDA(cudaStreamSynchronize(st));
+  return OK;
+}
 
 int aldic_icgn_autotune(int enable) {
   icgn_autotune(enable != 0);

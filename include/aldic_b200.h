@@ -307,6 +307,51 @@ ALDIC_API int aldic_qt_nodal_strain(aldic_ctx *ctx, aldic_qt_mesh *m, const doub
 ALDIC_API int aldic_qt_fill(aldic_ctx *ctx, aldic_qt_mesh *m, int nf, double *vals,
                             const uint8_t *bad);
 
+/* One quadtree frame, main_ALDIC_Quadtree.m Sections 3-6, driven from C++
+ * with every array on the device: the whole-field integer search on the
+ * uniform grid of the ROI, NaN inside the mask's hole (IntegerSearch.m:
+ * 68-73), Init's inpainting, the quadtree mesh of GenerateQuadtreeMesh.m
+ * (generated on the host; kept and reused while the search grid and the
+ * mask are unchanged -- the reference regenerates the same mesh every
+ * search frame), U0 interpolated onto its nodes, LocalICGN with the flags
+ * and refill, the three-value beta sweep of Subpb2Quadtree + nodal strain
+ * with the Dirichlet nodes keeping Subproblem 1's strains, then ADMM steps
+ * (Subpb1Quadtree flags with the floor 20 and refill, Subpb2Quadtree) until
+ * n_admm steps or an update norm below tol2.  The images come from
+ * aldic_set_ref (with the mask ImgRefMask) and aldic_set_def.  *mesh
+ * receives the frame's mesh, owned by the context (valid until its next
+ * quadtree frame); the results stay on the device for aldic_qt_frame_get.
+ * Left out as in the reference's non-interactive use: the outlier clicks
+ * of funRemoveOutliersQuadtree and the strain smoothing (regularizeNd). */
+typedef struct {
+  int winsize, step, search;
+  int gridx[2], gridy[2];   /* ROI; {0,0} = whole image */
+  double tol, mu, tol2;     /* 1e-2, 1e-3, 1e-2 in main_ALDIC_Quadtree.m */
+  int n_admm;               /* ADMM steps after step 1 at most (reference: 3) */
+  int min_size;             /* DICmesh.elementMinSize (reference: 2) */
+  int precision;            /* ALDIC_FP32 / ALDIC_FP64 */
+  int subsets;              /* 0: winsize everywhere (Subpb1Quadtree.m:50);
+                               1: twice the node's smallest element side, 16..64 */
+} aldic_qt_frame_params;
+typedef struct {
+  int n, ne, ndir;          /* mesh nodes, elements, Dirichlet nodes */
+  int bad_icgn;             /* LocalICGNBadPtNum */
+  int admm_steps;
+  int mesh_reused;          /* 1: the previous frame's mesh was kept */
+  double beta;
+  double update_y[16], update_y2[16];
+  double t_ms[6];           /* host wall time (ms): search + Init, mesh + U0, LocalICGN + refill,
+                               Section 5, ADMM, frame */
+} aldic_qt_frame_stats;
+ALDIC_API int aldic_qt_frame(aldic_ctx *ctx, const aldic_qt_frame_params *p, aldic_qt_mesh **mesh,
+                             aldic_qt_frame_stats *stats);
+/* The last quadtree frame's arrays (any pointer may be NULL; host or
+ * device): U0 (2n, the interpolated start), U_icgn (2n, LocalICGN after the
+ * refill), U (2n) and F (4n) of the last Subproblem 2, iters (n,
+ * ConvItPerEle of LocalICGN), wins (n, subset sizes). */
+ALDIC_API int aldic_qt_frame_get(aldic_ctx *ctx, double *U0, double *U_icgn, double *U, double *F,
+                                 int32_t *iters, int32_t *wins);
+
 /* Bad-subset flags on any node set: status < 0 or > 99, or iterations above
  * max(mean + 0.15 std over the good subsets, floor) -- LocalICGN.m:117-131
  * with floor = NaN, Subpb1Quadtree.m:172-181 with floor = 20.  bad: n bytes;
