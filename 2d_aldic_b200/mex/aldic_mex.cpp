@@ -258,17 +258,15 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
       mexErrMsgIdAndTxt("aldic:size", "coordinatesFEM is n x 2 and elementsFEM ne x 8");
     if (mxGetNumberOfElements(prhs[6]) != 2 * n || mxGetNumberOfElements(prhs[7]) != 4 * n)
       mexErrMsgIdAndTxt("aldic:size", "U is 2n and F is 4n");
-    // MATLAB column-major n x 2 / ne x 8 -> row-major pairs / 8-tuples
+    // the library's mesh arrays are MATLAB's column-major n x 2 / ne x 8 as
+    // they stand; only the element and Dirichlet indices change type
     const double *cs = dbl(prhs[1], "coordinatesFEM"), *es = dbl(prhs[2], "elementsFEM");
     const double *ds = dbl(prhs[3], "dirichlet");
-    std::vector<double> coords(2 * n);
     std::vector<int32_t> el(8 * ne), dir(nd);
-    for (size_t k = 0; k < n; ++k) { coords[2 * k] = cs[k]; coords[2 * k + 1] = cs[n + k]; }
-    for (size_t k = 0; k < ne; ++k)
-      for (int j = 0; j < 8; ++j) el[8 * k + j] = (int32_t)es[k + (size_t)j * ne];
+    for (size_t k = 0; k < 8 * ne; ++k) el[k] = (int32_t)es[k];
     for (size_t k = 0; k < nd; ++k) dir[k] = (int32_t)ds[k];
     aldic_qt_mesh *m = nullptr;
-    check(aldic_qt_mesh_create((int)n, coords.data(), (int)ne, el.data(), (int)nd, dir.data(), &m));
+    check(aldic_qt_mesh_create((int)n, cs, (int)ne, el.data(), (int)nd, dir.data(), &m));
     plhs[0] = mxCreateDoubleMatrix(2 * n, 1, mxREAL);
     const int rc = aldic_qt_subpb2(ctx(), m, mxGetScalar(prhs[4]), mxGetScalar(prhs[5]),
                                    dbl(prhs[6], "U"), dbl(prhs[7], "F"), mxGetPr(plhs[0]));

@@ -655,6 +655,60 @@ def largeshift_main(args, rank, world, local):
         }), flush=True)
 
 
+def initnet_main(args, rank, world, local):
+    """Forward pass of the learned initial guess's network alone (patch
+    extraction + the tcgen05 BF16 layers) on 16 384 patch pairs of a random
+    2048^2 image, random-init weights (its shapes do not depend on the
+    content or the weights): pairs/s and TFLOP/s against the bf16 peak."""
+    import torch
+    aldic = importlib.import_module("2d_aldic_b200")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = np.random.default_rng(0)
+    f = torch.from_numpy(r.integers(0, 255, (2048, 2048), dtype=np.uint8)).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = aldic.Context(local)
+    ctx.set_stream(stream)
+    ctx.set_ref(f)
+    ctx.set_def(f)
+    n = 16384
+    xy = np.stack([r.integers(40, 2008, n), r.integers(40, 2008, n)], 1).astype(np.float64)
+    net = aldic.InitNet(local, 1)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def run(k):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            net.predict(aldic.cnn_patches(ctx, xy), stream=stream)
+            b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    for k in range(max(1, args.warmup)):
+        run(k)
+    ms = [run(k) for k in range(args.steps)]
+    t = statistics.mean(ms)
+    fl = 2.0 * n * (2 * 64 * (64 * 128 + 128 * 128) + 64 * 64 * 128 + 4096 * 256 + 256 * 8)
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+    except Exception:
+        peak = 1590.0  # fallback burst figure
+    if rank == 0:
+        print(json.dumps({
+            "metric": "initial-guess network forward", "value": n / (t / 1e3), "unit": "pairs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 (FP32 accumulate)", "data": "synthetic (random image, random-init weights)",
+            "tflops": fl / (t / 1e3) / 1e12, "bf16_peak_tflops": peak,
+            "config": {"workload": "initnet16k: 16384 patch pairs of 64x64 from a 2048x2048 u8 image",
+                       "l2": "flushed between passes (256 MB write)"},
+        }), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -674,6 +728,9 @@ def main():
         return
     if args.workload.startswith("largeshift"):
         largeshift_main(args, rank, world, local)
+        return
+    if args.workload == "initnet16k":
+        initnet_main(args, rank, world, local)
         return
 
     import torch

@@ -19,10 +19,12 @@ def test_tuned_shapes_give_identical_results(aldic, oracle, synth, prec):
     gn, mg, _ = oracle.normalize(g)
     x, y, u, v, _, _ = oracle.int_search(f, g, mg, [1, W], [1, H], wl.winsize, wl.step,
                                          [wl.search, wl.search])
-    coords = np.stack([x.ravel(), y.ravel()], 1)
+    # the grid twice over: the tuner runs on launches of 2048 subsets or more
+    coords = np.tile(np.stack([x.ravel(), y.ravel()], 1), (2, 1))
     n = len(coords)
+    assert n >= 2048
     U0 = np.empty(2 * n)
-    U0[0::2], U0[1::2] = u.ravel(), v.ravel()
+    U0[0::2], U0[1::2] = np.tile(u.ravel(), 2), np.tile(v.ravel(), 2)
     p = aldic.FP64 if prec == "fp64" else aldic.FP32
     lib = aldic._lib.lib()
     ctx = aldic.Context(0)
