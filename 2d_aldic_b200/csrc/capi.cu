@@ -95,9 +95,8 @@ struct aldic_ctx {
     unsigned char *bad = nullptr;
   } qtf;
   DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
-  DevBuf g4;  // row runs of g32 (float4 per pixel) read by the FP32 IC-GN sampler
+  DevBuf gc;  // bicubic coefficients of g (4 float4 per pixel) read by the FP32 IC-GN sampler
   DevBuf gxy;  // (gx32, gy32) pairs (float2 per pixel) read by the FP32 IC-GN
-  DevBuf gp, gxyp;  // pixel-pair runs of g32 and of the gradients (float4 per pixel)
   DevBuf stats;   // double[4]: mean_f std_f mean_g std_g
   DevBuf isums;   // u64[2]
   DevBuf part;    // double[1024]
@@ -272,10 +271,8 @@ int check_grid_err(aldic_ctx *c) {
 IcgnImages images_of(aldic_ctx *c) {
   IcgnImages im;
   im.f32 = c->f32.as<float>(); im.g32 = c->g32.as<float>();
-  im.g4 = c->g4.as<float4>();
+  im.gc = c->gc.as<float4>();
   im.gxy = c->gxy.as<float2>();
-  im.gp = c->gp.as<float4>();
-  im.gxyp = c->gxyp.as<float4>();
   im.gx32 = c->gx32.as<float>(); im.gy32 = c->gy32.as<float>();
   im.f64 = c->f64.as<double>(); im.g64 = c->g64.as<double>();
   im.gx64 = c->gx64.as<double>(); im.gy64 = c->gy64.as<double>();
@@ -405,7 +402,7 @@ int aldic_ctx_destroy(aldic_ctx *c) {
   for (int k = 0; k < 8; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   DevBuf *bufs[] = {&c->f_raw, &c->g_raw, &c->f64, &c->g64, &c->f32, &c->g32, &c->gx64,
-                    &c->gy64, &c->gx32, &c->gy32, &c->g4, &c->gxy, &c->gp, &c->gxyp, &c->mask, &c->stats, &c->isums, &c->part,
+                    &c->gy64, &c->gx32, &c->gy32, &c->gc, &c->gxy, &c->mask, &c->stats, &c->isums, &c->part,
                     &c->gw_vec, &c->gw_part, &c->gw_mask, &c->gw_misc, &c->queue, &c->fr,
                     &c->hist};
   for (DevBuf *b : bufs) b->release();
@@ -453,10 +450,8 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     if ((rc = b->ensure(sizeof(double) * n))) return rc;
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
-  if ((rc = c->g4.ensure(sizeof(float4) * n))) return rc;
+  if ((rc = c->gc.ensure(4 * sizeof(float4) * n))) return rc;
   if ((rc = c->gxy.ensure(sizeof(float2) * n))) return rc;
-  if ((rc = c->gp.ensure(sizeof(float4) * n))) return rc;
-  if ((rc = c->gxyp.ensure(sizeof(float4) * n))) return rc;
   if ((rc = c->f_raw.ensure(es * n))) return rc;
   if ((rc = c->g_raw.ensure(es * n))) return rc;
   if (c->dtype != dtype || c->W != W || c->H != H) c->have_def = false;
@@ -496,9 +491,6 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     return rc;
   if ((rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
     return rc;
-  if ((rc = grad_pair_runs(c->gx32.as<float>(), c->gy32.as<float>(), W, H, c->gxyp.as<float4>(),
-                           c->stream)))
-    return rc;
   c->have_ref = true;
   return finish(c, true);
 }
@@ -511,8 +503,7 @@ static int prep_def(aldic_ctx *c) {
   if ((rc = normalize(c->g_raw.p, c->dtype, (long long)c->W * c->H, st + 2, c->g64.as<double>(),
                       c->g32.as<float>(), c->stream)))
     return rc;
-  if ((rc = row_runs(c->g32.as<float>(), c->W, c->H, c->g4.as<float4>(), c->stream))) return rc;
-  return pair_runs(c->g32.as<float>(), c->W, c->H, c->gp.as<float4>(), c->stream);
+  return cubic_table(c->g64.as<double>(), c->W, c->H, c->gc.as<float4>(), c->stream);
 }
 
 int aldic_set_def(aldic_ctx *c, const void *img, int dtype) {
@@ -544,15 +535,12 @@ int aldic_set_stats(aldic_ctx *c, const double stats[4]) {
                      c->gx64.as<double>(), c->gy64.as<double>(), c->gx32.as<float>(),
                      c->gy32.as<float>(), c->stream)))
     return rc;
-  if ((rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)) ||
-      (rc = grad_pair_runs(c->gx32.as<float>(), c->gy32.as<float>(), c->W, c->H, c->gxyp.as<float4>(),
-                           c->stream)))
+  if ((rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
     return rc;
   // the deformed image with stats[2..3] (not prep_def, which takes them from the ROI)
   if ((rc = normalize(c->g_raw.p, c->dtype, n, st + 2, c->g64.as<double>(), c->g32.as<float>(),
                       c->stream)) ||
-      (rc = row_runs(c->g32.as<float>(), c->W, c->H, c->g4.as<float4>(), c->stream)) ||
-      (rc = pair_runs(c->g32.as<float>(), c->W, c->H, c->gp.as<float4>(), c->stream)))
+      (rc = cubic_table(c->g64.as<double>(), c->W, c->H, c->gc.as<float4>(), c->stream)))
     return rc;
   return finish(c, true);
 }
@@ -630,10 +618,8 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     if ((rc = b->ensure(bytes))) return rc;
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
-  if ((rc = c->g4.ensure(sizeof(float4) * n))) return rc;
+  if ((rc = c->gc.ensure(4 * sizeof(float4) * n))) return rc;
   if ((rc = c->gxy.ensure(sizeof(float2) * n))) return rc;
-  if ((rc = c->gp.ensure(sizeof(float4) * n))) return rc;
-  if ((rc = c->gxyp.ensure(sizeof(float4) * n))) return rc;
   if (first) c->have_def = false;
   c->W = W; c->H = H; c->dtype = 3;
   c->prepared = true;
@@ -646,14 +632,9 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     ALDIC_CUDA(cudaMemcpyAsync(d64[k]->p, src[k], bytes, cudaMemcpyDefault, c->stream));
     k_to_f32<<<1184, 256, 0, c->stream>>>(d64[k]->as<double>(), d32[k]->as<float>(), n);
   }
-  if (gimg && (rc = row_runs(c->g32.as<float>(), W, H, c->g4.as<float4>(), c->stream))) return rc;
-  if (gimg && (rc = pair_runs(c->g32.as<float>(), W, H, c->gp.as<float4>(), c->stream))) return rc;
+  if (gimg && (rc = cubic_table(c->g64.as<double>(), W, H, c->gc.as<float4>(), c->stream))) return rc;
   if ((dfdx || dfdy) &&
       (rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
-    return rc;
-  if ((dfdx || dfdy) &&
-      (rc = grad_pair_runs(c->gx32.as<float>(), c->gy32.as<float>(), W, H, c->gxyp.as<float4>(),
-                           c->stream)))
     return rc;
   if (f) ALDIC_CUDA(cudaMemcpyAsync(c->f_raw.p, c->f64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
   if (gimg) ALDIC_CUDA(cudaMemcpyAsync(c->g_raw.p, c->g64.p, bytes, cudaMemcpyDeviceToDevice, c->stream));

@@ -195,7 +195,13 @@ int tridiagonal_qr(int n, std::vector<double> &d, std::vector<double> &e, std::v
 }
 
 // ---------------------------------------------------------------- device: FP64 products
-constexpr int TR = 32, TC = 32, KC = 16, GT = 64;  // 32 x 32 outputs per CTA, 4 x 4 per thread
+// 32 x 32 outputs per CTA, 2 x 4 per thread (128 threads).  The operand
+// tiles of a 128-wide K chunk are staged in shared memory at once (every
+// thread's loads in flight together), so a 243-long product takes two
+// load-compute rounds instead of a chain of small dependent ones: the solve's
+// products are latency-bound at these sizes.
+constexpr int TR = 32, TC = 32, KC = 128, GT = 128;
+constexpr int kSmem = 2 * KC * (TR + 1) * (int)sizeof(double);
 
 struct GemmArgs {
   const double *A, *B;
@@ -213,50 +219,49 @@ struct GemmArgs {
 };
 
 __global__ void __launch_bounds__(GT) k_fdm_gemm(GemmArgs g) {
-  __shared__ double As[KC][TR + 1];
-  __shared__ double Bs[KC][TC + 1];
+  extern __shared__ double sm[];
+  double *As = sm, *Bs = sm + KC * (TR + 1);  // [k][r], [k][c], rows padded to 33
   const int b = blockIdx.z;
   const int r0 = blockIdx.y * TR, c0 = blockIdx.x * TC;
-  const int tid = threadIdx.x, ty = tid >> 3, tx = tid & 7;
+  const int tid = threadIdx.x, ty = tid >> 3, tx = tid & 7;  // rows 2 ty.., columns 4 tx..
   const double *A = g.A + (long long)b * g.sab;
   const double *B = g.B + (long long)b * g.sbb;
-  double acc[4][4] = {};
+  double acc[2][4] = {};
   const bool a_rfast = g.sar <= g.sak, b_cfast = g.sbc <= g.sbk;
   for (int k0 = 0; k0 < g.K; k0 += KC) {
-    for (int e = tid; e < TR * KC; e += GT) {
-      const int rr = a_rfast ? e % TR : e / KC, kk = a_rfast ? e / TR : e % KC;
+    const int kc = g.K - k0 < KC ? g.K - k0 : KC;
+    for (int e = tid; e < TR * kc; e += GT) {
+      const int rr = a_rfast ? e % TR : e / kc, kk = a_rfast ? e / TR : e % kc;
       const int r = r0 + rr, k = k0 + kk;
-      As[kk][rr] = (r < g.R && k < g.K) ? A[(long long)r * g.sar + (long long)k * g.sak] : 0.0;
+      As[kk * (TR + 1) + rr] = r < g.R ? __ldg(A + (long long)r * g.sar + (long long)k * g.sak) : 0.0;
     }
-    for (int e = tid; e < TC * KC; e += GT) {
-      const int cc = b_cfast ? e % TC : e / KC, kk = b_cfast ? e / TC : e % KC;
+    for (int e = tid; e < TC * kc; e += GT) {
+      const int cc = b_cfast ? e % TC : e / kc, kk = b_cfast ? e / TC : e % kc;
       const int c = c0 + cc, k = k0 + kk;
-      Bs[kk][cc] = (c < g.Cn && k < g.K) ? B[(long long)k * g.sbk + (long long)c * g.sbc] : 0.0;
+      Bs[kk * (TC + 1) + cc] = c < g.Cn ? __ldg(B + (long long)k * g.sbk + (long long)c * g.sbc) : 0.0;
     }
     __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < KC; ++kk) {
-      double a[4], bb[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bb[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+#pragma unroll 4
+    for (int kk = 0; kk < kc; ++kk) {
+      const double *ar = As + kk * (TR + 1) + 2 * ty, *br = Bs + kk * (TC + 1) + 4 * tx;
+      const double a0 = ar[0], a1 = ar[1];
+      const double b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
+      acc[0][0] = fma(a0, b0, acc[0][0]); acc[0][1] = fma(a0, b1, acc[0][1]);
+      acc[0][2] = fma(a0, b2, acc[0][2]); acc[0][3] = fma(a0, b3, acc[0][3]);
+      acc[1][0] = fma(a1, b0, acc[1][0]); acc[1][1] = fma(a1, b1, acc[1][1]);
+      acc[1][2] = fma(a1, b2, acc[1][2]); acc[1][3] = fma(a1, b3, acc[1][3]);
     }
     __syncthreads();
   }
   const double beta = g.beta_ptr ? *g.beta_ptr : g.beta[b < 12 ? b : 11];
   double *C = g.C + (long long)b * g.scb;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = r0 + ty * 4 + i;
+  for (int i = 0; i < 2; ++i) {
+    const int r = r0 + 2 * ty + i;
     if (r >= g.R) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int c = c0 + tx * 4 + j;
+      const int c = c0 + 4 * tx + j;
       if (c >= g.Cn) continue;
       double v = acc[i][j];
       if (g.scale) v /= beta * (g.lr[r] + g.lc[c]) + g.mu;
@@ -265,9 +270,16 @@ __global__ void __launch_bounds__(GT) k_fdm_gemm(GemmArgs g) {
   }
 }
 
+// the kernel's dynamic shared memory (above the 48 KB default) on the current
+// device; set by fdm_ensure, ahead of any stream capture
+int gemm_setup() {
+  ALDIC_CUDA(cudaFuncSetAttribute(k_fdm_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+  return OK;
+}
+
 int gemm(const GemmArgs &g, int batch, cudaStream_t st) {
   dim3 grid((unsigned)((g.Cn + TC - 1) / TC), (unsigned)((g.R + TR - 1) / TR), (unsigned)batch);
-  k_fdm_gemm<<<grid, GT, 0, st>>>(g);
+  k_fdm_gemm<<<grid, GT, kSmem, st>>>(g);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
@@ -331,6 +343,8 @@ int fdm_basis_1d(int type, int n, double h, double *V, double *lam) {
 }
 
 int fdm_ensure(FdmBasis &B, int type, int M, int N, double h, cudaStream_t st) {
+  int rc0 = gemm_setup();
+  if (rc0) return rc0;
   if (B.type == type && B.M == M && B.N == N && B.h == h && B.buf.p) return OK;
   ALDIC_CHECK(M >= 1 && N >= 1, E_ARG, "fdm: empty grid");
   std::vector<double> host((size_t)M * M + (size_t)N * N + M + N);

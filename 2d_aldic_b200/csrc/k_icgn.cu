@@ -12,17 +12,15 @@
 // forms b, the convergence test and dP = -H\b with the FP64 Cholesky factor
 // of H, and applies the inverse-compositional update in FP64.
 //
-// FP32 evaluations sample two horizontally adjacent pixels (A, B) of a subset
-// row per lane and trip with the packed FP32 instructions of sm_100
-// (__ffma2_rn & co., two IEEE single-precision operations per instruction):
-// B's stencil is A's shifted one column whenever B's floor corner is A's
-// corner + (1, 0), and the pair runs gp (g[i], g[i+1], g[i+1], g[i+2]) then
-// hold the (A, B) tap pairs of a stencil row in two 16-byte loads -- the
-// weights, the 16 row products, the combination and the residual sums all
-// run on (A, B) pairs.  A pair whose B corner differs (the fraction of B
-// wrapped: about |F11| + |F21| of the pairs) drops B from the packed sums
-// and queues it in shared memory; the warp samples the queued pixels
-// together afterwards, one per lane, so the rare case costs no divergence.
+// FP32 sampling reads a per-cell table of the bicubic's polynomial
+// coefficients (cubic_table: 16 FP32 per pixel, four 16-byte loads), so a
+// sample is two Horner rules (15 FMA) instead of 8 Keys weights and 20 tap
+// products, and maps lanes to subset columns: lane l walks column l (then
+// l + 32, ...) down the rows, so X is fixed per lane and Y uniform per row
+// -- u and v are one FMA each from per-lane bases, the terms weighted by X
+// are summed unweighted and multiplied by X once, and the columns past the
+// last full 32 (one for a 33-pixel window) are spread over the lanes by
+// pixel.  FP64 keeps the plain stencil over the image, pixel per lane.
 //
 // ZNSSD residual (funICGN.m:238): r = (f - fbar)/bf - (g - gbar)/bg.  With
 // sd_k the steepest-descent images,
@@ -82,31 +80,15 @@ template <> struct Img<double> {
   static __device__ __forceinline__ const double *f(const IcgnImages &m) { return m.f64; }
 };
 
-// The reference gradients of a pixel.  FP32 Subpb1 reads the (gx, gy) pair
-// in one 8-byte load (its loop is L1-throughput bound); FP32 IC-GN (measured
-// faster with two 4-byte loads) and FP64 read the two fields.
-template <typename Real, bool PAIR> struct Grad;
-template <> struct Grad<float, true> {
-  const float2 *p;
-  __device__ __forceinline__ explicit Grad(const IcgnImages &m) : p(m.gxy) {}
-  __device__ __forceinline__ void at(int k, float *fx, float *fy) const {
-    const float2 t = __ldg(p + k);
-    *fx = t.x;
-    *fy = t.y;
-  }
-};
-template <typename Real> struct GradFields {
-  const Real *x, *y;
-  __device__ __forceinline__ void at(int k, Real *fx, Real *fy) const {
+// The FP64 reference gradients of a pixel (the FP32 path reads the (gx, gy)
+// pairs of IcgnImages::gxy).
+struct Grad64 {
+  const double *x, *y;
+  __device__ __forceinline__ explicit Grad64(const IcgnImages &m) : x(m.gx64), y(m.gy64) {}
+  __device__ __forceinline__ void at(int k, double *fx, double *fy) const {
     *fx = x[k];
     *fy = y[k];
   }
-};
-template <> struct Grad<float, false> : GradFields<float> {
-  __device__ __forceinline__ explicit Grad(const IcgnImages &m) : GradFields<float>{m.gx32, m.gy32} {}
-};
-template <bool PAIR> struct Grad<double, PAIR> : GradFields<double> {
-  __device__ __forceinline__ explicit Grad(const IcgnImages &m) : GradFields<double>{m.gx64, m.gy64} {}
 };
 
 // Cholesky of the 6x6 SPD matrix (lower, packed row-wise in L[21]); inv[i]
@@ -187,210 +169,250 @@ __device__ __forceinline__ Real sample(const Real *__restrict__ img, int W, int 
   return acc;
 }
 
-// Twice the Keys weights of keys_w (the same expressions without the final
-// multiplication by 1/2, which is exact in binary floating point).
-__device__ __forceinline__ void keys_w2(float t, float w[4]) {
-  const float t2 = t * t, t3 = t2 * t;
-  w[0] = fmaf(2.0f, t2, -t) - t3;
-  w[1] = fmaf(3.0f, t3, fmaf(-5.0f, t2, 2.0f));
-  w[2] = fmaf(-3.0f, t3, fmaf(4.0f, t2, t));
-  w[3] = t3 - t2;
-}
-
-// The same sample from the row runs of img (q[i] = img[i .. i+3]): each
-// stencil row is one aligned 16-byte load.  With both weight sets doubled
-// every product and partial sum is exactly 2x or 4x that of sample(), so the
-// returned 4x sample scaled by 1/4 is bit-identical to sample().
-__device__ __forceinline__ float sample4x(const float4 *__restrict__ q, int W, int cx, int cy,
-                                          float tu, float tv) {
-  float wu[4], wv[4];
-  keys_w2(tu, wu);
-  keys_w2(tv, wv);
-  const float4 *p = q + ((cy - 1) * W + (cx - 1));
-  float acc = 0;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const float4 t = __ldg(p + r * W);
-    const float s = wu[0] * t.x + wu[1] * t.y + wu[2] * t.z + wu[3] * t.w;
-    acc += wv[r] * s;
-  }
-  return acc;
-}
-
-// sample - c: one FMA of the exact 1/4 scaling (FP32 row runs), or the
-// FP64 sample minus c
-__device__ __forceinline__ float sample_minus(const float4 *q, int W, int cx, int cy, float tu,
-                                              float tv, float c) {
-  return fmaf(sample4x(q, W, cx, cy, tu, tv), 0.25f, -c);
-}
 __device__ __forceinline__ double sample_minus(const double *img, int W, int cx, int cy,
                                                double tu, double tv, double c) {
   return sample<double>(img, W, cx, cy, tu, tv) - c;
 }
 
-// Packed (A, B) arithmetic: two IEEE FP32 operations per instruction on sm_100.
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
-
-// keys_w2 of the two fractions in t (A, B)
-__device__ __forceinline__ void keys_w2x2(float2 t, float2 w[4]) {
-  const float2 t2 = __fmul2_rn(t, t), t3 = __fmul2_rn(t2, t);
-  const float2 nt = __fmul2_rn(t, f2(-1.f));
-  w[0] = __ffma2_rn(t3, f2(-1.f), __ffma2_rn(t2, f2(2.f), nt));     // 2t^2 - t - t^3
-  w[1] = __ffma2_rn(t3, f2(3.f), __ffma2_rn(t2, f2(-5.f), f2(2.f)));  // 3t^3 - 5t^2 + 2
-  w[2] = __ffma2_rn(t3, f2(-3.f), __ffma2_rn(t2, f2(4.f), t));        // -3t^3 + 4t^2 + t
-  w[3] = __ffma2_rn(t2, f2(-1.f), t3);                                // t^3 - t^2
+// FP32 bicubic at fractions (tu, tv) of the cell at q in plane 0 of the
+// coefficient table (cubic_table: plane j, `plane` float4 further on, holds
+// the tv^j coefficients of tu^0..tu^3).
+__device__ __forceinline__ float cubic_at(const float4 *__restrict__ q, long long plane, float tu,
+                                          float tv) {
+  const float4 c0 = __ldg(q), c1 = __ldg(q + plane), c2 = __ldg(q + 2 * plane),
+               c3 = __ldg(q + 3 * plane);
+  const float p0 = fmaf(fmaf(fmaf(c0.w, tu, c0.z), tu, c0.y), tu, c0.x);
+  const float p1 = fmaf(fmaf(fmaf(c1.w, tu, c1.z), tu, c1.y), tu, c1.x);
+  const float p2 = fmaf(fmaf(fmaf(c2.w, tu, c2.z), tu, c2.y), tu, c2.x);
+  const float p3 = fmaf(fmaf(fmaf(c3.w, tu, c3.z), tu, c3.y), tu, c3.x);
+  return fmaf(fmaf(fmaf(p3, tv, p2), tv, p1), tv, p0);
 }
 
-// Both 4x samples of a pixel pair whose B stencil is A's shifted one column:
-// p points at A's stencil origin in the pair runs.
-__device__ __forceinline__ float2 sample4x_pair(const float4 *__restrict__ p, int W, float2 tu,
-                                                float2 tv) {
-  float2 wu[4], wv[4];
-  keys_w2x2(tu, wu);
-  keys_w2x2(tv, wv);
-  float2 acc = f2(0.f);
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const float4 a = __ldg(p + r * W), b = __ldg(p + r * W + 2);
-    float2 s = __fmul2_rn(wu[0], f2(a.x, a.y));
-    s = __ffma2_rn(wu[1], f2(a.z, a.w), s);
-    s = __ffma2_rn(wu[2], f2(b.x, b.y), s);
-    s = __ffma2_rn(wu[3], f2(b.z, b.w), s);
-    acc = r == 0 ? __fmul2_rn(wv[0], s) : __ffma2_rn(wv[r], s, acc);
+// Pixel p of a block of nw-wide rows (x fastest): its column and row as
+// exact small integers in Real, and its offset row * W + column.
+// Branch-free, so the lanes of a warp (which wrap to the next row at
+// different p) stay converged.  row = floor((p + 1/2) / nw) is exact:
+// (p + 1/2) / nw lies at least 1/(2 nw) from an integer, and the two FP32
+// roundings err by at most (p / nw) 2^-23, far less for p < 2^20.
+template <typename Real> struct PixelMap {
+  Real fnw, inw;
+  int W;
+  __device__ __forceinline__ PixelMap(int nw, int W_)
+      : fnw((Real)nw), inw((Real)1 / (Real)nw), W(W_) {}
+  __device__ __forceinline__ int at(int p, Real *col, Real *row) const {
+    const Real fp = (Real)p;
+    const Real r = floor((fp + (Real)0.5) * inw);
+    const Real c = fp - r * fnw;
+    *col = c;
+    *row = r;
+    return (int)r * W + (int)c;
   }
-  return acc;
-}
+};
 
-// Residual sums of one FP32 evaluation over the subset's pixel pairs.  Pair
-// q of a row of nw pixels covers columns 2j, 2j+1 (j = q mod ppr, ppr =
-// ceil(nw / 2)); for odd nw the last pair's B lies outside the subset and
-// counts zero.  Queued B pixels (see the file header) are sampled by the
-// whole warp in fq_flush.  Per lane, acc holds (A, B) partial sums of
-// [d, d^2, fx d X, fy d X, fx d Y, fy d Y, fx d, fy d] with d = g - c at the
-// warped pixel (SUB: only d, d^2, fx d, fy d).
-struct PairEval {
-  const float4 *gp, *gxyp;
-  int W, nw, base, xb, yb;
+// One FP32 evaluation of the residual sums over an nw x nw subset whose
+// top-left pixel is `base` and whose pixel (0, 0) sits at (ox, oy) from the
+// subset centre: u = a11 X + a12 Y + c4, v = a21 X + a22 Y + c5 relative to
+// the floor corner (xb, yb) of the centre (c4, c5 carry the centre's
+// fraction).  Per lane: o = [sum d, sum d^2, sum X fx d, sum X fy d,
+// sum Y fx d, sum Y fy d, sum fx d, sum fy d], d = g(warped) - cg
+// (SUB: only o[0], o[1], o[6], o[7]).
+struct Eval32 {
+  const float4 *tab;  // cubic_table (plane 0) at the cell of the centre's floor corner - (1, 1)
+  const float2 *gxy;  // reference gradients at the subset's top-left pixel
+  long long plane;    // W H: float4 from one coefficient plane to the next
+  int W, nw;
   float ox, oy, a11, a12, a21, a22, c4, c5, cg;
 };
 
 template <bool SUB>
-__device__ __forceinline__ void add_terms(float2 d, float2 X, float Y, float4 G, float2 acc[8]) {
-  acc[0] = __fadd2_rn(acc[0], d);
-  acc[1] = __ffma2_rn(d, d, acc[1]);
-  const float2 ax = __fmul2_rn(f2(G.x, G.y), d), ay = __fmul2_rn(f2(G.z, G.w), d);
-  acc[6] = __fadd2_rn(acc[6], ax);
-  acc[7] = __fadd2_rn(acc[7], ay);
-  if (!SUB) {
-    acc[2] = __ffma2_rn(ax, X, acc[2]);
-    acc[3] = __ffma2_rn(ay, X, acc[3]);
-    acc[4] = __ffma2_rn(ax, f2(Y), acc[4]);
-    acc[5] = __ffma2_rn(ay, f2(Y), acc[5]);
-  }
-}
-
-// one queued B pixel (pair index q) sampled by a single lane with its own
-// stencil (two pair-run loads a row give its four taps), accumulated into
-// the B half of the lane's sums
-template <bool SUB>
-__device__ __forceinline__ void b_pixel(const PairEval &e, int ppr, int q, float2 acc[8]) {
-  const float rq = floor(((float)q + 0.5f) * (1.0f / (float)ppr));
-  const int row = (int)rq, colA = 2 * (q - row * ppr);
-  const float X = e.ox + (float)(colA + 1), Y = e.oy + rq;
-  const float ru = fmaf(e.a11, X, fmaf(e.a12, Y, e.c4));
-  const float rv = fmaf(e.a21, X, fmaf(e.a22, Y, e.c5));
-  const float fu = floor(ru), fv = floor(rv);
-  const int cx = e.xb + (int)fu - 1, cy = e.yb + (int)fv - 1;
-  float wu[4], wv[4];
-  keys_w2(ru - fu, wu);
-  keys_w2(rv - fv, wv);
-  const float4 *p = e.gp + ((cy - 1) * e.W + (cx - 1));
-  float a4 = 0.f;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const float4 u = __ldg(p + r * e.W), v = __ldg(p + r * e.W + 2);
-    const float t = wu[0] * u.x + wu[1] * u.y + wu[2] * v.x + wu[3] * v.y;
-    a4 += wv[r] * t;
-  }
-  const float d = fmaf(a4, 0.25f, -e.cg);
-  const float4 G = __ldg(e.gxyp + (e.base + row * e.W + colA));  // B's gradients: .y, .w
-  const float ax = G.y * d, ay = G.w * d;
-  acc[0].y += d;
-  acc[1].y = fmaf(d, d, acc[1].y);
-  acc[6].y += ax;
-  acc[7].y += ay;
-  if (!SUB) {
-    acc[2].y = fmaf(ax, X, acc[2].y);
-    acc[3].y = fmaf(ay, X, acc[3].y);
-    acc[4].y = fmaf(ax, Y, acc[4].y);
-    acc[5].y = fmaf(ay, Y, acc[5].y);
-  }
-}
-
-constexpr int FQ = 128;  // per-warp queue of B pixels
-
-template <bool SUB>
-__device__ __noinline__ void fq_flush(const PairEval &e, int ppr, const unsigned short *fq, int cnt,
-                                      int lane, float2 acc[8]) {
-  __syncwarp();
-  for (int i = lane; i < cnt; i += 32) b_pixel<SUB>(e, ppr, fq[i], acc);
-  __syncwarp();
-}
-
-template <bool SUB>
-__device__ __forceinline__ void eval_pairs(const PairEval &e, int lane, unsigned short *fq,
-                                           float out[8]) {
-  const int nw = e.nw, ppr = (nw + 1) >> 1, npairs = nw * ppr;
-  const float fppr = (float)ppr, ippr = 1.0f / fppr;
-  float2 acc[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) acc[k] = f2(0.f);
-  int qn = 0;  // queued B pixels (warp-uniform)
-  for (int q0 = 0; q0 < npairs; q0 += 32) {
-    const int q = q0 + lane;
-    bool queue = false;
-    if (q < npairs) {
-      const float rq = floor(((float)q + 0.5f) * ippr);
-      const float cj = (float)q - rq * fppr;
-      const int row = (int)rq, colA = 2 * (int)cj;
-      const float XA = fmaf(2.f, cj, e.ox);
-      const float2 X = f2(XA, XA + 1.f);
-      const float Y = e.oy + rq;
-      const float2 ru = __ffma2_rn(f2(e.a11), X, f2(fmaf(e.a12, Y, e.c4)));
-      const float2 rv = __ffma2_rn(f2(e.a21), X, f2(fmaf(e.a22, Y, e.c5)));
-      const float fu = floor(ru.x), fv = floor(rv.x);
-      const float2 tu = __fadd2_rn(ru, f2(-fu, -fu - 1.f));
-      const float2 tv = __fadd2_rn(rv, f2(-fv));
-      const int cx = e.xb + (int)fu - 1, cy = e.yb + (int)fv - 1;
-      const float2 a4 = sample4x_pair(e.gp + ((cy - 1) * e.W + (cx - 1)), e.W, tu, tv);
-      float2 d = __ffma2_rn(a4, f2(0.25f), f2(-e.cg));
-      const bool hasB = colA + 1 < nw;
-      const bool okB = tu.y >= 0.f && tu.y < 1.f && tv.y >= 0.f && tv.y < 1.f;
-      queue = hasB && !okB;
-      if (!(hasB && okB)) d.y = 0.f;
-      add_terms<SUB>(d, X, Y, __ldg(e.gxyp + (e.base + row * e.W + colA)), acc);
-    }
-    // queue the B pixels whose stencil is not A's shifted one column
-    const unsigned bal = __ballot_sync(0xffffffffu, queue);
-    if (bal) {
-      const int nb = __popc(bal);
-      if (qn + nb > FQ) {
-        fq_flush<SUB>(e, ppr, fq, qn, lane, acc);
-        qn = 0;
+__device__ __forceinline__ void eval32(const Eval32 &e, int lane, float o[8]) {
+  const int W = e.W, nw = e.nw;
+  float s1 = 0.f, s2 = 0.f, yx = 0.f, yy = 0.f, tx = 0.f, ty = 0.f, xx = 0.f, xy = 0.f;
+  // full 32-column blocks: lane = column, rows in order
+  const int nch = nw >> 5;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int col = (ch << 5) + lane;
+    const float X = e.ox + (float)col;
+    const float bu = fmaf(e.a11, X, e.c4), bv = fmaf(e.a21, X, e.c5);
+    const float2 *gp = e.gxy + col;
+    float cx = 0.f, cy = 0.f, Y = e.oy;
+    for (int r = 0; r < nw; ++r, Y += 1.f, gp += W) {
+      const float ru = fmaf(e.a12, Y, bu), rv = fmaf(e.a22, Y, bv);
+      const float fu = floorf(ru), fv = floorf(rv);
+      const float d = cubic_at(e.tab + ((int)fv * W + (int)fu), e.plane, ru - fu, rv - fv) - e.cg;
+      const float2 G = __ldg(gp);
+      s1 += d;
+      s2 = fmaf(d, d, s2);
+      const float ax = G.x * d, ay = G.y * d;
+      cx += ax;
+      cy += ay;
+      if (!SUB) {
+        yx = fmaf(ax, Y, yx);
+        yy = fmaf(ay, Y, yy);
       }
-      if (queue) fq[qn + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)q;
-      qn += nb;
+    }
+    tx += cx;
+    ty += cy;
+    if (!SUB) {
+      xx = fmaf(X, cx, xx);
+      xy = fmaf(X, cy, xy);
     }
   }
-  if (qn) fq_flush<SUB>(e, ppr, fq, qn, lane, acc);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) out[k] = acc[k].x + acc[k].y;
+  // the remaining columns (one for a 33-pixel window), pixel per lane
+  const int c0 = nch << 5, rem = nw - c0;
+  if (rem) {
+    const PixelMap<float> pm(rem, W);
+    const int np = rem * nw;
+    for (int p = lane; p < np; p += 32) {
+      float rc, rr;
+      const int k = c0 + pm.at(p, &rc, &rr);
+      const float X = e.ox + (float)c0 + rc, Y = e.oy + rr;
+      const float ru = fmaf(e.a11, X, fmaf(e.a12, Y, e.c4));
+      const float rv = fmaf(e.a21, X, fmaf(e.a22, Y, e.c5));
+      const float fu = floorf(ru), fv = floorf(rv);
+      const float d = cubic_at(e.tab + ((int)fv * W + (int)fu), e.plane, ru - fu, rv - fv) - e.cg;
+      const float2 G = __ldg(e.gxy + k);
+      s1 += d;
+      s2 = fmaf(d, d, s2);
+      const float ax = G.x * d, ay = G.y * d;
+      tx += ax;
+      ty += ay;
+      if (!SUB) {
+        xx = fmaf(ax, X, xx);
+        xy = fmaf(ay, X, xy);
+        yx = fmaf(ax, Y, yx);
+        yy = fmaf(ay, Y, yy);
+      }
+    }
+  }
+  o[0] = s1; o[1] = s2; o[2] = xx; o[3] = xy; o[4] = yx; o[5] = yy; o[6] = tx; o[7] = ty;
 }
 
-// the FP32 path samples the row runs, the FP64 path the image itself
-__device__ __forceinline__ const float4 *sample_src(const IcgnImages &m, float) { return m.g4; }
-__device__ __forceinline__ const double *sample_src(const IcgnImages &m, double) { return m.g64; }
+// The FP32 setup sums of one subset (c the centre pixel's value): the
+// zero-gradient count, a1 = sum (f - c), a2 = sum (f - c)^2, sk = sum sd_k,
+// sfk = sum sd_k (f - c) with sd = [fx X, fy X, fx Y, fy Y, fx, fy], and the
+// 18 distinct Hessian sums hh (index map in process()); lanes take columns
+// as in eval32, the X weights applied once per column.
+template <bool SUB>
+__device__ __forceinline__ void setup32(const float *fI, const float2 *gxy, int W, int nw,
+                                        int base, float ox, float oy, float c, int lane,
+                                        int *cnt_out, float *a1o, float *a2o, float sk[6],
+                                        float sfk[6], float hh[18]) {
+  int cnt = 0;
+  float a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) sk[q] = sfk[q] = 0.f;
+#pragma unroll
+  for (int q = 0; q < 18; ++q) hh[q] = 0.f;
+  const int nch = nw >> 5;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int col = (ch << 5) + lane;
+    const float X = ox + (float)col;
+    const float *fp = fI + base + col;
+    const float2 *gp = gxy + base + col;
+    // column sums: S1 = sum, SY = sum Y., SYY = sum Y^2. of fxx, fxy, fyy
+    float sx = 0.f, sy = 0.f, fdx = 0.f, fdy = 0.f;
+    float h1[3] = {0.f, 0.f, 0.f}, hY[3] = {0.f, 0.f, 0.f}, hYY[3] = {0.f, 0.f, 0.f};
+    float Y = oy;
+    for (int r = 0; r < nw; ++r, Y += 1.f, fp += W, gp += W) {
+      const float2 G = __ldg(gp);
+      const float d = __ldg(fp) - c;
+      cnt += G.x == 0.f;
+      a1 += d;
+      a2 = fmaf(d, d, a2);
+      sx += G.x;
+      sy += G.y;
+      const float ax = G.x * d, ay = G.y * d;
+      fdx += ax;
+      fdy += ay;
+      if (!SUB) {
+        sk[2] = fmaf(G.x, Y, sk[2]);
+        sk[3] = fmaf(G.y, Y, sk[3]);
+        sfk[2] = fmaf(ax, Y, sfk[2]);
+        sfk[3] = fmaf(ay, Y, sfk[3]);
+        const float YY = Y * Y;
+        const float f3[3] = {G.x * G.x, G.x * G.y, G.y * G.y};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          h1[q] += f3[q];
+          hY[q] = fmaf(Y, f3[q], hY[q]);
+          hYY[q] = fmaf(YY, f3[q], hYY[q]);
+        }
+      }
+    }
+    sk[4] += sx;
+    sk[5] += sy;
+    sfk[4] += fdx;
+    sfk[5] += fdy;
+    if (!SUB) {
+      const float XX = X * X;
+      sk[0] = fmaf(X, sx, sk[0]);
+      sk[1] = fmaf(X, sy, sk[1]);
+      sfk[0] = fmaf(X, fdx, sfk[0]);
+      sfk[1] = fmaf(X, fdy, sfk[1]);
+      hh[0] = fmaf(XX, h1[0], hh[0]);
+      hh[1] = fmaf(XX, h1[1], hh[1]);
+      hh[2] = fmaf(X, hY[0], hh[2]);
+      hh[3] = fmaf(X, hY[1], hh[3]);
+      hh[4] = fmaf(X, h1[0], hh[4]);
+      hh[5] = fmaf(X, h1[1], hh[5]);
+      hh[6] = fmaf(XX, h1[2], hh[6]);
+      hh[7] = fmaf(X, hY[2], hh[7]);
+      hh[8] = fmaf(X, h1[2], hh[8]);
+      hh[9] += hYY[0];
+      hh[10] += hYY[1];
+      hh[11] += hY[0];
+      hh[12] += hY[1];
+      hh[13] += hYY[2];
+      hh[14] += hY[2];
+      hh[15] += h1[0];
+      hh[16] += h1[1];
+      hh[17] += h1[2];
+    }
+  }
+  const int c0 = nch << 5, rem = nw - c0;
+  if (rem) {
+    const PixelMap<float> pm(rem, W);
+    const int np = rem * nw;
+    for (int p = lane; p < np; p += 32) {
+      float rc, rr;
+      const int k = base + c0 + pm.at(p, &rc, &rr);
+      const float2 G = __ldg(gxy + k);
+      const float d = __ldg(fI + k) - c;
+      cnt += G.x == 0.f;
+      a1 += d;
+      a2 = fmaf(d, d, a2);
+      if (SUB) {
+        sk[4] += G.x;
+        sk[5] += G.y;
+        sfk[4] = fmaf(G.x, d, sfk[4]);
+        sfk[5] = fmaf(G.y, d, sfk[5]);
+      } else {
+        const float X = ox + (float)c0 + rc, Y = oy + rr;
+        const float sd[6] = {G.x * X, G.y * X, G.x * Y, G.y * Y, G.x, G.y};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          sk[q] += sd[q];
+          sfk[q] = fmaf(sd[q], d, sfk[q]);
+        }
+        const float fxx = G.x * G.x, fyy = G.y * G.y, fxy = G.x * G.y;
+        const float XX = X * X, YY = Y * Y, XY = X * Y;
+        hh[0] = fmaf(XX, fxx, hh[0]);  hh[1] = fmaf(XX, fxy, hh[1]);
+        hh[2] = fmaf(XY, fxx, hh[2]);  hh[3] = fmaf(XY, fxy, hh[3]);
+        hh[4] = fmaf(X, fxx, hh[4]);   hh[5] = fmaf(X, fxy, hh[5]);
+        hh[6] = fmaf(XX, fyy, hh[6]);  hh[7] = fmaf(XY, fyy, hh[7]);
+        hh[8] = fmaf(X, fyy, hh[8]);   hh[9] = fmaf(YY, fxx, hh[9]);
+        hh[10] = fmaf(YY, fxy, hh[10]); hh[11] = fmaf(Y, fxx, hh[11]);
+        hh[12] = fmaf(Y, fxy, hh[12]); hh[13] = fmaf(YY, fyy, hh[13]);
+        hh[14] = fmaf(Y, fyy, hh[14]); hh[15] += fxx;
+        hh[16] += fxy;                 hh[17] += fyy;
+      }
+    }
+  }
+  *cnt_out = cnt;
+  *a1o = a1;
+  *a2o = a2;
+}
 
 // MATLAB's catch branch (LocalICGN.m:75-80, Subpb1.m:89-92): -1 and NaN
 template <bool SUB>
@@ -422,26 +444,6 @@ __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
   }
 }
 
-// Pixel p of an nw x nw subset (x fastest): its column and row as exact
-// small integers in Real, and its offset row * W + column from the subset's
-// top-left pixel.  Branch-free, so the lanes of a warp (which wrap to the
-// next row at different p) stay converged.  row = floor((p + 1/2) / nw) is
-// exact: (p + 1/2) / nw lies at least 1/(2 nw) from an integer, and the two
-// FP32 roundings err by at most (p / nw) 2^-23, far less for p < 2^20.
-template <typename Real> struct PixelMap {
-  Real fnw, inw;
-  int W;
-  __device__ __forceinline__ PixelMap(int nw, int W_)
-      : fnw((Real)nw), inw((Real)1 / (Real)nw), W(W_) {}
-  __device__ __forceinline__ int at(int p, Real *col, Real *row) const {
-    const Real fp = (Real)p;
-    const Real r = floor((fp + (Real)0.5) * inw);
-    const Real c = fp - r * fnw;
-    *col = c;
-    *row = r;
-    return (int)r * W + (int)c;
-  }
-};
 
 // ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
 // S_f[6] at 57, S[6] at 63 and 1 / diag(L) at 69 (kept out of registers to
@@ -449,7 +451,7 @@ template <typename Real> struct PixelMap {
 constexpr int WS = 76;
 
 template <typename Real, bool SUB>
-__device__ void process(const Args &a, long long s, int lane, double *ws, unsigned short *fq) {
+__device__ void process(const Args &a, long long s, int lane, double *ws) {
   double *Lsh = ws + 36, *Sfs = ws + 57, *Sks = ws + 63, *Linv = ws + 69;
   const IcgnImages &im = a.im;
   const double x0 = a.coords[s], y0 = a.coords[a.n + s];
@@ -476,8 +478,6 @@ __device__ void process(const Args &a, long long s, int lane, double *ws, unsign
     return;
   }
   const Real *fI = Img<Real>::f(im);
-  const auto *gI = sample_src(im, Real(0));
-  const Grad<Real, SUB> grad(im);
   const int W = im.W;
   // One fused pass over the subset: the masked-pixel count of funICGN.m:54,
   // the Hessian sums of :67-79, and -- with a shift c (the subset's centre
@@ -522,34 +522,39 @@ __device__ void process(const Args &a, long long s, int lane, double *ws, unsign
     for (int q = 0; q < 6; ++q) sk[q] = sfk[q] = 0;
 #pragma unroll
     for (int q = 0; q < 18; ++q) hh[q] = 0;
-    const PixelMap<Real> pm(nw, W);
-    for (int p = lane; p < npx; p += 32) {
-      Real rx, ry;
-      const int k = base + pm.at(p, &rx, &ry);
-      Real fx, fy;
-      grad.at(k, &fx, &fy);
-      const Real d = fI[k] - c;
-      cnt += fx == (Real)0;
-      a1 += d;
-      a2 += d * d;
-      if (SUB) {
-        sk[4] += fx; sk[5] += fy;
-        sfk[4] += fx * d; sfk[5] += fy * d;
-      } else {
-        const Real X = ox + rx, Y = oy + ry;
-        const Real sd[6] = {fx * X, fy * X, fx * Y, fy * Y, fx, fy};
+    if constexpr (sizeof(Real) == 4) {
+      setup32<SUB>(fI, im.gxy, W, nw, base, ox, oy, c, lane, &cnt, &a1, &a2, sk, sfk, hh);
+    } else {
+      const Grad64 grad(im);
+      const PixelMap<Real> pm(nw, W);
+      for (int p = lane; p < npx; p += 32) {
+        Real rx, ry;
+        const int k = base + pm.at(p, &rx, &ry);
+        Real fx, fy;
+        grad.at(k, &fx, &fy);
+        const Real d = fI[k] - c;
+        cnt += fx == (Real)0;
+        a1 += d;
+        a2 += d * d;
+        if (SUB) {
+          sk[4] += fx; sk[5] += fy;
+          sfk[4] += fx * d; sfk[5] += fy * d;
+        } else {
+          const Real X = ox + rx, Y = oy + ry;
+          const Real sd[6] = {fx * X, fy * X, fx * Y, fy * Y, fx, fy};
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          sk[q] += sd[q];
-          sfk[q] += sd[q] * d;
+          for (int q = 0; q < 6; ++q) {
+            sk[q] += sd[q];
+            sfk[q] += sd[q] * d;
+          }
+          const Real fxx = fx * fx, fyy = fy * fy, fxy = fx * fy;
+          const Real XX = X * X, YY = Y * Y, XY = X * Y;
+          hh[0] += XX * fxx;  hh[1] += XX * fxy;  hh[2] += XY * fxx;  hh[3] += XY * fxy;
+          hh[4] += X * fxx;   hh[5] += X * fxy;   hh[6] += XX * fyy;  hh[7] += XY * fyy;
+          hh[8] += X * fyy;   hh[9] += YY * fxx;  hh[10] += YY * fxy; hh[11] += Y * fxx;
+          hh[12] += Y * fxy;  hh[13] += YY * fyy; hh[14] += Y * fyy;  hh[15] += fxx;
+          hh[16] += fxy;      hh[17] += fyy;
         }
-        const Real fxx = fx * fx, fyy = fy * fy, fxy = fx * fy;
-        const Real XX = X * X, YY = Y * Y, XY = X * Y;
-        hh[0] += XX * fxx;  hh[1] += XX * fxy;  hh[2] += XY * fxx;  hh[3] += XY * fxy;
-        hh[4] += X * fxx;   hh[5] += X * fxy;   hh[6] += XX * fyy;  hh[7] += XY * fyy;
-        hh[8] += X * fyy;   hh[9] += YY * fxx;  hh[10] += YY * fxy; hh[11] += Y * fxx;
-        hh[12] += Y * fxy;  hh[13] += YY * fyy; hh[14] += Y * fyy;  hh[15] += fxx;
-        hh[16] += fxy;      hh[17] += fyy;
       }
     }
 #pragma unroll
@@ -684,18 +689,25 @@ __device__ void process(const Args &a, long long s, int lane, double *ws, unsign
 #pragma unroll
     for (int q = 0; q < 6; ++q) pfin &= isfinite(P[q]);
     double sums[8];
-    if (pfin && sizeof(Real) == 4) {
-      PairEval e;
-      e.gp = im.gp; e.gxyp = im.gxyp;
-      e.W = W; e.nw = nw; e.base = base; e.xb = xb; e.yb = yb;
+    if (!pfin) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sums[q] = nan64();
+    } else if constexpr (sizeof(Real) == 4) {
+      Eval32 e;
+      e.tab = im.gc + ((long long)(yb - 1) * W + (xb - 1));
+      e.plane = (long long)W * im.H;
+      e.gxy = im.gxy + base;
+      e.W = W; e.nw = nw;
       e.ox = (float)ox; e.oy = (float)oy;
       e.a11 = (float)(1 + P[0]); e.a12 = (float)P[2]; e.a21 = (float)P[1]; e.a22 = (float)(1 + P[3]);
       e.c4 = (float)P[4] + (float)fx0; e.c5 = (float)P[5] + (float)fy0; e.cg = (float)cg;
       float o[8];
-      eval_pairs<SUB>(e, lane, fq, o);
+      eval32<SUB>(e, lane, o);
 #pragma unroll
       for (int q = 0; q < 8; ++q) sums[q] = (SUB && q >= 2 && q < 6) ? 0.0 : warp_sum((double)o[q]);
-    } else if (pfin) {
+    } else {
+      const Real *gI = im.g64;
+      const Grad64 grad(im);
       const Real a11 = (Real)(1 + P[0]), a12 = (Real)P[2], a21 = (Real)P[1],
                  a22 = (Real)(1 + P[3]), p4 = (Real)P[4], p5 = (Real)P[5];
       Real s1 = 0, s2r = 0, t[6];
@@ -733,9 +745,6 @@ __device__ void process(const Args &a, long long s, int lane, double *ws, unsign
       sums[1] = warp_sum((double)s2r);
 #pragma unroll
       for (int q = 0; q < 6; ++q) sums[2 + q] = (SUB && q < 4) ? 0.0 : warp_sum((double)t[q]);
-    } else {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) sums[q] = nan64();
     }
     const double n = (double)npx;
     const double gm = sums[0] / n;                 // mean(g) - c
@@ -807,14 +816,13 @@ __device__ void process(const Args &a, long long s, int lane, double *ws, unsign
 template <typename Real, bool SUB, int NW, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) k_icgn(Args a) {
   __shared__ double Lsh[NW][WS];
-  __shared__ unsigned short Fq[NW][FQ];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   while (true) {
     unsigned int s = 0;
     if (lane == 0) s = atomicAdd(a.queue, 1u);
     s = __shfl_sync(0xffffffffu, s, 0);
     if ((long long)s >= a.n) break;
-    process<Real, SUB>(a, (long long)s, lane, Lsh[wid], Fq[wid]);
+    process<Real, SUB>(a, (long long)s, lane, Lsh[wid]);
     __syncwarp();
   }
 }

@@ -15,14 +15,12 @@ int normalize(const void *img, int dtype, long long n, const double *d_stats, do
               float *o32, cudaStream_t st);
 int gradient(const double *f, const double *mask, int W, int H, double *gx64, double *gy64,
              float *gx32, float *gy32, cudaStream_t st);
-// q[i] = g[i .. i+3] within the row (zero past its end), W*H float4
-int row_runs(const float *g, int W, int H, float4 *q, cudaStream_t st);
+// bicubic polynomial coefficients of every cell of the FP64 image g: four
+// planes of W H float4, q[j W H + y W + x] = the tv^j row (tu^0..3) of the
+// cell at (x, y)
+int cubic_table(const double *g, int W, int H, float4 *q, cudaStream_t st);
 // q[i] = (gx[i], gy[i]), n float2
 int grad_pairs(const float *gx, const float *gy, long long n, float2 *q, cudaStream_t st);
-// q[i] = (g[i], g[i+1], g[i+1], g[i+2]) within the row, W*H float4
-int pair_runs(const float *g, int W, int H, float4 *q, cudaStream_t st);
-// q[i] = (gx[i], gx[i+1], gy[i], gy[i+1]) within the row, W*H float4
-int grad_pair_runs(const float *gx, const float *gy, int W, int H, float4 *q, cudaStream_t st);
 int interp_f64(const double *F, long long M, long long N, long long P, const double *X,
                const double *Y, long long n, double *Z, cudaStream_t st);
 int interp_f32(const float *F, long long M, long long N, long long P, const float *X,
@@ -53,13 +51,8 @@ int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, co
 // ---- k_icgn.cu
 struct IcgnImages {
   const float *f32, *g32, *gx32, *gy32;
-  const float4 *g4;  // row runs of g32 (row_runs): the FP32 sampler's stencil rows
+  const float4 *gc;   // bicubic coefficients of g (cubic_table): the FP32 sampler's
   const float2 *gxy;  // (gx32, gy32) pairs (grad_pairs) read by the FP32 IC-GN
-  // pixel-pair runs read by the FP32 evaluation loop, which samples two
-  // horizontally adjacent pixels at once: gp[i] = (g[i], g[i+1], g[i+1],
-  // g[i+2]) (pair_runs) and gxyp[i] = (gx[i], gx[i+1], gy[i], gy[i+1])
-  // (grad_pair_runs), zero past the row's end
-  const float4 *gp, *gxyp;
   const double *f64, *g64, *gx64, *gy64;
   int W, H;
 };

@@ -36,6 +36,11 @@ def test_config2_frame_matches_oracle(aldic, c2, prec):
     assert r["M"] * r["N"] == 59049
     np.testing.assert_array_equal(r["x0"], ro["x0"])
     np.testing.assert_array_equal(r["y0"], ro["y0"])
+    # LocalICGN's -1 subsets (688 here: more than 10 % zero-gradient pixels
+    # grow the window to an odd size, whose bounds are not integral) and 102
+    it, ito = np.asarray(r["iters"]).ravel(), np.asarray(ro["iters_icgn"]).ravel()
+    for code in (-1, 102):
+        np.testing.assert_array_equal(it == code, ito == code)
     dU = r["U"] - ro["U"]
     dF = r["F"] - ro["F"]
     rms = float(np.sqrt(np.mean(dU ** 2)))

@@ -174,9 +174,16 @@ def check_icgn_converged(U, F, it, Uo, Fo, ito, prec, label):
     """Every subset that converged in both runs (status 1..100) is checked:
     FP64 within 1e-8 px / 1e-9; FP32 within the specification's 1e-3 px (U)
     and 1e-5 (F) where the iteration counts agree, within one stopping-test
-    step (ICGN_STEP_BOUND_*) where they differ.  Status codes outside 1..100
-    must agree exactly in FP64; the number of subsets whose counts differ is
-    reported and bounded."""
+    step (ICGN_STEP_BOUND_*) where they differ.  The statuses fixed before
+    the first evaluation -- -1 (bounds, or a window grown past them by more
+    than 10 % zero-gradient pixels) and 102 (half masked) -- agree exactly in
+    both precisions, 101 (no convergence) too in FP64; the number of subsets
+    whose counts differ is reported and bounded."""
+    it, ito = np.asarray(it), np.asarray(ito)
+    for code in (-1, 102):
+        np.testing.assert_array_equal(it == code, ito == code, err_msg=f"{label} {prec}: status {code}")
+    if prec == "fp64":
+        np.testing.assert_array_equal(it == 101, ito == 101, err_msg=f"{label} fp64: status 101")
     conv = (it >= 1) & (it <= 100) & (ito >= 1) & (ito <= 100)
     same = conv & (it == ito)
     diff = conv & (it != ito)
