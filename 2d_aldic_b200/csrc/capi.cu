@@ -95,7 +95,7 @@ struct aldic_ctx {
     unsigned char *bad = nullptr;
   } qtf;
   DevBuf f_raw, g_raw, f64, g64, f32, g32, gx64, gy64, gx32, gy32, mask;
-  DevBuf gc;  // bicubic coefficients of g (4 float4 per pixel) read by the FP32 IC-GN sampler
+  DevBuf gc;  // row-cubic coefficients of g (float4 per pixel) read by the FP32 IC-GN sampler
   DevBuf gxy;  // (gx32, gy32) pairs (float2 per pixel) read by the FP32 IC-GN
   DevBuf stats;   // double[4]: mean_f std_f mean_g std_g
   DevBuf isums;   // u64[2]
@@ -450,7 +450,7 @@ int aldic_set_ref(aldic_ctx *c, const void *img, int dtype, int W, int H, const 
     if ((rc = b->ensure(sizeof(double) * n))) return rc;
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
-  if ((rc = c->gc.ensure(4 * sizeof(float4) * n))) return rc;
+  if ((rc = c->gc.ensure(sizeof(float4) * n))) return rc;
   if ((rc = c->gxy.ensure(sizeof(float2) * n))) return rc;
   if ((rc = c->f_raw.ensure(es * n))) return rc;
   if ((rc = c->g_raw.ensure(es * n))) return rc;
@@ -503,7 +503,7 @@ static int prep_def(aldic_ctx *c) {
   if ((rc = normalize(c->g_raw.p, c->dtype, (long long)c->W * c->H, st + 2, c->g64.as<double>(),
                       c->g32.as<float>(), c->stream)))
     return rc;
-  return cubic_table(c->g64.as<double>(), c->W, c->H, c->gc.as<float4>(), c->stream);
+  return row_cubic(c->g64.as<double>(), c->W, c->H, c->gc.as<float4>(), c->stream);
 }
 
 int aldic_set_def(aldic_ctx *c, const void *img, int dtype) {
@@ -540,7 +540,7 @@ int aldic_set_stats(aldic_ctx *c, const double stats[4]) {
   // the deformed image with stats[2..3] (not prep_def, which takes them from the ROI)
   if ((rc = normalize(c->g_raw.p, c->dtype, n, st + 2, c->g64.as<double>(), c->g32.as<float>(),
                       c->stream)) ||
-      (rc = cubic_table(c->g64.as<double>(), c->W, c->H, c->gc.as<float4>(), c->stream)))
+      (rc = row_cubic(c->g64.as<double>(), c->W, c->H, c->gc.as<float4>(), c->stream)))
     return rc;
   return finish(c, true);
 }
@@ -618,7 +618,7 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     if ((rc = b->ensure(bytes))) return rc;
   for (DevBuf *b : b4)
     if ((rc = b->ensure(sizeof(float) * n))) return rc;
-  if ((rc = c->gc.ensure(4 * sizeof(float4) * n))) return rc;
+  if ((rc = c->gc.ensure(sizeof(float4) * n))) return rc;
   if ((rc = c->gxy.ensure(sizeof(float2) * n))) return rc;
   if (first) c->have_def = false;
   c->W = W; c->H = H; c->dtype = 3;
@@ -632,7 +632,7 @@ int aldic_set_fields(aldic_ctx *c, const double *f, const double *gimg, const do
     ALDIC_CUDA(cudaMemcpyAsync(d64[k]->p, src[k], bytes, cudaMemcpyDefault, c->stream));
     k_to_f32<<<1184, 256, 0, c->stream>>>(d64[k]->as<double>(), d32[k]->as<float>(), n);
   }
-  if (gimg && (rc = cubic_table(c->g64.as<double>(), W, H, c->gc.as<float4>(), c->stream))) return rc;
+  if (gimg && (rc = row_cubic(c->g64.as<double>(), W, H, c->gc.as<float4>(), c->stream))) return rc;
   if ((dfdx || dfdy) &&
       (rc = grad_pairs(c->gx32.as<float>(), c->gy32.as<float>(), n, c->gxy.as<float2>(), c->stream)))
     return rc;
@@ -1550,7 +1550,8 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     if ((rc = subpb1(im, B.coords, n, B.U2, B.F2, B.vdual, B.H21, nullptr, p->winsize, mu, p->tol,
                      p->precision, B.U1, B.itb, c->queue.as<unsigned int>(), st, B.cache)))
       return rc;
-    if ((rc = gridfit_load(c->gw, M, N, 2, B.U1, 2, B.itb, st))) return rc;
+    // subsets Subpb1 could not solve start the fit from Subproblem 2's U
+    if ((rc = gridfit_load(c->gw, M, N, 2, B.U1, 2, B.itb, st, 0, B.U2))) return rc;
     if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, 2, 0, 0, 1, lam2, kRtolFit, kMaxitFit, st))) return rc;
     if ((rc = grid_store(c->gw, M, N, 2, B.U1, 2, st))) return rc;
     ALDIC_CUDA(cudaMemcpyAsync(B.F1, B.F2, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, st));

@@ -195,13 +195,27 @@ int tridiagonal_qr(int n, std::vector<double> &d, std::vector<double> &e, std::v
 }
 
 // ---------------------------------------------------------------- device: FP64 products
-// 32 x 32 outputs per CTA, 2 x 4 per thread (128 threads).  The operand
-// tiles of a 128-wide K chunk are staged in shared memory at once (every
-// thread's loads in flight together), so a 243-long product takes two
-// load-compute rounds instead of a chain of small dependent ones: the solve's
-// products are latency-bound at these sizes.
-constexpr int TR = 32, TC = 32, KC = 128, GT = 128;
-constexpr int kSmem = 2 * KC * (TR + 1) * (int)sizeof(double);
+// 64 x 64 outputs per 256-thread CTA, 4 x 4 per thread taken strided (rows
+// ty + 16 i, columns tx + 16 j), so a warp's shared-memory reads of a k row
+// are 16 consecutive doubles (one wavefront, broadcast to the two row
+// groups) and each thread does 16 FMA per 8 loads.  The operand tiles of
+// 32-wide K chunks go to shared memory by cp.async (no register round trip),
+// double-buffered so that chunk c + 1 arrives while chunk c is multiplied.
+constexpr int TR = 64, TC = 64, KC = 32, GT = 256, LDT = TR + 1;
+constexpr int kBuf = 2 * KC * LDT;                              // doubles per buffer (A + B)
+constexpr int kSmem = 2 * kBuf * (int)sizeof(double);           // two buffers: 66 560 B
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 struct GemmArgs {
   const double *A, *B;
@@ -218,50 +232,76 @@ struct GemmArgs {
   const double *beta_ptr;  // if set, beta = *beta_ptr for every batch entry
 };
 
+// stage K chunk [k0, k0 + KC) of the A and B tiles into buffer `buf`
+// (zeros outside the operands)
+__device__ __forceinline__ void stage_chunk(const GemmArgs &g, const double *A, const double *B,
+                                            int r0, int c0, int k0, double *buf, bool a_rfast,
+                                            bool b_cfast) {
+  double *As = buf, *Bs = buf + KC * LDT;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < TR * KC; e += GT) {
+    const int rr = a_rfast ? (e & (TR - 1)) : (e >> 5), kk = a_rfast ? (e >> 6) : (e & (KC - 1));
+    const int r = r0 + rr, k = k0 + kk;
+    double *d = As + kk * LDT + rr;
+    if (r < g.R && k < g.K) cp_async8(d, A + (long long)r * g.sar + (long long)k * g.sak);
+    else *d = 0.0;
+  }
+#pragma unroll 4
+  for (int e = threadIdx.x; e < TC * KC; e += GT) {
+    const int cc = b_cfast ? (e & (TC - 1)) : (e >> 5), kk = b_cfast ? (e >> 6) : (e & (KC - 1));
+    const int c = c0 + cc, k = k0 + kk;
+    double *d = Bs + kk * LDT + cc;
+    if (c < g.Cn && k < g.K) cp_async8(d, B + (long long)k * g.sbk + (long long)c * g.sbc);
+    else *d = 0.0;
+  }
+  cp_async_commit();
+}
+
 __global__ void __launch_bounds__(GT) k_fdm_gemm(GemmArgs g) {
   extern __shared__ double sm[];
-  double *As = sm, *Bs = sm + KC * (TR + 1);  // [k][r], [k][c], rows padded to 33
   const int b = blockIdx.z;
   const int r0 = blockIdx.y * TR, c0 = blockIdx.x * TC;
-  const int tid = threadIdx.x, ty = tid >> 3, tx = tid & 7;  // rows 2 ty.., columns 4 tx..
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const double *A = g.A + (long long)b * g.sab;
   const double *B = g.B + (long long)b * g.sbb;
-  double acc[2][4] = {};
+  double acc[4][4] = {};
   const bool a_rfast = g.sar <= g.sak, b_cfast = g.sbc <= g.sbk;
-  for (int k0 = 0; k0 < g.K; k0 += KC) {
-    const int kc = g.K - k0 < KC ? g.K - k0 : KC;
-    for (int e = tid; e < TR * kc; e += GT) {
-      const int rr = a_rfast ? e % TR : e / kc, kk = a_rfast ? e / TR : e % kc;
-      const int r = r0 + rr, k = k0 + kk;
-      As[kk * (TR + 1) + rr] = r < g.R ? __ldg(A + (long long)r * g.sar + (long long)k * g.sak) : 0.0;
-    }
-    for (int e = tid; e < TC * kc; e += GT) {
-      const int cc = b_cfast ? e % TC : e / kc, kk = b_cfast ? e / TC : e % kc;
-      const int c = c0 + cc, k = k0 + kk;
-      Bs[kk * (TC + 1) + cc] = c < g.Cn ? __ldg(B + (long long)k * g.sbk + (long long)c * g.sbc) : 0.0;
+  const int nch = (g.K + KC - 1) / KC;
+  stage_chunk(g, A, B, r0, c0, 0, sm, a_rfast, b_cfast);
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) {
+      stage_chunk(g, A, B, r0, c0, (ch + 1) * KC, sm + ((ch + 1) & 1) * kBuf, a_rfast, b_cfast);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
-#pragma unroll 4
+    const double *As = sm + (ch & 1) * kBuf, *Bs = As + KC * LDT;
+    const int kc = g.K - ch * KC < KC ? g.K - ch * KC : KC;
+#pragma unroll 8
     for (int kk = 0; kk < kc; ++kk) {
-      const double *ar = As + kk * (TR + 1) + 2 * ty, *br = Bs + kk * (TC + 1) + 4 * tx;
-      const double a0 = ar[0], a1 = ar[1];
-      const double b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
-      acc[0][0] = fma(a0, b0, acc[0][0]); acc[0][1] = fma(a0, b1, acc[0][1]);
-      acc[0][2] = fma(a0, b2, acc[0][2]); acc[0][3] = fma(a0, b3, acc[0][3]);
-      acc[1][0] = fma(a1, b0, acc[1][0]); acc[1][1] = fma(a1, b1, acc[1][1]);
-      acc[1][2] = fma(a1, b2, acc[1][2]); acc[1][3] = fma(a1, b3, acc[1][3]);
+      const double *ar = As + kk * LDT + ty, *br = Bs + kk * LDT + tx;
+      double a[4], bb[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = ar[16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bb[j] = br[16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
     }
-    __syncthreads();
+    __syncthreads();  // buffer (ch & 1) is restaged by the next round
   }
   const double beta = g.beta_ptr ? *g.beta_ptr : g.beta[b < 12 ? b : 11];
   double *C = g.C + (long long)b * g.scb;
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int r = r0 + 2 * ty + i;
+  for (int i = 0; i < 4; ++i) {
+    const int r = r0 + ty + 16 * i;
     if (r >= g.R) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int c = c0 + 4 * tx + j;
+      const int c = c0 + tx + 16 * j;
       if (c >= g.Cn) continue;
       double v = acc[i][j];
       if (g.scale) v /= beta * (g.lr[r] + g.lc[c]) + g.mu;

@@ -679,8 +679,9 @@ __global__ void k_nodal_strain(int M, int N, double h, const double *__restrict_
 
 // ------------------------------------------------------------------ loaders
 __global__ void k_gridfit_load(int M, int N, int nf, const double *__restrict__ vals, int stride,
-                               const int *__restrict__ iters, double *__restrict__ b,
-                               double *__restrict__ x, unsigned char *__restrict__ mask) {
+                               const int *__restrict__ iters, const double *__restrict__ guess,
+                               double *__restrict__ b, double *__restrict__ x,
+                               unsigned char *__restrict__ mask) {
   const long long n = (long long)M * N;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
@@ -690,7 +691,7 @@ __global__ void k_gridfit_load(int M, int N, int nf, const double *__restrict__ 
       const bool ok = !bad && !isnan(v);
       mask[f * n + k] = ok;
       b[f * n + k] = ok ? v : 0.0;
-      x[f * n + k] = ok ? v : 0.0;
+      x[f * n + k] = ok ? v : (guess ? guess[k * stride + f] : 0.0);
     }
   }
 }
@@ -1113,10 +1114,10 @@ int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_
 }
 
 int gridfit_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
-                 const int *bad_iters, cudaStream_t st, int f0) {
+                 const int *bad_iters, cudaStream_t st, int f0, const double *guess) {
   const long long n = (long long)M * N;
-  k_gridfit_load<<<blocks_for(n), 256, 0, st>>>(M, N, nf, vals, stride, bad_iters, w.b + f0 * n,
-                                                w.x + f0 * n, w.mask + f0 * n);
+  k_gridfit_load<<<blocks_for(n), 256, 0, st>>>(M, N, nf, vals, stride, bad_iters, guess,
+                                                w.b + f0 * n, w.x + f0 * n, w.mask + f0 * n);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

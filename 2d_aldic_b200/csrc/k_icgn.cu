@@ -12,15 +12,19 @@
 // forms b, the convergence test and dP = -H\b with the FP64 Cholesky factor
 // of H, and applies the inverse-compositional update in FP64.
 //
-// FP32 sampling reads a per-cell table of the bicubic's polynomial
-// coefficients (cubic_table: 16 FP32 per pixel, four 16-byte loads), so a
-// sample is two Horner rules (15 FMA) instead of 8 Keys weights and 20 tap
-// products, and maps lanes to subset columns: lane l walks column l (then
-// l + 32, ...) down the rows, so X is fixed per lane and Y uniform per row
-// -- u and v are one FMA each from per-lane bases, the terms weighted by X
-// are summed unweighted and multiplied by X once, and the columns past the
-// last full 32 (one for a 33-pixel window) are spread over the lanes by
-// pixel.  FP64 keeps the plain stencil over the image, pixel per lane.
+// FP32 sampling reads the row-cubic coefficients of the deformed image
+// (row_cubic: per pixel the Keys cubic of its row around that floor column,
+// one 16-byte load): a sample is four Horner rules over tu on its four
+// stencil rows and one cubic over tv.  Lanes map to subset columns: lane l
+// walks column l (then l + 32, ...) down the rows, so X is fixed per lane and
+// Y uniform per row -- u and v are one FMA each from per-lane bases, the
+// terms weighted by X are summed unweighted and multiplied by X once -- and
+// a lane keeps its last four stencil rows in registers: the next row of the
+// column usually sits one image row lower on the same floor column
+// (F12, F22 small), so it loads one new stencil row instead of four.  The
+// columns past the last full 32 (one for a 33-pixel window) are spread over
+// the lanes by pixel.  FP64 keeps the plain stencil over the image, pixel per
+// lane.
 //
 // ZNSSD residual (funICGN.m:238): r = (f - fbar)/bf - (g - gbar)/bg.  With
 // sd_k the steepest-descent images,
@@ -28,6 +32,7 @@
 // where S_fk = sum sd_k (f - fbar), S_k = sum sd_k are fixed per subset and
 // T_k = sum sd_k (g - c), gm = mean(g) - c are accumulated per iteration with
 // the shift c = fbar (which keeps the one-pass variance well conditioned).
+#include <climits>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -174,18 +179,26 @@ __device__ __forceinline__ double sample_minus(const double *img, int W, int cx,
   return sample<double>(img, W, cx, cy, tu, tv) - c;
 }
 
-// FP32 bicubic at fractions (tu, tv) of the cell at q in plane 0 of the
-// coefficient table (cubic_table: plane j, `plane` float4 further on, holds
-// the tv^j coefficients of tu^0..tu^3).
-__device__ __forceinline__ float cubic_at(const float4 *__restrict__ q, long long plane, float tu,
-                                          float tv) {
-  const float4 c0 = __ldg(q), c1 = __ldg(q + plane), c2 = __ldg(q + 2 * plane),
-               c3 = __ldg(q + 3 * plane);
-  const float p0 = fmaf(fmaf(fmaf(c0.w, tu, c0.z), tu, c0.y), tu, c0.x);
-  const float p1 = fmaf(fmaf(fmaf(c1.w, tu, c1.z), tu, c1.y), tu, c1.x);
-  const float p2 = fmaf(fmaf(fmaf(c2.w, tu, c2.z), tu, c2.y), tu, c2.x);
-  const float p3 = fmaf(fmaf(fmaf(c3.w, tu, c3.z), tu, c3.y), tu, c3.x);
-  return fmaf(fmaf(fmaf(p3, tv, p2), tv, p1), tv, p0);
+// Packed (two-lane) FP32 arithmetic of sm_100: two IEEE single-precision
+// operations per instruction.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// FP32 bicubic from the four stencil rows' cubic coefficients (r0 .. r3 =
+// image rows floor - 1 .. floor + 2) at fractions (tu, tv): each row's cubic
+// at tu, then the Keys cubic over the four row values at tv (the same
+// polynomial form as row_cubic, applied down the column).
+__device__ __forceinline__ float horner3(const float4 &a, float t) {
+  return fmaf(fmaf(fmaf(a.w, t, a.z), t, a.y), t, a.x);
+}
+__device__ __forceinline__ float cubic_rows(const float4 &r0, const float4 &r1, const float4 &r2,
+                                           const float4 &r3, float tu, float tv) {
+  const float h0 = horner3(r0, tu), h1 = horner3(r1, tu), h2 = horner3(r2, tu),
+              h3 = horner3(r3, tu);
+  const float c1 = 0.5f * (h2 - h0);
+  const float c2 = fmaf(-0.5f, h3, fmaf(2.0f, h2, fmaf(-2.5f, h1, h0)));
+  const float c3 = fmaf(1.5f, h1 - h2, 0.5f * (h3 - h0));
+  return fmaf(fmaf(fmaf(c3, tv, c2), tv, c1), tv, h1);
 }
 
 // Pixel p of a block of nw-wide rows (x fastest): its column and row as
@@ -217,17 +230,62 @@ template <typename Real> struct PixelMap {
 // sum Y fx d, sum Y fy d, sum fx d, sum fy d], d = g(warped) - cg
 // (SUB: only o[0], o[1], o[6], o[7]).
 struct Eval32 {
-  const float4 *tab;  // cubic_table (plane 0) at the cell of the centre's floor corner - (1, 1)
+  const float4 *rc;   // row_cubic at (floor corner x of the centre - 1, its y - 2)
   const float2 *gxy;  // reference gradients at the subset's top-left pixel
-  long long plane;    // W H: float4 from one coefficient plane to the next
   int W, nw;
   float ox, oy, a11, a12, a21, a22, c4, c5, cg;
 };
 
+// Packed partial sums of an evaluation: (sum d, sum d^2), (sum fx d, sum fy d)
+// and their X- and Y-weighted versions.
+struct Acc32 {
+  float2 S, T, TX, TY;
+};
+
+// One row of a lane's column: u, v at Y; the stencil rows slide down by one
+// when the floor corner moved one row down the same column, else all four
+// reload.  Slot (K + j) & 3 of R holds stencil row j (K = row index mod 4,
+// fixed by the unrolled caller), so sliding moves no registers.
+template <bool SUB, int K>
+__device__ __forceinline__ void col_row(const Eval32 &e, float4 (&R)[4], int &pcx, int &pcy,
+                                        float bu, float bv, float Y, const float2 *gp, float2 &C,
+                                        Acc32 &a) {
+  const int W = e.W;
+  const float ru = fmaf(e.a12, Y, bu), rv = fmaf(e.a22, Y, bv);
+  const float fu = floorf(ru), fv = floorf(rv);
+  const int icx = (int)fu, icy = (int)fv;
+  const float4 *q = e.rc + (icy + 3) * W + icx;  // stencil row 3
+  const bool slide = icx == pcx && icy == pcy + 1;
+  R[(K + 3) & 3] = __ldg(q);
+  if (!slide) {
+    R[K & 3] = __ldg(q - 3 * W);
+    R[(K + 1) & 3] = __ldg(q - 2 * W);
+    R[(K + 2) & 3] = __ldg(q - W);
+  }
+  pcx = icx;
+  pcy = icy;
+  const float d = cubic_rows(R[K & 3], R[(K + 1) & 3], R[(K + 2) & 3], R[(K + 3) & 3], ru - fu,
+                             rv - fv) - e.cg;
+  const float2 G = __ldg(gp);
+  const float2 D = f2(d);
+  a.S = __ffma2_rn(D, f2(1.f, d), a.S);
+  const float2 A = __fmul2_rn(G, D);
+  C = __fadd2_rn(C, A);
+  if (!SUB) a.TY = __ffma2_rn(A, f2(Y), a.TY);
+}
+
+// One FP32 evaluation of the residual sums over an nw x nw subset whose
+// top-left pixel is `base` and whose pixel (0, 0) sits at (ox, oy) from the
+// subset centre: u = a11 X + a12 Y + c4, v = a21 X + a22 Y + c5 relative to
+// the floor corner (xb, yb) of the centre (c4, c5 carry the centre's
+// fraction).  Per lane: o = [sum d, sum d^2, sum X fx d, sum X fy d,
+// sum Y fx d, sum Y fy d, sum fx d, sum fy d], d = g(warped) - cg
+// (SUB: only o[0], o[1], o[6], o[7]).
 template <bool SUB>
 __device__ __forceinline__ void eval32(const Eval32 &e, int lane, float o[8]) {
   const int W = e.W, nw = e.nw;
-  float s1 = 0.f, s2 = 0.f, yx = 0.f, yy = 0.f, tx = 0.f, ty = 0.f, xx = 0.f, xy = 0.f;
+  Acc32 a;
+  a.S = a.T = a.TX = a.TY = f2(0.f);
   // full 32-column blocks: lane = column, rows in order
   const int nch = nw >> 5;
   for (int ch = 0; ch < nch; ++ch) {
@@ -235,28 +293,18 @@ __device__ __forceinline__ void eval32(const Eval32 &e, int lane, float o[8]) {
     const float X = e.ox + (float)col;
     const float bu = fmaf(e.a11, X, e.c4), bv = fmaf(e.a21, X, e.c5);
     const float2 *gp = e.gxy + col;
-    float cx = 0.f, cy = 0.f, Y = e.oy;
-    for (int r = 0; r < nw; ++r, Y += 1.f, gp += W) {
-      const float ru = fmaf(e.a12, Y, bu), rv = fmaf(e.a22, Y, bv);
-      const float fu = floorf(ru), fv = floorf(rv);
-      const float d = cubic_at(e.tab + ((int)fv * W + (int)fu), e.plane, ru - fu, rv - fv) - e.cg;
-      const float2 G = __ldg(gp);
-      s1 += d;
-      s2 = fmaf(d, d, s2);
-      const float ax = G.x * d, ay = G.y * d;
-      cx += ax;
-      cy += ay;
-      if (!SUB) {
-        yx = fmaf(ax, Y, yx);
-        yy = fmaf(ay, Y, yy);
-      }
+    float2 C = f2(0.f);
+    float4 R[4];
+    int pcx = INT_MIN, pcy = 0;
+    float Y = e.oy;
+    for (int r = 0; r < nw; r += 4, Y += 4.f, gp += 4 * W) {
+      col_row<SUB, 0>(e, R, pcx, pcy, bu, bv, Y, gp, C, a);
+      if (r + 1 < nw) col_row<SUB, 1>(e, R, pcx, pcy, bu, bv, Y + 1.f, gp + W, C, a);
+      if (r + 2 < nw) col_row<SUB, 2>(e, R, pcx, pcy, bu, bv, Y + 2.f, gp + 2 * W, C, a);
+      if (r + 3 < nw) col_row<SUB, 3>(e, R, pcx, pcy, bu, bv, Y + 3.f, gp + 3 * W, C, a);
     }
-    tx += cx;
-    ty += cy;
-    if (!SUB) {
-      xx = fmaf(X, cx, xx);
-      xy = fmaf(X, cy, xy);
-    }
+    a.T = __fadd2_rn(a.T, C);
+    if (!SUB) a.TX = __ffma2_rn(C, f2(X), a.TX);
   }
   // the remaining columns (one for a 33-pixel window), pixel per lane
   const int c0 = nch << 5, rem = nw - c0;
@@ -264,28 +312,28 @@ __device__ __forceinline__ void eval32(const Eval32 &e, int lane, float o[8]) {
     const PixelMap<float> pm(rem, W);
     const int np = rem * nw;
     for (int p = lane; p < np; p += 32) {
-      float rc, rr;
-      const int k = c0 + pm.at(p, &rc, &rr);
-      const float X = e.ox + (float)c0 + rc, Y = e.oy + rr;
+      float rcol, rrow;
+      const int k = c0 + pm.at(p, &rcol, &rrow);
+      const float X = e.ox + (float)c0 + rcol, Y = e.oy + rrow;
       const float ru = fmaf(e.a11, X, fmaf(e.a12, Y, e.c4));
       const float rv = fmaf(e.a21, X, fmaf(e.a22, Y, e.c5));
       const float fu = floorf(ru), fv = floorf(rv);
-      const float d = cubic_at(e.tab + ((int)fv * W + (int)fu), e.plane, ru - fu, rv - fv) - e.cg;
+      const float4 *q = e.rc + (int)fv * W + (int)fu;
+      const float d = cubic_rows(__ldg(q), __ldg(q + W), __ldg(q + 2 * W), __ldg(q + 3 * W),
+                                 ru - fu, rv - fv) - e.cg;
       const float2 G = __ldg(e.gxy + k);
-      s1 += d;
-      s2 = fmaf(d, d, s2);
-      const float ax = G.x * d, ay = G.y * d;
-      tx += ax;
-      ty += ay;
+      const float2 D = f2(d);
+      a.S = __ffma2_rn(D, f2(1.f, d), a.S);
+      const float2 A = __fmul2_rn(G, D);
+      a.T = __fadd2_rn(a.T, A);
       if (!SUB) {
-        xx = fmaf(ax, X, xx);
-        xy = fmaf(ay, X, xy);
-        yx = fmaf(ax, Y, yx);
-        yy = fmaf(ay, Y, yy);
+        a.TX = __ffma2_rn(A, f2(X), a.TX);
+        a.TY = __ffma2_rn(A, f2(Y), a.TY);
       }
     }
   }
-  o[0] = s1; o[1] = s2; o[2] = xx; o[3] = xy; o[4] = yx; o[5] = yy; o[6] = tx; o[7] = ty;
+  o[0] = a.S.x; o[1] = a.S.y; o[2] = a.TX.x; o[3] = a.TX.y;
+  o[4] = a.TY.x; o[5] = a.TY.y; o[6] = a.T.x; o[7] = a.T.y;
 }
 
 // The FP32 setup sums of one subset (c the centre pixel's value): the
@@ -310,64 +358,71 @@ __device__ __forceinline__ void setup32(const float *fI, const float2 *gxy, int 
     const float X = ox + (float)col;
     const float *fp = fI + base + col;
     const float2 *gp = gxy + base + col;
-    // column sums: S1 = sum, SY = sum Y., SYY = sum Y^2. of fxx, fxy, fyy
-    float sx = 0.f, sy = 0.f, fdx = 0.f, fdy = 0.f;
-    float h1[3] = {0.f, 0.f, 0.f}, hY[3] = {0.f, 0.f, 0.f}, hYY[3] = {0.f, 0.f, 0.f};
+    // column sums, packed in pairs: (sum d, sum d^2), (sum fx, sum fy),
+    // (sum fx d, sum fy d), their Y-weighted versions, and sum, sum Y,
+    // sum Y^2 of (fxx, fxy) and of fyy
+    float2 AD = f2(0.f), SG = f2(0.f), FD = f2(0.f), SGY = f2(0.f), FDY = f2(0.f);
+    float2 H1 = f2(0.f), HY = f2(0.f), HYY = f2(0.f);
+    float h1yy = 0.f, hYyy = 0.f, hYYyy = 0.f;
     float Y = oy;
+#pragma unroll 4
     for (int r = 0; r < nw; ++r, Y += 1.f, fp += W, gp += W) {
       const float2 G = __ldg(gp);
       const float d = __ldg(fp) - c;
       cnt += G.x == 0.f;
-      a1 += d;
-      a2 = fmaf(d, d, a2);
-      sx += G.x;
-      sy += G.y;
-      const float ax = G.x * d, ay = G.y * d;
-      fdx += ax;
-      fdy += ay;
+      const float2 D = f2(d);
+      AD = __ffma2_rn(D, f2(1.f, d), AD);
+      SG = __fadd2_rn(SG, G);
+      const float2 A = __fmul2_rn(G, D);
+      FD = __fadd2_rn(FD, A);
       if (!SUB) {
-        sk[2] = fmaf(G.x, Y, sk[2]);
-        sk[3] = fmaf(G.y, Y, sk[3]);
-        sfk[2] = fmaf(ax, Y, sfk[2]);
-        sfk[3] = fmaf(ay, Y, sfk[3]);
-        const float YY = Y * Y;
-        const float f3[3] = {G.x * G.x, G.x * G.y, G.y * G.y};
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          h1[q] += f3[q];
-          hY[q] = fmaf(Y, f3[q], hY[q]);
-          hYY[q] = fmaf(YY, f3[q], hYY[q]);
-        }
+        const float2 YP = f2(Y);
+        SGY = __ffma2_rn(G, YP, SGY);
+        FDY = __ffma2_rn(A, YP, FDY);
+        const float2 FX = __fmul2_rn(f2(G.x), G);  // (fxx, fxy)
+        const float fyy = G.y * G.y, YY = Y * Y;
+        H1 = __fadd2_rn(H1, FX);
+        HY = __ffma2_rn(YP, FX, HY);
+        HYY = __ffma2_rn(f2(YY), FX, HYY);
+        h1yy += fyy;
+        hYyy = fmaf(Y, fyy, hYyy);
+        hYYyy = fmaf(YY, fyy, hYYyy);
       }
     }
-    sk[4] += sx;
-    sk[5] += sy;
-    sfk[4] += fdx;
-    sfk[5] += fdy;
+    a1 += AD.x;
+    a2 += AD.y;
+    sk[4] += SG.x;
+    sk[5] += SG.y;
+    sfk[4] += FD.x;
+    sfk[5] += FD.y;
     if (!SUB) {
       const float XX = X * X;
-      sk[0] = fmaf(X, sx, sk[0]);
-      sk[1] = fmaf(X, sy, sk[1]);
-      sfk[0] = fmaf(X, fdx, sfk[0]);
-      sfk[1] = fmaf(X, fdy, sfk[1]);
-      hh[0] = fmaf(XX, h1[0], hh[0]);
-      hh[1] = fmaf(XX, h1[1], hh[1]);
-      hh[2] = fmaf(X, hY[0], hh[2]);
-      hh[3] = fmaf(X, hY[1], hh[3]);
-      hh[4] = fmaf(X, h1[0], hh[4]);
-      hh[5] = fmaf(X, h1[1], hh[5]);
-      hh[6] = fmaf(XX, h1[2], hh[6]);
-      hh[7] = fmaf(X, hY[2], hh[7]);
-      hh[8] = fmaf(X, h1[2], hh[8]);
-      hh[9] += hYY[0];
-      hh[10] += hYY[1];
-      hh[11] += hY[0];
-      hh[12] += hY[1];
-      hh[13] += hYY[2];
-      hh[14] += hY[2];
-      hh[15] += h1[0];
-      hh[16] += h1[1];
-      hh[17] += h1[2];
+      sk[0] = fmaf(X, SG.x, sk[0]);
+      sk[1] = fmaf(X, SG.y, sk[1]);
+      sk[2] += SGY.x;
+      sk[3] += SGY.y;
+      sfk[0] = fmaf(X, FD.x, sfk[0]);
+      sfk[1] = fmaf(X, FD.y, sfk[1]);
+      sfk[2] += FDY.x;
+      sfk[3] += FDY.y;
+      hh[0] = fmaf(XX, H1.x, hh[0]);
+      hh[1] = fmaf(XX, H1.y, hh[1]);
+      hh[2] = fmaf(X, HY.x, hh[2]);
+      hh[3] = fmaf(X, HY.y, hh[3]);
+      hh[4] = fmaf(X, H1.x, hh[4]);
+      hh[5] = fmaf(X, H1.y, hh[5]);
+      hh[6] = fmaf(XX, h1yy, hh[6]);
+      hh[7] = fmaf(X, hYyy, hh[7]);
+      hh[8] = fmaf(X, h1yy, hh[8]);
+      hh[9] += HYY.x;
+      hh[10] += HYY.y;
+      hh[11] += HY.x;
+      hh[12] += HY.y;
+      hh[13] += hYYyy;
+      hh[14] += hYyy;
+      hh[15] += H1.x;
+      hh[16] += H1.y;
+      hh[17] += h1yy;
     }
   }
   const int c0 = nch << 5, rem = nw - c0;
@@ -694,8 +749,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       for (int q = 0; q < 8; ++q) sums[q] = nan64();
     } else if constexpr (sizeof(Real) == 4) {
       Eval32 e;
-      e.tab = im.gc + ((long long)(yb - 1) * W + (xb - 1));
-      e.plane = (long long)W * im.H;
+      e.rc = im.gc + ((long long)(yb - 2) * W + (xb - 1));
       e.gxy = im.gxy + base;
       e.W = W; e.nw = nw;
       e.ox = (float)ox; e.oy = (float)oy;
@@ -817,13 +871,17 @@ template <typename Real, bool SUB, int NW, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) k_icgn(Args a) {
   __shared__ double Lsh[NW][WS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  while (true) {
-    unsigned int s = 0;
-    if (lane == 0) s = atomicAdd(a.queue, 1u);
-    s = __shfl_sync(0xffffffffu, s, 0);
-    if ((long long)s >= a.n) break;
+  unsigned int s = 0;
+  if (lane == 0) s = atomicAdd(a.queue, 1u);
+  s = __shfl_sync(0xffffffffu, s, 0);
+  while ((long long)s < a.n) {
+    // the next subset's index is requested before this one is processed, so
+    // the atomic's round trip overlaps the work
+    unsigned int next = 0;
+    if (lane == 0) next = atomicAdd(a.queue, 1u);
     process<Real, SUB>(a, (long long)s, lane, Lsh[wid]);
     __syncwarp();
+    s = __shfl_sync(0xffffffffu, next, 0);
   }
 }
 

@@ -132,19 +132,17 @@ int normalize(const void *img, int dtype, long long n, const double *d_stats, do
   return OK;
 }
 
-// ------------------------------------------------------ bicubic coefficients
-// The Keys cubic (a = -1/2) of ba_interp2.cpp as a polynomial per cell: with
-// taps g_k (k = 0..3 at offsets -1..2 from the floor corner) and fraction t,
-// sum_k w_k(t) g_k = sum_p t^p (M g)_p, where row p of M holds the t^p
-// coefficients of the four Keys weights.  A cell's bicubic is then
-// sum_{j,i} tv^j tu^i C_ji with C = M G M^T (G the 4 x 4 stencil, rows along
-// y), so the FP32 sampler evaluates two Horner rules instead of forming 8
-// weights and 20 tap products.  Plane j of the table holds, for the cell
-// whose 0-based floor corner is (x, y), q[j W H + y W + x] = (C_j0, C_j1,
-// C_j2, C_j3) -- planes, so that a warp reading neighbouring cells reads 512
-// contiguous bytes per plane -- from the FP64 image, rounded once to FP32;
-// cells whose stencil leaves the image hold zeros (the IC-GN out-of-image
-// test keeps every sampled corner in [2, W-3] x [2, H-3]).
+// ---------------------------------------------------- row-cubic coefficients
+// The Keys cubic (a = -1/2) of ba_interp2.cpp along one row as a polynomial:
+// with taps g_k (k = 0..3 at offsets -1..2 from the floor column) and
+// fraction t, sum_k w_k(t) g_k = a0 + a1 t + a2 t^2 + a3 t^3, where row p of
+// the 4 x 4 matrix behind keys_rows holds the t^p coefficients of the four
+// Keys weights.  q[y W + x] = (a0, a1, a2, a3) of row y with floor column x,
+// from the FP64 image and rounded once to FP32 (zeros where the stencil
+// leaves the row: the IC-GN out-of-image test keeps every sampled floor
+// column in [2, W-3]).  A bicubic sample is then four Horner rules over tu
+// on consecutive rows and one cubic over tv -- and consecutive rows of a
+// subset column share three of their four stencil rows.
 __device__ __forceinline__ void keys_rows(const double g[4], double a[4]) {
   a[0] = g[1];
   a[1] = 0.5 * (g[2] - g[0]);
@@ -152,42 +150,24 @@ __device__ __forceinline__ void keys_rows(const double g[4], double a[4]) {
   a[3] = 0.5 * (g[3] - g[0]) + 1.5 * (g[1] - g[2]);
 }
 
-__global__ void k_cubic_table(const double *__restrict__ g, int W, int H,
-                              float4 *__restrict__ q) {
-  const long long n = (long long)W * H;
+__global__ void k_row_cubic(const double *__restrict__ g, int W, long long n,
+                            float4 *__restrict__ q) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int y = (int)(i / W), x = (int)(i - (long long)y * W);
-    if (x < 1 || y < 1 || x > W - 3 || y > H - 3) {
-      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-      q[i] = q[n + i] = q[2 * n + i] = q[3 * n + i] = z;
+    const int x = (int)(i % W);
+    if (x < 1 || x > W - 3) {
+      q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       continue;
     }
-    // R[r][p]: the t^p coefficient along stencil row r
-    double R[4][4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const double *row = g + (long long)(y - 1 + r) * W + (x - 1);
-      const double t[4] = {__ldg(row), __ldg(row + 1), __ldg(row + 2), __ldg(row + 3)};
-      keys_rows(t, R[r]);
-    }
-    double C[4][4];  // C[j][p]: the tv^j tu^p coefficient
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const double col[4] = {R[0][p], R[1][p], R[2][p], R[3][p]};
-      double c[4];
-      keys_rows(col, c);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) C[j][p] = c[j];
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      q[j * n + i] = make_float4((float)C[j][0], (float)C[j][1], (float)C[j][2], (float)C[j][3]);
+    const double t[4] = {__ldg(g + i - 1), __ldg(g + i), __ldg(g + i + 1), __ldg(g + i + 2)};
+    double a[4];
+    keys_rows(t, a);
+    q[i] = make_float4((float)a[0], (float)a[1], (float)a[2], (float)a[3]);
   }
 }
 
-int cubic_table(const double *g, int W, int H, float4 *q, cudaStream_t st) {
-  k_cubic_table<<<1184, 256, 0, st>>>(g, W, H, q);
+int row_cubic(const double *g, int W, int H, float4 *q, cudaStream_t st) {
+  k_row_cubic<<<1184, 256, 0, st>>>(g, W, (long long)W * H, q);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

@@ -15,10 +15,9 @@ int normalize(const void *img, int dtype, long long n, const double *d_stats, do
               float *o32, cudaStream_t st);
 int gradient(const double *f, const double *mask, int W, int H, double *gx64, double *gy64,
              float *gx32, float *gy32, cudaStream_t st);
-// bicubic polynomial coefficients of every cell of the FP64 image g: four
-// planes of W H float4, q[j W H + y W + x] = the tv^j row (tu^0..3) of the
-// cell at (x, y)
-int cubic_table(const double *g, int W, int H, float4 *q, cudaStream_t st);
+// row-cubic coefficients of the FP64 image g: W H float4, q[y W + x] =
+// (a0, a1, a2, a3) of row y's Keys cubic on floor column x
+int row_cubic(const double *g, int W, int H, float4 *q, cudaStream_t st);
 // q[i] = (gx[i], gy[i]), n float2
 int grad_pairs(const float *gx, const float *gy, long long n, float2 *q, cudaStream_t st);
 int interp_f64(const double *F, long long M, long long N, long long P, const double *X,
@@ -51,7 +50,7 @@ int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, co
 // ---- k_icgn.cu
 struct IcgnImages {
   const float *f32, *g32, *gx32, *gy32;
-  const float4 *gc;   // bicubic coefficients of g (cubic_table): the FP32 sampler's
+  const float4 *gc;   // row-cubic coefficients of g (row_cubic): the FP32 sampler's
   const float2 *gxy;  // (gx32, gy32) pairs (grad_pairs) read by the FP32 IC-GN
   const double *f64, *g64, *gx64, *gy64;
   int W, H;
@@ -200,9 +199,12 @@ int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const do
 int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int f0 = 0);
 // nodal strain (funGlobal_NodalStrainAvg.m)
 int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st);
-// gridfit springs: load nf interleaved (stride, offset) fields, NaN = no data
+// gridfit springs: load nf interleaved (stride, offset) fields, NaN = no data;
+// the solve starts from the data and, at nodes without data, from guess (the
+// same layout as vals; 0 where null) -- the solution does not depend on it
 int gridfit_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
-                 const int *bad_iters, cudaStream_t st, int f0 = 0);
+                 const int *bad_iters, cudaStream_t st, int f0 = 0,
+                 const double *guess = nullptr);
 int grid_store(const GridWork &w, int M, int N, int nf, double *vals, int stride,
                cudaStream_t st, int f0 = 0);
 // inpaint springs: load nf fields, nodes flagged (NaN or bad) are unknown
