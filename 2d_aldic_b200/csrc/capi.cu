@@ -1401,12 +1401,18 @@ __global__ void k_beta_select(const double *err, double base, double *beta_out, 
   *beta_out = beta;
 }
 
-template <typename T>
-T *carve(char *&p, long long count) {
-  T *r = (T *)p;
-  p += ((sizeof(T) * count + 255) / 256) * 256;
-  return r;
-}
+// Lays out a slab of 256-byte-aligned arrays: a pass with no base only sums
+// the sizes, so a slab is sized by the same sequence of take() calls that
+// carves it.
+struct Carver {
+  char *base = nullptr;
+  size_t off = 0;
+  template <typename T> T *take(long long count) {
+    T *r = base ? (T *)(base + off) : nullptr;
+    off += ((sizeof(T) * (size_t)count + 255) / 256) * 256;
+    return r;
+  }
+};
 
 int frame_geometry(aldic_ctx *c, const aldic_frame_params *p, int gx[2], int gy[2], int *M, int *N,
                    int *gx1 = nullptr, int *gy1 = nullptr) {
@@ -1769,16 +1775,20 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
   aldic_qt_mesh &m = *Q.mesh;
   const long long n = m.n;
   const int nb = (int)((n + 255) / 256 > 1184 ? 1184 : (n + 255) / 256);
-  if ((rc = Q.slab.ensure(sizeof(double) * (49 * n + 2048) + sizeof(int) * (2 * n + 16) + n + 512)))
-    return rc;
   {
-    char *q = (char *)Q.slab.p;
-    Q.U0 = carve<double>(q, 2 * n); Q.U1 = carve<double>(q, 2 * n); Q.F1 = carve<double>(q, 4 * n);
-    Q.U2 = carve<double>(q, 2 * n); Q.F2 = carve<double>(q, 4 * n); Q.ud = carve<double>(q, 4 * n);
-    Q.vd = carve<double>(q, 2 * n); Q.U2old = carve<double>(q, 2 * n); Q.U1old = carve<double>(q, 2 * n);
-    Q.H21 = carve<double>(q, 21 * n); Q.norms = carve<double>(q, 2048); Q.Uicgn = carve<double>(q, 2 * n);
-    Q.it1 = carve<int>(q, n); Q.itb = carve<int>(q, n); Q.ints = carve<int>(q, 16);
-    Q.bad = carve<unsigned char>(q, n);
+    auto layout = [&](Carver &q) {
+      Q.U0 = q.take<double>(2 * n); Q.U1 = q.take<double>(2 * n); Q.F1 = q.take<double>(4 * n);
+      Q.U2 = q.take<double>(2 * n); Q.F2 = q.take<double>(4 * n); Q.ud = q.take<double>(4 * n);
+      Q.vd = q.take<double>(2 * n); Q.U2old = q.take<double>(2 * n); Q.U1old = q.take<double>(2 * n);
+      Q.H21 = q.take<double>(21 * n); Q.norms = q.take<double>(2048); Q.Uicgn = q.take<double>(2 * n);
+      Q.it1 = q.take<int>(n); Q.itb = q.take<int>(n); Q.ints = q.take<int>(16);
+      Q.bad = q.take<unsigned char>(n);
+    };
+    Carver sizing;
+    layout(sizing);
+    if ((rc = Q.slab.ensure(sizing.off))) return rc;
+    Carver q{(char *)Q.slab.p, 0};
+    layout(q);
     Q.n = (int)n;
   }
   double *part = Q.norms + 1024, *nrm = Q.norms;  // nrm: [0,8) sweep, [8,40) ADMM
@@ -1913,7 +1923,8 @@ int aldic_icgn_autotune(int enable) {
 
 int aldic_icgn_shape(int precision, int subpb1, int winsize, long long n, int *nwarps, int *minb,
                      float *ms, int *count) {
-  if (icgn_tuned_shape(precision, subpb1 != 0, winsize, n, nwarps, minb, ms, count) == OK) return OK;
+  ALDIC_CHECK(subpb1 >= 0 && subpb1 <= 2, E_ARG, "icgn_shape: instance must be 0, 1 or 2");
+  if (icgn_tuned_shape(precision, subpb1, winsize, n, nwarps, minb, ms, count) == OK) return OK;
   set_error("icgn_shape: no tuned launch shape for this geometry");
   return E_STATE;
 }
@@ -2052,28 +2063,29 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
       (rc = search_work_ensure(c->sw, c->W, c->H, M, N, p->search, p->winsize, c->dtype)))
     return rc;
   // frame slab
-  const long long ny_nx = n;
-  const size_t need = 256 * 40 + sizeof(double) * (5 * ny_nx + 2 * n + 2 * n + 2 * n + 2 * n + 4 * n +
-                                                   21 * n + 2 * n + 4 * n + 4 * n + 2 * n + 2 * n +
-                                                   2 * n + 8 * n + 4 * n + 64 + 1024) +
-                      sizeof(int) * (2 * n + 16) + n + 256;
+  FrameBufs B;
+  auto layout = [&](Carver &q) {
+    B.sx = q.take<double>(n); B.sy = q.take<double>(n); B.su = q.take<double>(n);
+    B.sv = q.take<double>(n); B.scc = q.take<double>(n);
+    B.coords = q.take<double>(2 * n); B.x0 = q.take<double>(n); B.y0 = q.take<double>(n);
+    B.U0 = q.take<double>(2 * n); B.U1 = q.take<double>(2 * n); B.F1 = q.take<double>(4 * n);
+    B.H21 = q.take<double>(21 * n); B.U2 = q.take<double>(2 * n); B.F2 = q.take<double>(4 * n);
+    B.udual = q.take<double>(4 * n); B.vdual = q.take<double>(2 * n);
+    B.U2old = q.take<double>(2 * n); B.U1old = q.take<double>(2 * n);
+    B.cache = q.take<double>((long long)kIcgnCache * n);
+    B.F0 = q.take<double>(4 * n);
+    B.err = q.take<double>(16); B.beta = q.take<double>(4); B.upd = q.take<double>(32);
+    B.part = q.take<double>(1024); B.meanit = q.take<double>(4);
+    B.it1 = q.take<int>(n); B.itb = q.take<int>(n); B.ints = q.take<int>(16);
+    B.bad = q.take<unsigned char>(n);
+  };
+  Carver sizing;
+  layout(sizing);
+  const size_t need = sizing.off;
   bool realloc = c->fr.cap < need;
   if ((rc = c->fr.ensure(need))) return rc;
-  char *q = (char *)c->fr.p;
-  FrameBufs B;
-  B.sx = carve<double>(q, n); B.sy = carve<double>(q, n); B.su = carve<double>(q, n);
-  B.sv = carve<double>(q, n); B.scc = carve<double>(q, n);
-  B.coords = carve<double>(q, 2 * n); B.x0 = carve<double>(q, n); B.y0 = carve<double>(q, n);
-  B.U0 = carve<double>(q, 2 * n); B.U1 = carve<double>(q, 2 * n); B.F1 = carve<double>(q, 4 * n);
-  B.H21 = carve<double>(q, 21 * n); B.U2 = carve<double>(q, 2 * n); B.F2 = carve<double>(q, 4 * n);
-  B.udual = carve<double>(q, 4 * n); B.vdual = carve<double>(q, 2 * n);
-  B.U2old = carve<double>(q, 2 * n); B.U1old = carve<double>(q, 2 * n);
-  B.cache = carve<double>(q, 8 * n);
-  B.F0 = carve<double>(q, 4 * n);
-  B.err = carve<double>(q, 16); B.beta = carve<double>(q, 4); B.upd = carve<double>(q, 32);
-  B.part = carve<double>(q, 1024); B.meanit = carve<double>(q, 4);
-  B.it1 = carve<int>(q, n); B.itb = carve<int>(q, n); B.ints = carve<int>(q, 16);
-  B.bad = carve<unsigned char>(q, n);
+  Carver q{(char *)c->fr.p, 0};
+  layout(q);
   // graph key: geometry, every parameter that changes the recorded work and
   // the buffers the graph addresses
   char key[512];

@@ -202,6 +202,10 @@ int tridiagonal_qr(int n, std::vector<double> &d, std::vector<double> &e, std::v
 // 32-wide K chunks go to shared memory by cp.async (no register round trip),
 // double-buffered so that chunk c + 1 arrives while chunk c is multiplied.
 constexpr int TR = 64, TC = 64, KC = 32, GT = 256, LDT = TR + 1;
+// Products with fewer tiles than SMs (the 2-field solves: 32 tiles at 243^2)
+// split K into up to kMaxSplit slices written to a partial buffer and summed
+// in a fixed order by k_fdm_reduce (deterministic, no atomics).
+constexpr int kMaxSplit = 4, kFdmPart = 8;  // partial capacity: kFdmPart fields of M N
 constexpr int kBuf = 2 * KC * LDT;                              // doubles per buffer (A + B)
 constexpr int kSmem = 2 * kBuf * (int)sizeof(double);           // two buffers: 66 560 B
 
@@ -230,6 +234,9 @@ struct GemmArgs {
   double mu;
   double beta[12];
   const double *beta_ptr;  // if set, beta = *beta_ptr for every batch entry
+  // split K: slice s of batch entry b writes P[(s batch + b) R Cn + r Cn + c]
+  int splits;
+  double *P;
 };
 
 // stage K chunk [k0, k0 + KC) of the A and B tiles into buffer `buf`
@@ -259,24 +266,28 @@ __device__ __forceinline__ void stage_chunk(const GemmArgs &g, const double *A, 
 
 __global__ void __launch_bounds__(GT) k_fdm_gemm(GemmArgs g) {
   extern __shared__ double sm[];
-  const int b = blockIdx.z;
+  const int nb = gridDim.z / g.splits;
+  const int b = blockIdx.z % nb, sp = blockIdx.z / nb;
   const int r0 = blockIdx.y * TR, c0 = blockIdx.x * TC;
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const double *A = g.A + (long long)b * g.sab;
   const double *B = g.B + (long long)b * g.sbb;
   double acc[4][4] = {};
   const bool a_rfast = g.sar <= g.sak, b_cfast = g.sbc <= g.sbk;
-  const int nch = (g.K + KC - 1) / KC;
-  stage_chunk(g, A, B, r0, c0, 0, sm, a_rfast, b_cfast);
-  for (int ch = 0; ch < nch; ++ch) {
-    if (ch + 1 < nch) {
-      stage_chunk(g, A, B, r0, c0, (ch + 1) * KC, sm + ((ch + 1) & 1) * kBuf, a_rfast, b_cfast);
+  // this slice's K range, in whole chunks
+  const int nall = (g.K + KC - 1) / KC, per = (nall + g.splits - 1) / g.splits;
+  const int ch0 = sp * per, ch1 = ch0 + per < nall ? ch0 + per : nall;
+  if (ch0 < ch1) stage_chunk(g, A, B, r0, c0, ch0 * KC, sm, a_rfast, b_cfast);
+  for (int ch = ch0; ch < ch1; ++ch) {
+    if (ch + 1 < ch1) {
+      stage_chunk(g, A, B, r0, c0, (ch + 1) * KC, sm + ((ch + 1 - ch0) & 1) * kBuf, a_rfast,
+                  b_cfast);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const double *As = sm + (ch & 1) * kBuf, *Bs = As + KC * LDT;
+    const double *As = sm + ((ch - ch0) & 1) * kBuf, *Bs = As + KC * LDT;
     const int kc = g.K - ch * KC < KC ? g.K - ch * KC : KC;
 #pragma unroll 8
     for (int kk = 0; kk < kc; ++kk) {
@@ -291,7 +302,21 @@ __global__ void __launch_bounds__(GT) k_fdm_gemm(GemmArgs g) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
     }
-    __syncthreads();  // buffer (ch & 1) is restaged by the next round
+    __syncthreads();  // this buffer is restaged by the next round
+  }
+  if (g.splits > 1) {
+    double *P = g.P + ((long long)sp * nb + b) * g.R * g.Cn;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = r0 + ty + 16 * i;
+      if (r >= g.R) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = c0 + tx + 16 * j;
+        if (c < g.Cn) P[(long long)r * g.Cn + c] = acc[i][j];
+      }
+    }
+    return;
   }
   const double beta = g.beta_ptr ? *g.beta_ptr : g.beta[b < 12 ? b : 11];
   double *C = g.C + (long long)b * g.scb;
@@ -317,10 +342,38 @@ int gemm_setup() {
   return OK;
 }
 
-int gemm(const GemmArgs &g, int batch, cudaStream_t st) {
-  dim3 grid((unsigned)((g.Cn + TC - 1) / TC), (unsigned)((g.R + TR - 1) / TR), (unsigned)batch);
+// the split-K slices of every output summed in slice order, then the epilogue
+__global__ void k_fdm_reduce(GemmArgs g, int batch) {
+  const long long rc = (long long)g.R * g.Cn, n = rc * batch;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / rc);
+    const long long e = i - (long long)b * rc;
+    const int r = (int)(e / g.Cn), c = (int)(e - (long long)r * g.Cn);
+    double v = 0.0;
+    for (int s = 0; s < g.splits; ++s) v += g.P[((long long)s * batch + b) * rc + e];
+    if (g.scale) {
+      const double beta = g.beta_ptr ? *g.beta_ptr : g.beta[b < 12 ? b : 11];
+      v /= beta * (g.lr[r] + g.lc[c]) + g.mu;
+    }
+    g.C[(long long)b * g.scb + (long long)r * g.scr + (long long)c * g.scc] = v;
+  }
+}
+
+int gemm(GemmArgs g, int batch, double *part, cudaStream_t st) {
+  const int tiles = ((g.Cn + TC - 1) / TC) * ((g.R + TR - 1) / TR) * batch;
+  int sp = 1;
+  while (sp < kMaxSplit && tiles * sp < 148 && (sp + 1) * batch <= kFdmPart) ++sp;
+  g.splits = sp;
+  g.P = part;
+  dim3 grid((unsigned)((g.Cn + TC - 1) / TC), (unsigned)((g.R + TR - 1) / TR), (unsigned)(batch * sp));
   k_fdm_gemm<<<grid, GT, kSmem, st>>>(g);
   ALDIC_CUDA(cudaGetLastError());
+  if (sp > 1) {
+    const long long n = (long long)g.R * g.Cn * batch;
+    k_fdm_reduce<<<(unsigned)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184), 256, 0, st>>>(g, batch);
+    ALDIC_CUDA(cudaGetLastError());
+  }
   return OK;
 }
 
@@ -393,7 +446,8 @@ int fdm_ensure(FdmBasis &B, int type, int M, int N, double h, cudaStream_t st) {
   if ((rc = fdm_basis_1d(type, M, h, Vx, lx))) return rc;
   if ((rc = fdm_basis_1d(type, N, h, Vy, ly))) return rc;
   B.type = -1;
-  if ((rc = B.buf.ensure(sizeof(double) * host.size()))) return rc;
+  const size_t nbasis = host.size();
+  if ((rc = B.buf.ensure(sizeof(double) * (nbasis + (size_t)kFdmPart * M * N)))) return rc;
   ALDIC_CUDA(cudaMemcpyAsync(B.buf.p, host.data(), sizeof(double) * host.size(),
                              cudaMemcpyHostToDevice, st));
   ALDIC_CUDA(cudaStreamSynchronize(st));  // the host vector goes out of scope
@@ -402,6 +456,7 @@ int fdm_ensure(FdmBasis &B, int type, int M, int N, double h, cudaStream_t st) {
   B.Vy = d + (size_t)M * M;
   B.lx = B.Vy + (size_t)N * N;
   B.ly = B.lx + M;
+  B.part = d + nbasis;
   B.type = type;
   B.M = M;
   B.N = N;
@@ -425,25 +480,25 @@ int fdm_solve(const FdmBasis &B, int nrhs, const double *b, double *x, double *t
   g.B = B.Vx; g.sbb = 0; g.sbk = M; g.sbc = 1;
   g.C = tmp; g.scb = n; g.scr = M; g.scc = 1;
   g.R = N; g.Cn = M; g.K = M; g.scale = 0;
-  if ((rc = gemm(g, nrhs, st))) return rc;
+  if ((rc = gemm(g, nrhs, B.part, st))) return rc;
   // 2. C = Vy' T, C[q][p] /= beta (ly[q] + lx[p]) + mu  -> x
   g.A = B.Vy; g.sab = 0; g.sar = 1; g.sak = N;
   g.B = tmp; g.sbb = n; g.sbk = M; g.sbc = 1;
   g.C = x; g.scb = n; g.scr = M; g.scc = 1;
   g.R = N; g.Cn = M; g.K = N; g.scale = 1; g.lr = B.ly; g.lc = B.lx;
-  if ((rc = gemm(g, nrhs, st))) return rc;
+  if ((rc = gemm(g, nrhs, B.part, st))) return rc;
   // 3. S = C Vx'  -> tmp
   g.A = x; g.sab = n; g.sar = M; g.sak = 1;
   g.B = B.Vx; g.sbb = 0; g.sbk = 1; g.sbc = M;
   g.C = tmp; g.scb = n; g.scr = M; g.scc = 1;
   g.R = N; g.Cn = M; g.K = M; g.scale = 0;
-  if ((rc = gemm(g, nrhs, st))) return rc;
+  if ((rc = gemm(g, nrhs, B.part, st))) return rc;
   // 4. X = Vy S  -> x
   g.A = B.Vy; g.sab = 0; g.sar = N; g.sak = 1;
   g.B = tmp; g.sbb = n; g.sbk = M; g.sbc = 1;
   g.C = x; g.scb = n; g.scr = M; g.scc = 1;
   g.R = N; g.Cn = M; g.K = N; g.scale = 0;
-  return gemm(g, nrhs, st);
+  return gemm(g, nrhs, B.part, st);
 }
 
 }  // namespace aldic

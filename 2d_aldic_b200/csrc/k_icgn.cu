@@ -473,7 +473,7 @@ __device__ __forceinline__ void setup32(const float *fI, const float2 *gxy, int 
 template <bool SUB>
 __device__ __forceinline__ void fail_minus1(const Args &a, long long s, int lane) {
   if (lane == 0) {
-    if (!SUB && a.cache) a.cache[8 * s + 7] = -1.0;
+    if (!SUB && a.cache) a.cache[kIcgnCache * s + 7] = -1.0;
     a.iters[s] = -1;
     a.U[2 * s] = nan64();
     a.U[2 * s + 1] = nan64();
@@ -488,7 +488,7 @@ __device__ __forceinline__ void fail_minus1(const Args &a, long long s, int lane
 template <bool SUB>
 __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
   if (lane == 0) {
-    if (!SUB && a.cache) a.cache[8 * s + 7] = 102.0;
+    if (!SUB && a.cache) a.cache[kIcgnCache * s + 7] = 102.0;
     a.iters[s] = 102;
     a.U[2 * s] = a.U0[2 * s];
     a.U[2 * s + 1] = a.U0[2 * s + 1];
@@ -500,23 +500,31 @@ __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
 }
 
 
+// What one launch of the IC-GN kernel does for a subset: everything
+// (MODE_FULL), the setup only -- status, window, sums and the Cholesky factor
+// of H written to the per-subset cache record, H21 to its output --
+// (MODE_SETUP), or the iterations from that record (MODE_ITER).  Splitting
+// the FP32 LocalICGN in two leaves each launch fewer live registers, so more
+// warps stay resident to hide the gathers' latency.
+enum { MODE_FULL = 0, MODE_SETUP = 1, MODE_ITER = 2 };
+
 // ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
 // S_f[6] at 57, S[6] at 63 and 1 / diag(L) at 69 (kept out of registers to
 // raise occupancy)
 constexpr int WS = 76;
 
-template <typename Real, bool SUB>
+template <typename Real, bool SUB, int MODE>
 __device__ void process(const Args &a, long long s, int lane, double *ws) {
   double *Lsh = ws + 36, *Sfs = ws + 57, *Sks = ws + 63, *Linv = ws + 69;
   const IcgnImages &im = a.im;
   const double x0 = a.coords[s], y0 = a.coords[a.n + s];
   int w = a.wins ? a.wins[s] : a.w;
   int xl, yl;
-  const bool cached = SUB && a.cache;
+  const bool cached = (SUB && a.cache) || MODE == MODE_ITER;
   if (cached) {
     // the IC-GN launch of this frame already ran the setup on the same
     // reference image and window
-    const double stc = a.cache[8 * s + 7];
+    const double stc = a.cache[kIcgnCache * s + 7];
     if (stc == -1.0) {
       fail_minus1<SUB>(a, s, lane);
       return;
@@ -525,7 +533,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       done_102<SUB>(a, s, lane);
       return;
     }
-    w = (int)a.cache[8 * s + 6];
+    w = (int)a.cache[kIcgnCache * s + 6];
   }
   bool ok = subset_ok(im, x0, y0, w, &xl, &yl);
   if (!ok) {
@@ -551,14 +559,22 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     ox = (Real)oxd;
     oy = (Real)oyd;
     base = (yl - 1) * W + (xl - 1);
-    meanf = a.cache[8 * s + 0];
-    const double bfc = a.cache[8 * s + 1];
+    meanf = a.cache[kIcgnCache * s + 0];
+    const double bfc = a.cache[kIcgnCache * s + 1];
     ssf = bfc * bfc;
     if (lane == 0) {
-      Sfs[4] = a.cache[8 * s + 2];
-      Sfs[5] = a.cache[8 * s + 3];
-      Sks[4] = a.cache[8 * s + 4];
-      Sks[5] = a.cache[8 * s + 5];
+      Sfs[4] = a.cache[kIcgnCache * s + 2];
+      Sfs[5] = a.cache[kIcgnCache * s + 3];
+      Sks[4] = a.cache[kIcgnCache * s + 4];
+      Sks[5] = a.cache[kIcgnCache * s + 5];
+    }
+    if (!SUB && MODE == MODE_ITER) {
+      // the rest of the setup record: S_f0..3, S_0..3, L, 1 / diag(L)
+      const double *cc = a.cache + kIcgnCache * s;
+      for (int k = lane; k < 35; k += 32) {
+        double *dst = k < 4 ? Sfs + k : (k < 8 ? Sks + (k - 4) : (k < 29 ? Lsh + (k - 8) : Linv + (k - 29)));
+        *dst = cc[8 + k];
+      }
     }
   } else {
   for (int attempt = 0;; ++attempt) {
@@ -658,7 +674,7 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) Sfs[q] -= dmc * Sks[q];  // sum sd_k (f - mean f)
     if (!SUB && a.cache) {
-      double *cc = a.cache + 8 * s;
+      double *cc = a.cache + kIcgnCache * s;
       cc[0] = meanf;
       cc[1] = sqrt(ssf);
       cc[2] = Sfs[4];
@@ -667,6 +683,12 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       cc[5] = Sks[5];
       cc[6] = (double)w;
       cc[7] = 0.0;
+      if (MODE == MODE_SETUP) {
+        for (int q = 0; q < 4; ++q) {
+          cc[8 + q] = Sfs[q];
+          cc[12 + q] = Sks[q];
+        }
+      }
     }
   }
   }  // setup pass
@@ -686,7 +708,10 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
   double *Hm = ws;
   bool spd = true;
   double s2 = 0, l11i = 0, l21 = 0, l22i = 0;
-  if (!SUB) {
+  if (!SUB && MODE == MODE_ITER) {
+    spd = a.cache[kIcgnCache * s + 43] != 0.0;
+    __syncwarp();
+  } else if (!SUB) {
     if (lane == 0) {
       // H of funICGN.m:67-79 from its 18 distinct sums (index map)
       const unsigned char map[36] = {0, 1, 2, 3, 4, 5,   1, 6, 3, 7, 5, 8,
@@ -699,6 +724,19 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     }
     spd = __shfl_sync(0xffffffffu, (int)spd, 0);
     __syncwarp();
+    if (MODE == MODE_SETUP) {
+      // the record for the iteration launch, and H21 (funICGN.m:320)
+      if (lane == 0) {
+        double *cc = a.cache + kIcgnCache * s;
+        for (int k = 0; k < 21; ++k) cc[16 + k] = Lsh[k];
+        for (int k = 0; k < 6; ++k) cc[37 + k] = Linv[k];
+        cc[43] = spd ? 1.0 : 0.0;
+        int idx = 0;
+        for (int c = 0; c < 6; ++c)
+          for (int r = c; r < 6; ++r) a.H21out[(long long)(idx++) * a.n + s] = Hm[r * 6 + c];
+      }
+      return;
+    }
   } else {
     __syncwarp();
     // funICGN_Subpb1.m:73,281-283
@@ -854,9 +892,11 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     a.U[2 * s + 1] = P[5];
     if (!SUB) {
       for (int q = 0; q < 4; ++q) a.F[4 * s + q] = P[q];
-      int idx = 0;
-      for (int c = 0; c < 6; ++c)
-        for (int r = c; r < 6; ++r) a.H21out[(long long)(idx++) * a.n + s] = Hm[r * 6 + c];
+      if (MODE == MODE_FULL) {
+        int idx = 0;
+        for (int c = 0; c < 6; ++c)
+          for (int r = c; r < 6; ++r) a.H21out[(long long)(idx++) * a.n + s] = Hm[r * 6 + c];
+      }
     }
   }
 }
@@ -864,10 +904,11 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 // Launch shapes the autotuner chooses from: NW warps per CTA and MINB
 // resident CTAs per SM in the launch bounds (NW * 32 * MINB threads share
 // the SM's 64 K registers, so MINB sets the register cap: 8 x 4 and 4 x 8 ->
-// 64 registers, 8 x 3 -> 80, 8 x 2 -> 128, 4 x 6 -> 80, 16 x 2 -> 64; FP64:
-// 8 x 2 -> 128, 4 x 3 -> 168).  Every shape runs the same per-subset code,
+// 64 registers, 8 x 3 -> 80, 8 x 2 -> 128, 4 x 6 -> 80, 16 x 2 -> 64,
+// 4 x 5 -> 96 (rounded to the allocation unit); FP64: 8 x 2 -> 128, 4 x 3 ->
+// 168).  Every shape runs the same per-subset code,
 // so the results are bit-identical and only the time differs.
-template <typename Real, bool SUB, int NW, int MINB>
+template <typename Real, bool SUB, int MODE, int NW, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) k_icgn(Args a) {
   __shared__ double Lsh[NW][WS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -879,7 +920,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_icgn(Args a) {
     // the atomic's round trip overlaps the work
     unsigned int next = 0;
     if (lane == 0) next = atomicAdd(a.queue, 1u);
-    process<Real, SUB>(a, (long long)s, lane, Lsh[wid]);
+    process<Real, SUB, MODE>(a, (long long)s, lane, Lsh[wid]);
     __syncwarp();
     s = __shfl_sync(0xffffffffu, next, 0);
   }
@@ -890,23 +931,24 @@ struct Shape {
   const void *fn;
 };
 
-template <typename Real, bool SUB>
+template <typename Real, bool SUB, int MODE>
 std::vector<Shape> make_shapes() {
   if constexpr (sizeof(Real) == 4)
-    return {{8, 4, (const void *)k_icgn<Real, SUB, 8, 4>},
-            {8, 3, (const void *)k_icgn<Real, SUB, 8, 3>},
-            {8, 2, (const void *)k_icgn<Real, SUB, 8, 2>},
-            {4, 8, (const void *)k_icgn<Real, SUB, 4, 8>},
-            {4, 6, (const void *)k_icgn<Real, SUB, 4, 6>},
-            {16, 2, (const void *)k_icgn<Real, SUB, 16, 2>}};
+    return {{8, 4, (const void *)k_icgn<Real, SUB, MODE, 8, 4>},
+            {8, 3, (const void *)k_icgn<Real, SUB, MODE, 8, 3>},
+            {8, 2, (const void *)k_icgn<Real, SUB, MODE, 8, 2>},
+            {4, 8, (const void *)k_icgn<Real, SUB, MODE, 4, 8>},
+            {4, 6, (const void *)k_icgn<Real, SUB, MODE, 4, 6>},
+            {16, 2, (const void *)k_icgn<Real, SUB, MODE, 16, 2>},
+            {4, 5, (const void *)k_icgn<Real, SUB, MODE, 4, 5>}};
   else
-    return {{8, 2, (const void *)k_icgn<Real, SUB, 8, 2>},
-            {4, 3, (const void *)k_icgn<Real, SUB, 4, 3>}};
+    return {{8, 2, (const void *)k_icgn<Real, SUB, MODE, 8, 2>},
+            {4, 3, (const void *)k_icgn<Real, SUB, MODE, 4, 3>}};
 }
 
-template <typename Real, bool SUB>
+template <typename Real, bool SUB, int MODE>
 const std::vector<Shape> &shapes() {
-  static const std::vector<Shape> v = make_shapes<Real, SUB>();
+  static const std::vector<Shape> v = make_shapes<Real, SUB, MODE>();
   return v;
 }
 
@@ -952,18 +994,23 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
 bool g_tune_on = true;
 
-TuneKey tune_key(int prec, bool sub, int w, long long n) {
+// instance: 0 the LocalICGN iteration launch, 1 Subpb1, 2 the LocalICGN
+// setup launch, 3 LocalICGN in one launch
+int instance_of(bool sub, int mode) {
+  return sub ? 1 : (mode == MODE_SETUP ? 2 : (mode == MODE_ITER ? 0 : 3));
+}
+TuneKey tune_key(int prec, int inst, int w, long long n) {
   int dev = 0;
   cudaGetDevice(&dev);
   int nl = 0;
   while ((1LL << (nl + 1)) <= n) ++nl;
-  return TuneKey{prec, sub ? 1 : 0, dev, w, nl};
+  return TuneKey{prec, inst, dev, w, nl};
 }
 
-template <typename Real, bool SUB>
+template <typename Real, bool SUB, int MODE>
 int launch(const Args &a, cudaStream_t st) {
-  const auto &sv = shapes<Real, SUB>();
-  const TuneKey key = tune_key(sizeof(Real) == 8, SUB, a.wins ? -1 : a.w, a.n);
+  const auto &sv = shapes<Real, SUB, MODE>();
+  const TuneKey key = tune_key(sizeof(Real) == 8, instance_of(SUB, MODE), a.wins ? -1 : a.w, a.n);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
@@ -1014,13 +1061,20 @@ int icgn(const IcgnImages &im, const double *coords, long long n, const double *
   a.F0 = F0;
   a.im = im; a.coords = coords; a.n = n; a.U0 = U0; a.wins = wins; a.w = w; a.tol = tol;
   a.U = U; a.F = F; a.H21out = H21; a.iters = iters; a.queue = queue;
-  return precision ? launch<double, false>(a, st) : launch<float, false>(a, st);
+  if (precision) return launch<double, false, MODE_FULL>(a, st);
+  if (!cache) return launch<float, false, MODE_FULL>(a, st);
+  // FP32 with a setup record: setup launch, then the iterations from it
+  const int rc = launch<float, false, MODE_SETUP>(a, st);
+  return rc ? rc : launch<float, false, MODE_ITER>(a, st);
 }
 
 bool icgn_tuned(int precision, bool sub, int w, long long n) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   if (!g_tune_on || n < 2048) return true;
-  return g_tune.count(tune_key(precision ? 1 : 0, sub, w, n)) != 0;
+  const int p = precision ? 1 : 0;
+  if (sub) return g_tune.count(tune_key(p, 1, w, n)) != 0;
+  if (precision) return g_tune.count(tune_key(p, 3, w, n)) != 0;
+  return g_tune.count(tune_key(p, 0, w, n)) != 0 && g_tune.count(tune_key(p, 2, w, n)) != 0;
 }
 
 void icgn_autotune(bool on) {
@@ -1029,13 +1083,18 @@ void icgn_autotune(bool on) {
   if (!on) g_tune.clear();
 }
 
-int icgn_tuned_shape(int precision, bool sub, int w, long long n, int *nwarps, int *minb,
+int icgn_tuned_shape(int precision, int instance, int w, long long n, int *nwarps, int *minb,
                      float ms[8], int *count) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tune.find(tune_key(precision ? 1 : 0, sub, w, n));
+  const int p = precision ? 1 : 0;
+  auto it = g_tune.find(tune_key(p, instance, w, n));
+  if (it == g_tune.end() && instance == 0) it = g_tune.find(tune_key(p, 3, w, n));
   if (it == g_tune.end()) return E_STATE;
-  const auto &sv = precision ? (sub ? shapes<double, true>() : shapes<double, false>())
-                             : (sub ? shapes<float, true>() : shapes<float, false>());
+  // every mode's shape table has the same (warps, CTAs) entries
+  const auto &sv = precision ? (instance == 1 ? shapes<double, true, MODE_FULL>()
+                                              : shapes<double, false, MODE_FULL>())
+                             : (instance == 1 ? shapes<float, true, MODE_FULL>()
+                                              : shapes<float, false, MODE_FULL>());
   const Shape &sh = sv[it->second.shape];
   if (nwarps) *nwarps = sh.nw;
   if (minb) *minb = sh.minb;
@@ -1055,7 +1114,7 @@ int subpb1(const IcgnImages &im, const double *coords, long long n, const double
   a.im = im; a.coords = coords; a.n = n; a.U0 = UOld; a.FOld = FOld; a.vdual = vdual;
   a.H21in = H21; a.wins = wins; a.w = w; a.mu = mu; a.tol = tol; a.U = U; a.iters = iters;
   a.queue = queue;
-  return precision ? launch<double, true>(a, st) : launch<float, true>(a, st);
+  return precision ? launch<double, true, MODE_FULL>(a, st) : launch<float, true, MODE_FULL>(a, st);
 }
 
 }  // namespace aldic

@@ -48,6 +48,10 @@ int int_search(const void *f_raw, const void *g_raw, int dtype, int W, int H, co
                double *pce, double *ppe, cudaStream_t st, SearchWork *sw = nullptr);
 
 // ---- k_icgn.cu
+// doubles per subset of the IC-GN setup record (the cache argument of icgn
+// and subpb1): [mean f, bf, S_f5, S_f6, S_5, S_6, w, status], then S_f0..3,
+// S_0..3, the Cholesky factor of H (21), 1 / diag (6), SPD flag
+constexpr int kIcgnCache = 44;
 struct IcgnImages {
   const float *f32, *g32, *gx32, *gy32;
   const float4 *gc;   // row-cubic coefficients of g (row_cubic): the FP32 sampler's
@@ -62,7 +66,9 @@ int icgn(const IcgnImages &im, const double *coords, long long n, const double *
 // launch-shape autotuner of the IC-GN / Subpb1 kernels (k_icgn.cu)
 bool icgn_tuned(int precision, bool sub, int w, long long n);
 void icgn_autotune(bool on);
-int icgn_tuned_shape(int precision, bool sub, int w, long long n, int *nwarps, int *minb,
+// instance 0 LocalICGN (its iteration launch when the setup runs apart), 1
+// Subpb1, 2 the LocalICGN setup launch
+int icgn_tuned_shape(int precision, int instance, int w, long long n, int *nwarps, int *minb,
                      float ms[8], int *count);
 int subpb1(const IcgnImages &im, const double *coords, long long n, const double *UOld,
            const double *FOld, const double *vdual, const double *H21, const int *wins, int w,
@@ -90,8 +96,8 @@ enum { FDM_FE = 0, FDM_FD = 1 };
 struct FdmBasis {
   int type = -1, M = 0, N = 0;
   double h = 0.0;
-  DevBuf buf;  // Vx (M x M), Vy (N x N), lx (M), ly (N)
-  double *Vx = nullptr, *Vy = nullptr, *lx = nullptr, *ly = nullptr;
+  DevBuf buf;  // Vx (M x M), Vy (N x N), lx (M), ly (N), split-K partials (kFdmPart M N)
+  double *Vx = nullptr, *Vy = nullptr, *lx = nullptr, *ly = nullptr, *part = nullptr;
   void release() {
     buf.release();
     type = -1;

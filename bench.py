@@ -174,7 +174,7 @@ def icgn_bytes(iters: np.ndarray, winsize: int) -> float:
 
 
 ICGN_SOURCES = ("2d_aldic_b200/csrc/k_icgn.cu", "2d_aldic_b200/csrc/kernels.cuh",
-                "2d_aldic_b200/csrc/aldic_internal.cuh")
+                "2d_aldic_b200/csrc/aldic_internal.cuh", "2d_aldic_b200/csrc/k_image.cu")
 
 
 def icgn_source_digest() -> str:
@@ -190,8 +190,9 @@ def icgn_source_digest() -> str:
 
 
 def icgn_traffic_from_profile():
-    """DRAM bytes (read + write) of one IC-GN launch from the committed ncu
-    summary of this workload (profiles/k_icgn_uniform2048.md) when the
+    """DRAM bytes (read + write) of one LocalICGN (its setup and iteration
+    launches) from the committed ncu summary of this workload
+    (profiles/k_icgn_uniform2048.md) when the
     summary's "source digest" line matches the kernel sources being run;
     otherwise None (the traffic of this build is unmeasured)."""
     import re
@@ -202,17 +203,19 @@ def icgn_traffic_from_profile():
     m = re.search(r"source digest: `([0-9a-f]+)`", text)
     if not m or m.group(1) != icgn_source_digest():
         return None
-    sec = text.split("#### `k_icgn<float, 0>`", 1)
-    if len(sec) < 2:
+    # LocalICGN is its setup launch plus its iteration launch: one section each
+    parts = text.split("#### `k_icgn<float, 0")[1:]
+    if not parts:
         return None
-    sec = sec[1].split("####", 1)[0]
     tot = 0.0
-    for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
-        m = re.search(r"`" + re.escape(key) + r"` \| ([0-9.]+) (\w+)", sec)
-        if not m:
-            return None
-        scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}.get(m.group(2), 1)
-        tot += float(m.group(1)) * scale
+    for sec in parts:
+        sec = sec.split("####", 1)[0]
+        for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            m = re.search(r"`" + re.escape(key) + r"` \| ([0-9.]+) (\w+)", sec)
+            if not m:
+                return None
+            scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}.get(m.group(2), 1)
+            tot += float(m.group(1)) * scale
     return tot
 
 
@@ -273,12 +276,12 @@ def north_star_block(aldic, synth, dev, with_oracle, steps=5, warmup=2):
 
 def icgn_shapes(aldic, winsize, n):
     """Launch shapes the IC-GN autotuner chose (warps per CTA x resident CTAs
-    per SM in the launch bounds) for LocalICGN and Subpb1, with the trial
-    time of each candidate."""
+    per SM in the launch bounds) for LocalICGN (its setup and iteration
+    launches) and Subpb1, with the trial time of each candidate."""
     import ctypes as C
     lib = aldic._lib.lib()
     out = {}
-    for name, sub in (("local_icgn", 0), ("subpb1", 1)):
+    for name, sub in (("local_icgn_setup", 2), ("local_icgn", 0), ("subpb1", 1)):
         nw, mb, cnt = C.c_int(), C.c_int(), C.c_int()
         ms = (C.c_float * 8)()
         if lib.aldic_icgn_shape(0, sub, winsize, C.c_longlong(n), C.byref(nw), C.byref(mb), ms,

@@ -523,10 +523,13 @@ typedef struct {
  * frame before its first capture of a geometry for that.  enable = 0 turns
  * the trials off (and forgets the choices): the default shape is used. */
 ALDIC_API int aldic_icgn_autotune(int enable);
-/* The shape chosen for (precision, subpb1 0/1, winsize -- -1 for per-subset
+/* The shape chosen for (precision, instance, winsize -- -1 for per-subset
  * sizes --, n subsets): warps per CTA, resident CTAs per SM in the launch
  * bounds, and the trial time of each candidate shape (ms[count], count <= 8).
- * ALDIC_E_STATE if that geometry has not been tuned. */
+ * instance (the argument named subpb1): 0 LocalICGN -- in an FP32 frame its
+ * iteration launch, which follows a separate setup launch --, 1 Subpb1, 2
+ * that LocalICGN setup launch.  ALDIC_E_STATE if that geometry has not been
+ * tuned. */
 ALDIC_API int aldic_icgn_shape(int precision, int subpb1, int winsize, long long n, int *nwarps,
                                int *minb, float *ms, int *count);
 
