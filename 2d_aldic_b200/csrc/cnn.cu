@@ -203,6 +203,19 @@ __global__ void k_splitk_sum(const float *__restrict__ part, int splits, long lo
   }
 }
 
+// the split-K partials of a forward layer summed in split order, + bias,
+// ReLU, rounded to bf16 (the epilogue the unsplit product applies)
+__global__ void k_splitk_relu(const float *__restrict__ part, int splits, long long n, int N,
+                              const float *__restrict__ bias, bf16 *__restrict__ out) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int z = 0; z < splits; ++z) s += part[(long long)z * n + k];
+    s += bias[k % N];
+    out[k] = __float2bfloat16_rn(s > 0.f ? s : 0.f);
+  }
+}
+
 // Adam (beta1 0.9, beta2 0.999, eps 1e-8) on an FP32 block; optional bf16 copy
 __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
                        float *__restrict__ v, long long n, float lr, float c1, float c2,
@@ -327,11 +340,21 @@ int forward(aldic_cnn *c, int B, cudaStream_t st) {
                       src(c->e2.as<bf16>() + b * fs, GEMM_ROW, cnn::CELLS, cnn::C2, cnn::C2, 0, 0, 0, 0, fs),
                       dc, 1, err, st, B)))
     return rc;
-  // L3
-  if ((rc = gemm_bf16(src(c->corr.p, GEMM_ROW, b, cnn::K3, cnn::K3),
-                      src(c->Wb(2), GEMM_ROW, cnn::F3, cnn::K3, cnn::K3),
-                      dst(c->y3.p, b, cnn::F3, cnn::F3, 0, c->Bv(2), 1), 1, err, st)))
-    return rc;
+  // L3: K = 4096 on only b / 128 row tiles -- split K eight ways into FP32
+  // partials, then sum, bias and ReLU in one pass
+  {
+    constexpr int kL3Split = 8;
+    const long long n3 = b * cnn::F3;
+    if ((rc = c->part.ensure(sizeof(float) * n3 * kL3Split))) return rc;
+    GemmDst d3 = dst(c->part.p, b, cnn::F3, cnn::F3, 1, nullptr, 0);
+    d3.split_stride = n3;
+    if ((rc = gemm_bf16(src(c->corr.p, GEMM_ROW, b, cnn::K3, cnn::K3),
+                        src(c->Wb(2), GEMM_ROW, cnn::F3, cnn::K3, cnn::K3), d3, kL3Split, err, st)))
+      return rc;
+    k_splitk_relu<<<nblk(n3), 256, 0, st>>>(c->part.as<float>(), kL3Split, n3, cnn::F3, c->Bv(2),
+                                            c->y3.as<bf16>());
+    ALDIC_CUDA(cudaGetLastError());
+  }
   k_fc5<<<nblk(b * cnn::NOUT), 256, 0, st>>>(c->y3.as<bf16>(), c->W(3), c->Bv(3), c->out.as<float>(), B);
   ALDIC_CUDA(cudaGetLastError());
   return OK;

@@ -1114,6 +1114,10 @@ int subpb1(const IcgnImages &im, const double *coords, long long n, const double
   a.im = im; a.coords = coords; a.n = n; a.U0 = UOld; a.FOld = FOld; a.vdual = vdual;
   a.H21in = H21; a.wins = wins; a.w = w; a.mu = mu; a.tol = tol; a.U = U; a.iters = iters;
   a.queue = queue;
+  // with the LocalICGN record the setup is skipped: the iteration-only
+  // instance, which carries no setup code (fewer registers)
+  if (cache)
+    return precision ? launch<double, true, MODE_ITER>(a, st) : launch<float, true, MODE_ITER>(a, st);
   return precision ? launch<double, true, MODE_FULL>(a, st) : launch<float, true, MODE_FULL>(a, st);
 }
 

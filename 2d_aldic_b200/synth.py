@@ -124,6 +124,7 @@ class Workload:
     dtype: type = np.uint8
     scale: float = 1.0
     hole: tuple | None = None      # (cx, cy, radius) of a circular hole
+    min_size: int = 2              # quadtree elementMinSize (elements refined to 2x this)
 
     def mask(self):
         """ImgRefMask (H, W): 1 on the specimen, 0 in the hole."""
@@ -218,6 +219,12 @@ WORKLOADS = {
     # 16 px grid, subset 32
     "plate2048": Workload("plate2048", 2048, 2048, 130_000, 2, 32, 16, 16, 2.0,
                           plate_hole(1024.0, 1024.0, 300.0), hole=(1024.0, 1024.0, 300.0)),
+    # the same plate with the element range of its specification: a 64 px
+    # grid (subset 64) refined toward the hole edge down to 8 px elements
+    # (elementMinSize 4), element-sized subsets of 16-64 px
+    "plate2048e": Workload("plate2048e", 2048, 2048, 130_000, 2, 64, 64, 16, 2.0,
+                           plate_hole(1024.0, 1024.0, 300.0), hole=(1024.0, 1024.0, 300.0),
+                           min_size=4),
     # displacements larger than the subset (up to 46 px): the multigrid
     # search (funIntegerSearchMg) initialises the frame; subset 32, step 16;
     # search 48 is the whole-field search radius that would cover the field

@@ -383,7 +383,7 @@ def quadtree_main(args, rank, world, local):
     ctx = aldic.Context(local)
     ctx.set_stream(stream)
     qt = aldic.ALDICQuadtree(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=wl.n_admm,
-                             subsets="element", ctx=ctx)
+                             min_size=wl.min_size, subsets="element", ctx=ctx)
     qt.set_images(f, g, mask)
     for _ in range(max(1, args.warmup)):
         r = qt.frame()
@@ -419,7 +419,11 @@ def quadtree_main(args, rank, world, local):
             "config": {"workload": f"{wl.name}: {wl.W}x{wl.H} u8 speckle (seed {wl.seed}), hole "
                                    f"r={wl.hole[2]:.0f} at ({wl.hole[0]:.0f},{wl.hole[1]:.0f}), "
                                    f"plate-with-hole field, noise {wl.noise}; quadtree from a "
-                                   f"{wl.step} px grid, element-sized subsets",
+                                   f"{wl.step} px grid (subset {wl.winsize}), elementMinSize "
+                                   f"{wl.min_size}, element-sized subsets",
+                       "element_sizes": {int(k): int(v) for k, v in zip(*np.unique(
+                           np.abs(c[r["elems"][:, 2] - 1, 0] - c[r["elems"][:, 0] - 1, 0]),
+                           return_counts=True))},
                        "nodes": len(c), "elements": int(len(r["elems"])),
                        "subset_sizes": {int(k): int(v) for k, v in zip(sizes, counts)},
                        "admm_steps": len(r["update_y"]), "beta": r["beta"],

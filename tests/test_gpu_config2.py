@@ -80,3 +80,28 @@ def test_config2_icgn_all_converged_subsets(aldic, oracle, c2, prec):
         ctx.close()
     Uo, Fo, ito, _ = oracle.icgn_batch(fn, gn, dx, dy, coords, U0, wl.winsize, wl.tol)
     check_icgn_converged(U, F, it, Uo, Fo, ito, prec, "uniform2048")
+
+
+def test_config2_split_icgn_equals_one_launch(aldic, c2):
+    """The FP32 frame runs LocalICGN as a setup launch and an iteration launch
+    that share a per-subset record (k_icgn.cu MODE_SETUP / MODE_ITER); the
+    C ABI's aldic_icgn runs it in one launch.  Same arithmetic, so the same
+    status and iteration count on every subset of the headline frame."""
+    wl, f, g, _ = c2
+    H, W = f.shape
+    al = aldic.ALDIC(wl.winsize, wl.step, wl.search, tol=wl.tol, n_admm=0, precision=aldic.FP32)
+    al.set_images(f, g)
+    r = al.frame()
+    xs, ys, us, vs, _ = aldic.funIntegerSearch(f, g, wl.search, [1, W], [1, H], wl.winsize, wl.step,
+                                               0, qfactors=False)
+    coords = np.stack([xs.ravel(), ys.ravel()], 1)
+    U0 = np.empty(2 * xs.size)
+    U0[0::2], U0[1::2] = us.ravel(), vs.ravel()
+    ctx = aldic.Context(0)
+    try:
+        ctx.set_ref(f)
+        ctx.set_def(g)
+        _, _, it, _ = aldic.local_icgn(ctx, coords, U0, wl.winsize, wl.tol, aldic.FP32)
+    finally:
+        ctx.close()
+    np.testing.assert_array_equal(np.asarray(r["iters"]).ravel(), it)
