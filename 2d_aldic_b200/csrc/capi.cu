@@ -830,12 +830,6 @@ int aldic_subpb1(aldic_ctx *c, const double *coords, int64_t n, const double *UO
 }
 
 // ---------------------------------------------------------------- grid ops
-static int do_inpaint(aldic_ctx *c, int M, int N, int nf, double *vals, int stride,
-                      const unsigned char *bad, int f0, bool solve) {
-  int rc = inpaint_load(c->gw, M, N, nf, vals, stride, bad, c->stream, f0);
-  if (rc || !solve) return rc;
-  return OK;
-}
 
 int aldic_localicgn_post(aldic_ctx *c, int M, int N, const int32_t *iters, double *U, double *F,
                          int *bad_num) {
@@ -854,12 +848,10 @@ int aldic_localicgn_post(aldic_ctx *c, int M, int N, const int32_t *iters, doubl
   ALDIC_CHECK(bad && dnum, E_NOMEM, "staging buffer allocation failed");
   if ((rc = icgn_flags(M, N, (const int *)ai.dev, bad, dnum, (double *)(dnum + 2), dnum + 4, c->stream)))
     return rc;
-  if ((rc = do_inpaint(c, M, N, 2, au.dev, 2, bad, 0, false))) return rc;
-  if ((rc = do_inpaint(c, M, N, 4, af.dev, 4, bad, 2, false))) return rc;
-  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 6, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, c->stream)))
+  // the refill of the flagged subsets' U and F (LocalICGN.m:128-150), as the frame runs it
+  if ((rc = inpaint_cta(c->gw, M, N, au.dev, 2, 2, af.dev, 4, 4, bad, kRtolInpaint, kMaxitInpaint,
+                        c->stream)))
     return rc;
-  if ((rc = inpaint_store(c->gw, M, N, 2, au.dev, 2, c->stream, 0))) return rc;
-  if ((rc = inpaint_store(c->gw, M, N, 4, af.dev, 4, c->stream, 2))) return rc;
   arg_back(c, au); arg_back(c, af);
   int hb = 0;
   ALDIC_CUDA(cudaMemcpyAsync(&hb, dnum, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1490,11 +1482,10 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     return rc;
   if ((rc = mark(c, 3))) return rc;
   if ((rc = icgn_flags(M, N, B.it1, B.bad, B.ints, B.meanit, B.ints + 1, st))) return rc;
-  if ((rc = inpaint_load(c->gw, M, N, 2, B.U1, 2, B.bad, st, 0))) return rc;
-  if ((rc = inpaint_load(c->gw, M, N, 4, B.F1, 4, B.bad, st, 2))) return rc;
-  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 6, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st))) return rc;
-  if ((rc = inpaint_store(c->gw, M, N, 2, B.U1, 2, st, 0))) return rc;
-  if ((rc = inpaint_store(c->gw, M, N, 4, B.F1, 4, st, 2))) return rc;
+  // LocalICGN.m:128-150: the flagged subsets' U and F refilled by
+  // inpaint_nans(., 4) -- one CTA over the flagged nodes only
+  if ((rc = inpaint_cta(c->gw, M, N, B.U1, 2, 2, B.F1, 4, 4, B.bad, kRtolInpaint, kMaxitInpaint, st)))
+    return rc;
   // Section 5
   if ((rc = mark(c, 4))) return rc;
   if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F1))) return rc;

@@ -557,6 +557,265 @@ __device__ __forceinline__ void search_point_u8(const uint8_t *__restrict__ f,
   peak_epilogue(map, G, ii, jj, out_idx, redv, redi, ox, oy, ou, ov, occ);
 }
 
+// ---- 16-bit images: the same strips with __dp2a (16-bit x 8-bit, exact).
+// The padded region is staged as two byte planes (high and low bytes of each
+// pixel) in the word layout of the 8-bit path, the template as 16-bit pairs;
+// with g = 256 gh + gl, sum t g = 256 sum t gh + sum t gl, and __dp2a_lo /
+// __dp2a_hi take the pixel pair at bytes 0-1 / 2-3 of a plane word, so the
+// words at byte offsets 2j, 2j+1, 2j+4, 2j+5 from a strip's first shift give
+// all 8 shifts of template pair j.  Per template row the two 32-bit partial
+// sums (at most 17 pairs of products below 2^25) are folded into a 64-bit
+// total.
+struct U16Layout {
+  int tw4, tp, dqw;  // 4-pixel template groups per row, pair words per row, plane words per row
+  size_t tb, dh, dl, tq, rs, rs2, cs, cs2, map, red, total;
+  __host__ __device__ U16Layout(const SearchGeom &g) {
+    tw4 = (g.tw + 3) / 4;
+    tp = 2 * tw4;
+    int need = 2 * g.nsx + tw4 + 2;
+    const int nb = (g.cr + g.tw + 3) / 4 + 1;
+    if (need < nb) need = nb;
+    dqw = need | 1;
+    size_t o = 0;
+    tb = o; o = align16(o + sizeof(uint16_t) * g.tw * g.tw);
+    dh = o; o = align16(o + sizeof(unsigned) * g.dph * dqw);
+    dl = o; o = align16(o + sizeof(unsigned) * g.dph * dqw);
+    tq = o; o = align16(o + sizeof(unsigned) * g.tw * tp);
+    // window row sums (dead once the box sums are formed: the map reuses them)
+    rs = o;
+    const size_t rsz = (sizeof(int) + sizeof(long long)) * g.dph * g.cr + 16,
+                 msz = sizeof(double) * g.cr * g.cc;
+    rs2 = align16(rs + sizeof(int) * g.dph * g.cr);
+    o = align16(o + (rsz > msz ? rsz : msz));
+    map = rs;
+    cs = o; o = align16(o + sizeof(int) * g.cc * g.cr);
+    cs2 = o; o = align16(o + sizeof(long long) * g.cc * g.cr);
+    red = o; o = align16(o + (sizeof(double) + sizeof(int)) * 32 + 64);
+    total = o;
+  }
+};
+
+__device__ __forceinline__ void search_point_u16(const uint16_t *__restrict__ f,
+                                                 const uint16_t *__restrict__ g,
+                                                 const SearchGeom &G, const int pt,
+                                                 double *__restrict__ ox, double *__restrict__ oy,
+                                                 double *__restrict__ ou, double *__restrict__ ov,
+                                                 double *__restrict__ occ) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const U16Layout L(G);
+  uint16_t *Tb = (uint16_t *)(smem + L.tb);   // template, tw x tw
+  unsigned *Dh = (unsigned *)(smem + L.dh);   // padded region, high bytes, dph rows of dqw words
+  unsigned *Dl = (unsigned *)(smem + L.dl);   // low bytes
+  unsigned *Tq = (unsigned *)(smem + L.tq);   // template pairs, tp words per row
+  int *RS = (int *)(smem + L.rs);
+  long long *RS2 = (long long *)(smem + L.rs2);
+  int *CS = (int *)(smem + L.cs);
+  long long *CS2 = (long long *)(smem + L.cs2);
+  double *map = (double *)(smem + L.map);
+  double *redv = (double *)(smem + L.red);
+  int *redi = (int *)(redv + 32);
+  __shared__ long long s_st, s_st2;
+  __shared__ int colsum_s[72], rowsum_s[72];
+  const double mu = *G.mu;
+  const int ix = pt % G.nx, iy = pt / G.nx;
+  const int ii = G.gx1 + ix * G.step, jj = G.gy1 + iy * G.step;  // 1-based
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5, nwarp = nth >> 5;
+  const uint16_t *trow0 = f + (long long)(jj - 1) * G.W + (ii - 1);
+  const uint16_t *drow0 = g + (long long)(jj - 1 - G.sy) * G.W + (ii - 1 - G.sx);
+  // ---- stage the template and the region's byte planes (1-pixel zero
+  // border at the top/left, zeros beyond the region)
+  for (int ty = wid; ty < G.tw; ty += nwarp)
+    for (int tx = lane; tx < G.tw; tx += 32) Tb[ty * G.tw + tx] = trow0[(long long)ty * G.W + tx];
+  for (int y = wid; y < G.dph; y += nwarp) {
+    const bool rin = y >= 1 && y <= G.dh;
+    const uint16_t *src = drow0 + (long long)(y - 1) * G.W;
+    for (int w4 = lane; w4 < L.dqw; w4 += 32) {
+      unsigned vh = 0, vl = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int x = 4 * w4 + k;
+        if (rin && x >= 1 && x <= G.dw) {
+          const unsigned v = src[x - 1];
+          vh |= (v >> 8) << (8 * k);
+          vl |= (v & 0xFFu) << (8 * k);
+        }
+      }
+      Dh[y * L.dqw + w4] = vh;
+      Dl[y * L.dqw + w4] = vl;
+    }
+  }
+  __syncthreads();
+  // ---- template pair words, window row sums, template sums
+  for (int ty = wid; ty < G.tw; ty += nwarp)
+    for (int w = lane; w < L.tp; w += 32) {
+      const int tx = 2 * w;
+      const unsigned a = tx < G.tw ? Tb[ty * G.tw + tx] : 0u;
+      const unsigned b = tx + 1 < G.tw ? Tb[ty * G.tw + tx + 1] : 0u;
+      Tq[ty * L.tp + w] = a | (b << 16);
+    }
+  for (int y = tid; y < G.dph; y += nth) {
+    const uint8_t *rh = (const uint8_t *)(Dh + y * L.dqw), *rl = (const uint8_t *)(Dl + y * L.dqw);
+    int s1 = 0;
+    long long s2 = 0;
+    for (int k = 0; k < G.tw; ++k) {
+      const long long v = 256 * rh[k] + rl[k];
+      s1 += (int)v;
+      s2 += v * v;
+    }
+    for (int a = 0; a < G.cr; ++a) {
+      RS[y * G.cr + a] = s1;
+      RS2[y * G.cr + a] = s2;
+      const long long vo = 256 * rh[a] + rl[a], vi = 256 * rh[a + G.tw] + rl[a + G.tw];
+      s1 += (int)(vi - vo);
+      s2 += vi * vi - vo * vo;
+    }
+  }
+  for (int i = tid; i < G.tw; i += nth) {
+    int cs = 0, rsum = 0;
+    for (int k = 0; k < G.tw; ++k) {
+      cs += Tb[k * G.tw + i];
+      rsum += Tb[i * G.tw + k];
+    }
+    colsum_s[i] = cs;
+    rowsum_s[i] = rsum;
+  }
+  if (tid < 32) {
+    long long a = 0, a2 = 0;
+    for (int i = tid; i < G.tw * G.tw; i += 32) {
+      const long long v = Tb[i];
+      a += v;
+      a2 += v * v;
+    }
+    a = warp_sum_ll(a);
+    a2 = warp_sum_ll(a2);
+    if (tid == 0) {
+      s_st = a;
+      s_st2 = a2;
+    }
+  }
+  __syncthreads();
+  // ---- box sums of D and D^2 over every window: slide the row sums down
+  for (int a = tid; a < 2 * G.cr; a += nth) {
+    const int col = a < G.cr ? a : a - G.cr;
+    if (a < G.cr) {
+      int s1 = 0;
+      for (int k = 0; k < G.tw; ++k) s1 += RS[k * G.cr + col];
+      for (int b = 0; b < G.cc; ++b) {
+        CS[b * G.cr + col] = s1;
+        s1 += RS[(b + G.tw) * G.cr + col] - RS[b * G.cr + col];
+      }
+    } else {
+      long long s2 = 0;
+      for (int k = 0; k < G.tw; ++k) s2 += RS2[k * G.cr + col];
+      for (int b = 0; b < G.cc; ++b) {
+        CS2[b * G.cr + col] = s2;
+        s2 += RS2[(b + G.tw) * G.cr + col] - RS2[b * G.cr + col];
+      }
+    }
+  }
+  __syncthreads();  // RS is dead from here on; the map takes its place
+  const long long st = s_st, st2 = s_st2;
+  const long long mn = (long long)G.tw * G.tw;
+  const long long out_idx = (long long)iy + (long long)ix * G.ny;
+  if (mn * st2 - st * st == 0) {
+    if (tid == 0) {
+      const double nan = __longlong_as_double(0x7ff8000000000000ll);
+      ox[out_idx] = (ii + ii + G.w) / 2.0;
+      oy[out_idx] = (jj + jj + G.w) / 2.0;
+      ou[out_idx] = nan;
+      ov[out_idx] = nan;
+      occ[out_idx] = nan;
+    }
+    return;
+  }
+  // ---- correlation strips: 8 shifts of one window row per thread
+  const int nstrips = G.cc * G.nsx;
+  for (int sidx = tid; sidx < nstrips; sidx += nth) {
+    const int b = sidx / G.nsx;
+    const int a0 = (sidx % G.nsx) * KX;  // multiple of 8
+    unsigned long long acc[KX];
+#pragma unroll
+    for (int k = 0; k < KX; ++k) acc[k] = 0ull;
+    const int wbase = a0 >> 2;
+    for (int ty = 0; ty < G.tw; ++ty) {
+      const unsigned *trow = Tq + ty * L.tp;
+      const unsigned *dh = Dh + (b + ty) * L.dqw + wbase, *dl = Dl + (b + ty) * L.dqw + wbase;
+      unsigned ah[KX], al[KX];
+#pragma unroll
+      for (int k = 0; k < KX; ++k) ah[k] = al[k] = 0u;
+      // words w0, w1 of each plane and their 1-byte shift, carried along
+      unsigned h0 = dh[0], h1 = dh[1], l0 = dl[0], l1 = dl[1];
+      unsigned hs = __funnelshift_r(h0, h1, 8), ls = __funnelshift_r(l0, l1, 8);
+#pragma unroll 2
+      for (int m = 0; m < L.tw4; ++m) {
+        const unsigned te = trow[2 * m], to = trow[2 * m + 1];  // template pairs 2m, 2m+1
+        const unsigned h2 = dh[m + 2], l2 = dl[m + 2];
+        const unsigned hn = __funnelshift_r(h1, h2, 8), ln = __funnelshift_r(l1, l2, 8);
+        const unsigned h16 = __funnelshift_r(h0, h1, 16), h24 = __funnelshift_r(h0, h1, 24);
+        const unsigned l16 = __funnelshift_r(l0, l1, 16), l24 = __funnelshift_r(l0, l1, 24);
+        const unsigned h16n = __funnelshift_r(h1, h2, 16), h24n = __funnelshift_r(h1, h2, 24);
+        const unsigned l16n = __funnelshift_r(l1, l2, 16), l24n = __funnelshift_r(l1, l2, 24);
+        // pair 2m: byte offsets 4m + k; words at 4m (h0), 4m+1 (hs), 4m+4 (h1), 4m+5 (hn)
+        ah[0] = __dp2a_lo(te, h0, ah[0]);  al[0] = __dp2a_lo(te, l0, al[0]);
+        ah[2] = __dp2a_hi(te, h0, ah[2]);  al[2] = __dp2a_hi(te, l0, al[2]);
+        ah[1] = __dp2a_lo(te, hs, ah[1]);  al[1] = __dp2a_lo(te, ls, al[1]);
+        ah[3] = __dp2a_hi(te, hs, ah[3]);  al[3] = __dp2a_hi(te, ls, al[3]);
+        ah[4] = __dp2a_lo(te, h1, ah[4]);  al[4] = __dp2a_lo(te, l1, al[4]);
+        ah[6] = __dp2a_hi(te, h1, ah[6]);  al[6] = __dp2a_hi(te, l1, al[6]);
+        ah[5] = __dp2a_lo(te, hn, ah[5]);  al[5] = __dp2a_lo(te, ln, al[5]);
+        ah[7] = __dp2a_hi(te, hn, ah[7]);  al[7] = __dp2a_hi(te, ln, al[7]);
+        // pair 2m+1: byte offsets 4m + 2 + k; words at 4m+2, 4m+3, 4m+6, 4m+7
+        ah[0] = __dp2a_lo(to, h16, ah[0]);  al[0] = __dp2a_lo(to, l16, al[0]);
+        ah[2] = __dp2a_hi(to, h16, ah[2]);  al[2] = __dp2a_hi(to, l16, al[2]);
+        ah[1] = __dp2a_lo(to, h24, ah[1]);  al[1] = __dp2a_lo(to, l24, al[1]);
+        ah[3] = __dp2a_hi(to, h24, ah[3]);  al[3] = __dp2a_hi(to, l24, al[3]);
+        ah[4] = __dp2a_lo(to, h16n, ah[4]);  al[4] = __dp2a_lo(to, l16n, al[4]);
+        ah[6] = __dp2a_hi(to, h16n, ah[6]);  al[6] = __dp2a_hi(to, l16n, al[6]);
+        ah[5] = __dp2a_lo(to, h24n, ah[5]);  al[5] = __dp2a_lo(to, l24n, al[5]);
+        ah[7] = __dp2a_hi(to, h24n, ah[7]);  al[7] = __dp2a_hi(to, l24n, al[7]);
+        h0 = h1; h1 = h2; l0 = l1; l1 = l2; hs = hn; ls = ln;
+      }
+#pragma unroll
+      for (int k = 0; k < KX; ++k) acc[k] += ((unsigned long long)ah[k] << 8) + al[k];
+    }
+    const bool ring_b = (b == 0 || b == G.cc - 1);
+#pragma unroll
+    for (int k = 0; k < KX; ++k) {
+      const int a = a0 + k;
+      if (a >= G.cr) break;
+      const long long sd = CS[b * G.cr + a], sd2 = CS2[b * G.cr + a];
+      int st_out = 0;
+      long long n_out = 0;
+      if (ring_b || a == 0 || a == G.cr - 1) {
+        const int oc = a == 0 ? 0 : (a == G.cr - 1 ? G.tw - 1 : -1);
+        const int orow = b == 0 ? 0 : (b == G.cc - 1 ? G.tw - 1 : -1);
+        if (oc >= 0) st_out += colsum_s[oc];
+        if (orow >= 0) st_out += rowsum_s[orow];
+        if (oc >= 0 && orow >= 0) st_out -= Tb[orow * G.tw + oc];
+        const long long nco = oc >= 0, nro = orow >= 0;
+        n_out = nco * G.tw + nro * G.tw - nco * nro;
+      }
+      map[b * G.cr + a] = ncc_combine(mn, st, st2, (long long)acc[k], sd, sd2, st_out, n_out, mu);
+    }
+  }
+  __syncthreads();
+  peak_epilogue(map, G, ii, jj, out_idx, redv, redi, ox, oy, ou, ov, occ);
+}
+
+__global__ void __launch_bounds__(512) k_search_u16(const uint16_t *__restrict__ f,
+                                                    const uint16_t *__restrict__ g, SearchGeom G,
+                                                    double *__restrict__ ox,
+                                                    double *__restrict__ oy,
+                                                    double *__restrict__ ou,
+                                                    double *__restrict__ ov,
+                                                    double *__restrict__ occ) {
+  for (int pt = blockIdx.x; pt < G.nx * G.ny; pt += gridDim.x) {
+    search_point_u16(f, g, G, pt, ox, oy, ou, ov, occ);
+    __syncthreads();  // the next point restages shared memory
+  }
+}
+
 __global__ void __launch_bounds__(512) k_search_u8(const uint8_t *__restrict__ f,
                                                    const uint8_t *__restrict__ g, SearchGeom G,
                                                    double *__restrict__ ox,
@@ -1631,6 +1890,12 @@ int launch_search(const void *f, const void *g, const SearchGeom &G, double *x, 
     if (!tiled)
       k_search_u8<<<npts, threads, L.total, st>>>((const uint8_t *)f, (const uint8_t *)g, G, x,
                                                    y, u, v, cc);
+  } else if (sizeof(T) == 2 && U16Layout(G).total <= kSmemMax && G.tw <= 72) {
+    const U16Layout L(G);
+    ALDIC_CUDA(cudaFuncSetAttribute(k_search_u16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)L.total));
+    k_search_u16<<<npts, threads, L.total, st>>>((const uint16_t *)f, (const uint16_t *)g, G, x, y,
+                                                  u, v, cc);
   } else {
     SmemLayout<V, S> L(G);
     if (L.total > kSmemMax) {
@@ -1694,7 +1959,8 @@ size_t big_bytes(const SearchGeom &G) {
   using Tr = SearchTraits<T>;
   using S = typename SumT<Tr::integer>::type;
   const bool small = sizeof(T) == 1 ? (U8Layout(G).total <= kSmemMax && G.tw <= 72)
-                                    : SmemLayout<typename Tr::V, S>(G).total <= kSmemMax;
+                                    : ((sizeof(T) == 2 && U16Layout(G).total <= kSmemMax && G.tw <= 72) ||
+                                       SmemLayout<typename Tr::V, S>(G).total <= kSmemMax);
   if (small) return 0;
   const int npts = G.nx * G.ny;
   return SmemLayout<typename Tr::V, S>(G, true).slot * (size_t)(npts < kBigBlocks ? npts : kBigBlocks);

@@ -112,6 +112,26 @@ def test_int_search_large_region_bit_exact(aldic, oracle, plain, scale):
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("search", [20, 24])
+def test_int_search_16bit_full_range_bit_exact(aldic, oracle, plain, search):
+    """Genuinely 16-bit images (every bit of both bytes in use: the 8-bit
+    speckle times 256 plus independent low-byte noise), for the 16-bit
+    kernel's high/low byte-plane products: u, v and cc.max bit-exact."""
+    rng = np.random.default_rng(16)
+    f8, g8 = plain["f"], plain["g"]
+    f = (f8.astype(np.uint32) * 256 + rng.integers(0, 256, f8.shape)).astype(np.uint16)
+    g = (g8.astype(np.uint32) * 256 + rng.integers(0, 256, g8.shape)).astype(np.uint16)
+    H, W = f.shape
+    for w, step in ((20, 10), (32, 16)):
+        x, y, u, v, cc = aldic.funIntegerSearch(f, g, search, [1, W], [1, H], w, step, 0,
+                                                qfactors=False)
+        mg = g.astype(np.float64).mean()
+        xo, yo, uo, vo, co, _ = oracle.int_search(f, g, mg, [1, W], [1, H], w, step,
+                                                  [search, search])
+        for a, b in ((x, xo), (y, yo), (u, uo), (v, vo), (cc["max"], co)):
+            np.testing.assert_array_equal(a, b)
+
+
 def test_int_search_qfactors_and_edges(aldic, oracle, synth):
     W = H = 160
     f = synth.speckle(W, H, 800, 21)
