@@ -91,6 +91,7 @@ struct aldic_ctx {
     double *U0 = nullptr, *U1 = nullptr, *F1 = nullptr, *U2 = nullptr, *F2 = nullptr;
     double *ud = nullptr, *vd = nullptr, *U2old = nullptr, *U1old = nullptr, *H21 = nullptr;
     double *norms = nullptr, *Uicgn = nullptr;
+    double *cache = nullptr;  // IC-GN setup records (kIcgnCache a node), read by Subpb1
     int *it1 = nullptr, *itb = nullptr, *ints = nullptr;
     unsigned char *bad = nullptr;
   } qtf;
@@ -848,10 +849,12 @@ int aldic_localicgn_post(aldic_ctx *c, int M, int N, const int32_t *iters, doubl
   ALDIC_CHECK(bad && dnum, E_NOMEM, "staging buffer allocation failed");
   if ((rc = icgn_flags(M, N, (const int *)ai.dev, bad, dnum, (double *)(dnum + 2), dnum + 4, c->stream)))
     return rc;
-  // the refill of the flagged subsets' U and F (LocalICGN.m:128-150), as the frame runs it
-  if ((rc = inpaint_cta(c->gw, M, N, au.dev, 2, 2, af.dev, 4, 4, bad, kRtolInpaint, kMaxitInpaint,
-                        c->stream)))
+  if ((rc = inpaint_load(c->gw, M, N, 2, au.dev, 2, bad, c->stream, 0))) return rc;
+  if ((rc = inpaint_load(c->gw, M, N, 4, af.dev, 4, bad, c->stream, 2))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 6, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, c->stream)))
     return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 2, au.dev, 2, c->stream, 0))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 4, af.dev, 4, c->stream, 2))) return rc;
   arg_back(c, au); arg_back(c, af);
   int hb = 0;
   ALDIC_CUDA(cudaMemcpyAsync(&hb, dnum, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1482,10 +1485,11 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     return rc;
   if ((rc = mark(c, 3))) return rc;
   if ((rc = icgn_flags(M, N, B.it1, B.bad, B.ints, B.meanit, B.ints + 1, st))) return rc;
-  // LocalICGN.m:128-150: the flagged subsets' U and F refilled by
-  // inpaint_nans(., 4) -- one CTA over the flagged nodes only
-  if ((rc = inpaint_cta(c->gw, M, N, B.U1, 2, 2, B.F1, 4, 4, B.bad, kRtolInpaint, kMaxitInpaint, st)))
-    return rc;
+  if ((rc = inpaint_load(c->gw, M, N, 2, B.U1, 2, B.bad, st, 0))) return rc;
+  if ((rc = inpaint_load(c->gw, M, N, 4, B.F1, 4, B.bad, st, 2))) return rc;
+  if ((rc = grid_pcg(c->gw, OP_INPAINT, M, N, 6, 0, 0, 1, 0, kRtolInpaint, kMaxitInpaint, st))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 2, B.U1, 2, st, 0))) return rc;
+  if ((rc = inpaint_store(c->gw, M, N, 4, B.F1, 4, st, 2))) return rc;
   // Section 5
   if ((rc = mark(c, 4))) return rc;
   if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F1))) return rc;
@@ -1772,6 +1776,7 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
       Q.U2 = q.take<double>(2 * n); Q.F2 = q.take<double>(4 * n); Q.ud = q.take<double>(4 * n);
       Q.vd = q.take<double>(2 * n); Q.U2old = q.take<double>(2 * n); Q.U1old = q.take<double>(2 * n);
       Q.H21 = q.take<double>(21 * n); Q.norms = q.take<double>(2048); Q.Uicgn = q.take<double>(2 * n);
+      Q.cache = q.take<double>((long long)kIcgnCache * n);
       Q.it1 = q.take<int>(n); Q.itb = q.take<int>(n); Q.ints = q.take<int>(16);
       Q.bad = q.take<unsigned char>(n);
     };
@@ -1792,7 +1797,7 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
   const double *qcoords = m.d_coords.as<double>();
   const int *wins = Q.wins.as<int>();
   if ((rc = icgn(im, qcoords, n, Q.U0, wins, w, p->tol, p->precision, Q.U1, Q.F1, Q.it1, Q.H21,
-                 c->queue.as<unsigned int>(), st, nullptr)))
+                 c->queue.as<unsigned int>(), st, Q.cache)))
     return rc;
   double *mean = (double *)(Q.ints + 8);
   if ((rc = icgn_flags((int)n, 1, Q.it1, Q.bad, Q.ints, mean, Q.ints + 1, st))) return rc;
@@ -1838,7 +1843,7 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
   for (int a = 0; a < p->n_admm; ++a) {
     ALDIC_CUDA(cudaMemcpyAsync(Q.U2old, Q.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
     if ((rc = subpb1(im, qcoords, n, Q.U2, Q.F2, Q.vd, Q.H21, wins, w, mu, p->tol, p->precision, Q.U1,
-                     Q.itb, c->queue.as<unsigned int>(), st, nullptr)))
+                     Q.itb, c->queue.as<unsigned int>(), st, Q.cache)))
       return rc;
     if ((rc = icgn_flags((int)n, 1, Q.itb, Q.bad, Q.ints + 4, mean, Q.ints + 5, st, 20.0))) return rc;
     k_zero_bad<<<nb, 256, 0, st>>>(n, 2, Q.U1, Q.bad);

@@ -740,234 +740,6 @@ __global__ void k_inpaint_load(int M, int N, int nf, const double *__restrict__ 
   }
 }
 
-// ----------------------------------------------------- compact inpainting
-// inpaint_nans(., 4) of LocalICGN's flagged subsets (the same system as
-// OP_INPAINT: per field, an unknown node's row is deg x_k - sum of its
-// unknown in-grid neighbours = sum of its known neighbours' values) solved
-// by one 1024-thread CTA over the unknown nodes only.  The flagged subsets
-// are ~1 % of a frame's nodes in small clusters, so a grid-wide sweep and
-// grid barrier per iteration (the cooperative PCG) spends its time on
-// nodes that do not change; here one CTA compacts the unknown nodes once,
-// then runs Jacobi-preconditioned CG on them with block barriers only.
-// The stopping rule is the cooperative solver's: |r| <= rtol |b| per field,
-// b over every node (known values included), so the two agree to rounding.
-constexpr int kIpThreads = 1024;
-constexpr int kIpMaxF = 6;
-
-struct IpSrc {
-  double *vals[2];
-  int stride[2], nf[2];  // fields [0, nf0) from vals[0], [nf0, nf0 + nf1) from vals[1]
-};
-
-__device__ __forceinline__ double *ip_val(const IpSrc &S, long long k, int f) {
-  return f < S.nf[0] ? S.vals[0] + k * S.stride[0] + f
-                     : S.vals[1] + k * S.stride[1] + (f - S.nf[0]);
-}
-
-// block-wide sums of nv values (nv <= 2 kIpMaxF), result in out[0..nv)
-__device__ void ip_block_sums(double (&v)[2 * kIpMaxF], int nv, double *red, double *out) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int q = 0; q < nv; ++q) {
-    const double t = warp_sum(v[q]);
-    if (lane == 0) red[wid * 2 * kIpMaxF + q] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x < nv) {
-    double t = 0.0;
-    for (int w = 0; w < kIpThreads / 32; ++w) t += red[w * 2 * kIpMaxF + threadIdx.x];
-    out[threadIdx.x] = t;
-  }
-  __syncthreads();
-}
-
-__global__ void __launch_bounds__(kIpThreads, 1)
-    k_inpaint_cta(int M, int N, IpSrc S, const unsigned char *__restrict__ bad, int *cidx, int *nodes,
-                  int *nbc, double *X, double *R, double *Z, double *P, double *AP, double *DG,
-                  unsigned char *unk, double rtol, int maxit, int *err, int *iters_out) {
-  __shared__ double red[(kIpThreads / 32) * 2 * kIpMaxF];
-  __shared__ double sums[2 * kIpMaxF], bb[kIpMaxF], rz[kIpMaxF], alpha[kIpMaxF], beta[kIpMaxF];
-  __shared__ int done[kIpMaxF];
-  __shared__ int scan[kIpThreads];
-  __shared__ int total;
-  const long long n = (long long)M * N;
-  const int nf = S.nf[0] + S.nf[1];
-  const int t = threadIdx.x;
-  auto known = [&](long long k, int f) { return !(bad && bad[k]) && !isnan(*ip_val(S, k, f)); };
-  // ---- compaction: nodes unknown in any field, in node order
-  const long long chunk = (n + kIpThreads - 1) / kIpThreads;
-  const long long k0 = t * chunk, k1 = k0 + chunk < n ? k0 + chunk : n;
-  int cnt = 0;
-  double bpart[2 * kIpMaxF];
-  for (int f = 0; f < 2 * kIpMaxF; ++f) bpart[f] = 0.0;
-  for (long long k = k0; k < k1; ++k) {
-    bool any = false;
-    for (int f = 0; f < nf; ++f) {
-      if (known(k, f)) {
-        const double v = *ip_val(S, k, f);
-        bpart[f] += v * v;  // the known rows' part of |b|^2
-      } else {
-        any = true;
-      }
-    }
-    cnt += any;
-  }
-  scan[t] = cnt;
-  __syncthreads();
-  for (int o = 1; o < kIpThreads; o <<= 1) {  // inclusive scan
-    const int v = t >= o ? scan[t - o] : 0;
-    __syncthreads();
-    scan[t] += v;
-    __syncthreads();
-  }
-  int pos = scan[t] - cnt;
-  if (t == kIpThreads - 1) total = scan[t];
-  for (long long k = k0; k < k1; ++k) {
-    bool any = false;
-    for (int f = 0; f < nf; ++f) any |= !known(k, f);
-    if (any) {
-      nodes[pos] = (int)k;
-      cidx[k] = pos++;
-    } else {
-      cidx[k] = -1;
-    }
-  }
-  __syncthreads();
-  const int u = total;
-  // ---- rows: neighbours, degree, right-hand side, start (the mean of the
-  // known neighbours, as k_inpaint_load), residual
-  for (int i = t; i < u; i += kIpThreads) {
-    const long long k = nodes[i];
-    const int ii = (int)(k % M), jj = (int)(k / M);
-    const long long nb[4] = {ii > 0 ? k - 1 : -1, ii < M - 1 ? k + 1 : -1, jj > 0 ? k - M : -1,
-                             jj < N - 1 ? k + M : -1};
-    int deg = 0;
-    for (int q = 0; q < 4; ++q) {
-      nbc[4 * i + q] = nb[q] >= 0 ? cidx[nb[q]] : -1;
-      deg += nb[q] >= 0;
-    }
-    DG[i] = (double)deg;
-    for (int f = 0; f < nf; ++f) {
-      const long long o = (long long)f * u + i;
-      const bool kn = known(k, f);
-      unk[o] = !kn;
-      double bv = 0.0;
-      int kc = 0;
-      if (kn) {
-        bv = *ip_val(S, k, f);
-      } else {
-        for (int q = 0; q < 4; ++q)
-          if (nb[q] >= 0 && known(nb[q], f)) { bv += *ip_val(S, nb[q], f); ++kc; }
-        bpart[f] += bv * bv;
-      }
-      X[o] = kn ? bv : (kc > 0 ? bv / kc : 0.0);
-      R[o] = bv;  // b; the residual follows once every start is in place
-    }
-  }
-  ip_block_sums(bpart, nf, red, sums);
-  if (t < nf) {
-    bb[t] = sums[t];
-    done[t] = 0;
-  }
-  __syncthreads();
-  // r = b - A x0 on the unknown entries (0 on the known ones), z = r / deg, p = z
-  for (int i = t; i < u; i += kIpThreads)
-    for (int f = 0; f < nf; ++f) {
-      const long long o = (long long)f * u + i;
-      if (!unk[o]) {
-        R[o] = Z[o] = P[o] = 0.0;
-        continue;
-      }
-      double ax = DG[i] * X[o];
-      for (int q = 0; q < 4; ++q) {
-        const int c = nbc[4 * i + q];
-        if (c >= 0 && unk[(long long)f * u + c]) ax -= X[(long long)f * u + c];
-      }
-      const double r = R[o] - ax;
-      R[o] = r;
-      Z[o] = r / DG[i];
-      P[o] = Z[o];
-    }
-  __syncthreads();
-  double part[2 * kIpMaxF];
-  for (int q = 0; q < 2 * kIpMaxF; ++q) part[q] = 0.0;
-  for (int i = t; i < u; i += kIpThreads)
-    for (int f = 0; f < nf; ++f) {
-      const long long o = (long long)f * u + i;
-      part[f] += R[o] * Z[o];
-      part[kIpMaxF + f] += R[o] * R[o];
-    }
-  ip_block_sums(part, 2 * kIpMaxF, red, sums);
-  if (t < nf) {
-    rz[t] = sums[t];
-    if (sums[kIpMaxF + t] <= rtol * rtol * bb[t]) done[t] = 1;
-  }
-  __syncthreads();
-  int it = 0;
-  for (; it < maxit; ++it) {
-    bool all = true;
-    for (int f = 0; f < nf; ++f) all &= done[f] != 0;
-    if (all) break;
-    // Ap and p.Ap
-    for (int q = 0; q < 2 * kIpMaxF; ++q) part[q] = 0.0;
-    for (int i = t; i < u; i += kIpThreads)
-      for (int f = 0; f < nf; ++f) {
-        const long long o = (long long)f * u + i;
-        if (done[f] || !unk[o]) continue;
-        double ap = DG[i] * P[o];
-        for (int q = 0; q < 4; ++q) {
-          const int c = nbc[4 * i + q];
-          if (c >= 0 && unk[(long long)f * u + c]) ap -= P[(long long)f * u + c];
-        }
-        AP[o] = ap;
-        part[f] += P[o] * ap;
-      }
-    ip_block_sums(part, nf, red, sums);
-    if (t < nf) alpha[t] = (done[t] || !(sums[t] != 0.0)) ? 0.0 : rz[t] / sums[t];
-    __syncthreads();
-    for (int q = 0; q < 2 * kIpMaxF; ++q) part[q] = 0.0;
-    for (int i = t; i < u; i += kIpThreads)
-      for (int f = 0; f < nf; ++f) {
-        const long long o = (long long)f * u + i;
-        if (done[f] || !unk[o]) continue;
-        X[o] += alpha[f] * P[o];
-        const double r = R[o] - alpha[f] * AP[o];
-        R[o] = r;
-        const double z = r / DG[i];
-        Z[o] = z;
-        part[f] += r * z;
-        part[kIpMaxF + f] += r * r;
-      }
-    ip_block_sums(part, 2 * kIpMaxF, red, sums);
-    if (t < nf && !done[t]) {
-      beta[t] = rz[t] != 0.0 ? sums[t] / rz[t] : 0.0;
-      rz[t] = sums[t];
-      if (sums[kIpMaxF + t] <= rtol * rtol * bb[t]) done[t] = 1;
-    }
-    __syncthreads();
-    for (int i = t; i < u; i += kIpThreads)
-      for (int f = 0; f < nf; ++f) {
-        const long long o = (long long)f * u + i;
-        if (done[f] || !unk[o]) continue;
-        P[o] = Z[o] + beta[f] * P[o];
-      }
-    __syncthreads();
-  }
-  if (t == 0) {
-    bool all = true;
-    for (int f = 0; f < nf; ++f) all &= done[f] != 0;
-    if (!all) *err = 2;
-    if (iters_out) *iters_out = it > *iters_out ? it : *iters_out;
-  }
-  // ---- the solution into the unknown entries
-  for (int i = t; i < u; i += kIpThreads) {
-    const long long k = nodes[i];
-    for (int f = 0; f < nf; ++f) {
-      const long long o = (long long)f * u + i;
-      if (unk[o]) *ip_val(S, k, f) = X[o];
-    }
-  }
-}
-
 // ------------------------------------------------------------------ flags
 __global__ void k_icgn_flags(long long n, const int *__restrict__ it,
                              unsigned char *__restrict__ bad, int *badnum, double *meanit,
@@ -1337,27 +1109,6 @@ int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int
 int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_t st) {
   const long long n = (long long)M * N;
   k_nodal_strain<<<blocks_for(n), 256, 0, st>>>(M, N, h, U, F);
-  ALDIC_CUDA(cudaGetLastError());
-  return OK;
-}
-
-int inpaint_cta(GridWork &w, int M, int N, double *vals0, int stride0, int nf0, double *vals1,
-                int stride1, int nf1, const unsigned char *badmask, double rtol, int maxit,
-                cudaStream_t st) {
-  const long long n = (long long)M * N;
-  ALDIC_CHECK(n < (1LL << 31) && nf0 >= 0 && nf1 >= 0 && nf0 + nf1 >= 1 && nf0 + nf1 <= kIpMaxF,
-              E_ARG, "inpaint: 1..6 fields on fewer than 2^31 nodes");
-  IpSrc S;
-  S.vals[0] = vals0; S.vals[1] = vals1 ? vals1 : vals0;
-  S.stride[0] = stride0; S.stride[1] = vals1 ? stride1 : stride0;
-  S.nf[0] = nf0; S.nf[1] = vals1 ? nf1 : 0;
-  // scratch in the grid work vectors (12 regions of 12 n doubles): the CG
-  // vectors in x, r, z, p, q, b (6 n doubles each), the index arrays and
-  // degrees in diag, the unknown flags in mask
-  int *cidx = reinterpret_cast<int *>(w.diag), *nodes = cidx + n, *nbc = nodes + n;
-  double *dg = reinterpret_cast<double *>(nbc + 4 * n + 2);
-  k_inpaint_cta<<<1, kIpThreads, 0, st>>>(M, N, S, badmask, cidx, nodes, nbc, w.x, w.r, w.z, w.p,
-                                          w.q, dg, w.mask, rtol, maxit, w.err, w.iters_out);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

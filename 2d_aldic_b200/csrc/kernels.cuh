@@ -208,12 +208,6 @@ int nodal_strain(int M, int N, double h, const double *U, double *F, cudaStream_
 // gridfit springs: load nf interleaved (stride, offset) fields, NaN = no data;
 // the solve starts from the data and, at nodes without data, from guess (the
 // same layout as vals; 0 where null) -- the solution does not depend on it
-// inpaint_nans(., 4) of the nodes flagged in badmask (or NaN) in place, by
-// one CTA over the unknown nodes only: fields [0, nf0) of vals0 (stride0
-// values a node) and [0, nf1) of vals1 (may be null), at most 6 in all
-int inpaint_cta(GridWork &w, int M, int N, double *vals0, int stride0, int nf0, double *vals1,
-                int stride1, int nf1, const unsigned char *badmask, double rtol, int maxit,
-                cudaStream_t st);
 int gridfit_load(GridWork &w, int M, int N, int nf, const double *vals, int stride,
                  const int *bad_iters, cudaStream_t st, int f0 = 0,
                  const double *guess = nullptr);

@@ -201,8 +201,8 @@ ALDIC_API int aldic_subpb2(aldic_ctx *ctx, int M, int N, double step, double bet
  * solver's work vectors live in one fixed static device array of the library
  * (about 12.7 MB, held on every GPU that loads the library until exit), so at
  * most 65536 nodes are accepted -- larger grids return ALDIC_E_ARG.  The
- * first call on a device looks up that array's device address (make it
- * before any stream capture) and keeps it for the process; a cudaDeviceReset
+ * first call on a device looks up that array's device address and keeps it
+ * for the process; a cudaDeviceReset
  * of that device invalidates it, so do not call this entry point on a device
  * after resetting it.  The array is shared by every call: calls whose GPU
  * work overlaps (other streams or threads) race.  Every call synchronises
