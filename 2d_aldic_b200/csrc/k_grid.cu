@@ -202,6 +202,26 @@ __device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i,
   }
 }
 
+// The operator on a direction vector of the iteration sweep.  Inpainting:
+// directions are 0 at every known entry (both m buffers are cleared at
+// set-up and only unknown entries are ever written), so the neighbour terms
+// need no mask -- the same value as op_apply without its four mask loads.
+template <int OP>
+__device__ __forceinline__ double op_apply_dir(const PcgArgs &A, double beta, int i, int j,
+                                               long long k, int f, const double *__restrict__ v) {
+  if (OP == OP_INPAINT) {
+    const int M = A.M, N = A.N;
+    const double xk = v[k];
+    double s = 0.0;
+    if (i > 0) s += xk - v[k - 1];
+    if (i < M - 1) s += xk - v[k + 1];
+    if (j > 0) s += xk - v[k - M];
+    if (j < N - 1) s += xk - v[k + M];
+    return s;
+  }
+  return op_apply<OP>(A, beta, i, j, k, f, v);
+}
+
 // Per-warp partials staged in shared memory: sh[warp][slot]; a warp adds
 // its butterfly-reduced values for `cnt` slots starting at s0.
 struct PcgShared {
@@ -308,6 +328,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
       const double wv = op_apply<OP>(A, bt, i, j, k, f, Uv + f * n);
       Wv[o] = wv;
       Mv[0][o] = wv * Di[o];
+      Mv[1][o] = 0.0;  // known inpainting entries are never written again
       const double rv = R[o], uv = Uv[o], bv = A.b[o];
       a0 += rv * uv;
       a1 += wv * uv;
@@ -341,23 +362,25 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
     double *Mn = Mv[(it + 1) & 1];
     double *part = A.part + ((it + 1) & 1) * pstride;
     // ---- n = A m; directions and iterates; next partials and m.  Fields
-    // go in pairs, every load of a pair before any store, so the two fields'
-    // memory round trips overlap.
+    // go in groups (pairs; threes for inpainting, whose sweep is a few
+    // dependent loads a node), every load of a group before any store, so
+    // the fields' memory round trips overlap.
+    constexpr int G2 = (OP == OP_INPAINT && NR % 3 == 0) ? 3 : (NR >= 2 ? 2 : 1);
 #pragma unroll 1
-    for (int f0 = 0; f0 < NR; f0 += 2) {
-      constexpr int G2 = NR >= 2 ? 2 : 1;
+    for (int f0 = 0; f0 < NR; f0 += G2) {
       double a0[G2], a1[G2], a2[G2], al[G2], be[G2], bt[G2];
-      bool live[G2];
+      bool live[G2], anylive = false;
 #pragma unroll
       for (int q = 0; q < G2; ++q) {
         a0[q] = a1[q] = a2[q] = 0.0;
         const int f = f0 + q;
         live[q] = f < NR && !S.done[f];
+        anylive |= live[q];
         bt[q] = f < NR ? A.beta[f] : 0.0;
         al[q] = f < NR ? S.alpha[f] : 0.0;
         be[q] = f < NR ? S.beta[f] : 0.0;
       }
-      if (live[0] || (G2 > 1 && live[G2 - 1])) {
+      if (anylive) {
         for (long long k = tid0; k < n; k += stride) {
           const int j = (int)k / M, i = (int)k - j * M;  // n < 2^31 (checked at launch)
           double nv[G2], zo[G2], qo[G2], so[G2], po[G2], mo[G2], wo[G2], uo[G2], ro[G2], xo[G2],
@@ -374,7 +397,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
             if (!act[q]) continue;
             const int f = f0 + q;
             const long long o = f * n + k;
-            nv[q] = op_apply<OP>(A, bt[q], i, j, k, f, Mo + f * n);
+            nv[q] = op_apply_dir<OP>(A, bt[q], i, j, k, f, Mo + f * n);
             zo[q] = Zd[o]; qo[q] = Qd[o]; so[q] = Sd[o]; po[q] = Pd[o];
             mo[q] = Mo[o]; wo[q] = Wv[o]; uo[q] = Uv[o]; ro[q] = R[o]; xo[q] = X[o]; di[q] = Di[o];
           }

@@ -274,6 +274,28 @@ __device__ __forceinline__ void col_row(const Eval32 &e, float4 (&R)[4], int &pc
   if (!SUB) a.TY = __ffma2_rn(A, f2(Y), a.TY);
 }
 
+// One row of a lane's column under a pure translation (a11 = a22 = 1,
+// a12 = a21 = 0): the fractions (tu, tv) are the same at every pixel and
+// the floor corner moves down exactly one image row per subset row, so the
+// window holds each stencil row's cubic at tu, formed once as the row
+// enters (slot (K + 3) & 3, as in col_row), and the sample is the Keys
+// weights at tv over the four values.
+template <bool SUB, int K>
+__device__ __forceinline__ void shift_row(float (&H)[4], const float4 *&q, int W, float tu,
+                                          const float4 &wv, float cg, float Y, const float2 *gp,
+                                          float2 &C, Acc32 &a) {
+  H[(K + 3) & 3] = horner3(__ldg(q), tu);
+  q += W;
+  const float d = fmaf(wv.w, H[(K + 3) & 3],
+                       fmaf(wv.z, H[(K + 2) & 3], fmaf(wv.y, H[(K + 1) & 3], fmaf(wv.x, H[K & 3], -cg))));
+  const float2 G = __ldg(gp);
+  const float2 D = f2(d);
+  a.S = __ffma2_rn(D, f2(1.f, d), a.S);
+  const float2 A = __fmul2_rn(G, D);
+  C = __fadd2_rn(C, A);
+  if (!SUB) a.TY = __ffma2_rn(A, f2(Y), a.TY);
+}
+
 // One FP32 evaluation of the residual sums over an nw x nw subset whose
 // top-left pixel is `base` and whose pixel (0, 0) sits at (ox, oy) from the
 // subset centre: u = a11 X + a12 Y + c4, v = a21 X + a22 Y + c5 relative to
@@ -288,23 +310,58 @@ __device__ __forceinline__ void eval32(const Eval32 &e, int lane, float o[8]) {
   a.S = a.T = a.TX = a.TY = f2(0.f);
   // full 32-column blocks: lane = column, rows in order
   const int nch = nw >> 5;
-  for (int ch = 0; ch < nch; ++ch) {
-    const int col = (ch << 5) + lane;
-    const float X = e.ox + (float)col;
-    const float bu = fmaf(e.a11, X, e.c4), bv = fmaf(e.a21, X, e.c5);
-    const float2 *gp = e.gxy + col;
-    float2 C = f2(0.f);
-    float4 R[4];
-    int pcx = INT_MIN, pcy = 0;
-    float Y = e.oy;
-    for (int r = 0; r < nw; r += 4, Y += 4.f, gp += 4 * W) {
-      col_row<SUB, 0>(e, R, pcx, pcy, bu, bv, Y, gp, C, a);
-      if (r + 1 < nw) col_row<SUB, 1>(e, R, pcx, pcy, bu, bv, Y + 1.f, gp + W, C, a);
-      if (r + 2 < nw) col_row<SUB, 2>(e, R, pcx, pcy, bu, bv, Y + 2.f, gp + 2 * W, C, a);
-      if (r + 3 < nw) col_row<SUB, 3>(e, R, pcx, pcy, bu, bv, Y + 3.f, gp + 3 * W, C, a);
+  const bool shift = e.a11 == 1.f && e.a22 == 1.f && e.a12 == 0.f && e.a21 == 0.f;  // warp-uniform
+  if (shift) {
+    // v at row 0 (the general path's fmaf(1, Y, c5)); tv and the Keys
+    // weights (a = -1/2) at it hold for every row
+    const float rv0 = e.oy + e.c5, fv0 = floorf(rv0), tv = rv0 - fv0;
+    const float t2 = tv * tv, t3 = t2 * tv;
+    const float4 wv = make_float4(fmaf(-0.5f, t3, fmaf(-0.5f, tv, t2)),
+                                  fmaf(1.5f, t3, fmaf(-2.5f, t2, 1.f)),
+                                  fmaf(-1.5f, t3, fmaf(0.5f, tv, 2.f * t2)),
+                                  0.5f * (t3 - t2));
+    const int icy0 = (int)fv0;
+    for (int ch = 0; ch < nch; ++ch) {
+      const int col = (ch << 5) + lane;
+      const float X = e.ox + (float)col;
+      const float ru = X + e.c4, fu = floorf(ru), tu = ru - fu;
+      const float4 *q = e.rc + icy0 * W + (int)fu;  // stencil row 0 of subset row 0
+      const float2 *gp = e.gxy + col;
+      float2 C = f2(0.f);
+      float H[4];
+      H[0] = horner3(__ldg(q), tu);
+      H[1] = horner3(__ldg(q + W), tu);
+      H[2] = horner3(__ldg(q + 2 * W), tu);
+      q += 3 * W;
+      float Y = e.oy;
+      for (int r = 0; r < nw; r += 4, Y += 4.f, gp += 4 * W) {
+        shift_row<SUB, 0>(H, q, W, tu, wv, e.cg, Y, gp, C, a);
+        if (r + 1 < nw) shift_row<SUB, 1>(H, q, W, tu, wv, e.cg, Y + 1.f, gp + W, C, a);
+        if (r + 2 < nw) shift_row<SUB, 2>(H, q, W, tu, wv, e.cg, Y + 2.f, gp + 2 * W, C, a);
+        if (r + 3 < nw) shift_row<SUB, 3>(H, q, W, tu, wv, e.cg, Y + 3.f, gp + 3 * W, C, a);
+      }
+      a.T = __fadd2_rn(a.T, C);
+      if (!SUB) a.TX = __ffma2_rn(C, f2(X), a.TX);
     }
-    a.T = __fadd2_rn(a.T, C);
-    if (!SUB) a.TX = __ffma2_rn(C, f2(X), a.TX);
+  } else {
+    for (int ch = 0; ch < nch; ++ch) {
+      const int col = (ch << 5) + lane;
+      const float X = e.ox + (float)col;
+      const float bu = fmaf(e.a11, X, e.c4), bv = fmaf(e.a21, X, e.c5);
+      const float2 *gp = e.gxy + col;
+      float2 C = f2(0.f);
+      float4 R[4];
+      int pcx = INT_MIN, pcy = 0;
+      float Y = e.oy;
+      for (int r = 0; r < nw; r += 4, Y += 4.f, gp += 4 * W) {
+        col_row<SUB, 0>(e, R, pcx, pcy, bu, bv, Y, gp, C, a);
+        if (r + 1 < nw) col_row<SUB, 1>(e, R, pcx, pcy, bu, bv, Y + 1.f, gp + W, C, a);
+        if (r + 2 < nw) col_row<SUB, 2>(e, R, pcx, pcy, bu, bv, Y + 2.f, gp + 2 * W, C, a);
+        if (r + 3 < nw) col_row<SUB, 3>(e, R, pcx, pcy, bu, bv, Y + 3.f, gp + 3 * W, C, a);
+      }
+      a.T = __fadd2_rn(a.T, C);
+      if (!SUB) a.TX = __ffma2_rn(C, f2(X), a.TX);
+    }
   }
   // the remaining columns (one for a 33-pixel window), pixel per lane
   const int c0 = nch << 5, rem = nw - c0;
