@@ -1329,6 +1329,7 @@ __global__ void __launch_bounds__(256) k_box_tab(const uint8_t *__restrict__ g, 
 // the neighbours' exact values; outputs of funIntegerSearch.m:148-159.
 constexpr int kPeakWarps = 8;
 constexpr int kPeakUnroll = 4;  // map entries a lane has in flight
+constexpr int kRingUnroll = 5;  // outer-ring entries a lane takes a round (136 for s = 16: one round)
 
 struct PeakArgs {
   const unsigned *cmap;   // exact correlation sums, tile by tile
@@ -1342,7 +1343,7 @@ struct PeakArgs {
   long long mn;
 };
 
-__global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakArgs A) {
+__global__ void __launch_bounds__(kPeakWarps * 32, 4) k_search_peak(const PeakArgs A) {
   __shared__ uint3 qbuf[kPeakWarps][kTileQueue];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint3 *queue = qbuf[wid];
@@ -1390,18 +1391,26 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
     int nq = 0;          // queued entries (the same in every lane)
     // kPeakUnroll entries a lane at a time: the loads first, one bound update,
     // then the queue (ballot order keeps it dense)
-    auto screen = [&](const bool (&valid)[kPeakUnroll], const int (&k)[kPeakUnroll],
-                      const unsigned (&C)[kPeakUnroll], const float (&e)[kPeakUnroll]) {
+    // (rounds where no lane keeps an entry -- most, once the bound is near
+    // the peak -- skip the queue bookkeeping)
+    auto screen = [&](auto const &valid, auto const &k, auto const &C, auto const &e) {
+      constexpr int U = sizeof(e) / sizeof(float);
       float mx = -INFINITY;
 #pragma unroll
-      for (int j = 0; j < kPeakUnroll; ++j)
+      for (int j = 0; j < U; ++j)
         if (valid[j]) mx = fmaxf(mx, e[j] - kTileEps);
       tkey = max(tkey, __reduce_max_sync(0xffffffffu, fkey(mx)));
+      bool keep[U], any = false;
 #pragma unroll
-      for (int j = 0; j < kPeakUnroll; ++j) {
-        const bool keep = valid[j] && fkey(e[j] + kTileEps) >= tkey;
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (keep) {
+      for (int j = 0; j < U; ++j) {
+        keep[j] = valid[j] && fkey(e[j] + kTileEps) >= tkey;
+        any |= keep[j];
+      }
+      if (!__any_sync(0xffffffffu, any)) return;
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        const unsigned bal = __ballot_sync(0xffffffffu, keep[j]);
+        if (keep[j]) {
           const int pos = nq + __popc(bal & ((1u << lane) - 1u));
           if (pos < kTileQueue) queue[pos] = make_uint3((unsigned)k[j], C[j], __float_as_uint(e[j]));
         }
@@ -1450,14 +1459,14 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
       screen(valid, k, C, e);
     }
     // the outer ring, from ncc_combine's own FP64 numerator and denominator
-    for (int k0 = 0; k0 < nring; k0 += 32 * kPeakUnroll) {
-      bool valid[kPeakUnroll];
-      int k[kPeakUnroll], ra[kPeakUnroll], rb[kPeakUnroll];
-      unsigned C[kPeakUnroll];
-      uint2 w[kPeakUnroll];
-      float e[kPeakUnroll];
+    for (int k0 = 0; k0 < nring; k0 += 32 * kRingUnroll) {
+      bool valid[kRingUnroll];
+      int k[kRingUnroll], ra[kRingUnroll], rb[kRingUnroll];
+      unsigned C[kRingUnroll];
+      uint2 w[kRingUnroll];
+      float e[kRingUnroll];
 #pragma unroll
-      for (int j = 0; j < kPeakUnroll; ++j) {
+      for (int j = 0; j < kRingUnroll; ++j) {
         const int r = k0 + 32 * j + lane;
         valid[j] = r < nring;
         ring_pos(valid[j] ? r : 0, cr, cc, &ra[j], &rb[j]);
@@ -1466,7 +1475,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 3) k_search_peak(const PeakAr
         w[j] = valid[j] ? rw[r] : make_uint2(0, 0);
       }
 #pragma unroll
-      for (int j = 0; j < kPeakUnroll; ++j) {
+      for (int j = 0; j < kRingUnroll; ++j) {
         e[j] = 0.f;
         if (valid[j]) {
           long long st_out, n_out;
