@@ -302,6 +302,7 @@ double springs_lam2(int M, int N) {
 
 // PCG tolerances of the node-grid solves
 constexpr double kRtolFit = 1e-11, kRtolInpaint = 1e-11;
+constexpr int kFramePart = 2048;  // frame partial sums: norms, the beta sweep's 12 x 148
 constexpr int kMaxitFit = 8000, kMaxitInpaint = 50000;
 
 }  // namespace
@@ -1264,7 +1265,7 @@ struct FrameBufs {
   double *err;                      // [6] Err1, [6] Err2, misc
   double *beta;                     // [1]
   double *upd;                      // [2*16] update norms
-  double *part;                     // [1024]
+  double *part;                     // [kFramePart]
   int *it1, *itb;
   unsigned char *bad;
   int *ints;                        // [8] bad num, nconv, ...
@@ -1354,7 +1355,6 @@ __global__ void k_zero(double *a, long long n) {
 
 __global__ void k_set1(double *a, double v) { *a = v; }
 
-__global__ void k_scale_store(const double *src, double *dst, double s) { *dst = *src * s; }
 
 // main_ALDIC.m:285-301: beta from the sweep (device-side so the frame stays
 // capturable); err[0..5] = Err1, err[6..11] = Err2, betas on the fly
@@ -1515,26 +1515,33 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   };
   auto dual = [&](int accumulate) {
     if (fd) return fd_dual(M, N, B.F2, B.F1, B.U2, B.U1, B.udual, B.vdual, accumulate, st);
-    int r = vsub(B.F2, B.F1, B.udual, 4 * n, st);
-    return r ? r : vsub(B.U2, B.U1, B.vdual, 2 * n, st);
+    return vsub2(B.F2, B.F1, B.udual, 4 * n, B.U2, B.U1, B.vdual, 2 * n, st);
   };
   if (p->beta > 0) {
     k_set1<<<1, 1, 0, st>>>(B.beta, p->beta);
   } else {
     const double base = h * h * mu;
     const double bl[6] = {1e-3, std::sqrt(1e-5), 1e-2, std::sqrt(1e-3), 1e-1, std::sqrt(1e-1)};
-    double be[12];
+    double be[12], b6[6];
     for (int k = 0; k < 6; ++k) {
-      be[2 * k] = be[2 * k + 1] = bl[k] * base;
-      if ((rc = rhs(bl[k] * base, nullptr, 2 * k))) return rc;
+      be[2 * k] = be[2 * k + 1] = b6[k] = bl[k] * base;
+      if (fd && (rc = rhs(bl[k] * base, nullptr, 2 * k))) return rc;
     }
+    if (!fd && (rc = fe_rhs_sweep(c->gw, M, N, h, b6, mu, B.U1, B.F1, B.udual, B.vdual, st)))
+      return rc;
     // the six systems of the sweep in one launch (12 right-hand sides)
     if ((rc = pcg(12, nullptr, be))) return rc;
-    for (int k = 0; k < 6; ++k) {
-      if ((rc = store(2 * k))) return rc;
-      if ((rc = strain())) return rc;
-      if ((rc = vdiffnorm(B.U1, B.U2, 2 * n, B.part, B.err + k, st))) return rc;
-      if ((rc = vdiffnorm(B.F1, B.F2, 4 * n, B.part, B.err + 6 + k, st))) return rc;
+    if (fd) {
+      for (int k = 0; k < 6; ++k) {
+        if ((rc = store(2 * k))) return rc;
+        if ((rc = strain())) return rc;
+        if ((rc = vdiffnorm(B.U1, B.U2, 2 * n, B.part, B.err + k, st))) return rc;
+        if ((rc = vdiffnorm(B.F1, B.F2, 4 * n, B.part, B.err + 6 + k, st))) return rc;
+      }
+    } else {
+      // store, nodal strain and both norms of every candidate in one pass
+      if ((rc = sweep_err(M, N, 6, h, c->gw.x, B.U1, B.F1, B.part, kFramePart, B.err, st)))
+        return rc;
     }
     k_beta_select<<<1, 1, 0, st>>>(B.err, base, B.beta, fd ? h : 0.0);
   }
@@ -1546,8 +1553,11 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
   // Section 6: ADMM iterations
   if ((rc = mark(c, 5))) return rc;
   const double inv = 1.0 / std::sqrt((double)(2 * n));
+  bool u2old_current = false;  // the last update norm already copied U2 into U2old
   for (int a = 0; a < p->n_admm; ++a) {
-    ALDIC_CUDA(cudaMemcpyAsync(B.U2old, B.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    if (!u2old_current)
+      ALDIC_CUDA(cudaMemcpyAsync(B.U2old, B.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    u2old_current = false;
     if ((rc = subpb1(im, B.coords, n, B.U2, B.F2, B.vdual, B.H21, nullptr, p->winsize, mu, p->tol,
                      p->precision, B.U1, B.itb, c->queue.as<unsigned int>(), st, B.cache)))
       return rc;
@@ -1556,19 +1566,19 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
     if ((rc = grid_pcg(c->gw, OP_GRIDFIT, M, N, 2, 0, 0, 1, lam2, kRtolFit, kMaxitFit, st))) return rc;
     if ((rc = grid_store(c->gw, M, N, 2, B.U1, 2, st))) return rc;
     ALDIC_CUDA(cudaMemcpyAsync(B.F1, B.F2, sizeof(double) * 4 * n, cudaMemcpyDeviceToDevice, st));
-    if (a < 16) {
-      if ((rc = vdiffnorm(B.U1old, B.U1, 2 * n, B.part, B.upd + 16 + a, st))) return rc;
-      k_scale_store<<<1, 1, 0, st>>>(B.upd + 16 + a, B.upd + 16 + a, inv);
+    if (a < 16) {  // the update norm, and U1old <- U1 in the same pass
+      if ((rc = diffnorm_update(B.U1old, B.U1, 2 * n, B.part, B.upd + 16 + a, inv, st))) return rc;
+    } else {
+      ALDIC_CUDA(cudaMemcpyAsync(B.U1old, B.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
     }
-    ALDIC_CUDA(cudaMemcpyAsync(B.U1old, B.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
     if (p->smooth && (rc = smooth_dev(c, M, N, 2, B.U1))) return rc;
     if ((rc = rhs(0, B.beta, 0)) || (rc = pcg(2, B.beta, nullptr)) || (rc = store(0))) return rc;
     if (p->smooth && (rc = smooth_dev(c, M, N, 2, B.U2))) return rc;
     if ((rc = strain())) return rc;
     if (p->smooth && (rc = smooth_dev(c, M, N, 4, B.F2))) return rc;
-    if (a < 16) {
-      if ((rc = vdiffnorm(B.U2old, B.U2, 2 * n, B.part, B.upd + a, st))) return rc;
-      k_scale_store<<<1, 1, 0, st>>>(B.upd + a, B.upd + a, inv);
+    if (a < 16) {  // U2 is not written again before the next Subpb1
+      if ((rc = diffnorm_update(B.U2old, B.U2, 2 * n, B.part, B.upd + a, inv, st))) return rc;
+      u2old_current = true;
     }
     if ((rc = dual(1))) return rc;   // FE resets the duals, FD accumulates (main_ALDIC.m:434-441)
   }
@@ -1841,7 +1851,9 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
   int steps = 0;
   const double inv = 1.0 / std::sqrt((double)(2 * n));
   for (int a = 0; a < p->n_admm; ++a) {
-    ALDIC_CUDA(cudaMemcpyAsync(Q.U2old, Q.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+    // (from the second iteration on, the update norm below left U2old = U2)
+    if (a == 0)
+      ALDIC_CUDA(cudaMemcpyAsync(Q.U2old, Q.U2, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
     if ((rc = subpb1(im, qcoords, n, Q.U2, Q.F2, Q.vd, Q.H21, wins, w, mu, p->tol, p->precision, Q.U1,
                      Q.itb, c->queue.as<unsigned int>(), st, Q.cache)))
       return rc;
@@ -1852,11 +1864,11 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
     if ((rc = qt_subpb2(m, c->gw, beta, mu, Q.U1, Q.F1, Q.U2, st)) || (rc = qt_strain(m, Q.U2, Q.F2, st)))
       return rc;
     k_qt_keep_dirichlet<<<nb, 256, 0, st>>>(n, kind, Q.F1, Q.F2);
-    if ((rc = vdiffnorm(Q.U2old, Q.U2, 2 * n, part, nrm + 8, st)) ||
-        (rc = vdiffnorm(Q.U1old, Q.U1, 2 * n, part, nrm + 9, st)))
+    // the update norms, each old vector refreshed in the same pass
+    if ((rc = diffnorm_update(Q.U2old, Q.U2, 2 * n, part, nrm + 8, 1.0, st)) ||
+        (rc = diffnorm_update(Q.U1old, Q.U1, 2 * n, part, nrm + 9, 1.0, st)))
       return rc;
-    ALDIC_CUDA(cudaMemcpyAsync(Q.U1old, Q.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
-    if ((rc = vsub(Q.F2, Q.F1, Q.ud, 4 * n, st)) || (rc = vsub(Q.U2, Q.U1, Q.vd, 2 * n, st))) return rc;
+    if ((rc = vsub2(Q.F2, Q.F1, Q.ud, 4 * n, Q.U2, Q.U1, Q.vd, 2 * n, st))) return rc;
     double hv[2];
     ALDIC_CUDA(cudaMemcpyAsync(hv, nrm + 8, sizeof(hv), cudaMemcpyDeviceToHost, st));
     ALDIC_CUDA(cudaStreamSynchronize(st));  // the stop test needs the two norms
@@ -2071,7 +2083,7 @@ int aldic_frame(aldic_ctx *c, const aldic_frame_params *p, double *x0, double *y
     B.cache = q.take<double>((long long)kIcgnCache * n);
     B.F0 = q.take<double>(4 * n);
     B.err = q.take<double>(16); B.beta = q.take<double>(4); B.upd = q.take<double>(32);
-    B.part = q.take<double>(1024); B.meanit = q.take<double>(4);
+    B.part = q.take<double>(kFramePart); B.meanit = q.take<double>(4);
     B.it1 = q.take<int>(n); B.itb = q.take<int>(n); B.ints = q.take<int>(16);
     B.bad = q.take<unsigned char>(n);
   };

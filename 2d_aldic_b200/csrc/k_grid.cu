@@ -463,11 +463,19 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
 
 // ------------------------------------------------------------------ Subpb2 RHS
 // Subpb2.m:88-149 per node, gathered from its (up to 4) elements.
-__global__ void k_fe_rhs(int M, int N, double h, double beta, const double *beta_ptr, double mu,
+// NB right-hand sides at once (the beta sweep: one per beta, the same
+// operations for each as a single one), and the solve's start x = U with every
+// entry unknown: fields (2q, 2q + 1) of b and x for beta[q].
+struct FeBetas {
+  double v[6];
+};
+template <int NB>
+__global__ void k_fe_rhs(int M, int N, double h, FeBetas be, const double *beta_ptr, double mu,
                          const double *__restrict__ U, const double *__restrict__ F,
                          const double *__restrict__ ud, const double *__restrict__ vd,
-                         double *__restrict__ b) {
-  if (beta_ptr) beta = *beta_ptr;
+                         double *__restrict__ b, double *__restrict__ x,
+                         unsigned char *__restrict__ mask) {
+  if (beta_ptr) be.v[0] = *beta_ptr;
   const long long n = (long long)M * N;
   const double gp[3] = {-0.7745966692414834, 0.0, 0.7745966692414834};  // sqrt(3/5)
   const double gw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
@@ -479,7 +487,9 @@ __global__ void k_fe_rhs(int M, int N, double h, double beta, const double *beta
     const double fw1 = F[4 * k + 2] - ud[4 * k + 2];
     const double fw2 = F[4 * k + 1] - ud[4 * k + 1];
     const double fw3 = F[4 * k + 3] - ud[4 * k + 3];
-    double bu = 0.0, bv = 0.0;
+    double bu[NB], bv[NB];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) bu[q] = bv[q] = 0.0;
     for (int ej = j - 1; ej <= j; ++ej)
       for (int ei = i - 1; ei <= i; ++ei) {
         if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
@@ -504,12 +514,23 @@ __global__ void k_fe_rhs(int M, int N, double h, double beta, const double *beta
               nu += Nn[lb] * uvu[lb];
               nv += Nn[lb] * uvv[lb];
             }
-            bu += s * (beta * (gx * fw0 + gy * fw1) + mu * Nn[la] * nu);
-            bv += s * (beta * (gx * fw2 + gy * fw3) + mu * Nn[la] * nv);
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+              bu[q] += s * (be.v[q] * (gx * fw0 + gy * fw1) + mu * Nn[la] * nu);
+              bv[q] += s * (be.v[q] * (gx * fw2 + gy * fw3) + mu * Nn[la] * nv);
+            }
           }
       }
-    b[k] = bu;
-    b[n + k] = bv;
+    const double u0 = U[2 * k], v0 = U[2 * k + 1];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+      b[2 * q * n + k] = bu[q];
+      b[(2 * q + 1) * n + k] = bv[q];
+      x[2 * q * n + k] = u0;
+      x[(2 * q + 1) * n + k] = v0;
+      mask[2 * q * n + k] = 1;
+      mask[(2 * q + 1) * n + k] = 1;
+    }
   }
 }
 
@@ -622,20 +643,6 @@ __global__ void k_fd_dual(int M, int N, const double *__restrict__ F2, const dou
   }
 }
 
-// The solve starts from the U that enters Subproblem 2 (the local solution,
-// which the global one differs from by the ADMM residual): the PCG then needs
-// fewer iterations to the same relative residual than from zero.
-__global__ void k_fe_init(long long n, const double *__restrict__ U, double *__restrict__ x,
-                          unsigned char *mask) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
-    x[k] = U[2 * k];
-    x[n + k] = U[2 * k + 1];
-    mask[k] = 1;
-    mask[n + k] = 1;
-  }
-}
-
 __global__ void k_fe_store(long long n, const double *__restrict__ x, double *__restrict__ U) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
@@ -649,9 +656,11 @@ __global__ void k_fe_store(long long n, const double *__restrict__ x, double *__
 // in the order (-,-), (+,-), (+,+), (-,+); extrapolated to the corners with
 // the matrix of :105-108; averaged over the elements sharing a node.  Output
 // slots per node are [du/dx, du/dy, dv/dx, dv/dy] as written at :123-137.
-__global__ void k_nodal_strain(int M, int N, double h, const double *__restrict__ U,
-                               double *__restrict__ F) {
-  const long long n = (long long)M * N;
+// The nodal strain of node (i, j); ld(q, &u, &v) reads the displacement of
+// node q.
+template <class Load>
+__device__ __forceinline__ void nodal_strain_node(int M, int N, double h, int i, int j,
+                                                  const Load &ld, double out[4]) {
   const double r3 = 0.5773502691896257;  // 1/sqrt(3)
   const double s3 = 1.7320508075688772;
   const double gks[4] = {-r3, r3, r3, -r3}, get_[4] = {-r3, -r3, r3, r3};
@@ -659,45 +668,134 @@ __global__ void k_nodal_strain(int M, int N, double h, const double *__restrict_
                           {-0.5, 1 + 0.5 * s3, -0.5, 1 - 0.5 * s3},
                           {1 - 0.5 * s3, -0.5, 1 + 0.5 * s3, -0.5},
                           {-0.5, 1 - 0.5 * s3, -0.5, 1 + 0.5 * s3}};
+  double acc[4] = {0, 0, 0, 0};
+  int cnt = 0;
+  for (int ej = j - 1; ej <= j; ++ej)
+    for (int ei = i - 1; ei <= i; ++ei) {
+      if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
+      const int la = (i - ei) + (j - ej) * 3 - 2 * (i - ei) * (j - ej);
+      double ue[8];
+      for (int lb = 0; lb < 4; ++lb) {
+        const long long q = (long long)(ej + ly(lb)) * M + (ei + lx(lb));
+        ld(q, &ue[2 * lb], &ue[2 * lb + 1]);
+      }
+      double G[4][4];
+      for (int g = 0; g < 4; ++g) {
+        const double ksi = gks[g], eta = get_[g];
+        const double dks[4] = {-(1 - eta) / 4, (1 - eta) / 4, (1 + eta) / 4, -(1 + eta) / 4};
+        const double det_[4] = {-(1 - ksi) / 4, -(1 + ksi) / 4, (1 + ksi) / 4, (1 - ksi) / 4};
+        double v[4] = {0, 0, 0, 0};
+        for (int a = 0; a < 4; ++a) {
+          const double gx = (2.0 / h) * dks[a], gy = (2.0 / h) * det_[a];
+          v[0] += gx * ue[2 * a];
+          v[1] += gy * ue[2 * a];
+          v[2] += gx * ue[2 * a + 1];
+          v[3] += gy * ue[2 * a + 1];
+        }
+        for (int c = 0; c < 4; ++c) G[g][c] = v[c];
+      }
+      for (int c = 0; c < 4; ++c) {
+        double s = 0.0;
+        for (int g = 0; g < 4; ++g) s += E[la][g] * G[g][c];
+        acc[c] += s;
+      }
+      cnt++;
+    }
+  for (int c = 0; c < 4; ++c) out[c] = acc[c] / cnt;
+}
+
+__global__ void k_nodal_strain(int M, int N, double h, const double *__restrict__ U,
+                               double *__restrict__ F) {
+  const long long n = (long long)M * N;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k % M), j = (int)(k / M);
-    double acc[4] = {0, 0, 0, 0};
-    int cnt = 0;
-    for (int ej = j - 1; ej <= j; ++ej)
-      for (int ei = i - 1; ei <= i; ++ei) {
-        if (ei < 0 || ei >= M - 1 || ej < 0 || ej >= N - 1) continue;
-        const int la = (i - ei) + (j - ej) * 3 - 2 * (i - ei) * (j - ej);
-        double ue[8];
-        for (int lb = 0; lb < 4; ++lb) {
-          const long long q = (long long)(ej + ly(lb)) * M + (ei + lx(lb));
-          ue[2 * lb] = U[2 * q];
-          ue[2 * lb + 1] = U[2 * q + 1];
-        }
-        double G[4][4];
-        for (int g = 0; g < 4; ++g) {
-          const double ksi = gks[g], eta = get_[g];
-          const double dks[4] = {-(1 - eta) / 4, (1 - eta) / 4, (1 + eta) / 4, -(1 + eta) / 4};
-          const double det_[4] = {-(1 - ksi) / 4, -(1 + ksi) / 4, (1 + ksi) / 4, (1 - ksi) / 4};
-          double v[4] = {0, 0, 0, 0};
-          for (int a = 0; a < 4; ++a) {
-            const double gx = (2.0 / h) * dks[a], gy = (2.0 / h) * det_[a];
-            v[0] += gx * ue[2 * a];
-            v[1] += gy * ue[2 * a];
-            v[2] += gx * ue[2 * a + 1];
-            v[3] += gy * ue[2 * a + 1];
-          }
-          for (int c = 0; c < 4; ++c) G[g][c] = v[c];
-        }
-        for (int c = 0; c < 4; ++c) {
-          double s = 0.0;
-          for (int g = 0; g < 4; ++g) s += E[la][g] * G[g][c];
-          acc[c] += s;
-        }
-        cnt++;
-      }
-    for (int c = 0; c < 4; ++c) F[4 * k + c] = acc[c] / cnt;
+    double out[4];
+    nodal_strain_node(M, N, h, i, j,
+                      [&](long long q, double *u, double *v) {
+                        *u = U[2 * q];
+                        *v = U[2 * q + 1];
+                      },
+                      out);
+    for (int c = 0; c < 4; ++c) F[4 * k + c] = out[c];
   }
+}
+
+// ------------------------------------------------------------------ beta sweep errors
+// The beta sweep of Subproblem 2 (main_ALDIC.m:206-230) stores each
+// candidate solution, forms its nodal strain and takes |U1 - U2| and
+// |F1 - F2|; only those two norms outlive the sweep.  One pass over the
+// nodes forms both for every candidate c (fields 2c, 2c + 1 of the solver's
+// x, node order) without writing the candidates out: block partials go to
+// part[s * gridDim.x + block], s = c for the displacement norm and
+// kSweepMax + c for the strain norm.
+constexpr int kSweepMax = 6;
+constexpr int kSweepThreads = 256;
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_err(int M, int N, int nc, double h,
+                                                             const double *__restrict__ x,
+                                                             const double *__restrict__ U1,
+                                                             const double *__restrict__ F1,
+                                                             double *__restrict__ part) {
+  const long long n = (long long)M * N;
+  double su[kSweepMax], sf[kSweepMax];
+#pragma unroll
+  for (int c = 0; c < kSweepMax; ++c) su[c] = sf[c] = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % M), j = (int)(k / M);
+    const double u1 = U1[2 * k], v1 = U1[2 * k + 1];
+    double f1[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) f1[m] = F1[4 * k + m];
+#pragma unroll
+    for (int c = 0; c < kSweepMax; ++c) {
+      if (c >= nc) break;
+      const double *xu = x + 2 * c * n, *xv = xu + n;
+      const double du = u1 - xu[k], dv = v1 - xv[k];
+      su[c] += du * du + dv * dv;
+      double fn[4];
+      nodal_strain_node(M, N, h, i, j,
+                        [&](long long q, double *u, double *v) {
+                          *u = xu[q];
+                          *v = xv[q];
+                        },
+                        fn);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const double d = f1[m] - fn[m];
+        sf[c] += d * d;
+      }
+    }
+  }
+  __shared__ double sh[2 * kSweepMax][kSweepThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < kSweepMax; ++c) {
+    const double a = warp_sum(su[c]), b = warp_sum(sf[c]);
+    if (lane == 0) {
+      sh[c][wid] = a;
+      sh[kSweepMax + c][wid] = b;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * kSweepMax) {
+    double t = 0.0;
+    for (int w = 0; w < kSweepThreads / 32; ++w) t += sh[threadIdx.x][w];
+    part[threadIdx.x * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// err[c] = |U1 - U2_c|, err[kSweepMax + c] = |F1 - F2_c|: one warp per norm,
+// fixed summation order
+__global__ void k_sweep_err_final(const double *__restrict__ part, int nb, int nc,
+                                  double *__restrict__ err) {
+  const int s = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = s % kSweepMax;
+  if (c >= nc) return;
+  double t = 0.0;
+  for (int b = lane; b < nb; b += 32) t += part[s * nb + b];
+  t = warp_sum(t);
+  if (lane == 0) err[s] = sqrt(t);
 }
 
 // ------------------------------------------------------------------ loaders
@@ -873,12 +971,26 @@ __global__ void k_vsub(const double *a, const double *b, double *o, long long n)
     o[k] = a[k] - b[k];
 }
 
-__global__ void k_diffnorm_part(const double *a, const double *b, long long n, double *part) {
+// o1 = a1 - b1 (n1 entries) and o2 = a2 - b2 (n2) in one launch
+__global__ void k_vsub2(const double *a1, const double *b1, double *o1, long long n1,
+                        const double *a2, const double *b2, double *o2, long long n2) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n1 + n2;
+       k += (long long)gridDim.x * blockDim.x) {
+    if (k < n1) o1[k] = a1[k] - b1[k];
+    else o2[k - n1] = a2[k - n1] - b2[k - n1];
+  }
+}
+
+// block partials of |a - b|^2; with copy, a <- b as it goes (the caller's
+// "old" vector refreshed in the same pass)
+__global__ void k_diffnorm_part(double *a, const double *b, long long n, double *part, bool copy) {
   double s = 0.0;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
-    const double d = a[k] - b[k];
+    const double bk = b[k];
+    const double d = a[k] - bk;
     s += d * d;
+    if (copy) a[k] = bk;
   }
   s = warp_sum(s);
   __shared__ double sh[32];
@@ -891,8 +1003,9 @@ __global__ void k_diffnorm_part(const double *a, const double *b, long long n, d
   }
 }
 
-// one 256-thread block: strided partial sums, then a fixed-order tree
-__global__ void k_diffnorm_final(const double *part, int np, double *res) {
+// one 256-thread block: strided partial sums, then a fixed-order tree;
+// res = sqrt(sum) * scale
+__global__ void k_diffnorm_final(const double *part, int np, double *res, double scale) {
   double t = 0.0;
   for (int k = threadIdx.x; k < np; k += blockDim.x) t += part[k];
   t = warp_sum(t);
@@ -902,7 +1015,7 @@ __global__ void k_diffnorm_final(const double *part, int np, double *res) {
   if (threadIdx.x == 0) {
     double u = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) u += sh[w];
-    *res = sqrt(u);
+    *res = sqrt(u) * scale;
   }
 }
 
@@ -1016,9 +1129,22 @@ int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const do
            const double *F, const double *udual, const double *vdual, cudaStream_t st,
            const double *beta_ptr, int f0) {
   const long long n = (long long)M * N;
-  k_fe_rhs<<<blocks_for(n), 256, 0, st>>>(M, N, h, beta, beta_ptr, mu, U, F, udual, vdual,
-                                          w.b + f0 * n);
-  k_fe_init<<<blocks_for(n), 256, 0, st>>>(n, U, w.x + f0 * n, w.mask + f0 * n);
+  FeBetas be{};
+  be.v[0] = beta;
+  k_fe_rhs<1><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, beta_ptr, mu, U, F, udual, vdual,
+                                             w.b + f0 * n, w.x + f0 * n, w.mask + f0 * n);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int fe_rhs_sweep(GridWork &w, int M, int N, double h, const double beta[6], double mu,
+                 const double *U, const double *F, const double *udual, const double *vdual,
+                 cudaStream_t st) {
+  const long long n = (long long)M * N;
+  FeBetas be;
+  for (int q = 0; q < 6; ++q) be.v[q] = beta[q];
+  k_fe_rhs<6><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, nullptr, mu, U, F, udual, vdual, w.b,
+                                             w.x, w.mask);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
@@ -1195,11 +1321,41 @@ int vsub(const double *a, const double *b, double *out, long long n, cudaStream_
   return OK;
 }
 
+int sweep_err(int M, int N, int nc, double h, const double *x, const double *U1,
+              const double *F1, double *part, int npart, double *err, cudaStream_t st) {
+  ALDIC_CHECK(nc >= 1 && nc <= kSweepMax, E_ARG, "sweep_err: 1..6 candidates");
+  const long long n = (long long)M * N;
+  int nb = npart / (2 * kSweepMax);
+  if (nb > 148) nb = 148;
+  if ((long long)nb * kSweepThreads > n) nb = (int)((n + kSweepThreads - 1) / kSweepThreads);
+  ALDIC_CHECK(nb >= 1, E_ARG, "sweep_err: partials buffer too small");
+  k_sweep_err<<<nb, kSweepThreads, 0, st>>>(M, N, nc, h, x, U1, F1, part);
+  k_sweep_err_final<<<1, 2 * kSweepMax * 32, 0, st>>>(part, nb, nc, err);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int vsub2(const double *a1, const double *b1, double *o1, long long n1, const double *a2,
+          const double *b2, double *o2, long long n2, cudaStream_t st) {
+  k_vsub2<<<blocks_for(n1 + n2), 256, 0, st>>>(a1, b1, o1, n1, a2, b2, o2, n2);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
 int vdiffnorm(const double *a, const double *b, long long n, double *part, double *res,
               cudaStream_t st) {
   const int nb = 148;
-  k_diffnorm_part<<<nb, 256, 0, st>>>(a, b, n, part);
-  k_diffnorm_final<<<1, 256, 0, st>>>(part, nb, res);
+  k_diffnorm_part<<<nb, 256, 0, st>>>(const_cast<double *>(a), b, n, part, false);
+  k_diffnorm_final<<<1, 256, 0, st>>>(part, nb, res, 1.0);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int diffnorm_update(double *old, const double *cur, long long n, double *part, double *res,
+                    double scale, cudaStream_t st) {
+  const int nb = 148;
+  k_diffnorm_part<<<nb, 256, 0, st>>>(old, cur, n, part, true);
+  k_diffnorm_final<<<1, 256, 0, st>>>(part, nb, res, scale);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

@@ -179,6 +179,18 @@ __device__ __forceinline__ double sample_minus(const double *img, int W, int cx,
   return sample<double>(img, W, cx, cy, tu, tv) - c;
 }
 
+// floor(x) and the same value as an int, for |x| < 2^22: x + 1.5 * 2^23
+// rounded toward -infinity lands on the float grid of spacing 1, so it holds
+// floor(x) + 1.5 * 2^23 exactly and floor(x) sits in its low mantissa bits
+// (magic-number rounding).  Equal to floorf / (int) bit for bit, on the FP32
+// and integer pipes instead of the conversion unit.  The sampled positions
+// lie inside the image (the out-of-image test runs first), far below 2^22.
+__device__ __forceinline__ float floor_i(float x, int *i) {
+  const float t = __fadd_rd(x, 12582912.0f);
+  *i = __float_as_int(t) - 0x4B400000;
+  return t - 12582912.0f;
+}
+
 // Packed (two-lane) FP32 arithmetic of sm_100: two IEEE single-precision
 // operations per instruction.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
@@ -252,8 +264,8 @@ __device__ __forceinline__ void col_row(const Eval32 &e, float4 (&R)[4], int &pc
                                         Acc32 &a) {
   const int W = e.W;
   const float ru = fmaf(e.a12, Y, bu), rv = fmaf(e.a22, Y, bv);
-  const float fu = floorf(ru), fv = floorf(rv);
-  const int icx = (int)fu, icy = (int)fv;
+  int icx, icy;
+  const float fu = floor_i(ru, &icx), fv = floor_i(rv, &icy);
   const float4 *q = e.rc + (icy + 3) * W + icx;  // stencil row 3
   const bool slide = icx == pcx && icy == pcy + 1;
   R[(K + 3) & 3] = __ldg(q);
@@ -374,8 +386,9 @@ __device__ __forceinline__ void eval32(const Eval32 &e, int lane, float o[8]) {
       const float X = e.ox + (float)c0 + rcol, Y = e.oy + rrow;
       const float ru = fmaf(e.a11, X, fmaf(e.a12, Y, e.c4));
       const float rv = fmaf(e.a21, X, fmaf(e.a22, Y, e.c5));
-      const float fu = floorf(ru), fv = floorf(rv);
-      const float4 *q = e.rc + (int)fv * W + (int)fu;
+      int iu, iv;
+      const float fu = floor_i(ru, &iu), fv = floor_i(rv, &iv);
+      const float4 *q = e.rc + iv * W + iu;
       const float d = cubic_rows(__ldg(q), __ldg(q + W), __ldg(q + 2 * W), __ldg(q + 3 * W),
                                  ru - fu, rv - fv) - e.cg;
       const float2 G = __ldg(e.gxy + k);

@@ -201,6 +201,10 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
 int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
            const double *F, const double *udual, const double *vdual, cudaStream_t st,
            const double *beta_ptr = nullptr, int f0 = 0);
+// the six right-hand sides of the beta sweep (beta[q] into fields 2q, 2q + 1)
+int fe_rhs_sweep(GridWork &w, int M, int N, double h, const double beta[6], double mu,
+                 const double *U, const double *F, const double *udual, const double *vdual,
+                 cudaStream_t st);
 // interleave w.x (2 fields from slot f0) into Uhat
 int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int f0 = 0);
 // nodal strain (funGlobal_NodalStrainAvg.m)
@@ -228,9 +232,19 @@ int subpb1_flags(int n, const int *iters, unsigned char *badmask, int *d_badnum,
 int nanconv3(GridWork &w, int M, int N, int nf, cudaStream_t st);
 // out = a - b (n elements)
 int vsub(const double *a, const double *b, double *out, long long n, cudaStream_t st);
+// o1 = a1 - b1, o2 = a2 - b2 in one launch
+int vsub2(const double *a1, const double *b1, double *o1, long long n1, const double *a2,
+          const double *b2, double *o2, long long n2, cudaStream_t st);
 // ||a - b||_2 into *res (deterministic)
+// the beta sweep's errors |U1 - U2_c| -> err[c], |F1 - F2_c| -> err[6 + c] for
+// the nc <= 6 FE candidates in fields (2c, 2c + 1) of x; part holds npart doubles
+int sweep_err(int M, int N, int nc, double h, const double *x, const double *U1,
+              const double *F1, double *part, int npart, double *err, cudaStream_t st);
 int vdiffnorm(const double *a, const double *b, long long n, double *part, double *res,
               cudaStream_t st);
+// res = |old - cur| * scale (part: 148 doubles), and old <- cur in the same pass
+int diffnorm_update(double *old, const double *cur, long long n, double *part, double *res,
+                    double scale, cudaStream_t st);
 
 // ---- multigrid integer search (k_searchmg.cu, funIntegerSearchMg.m)
 struct MgWork {
