@@ -177,15 +177,34 @@ ICGN_SOURCES = ("2d_aldic_b200/csrc/k_icgn.cu", "2d_aldic_b200/csrc/kernels.cuh"
                 "2d_aldic_b200/csrc/aldic_internal.cuh", "2d_aldic_b200/csrc/k_image.cu")
 
 
+def _icgn_part(rel: str, text: bytes) -> bytes:
+    """The part of a source file the IC-GN kernel is built from: all of it,
+    except for the shared declarations header, where only its preamble and
+    its k_icgn.cu section count (its other sections declare other files'
+    entry points)."""
+    if not rel.endswith("kernels.cuh"):
+        return text
+    marks = [i for i in range(len(text)) if text.startswith(b"// ---- ", i)
+             and (i == 0 or text[i - 1:i] == b"\n")]
+    if not marks:
+        return text
+    pre = text[:marks[0]]
+    for k, i in enumerate(marks):
+        if text.startswith(b"// ---- k_icgn.cu", i):
+            end = marks[k + 1] if k + 1 < len(marks) else len(text)
+            return pre + text[i:end]
+    return text
+
+
 def icgn_source_digest() -> str:
-    """sha1 over the IC-GN kernel's source files: the ncu summary records the
+    """sha1 over the IC-GN kernel's sources: the ncu summary records the
     digest of the build it measured, so a summary of an older kernel is not
     reported as this one's traffic."""
     import hashlib
     h = hashlib.sha1()
     for rel in ICGN_SOURCES:
         with open(os.path.join(ROOT, rel), "rb") as fh:
-            h.update(fh.read())
+            h.update(_icgn_part(rel, fh.read()))
     return h.hexdigest()[:12]
 
 
