@@ -1813,8 +1813,7 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
   if ((rc = icgn_flags((int)n, 1, Q.it1, Q.bad, Q.ints, mean, Q.ints + 1, st))) return rc;
   k_zero_bad<<<nb, 256, 0, st>>>(n, 2, Q.U1, Q.bad);
   k_zero_bad<<<nb, 256, 0, st>>>(n, 4, Q.F1, Q.bad);
-  if ((rc = qt_fill(m, c->gw, 2, Q.U1, Q.bad, st)) || (rc = qt_fill(m, c->gw, 4, Q.F1, Q.bad, st)))
-    return rc;
+  if ((rc = qt_fill2(m, c->gw, 2, Q.U1, 4, Q.F1, Q.bad, st))) return rc;  // U and F in one solve
   ALDIC_CUDA(cudaMemcpyAsync(Q.Uicgn, Q.U1, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
   int nbad = 0;
   ALDIC_CUDA(cudaMemcpyAsync(&nbad, Q.ints, sizeof(int), cudaMemcpyDeviceToHost, st));

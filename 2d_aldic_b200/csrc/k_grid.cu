@@ -202,13 +202,20 @@ __device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i,
   }
 }
 
-// The operator on a direction vector of the iteration sweep.  Inpainting:
-// directions are 0 at every known entry (both m buffers are cleared at
-// set-up and only unknown entries are ever written), so the neighbour terms
-// need no mask -- the same value as op_apply without its four mask loads.
+// The operator on a direction vector of the iteration sweep, at an unknown
+// entry.  Inpainting and CSR (masked) systems: directions are 0 at every
+// known entry (both m buffers are cleared at set-up and only unknown entries
+// are ever written), so the neighbour terms need no mask -- the same value
+// as op_apply without its mask loads.
 template <int OP>
 __device__ __forceinline__ double op_apply_dir(const PcgArgs &A, double beta, int i, int j,
                                                long long k, int f, const double *__restrict__ v) {
+  if (OP == OP_CSR) {
+    double y = 0.0;
+    const int p1 = A.csr.row[k + 1];
+    for (int p = A.csr.row[k]; p < p1; ++p) y += A.csr.val[p] * v[A.csr.col[p]];
+    return y;
+  }
   if (OP == OP_INPAINT) {
     const int M = A.M, N = A.N;
     const double xk = v[k];
@@ -365,7 +372,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
     // go in groups (pairs; threes for inpainting, whose sweep is a few
     // dependent loads a node), every load of a group before any store, so
     // the fields' memory round trips overlap.
-    constexpr int G2 = (OP == OP_INPAINT && NR % 3 == 0) ? 3 : (NR >= 2 ? 2 : 1);
+    constexpr int G2 = ((OP == OP_INPAINT || OP == OP_CSR) && NR % 3 == 0) ? 3 : (NR >= 2 ? 2 : 1);
 #pragma unroll 1
     for (int f0 = 0; f0 < NR; f0 += G2) {
       double a0[G2], a1[G2], a2[G2], al[G2], be[G2], bt[G2];
@@ -385,13 +392,14 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
           const int j = (int)k / M, i = (int)k - j * M;  // n < 2^31 (checked at launch)
           double nv[G2], zo[G2], qo[G2], so[G2], po[G2], mo[G2], wo[G2], uo[G2], ro[G2], xo[G2],
               di[G2];
-          // inpainting: a known entry is an identity row whose r, u, w, m and
-          // directions are 0 after the set-up sweeps and stay 0, and no
-          // unknown row reads it -- skip it (its dot-product terms are 0)
+          // inpainting and CSR: a known entry is an identity row whose r, u,
+          // w, m and directions are 0 after the set-up sweeps and stay 0, and
+          // no unknown row reads it -- skip it (its dot-product terms are 0)
+          constexpr bool kMasked = OP == OP_INPAINT || OP == OP_CSR;
           bool act[G2];
 #pragma unroll
           for (int q = 0; q < G2; ++q)
-            act[q] = live[q] && (OP != OP_INPAINT || A.mask[(long long)(f0 + q) * n + k]);
+            act[q] = live[q] && (!kMasked || A.mask[(long long)(f0 + q) * n + k]);
 #pragma unroll
           for (int q = 0; q < G2; ++q) {
             if (!act[q]) continue;

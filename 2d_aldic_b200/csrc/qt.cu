@@ -788,15 +788,16 @@ __global__ void k_qt_strain_gather(int n, const int *__restrict__ iptr, const in
   for (int c = 0; c < 4; ++c) F[4 * a + c] = cnt ? s[c] / cnt : 0.0;
 }
 
-// refill: bad nodes are unknowns of (L + t I) x = sum of good neighbours
-__global__ void k_qt_fill_prep(int n, int nf, const double *__restrict__ vals,
+// refill: bad nodes are unknowns of (L + t I) x = sum of good neighbours;
+// the nf interleaved fields of vals go to solver fields f0 .. f0 + nf - 1
+__global__ void k_qt_fill_prep(int n, int nf, int f0, const double *__restrict__ vals,
                                const unsigned char *__restrict__ bad, const int *__restrict__ row,
                                const int *__restrict__ col, double *__restrict__ b,
                                double *__restrict__ x, unsigned char *__restrict__ mask) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   for (int f = 0; f < nf; ++f) {
-    const long long o = (long long)f * n + a;
+    const long long o = (long long)(f0 + f) * n + a;
     if (bad[a]) {
       double s = 0.0;
       for (int p = row[a]; p < row[a + 1]; ++p) {
@@ -815,11 +816,11 @@ __global__ void k_qt_fill_prep(int n, int nf, const double *__restrict__ vals,
   }
 }
 
-__global__ void k_qt_fill_store(int n, int nf, const double *__restrict__ x,
+__global__ void k_qt_fill_store(int n, int nf, int f0, const double *__restrict__ x,
                                 const unsigned char *__restrict__ bad, double *__restrict__ vals) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n || !bad[a]) return;
-  for (int f = 0; f < nf; ++f) vals[(long long)a * nf + f] = x[(long long)f * n + a];
+  for (int f = 0; f < nf; ++f) vals[(long long)a * nf + f] = x[(long long)(f0 + f) * n + a];
 }
 
 inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
@@ -1032,16 +1033,25 @@ int qt_strain(aldic_qt_mesh &m, const double *U, double *F, cudaStream_t st) {
 
 int qt_fill(aldic_qt_mesh &m, GridWork &w, int nf, double *vals, const unsigned char *bad,
             cudaStream_t st) {
-  ALDIC_CHECK(nf >= 1 && nf <= 6, E_ARG, "qt_fill: 1..6 fields");
+  return qt_fill2(m, w, nf, vals, 0, nullptr, bad, st);
+}
+
+int qt_fill2(aldic_qt_mesh &m, GridWork &w, int nf1, double *vals1, int nf2, double *vals2,
+             const unsigned char *bad, cudaStream_t st) {
+  ALDIC_CHECK(nf1 >= 1 && nf2 >= 0 && nf1 + nf2 <= 6 && (nf2 == 0 || vals2), E_ARG,
+              "qt_fill: 1..6 fields");
   int rc;
   if ((rc = qt_upload(m, st))) return rc;
   const int n = m.n;
-  k_qt_fill_prep<<<nblk(n), 256, 0, st>>>(n, nf, vals, bad, m.d_arow.as<int>(), m.d_acol.as<int>(),
-                                          w.b, w.x, w.mask);
+  const int *row = m.d_arow.as<int>(), *col = m.d_acol.as<int>();
+  k_qt_fill_prep<<<nblk(n), 256, 0, st>>>(n, nf1, 0, vals1, bad, row, col, w.b, w.x, w.mask);
+  if (nf2)
+    k_qt_fill_prep<<<nblk(n), 256, 0, st>>>(n, nf2, nf1, vals2, bad, row, col, w.b, w.x, w.mask);
   ALDIC_CUDA(cudaGetLastError());
-  const CsrOp op{m.d_arow.as<int>(), m.d_acol.as<int>(), m.d_aval.as<double>(), m.d_adiag.as<double>()};
-  if ((rc = csr_pcg(w, op, n, nf, kQtRtol, kQtMaxit, st))) return rc;
-  k_qt_fill_store<<<nblk(n), 256, 0, st>>>(n, nf, w.x, bad, vals);
+  const CsrOp op{row, col, m.d_aval.as<double>(), m.d_adiag.as<double>()};
+  if ((rc = csr_pcg(w, op, n, nf1 + nf2, kQtRtol, kQtMaxit, st))) return rc;
+  k_qt_fill_store<<<nblk(n), 256, 0, st>>>(n, nf1, 0, w.x, bad, vals1);
+  if (nf2) k_qt_fill_store<<<nblk(n), 256, 0, st>>>(n, nf2, nf1, w.x, bad, vals2);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

@@ -52,6 +52,9 @@ int qt_strain(aldic_qt_mesh &m, const double *U, double *F, cudaStream_t st);
 // bad[k] != 0 from the graph Laplacian of the mesh edges
 int qt_fill(aldic_qt_mesh &m, GridWork &w, int nf, double *vals, const unsigned char *bad,
             cudaStream_t st);
+// the same for two interleaved arrays (nf1 + nf2 <= 6 fields) in one solve
+int qt_fill2(aldic_qt_mesh &m, GridWork &w, int nf1, double *vals1, int nf2, double *vals2,
+             const unsigned char *bad, cudaStream_t st);
 
 constexpr double kQtFillTether = 1e-6;
 
