@@ -579,9 +579,22 @@ __device__ __forceinline__ void done_102(const Args &a, long long s, int lane) {
 enum { MODE_FULL = 0, MODE_SETUP = 1, MODE_ITER = 2 };
 
 // ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
-// S_f[6] at 57, S[6] at 63 and 1 / diag(L) at 69 (kept out of registers to
-// raise occupancy)
-constexpr int WS = 76;
+// S_f[6] at 57, S[6] at 63, 1 / diag(L) at 69, the warp parameters P[6] at 76
+// and per-subset constants at 82 (x0, y0, the window's top-left offsets,
+// bf, Subpb1's 2x2 factor, the first gradient norm) and at 92 the FP32
+// evaluation's fixed inputs (EvalBase) -- values every lane holds alike,
+// kept out of registers so that the evaluation's column loop has them to
+// itself (fewer spills) and more warps stay resident
+constexpr int WS = 98;
+
+// the per-subset inputs of eval32 that stay fixed over the iterations
+struct EvalBase {
+  const float4 *rc;
+  const float2 *gxy;
+  int nw, w;
+  float ox, oy, fx0, fy0, cg, pad;
+};
+static_assert(sizeof(EvalBase) <= 6 * sizeof(double), "EvalBase fits its scratch slots");
 
 template <typename Real, bool SUB, int MODE>
 __device__ void process(const Args &a, long long s, int lane, double *ws) {
@@ -762,17 +775,22 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     }
   }
   }  // setup pass
-  double P[6];
-  if (SUB) {
-    for (int q = 0; q < 4; ++q) P[q] = a.FOld[4 * s + q];
-  } else {
-    // funICGN.m:39 starts from P = [0 0 0 0 u v]; an external guess may give
-    // the gradient terms too
-    for (int q = 0; q < 4; ++q) P[q] = a.F0 ? a.F0[4 * s + q] : 0.0;
-  }
-  P[4] = a.U0[2 * s];
-  P[5] = a.U0[2 * s + 1];
+  // P and the subset's constants in the warp's scratch (written by lane 0;
+  // funICGN.m:39 starts from P = [0 0 0 0 u v], an external guess may give
+  // the gradient terms too)
+  double *const Pw = ws + 76, *const Gw = ws + 82;
   const double bf = sqrt(ssf);
+  __syncwarp();
+  if (lane == 0) {
+    for (int q = 0; q < 4; ++q) Pw[q] = SUB ? a.FOld[4 * s + q] : (a.F0 ? a.F0[4 * s + q] : 0.0);
+    Pw[4] = a.U0[2 * s];
+    Pw[5] = a.U0[2 * s + 1];
+    Gw[0] = x0;
+    Gw[1] = y0;
+    Gw[2] = oxd;
+    Gw[3] = oyd;
+    Gw[4] = bf;
+  }
 
   // ---- Hessian factor (IC-GN) or the damped 2x2 system (Subpb1)
   double *Hm = ws;
@@ -821,27 +839,51 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     l11i = 1.0 / l11;
     l21 = H2b * l11i;
     l22i = 1.0 / sqrt(Hd - l21 * l21);
+    if (lane == 0) {
+      Gw[5] = s2;
+      Gw[6] = l11i;
+      Gw[7] = l21;
+      Gw[8] = l22i;
+    }
   }
+  __syncwarp();
 
   // ---- iterations (funICGN.m:107-294 / funICGN_Subpb1.m:94-337)
   const double tol = a.tol;
-  double normNew = 1, normAbs = 1, normInit = 1;
+  double normNew = 1, normAbs = 1;
   int step = 0;
   const Real cg = (Real)meanf;
   // u22 = x0 + ru: split x0 into its floor xb and fraction (0 or 1/2)
   const double xbd = floor(x0), ybd = floor(y0);
   const int xb = (int)xbd, yb = (int)ybd;
   const Real fx0 = (Real)(x0 - xbd), fy0 = (Real)(y0 - ybd);
+  EvalBase *const eb = reinterpret_cast<EvalBase *>(ws + 92);
+  if (sizeof(Real) == 4 && lane == 0) {
+    eb->rc = im.gc + ((long long)(yb - 2) * W + (xb - 1));
+    eb->gxy = im.gxy + base;
+    eb->nw = nw;
+    eb->w = w;
+    eb->ox = (float)ox;
+    eb->oy = (float)oy;
+    eb->fx0 = (float)fx0;
+    eb->fy0 = (float)fy0;
+    eb->cg = (float)cg;
+  }
+  __syncwarp();
   while (step <= 100 && normNew > tol && normAbs > tol) {
     step++;
+    double P[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) P[q] = Pw[q];
     // out-of-image test (funICGN.m:118): an affine map takes its extremes at
     // the subset corners
     bool out = false;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const double X = (c & 1) ? oxd + w : oxd, Y = (c & 2) ? oyd + w : oyd;
-      const double u22 = (1 + P[0]) * X + P[2] * Y + (x0 + P[4]);
-      const double v22 = P[1] * X + (1 + P[3]) * Y + (y0 + P[5]);
+      const int wv = sizeof(Real) == 4 ? eb->w : w;
+      const double X = (c & 1) ? Gw[2] + wv : Gw[2], Y = (c & 2) ? Gw[3] + wv : Gw[3];
+      const double u22 = (1 + P[0]) * X + P[2] * Y + (Gw[0] + P[4]);
+      const double v22 = P[1] * X + (1 + P[3]) * Y + (Gw[1] + P[5]);
       out |= (u22 < 3 || u22 > W - 2 || v22 < 3 || v22 > im.H - 2);
     }
     if (out) {
@@ -857,12 +899,12 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       for (int q = 0; q < 8; ++q) sums[q] = nan64();
     } else if constexpr (sizeof(Real) == 4) {
       Eval32 e;
-      e.rc = im.gc + ((long long)(yb - 2) * W + (xb - 1));
-      e.gxy = im.gxy + base;
-      e.W = W; e.nw = nw;
-      e.ox = (float)ox; e.oy = (float)oy;
+      e.rc = eb->rc;
+      e.gxy = eb->gxy;
+      e.W = W; e.nw = eb->nw;
+      e.ox = eb->ox; e.oy = eb->oy;
       e.a11 = (float)(1 + P[0]); e.a12 = (float)P[2]; e.a21 = (float)P[1]; e.a22 = (float)(1 + P[3]);
-      e.c4 = (float)P[4] + (float)fx0; e.c5 = (float)P[5] + (float)fy0; e.cg = (float)cg;
+      e.c4 = (float)P[4] + eb->fx0; e.c5 = (float)P[5] + eb->fy0; e.cg = eb->cg;
       float o[8];
       eval32<SUB>(e, lane, o);
 #pragma unroll
@@ -908,13 +950,15 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) sums[2 + q] = (SUB && q < 4) ? 0.0 : warp_sum((double)t[q]);
     }
-    const double n = (double)npx;
+    __syncwarp();  // (P and the constants are read again from the scratch)
+    const double n = sizeof(Real) == 4 ? (double)(eb->nw * eb->nw) : (double)npx;
     const double gm = sums[0] / n;                 // mean(g) - c
     const double ssg = sums[1] - sums[0] * gm;     // sum (g - gbar)^2
     const double bg = sqrt(ssg);
     // b_k = bf (S_fk / bf - (T_k - gm S_k) / bg) = S_fk - (bf / bg)(T_k - gm S_k)
     // (a flat reference subset, bf = 0, stays NaN as the division gives it)
-    const double rfg = bf > 0.0 ? bf / bg : nan64();
+    const double bfw = Gw[4];
+    const double rfg = bfw > 0.0 ? bfw / bg : nan64();
     double b[6], nb = 0;
     if (!SUB) {
 #pragma unroll
@@ -925,13 +969,15 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
     } else {
       const double b5 = Sfs[4] - rfg * (sums[6] - gm * Sks[4]);
       const double b6 = Sfs[5] - rfg * (sums[7] - gm * Sks[5]);
-      b[4] = b5 * s2 + a.mu * (P[4] - a.U0[2 * s] - a.vdual[2 * s]);
-      b[5] = b6 * s2 + a.mu * (P[5] - a.U0[2 * s + 1] - a.vdual[2 * s + 1]);
+      const double s2w = Gw[5];
+      b[4] = b5 * s2w + a.mu * (Pw[4] - a.U0[2 * s] - a.vdual[2 * s]);
+      b[5] = b6 * s2w + a.mu * (Pw[5] - a.U0[2 * s + 1] - a.vdual[2 * s + 1]);
       nb = b[4] * b[4] + b[5] * b[5];
     }
     normNew = sqrt(nb);
     normAbs = normNew;
-    if (step == 1) normInit = normNew;
+    const double normInit = step == 1 ? normNew : Gw[9];
+    if (step == 1 && lane == 0) Gw[9] = normNew;
     if (normInit > tol) normNew = normNew / normInit;
     else normNew = 0;
     if (normNew < tol || normAbs < tol) break;
@@ -947,21 +993,29 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       }
     } else {
       // 2x2 SPD solve with the Cholesky factor of the damped matrix
-      const double y1 = b[4] * l11i, y2 = (b[5] - l21 * y1) * l22i;
-      const double x2 = y2 * l22i, x1 = (y1 - l21 * x2) * l11i;
+      const double f11i = Gw[6], f21 = Gw[7], f22i = Gw[8];
+      const double y1 = b[4] * f11i, y2 = (b[5] - f21 * y1) * f22i;
+      const double x2 = y2 * f22i, x1 = (y1 - f21 * x2) * f11i;
       dP[4] = -x1;
       dP[5] = -x2;
     }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) P[q] = Pw[q];
     if (!ic_compose(P, dP)) break;
+    __syncwarp();
+    if (lane == 0)
+      for (int q = 0; q < 6; ++q) Pw[q] = P[q];
+    __syncwarp();
   }
+  __syncwarp();
   if (!(normNew < tol || normAbs < tol)) step = 101;
   if (isnan(normNew)) step = 101;
   if (lane == 0) {
     a.iters[s] = step;
-    a.U[2 * s] = P[4];
-    a.U[2 * s + 1] = P[5];
+    a.U[2 * s] = Pw[4];
+    a.U[2 * s + 1] = Pw[5];
     if (!SUB) {
-      for (int q = 0; q < 4; ++q) a.F[4 * s + q] = P[q];
+      for (int q = 0; q < 4; ++q) a.F[4 * s + q] = Pw[q];
       if (MODE == MODE_FULL) {
         int idx = 0;
         for (int c = 0; c < 6; ++c)
