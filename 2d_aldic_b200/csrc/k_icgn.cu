@@ -581,11 +581,13 @@ enum { MODE_FULL = 0, MODE_SETUP = 1, MODE_ITER = 2 };
 // ws: per-warp shared scratch, H[36] at 0, its Cholesky factor L[21] at 36,
 // S_f[6] at 57, S[6] at 63, 1 / diag(L) at 69, the warp parameters P[6] at 76
 // and per-subset constants at 82 (x0, y0, the window's top-left offsets,
-// bf, Subpb1's 2x2 factor, the first gradient norm) and at 92 the FP32
-// evaluation's fixed inputs (EvalBase) -- values every lane holds alike,
+// bf, Subpb1's 2x2 factor, the first gradient norm), at 92 the FP32
+// evaluation's fixed inputs (EvalBase) and at 98 the Eval32 block of the
+// current evaluation, which eval32 reads from there -- values every lane
+// holds alike,
 // kept out of registers so that the evaluation's column loop has them to
 // itself (fewer spills) and more warps stay resident
-constexpr int WS = 98;
+constexpr int WS = 108;
 
 // the per-subset inputs of eval32 that stay fixed over the iterations
 struct EvalBase {
@@ -595,6 +597,7 @@ struct EvalBase {
   float ox, oy, fx0, fy0, cg, pad;
 };
 static_assert(sizeof(EvalBase) <= 6 * sizeof(double), "EvalBase fits its scratch slots");
+static_assert(sizeof(Eval32) <= 10 * sizeof(double), "Eval32 fits its scratch slots");
 
 template <typename Real, bool SUB, int MODE>
 __device__ void process(const Args &a, long long s, int lane, double *ws) {
@@ -898,15 +901,20 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) sums[q] = nan64();
     } else if constexpr (sizeof(Real) == 4) {
-      Eval32 e;
-      e.rc = eb->rc;
-      e.gxy = eb->gxy;
-      e.W = W; e.nw = eb->nw;
-      e.ox = eb->ox; e.oy = eb->oy;
-      e.a11 = (float)(1 + P[0]); e.a12 = (float)P[2]; e.a21 = (float)P[1]; e.a22 = (float)(1 + P[3]);
-      e.c4 = (float)P[4] + eb->fx0; e.c5 = (float)P[5] + eb->fy0; e.cg = eb->cg;
+      Eval32 *const ep = reinterpret_cast<Eval32 *>(ws + 98);
+      if (lane == 0) {
+        Eval32 e;
+        e.rc = eb->rc;
+        e.gxy = eb->gxy;
+        e.W = W; e.nw = eb->nw;
+        e.ox = eb->ox; e.oy = eb->oy;
+        e.a11 = (float)(1 + P[0]); e.a12 = (float)P[2]; e.a21 = (float)P[1]; e.a22 = (float)(1 + P[3]);
+        e.c4 = (float)P[4] + eb->fx0; e.c5 = (float)P[5] + eb->fy0; e.cg = eb->cg;
+        *ep = e;
+      }
+      __syncwarp();
       float o[8];
-      eval32<SUB>(e, lane, o);
+      eval32<SUB>(*ep, lane, o);
 #pragma unroll
       for (int q = 0; q < 8; ++q) sums[q] = (SUB && q >= 2 && q < 6) ? 0.0 : warp_sum((double)o[q]);
     } else {
