@@ -1356,7 +1356,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32, 4) k_search_peak(const PeakAr
     const int gix = (int)(pt % A.nx), giy = (int)(pt / A.nx);
     const size_t ps = (size_t)((giy / A.tsy) * A.tiles_x + gix / kTileTSX) * NS +
                       (giy % A.tsy) * kTileTSX + gix % kTileTSX;
-    const TileSub P = A.subs[ps];
+    const TileSub &P = A.subs[ps];  // fields loaded where used (L1), not held in registers
     const long long out_idx = (long long)giy + (long long)gix * A.ny;
     const int px = A.px1 + gix * A.step, py = A.py1 + giy * A.step;
     const int ii = px + 1, jj = py + 1;  // 1-based
