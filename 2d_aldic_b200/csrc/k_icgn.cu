@@ -191,6 +191,35 @@ __device__ __forceinline__ float floor_i(float x, int *i) {
   return t - 12582912.0f;
 }
 
+// Transposed butterfly over the warp: NV partial sums a lane (NV a power of
+// two up to 32).  At each level a lane keeps the half of its values that its
+// partner gives away and adds the partner's copy of that half, so NV sums
+// take NV - 1 exchanges (then plain butterfly levels once a lane holds one)
+// instead of NV butterflies of five.  Afterwards v[0] of lane l holds the
+// total of value l >> (5 - log2 NV).  Each total is formed from the same
+// pairs in the same order as warp_sum's (own partial + partner's), so the
+// values are bit-identical to NV warp_sum calls.
+template <int NV>
+__device__ __forceinline__ double warp_sum_t(double (&v)[NV], int lane) {
+#pragma unroll
+  for (int lvl = 0; lvl < 5; ++lvl) {
+    const int o = 16 >> lvl;
+    const int m = NV >> lvl;  // values a lane still holds
+    if (m > 1) {
+      const bool hi = (lane & o) != 0;
+#pragma unroll
+      for (int i = 0; i < m / 2; ++i) {
+        const double lo_v = v[i], hi_v = v[i + m / 2];
+        const double send = hi ? lo_v : hi_v, keep = hi ? hi_v : lo_v;
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    }
+  }
+  return v[0];
+}
+
 // Packed (two-lane) FP32 arithmetic of sm_100: two IEEE single-precision
 // operations per instruction.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
@@ -731,25 +760,28 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
         continue;
       }
     }
-    A1 = warp_sum((double)a1);
-    A2 = warp_sum((double)a2);
+    {
+      // the 32 sums in one transposed butterfly: lane l ends with sum l of
+      // [a1, a2, S_k (6), sum sd_k (f - c) (6, corrected to f - mean f
+      // below), the 18 distinct Hessian sums (staged in ws[0..17] until H is
+      // expanded in place below)]
+      double v[32];
+      v[0] = (double)a1;
+      v[1] = (double)a2;
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      const double vk = (SUB && q < 4) ? 0.0 : warp_sum((double)sk[q]);
-      const double vf = (SUB && q < 4) ? 0.0 : warp_sum((double)sfk[q]);
-      if (lane == 0) {
-        Sks[q] = vk;
-        Sfs[q] = vf;  // sum sd_k (f - c); corrected to f - mean f below
+      for (int q = 0; q < 6; ++q) {
+        v[2 + q] = (double)sk[q];
+        v[8 + q] = (double)sfk[q];
       }
-    }
-    if (!SUB) {
-      // the 18 distinct Hessian sums are staged in ws[0..17] (lane 0) until
-      // H is expanded in place below
 #pragma unroll
-      for (int q = 0; q < 18; ++q) {
-        const double v = warp_sum((double)hh[q]);
-        if (lane == 0) ws[q] = v;
-      }
+      for (int q = 0; q < 18; ++q) v[14 + q] = (double)hh[q];
+      const double t = warp_sum_t<32>(v, lane);
+      A1 = __shfl_sync(0xffffffffu, t, 0);
+      A2 = __shfl_sync(0xffffffffu, t, 1);
+      if (lane >= 2 && lane < 8) Sks[lane - 2] = (SUB && lane < 6) ? 0.0 : t;
+      else if (lane >= 8 && lane < 14) Sfs[lane - 8] = (SUB && lane < 12) ? 0.0 : t;
+      else if (!SUB && lane >= 14) ws[lane - 14] = t;
+      __syncwarp();
     }
     break;
   }
@@ -915,8 +947,22 @@ __device__ void process(const Args &a, long long s, int lane, double *ws) {
       __syncwarp();
       float o[8];
       eval32<SUB>(*ep, lane, o);
+      if (SUB) {  // o[0], o[1], o[6], o[7]: totals at lanes 0, 8, 16, 24
+        double v[4] = {(double)o[0], (double)o[1], (double)o[6], (double)o[7]};
+        const double t = warp_sum_t<4>(v, lane);
+        sums[0] = __shfl_sync(0xffffffffu, t, 0);
+        sums[1] = __shfl_sync(0xffffffffu, t, 8);
+        sums[6] = __shfl_sync(0xffffffffu, t, 16);
+        sums[7] = __shfl_sync(0xffffffffu, t, 24);
+        sums[2] = sums[3] = sums[4] = sums[5] = 0.0;
+      } else {  // totals at lanes 0, 4, .., 28
+        double v[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) sums[q] = (SUB && q >= 2 && q < 6) ? 0.0 : warp_sum((double)o[q]);
+        for (int q = 0; q < 8; ++q) v[q] = (double)o[q];
+        const double t = warp_sum_t<8>(v, lane);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) sums[q] = __shfl_sync(0xffffffffu, t, 4 * q);
+      }
     } else {
       const Real *gI = im.g64;
       const Grad64 grad(im);
