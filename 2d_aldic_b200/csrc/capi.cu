@@ -1823,9 +1823,11 @@ int aldic_qt_frame(aldic_ctx *c, const aldic_qt_frame_params *p, aldic_qt_mesh *
   // ---- Section 5: beta sweep, Subpb2Quadtree, nodal strain (main_ALDIC_Quadtree.m:175-207)
   const double mu = p->mu;
   const double betas[3] = {1e-3 * step * step * mu, 1e-2 * step * step * mu, 1e-1 * step * step * mu};
+  // the three systems in one 6-field solve, then each candidate's strain and
+  // the two norms (U2, F2 end as candidate 2's, as the sequential sweep left them)
+  if ((rc = qt_subpb2_sweep(m, c->gw, betas, mu, Q.U1, Q.F1, st))) return rc;
   for (int k = 0; k < 3; ++k) {
-    if ((rc = qt_subpb2(m, c->gw, betas[k], mu, Q.U1, Q.F1, Q.U2, st)) ||
-        (rc = qt_strain(m, Q.U2, Q.F2, st)) ||
+    if ((rc = qt_store_candidate(m, c->gw, k, Q.U2, st)) || (rc = qt_strain(m, Q.U2, Q.F2, st)) ||
         (rc = vdiffnorm(Q.U1, Q.U2, 2 * n, part, nrm + k, st)) ||
         (rc = vdiffnorm(Q.F1, Q.F2, 4 * n, part, nrm + 4 + k, st)))
       return rc;

@@ -109,7 +109,8 @@ __device__ __forceinline__ double op_diag(const PcgArgs &A, double beta, int i, 
   } else if (OP == OP_FD) {
     return beta * (fd_diag1(i, M) + fd_diag1(j, N)) / (4.0 * A.h * A.h) + A.mu;
   } else if (OP == OP_CSR) {
-    return A.mask[(long long)f * M * N + k] ? A.csr.diag[k] : 1.0;
+    if (!A.mask[(long long)f * M * N + k]) return 1.0;
+    return A.csr.valM ? beta * A.csr.diag[k] + A.mu * A.csr.diagM[k] : A.csr.diag[k];
   } else if (OP == OP_GRIDFIT) {
     const double w = A.ata ? A.ata[9 * k + 4] : (A.mask[(long long)f * M * N + k] ? 1.0 : 0.0);
     const int na = (i > 0) + (i < M - 1) + (j > 0) + (j < N - 1);
@@ -153,9 +154,16 @@ __device__ __forceinline__ double op_apply(const PcgArgs &A, double beta, int i,
     if (!fr[k]) return v[k];
     double y = 0.0;
     const int p1 = A.csr.row[k + 1];
-    for (int p = A.csr.row[k]; p < p1; ++p) {
-      const int c = A.csr.col[p];
-      if (fr[c]) y += A.csr.val[p] * v[c];
+    if (A.csr.valM) {
+      for (int p = A.csr.row[k]; p < p1; ++p) {
+        const int c = A.csr.col[p];
+        if (fr[c]) y += (beta * A.csr.val[p] + A.mu * A.csr.valM[p]) * v[c];
+      }
+    } else {
+      for (int p = A.csr.row[k]; p < p1; ++p) {
+        const int c = A.csr.col[p];
+        if (fr[c]) y += A.csr.val[p] * v[c];
+      }
     }
     return y;
   } else if (OP == OP_GRIDFIT) {
@@ -213,7 +221,12 @@ __device__ __forceinline__ double op_apply_dir(const PcgArgs &A, double beta, in
   if (OP == OP_CSR) {
     double y = 0.0;
     const int p1 = A.csr.row[k + 1];
-    for (int p = A.csr.row[k]; p < p1; ++p) y += A.csr.val[p] * v[A.csr.col[p]];
+    if (A.csr.valM) {
+      for (int p = A.csr.row[k]; p < p1; ++p)
+        y += (beta * A.csr.val[p] + A.mu * A.csr.valM[p]) * v[A.csr.col[p]];
+    } else {
+      for (int p = A.csr.row[k]; p < p1; ++p) y += A.csr.val[p] * v[A.csr.col[p]];
+    }
     return y;
   }
   if (OP == OP_INPAINT) {
@@ -1091,7 +1104,7 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
 }
 
 int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, int maxit,
-            cudaStream_t st) {
+            cudaStream_t st, const double *beta_each, double mu) {
   ALDIC_CHECK(nrhs >= 1 && nrhs <= 6, E_ARG, "csr_pcg: 1..6 right-hand sides");
   ALDIC_CHECK(n >= 1 && n < (1LL << 31), E_ARG, "csr_pcg: bad size");
   int dev = 0, sms = 148;
@@ -1120,8 +1133,8 @@ int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, in
     ALDIC_CUDA(cudaMemsetAsync(w.mask + nrhs * n, 0, (size_t)(nr_pad - nrhs) * n, st));
   }
   A.M = (int)n; A.N = 1; A.nrhs = nr_pad; A.maxit = maxit; A.blocks = (int)blocks;
-  for (int f = 0; f < MAXRHS; ++f) A.beta[f] = 0.0;
-  A.mu = 0; A.h = 1; A.lam2 = 0; A.rtol = rtol;
+  for (int f = 0; f < MAXRHS; ++f) A.beta[f] = (beta_each && f < nrhs) ? beta_each[f] : 0.0;
+  A.mu = mu; A.h = 1; A.lam2 = 0; A.rtol = rtol;
   A.gs.count = w.bar; A.gs.gen = w.bar + 1; A.gs.err = w.err;
   A.iters_out = w.iters_out;
   A.beta_ptr = nullptr;

@@ -140,12 +140,15 @@ int finite_strain(long long n, int type, const double *F, double *out, cudaStrea
 // columns), its diagonal, shared by every field.  Rows whose field mask is 0
 // are identity rows; columns whose mask is 0 are skipped (their values were
 // moved to the right-hand side).
+// A CSR operator; with valM / diagM set, field f's matrix is
+// beta[f] val + mu valM (a stiffness and a mass part on one pattern)
 struct CsrOp {
   const int *row, *col;
   const double *val, *diag;
+  const double *valM = nullptr, *diagM = nullptr;
 };
 int csr_pcg(GridWork &w, const CsrOp &op, long long n, int nrhs, double rtol, int maxit,
-            cudaStream_t st);
+            cudaStream_t st, const double *beta_each = nullptr, double mu = 0.0);
 
 // ---- BF16 tensor-core GEMM (k_gemm.cu): D = A . B^T over K
 enum GemmMode { GEMM_ROW = 0, GEMM_PATCH = 1, GEMM_TRANS = 2, GEMM_PATCHT = 3 };

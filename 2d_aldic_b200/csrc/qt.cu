@@ -37,7 +37,7 @@ SlabCache &slab_cache() {
 void aldic_qt_mesh::release() {
   aldic::DevBuf *b[] = {&d_coords, &d_elems, &d_row, &d_col, &d_dpos, &d_iptr, &d_inc, &d_ipos,
                         &d_kind, &d_val, &d_diag, &d_ke, &d_be, &d_es, &d_arow, &d_acol,
-                        &d_aval, &d_adiag};
+                        &d_aval, &d_adiag, &d_valM, &d_diagM};
   for (auto *x : b) {  // views into the slab
     x->p = nullptr;
     x->cap = 0;
@@ -717,6 +717,48 @@ __global__ void k_qt_elim(int n, const int *__restrict__ row, const int *__restr
   }
 }
 
+// The beta sweep's three systems from the stiffness (valK, b fields 0-1)
+// and mass (valM, b fields 2-3) parts: for beta[q], fields 2q, 2q + 1 of b,
+// x and mask as k_qt_elim sets them for beta[q] K + mu M, and the two
+// diagonals (each node reads its own four b entries before writing six).
+struct QtBetas {
+  double v[3];
+};
+__global__ void k_qt_elim3(int n, const int *__restrict__ row, const int *__restrict__ col,
+                           const double *__restrict__ valK, const double *__restrict__ valM,
+                           const int *__restrict__ dpos, const unsigned char *__restrict__ kind,
+                           const double *__restrict__ U, QtBetas be, double mu,
+                           double *__restrict__ b, double *__restrict__ x,
+                           unsigned char *__restrict__ mask, double *__restrict__ diagK,
+                           double *__restrict__ diagM) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int kd = kind[a];
+  diagK[a] = kd == 2 ? 1.0 : valK[dpos[a]];
+  diagM[a] = kd == 2 ? 0.0 : valM[dpos[a]];
+  const double bK[2] = {b[a], b[(long long)n + a]};
+  const double bM[2] = {b[2LL * n + a], b[3LL * n + a]};
+  for (int q = 0; q < 3; ++q)
+    for (int f = 0; f < 2; ++f) {
+      const long long o = (long long)(2 * q + f) * n + a;
+      if (kd == 0) {
+        double s = be.v[q] * bK[f] + mu * bM[f];
+        for (int p = row[a]; p < row[a + 1]; ++p) {
+          const int c = col[p];
+          if (kind[c] == 1) s -= (be.v[q] * valK[p] + mu * valM[p]) * U[2 * c + f];
+        }
+        b[o] = s;
+        x[o] = U[2 * a + f];
+        mask[o] = 1;
+      } else {
+        const double v = kd == 1 ? U[2 * a + f] : 0.0;
+        b[o] = v;
+        x[o] = v;
+        mask[o] = 0;
+      }
+    }
+}
+
 __global__ void k_qt_store(int n, const double *__restrict__ x, double *__restrict__ Uhat) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
@@ -963,6 +1005,8 @@ int qt_upload(aldic_qt_mesh &m, cudaStream_t st) {
       {&m.d_adiag, adiag.data(), sizeof(double) * adiag.size()},
       {&m.d_val, nullptr, sizeof(double) * (col.size() + 1)},
       {&m.d_diag, nullptr, sizeof(double) * n},
+      {&m.d_valM, nullptr, sizeof(double) * (col.size() + 1)},
+      {&m.d_diagM, nullptr, sizeof(double) * n},
       {&m.d_ke, nullptr, sizeof(double) * 64 * ne},
       {&m.d_be, nullptr, sizeof(double) * 16 * ne},
       {&m.d_es, nullptr, sizeof(double) * 16 * ne},
@@ -1015,6 +1059,45 @@ int qt_subpb2(aldic_qt_mesh &m, GridWork &w, double beta, double mu, const doubl
   const CsrOp op{m.d_row.as<int>(), m.d_col.as<int>(), m.d_val.as<double>(), m.d_diag.as<double>()};
   if ((rc = csr_pcg(w, op, n, 2, kQtRtol, kQtMaxit, st))) return rc;
   k_qt_store<<<nblk(n), 256, 0, st>>>(n, w.x, Uhat);
+  ALDIC_CUDA(cudaGetLastError());
+  return OK;
+}
+
+int qt_subpb2_sweep(aldic_qt_mesh &m, GridWork &w, const double beta[3], double mu,
+                    const double *U, const double *F, cudaStream_t st) {
+  int rc;
+  if ((rc = qt_upload(m, st))) return rc;
+  const int n = m.n, ne = m.ne;
+  const double *cx = m.d_coords.as<double>(), *cy = cx + n;
+  // stiffness part (beta 1, mu 0) into d_val and b fields 0-1, mass part
+  // (beta 0, mu 1) into d_valM and b fields 2-3
+  for (int part = 0; part < 2; ++part) {
+    k_qt_elem<<<nblk(8LL * ne), 256, 0, st>>>(ne, m.d_elems.as<int>(), cx, cy, part ? 0.0 : 1.0,
+                                              part ? 1.0 : 0.0, U, F, m.d_ke.as<double>(),
+                                              m.d_be.as<double>());
+    k_qt_gather<<<nblk(n), 256, 0, st>>>(n, m.d_iptr.as<int>(), m.d_inc.as<int>(),
+                                         m.d_ipos.as<int>(), m.d_row.as<int>(), m.d_ke.as<double>(),
+                                         m.d_be.as<double>(),
+                                         (part ? m.d_valM : m.d_val).as<double>(),
+                                         w.b + 2LL * part * n);
+  }
+  QtBetas be;
+  for (int q = 0; q < 3; ++q) be.v[q] = beta[q];
+  k_qt_elim3<<<nblk(n), 256, 0, st>>>(n, m.d_row.as<int>(), m.d_col.as<int>(), m.d_val.as<double>(),
+                                      m.d_valM.as<double>(), m.d_dpos.as<int>(),
+                                      m.d_kind.as<unsigned char>(), U, be, mu, w.b, w.x, w.mask,
+                                      m.d_diag.as<double>(), m.d_diagM.as<double>());
+  ALDIC_CUDA(cudaGetLastError());
+  CsrOp op{m.d_row.as<int>(), m.d_col.as<int>(), m.d_val.as<double>(), m.d_diag.as<double>()};
+  op.valM = m.d_valM.as<double>();
+  op.diagM = m.d_diagM.as<double>();
+  const double be6[6] = {beta[0], beta[0], beta[1], beta[1], beta[2], beta[2]};
+  return csr_pcg(w, op, n, 6, kQtRtol, kQtMaxit, st, be6, mu);
+}
+
+int qt_store_candidate(aldic_qt_mesh &m, const GridWork &w, int q, double *Uhat, cudaStream_t st) {
+  ALDIC_CHECK(q >= 0 && q < 3, E_ARG, "qt_store_candidate: candidate 0..2");
+  k_qt_store<<<nblk(m.n), 256, 0, st>>>(m.n, w.x + 2LL * q * m.n, Uhat);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }

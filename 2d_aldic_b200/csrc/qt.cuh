@@ -28,6 +28,7 @@ struct aldic_qt_mesh {
   aldic::DevBuf d_iptr, d_inc, d_ipos;  // node -> (element*8 + slot), scatter map
   aldic::DevBuf d_kind;          // 0 free, 1 Dirichlet, 2 in no element
   aldic::DevBuf d_val, d_diag, d_ke, d_be, d_es;
+  aldic::DevBuf d_valM, d_diagM;  // mass part of the operator (the beta sweep's split)
   aldic::DevBuf d_arow, d_acol, d_aval, d_adiag;  // refill graph Laplacian
   aldic::DevBuf slab;            // one allocation; the arrays above are views into it
   void release();
@@ -50,6 +51,12 @@ int qt_subpb2(aldic_qt_mesh &m, GridWork &w, double beta, double mu, const doubl
 int qt_strain(aldic_qt_mesh &m, const double *U, double *F, cudaStream_t st);
 // refill of flagged nodes: nf interleaved fields (stride nf) at nodes with
 // bad[k] != 0 from the graph Laplacian of the mesh edges
+// the beta sweep of Subpb2Quadtree: the three systems (beta[q], mu) in one
+// 6-field solve (stiffness and mass parts assembled apart), candidate q in
+// solver fields 2q, 2q + 1; qt_store_candidate interleaves candidate q
+int qt_subpb2_sweep(aldic_qt_mesh &m, GridWork &w, const double beta[3], double mu,
+                    const double *U, const double *F, cudaStream_t st);
+int qt_store_candidate(aldic_qt_mesh &m, const GridWork &w, int q, double *Uhat, cudaStream_t st);
 int qt_fill(aldic_qt_mesh &m, GridWork &w, int nf, double *vals, const unsigned char *bad,
             cudaStream_t st);
 // the same for two interleaved arrays (nf1 + nf2 <= 6 fields) in one solve
