@@ -1527,10 +1527,16 @@ int frame_device(aldic_ctx *c, const aldic_frame_params *p, const FrameBufs &B, 
       be[2 * k] = be[2 * k + 1] = b6[k] = bl[k] * base;
       if (fd && (rc = rhs(bl[k] * base, nullptr, 2 * k))) return rc;
     }
-    if (!fd && (rc = fe_rhs_sweep(c->gw, M, N, h, b6, mu, B.U1, B.F1, B.udual, B.vdual, st)))
-      return rc;
-    // the six systems of the sweep in one launch (12 right-hand sides)
-    if ((rc = pcg(12, nullptr, be))) return rc;
+    if (fd) {
+      // the six systems of the sweep in one launch (12 right-hand sides)
+      if ((rc = pcg(12, nullptr, be))) return rc;
+    } else {
+      // the right-hand side is linear in beta: its two parts, transformed
+      // once, give the six systems' solutions
+      if ((rc = fe_rhs_parts(c->gw, M, N, h, B.U1, B.F1, B.udual, B.vdual, st)) ||
+          (rc = fdm_solve_sweep(c->fdm, b6, c->gw.b, c->gw.x, c->gw.r, mu, st)))
+        return rc;
+    }
     if (fd) {
       for (int k = 0; k < 6; ++k) {
         if ((rc = store(2 * k))) return rc;

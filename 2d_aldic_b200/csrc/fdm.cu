@@ -501,6 +501,71 @@ int fdm_solve(const FdmBasis &B, int nrhs, const double *b, double *x, double *t
   return gemm(g, nrhs, B.part, st);
 }
 
+// The beta sweep's eigen-domain solutions from the two transformed
+// right-hand-side parts C4 (fields 0-1 beta part, 2-3 mu part; entry
+// (q, p) at q M + p): X field 2k + c = (beta_k F_c + mu U_c) /
+// (beta_k (ly[q] + lx[p]) + mu), the divisor of the one-system epilogue.
+struct SweepBetas {
+  double v[6];
+};
+__global__ void k_fdm_sweep_combine(int M, int N, const double *__restrict__ ly,
+                                    const double *__restrict__ lx, SweepBetas be, double mu,
+                                    const double *__restrict__ C4, double *__restrict__ X) {
+  const long long n = (long long)M * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(idx / M), p = (int)(idx - (long long)q * M);
+    const double lam = ly[q] + lx[p];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const double F = C4[c * n + idx], U = C4[(2 + c) * n + idx];
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        X[(2 * k + c) * n + idx] = (be.v[k] * F + mu * U) / (be.v[k] * lam + mu);
+    }
+  }
+}
+
+int fdm_solve_sweep(const FdmBasis &B, const double beta[6], const double *b, double *x,
+                    double *tmp, double mu, cudaStream_t st) {
+  ALDIC_CHECK(B.buf.p, E_ARG, "fdm sweep: no basis");
+  const int M = B.M, N = B.N;
+  const long long n = (long long)M * N;
+  GemmArgs g{};
+  g.mu = mu;
+  int rc;
+  // 1. T = B_f Vx for the two parts (4 fields) -> tmp fields 0-3
+  g.A = b; g.sab = n; g.sar = M; g.sak = 1;
+  g.B = B.Vx; g.sbb = 0; g.sbk = M; g.sbc = 1;
+  g.C = tmp; g.scb = n; g.scr = M; g.scc = 1;
+  g.R = N; g.Cn = M; g.K = M; g.scale = 0;
+  if ((rc = gemm(g, 4, B.part, st))) return rc;
+  // 2. C = Vy' T, unscaled -> tmp fields 4-7
+  g.A = B.Vy; g.sab = 0; g.sar = 1; g.sak = N;
+  g.B = tmp; g.sbb = n; g.sbk = M; g.sbc = 1;
+  g.C = tmp + 4 * n; g.scb = n; g.scr = M; g.scc = 1;
+  g.R = N; g.Cn = M; g.K = N; g.scale = 0;
+  if ((rc = gemm(g, 4, B.part, st))) return rc;
+  // the six systems' scaled eigen-domain solutions -> x fields 0-11
+  SweepBetas be;
+  for (int k = 0; k < 6; ++k) be.v[k] = beta[k];
+  const long long nb = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+  k_fdm_sweep_combine<<<(unsigned)nb, 256, 0, st>>>(M, N, B.ly, B.lx, be, mu, tmp + 4 * n, x);
+  ALDIC_CUDA(cudaGetLastError());
+  // 3. S = C Vx' -> tmp (12 fields)
+  g.A = x; g.sab = n; g.sar = M; g.sak = 1;
+  g.B = B.Vx; g.sbb = 0; g.sbk = 1; g.sbc = M;
+  g.C = tmp; g.scb = n; g.scr = M; g.scc = 1;
+  g.R = N; g.Cn = M; g.K = M; g.scale = 0;
+  if ((rc = gemm(g, 12, B.part, st))) return rc;
+  // 4. X = Vy S -> x
+  g.A = B.Vy; g.sab = 0; g.sar = N; g.sak = 1;
+  g.B = tmp; g.sbb = n; g.sbk = M; g.sbc = 1;
+  g.C = x; g.scb = n; g.scr = M; g.scc = 1;
+  g.R = N; g.Cn = M; g.K = N; g.scale = 0;
+  return gemm(g, 12, B.part, st);
+}
+
 }  // namespace aldic
 
 extern "C" ALDIC_API int aldic_fdm_basis(int type, int n, double h, double *V, double *lam) {

@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs A) {
 // operations for each as a single one), and the solve's start x = U with every
 // entry unknown: fields (2q, 2q + 1) of b and x for beta[q].
 struct FeBetas {
-  double v[6];
+  double v[6], m[6];  // beta and mu of each right-hand side
 };
 template <int NB>
 __global__ void k_fe_rhs(int M, int N, double h, FeBetas be, const double *beta_ptr, double mu,
@@ -537,8 +537,8 @@ __global__ void k_fe_rhs(int M, int N, double h, FeBetas be, const double *beta_
             }
 #pragma unroll
             for (int q = 0; q < NB; ++q) {
-              bu[q] += s * (be.v[q] * (gx * fw0 + gy * fw1) + mu * Nn[la] * nu);
-              bv[q] += s * (be.v[q] * (gx * fw2 + gy * fw3) + mu * Nn[la] * nv);
+              bu[q] += s * (be.v[q] * (gx * fw0 + gy * fw1) + be.m[q] * Nn[la] * nu);
+              bv[q] += s * (be.v[q] * (gx * fw2 + gy * fw3) + be.m[q] * Nn[la] * nv);
             }
           }
       }
@@ -1152,19 +1152,20 @@ int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const do
   const long long n = (long long)M * N;
   FeBetas be{};
   be.v[0] = beta;
+  be.m[0] = mu;
   k_fe_rhs<1><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, beta_ptr, mu, U, F, udual, vdual,
                                              w.b + f0 * n, w.x + f0 * n, w.mask + f0 * n);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
 }
 
-int fe_rhs_sweep(GridWork &w, int M, int N, double h, const double beta[6], double mu,
-                 const double *U, const double *F, const double *udual, const double *vdual,
-                 cudaStream_t st) {
+int fe_rhs_parts(GridWork &w, int M, int N, double h, const double *U, const double *F,
+                 const double *udual, const double *vdual, cudaStream_t st) {
   const long long n = (long long)M * N;
-  FeBetas be;
-  for (int q = 0; q < 6; ++q) be.v[q] = beta[q];
-  k_fe_rhs<6><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, nullptr, mu, U, F, udual, vdual, w.b,
+  FeBetas be{};
+  be.v[0] = 1.0;  // fields 0-1: the beta part (beta 1, mu 0)
+  be.m[1] = 1.0;  // fields 2-3: the mu part (beta 0, mu 1)
+  k_fe_rhs<2><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, nullptr, 0.0, U, F, udual, vdual, w.b,
                                              w.x, w.mask);
   ALDIC_CUDA(cudaGetLastError());
   return OK;

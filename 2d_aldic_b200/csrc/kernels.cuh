@@ -114,6 +114,11 @@ int fdm_ensure(FdmBasis &B, int type, int M, int N, double h, cudaStream_t st);
 // else beta_each[f] if given, else beta; tmp: nrhs*M*N doubles
 int fdm_solve(const FdmBasis &B, int nrhs, const double *b, double *x, double *tmp, double mu,
               double beta, const double *beta_each, const double *beta_ptr, cudaStream_t st);
+// the beta sweep's six systems at once from the two right-hand-side parts
+// (b fields 0-1: beta part, 2-3: mu part): x fields 2q, 2q + 1 solve
+// (beta[q] K + mu M) x = beta[q] b_beta + mu b_mu; tmp holds 12 fields
+int fdm_solve_sweep(const FdmBasis &B, const double beta[6], const double *b, double *x,
+                    double *tmp, double mu, cudaStream_t st);
 
 // Finite-difference Subproblem 2 (funDerivativeOp.m, main_ALDIC.m:243-278):
 // (beta D'D + mu I) x = beta D' a + mu b on the interior (M-2) x (N-2) nodes,
@@ -204,10 +209,10 @@ int grid_pcg(GridWork &w, int op, int M, int N, int nrhs, double beta, double mu
 int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const double *U,
            const double *F, const double *udual, const double *vdual, cudaStream_t st,
            const double *beta_ptr = nullptr, int f0 = 0);
-// the six right-hand sides of the beta sweep (beta[q] into fields 2q, 2q + 1)
-int fe_rhs_sweep(GridWork &w, int M, int N, double h, const double beta[6], double mu,
-                 const double *U, const double *F, const double *udual, const double *vdual,
-                 cudaStream_t st);
+// the two parts of the Subpb2 right-hand side, linear in beta and mu: the
+// beta part into fields 0-1, the mu part into 2-3 (for the beta sweep)
+int fe_rhs_parts(GridWork &w, int M, int N, double h, const double *U, const double *F,
+                 const double *udual, const double *vdual, cudaStream_t st);
 // interleave w.x (2 fields from slot f0) into Uhat
 int fe_store(const GridWork &w, int M, int N, double *Uhat, cudaStream_t st, int f0 = 0);
 // nodal strain (funGlobal_NodalStrainAvg.m)
