@@ -491,7 +491,7 @@ struct FeBetas {
   double v[6], m[6];  // beta and mu of each right-hand side
 };
 template <int NB>
-__global__ void k_fe_rhs(int M, int N, double h, FeBetas be, const double *beta_ptr, double mu,
+__global__ void k_fe_rhs(int M, int N, double h, FeBetas be, const double *beta_ptr,
                          const double *__restrict__ U, const double *__restrict__ F,
                          const double *__restrict__ ud, const double *__restrict__ vd,
                          double *__restrict__ b, double *__restrict__ x,
@@ -1153,7 +1153,7 @@ int fe_rhs(GridWork &w, int M, int N, double h, double beta, double mu, const do
   FeBetas be{};
   be.v[0] = beta;
   be.m[0] = mu;
-  k_fe_rhs<1><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, beta_ptr, mu, U, F, udual, vdual,
+  k_fe_rhs<1><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, beta_ptr, U, F, udual, vdual,
                                              w.b + f0 * n, w.x + f0 * n, w.mask + f0 * n);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
@@ -1165,7 +1165,7 @@ int fe_rhs_parts(GridWork &w, int M, int N, double h, const double *U, const dou
   FeBetas be{};
   be.v[0] = 1.0;  // fields 0-1: the beta part (beta 1, mu 0)
   be.m[1] = 1.0;  // fields 2-3: the mu part (beta 0, mu 1)
-  k_fe_rhs<2><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, nullptr, 0.0, U, F, udual, vdual, w.b,
+  k_fe_rhs<2><<<blocks_for(n), 256, 0, st>>>(M, N, h, be, nullptr, U, F, udual, vdual, w.b,
                                              w.x, w.mask);
   ALDIC_CUDA(cudaGetLastError());
   return OK;
