@@ -46,6 +46,9 @@ def test_config2_frame_matches_oracle(aldic, c2, prec):
     rms = float(np.sqrt(np.mean(dU ** 2)))
     print(f"config 2 {prec}: max |dU| {np.abs(dU).max():.3g} px, RMS {rms:.3g} px, "
           f"max |dF| {np.abs(dF).max():.3g}, beta {r['stats']['beta']:.6g} vs {ro['beta']:.6g}")
+    # the beta sweep (its six systems solved from the right-hand side's two
+    # parts, the errors in one pass) selects the oracle's beta
+    assert r["stats"]["beta"] == pytest.approx(ro["beta"], rel=1e-6)
     if prec == "fp64":
         assert np.abs(dU).max() < 1e-4 and np.abs(dF).max() < 1e-4
     else:
