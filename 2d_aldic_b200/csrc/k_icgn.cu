@@ -7,10 +7,13 @@
 // lane, lane+32, ... of the (w+1)^2 subset.  Per iteration a lane samples the
 // deformed image at its warped pixels (Keys bicubic, a = -1/2, as
 // ba_interp2.cpp) and accumulates 8 residual sums in the working precision;
-// the warp reduces them in FP64 with a butterfly (every lane ends with the
-// identical value, so control flow stays warp-uniform), and every lane then
-// forms b, the convergence test and dP = -H\b with the FP64 Cholesky factor
-// of H, and applies the inverse-compositional update in FP64.
+// the warp reduces them in FP64 in one transposed butterfly (warp_sum_t:
+// lane 4q ends with sum q, then every lane reads all eight, so control flow
+// stays warp-uniform), and every lane then forms b, the convergence test and
+// dP = -H\b with the FP64 Cholesky factor of H, and applies the
+// inverse-compositional update in FP64.  State every lane holds alike (P,
+// the subset's constants, the evaluation's inputs) lives in the warp's
+// shared scratch rather than in registers.
 //
 // FP32 sampling reads the row-cubic coefficients of the deformed image
 // (row_cubic: per pixel the Keys cubic of its row around that floor column,
