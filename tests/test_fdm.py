@@ -134,3 +134,36 @@ def test_fd_operator_is_the_kronecker_sum(aldic, M, N):
         for f in (0, 1):
             X = fdm_apply_inverse(Vx, lx, Vy, ly, beta, mu, rhs[f::2].reshape(Ni, Mi))
             np.testing.assert_allclose(X.reshape(-1), ref[iU][f::2], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("M,N", [(9, 7), (16, 23)])
+def test_fe_beta_sweep_from_the_right_hand_side_parts(aldic, M, N):
+    """The identity fdm_solve_sweep rests on: the Subpb2 right-hand side is
+    beta b(1, 0) + mu b(0, 1), so transforming the two parts once and forming
+    (beta C_beta + mu C_mu) / (beta (ly + lx) + mu) in the eigen domain gives
+    each of the sweep's six systems' solutions."""
+    rng = np.random.default_rng(5)
+    h, mu = 8.0, 1e-3
+    n = M * N
+    U = rng.standard_normal(2 * n)
+    F = 0.01 * rng.standard_normal(4 * n)
+    ud = 0.001 * rng.standard_normal(4 * n)
+    vd = 0.01 * rng.standard_normal(2 * n)
+    Vx, lx = basis(aldic, FDM_FE, M, h)
+    Vy, ly = basis(aldic, FDM_FE, N, h)
+    _, b_beta = subpb2_system(M, N, h, 1.0, 0.0, U, F, ud, vd)
+    _, b_mu = subpb2_system(M, N, h, 0.0, 1.0, U, F, ud, vd)
+    lam = ly[:, None] + lx[None, :]
+    base = h * h * mu
+    for k, scale in enumerate((1e-3, 1e-5 ** 0.5, 1e-2, 1e-3 ** 0.5, 1e-1, 1e-1 ** 0.5)):
+        beta = scale * base
+        A, b = subpb2_system(M, N, h, beta, mu, U, F, ud, vd)
+        np.testing.assert_allclose(b, beta * b_beta + mu * b_mu, rtol=1e-12,
+                                   atol=1e-14 * np.abs(b).max())
+        ref = spla.spsolve(A.tocsc(), b)
+        for f in (0, 1):
+            Cb = Vy.T @ b_beta[f::2].reshape(N, M) @ Vx
+            Cm = Vy.T @ b_mu[f::2].reshape(N, M) @ Vx
+            X = Vy @ ((beta * Cb + mu * Cm) / (beta * lam + mu)) @ Vx.T
+            np.testing.assert_allclose(X.reshape(-1), ref[f::2], rtol=1e-10,
+                                       atol=1e-10 * np.abs(ref).max())
